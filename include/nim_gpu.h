@@ -1,0 +1,216 @@
+/*
+ * nim_gpu.h -- C ABI of the B200 (sm_100a) NIM time-advance library.
+ *
+ * The reference solver (ijarrah2/NIM-CONV22-SHARED, Fortran 90 + OpenMP)
+ * advances incompressible Navier-Stokes + Boussinesq energy with the nodal
+ * integral method by calling argument-less subroutines that work on module
+ * globals (src/parameters.f90:222-292).  This header replaces those calls
+ * with plain-C entry points taking pointers and sizes; a Fortran host binds
+ * them with iso_c_binding (the interface block is in INTEGRATION.md).
+ *
+ * Conventions
+ *   - Every entry point returns an int status: NIM_OK (0) or a negative
+ *     NIM_ERR_* code; nim_gpu_strerror() turns it into text.
+ *   - Arrays crossing the boundary use the reference's own layout:
+ *     column-major (component, index) with 1-based cell / face / node
+ *     numbers, exactly as meshes_faces(1:6,1:NMESH) etc. in
+ *     src/parameters.f90.  The library copies what it needs during the
+ *     call and never keeps a host pointer.
+ *   - A context is bound to the CUDA device that is current when it is
+ *     created and to its own stream; calls on one context must come from one
+ *     host thread at a time (the reference runs single-threaded, run.sh:2).
+ *   - Device state stays resident between calls; host copies happen only in
+ *     nim_gpu_create, nim_gpu_download and nim_gpu_upload.
+ */
+#ifndef NIM_GPU_H
+#define NIM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+  NIM_OK = 0,
+  NIM_ERR_BAD_ARG = -1,       /* null pointer, bad size, unsupported mesh   */
+  NIM_ERR_CUDA = -2,          /* a CUDA runtime call failed                 */
+  NIM_ERR_NOT_CONVERGED = -3, /* inner loop hit max_iters (nse.f90:129 has
+                                 no cap; this is the added guard)           */
+  NIM_ERR_NONFINITE = -4,     /* NaN/Inf seen by the fused error reduction  */
+  NIM_ERR_TIMEOUT = -5,       /* a bounded device wait expired              */
+  NIM_ERR_STATE = -6          /* call out of order (e.g. step before init)  */
+};
+
+/* BC ids of the cylinder case, create_geometry.f90:474-594:
+   1 interior, 2 bottom (z=0), 3 top (z=L), 4 inner hexagon, 5 outer wall. */
+#define NIM_NBC 5
+
+/* Fields for nim_gpu_download / nim_gpu_upload, in reference names. */
+typedef enum nim_field {
+  NIM_FIELD_FACES_U = 0,     /* faces_u(NFACE)          */
+  NIM_FIELD_FACES_V = 1,     /* faces_v(NFACE)          */
+  NIM_FIELD_FACES_W = 2,     /* faces_w(NFACE)          */
+  NIM_FIELD_FACES_P = 3,     /* faces_p(NFACE)          */
+  NIM_FIELD_FACES_T = 4,     /* faces_T(NFACE)          */
+  NIM_FIELD_MESHES_U = 5,    /* meshes_uxyz(NMESH)      */
+  NIM_FIELD_MESHES_V = 6,    /* meshes_vxyz(NMESH)      */
+  NIM_FIELD_MESHES_W = 7,    /* meshes_wxyz(NMESH)      */
+  NIM_FIELD_MESHES_T = 8,    /* meshes_Txyz(NMESH)      */
+  NIM_FIELD_MESHES_U_OLD = 9,   /* meshes_uxyz_old       */
+  NIM_FIELD_MESHES_V_OLD = 10,  /* meshes_vxyz_old       */
+  NIM_FIELD_MESHES_W_OLD = 11,  /* meshes_wxyz_old       */
+  NIM_FIELD_MESHES_T_OLD = 12,  /* meshes_Txyz_old       */
+  NIM_FIELD_MESHES_UT = 13,  /* meshes_uxyzt (time average, nse.f90:1299) */
+  NIM_FIELD_MESHES_VT = 14,  /* meshes_vxyzt            */
+  NIM_FIELD_MESHES_WT = 15,  /* meshes_wxyzt            */
+  NIM_FIELD_MESHES_TT = 16,  /* meshes_Txyzt            */
+  NIM_FIELD_MESHES_P = 17,   /* meshes_p (face mean, nse.f90:1307)        */
+  NIM_FIELD_MESHES_DILA = 18,/* meshes_dila (evaluate_D, nse.f90:2530)    */
+  /* init-time geometry (read-only; download only) */
+  NIM_FIELD_MESHES_VOLUME = 32,  /* meshes_volume(NMESH)                  */
+  NIM_FIELD_FACES_AREA = 33,     /* faces_area(NFACE)                     */
+  NIM_FIELD_FACES_NORMAL = 34,   /* faces_normal(3,NFACE)                 */
+  NIM_FIELD_FACES_MID = 35,      /* faces_mid_coordinates(3,NFACE)        */
+  NIM_FIELD_MESHES_GIJ = 36,     /* meshes_gij(3,3,NMESH)                 */
+  NIM_FIELD_MESHES_XI_X = 37,    /* meshes_xi_x(3,3,NMESH)                */
+  NIM_FIELD_MESHES_G = 38,       /* (G1,G2,G3) as (3,NMESH)               */
+  NIM_FIELD_MESHES_GIJ_FACES = 39,/* meshes_gij_faces(3,3,6,NMESH)        */
+  NIM_FIELD_FACES_TANGENTIAL = 40,   /* faces_tangential(3,NFACE)         */
+  NIM_FIELD_FACES_BITANGENTIAL = 41, /* faces_bitangential(3,NFACE)       */
+  NIM_FIELD_BCS_FACES_A = 42,    /* BCs_faces_a(1:5,tot_faces_bcs) used   */
+  NIM_FIELD_BCS_FACES_AP = 43,   /* BCs_faces_ap(8,tot_faces_bcs)         */
+  NIM_FIELD_AA_PX = 44,          /* AA_px(15,NMESH) (0 where no +neighbour)*/
+  NIM_FIELD_AA_PY = 45,
+  NIM_FIELD_AA_PZ = 46,
+  /* per-step NIM coefficients (download only) */
+  NIM_FIELD_M_F4 = 48,           /* M_F4(8,NMESH)                         */
+  NIM_FIELD_M_F1 = 49,           /* M_F1(5,NMESH)                         */
+  NIM_FIELD_M_F2 = 50,
+  NIM_FIELD_M_F3 = 51
+} nim_field;
+
+/*
+ * Mesh as the reference host builds it (create_hollow, prepare_mesh,
+ * fill_global_arrays: create_geometry.f90:321-664, prepare_mesh.f90:11-183,
+ * geometry.f90:978-1032).  All index arrays are 1-based, column-major.
+ * The library accepts the structured O-grid these routines produce
+ * (n_theta x n_r x n_z cells, periodic in theta); create() verifies the
+ * connectivity against that pattern and refuses anything else.
+ */
+typedef struct nim_mesh_desc {
+  int32_t n_theta, n_r, n_z;     /* NMESH_i, NMESH_j, NMESH_k               */
+  int32_t nnode, nmesh, nface;   /* NNODE, NMESH, NFACE (parameters.f90:115-119) */
+  int32_t nbcface;               /* tot_faces_bcs                           */
+  const double  *node_xyz;       /* (3,NNODE): NODES_ARRAY(:)%x,%y,%z       */
+  const int32_t *meshes_nodes;   /* (8,NMESH): MESHES_ARRAY(:)%nodes        */
+  const int32_t *meshes_faces;   /* (6,NMESH)                               */
+  const int32_t *meshes_neighbors; /* (6,NMESH), 0 = wall                   */
+  const int32_t *faces_bc;       /* (NFACE): faces_BC                       */
+  const int32_t *bcs_faces;      /* (tot_faces_bcs): BCs_faces             */
+  const int32_t *bcs_faces_id;   /* BCs_faces_id                            */
+  const int32_t *bcs_faces_position; /* BCs_faces_position (1..6)           */
+  const int32_t *bcs_faces_mesh_num; /* BCs_faces_mesh_num                  */
+} nim_mesh_desc;
+
+/*
+ * Run-time counterpart of the compile-time parameters in parameters.f90.
+ * nim_params_reference() fills the reference defaults.
+ */
+typedef struct nim_params {
+  double DT;            /* half-width of the NIM time element (parameters.f90:134);
+                           one step advances time by 2*DT (nse.f90:1296)       */
+  double nu, alpha, rho, g_beta;   /* parameters.f90:163-173                  */
+  double w_u, w_v, w_w, w_p, w_p2, w_T; /* relaxation (parameters.f90:152-157) */
+  double tol_u, tol_v, tol_w, tol_p, tol_T; /* parameters.f90:146-150          */
+  double v_limit;       /* exact/series switch on |cell Peclet| (parameters.f90:128) */
+  double dudt_epsilon;  /* steady-state threshold (parameters.f90:151)         */
+  double R_i, R_o;      /* radii in the Nusselt scaling of find_Nu2 (nse.f90:2794) */
+  /* Dirichlet value of each field on each BC id (general.f90:34-149), used as
+     constants integrated over the face like apply_dirichlet_bc_i (bc.f90:59-88).
+     Index [field][bc_id-1], field 0..4 = u, v, w, p, T. */
+  double bc_value[5][NIM_NBC];
+  int32_t max_iters;    /* cap on inner iterations per step (new guard)       */
+  int32_t check_steady; /* 1: stop nim_gpu_step when dudt,dTdt < dudt_epsilon
+                           (is_check_steady_state, nse.f90:60-69)              */
+  int32_t dpdx_tolerance; /* 1: err_p from pressure gradients (is_dpdx_tolerance,
+                           nse.f90:292-307)                                     */
+  int32_t reserved;
+} nim_params;
+
+/* Statistics of one time step (the values the reference prints at
+   nse.f90:169-171 and nse.f90:2793-2794, returned instead of printed). */
+typedef struct nim_step_stats {
+  int32_t step;         /* STEP before update_time_step                      */
+  int32_t iters;        /* inner iterations (cnt)                            */
+  double err_u, err_v, err_w, err_p, err_T;
+  double dilatation;    /* evaluate_D RMS continuity residual                */
+  double dudt_max, dTdt_max;  /* check_steady_state                          */
+  double nu_outer, nu_inner;  /* printed Nu_H (outer, position 2) and Nu_C
+                                 (inner hexagon = hot wall, position 1)      */
+  double area_outer, area_inner; /* sumA1, sumA2                            */
+  double time;          /* TI after update_time_step                         */
+  int32_t steady;       /* 1 if the steady-state test fired at this step     */
+  int32_t status;       /* NIM_OK or an error of this step                   */
+} nim_step_stats;
+
+typedef struct nim_ctx nim_ctx;
+
+/* Fill p with the reference defaults (parameters.f90, nim_formulation=2). */
+void nim_params_reference(nim_params *p);
+
+/* Copy the mesh and parameters to the device.  Replaces the module-global
+   allocation of parameters.f90:222-292.  *out receives the context. */
+int nim_gpu_create(const nim_mesh_desc *mesh, const nim_params *params,
+                   nim_ctx **out);
+
+/* Init-time geometry and constants: evaluate_all_mesh_constants
+   (geometry.f90:14-32), evaluate_pressure_bc_array (geometry.f90:879-975),
+   calculate_pressure_nim_constants (nim.f90:556-743),
+   find_derivatives_pressure_boundary (bc.f90:122-137) and
+   apply_all_dirichlet_bcs (bc.f90:13-19); sets TI=DT, STEP=1
+   (nse.f90:31-38). */
+int nim_gpu_init(nim_ctx *ctx);
+
+/* calculate_velocity_nim_constants_formulation2 (nim.f90:160-330). */
+int nim_gpu_begin_step(nim_ctx *ctx);
+
+/* integrate_nse (nse.f90:117-176) with the max_iters guard; fills
+   iters, err_u..err_T, dilatation, dudt_max, dTdt_max of *stats
+   (stats may be NULL). */
+int nim_gpu_integrate(nim_ctx *ctx, nim_step_stats *stats);
+
+/* Exactly n passes of the integrate_nse loop body (nse.f90:131-160) with no
+   convergence test: for step-by-step parity checks and fixed-work timing.
+   Fills iters and err_u..err_T of *stats (stats may be NULL). */
+int nim_gpu_iterate(nim_ctx *ctx, int32_t n, nim_step_stats *stats);
+
+/* update_time_step (nse.f90:1292-1313) + find_Nu2 (nse.f90:2699-2798);
+   fills step, nu_outer, nu_inner, area_outer, area_inner and time of
+   *stats (stats may be NULL). */
+int nim_gpu_end_step(nim_ctx *ctx, nim_step_stats *stats);
+
+/* nsteps iterations of the reference time loop (nse.f90:47-75) fully on
+   the device; per_step (may be NULL) receives nsteps records.  Stops early,
+   like the reference, when check_steady is set and the steady test fires;
+   *done (may be NULL) receives the number of steps advanced. */
+int nim_gpu_step(nim_ctx *ctx, int32_t nsteps, nim_step_stats *per_step,
+                 int32_t *done);
+
+/* Copy a field to/from host memory in the reference layout (for
+   write_data / write_restart / read_restart, postprocess.f90, restart.f90).
+   n = number of doubles the host buffer holds. */
+int nim_gpu_download(nim_ctx *ctx, nim_field field, double *host, int64_t n);
+int nim_gpu_upload(nim_ctx *ctx, nim_field field, const double *host, int64_t n);
+
+/* Block until all work queued on the context's stream has finished. */
+int nim_gpu_synchronize(nim_ctx *ctx);
+
+void nim_gpu_destroy(nim_ctx *ctx);
+const char *nim_gpu_strerror(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NIM_GPU_H */

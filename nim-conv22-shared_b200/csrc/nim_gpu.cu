@@ -1,0 +1,666 @@
+// Host side of the NIM CUDA library: the C ABI of include/nim_gpu.h.
+//
+// Replaces the OpenMP loops the reference runs from solve_nse (nse.f90:23-85):
+//   nim_gpu_init       initialize_nse + apply_all_dirichlet_bcs (nse.f90:31-38)
+//   nim_gpu_begin_step calculate_velocity_nim_constants_formulation2 (nse.f90:52)
+//   nim_gpu_integrate  integrate_nse (nse.f90:57, 117-176)
+//   nim_gpu_end_step   update_time_step + find_Nu2 (nse.f90:72-73)
+// The inner loop runs as CUDA graphs of whole iterations; the stop test lives
+// on the device (k_iter_end) and the host only polls it between batches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "nim_gpu.h"
+#include "nim_common.cuh"
+#include "nim_kernels.cuh"
+
+using namespace nim;
+
+namespace {
+
+const double MATH_PI = 3.14159265359;  // parameters.f90:31
+
+struct Buf {
+  void *p = nullptr;
+};
+
+}  // namespace
+
+struct nim_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Dims d{};
+  nim_params params{};
+  Phys phys{};
+  GaussRule gq{};
+  Geo g{};
+  Fields F{};
+  Ctrl *ctl = nullptr;       // device
+  Ctrl *ctl_host = nullptr;  // pinned mirror
+  double *node_xyz = nullptr;
+  double *bcv = nullptr;     // [5][5] Dirichlet constants
+  int *perm = nullptr;       // reference face number - 1 -> structured face index
+  double *scratch = nullptr; // gather/scatter staging [54*Nc or 3*NF]
+  double *sums = nullptr;    // [8] outputs of k_finish_sum
+  int nblk_c = 0, nblk_b = 0;
+  std::vector<void *> allocs;
+  cudaGraphExec_t graph = nullptr;
+  int graph_iters = 0;
+  bool initialized = false;
+  bool in_step = false;
+  int32_t STEP = 0;
+  double TI = 0;
+  int last_iters = 0;
+  double host_sums[8] = {0};
+};
+
+namespace {
+
+#define CK(call)                                                   \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) {                                       \
+      std::fprintf(stderr, "nim_gpu: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return NIM_ERR_CUDA;                                         \
+    }                                                              \
+  } while (0)
+
+template <typename T>
+int dalloc(nim_ctx *x, T **p, size_t n) {
+  void *q = nullptr;
+  CK(cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)));
+  CK(cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(T), x->stream));
+  x->allocs.push_back(q);
+  *p = static_cast<T *>(q);
+  return NIM_OK;
+}
+
+#define TRY(call)            \
+  do {                       \
+    int s_ = (call);         \
+    if (s_ != NIM_OK) return s_; \
+  } while (0)
+
+inline int grid(int n) { return (n + BLK - 1) / BLK; }
+
+inline double bits_to_double(unsigned long long b) {
+  double v;
+  std::memcpy(&v, &b, sizeof(v));
+  return v;
+}
+
+GaussRule make_gauss() {
+  GaussRule g;
+  g.x[0] = -(1. / 3. * std::sqrt(5. - 2. * std::sqrt(10. / 7.)));
+  g.x[1] = 1. / 3. * std::sqrt(5. - 2. * std::sqrt(10. / 7.));
+  g.x[2] = 0.;
+  g.x[3] = -(1. / 3. * std::sqrt(5. + 2. * std::sqrt(10. / 7.)));
+  g.x[4] = 1. / 3. * std::sqrt(5. + 2. * std::sqrt(10. / 7.));
+  g.w[0] = (322. + 13. * std::sqrt(70.)) / 900.;
+  g.w[1] = (322. + 13. * std::sqrt(70.)) / 900.;
+  g.w[2] = 128. / 225.;
+  g.w[3] = (322. - 13. * std::sqrt(70.)) / 900.;
+  g.w[4] = (322. - 13. * std::sqrt(70.)) / 900.;
+  return g;
+}
+
+// Check that the reference arrays describe the structured O-grid that
+// create_hollow + link_mesh produce, and build the face permutation.
+int verify_mesh(const nim_mesh_desc *m, const Dims &d, std::vector<int> &perm) {
+  const int NT = d.NT, NR = d.NR, NZ = d.NZ;
+  if ((int64_t)NT * (NR + 1) * (NZ + 1) != m->nnode || d.Nc != m->nmesh || d.NF != m->nface || d.NBF != m->nbcface)
+    return NIM_ERR_BAD_ARG;
+  perm.assign(d.NF, -1);
+  std::vector<char> seen(d.NF, 0);
+  for (int c = 0; c < d.Nc; ++c) {
+    const Cell x = Cell::of(d, c);
+    const int ip = (x.i == NT - 1) ? 0 : x.i + 1;
+    auto node = [&](int i, int j, int k) { return 1 + i + NT * (j + (NR + 1) * k); };
+    const int nd[8] = {node(x.i, x.j, x.k),      node(x.i, x.j + 1, x.k),      node(ip, x.j + 1, x.k),
+                       node(ip, x.j, x.k),       node(x.i, x.j, x.k + 1),      node(x.i, x.j + 1, x.k + 1),
+                       node(ip, x.j + 1, x.k + 1), node(ip, x.j, x.k + 1)};
+    for (int n = 0; n < 8; ++n)
+      if (m->meshes_nodes[8 * (size_t)c + n] != nd[n]) return NIM_ERR_BAD_ARG;
+    for (int pos = 1; pos <= 6; ++pos) {
+      const int nb = x.has_nb(d, pos) ? x.nb(d, pos).c + 1 : 0;
+      if (m->meshes_neighbors[6 * (size_t)c + pos - 1] != nb) return NIM_ERR_BAD_ARG;
+      const int rf = m->meshes_faces[6 * (size_t)c + pos - 1];
+      if (rf < 1 || rf > d.NF) return NIM_ERR_BAD_ARG;
+      const int sf = x.face(d, pos);
+      if (perm[rf - 1] == -1) {
+        if (seen[sf]) return NIM_ERR_BAD_ARG;
+        perm[rf - 1] = sf;
+        seen[sf] = 1;
+      } else if (perm[rf - 1] != sf) {
+        return NIM_ERR_BAD_ARG;
+      }
+      const int bc = m->faces_bc[rf - 1];
+      if (x.has_nb(d, pos) != (bc == 1)) return NIM_ERR_BAD_ARG;
+    }
+  }
+  for (int f = 0; f < d.NF; ++f)
+    if (perm[f] < 0) return NIM_ERR_BAD_ARG;
+  for (int b = 0; b < d.NBF; ++b) {
+    const BFace B = bface(d, b);
+    if (m->bcs_faces_position[b] != B.pos || m->bcs_faces_id[b] != B.id ||
+        m->bcs_faces_mesh_num[b] != B.cell.c + 1)
+      return NIM_ERR_BAD_ARG;
+    const int rf = m->bcs_faces[b];
+    if (rf < 1 || rf > d.NF || perm[rf - 1] != B.cell.face(d, B.pos) || m->faces_bc[rf - 1] != B.id)
+      return NIM_ERR_BAD_ARG;
+  }
+  return NIM_OK;
+}
+
+Phys make_phys(const nim_params &p) {
+  Phys P;
+  P.DT = p.DT; P.nu = p.nu; P.alpha = p.alpha; P.rho = p.rho; P.g_beta = p.g_beta;
+  P.w[0] = p.w_u; P.w[1] = p.w_v; P.w[2] = p.w_w; P.w[3] = p.w_T;
+  P.w_p = p.w_p; P.w_p2 = p.w_p2;
+  P.tol[0] = p.tol_u; P.tol[1] = p.tol_v; P.tol[2] = p.tol_w; P.tol[3] = p.tol_p; P.tol[4] = p.tol_T;
+  P.v_limit = p.v_limit; P.dudt_epsilon = p.dudt_epsilon; P.R_i = p.R_i; P.R_o = p.R_o;
+  const double Re = 1. / p.nu;
+  P.inv_Re = 1 / Re;
+  P.inv_rho = 1 / p.rho;
+  P.max_iters = p.max_iters;
+  P.dpdx_tolerance = p.dpdx_tolerance;
+  return P;
+}
+
+// one pass of integrate_nse's loop body
+int launch_iteration(nim_ctx *x) {
+  const Dims &d = x->d;
+  cudaStream_t s = x->stream;
+  const int gc = x->nblk_c, gb = x->nblk_b;
+  k_vel_cell<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_vel_face<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_p_src<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_p_bc<<<gb, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_p_bc_copy<<<gb, BLK, 0, s>>>(d, x->F, x->ctl);
+  k_p_face<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  if (x->phys.dpdx_tolerance) k_p_dpdx<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+  k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+  k_T_cell<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_T_face<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
+  CK(cudaGetLastError());
+  return NIM_OK;
+}
+
+int build_graph(nim_ctx *x, int iters) {
+  if (x->graph) {
+    cudaGraphExecDestroy(x->graph);
+    x->graph = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < iters; ++k) {
+    const int st = launch_iteration(x);
+    if (st != NIM_OK) {
+      cudaStreamEndCapture(x->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+  }
+  CK(cudaStreamEndCapture(x->stream, &g));
+  cudaError_t e = cudaGraphInstantiate(&x->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return NIM_ERR_CUDA;
+  x->graph_iters = iters;
+  return NIM_OK;
+}
+
+int read_ctrl(nim_ctx *x) {
+  CK(cudaMemcpyAsync(x->ctl_host, x->ctl, sizeof(Ctrl), cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  return NIM_OK;
+}
+
+__global__ void k_step_reset(Ctrl *ctl) {
+  ctl->done = 0;
+  ctl->step_iters = 0;
+  ctl->status = 0;
+  for (int q = 0; q < 4; ++q) ctl->red[q] = 0ull;
+}
+
+__global__ void k_run_reset(Ctrl *ctl) {
+  for (int p = 0; p < 2; ++p)
+    for (int q = 0; q < 8; ++q) ctl->err[p][q] = 0ull;
+  for (int q = 0; q < 8; ++q) ctl->wall_floor[q] = 0ull;
+  ctl->iter = 0;
+  ctl->step_iters = 0;
+  ctl->done = 0;
+  ctl->status = 0;
+  ctl->first = 1;
+}
+
+// dst[i*K + k] = src[k*stride + (perm ? perm[i] : i)]
+__global__ void k_gather(const double *__restrict__ src, size_t stride, int K, const int *__restrict__ perm, int n,
+                         double *__restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int s = perm ? perm[i] : i;
+  for (int k = 0; k < K; ++k) dst[(size_t)i * K + k] = src[(size_t)k * stride + s];
+}
+__global__ void k_scatter(const double *__restrict__ src, const int *__restrict__ perm, int n, double *dst0,
+                          double *dst1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int s = perm ? perm[i] : i;
+  dst0[s] = src[i];
+  if (dst1) dst1[s] = src[i];
+}
+
+struct FieldView {
+  const double *src = nullptr;
+  double *dst1 = nullptr;  // second half (face fields)
+  size_t stride = 0;
+  int K = 1, n = 0;
+  bool face = false, writable = false;
+};
+
+int field_view(nim_ctx *x, nim_field f, int par, FieldView &v) {
+  const Dims &d = x->d;
+  const size_t Nc = d.Nc, NF = d.NF, NB = d.NBF;
+  auto cellf = [&](double *p) { v.src = p; v.n = d.Nc; v.stride = Nc; v.writable = true; };
+  switch (f) {
+    case NIM_FIELD_FACES_U: case NIM_FIELD_FACES_V: case NIM_FIELD_FACES_W: case NIM_FIELD_FACES_P:
+    case NIM_FIELD_FACES_T: {
+      double *base = x->F.f[(int)f];
+      v.src = base + par * NF;
+      v.dst1 = base + (1 - par) * NF;
+      v.n = d.NF; v.stride = NF; v.face = true; v.writable = true;
+      return NIM_OK;
+    }
+    case NIM_FIELD_MESHES_U: case NIM_FIELD_MESHES_V: case NIM_FIELD_MESHES_W: case NIM_FIELD_MESHES_T:
+      cellf(x->F.c[(int)f - 5]); return NIM_OK;
+    case NIM_FIELD_MESHES_U_OLD: case NIM_FIELD_MESHES_V_OLD: case NIM_FIELD_MESHES_W_OLD:
+    case NIM_FIELD_MESHES_T_OLD:
+      cellf(x->F.co[(int)f - 9]); return NIM_OK;
+    case NIM_FIELD_MESHES_UT: case NIM_FIELD_MESHES_VT: case NIM_FIELD_MESHES_WT: case NIM_FIELD_MESHES_TT:
+      cellf(x->F.ct[(int)f - 13]); return NIM_OK;
+    case NIM_FIELD_MESHES_P: cellf(x->F.mp); return NIM_OK;
+    case NIM_FIELD_MESHES_DILA: cellf(x->F.dila); return NIM_OK;
+    default: break;
+  }
+  v.writable = false;
+  switch (f) {
+    case NIM_FIELD_MESHES_VOLUME: v.src = x->g.vol; v.n = d.Nc; v.stride = Nc; return NIM_OK;
+    case NIM_FIELD_FACES_AREA: v.src = x->g.area; v.n = d.NF; v.stride = NF; v.face = true; return NIM_OK;
+    case NIM_FIELD_FACES_NORMAL: v.src = x->g.normal; v.n = d.NF; v.stride = NF; v.K = 3; v.face = true; return NIM_OK;
+    case NIM_FIELD_FACES_MID: v.src = x->g.mid; v.n = d.NF; v.stride = NF; v.K = 3; v.face = true; return NIM_OK;
+    case NIM_FIELD_FACES_TANGENTIAL: v.src = x->g.tang; v.n = d.NF; v.stride = NF; v.K = 3; v.face = true; return NIM_OK;
+    case NIM_FIELD_FACES_BITANGENTIAL: v.src = x->g.bitang; v.n = d.NF; v.stride = NF; v.K = 3; v.face = true; return NIM_OK;
+    case NIM_FIELD_MESHES_GIJ: v.src = x->g.gij; v.n = d.Nc; v.stride = Nc; v.K = 9; return NIM_OK;
+    case NIM_FIELD_MESHES_XI_X: v.src = x->g.xi; v.n = d.Nc; v.stride = Nc; v.K = 9; return NIM_OK;
+    case NIM_FIELD_MESHES_G: v.src = x->g.G; v.n = d.Nc; v.stride = Nc; v.K = 3; return NIM_OK;
+    case NIM_FIELD_MESHES_GIJ_FACES: v.src = x->g.gf; v.n = d.Nc; v.stride = Nc; v.K = 54; return NIM_OK;
+    case NIM_FIELD_BCS_FACES_A: v.src = x->g.bca; v.n = d.NBF; v.stride = NB; v.K = 5; return NIM_OK;
+    case NIM_FIELD_BCS_FACES_AP: v.src = x->g.bcap; v.n = d.NBF; v.stride = NB; v.K = 8; return NIM_OK;
+    case NIM_FIELD_AA_PX: v.src = x->g.AA; v.n = d.Nc; v.stride = Nc; v.K = 15; return NIM_OK;
+    case NIM_FIELD_AA_PY: v.src = x->g.AA + 15 * Nc; v.n = d.Nc; v.stride = Nc; v.K = 15; return NIM_OK;
+    case NIM_FIELD_AA_PZ: v.src = x->g.AA + 30 * Nc; v.n = d.Nc; v.stride = Nc; v.K = 15; return NIM_OK;
+    case NIM_FIELD_M_F4: v.src = x->F.MF4; v.n = d.Nc; v.stride = Nc; v.K = 8; return NIM_OK;
+    case NIM_FIELD_M_F1: v.src = x->F.MF; v.n = d.Nc; v.stride = Nc; v.K = 5; return NIM_OK;
+    case NIM_FIELD_M_F2: v.src = x->F.MF + 5 * Nc; v.n = d.Nc; v.stride = Nc; v.K = 5; return NIM_OK;
+    case NIM_FIELD_M_F3: v.src = x->F.MF + 10 * Nc; v.n = d.Nc; v.stride = Nc; v.K = 5; return NIM_OK;
+    default: return NIM_ERR_BAD_ARG;
+  }
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+extern "C" void nim_params_reference(nim_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  const double Ra = 1.0E5, Pr = 0.7, g_beta = 1., th_tc = 1.;  // parameters.f90:166-170
+  p->DT = 0.01;
+  p->nu = 1. / std::sqrt(Ra / (g_beta * th_tc * Pr));
+  p->alpha = p->nu / Pr;
+  p->rho = 1.0;
+  p->g_beta = g_beta;
+  p->w_u = p->w_v = p->w_w = p->w_p = p->w_p2 = p->w_T = .4;
+  p->tol_u = p->tol_v = p->tol_w = p->tol_T = 1E-6;
+  p->tol_p = 5E-3;
+  p->v_limit = 1E-2;
+  p->dudt_epsilon = 1E-5;
+  p->R_i = 1.0 * (MATH_PI / 3.0);
+  p->R_o = 2.0;
+  p->bc_value[4][3] = 1.;  // T = 1 on BC 4 (general.f90:96-97)
+  p->max_iters = 100000;
+  p->check_steady = 1;
+  p->dpdx_tolerance = 0;
+}
+
+extern "C" const char *nim_gpu_strerror(int s) {
+  switch (s) {
+    case NIM_OK: return "ok";
+    case NIM_ERR_BAD_ARG: return "bad argument or unsupported mesh";
+    case NIM_ERR_CUDA: return "CUDA runtime error";
+    case NIM_ERR_NOT_CONVERGED: return "inner iteration reached max_iters";
+    case NIM_ERR_NONFINITE: return "non-finite value in the iteration";
+    case NIM_ERR_TIMEOUT: return "device wait timed out";
+    case NIM_ERR_STATE: return "call out of order";
+    default: return "unknown status";
+  }
+}
+
+static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) {
+  CK(cudaGetDevice(&x->device));
+  CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
+  x->d = make_dims(m->n_theta, m->n_r, m->n_z);
+  const Dims &d = x->d;
+  std::vector<int> perm;
+  TRY(verify_mesh(m, d, perm));
+  x->params = *p;
+  x->phys = make_phys(*p);
+  x->gq = make_gauss();
+  x->nblk_c = grid(d.Nc);
+  x->nblk_b = grid(d.NBF);
+  const size_t Nc = d.Nc, NF = d.NF, NB = d.NBF;
+  Geo &g = x->g;
+  TRY(dalloc(x, &g.vol, Nc));
+  TRY(dalloc(x, &g.G, 3 * Nc));
+  TRY(dalloc(x, &g.gij, 9 * Nc));
+  TRY(dalloc(x, &g.xi, 9 * Nc));
+  TRY(dalloc(x, &g.gf, 54 * Nc));
+  TRY(dalloc(x, &g.gfd, 6 * Nc));
+  TRY(dalloc(x, &g.dg, 6 * Nc));
+  TRY(dalloc(x, &g.area, NF));
+  TRY(dalloc(x, &g.normal, 3 * NF));
+  TRY(dalloc(x, &g.mid, 3 * NF));
+  TRY(dalloc(x, &g.tang, 3 * NF));
+  TRY(dalloc(x, &g.bitang, 3 * NF));
+  TRY(dalloc(x, &g.AA, 45 * Nc));
+  TRY(dalloc(x, &g.bcpts, 5 * NB));
+  TRY(dalloc(x, &g.bca, 5 * NB));
+  TRY(dalloc(x, &g.bcap, 8 * NB));
+  TRY(dalloc(x, &g.bcg, 2 * NB));
+  TRY(dalloc(x, &g.zf, 4 * NB));
+  TRY(dalloc(x, &g.nuw, 4 * NB));
+  TRY(dalloc(x, &g.bcval, 4 * NB));
+  Fields &F = x->F;
+  for (int q = 0; q < 5; ++q) TRY(dalloc(x, &F.f[q], 2 * NF));
+  for (int q = 0; q < 4; ++q) {
+    TRY(dalloc(x, &F.c[q], Nc));
+    TRY(dalloc(x, &F.co[q], Nc));
+    TRY(dalloc(x, &F.ct[q], Nc));
+  }
+  TRY(dalloc(x, &F.mp, Nc));
+  TRY(dalloc(x, &F.dila, Nc));
+  TRY(dalloc(x, &F.dila_old, Nc));
+  TRY(dalloc(x, &F.Rp, Nc));
+  TRY(dalloc(x, &F.MA, 18 * Nc));
+  TRY(dalloc(x, &F.MF4, 8 * Nc));
+  TRY(dalloc(x, &F.MF, 15 * Nc));
+  TRY(dalloc(x, &F.MTF, 15 * Nc));
+  TRY(dalloc(x, &F.dpd, 3 * Nc));
+  TRY(dalloc(x, &F.part, 8 * (size_t)std::max(x->nblk_c, grid(2 * d.NT * d.NZ))));
+  TRY(dalloc(x, &x->ctl, 1));
+  TRY(dalloc(x, &x->node_xyz, 3 * (size_t)m->nnode));
+  TRY(dalloc(x, &x->bcv, 25));
+  TRY(dalloc(x, &x->perm, NF));
+  TRY(dalloc(x, &x->scratch, std::max(54 * Nc, 3 * NF)));
+  TRY(dalloc(x, &x->sums, 8));
+  CK(cudaMallocHost(&x->ctl_host, sizeof(Ctrl)));
+  CK(cudaMemcpyAsync(x->node_xyz, m->node_xyz, 3 * sizeof(double) * m->nnode, cudaMemcpyHostToDevice, x->stream));
+  double bcv[25];
+  for (int f = 0; f < 5; ++f)
+    for (int b = 0; b < 5; ++b) bcv[5 * f + b] = p->bc_value[f][b];
+  CK(cudaMemcpyAsync(x->bcv, bcv, sizeof(bcv), cudaMemcpyHostToDevice, x->stream));
+  CK(cudaMemcpyAsync(x->perm, perm.data(), sizeof(int) * NF, cudaMemcpyHostToDevice, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  return NIM_OK;
+}
+
+extern "C" int nim_gpu_create(const nim_mesh_desc *m, const nim_params *p, nim_ctx **out) {
+  if (!m || !p || !out || !m->node_xyz || !m->meshes_nodes || !m->meshes_faces || !m->meshes_neighbors ||
+      !m->faces_bc || !m->bcs_faces || !m->bcs_faces_id || !m->bcs_faces_position || !m->bcs_faces_mesh_num)
+    return NIM_ERR_BAD_ARG;
+  if (m->n_theta < 6 || m->n_r < 3 || m->n_z < 3) return NIM_ERR_BAD_ARG;
+  if ((int64_t)m->n_theta * m->n_r * m->n_z > (int64_t)INT32_MAX / 4) return NIM_ERR_BAD_ARG;
+  if (!(p->DT > 0) || !(p->nu > 0) || !(p->alpha > 0) || !(p->rho > 0)) return NIM_ERR_BAD_ARG;
+  *out = nullptr;
+  nim_ctx *x = new (std::nothrow) nim_ctx();
+  if (!x) return NIM_ERR_BAD_ARG;
+  const int st = create_impl(m, p, x);
+  if (st != NIM_OK) {
+    nim_gpu_destroy(x);
+    return st;
+  }
+  *out = x;
+  return NIM_OK;
+}
+
+extern "C" int nim_gpu_init(nim_ctx *x) {
+  if (!x) return NIM_ERR_BAD_ARG;
+  CK(cudaSetDevice(x->device));
+  const Dims &d = x->d;
+  cudaStream_t s = x->stream;
+  k_run_reset<<<1, 1, 0, s>>>(x->ctl);
+  k_cell_geometry<<<x->nblk_c, BLK, 0, s>>>(d, x->gq, x->node_xyz, x->g);
+  k_metric_derived<<<x->nblk_c, BLK, 0, s>>>(d, x->g);
+  k_pressure_coeffs<<<x->nblk_c, BLK, 0, s>>>(d, x->g, x->params.rho);
+  k_bc_geometry<<<x->nblk_b, BLK, 0, s>>>(d, x->gq, x->node_xyz, x->g, x->params.rho, x->bcv);
+  // initial conditions: zero (general.f90:16-31), then the Dirichlet faces
+  const size_t Nc = d.Nc, NF = d.NF;
+  for (int q = 0; q < 5; ++q) CK(cudaMemsetAsync(x->F.f[q], 0, 2 * NF * sizeof(double), s));
+  for (int q = 0; q < 4; ++q) {
+    CK(cudaMemsetAsync(x->F.c[q], 0, Nc * sizeof(double), s));
+    CK(cudaMemsetAsync(x->F.co[q], 0, Nc * sizeof(double), s));
+    CK(cudaMemsetAsync(x->F.ct[q], 0, Nc * sizeof(double), s));
+  }
+  CK(cudaMemsetAsync(x->F.dpd, 0, 3 * Nc * sizeof(double), s));
+  CK(cudaMemsetAsync(x->F.dila, 0, Nc * sizeof(double), s));
+  CK(cudaMemsetAsync(x->F.mp, 0, Nc * sizeof(double), s));
+  k_apply_dirichlet<<<x->nblk_b, BLK, 0, s>>>(d, x->g, x->F);
+  k_wall_floor<<<x->nblk_b, BLK, 0, s>>>(d, x->g, x->ctl);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  x->TI = x->params.DT;  // nse.f90:31
+  x->STEP = 1;           // nse.f90:32
+  x->initialized = true;
+  x->in_step = false;
+  x->last_iters = 0;
+  return NIM_OK;
+}
+
+extern "C" int nim_gpu_begin_step(nim_ctx *x) {
+  if (!x) return NIM_ERR_BAD_ARG;
+  if (!x->initialized) return NIM_ERR_STATE;
+  const Dims &d = x->d;
+  k_step_reset<<<1, 1, 0, x->stream>>>(x->ctl);
+  k_vel_coef_A<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->g, x->F, x->phys);
+  k_vel_coef_F<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->F, x->phys);
+  CK(cudaGetLastError());
+  x->in_step = true;
+  return NIM_OK;
+}
+
+static int fill_iter_stats(nim_ctx *x, nim_step_stats *s) {
+  if (!s) return NIM_OK;
+  const Ctrl &c = *x->ctl_host;
+  s->step = x->STEP;
+  s->iters = c.step_iters;
+  s->err_u = c.last_err[0];
+  s->err_v = c.last_err[1];
+  s->err_w = c.last_err[2];
+  s->err_p = c.last_err[3];
+  s->err_T = c.last_err[4];
+  s->status = c.status;
+  return NIM_OK;
+}
+
+extern "C" int nim_gpu_iterate(nim_ctx *x, int32_t n, nim_step_stats *s) {
+  if (!x || n < 0) return NIM_ERR_BAD_ARG;
+  if (!x->initialized) return NIM_ERR_STATE;
+  // fixed number of passes: keep the stop flag clear and the cap out of reach
+  const Phys keep = x->phys;
+  x->phys.max_iters = 0;
+  for (int q = 0; q < 5; ++q) x->phys.tol[q] = -1.0;
+  int st = NIM_OK;
+  k_step_reset<<<1, 1, 0, x->stream>>>(x->ctl);
+  for (int k = 0; k < n && st == NIM_OK; ++k) st = launch_iteration(x);
+  x->phys = keep;
+  TRY(st);
+  TRY(read_ctrl(x));
+  fill_iter_stats(x, s);
+  return x->ctl_host->status;
+}
+
+extern "C" int nim_gpu_integrate(nim_ctx *x, nim_step_stats *s) {
+  if (!x) return NIM_ERR_BAD_ARG;
+  if (!x->initialized || !x->in_step) return NIM_ERR_STATE;
+  const int G = 4;  // iterations per graph launch
+  if (!x->graph || x->graph_iters != G) TRY(build_graph(x, G));
+  // launch ahead by the previous step's count, then poll
+  int ahead = std::max(1, (x->last_iters * 7 / 8) / G);
+  // with max_iters <= 0 the device never stops on its own; bound the host loop
+  const long long cap = (x->params.max_iters > 0) ? (long long)x->params.max_iters + G : 100000000LL;
+  long long launched = 0;
+  bool capped = false;
+  for (;;) {
+    for (int k = 0; k < ahead; ++k) CK(cudaGraphLaunch(x->graph, x->stream));
+    launched += (long long)ahead * G;
+    TRY(read_ctrl(x));
+    if (x->ctl_host->done) break;
+    if (launched >= cap) {
+      capped = true;
+      break;
+    }
+    ahead = 1;
+  }
+  const Dims &d = x->d;
+  k_after_integrate<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->g, x->F, x->phys, x->ctl, x->nblk_c);
+  k_finish_sum<<<1, BLK, 0, x->stream>>>(x->F.part, x->nblk_c, 1, x->sums);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(x->host_sums, x->sums, sizeof(double), cudaMemcpyDeviceToHost, x->stream));
+  TRY(read_ctrl(x));
+  x->last_iters = x->ctl_host->step_iters;
+  if (capped && x->ctl_host->status == NIM_OK) x->ctl_host->status = NIM_ERR_NOT_CONVERGED;
+  if (s) {
+    fill_iter_stats(x, s);
+    s->dilatation = std::sqrt(x->host_sums[0] / d.Nc);
+    s->dudt_max = bits_to_double(x->ctl_host->red[0]);
+    s->dTdt_max = bits_to_double(x->ctl_host->red[1]);
+  }
+  return x->ctl_host->status;
+}
+
+extern "C" int nim_gpu_end_step(nim_ctx *x, nim_step_stats *s) {
+  if (!x) return NIM_ERR_BAD_ARG;
+  if (!x->initialized || !x->in_step) return NIM_ERR_STATE;
+  const Dims &d = x->d;
+  const int nr = 2 * d.NT * d.NZ, gn = grid(nr);
+  k_update_time<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->F, x->ctl);
+  k_nusselt<<<gn, BLK, 0, x->stream>>>(d, x->g, x->F, x->ctl, gn);
+  k_finish_sum<<<1, BLK, 0, x->stream>>>(x->F.part, gn, 4, x->sums);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(x->host_sums, x->sums, 4 * sizeof(double), cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  const int32_t step_done = x->STEP;
+  x->STEP = x->STEP + 1;                 // nse.f90:1295
+  x->TI = x->TI + 2 * x->params.DT;      // nse.f90:1296
+  x->in_step = false;
+  if (s) {
+    const double sum1 = x->host_sums[0], sumA1 = x->host_sums[1], sum2 = x->host_sums[2], sumA2 = x->host_sums[3];
+    s->step = step_done;
+    s->nu_outer = -(sum1 / sumA1 * x->params.R_o);  // nse.f90:2794, printed Nu_H
+    s->nu_inner = -(sum2 / sumA2 * x->params.R_i);  // printed Nu_C (hot hexagon)
+    s->area_outer = sumA1;
+    s->area_inner = sumA2;
+    s->time = x->TI;
+  }
+  return NIM_OK;
+}
+
+extern "C" int nim_gpu_step(nim_ctx *x, int32_t nsteps, nim_step_stats *per, int32_t *done) {
+  if (!x || nsteps < 0) return NIM_ERR_BAD_ARG;
+  if (!x->initialized) return NIM_ERR_STATE;
+  int32_t k = 0;
+  int st = NIM_OK;
+  for (; k < nsteps; ++k) {
+    nim_step_stats rec;
+    std::memset(&rec, 0, sizeof(rec));
+    TRY(nim_gpu_begin_step(x));
+    st = nim_gpu_integrate(x, &rec);
+    rec.status = st;
+    if (st != NIM_OK) {
+      x->in_step = false;
+      if (per) per[k] = rec;
+      ++k;
+      break;
+    }
+    // steady-state exit of the time loop (nse.f90:60-69)
+    if (x->params.check_steady && rec.dudt_max < x->params.dudt_epsilon && rec.dTdt_max < x->params.dudt_epsilon) {
+      rec.steady = 1;
+      x->in_step = false;
+      if (per) per[k] = rec;
+      ++k;
+      break;
+    }
+    const int st2 = nim_gpu_end_step(x, &rec);
+    if (per) per[k] = rec;
+    if (st2 != NIM_OK) {
+      st = st2;
+      ++k;
+      break;
+    }
+  }
+  if (done) *done = k;
+  return st;
+}
+
+extern "C" int nim_gpu_download(nim_ctx *x, nim_field f, double *host, int64_t n) {
+  if (!x || !host) return NIM_ERR_BAD_ARG;
+  if (!x->initialized) return NIM_ERR_STATE;
+  TRY(read_ctrl(x));
+  FieldView v;
+  TRY(field_view(x, f, x->ctl_host->iter & 1, v));
+  const int64_t len = (int64_t)v.n * v.K;
+  if (n < len) return NIM_ERR_BAD_ARG;
+  k_gather<<<grid(v.n), BLK, 0, x->stream>>>(v.src, v.stride, v.K, v.face ? x->perm : nullptr, v.n, x->scratch);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, x->scratch, sizeof(double) * len, cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  return NIM_OK;
+}
+
+extern "C" int nim_gpu_upload(nim_ctx *x, nim_field f, const double *host, int64_t n) {
+  if (!x || !host) return NIM_ERR_BAD_ARG;
+  if (!x->initialized) return NIM_ERR_STATE;
+  TRY(read_ctrl(x));
+  FieldView v;
+  TRY(field_view(x, f, x->ctl_host->iter & 1, v));
+  if (!v.writable || v.K != 1) return NIM_ERR_BAD_ARG;
+  if (n < v.n) return NIM_ERR_BAD_ARG;
+  CK(cudaMemcpyAsync(x->scratch, host, sizeof(double) * v.n, cudaMemcpyHostToDevice, x->stream));
+  k_scatter<<<grid(v.n), BLK, 0, x->stream>>>(x->scratch, v.face ? x->perm : nullptr, v.n, const_cast<double *>(v.src),
+                                                 v.dst1);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(x->stream));
+  return NIM_OK;
+}
+
+extern "C" int nim_gpu_synchronize(nim_ctx *x) {
+  if (!x) return NIM_ERR_BAD_ARG;
+  CK(cudaStreamSynchronize(x->stream));
+  return NIM_OK;
+}
+
+extern "C" void nim_gpu_destroy(nim_ctx *x) {
+  if (!x) return;
+  if (x->stream) cudaStreamSynchronize(x->stream);
+  if (x->graph) cudaGraphExecDestroy(x->graph);
+  for (void *p : x->allocs) cudaFree(p);
+  if (x->ctl_host) cudaFreeHost(x->ctl_host);
+  if (x->stream) cudaStreamDestroy(x->stream);
+  delete x;
+}

@@ -1,0 +1,1201 @@
+// Device kernels of the NIM time advance (FP64 path).
+//
+// Each kernel restates one or more reference routines; the file:line of the
+// routine is given at the kernel.  Arithmetic follows the reference's
+// expression order (built with -fmad=false, IEEE division/sqrt) so every value
+// matches the CPU oracle's parallel schedule up to the last bit of exp().
+//
+// Iteration schedule (one pass of integrate_nse, nse.f90:131-160), parity
+// par = ctrl->iter & 1 selects the current half of every double-buffered face
+// array; the other half receives the sweep's results:
+//   k_vel_cell   calculate_gforces + calculate_R_b + calculate_R_D2 + the
+//                cell-average update of u,v,w                (in place)
+//   k_vel_face   +xi face updates of u,v,w                    (cur -> next)
+//   k_p_src      calculate_R_b_p + calculate_R_D_p2           (-> Rp, dila)
+//   k_p_bc       apply_pressure_bc                            (cur -> next, walls)
+//   k_p_bc_copy  new wall values into cur
+//   k_p_face     integrate_pressure_field_i                   (cur -> next)
+//   k_zero_flux  apply_zero_flux                              (in place, cur)
+//   k_T_cell     calculate_temperature_nim_constants_formulation2 +
+//                calculate_R_D_T + cell-average update of T   (in place)
+//   k_T_face     +xi face updates of T                        (cur -> next)
+//   k_iter_end   find_error's maxima -> convergence flag, iteration count
+// Every sweep reads only values from before the sweep, so the result does not
+// depend on thread order.
+#pragma once
+#include "nim_common.cuh"
+
+namespace nim {
+
+// ------------------------------------------------------------ device state
+struct Geo {
+  double *vol;     // [Nc]
+  double *G;       // [3][Nc]   G1, G2, G3
+  double *gij;     // [9][Nc]   meshes_gij(a,b) at a-1+3(b-1)
+  double *xi;      // [9][Nc]   meshes_xi_x(a,b) at a-1+3(b-1)
+  double *gf;      // [54][Nc]  meshes_gij_faces(a,b,f) at a-1+3(b-1)+9(f-1)
+  double *gfd;     // [6][Nc]   gf(d,d,2d-1), gf(d,d,2d) at 2(d-1)+{0,1}
+  double *dg;      // [6][Nc]   gf(d,e,2d-1,i2)-gf(d,e,2d,i), e=tr1,tr2 at 2(d-1)+{0,1}
+  double *area;    // [NF]
+  double *normal;  // [3][NF]
+  double *mid;     // [3][NF]
+  double *tang;    // [3][NF]
+  double *bitang;  // [3][NF]
+  double *AA;      // [45][Nc]  AA_px/py/pz(k) at 15(d-1)+k-1
+  int *bcpts;      // [5][NBF]  BCs_faces_points as structured face indices
+  double *bca;     // [5][NBF]  BCs_faces_a(1:5)
+  double *bcap;    // [8][NBF]  BCs_faces_ap(1:8)
+  double *bcg;     // [2][NBF]  gij_faces factors of B2, B3 in apply_pressure_bc
+  double *zf;      // [4][NBF]  zero-flux weights (B, C, D, A) for z walls
+  double *nuw;     // [4][NBF]  find_Nu2 weights (A, B, C, D) for r walls
+  double *bcval;   // [4][NBF]  Dirichlet face values of u, v, w, T
+};
+
+struct Fields {
+  double *f[5];    // faces u, v, w, p, T: each [2][NF]
+  double *c[4];    // cells u, v, w, T (meshes_*xyz)
+  double *co[4];   // meshes_*xyz_old
+  double *ct[4];   // meshes_*xyzt
+  double *mp, *dila, *dila_old, *Rp;
+  double *MA;      // [18][Nc] velocity M_A (per step scratch)
+  double *MF4;     // [8][Nc]
+  double *MF;      // [15][Nc]  M_F1..3(k) at 5(d-1)+k-1
+  double *MTF;     // [15][Nc]  MT_F1..3
+  double *dpd;     // [3][Nc]   dpdx_old, dpdy_old, dpdz_old
+  double *part;    // [8][nblk] per-block partial sums
+};
+
+struct Phys {
+  double DT, nu, alpha, rho, g_beta;
+  double w[4];     // u, v, w, T relaxation
+  double w_p, w_p2;
+  double tol[5];
+  double v_limit, dudt_epsilon, R_i, R_o;
+  double inv_Re;   // 1/Re with Re = 1/nu (parameters.f90:172, nse.f90:1852)
+  double inv_rho;  // 1/rho
+  int max_iters, dpdx_tolerance;
+};
+
+// Control block in device memory; k_iter_end is its only writer during an
+// iteration, the host reads it between batches.
+struct Ctrl {
+  unsigned long long err[2][8];  // max-accumulators per parity: u,v,w,p,T,dpdx
+  int iter;         // iterations since init (parity source)
+  int step_iters;   // iterations of the current step (cnt)
+  int done;         // 1: current step's inner loop has stopped
+  int status;       // NIM_OK / NIM_ERR_NOT_CONVERGED / NIM_ERR_NONFINITE
+  int first;        // 1 until the first iteration after init has finished
+  int pad[3];
+  double last_err[5];
+  unsigned long long wall_floor[8];  // max |Dirichlet wall value| bits (find_error
+                                     // compares with zero-initialised arrays once)
+  unsigned long long red[4];  // dudt, dTdt maxima (after integrate)
+  double dilatation, nu_outer, nu_inner, area_outer, area_inner;
+};
+
+constexpr int BLK = 256;
+
+// ------------------------------------------------------------ reductions
+// Max of non-negative doubles through their bit patterns (IEEE order equals
+// integer order for x >= 0; NaN sorts above +Inf and is caught as non-finite).
+template <int N>
+__device__ __forceinline__ void block_max(const double (&v)[N], unsigned long long *dst) {
+  __shared__ unsigned long long sm[N][BLK / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int n = 0; n < N; ++n) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(v[n]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long t = __shfl_xor_sync(0xffffffffu, b, o);
+      b = (t > b) ? t : b;
+    }
+    if (lane == 0) sm[n][warp] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x < N) {
+    unsigned long long m = 0;
+    for (int w = 0; w < BLK / 32; ++w) m = (sm[threadIdx.x][w] > m) ? sm[threadIdx.x][w] : m;
+    if (m) atomicMax(dst + threadIdx.x, m);
+  }
+}
+
+// Deterministic block sums written to part[n][blockIdx.x].
+template <int N>
+__device__ __forceinline__ void block_sum(const double (&v)[N], double *part, int nblk) {
+  __shared__ double sm[N][BLK];
+#pragma unroll
+  for (int n = 0; n < N; ++n) sm[n][threadIdx.x] = v[n];
+  __syncthreads();
+  for (int s = BLK / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+#pragma unroll
+      for (int n = 0; n < N; ++n) sm[n][threadIdx.x] = sm[n][threadIdx.x] + sm[n][threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int n = 0; n < N; ++n) part[(size_t)n * nblk + blockIdx.x] = sm[n][0];
+  }
+}
+
+// ================================================================ init
+__device__ __forceinline__ int node_index(const Dims &d, int i, int j, int k) {
+  return i + d.NT * (j + (d.NR + 1) * k);
+}
+
+// mesh_calculate_mapping_coefficients (create_mesh.f90:254-303) from the
+// arranged nodes 1..8 of the cell (create_mesh.f90:326-333 drawing).
+__device__ void cell_map(const Dims &d, const double *__restrict__ nx, const Cell &x, Map &M) {
+  const int ip = (x.i == d.NT - 1) ? 0 : x.i + 1;
+  int nd[9];
+  nd[1] = node_index(d, x.i, x.j, x.k);
+  nd[2] = node_index(d, x.i, x.j + 1, x.k);
+  nd[3] = node_index(d, ip, x.j + 1, x.k);
+  nd[4] = node_index(d, ip, x.j, x.k);
+  nd[5] = node_index(d, x.i, x.j, x.k + 1);
+  nd[6] = node_index(d, x.i, x.j + 1, x.k + 1);
+  nd[7] = node_index(d, ip, x.j + 1, x.k + 1);
+  nd[8] = node_index(d, ip, x.j, x.k + 1);
+  for (int comp = 0; comp < 3; ++comp) {
+    double v[9];
+    for (int n = 1; n <= 8; ++n) v[n] = nx[3 * (size_t)nd[n] + comp];
+    double *C = (comp == 0) ? M.C : (comp == 1) ? M.D : M.E;
+    C[0] = (v[7] + v[8] + v[5] + v[6] + v[3] + v[4] + v[1] + v[2]) / 8.;
+    C[1] = (v[7] - v[8] - v[5] + v[6] + v[3] - v[4] - v[1] + v[2]) / 8.;
+    C[2] = (v[7] + v[8] - v[5] - v[6] + v[3] + v[4] - v[1] - v[2]) / 8.;
+    C[3] = (v[7] + v[8] + v[5] + v[6] - v[3] - v[4] - v[1] - v[2]) / 8.;
+    C[4] = (v[7] - v[8] + v[5] - v[6] + v[3] - v[4] + v[1] - v[2]) / 8.;
+    C[5] = (v[7] - v[8] - v[5] + v[6] - v[3] + v[4] + v[1] - v[2]) / 8.;
+    C[6] = (v[7] + v[8] - v[5] - v[6] - v[3] - v[4] + v[1] + v[2]) / 8.;
+    C[7] = (v[7] - v[8] + v[5] - v[6] - v[3] + v[4] - v[1] + v[2]) / 8.;
+  }
+}
+
+// Does this cell hold the final (highest cell number) write of its face pos?
+// The reference writes shared-face geometry from both cells in cell-number
+// order (geometry.f90:100-189, 468-496), so the later cell wins.
+__device__ __forceinline__ bool owns_face(const Dims &d, const Cell &x, int pos) {
+  switch (pos) {
+    case 1: return true;
+    case 2: return x.j == d.NR - 1;
+    case 3: return x.i > 0;
+    case 4: return x.i == d.NT - 1;
+    case 5: return true;
+    default: return x.k == d.NZ - 1;
+  }
+}
+
+// evaluate_all_mesh_constants for one cell (geometry.f90:14-32):
+// volume_calculate (create_mesh.f90:306-322), find_normal (geometry.f90:
+// 76-190), calculate_defusion_tensor_over_faces (geometry.f90:395-497, the 25
+// points per face that Gauss_integration2d_face keeps) and
+// convection_diffusion_constants_mesh_i (geometry.f90:500-632).  The volume
+// and the volume-averaged metrics share their 125 Gauss points.
+__global__ void __launch_bounds__(BLK) k_cell_geometry(Dims d, GaussRule gq, const double *__restrict__ nx, Geo g) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.Nc) return;
+  const Cell x = Cell::of(d, c);
+  Map M;
+  cell_map(d, nx, x, M);
+  const size_t Nc = d.Nc, NF = d.NF;
+  Curvi C;
+  {
+    double V = 0., sG[3] = {0., 0., 0.}, sK[9], sJ[9];
+    for (int n = 0; n < 9; ++n) sK[n] = sJ[n] = 0.;
+    for (int i = 0; i < 5; ++i)
+      for (int j = 0; j < 5; ++j)
+        for (int k = 0; k < 5; ++k) {
+          curvi_point(M, gq.x[i], gq.x[j], gq.x[k], C);
+          const double w = gq.w[i] * gq.w[j] * gq.w[k];
+          V = V + w * (1. * C.detJ);
+          // gamma_tensor (curvilinear.f90:109-160) contracted with g^ij
+          const double g12[3] = {M.C[4] + M.C[7] * gq.x[k], M.D[4] + M.D[7] * gq.x[k], M.E[4] + M.E[7] * gq.x[k]};
+          const double g13[3] = {M.C[5] + M.C[7] * gq.x[j], M.D[5] + M.D[7] * gq.x[j], M.E[5] + M.E[7] * gq.x[j]};
+          const double g23[3] = {M.C[6] + M.C[7] * gq.x[i], M.D[6] + M.D[7] * gq.x[i], M.E[6] + M.E[7] * gq.x[i]};
+          double gu[3][3];  // gu[a][comp] = g^a
+          for (int a = 0; a < 3; ++a)
+            for (int cc = 0; cc < 3; ++cc) gu[a][cc] = C.jacinv[cc][a];
+          double G[3][3];
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) G[a][b] = dot3(gu[a], gu[b]);
+          for (int a = 0; a < 3; ++a) {
+            const double a12 = dot3(gu[a], g12), a13 = dot3(gu[a], g13), a23 = dot3(gu[a], g23);
+            const double Ga = (a12 * G[0][1] + a12 * G[1][0] + a13 * G[0][2] + a13 * G[2][0] + a23 * G[1][2] +
+                               a23 * G[2][1]);
+            sG[a] = sG[a] + w * (Ga * C.detJ);
+          }
+          for (int r = 0; r < 3; ++r)
+            for (int cc = 0; cc < 3; ++cc) {
+              sK[r + 3 * cc] = sK[r + 3 * cc] + w * (G[r][cc] * C.detJ);
+              sJ[r + 3 * cc] = sJ[r + 3 * cc] + w * (C.jacinv[r][cc] * C.detJ);
+            }
+        }
+    g.vol[c] = V;
+    for (int a = 0; a < 3; ++a) g.G[a * Nc + c] = sG[a] / V;
+    for (int r = 0; r < 3; ++r)
+      for (int cc = 0; cc < 3; ++cc) {
+        g.gij[(r + 3 * cc) * Nc + c] = sK[r + 3 * cc] / V;
+        g.xi[(cc + 3 * r) * Nc + c] = sJ[r + 3 * cc] / V;  // xi_x(a,b) = <jacinv(b,a)>
+      }
+  }
+  // find_normal: contravariant unit normal, covariant unit tangents, centre
+  for (int fn = 1; fn <= 6; ++fn) {
+    if (!owns_face(d, x, fn)) continue;
+    double px, py, pz;
+    face_point(fn, 0.0, 0.0, px, py, pz);
+    curvi_point(M, px, py, pz, C);
+    const int dd = (fn - 1) / 2, t1 = (dd == 0) ? 1 : 0, t2 = (dd == 2) ? 1 : 2;
+    const int f = x.face(d, fn);
+    const double sn = sqrt(gup(C, dd, dd)), s1 = sqrt(glow(C, t1, t1)), s2 = sqrt(glow(C, t2, t2));
+    for (int cc = 0; cc < 3; ++cc) {
+      g.normal[cc * NF + f] = C.jacinv[cc][dd] / sn;
+      g.tang[cc * NF + f] = C.jac[t1][cc] / s1;
+      g.bitang[cc * NF + f] = C.jac[t2][cc] / s2;
+    }
+    g.mid[0 * NF + f] = C.x;
+    g.mid[1 * NF + f] = C.y;
+    g.mid[2 * NF + f] = C.z;
+  }
+  // face-averaged metric and face areas
+  for (int fn = 1; fn <= 6; ++fn) {
+    const int dd = (fn - 1) / 2;
+    double A = 0., K[9];
+    for (int n = 0; n < 9; ++n) K[n] = 0.;
+    for (int a = 0; a < 5; ++a)
+      for (int b = 0; b < 5; ++b) {
+        double px, py, pz;
+        face_point(fn, gq.x[a], gq.x[b], px, py, pz);
+        curvi_point(M, px, py, pz, C);
+        const double w = gq.w[a] * gq.w[b];
+        const double dS = C.detJ * sqrt(gup(C, dd, dd));
+        A = A + w * dS;
+        for (int r = 0; r < 3; ++r) {
+          const double srr = sqrt(gup(C, r, r));
+          for (int cc = 0; cc < 3; ++cc) K[r + 3 * cc] = K[r + 3 * cc] + w * (gup(C, r, cc) / srr * dS);
+        }
+      }
+    if (owns_face(d, x, fn)) g.area[x.face(d, fn)] = A;
+    for (int n = 0; n < 9; ++n) g.gf[(n + 9 * (fn - 1)) * Nc + c] = K[n] / A;
+  }
+}
+
+// Compact per-cell copies of the metric entries the sweeps read: the
+// diagonal face metric (M_A) and the differences of off-diagonal face metric
+// across each +xi face (the B3/B4 terms, nse.f90:882-885 and alike).
+__global__ void __launch_bounds__(BLK) k_metric_derived(Dims d, Geo g) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.Nc) return;
+  const Cell x = Cell::of(d, c);
+  const size_t Nc = d.Nc;
+  auto gfa = [&](int a, int b, int f, int cell) { return g.gf[(size_t)(a - 1 + 3 * (b - 1) + 9 * (f - 1)) * Nc + cell]; };
+  for (int dd = 1; dd <= 3; ++dd) {
+    g.gfd[(2 * (dd - 1) + 0) * Nc + c] = gfa(dd, dd, 2 * dd - 1, c);
+    g.gfd[(2 * (dd - 1) + 1) * Nc + c] = gfa(dd, dd, 2 * dd, c);
+    double v0 = 0., v1 = 0.;
+    if (x.has_nb(d, 2 * dd)) {
+      const int i2 = x.nb(d, 2 * dd).c;
+      v0 = gfa(dd, tr1(dd), 2 * dd - 1, i2) - gfa(dd, tr1(dd), 2 * dd, c);
+      v1 = gfa(dd, tr2(dd), 2 * dd - 1, i2) - gfa(dd, tr2(dd), 2 * dd, c);
+    }
+    g.dg[(2 * (dd - 1) + 0) * Nc + c] = v0;
+    g.dg[(2 * (dd - 1) + 1) * Nc + c] = v1;
+  }
+}
+
+// Zero-velocity NIM constants of calculate_pressure_nim_constants
+// (nim.f90:567-612): C_nim..J_nim in their series branch at u = 0.
+struct PConst {
+  double CC[3], EE[3], FF[3], GG[3], HH[3], II[3], JJ[3], Det;
+};
+__device__ __forceinline__ PConst pconst(const Geo &g, size_t Nc, int c, double rho) {
+  PConst p;
+  const double a = 1.;
+  for (int dd = 0; dd < 3; ++dd) {
+    const double Fk = g.gij[(size_t)(dd + 3 * dd) * Nc + c] / rho;
+    p.CC[dd] = -(a * a / (3. * Fk));
+    p.GG[dd] = 1 / (2. * a);
+    p.HH[dd] = a / Fk;
+    p.II[dd] = 1 / (2. * a);
+    p.JJ[dd] = -(a / Fk);
+  }
+  p.Det = 1. / (p.CC[0] * p.CC[1] + p.CC[1] * p.CC[2] + p.CC[0] * p.CC[2]);
+  for (int dd = 0; dd < 3; ++dd) {
+    p.EE[dd] = p.Det / 2.;
+    p.FF[dd] = p.Det / 2.;
+  }
+  return p;
+}
+
+// AA_px/py/pz (nim.f90:616-678)
+__global__ void __launch_bounds__(BLK) k_pressure_coeffs(Dims d, Geo g, double rho) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.Nc) return;
+  const Cell x = Cell::of(d, c);
+  const size_t Nc = d.Nc;
+  const PConst P = pconst(g, Nc, c, rho);
+  auto gfa = [&](int a, int b, int f, int cell) { return g.gf[(size_t)(a - 1 + 3 * (b - 1) + 9 * (f - 1)) * Nc + cell]; };
+  double A[15];
+  // +r face
+  for (int n = 0; n < 15; ++n) A[n] = 0.;
+  if (x.has_nb(d, 2)) {
+    const int i2 = x.nb(d, 2).c;
+    const PConst Q = pconst(g, Nc, i2, rho);
+    const double gg = gfa(1, 1, 2, c), g2 = gfa(1, 1, 1, i2);
+    A[0] = -(P.GG[0] + (P.CC[1] + P.CC[2]) * P.EE[0] * P.HH[0]) * gg;
+    A[1] = (P.GG[0] - (P.CC[1] + P.CC[2]) * P.FF[0] * P.HH[0]) * gg + (Q.II[0] + (Q.CC[1] + Q.CC[2]) * Q.EE[0] * Q.JJ[0]) * g2;
+    A[2] = -(Q.II[0] - (Q.CC[1] + Q.CC[2]) * Q.FF[0] * Q.JJ[0]) * g2;
+    A[3] = P.CC[2] * P.EE[1] * P.HH[0] * gg;
+    A[4] = P.CC[2] * P.FF[1] * P.HH[0] * gg;
+    A[5] = -(Q.CC[2] * Q.EE[1] * Q.JJ[0] * g2);
+    A[6] = -(Q.CC[2] * Q.FF[1] * Q.JJ[0] * g2);
+    A[7] = P.CC[1] * P.EE[2] * P.HH[0] * gg;
+    A[8] = P.CC[1] * P.FF[2] * P.HH[0] * gg;
+    A[9] = -(Q.CC[1] * Q.EE[2] * Q.JJ[0] * g2);
+    A[10] = -(Q.CC[1] * Q.FF[2] * Q.JJ[0] * g2);
+    A[11] = P.CC[1] * P.CC[2] * P.Det * P.HH[0] * gg;
+    A[12] = -(P.CC[1] * P.CC[2] * P.Det * P.HH[0] * gg);
+    A[13] = -(Q.CC[1] * Q.CC[2] * Q.Det * Q.JJ[0] * g2);
+    A[14] = Q.CC[1] * Q.CC[2] * Q.Det * Q.JJ[0] * g2;
+  }
+  for (int n = 0; n < 15; ++n) g.AA[(size_t)n * Nc + c] = A[n];
+  // +theta face
+  {
+    const int i2 = x.nb(d, 4).c;
+    const PConst Q = pconst(g, Nc, i2, rho);
+    const double gg = gfa(2, 2, 4, c), g2 = gfa(2, 2, 3, i2);
+    A[0] = P.CC[2] * P.EE[0] * P.HH[1] * gg;
+    A[1] = P.CC[2] * P.FF[0] * P.HH[1] * gg;
+    A[2] = -(Q.CC[2] * Q.EE[0] * Q.JJ[1] * g2);
+    A[3] = -(Q.CC[2] * Q.FF[0] * Q.JJ[1] * g2);
+    A[4] = -(P.GG[1] + (P.CC[0] + P.CC[2]) * P.EE[1] * P.HH[1]) * gg;
+    A[5] = (P.GG[1] - (P.CC[0] + P.CC[2]) * P.FF[1] * P.HH[1]) * gg + (Q.II[1] + (Q.CC[0] + Q.CC[2]) * Q.EE[1] * Q.JJ[1]) * g2;
+    A[6] = -(Q.II[1] - (Q.CC[0] + Q.CC[2]) * Q.FF[1] * Q.JJ[1]) * g2;
+    A[7] = P.CC[0] * P.EE[2] * P.HH[1] * gg;
+    A[8] = P.CC[0] * P.FF[2] * P.HH[1] * gg;
+    A[9] = -(Q.CC[0] * Q.EE[2] * Q.JJ[1] * g2);
+    A[10] = -(Q.CC[0] * Q.FF[2] * Q.JJ[1] * g2);
+    A[11] = P.CC[0] * P.CC[2] * P.Det * P.HH[1] * gg;
+    A[12] = -(P.CC[0] * P.CC[2] * P.Det * P.HH[1] * gg);
+    A[13] = -(Q.CC[0] * Q.CC[2] * Q.Det * Q.JJ[1] * g2);
+    A[14] = Q.CC[0] * Q.CC[2] * Q.Det * Q.JJ[1] * g2;
+  }
+  for (int n = 0; n < 15; ++n) g.AA[(size_t)(15 + n) * Nc + c] = A[n];
+  // +z face
+  for (int n = 0; n < 15; ++n) A[n] = 0.;
+  if (x.has_nb(d, 6)) {
+    const int i2 = x.nb(d, 6).c;
+    const PConst Q = pconst(g, Nc, i2, rho);
+    const double gg = gfa(3, 3, 6, c), g2 = gfa(3, 3, 5, i2);
+    A[0] = P.CC[1] * P.EE[0] * P.HH[2] * gg;
+    A[1] = P.CC[1] * P.FF[0] * P.HH[2] * gg;
+    A[2] = -(Q.CC[1] * Q.EE[0] * Q.JJ[2] * g2);
+    A[3] = -(Q.CC[1] * Q.FF[0] * Q.JJ[2] * g2);
+    A[4] = P.CC[0] * P.EE[1] * P.HH[2] * gg;
+    A[5] = P.CC[0] * P.FF[1] * P.HH[2] * gg;
+    A[6] = -(Q.CC[0] * Q.EE[1] * Q.JJ[2] * g2);
+    A[7] = -(Q.CC[0] * Q.FF[1] * Q.JJ[2] * g2);
+    A[8] = -(P.GG[2] + (P.CC[0] + P.CC[1]) * P.EE[2] * P.HH[2]) * gg;
+    A[9] = (P.GG[2] - (P.CC[0] + P.CC[1]) * P.FF[2] * P.HH[2]) * gg + (Q.II[2] + (Q.CC[0] + Q.CC[1]) * Q.EE[2] * Q.JJ[2]) * g2;
+    A[10] = -(Q.II[2] - (Q.CC[0] + Q.CC[1]) * Q.FF[2] * Q.JJ[2]) * g2;
+    A[11] = P.CC[0] * P.CC[1] * P.Det * P.HH[2] * gg;
+    A[12] = -(P.CC[0] * P.CC[1] * P.Det * P.HH[2] * gg);
+    A[13] = -(Q.CC[0] * Q.CC[1] * Q.Det * Q.JJ[2] * g2);
+    A[14] = Q.CC[0] * Q.CC[1] * Q.Det * Q.JJ[2] * g2;
+  }
+  for (int n = 0; n < 15; ++n) g.AA[(size_t)(30 + n) * Nc + c] = A[n];
+}
+
+// Boundary-face constants, one thread per wall face b (reference BC order):
+// evaluate_pressure_bc_array (geometry.f90:879-975), BCs_faces_ap
+// (nim.f90:682-742), apply_dirichlet_bc_i face averages (bc.f90:59-88) and
+// the distance weights of apply_zero_flux (bc.f90:355-384) and find_Nu2
+// (nse.f90:2721-2764).
+__global__ void __launch_bounds__(BLK) k_bc_geometry(Dims d, GaussRule gq, const double *__restrict__ nx, Geo g,
+                                                     double rho, const double *__restrict__ bcv /* [5][5] */) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.NBF) return;
+  const size_t Nc = d.Nc, NF = d.NF, NB = d.NBF;
+  const BFace B = bface(d, b);
+  const Cell M1 = B.cell;
+  const int pos = B.pos;
+  const int f0 = M1.face(d, pos);
+  // ---- 5-point normal stencil
+  const int fn = (pos % 2 == 1) ? pos + 1 : pos - 1;
+  const Cell M2 = M1.nb(d, fn);
+  const int t1a = (pos <= 2) ? 4 : 2, t1b = (pos <= 2) ? 3 : 1;
+  const int t2a = (pos <= 4) ? 6 : 4, t2b = (pos <= 4) ? 5 : 3;
+  const Cell M3 = M1.has_nb(d, t1a) ? M1.nb(d, t1a) : M1.nb(d, t1b);
+  const Cell M4 = M1.has_nb(d, t2a) ? M1.nb(d, t2a) : M1.nb(d, t2b);
+  int pts[6];
+  pts[1] = f0;
+  pts[2] = M1.face(d, fn);
+  pts[3] = M2.face(d, fn);
+  pts[4] = M3.face(d, fn);
+  pts[5] = M4.face(d, fn);
+  for (int j = 1; j <= 5; ++j) g.bcpts[(j - 1) * NB + b] = pts[j];
+  double n[6], t[6], s[6];
+  const double nv[3] = {g.normal[f0], g.normal[NF + f0], g.normal[2 * NF + f0]};
+  const double tv[3] = {g.tang[f0], g.tang[NF + f0], g.tang[2 * NF + f0]};
+  const double sv[3] = {g.bitang[f0], g.bitang[NF + f0], g.bitang[2 * NF + f0]};
+  for (int j = 1; j <= 5; ++j) {
+    double dv[3];
+    for (int cc = 0; cc < 3; ++cc) dv[cc] = g.mid[cc * NF + pts[j]] - g.mid[cc * NF + pts[1]];
+    n[j] = dot3(dv, nv);
+    t[j] = dot3(dv, tv);
+    s[j] = dot3(dv, sv);
+  }
+  const double D =
+      (n[3] * s[4] * t[2] - n[3] * s[5] * t[2] - n[2] * s[4] * t[3] + n[2] * s[5] * t[3] - n[3] * s[2] * t[4] +
+       n[2] * s[3] * t[4] - n[2] * s[5] * t[4] + n[3] * s[5] * t[4] + n[5] * s[3] * t[2] - n[5] * s[4] * t[2] -
+       n[5] * s[2] * t[3] + n[5] * s[4] * t[3] + n[5] * s[2] * t[4] - n[5] * s[3] * t[4] + n[3] * s[2] * t[5] -
+       n[2] * s[3] * t[5] + n[2] * s[4] * t[5] - n[3] * s[4] * t[5] +
+       n[4] * (s[5] * t[2] + s[2] * t[3] - s[5] * t[3] - s[2] * t[5] + s[3] * (-t[2] + t[5])));
+  double a[6];
+  a[2] = 2 * (-(n[5] * s[4] * t[3]) + n[4] * s[5] * t[3] + n[5] * s[3] * t[4] - n[3] * s[5] * t[4] -
+              n[4] * s[3] * t[5] + n[3] * s[4] * t[5]) / ((n[2] * n[2]) * D);
+  a[3] = 2 * (n[5] * s[4] * t[2] - n[4] * s[5] * t[2] - n[5] * s[2] * t[4] + n[2] * s[5] * t[4] +
+              n[4] * s[2] * t[5] - n[2] * s[4] * t[5]) / ((n[3] * n[3]) * D);
+  a[4] = 2 * (n[5] * s[3] * t[2] - n[3] * s[5] * t[2] - n[5] * s[2] * t[3] + n[2] * s[5] * t[3] +
+              n[3] * s[2] * t[5] - n[2] * s[3] * t[5]) / ((n[4] * n[4]) * D);
+  a[5] = 2 * (n[4] * s[3] * t[2] - n[3] * s[4] * t[2] - n[4] * s[2] * t[3] + n[2] * s[4] * t[3] +
+              n[3] * s[2] * t[4] - n[2] * s[3] * t[4]) / ((n[5] * n[5]) * D);
+  a[1] = -a[2] - a[3] - a[4] - a[5];
+  for (int k = 1; k <= 5; ++k) g.bca[(k - 1) * NB + b] = a[k];
+
+  // ---- BCs_faces_ap
+  auto gfa = [&](int aa, int bb, int f, int cell) { return g.gf[(size_t)(aa - 1 + 3 * (bb - 1) + 9 * (f - 1)) * Nc + cell]; };
+  const PConst P = pconst(g, Nc, M1.c, rho);
+  {
+    const int dd = (pos + 1) / 2, e1 = tr1(dd), e2 = tr2(dd);
+    const bool minus = (pos % 2 == 1);
+    const double gg = gfa(dd, dd, pos, M1.c);
+    const double P0 = minus ? P.II[dd - 1] : P.GG[dd - 1];
+    const double Q = minus ? P.JJ[dd - 1] : P.HH[dd - 1];
+    const double cs = P.CC[e1 - 1] + P.CC[e2 - 1];
+    double ap[8];
+    ap[2 * dd - 2] = -(P0 + cs * P.EE[dd - 1] * Q) * gg;
+    ap[2 * dd - 1] = (P0 - cs * P.FF[dd - 1] * Q) * gg;
+    ap[2 * e1 - 2] = P.CC[e2 - 1] * P.EE[e1 - 1] * Q * gg;
+    ap[2 * e1 - 1] = P.CC[e2 - 1] * P.FF[e1 - 1] * Q * gg;
+    ap[2 * e2 - 2] = P.CC[e1 - 1] * P.EE[e2 - 1] * Q * gg;
+    ap[2 * e2 - 1] = P.CC[e1 - 1] * P.FF[e2 - 1] * Q * gg;
+    ap[6] = P.CC[e1 - 1] * P.CC[e2 - 1] * P.Det * Q * gg;
+    ap[7] = -(P.CC[e1 - 1] * P.CC[e2 - 1] * P.Det * Q * gg);
+    for (int k = 0; k < 8; ++k) g.bcap[k * NB + b] = ap[k];
+    // gij_faces factors of B2 / B3; position 6 takes (3,2) in the centred
+    // branch of B2 (bc.f90:318)
+    const bool centred = M1.has_nb(d, 2 * e1 - 1) && M1.has_nb(d, 2 * e1);
+    const int e1g = (pos == 6 && centred) ? 2 : e1;
+    g.bcg[0 * NB + b] = gfa(dd, e1g, pos, M1.c);
+    g.bcg[1 * NB + b] = gfa(dd, e2, pos, M1.c);
+  }
+  // ---- Dirichlet face values (u, v, w, T) of this BC id
+  {
+    Map M;
+    cell_map(d, nx, M1, M);
+    const int dd = (pos - 1) / 2;
+    double dS[25];
+    Curvi C;
+    for (int i = 0; i < 5; ++i)
+      for (int j = 0; j < 5; ++j) {
+        double px, py, pz;
+        face_point(pos, gq.x[i], gq.x[j], px, py, pz);
+        curvi_point(M, px, py, pz, C);
+        dS[5 * i + j] = C.detJ * sqrt(gup(C, dd, dd));
+      }
+    const int fld[4] = {0, 1, 2, 4};
+    for (int q = 0; q < 4; ++q) {
+      const double cv = bcv[fld[q] * 5 + (B.id - 1)];
+      double Int = 0.;
+      for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 5; ++j) Int = Int + gq.w[i] * gq.w[j] * (cv * dS[5 * i + j]);
+      g.bcval[q * NB + b] = Int / g.area[f0];
+    }
+  }
+  // ---- distance weights along the wall-normal chain of faces
+  {
+    const int in = (pos % 2 == 1) ? pos + 1 : pos - 1;  // faces on the far side
+    const Cell c2 = M1.nb(d, in), c3 = c2.nb(d, in);
+    const int f1 = f0, f2 = M1.face(d, in), f3 = c2.face(d, in), f4 = c3.face(d, in);
+    auto dist = [&](int p, int q) {
+      const double dx = g.mid[p] - g.mid[q], dy = g.mid[NF + p] - g.mid[NF + q], dz = g.mid[2 * NF + p] - g.mid[2 * NF + q];
+      return sqrt(dx * dx + dy * dy + dz * dz);
+    };
+    const double h1 = dist(f1, f2), h2 = dist(f2, f3), h3 = dist(f3, f4);
+    const double wA = (1. / h1 + 1. / (h1 + h2) + 1. / (h1 + h2 + h3));
+    const double wB = ((h1 + h2) * (h1 + h2 + h3)) / (h1 * h2 * (h2 + h3));
+    const double wC = (h1 * (h1 + h2 + h3)) / (h2 * h3 * (h1 + h2));
+    const double wD = (h1 * (h1 + h2)) / (h3 * (h2 + h3) * (h1 + h2 + h3));
+    double *dst = (pos >= 5) ? g.zf : g.nuw;
+    dst[0 * NB + b] = wA;
+    dst[1 * NB + b] = wB;
+    dst[2 * NB + b] = wC;
+    dst[3 * NB + b] = wD;
+  }
+}
+
+// Dirichlet values into both halves of the u, v, w, T face arrays
+// (apply_all_dirichlet_bcs, bc.f90:13-57).
+__global__ void k_apply_dirichlet(Dims d, Geo g, Fields F) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.NBF) return;
+  const BFace B = bface(d, b);
+  const int f = B.cell.face(d, B.pos);
+  const int fld[4] = {0, 1, 2, 4};
+  for (int q = 0; q < 4; ++q) {
+    const double v = g.bcval[q * (size_t)d.NBF + b];
+    F.f[fld[q]][f] = v;
+    F.f[fld[q]][d.NF + f] = v;
+  }
+}
+
+// ============================================================= per step
+// NIM coefficients of one direction for contravariant speed u and
+// diffusivity k: M_A(d,1:6) / MT_A(d,1:6) (nim.f90:181-287, 354-460).
+__device__ __forceinline__ void nim_direction(double u, double k, double gminus, double gplus, double v_limit,
+                                              double A[6]) {
+  const double a = 1.;
+  const double Re = 2 * a * u / k;
+  if (fabs(Re) > v_limit) {
+    const double e = exp(Re);
+    A[0] = (2 * a / (k * (1. / e - 1.)) + 1. / u) * gplus;
+    A[1] = (-(2 * a / (k * (1. - e))) - 1. / u) * gminus;
+    A[2] = (u / (k * (1. / e - 1.))) * gplus;
+    A[3] = (u / (k * (1. - e))) * gminus;
+    if (Re > 0) {
+      A[4] = (-k + (a * u * (1. / e + 1.) / (-(1. / e) + 1.))) / (u * u);
+      A[5] = 1. / (-(1. / e) + 1.) - 1. / (Re);
+    } else {
+      A[4] = (-k + (a * u * (1. + e) / (-1. + e))) / (u * u);
+      A[5] = e / (-1. + e) - 1. / (Re);
+    }
+  } else {
+    const Pw U(u), K(k);
+    A[0] = (-(a / k) - (u) / (3. * K[2]) + (U[3]) / (45. * K[4]) - (2 * U[5]) / (945. * K[6]) +
+            -((U[7]) / (4725. * K[8])) - (2 * U[9]) / (93555. * K[10])) * gplus;
+    A[1] = (-(a / k) + (u) / (3. * K[2]) - (U[3]) / (45. * K[4]) + (2 * U[5]) / (945. * K[6]) -
+            -((U[7]) / (4725. * K[8])) + (2 * U[9]) / (93555. * K[10])) * gminus;
+    A[2] = (-(1 / (2. * a)) - u / (2. * k) - (U[2]) / (6. * K[2]) + (U[4]) / (90. * K[4]) -
+            -((U[6]) / (945. * K[6])) + (U[8]) / (9450. * K[8]) - (U[10]) / (93555. * K[10])) * gplus;
+    A[3] = (-(1 / (2. * a)) + u / (2. * k) - (U[2]) / (6. * K[2]) + (U[4]) / (90. * K[4]) -
+            -((U[6]) / (945. * K[6])) + (U[8]) / (9450. * K[8]) - (U[10]) / (93555. * K[10])) * gminus;
+    A[4] = 1. / (3. * k) - (U[2]) / (45. * K[3]) + (2 * U[4]) / (945. * K[5]) - -((U[6]) / (4725. * K[7])) +
+           (2 * U[8]) / (93555. * K[9]) - -((1382 * U[10]) / (6.38512875e8 * K[11]));
+    A[5] = 0.5 + (u) / (6. * k) - (U[3]) / (90. * K[3]) + (U[5]) / (945. * K[5]) - -((U[7]) / (9450. * K[7])) +
+           (U[9]) / (93555. * K[9]);
+  }
+}
+
+// contravariant component dd (1..3) of a Cartesian velocity in cell c
+__device__ __forceinline__ double contravariant(const double *xi, size_t Nc, int c, int dd, double u, double v, double w) {
+  return u * xi[(size_t)(dd - 1 + 0) * Nc + c] + v * xi[(size_t)(dd - 1 + 3) * Nc + c] + w * xi[(size_t)(dd - 1 + 6) * Nc + c];
+}
+
+// calculate_velocity_nim_constants_formulation2, first pass (nim.f90:165-289)
+__global__ void __launch_bounds__(BLK) k_vel_coef_A(Dims d, Geo g, Fields F, Phys P) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.Nc) return;
+  const size_t Nc = d.Nc;
+  const double ut = F.ct[0][c], vt = F.ct[1][c], wt = F.ct[2][c];
+  for (int dd = 1; dd <= 3; ++dd) {
+    const double u = contravariant(g.xi, Nc, c, dd, ut, vt, wt);
+    double A[6];
+    nim_direction(u, g.gij[(size_t)(dd - 1 + 3 * (dd - 1)) * Nc + c] * P.nu, g.gfd[(2 * (dd - 1)) * Nc + c],
+                  g.gfd[(2 * (dd - 1) + 1) * Nc + c], P.v_limit, A);
+    for (int k = 0; k < 6; ++k) F.MA[(size_t)(3 * k + dd - 1) * Nc + c] = A[k];
+  }
+}
+
+// M_F4 and M_F1..3 from M_A (nim.f90:293-328); also used for the
+// temperature's MT_F (nim.f90:466-500).
+__device__ __forceinline__ void form_F4(const double A[3][6], double DT, double F4[8]) {
+  F4[1] = 0.5 * (1. / A[0][4] + 1. / A[1][4] + 1. / A[2][4] - 1. / DT);
+  F4[2] = -(A[0][5] / A[0][4]);
+  F4[3] = (A[0][5] - 1.) / A[0][4];
+  F4[4] = -(A[1][5] / A[1][4]);
+  F4[5] = (A[1][5] - 1.) / A[1][4];
+  F4[6] = -(A[2][5] / A[2][4]);
+  F4[7] = (A[2][5] - 1.) / A[2][4];
+  F4[0] = F4[1] + F4[2] + F4[3] + F4[4] + F4[5] + F4[6] + F4[7];
+}
+__device__ __forceinline__ void form_Fd(const double Ai[6], const double A2[6], double G[5]) {
+  G[1] = Ai[2] - (Ai[0] * Ai[5] / Ai[4]);
+  G[2] = A2[3] - A2[1] / A2[4] + A2[1] * A2[5] / A2[4];
+  G[3] = Ai[0] / (2. * Ai[4]);
+  G[4] = A2[1] / (2. * A2[4]);
+  G[0] = G[1] + G[2] + 2. * G[3] + 2. * G[4];
+}
+
+__global__ void __launch_bounds__(BLK) k_vel_coef_F(Dims d, Fields F, Phys P) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.Nc) return;
+  const Cell x = Cell::of(d, c);
+  const size_t Nc = d.Nc;
+  double A[3][6];
+  for (int dd = 0; dd < 3; ++dd)
+    for (int k = 0; k < 6; ++k) A[dd][k] = F.MA[(size_t)(3 * k + dd) * Nc + c];
+  double F4[8];
+  form_F4(A, P.DT, F4);
+  for (int k = 0; k < 8; ++k) F.MF4[(size_t)k * Nc + c] = F4[k];
+  for (int dd = 1; dd <= 3; ++dd) {
+    double G[5] = {0., 0., 0., 0., 0.};
+    if (x.has_nb(d, 2 * dd)) {
+      const int i2 = x.nb(d, 2 * dd).c;
+      double A2[6];
+      for (int k = 0; k < 6; ++k) A2[k] = F.MA[(size_t)(3 * k + dd - 1) * Nc + i2];
+      form_Fd(A[dd - 1], A2, G);
+    }
+    for (int k = 0; k < 5; ++k) F.MF[(size_t)(5 * (dd - 1) + k) * Nc + c] = G[k];
+  }
+}
+
+// =========================================================== iteration
+__device__ __forceinline__ int parity(const Ctrl *ctl) { return ctl->iter & 1; }
+
+// Green-Gauss derivative dphi_dx2/dy2/dz2 (nse.f90:2866-2903), component cc
+__device__ __forceinline__ double green_gauss(const Geo &g, size_t NF, double invV, const double phi[7],
+                                              const int f[7], int cc) {
+  const double *A = g.area, *n = g.normal + cc * NF;
+  return invV * (phi[2] * A[f[2]] * (n[f[2]]) - phi[1] * A[f[1]] * (n[f[1]]) + phi[4] * A[f[4]] * (n[f[4]]) -
+                 phi[3] * A[f[3]] * (n[f[3]]) + phi[6] * A[f[6]] * (n[f[6]]) - phi[5] * A[f[5]] * (n[f[5]]));
+}
+
+// Derivative of face field phi along local direction e on face fpos of cell
+// x: centred, or second-order one-sided at walls (the ni/nj/nk stencils of
+// calculate_R_D2, nse.f90:1635-1838; integrate_pressure_field_i; bc.f90).
+__device__ __forceinline__ double tangential(const Dims &d, const double *__restrict__ phi, const Cell &x, int fpos,
+                                             int e) {
+  const bool lo = !x.has_nb(d, 2 * e - 1), hi = !x.has_nb(d, 2 * e);
+  if (lo) {
+    const Cell m2 = x.nb(d, 2 * e), m3 = m2.nb(d, 2 * e);
+    return (-(3 * phi[x.face(d, fpos)]) + 4 * phi[m2.face(d, fpos)] - phi[m3.face(d, fpos)]) / 4.;
+  } else if (hi) {
+    const Cell m1 = x.nb(d, 2 * e - 1), m3 = m1.nb(d, 2 * e - 1);
+    return (3 * phi[x.face(d, fpos)] - 4 * phi[m1.face(d, fpos)] + phi[m3.face(d, fpos)]) / 4.;
+  }
+  return (phi[x.nb(d, 2 * e).face(d, fpos)] - phi[x.nb(d, 2 * e - 1).face(d, fpos)]) / 4.;
+}
+
+// G_i d_i phi - g^ij d_ij phi of calculate_R_D2 / R_D_p2 / R_D_T
+// (nse.f90:1852-1859, 1995-1996, 2132-2133), before the coefficient.
+__device__ __forceinline__ double diffusion_source(const Dims &d, const Geo &g, const double *__restrict__ phi,
+                                                   const Cell &x, const int f[7]) {
+  const size_t Nc = d.Nc;
+  const int c = x.c;
+  const double pxy = 0.5 * (tangential(d, phi, x, 2, 2) - tangential(d, phi, x, 1, 2));
+  const double pzy = 0.5 * (tangential(d, phi, x, 6, 2) - tangential(d, phi, x, 5, 2));
+  const double pyx = 0.5 * (tangential(d, phi, x, 4, 1) - tangential(d, phi, x, 3, 1));
+  const double pzx = 0.5 * (tangential(d, phi, x, 6, 1) - tangential(d, phi, x, 5, 1));
+  const double pxz = 0.5 * (tangential(d, phi, x, 2, 3) - tangential(d, phi, x, 1, 3));
+  const double pyz = 0.5 * (tangential(d, phi, x, 4, 3) - tangential(d, phi, x, 3, 3));
+  const double px = (phi[f[2]] - phi[f[1]]) / 2.;
+  const double py = (phi[f[4]] - phi[f[3]]) / 2.;
+  const double pz = (phi[f[6]] - phi[f[5]]) / 2.;
+  const double *G = g.G, *gij = g.gij;
+  return (G[c] * px + G[Nc + c] * py + G[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy - gij[1 * Nc + c] * pyx -
+          gij[6 * Nc + c] * pxz - gij[2 * Nc + c] * pzx - gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
+}
+
+__device__ __forceinline__ void cell_faces(const Dims &d, const Cell &x, int f[7]) {
+  f[1] = x.c + d.NT * x.k;
+  f[2] = f[1] + d.NT;
+  f[3] = d.offT + x.c;
+  f[4] = d.offT + x.c - x.i + ((x.i == d.NT - 1) ? 0 : x.i + 1);
+  f[5] = d.offZ + x.c;
+  f[6] = f[5] + d.plane;
+}
+
+// Cell-average update (nse.f90:840-848; T: 1018-1026)
+__device__ __forceinline__ double cell_update(const double *__restrict__ fr, const int f[7], double c, double cold,
+                                              double B, const double F4[8], double w) {
+  return (1 - w) * c +
+         (w / F4[0]) * (+F4[1] * cold + F4[2] * fr[f[1]] + F4[3] * fr[f[2]] + F4[4] * fr[f[3]] + F4[5] * fr[f[4]] +
+                        F4[6] * fr[f[5]] + F4[7] * fr[f[6]] + B);
+}
+
+// +xi_d face update (nse.f90:878-1005; T: 1033-1088)
+__device__ __forceinline__ double face_update(const Dims &d, const double *__restrict__ fr, const double *__restrict__ cv,
+                                              const double *__restrict__ co, const double Fd[5], double dg0,
+                                              double dg1, int dd, const Cell &x, const Cell &x2, double w) {
+  const int e1 = tr1(dd), e2 = tr2(dd);
+  const double B3 = (dg0) * (fr[x.face(d, 2 * e1)] - fr[x.face(d, 2 * e1 - 1)] + fr[x2.face(d, 2 * e1)] -
+                             fr[x2.face(d, 2 * e1 - 1)]) / 4.0;
+  const double B4 = (dg1) * (fr[x.face(d, 2 * e2)] - fr[x.face(d, 2 * e2 - 1)] + fr[x2.face(d, 2 * e2)] -
+                             fr[x2.face(d, 2 * e2 - 1)]) / 4.0;
+  return (1 - w) * fr[x.face(d, 2 * dd)] +
+         (w / Fd[0]) * (+Fd[1] * fr[x.face(d, 2 * dd - 1)] + Fd[2] * fr[x2.face(d, 2 * dd)] +
+                        Fd[3] * (cv[x.c] + co[x.c]) + Fd[4] * (cv[x2.c] + co[x2.c]) - B3 - B4);
+}
+
+__device__ __forceinline__ double errv(double nw, double old, bool first) { return fabs(nw - (first ? 0.0 : old)); }
+// max that keeps a NaN (fmax would drop it and hide a blow-up)
+__device__ __forceinline__ double nmax(double a, double b) { return (b > a || b != b) ? b : a; }
+
+// ---- K1: velocity sources + cell update (update_velocity_sources
+// nse.f90:199-211 with calculate_gforces 2484-2502, calculate_R_b 1562-1592,
+// calculate_R_D2 1628-1860; cell part of integrate_velocity_field_formulation2_i
+// 839-872).  R_C (calculate_R_c_new, 1393-1434) is identically zero.
+__global__ void __launch_bounds__(BLK) k_vel_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+  if (ctl->done) return;
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double e[3] = {0., 0., 0.};
+  if (c < d.Nc) {
+    const Cell x = Cell::of(d, c);
+    const size_t Nc = d.Nc, NF = d.NF;
+    int f[7];
+    cell_faces(d, x, f);
+    const double *fp = F.f[3] + par * NF;
+    const double bz = -(P.g_beta * 0.5 * (F.c[3][c] + F.co[3][c]));
+    double pf[7];
+    for (int k = 1; k <= 6; ++k) pf[k] = fp[f[k]];
+    const double invV = 1. / g.vol[c];
+    const double RB[3] = {0. + P.inv_rho * green_gauss(g, NF, invV, pf, f, 0),
+                          0. + P.inv_rho * green_gauss(g, NF, invV, pf, f, 1),
+                          bz + P.inv_rho * green_gauss(g, NF, invV, pf, f, 2)};
+    double F4[8];
+    for (int k = 0; k < 8; ++k) F4[k] = F.MF4[(size_t)k * Nc + c];
+    for (int q = 0; q < 3; ++q) {
+      const double *fr = F.f[q] + par * NF;
+      const double RD = P.inv_Re * diffusion_source(d, g, fr, x, f);
+      const double B = (0. + RD + RB[q]);
+      const double cold = F.c[q][c];
+      const double nw = cell_update(fr, f, cold, F.co[q][c], B, F4, P.w[q]);
+      F.c[q][c] = nw;
+      e[q] = errv(nw, cold, first);
+    }
+  }
+  block_max<3>(e, ctl->err[par]);
+}
+
+// ---- K2: +xi face updates of u, v, w (nse.f90:878-1005)
+__global__ void __launch_bounds__(BLK) k_vel_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+  if (ctl->done) return;
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double e[3] = {0., 0., 0.};
+  if (c < d.Nc) {
+    const Cell x = Cell::of(d, c);
+    const size_t Nc = d.Nc, NF = d.NF;
+    for (int dd = 1; dd <= 3; ++dd) {
+      if (!x.has_nb(d, 2 * dd)) continue;
+      const Cell x2 = x.nb(d, 2 * dd);
+      double Fd[5];
+      for (int k = 0; k < 5; ++k) Fd[k] = F.MF[(size_t)(5 * (dd - 1) + k) * Nc + c];
+      const double dg0 = g.dg[(2 * (dd - 1)) * Nc + c], dg1 = g.dg[(2 * (dd - 1) + 1) * Nc + c];
+      const int fo = x.face(d, 2 * dd);
+      for (int q = 0; q < 3; ++q) {
+        const double *fr = F.f[q] + par * NF;
+        const double nw = face_update(d, fr, F.c[q], F.co[q], Fd, dg0, dg1, dd, x, x2, P.w[q]);
+        F.f[q][(1 - par) * NF + fo] = nw;
+        e[q] = nmax(e[q], errv(nw, fr[fo], first));
+      }
+    }
+  }
+  block_max<3>(e, ctl->err[par]);
+}
+
+// ---- K3: pressure sources (calculate_R_b_p nse.f90:2362-2407,
+// calculate_R_D_p2 1863-1997)
+__global__ void __launch_bounds__(BLK) k_p_src(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+  if (ctl->done) return;
+  const int par = parity(ctl);
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.Nc) return;
+  const Cell x = Cell::of(d, c);
+  const size_t NF = d.NF;
+  int f[7];
+  cell_faces(d, x, f);
+  const double *fu = F.f[0] + (1 - par) * NF, *fv = F.f[1] + (1 - par) * NF, *fw = F.f[2] + (1 - par) * NF;
+  const double *fT = F.f[4] + par * NF, *fp = F.f[3] + par * NF;
+  double uf[7], vf[7], wf[7], bzf[7];
+  for (int k = 1; k <= 6; ++k) {
+    uf[k] = fu[f[k]];
+    vf[k] = fv[f[k]];
+    wf[k] = fw[f[k]];
+    bzf[k] = -(P.g_beta * (fT[f[k]]));
+  }
+  const double invV = 1. / g.vol[c];
+  const double du_dx = green_gauss(g, NF, invV, uf, f, 0), du_dy = green_gauss(g, NF, invV, uf, f, 1),
+               du_dz = green_gauss(g, NF, invV, uf, f, 2);
+  const double dv_dx = green_gauss(g, NF, invV, vf, f, 0), dv_dy = green_gauss(g, NF, invV, vf, f, 1),
+               dv_dz = green_gauss(g, NF, invV, vf, f, 2);
+  const double dw_dx = green_gauss(g, NF, invV, wf, f, 0), dw_dy = green_gauss(g, NF, invV, wf, f, 1),
+               dw_dz = green_gauss(g, NF, invV, wf, f, 2);
+  const double dbz_dz = green_gauss(g, NF, invV, bzf, f, 2);
+  const double Dila = du_dx + dv_dy + dw_dz;
+  F.dila[c] = Dila;
+  const double RBp = -(du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) -
+                     2.0 * (du_dy * dv_dx + dv_dz * dw_dy + dw_dx * du_dz) - dbz_dz + Dila / (2 * P.DT);
+  const double RDp = P.inv_rho * diffusion_source(d, g, fp, x, f);
+  F.Rp[c] = RDp + RBp;
+}
+
+// ---- K4: apply_pressure_bc (bc.f90:141-342), reading cur, writing next
+__global__ void __launch_bounds__(BLK) k_p_bc(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+  if (ctl->done) return;
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  double e[1] = {0.};
+  if (b < d.NBF) {
+    const size_t NF = d.NF, NB = d.NBF;
+    const BFace B = bface(d, b);
+    const Cell M1 = B.cell;
+    const int pos = B.pos;
+    const int fw0 = M1.face(d, pos);
+    const double *pr = F.f[3] + par * NF;
+    const double *fu = F.f[0] + (1 - par) * NF, *fv = F.f[1] + (1 - par) * NF, *fwv = F.f[2] + (1 - par) * NF;
+    const double n[3] = {g.normal[fw0], g.normal[NF + fw0], g.normal[2 * NF + fw0]};
+    const double bvec[3] = {0., 0., -(P.g_beta * (F.f[4][par * NF + fw0]))};
+    const double b_n = dot3(bvec, n);
+    double vn[6];
+    for (int j = 1; j <= 5; ++j) {
+      const int pt = g.bcpts[(j - 1) * NB + b];
+      const double v[3] = {fu[pt], fv[pt], fwv[pt]};
+      vn[j] = dot3(v, n);
+    }
+    const double *a = g.bca;
+    const double d2udn2 = -(a[b] * vn[1]) - a[NB + b] * vn[2] - a[2 * NB + b] * vn[3] - a[3 * NB + b] * vn[4] -
+                          a[4 * NB + b] * vn[5];
+    const int dd = (pos + 1) / 2;
+    const double B2 = tangential(d, pr, M1, pos, tr1(dd)) * g.bcg[b];
+    const double B3 = tangential(d, pr, M1, pos, tr2(dd)) * g.bcg[NB + b];
+    const double *ap = g.bcap;
+    const double B1 = ap[7 * NB + b] * (F.Rp[M1.c]);
+    double s = 0.0;
+    bool firstterm = true;
+    for (int k = 1; k <= 6; ++k) {
+      if (k == pos) continue;
+      const double t = ap[(k - 1) * NB + b] * pr[M1.face(d, k)];
+      s = firstterm ? -t : s - t;
+      firstterm = false;
+    }
+    const double w = P.w_p2;
+    const double nw = (1 - w) * pr[fw0] + w / (ap[(pos - 1) * NB + b]) * (s + B1 - B2 - B3 + (P.nu * P.rho * d2udn2 - b_n * P.rho));
+    F.f[3][(1 - par) * NF + fw0] = nw;
+    e[0] = errv(nw, pr[fw0], first);
+  }
+  block_max<1>(e, ctl->err[par] + 3);
+}
+
+__global__ void k_p_bc_copy(Dims d, Fields F, Ctrl *ctl) {
+  if (ctl->done) return;
+  const int par = parity(ctl);
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.NBF) return;
+  const BFace B = bface(d, b);
+  const int f = B.cell.face(d, B.pos);
+  F.f[3][par * (size_t)d.NF + f] = F.f[3][(1 - par) * (size_t)d.NF + f];
+}
+
+// ---- K5: integrate_pressure_field_i (nse.f90:1091-1289), cur -> next
+__global__ void __launch_bounds__(BLK) k_p_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+  if (ctl->done) return;
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double e[1] = {0.};
+  if (c < d.Nc) {
+    const Cell x = Cell::of(d, c);
+    const size_t Nc = d.Nc, NF = d.NF;
+    const double *pr = F.f[3] + par * NF;
+    // (coefficient, face, cell) of the ten off-diagonal terms, source order
+    const unsigned char tab[3][10][3] = {
+        {{1, 1, 1}, {3, 2, 2}, {4, 3, 1}, {5, 4, 1}, {6, 3, 2}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
+        {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
+        {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {6, 4, 1}, {7, 3, 2}, {8, 4, 2}, {9, 5, 1}, {11, 6, 2}}};
+    const int diag[3] = {2, 6, 10};
+#pragma unroll
+    for (int dd = 1; dd <= 3; ++dd) {
+      if (!x.has_nb(d, 2 * dd)) continue;
+      const Cell n2 = x.nb(d, 2 * dd);
+      const double *A = g.AA + (size_t)15 * (dd - 1) * Nc;
+      const double B1 = (F.Rp[c]) * A[12 * Nc + c];
+      const double B2 = (F.Rp[n2.c]) * A[14 * Nc + c];
+      const double B3 = (g.dg[(2 * (dd - 1)) * Nc + c]) * tangential(d, pr, x, 2 * dd, tr1(dd));
+      const double B4 = (g.dg[(2 * (dd - 1) + 1) * Nc + c]) * tangential(d, pr, x, 2 * dd, tr2(dd));
+      double s = 0.0;
+#pragma unroll
+      for (int t = 0; t < 10; ++t) {
+        const Cell &cl = (tab[dd - 1][t][2] == 1) ? x : n2;
+        const double term = A[(size_t)(tab[dd - 1][t][0] - 1) * Nc + c] * pr[cl.face(d, tab[dd - 1][t][1])];
+        s = (t == 0) ? -term : s - term;
+      }
+      const int fo = x.face(d, 2 * dd);
+      const double w = P.w_p;
+      const double nw = (1 - w) * pr[fo] + w / (A[(size_t)(diag[dd - 1] - 1) * Nc + c]) * (s + B1 + B2 + B3 + B4);
+      F.f[3][(1 - par) * NF + fo] = nw;
+      e[0] = nmax(e[0], errv(nw, pr[fo], first));
+    }
+  }
+  block_max<1>(e, ctl->err[par] + 3);
+}
+
+// ---- K5b (is_dpdx_tolerance): cell pressure gradients (nse.f90:292-307)
+__global__ void __launch_bounds__(BLK) k_p_dpdx(Dims d, Geo g, Fields F, Ctrl *ctl) {
+  if (ctl->done) return;
+  const int par = parity(ctl);
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double e[1] = {0.};
+  if (c < d.Nc) {
+    const Cell x = Cell::of(d, c);
+    const size_t Nc = d.Nc, NF = d.NF;
+    int f[7];
+    cell_faces(d, x, f);
+    const double *p = F.f[3] + (1 - par) * NF;
+    const double v[3] = {(p[f[2]] - p[f[1]]) / 2. * g.xi[0 * Nc + c], (p[f[4]] - p[f[3]]) / 2. * g.xi[4 * Nc + c],
+                         (p[f[6]] - p[f[5]]) / 2. * g.xi[8 * Nc + c]};
+    for (int q = 0; q < 3; ++q) {
+      e[0] = nmax(e[0], fabs(v[q] - F.dpd[q * Nc + c]));
+      F.dpd[q * Nc + c] = v[q];
+    }
+  }
+  block_max<1>(e, ctl->err[par] + 5);
+}
+
+// ---- K6: apply_zero_flux (bc.f90:345-390) on the z walls, in place
+__global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, Geo g, Fields F, Ctrl *ctl) {
+  if (ctl->done) return;
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  double e[1] = {0.};
+  if (b < 2 * d.plane) {
+    const size_t NF = d.NF, NB = d.NBF;
+    const BFace B = bface(d, b);
+    const int in = (B.pos == 5) ? 6 : 5;
+    const Cell c2 = B.cell.nb(d, in), c3 = c2.nb(d, in);
+    double *T = F.f[4] + par * NF;
+    const int f1 = B.cell.face(d, B.pos);
+    const double nw = (+g.zf[NB + b] * T[B.cell.face(d, in)] - g.zf[2 * NB + b] * T[c2.face(d, in)] +
+                       g.zf[3 * NB + b] * T[c3.face(d, in)]) / g.zf[b];
+    e[0] = errv(nw, T[f1], first);
+    T[f1] = nw;
+  }
+  block_max<1>(e, ctl->err[par] + 4);
+}
+
+// ---- K7: calculate_temperature_nim_constants_formulation2 (nim.f90:334-502),
+// calculate_R_D_T (nse.f90:2000-2134) and the cell update of T (1017-1026)
+__global__ void __launch_bounds__(BLK) k_T_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+  if (ctl->done) return;
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double e[1] = {0.};
+  if (c < d.Nc) {
+    const Cell x = Cell::of(d, c);
+    const size_t Nc = d.Nc, NF = d.NF;
+    auto coefA = [&](int cell, int dd, double A[6]) {
+      const double ut = 0.5 * (F.c[0][cell] + F.co[0][cell]);
+      const double vt = 0.5 * (F.c[1][cell] + F.co[1][cell]);
+      const double wt = 0.5 * (F.c[2][cell] + F.co[2][cell]);
+      const double u = contravariant(g.xi, Nc, cell, dd, ut, vt, wt);
+      nim_direction(u, g.gij[(size_t)(dd - 1 + 3 * (dd - 1)) * Nc + cell] * P.alpha, g.gfd[(2 * (dd - 1)) * Nc + cell],
+                    g.gfd[(2 * (dd - 1) + 1) * Nc + cell], P.v_limit, A);
+    };
+    double A[3][6];
+    for (int dd = 1; dd <= 3; ++dd) coefA(c, dd, A[dd - 1]);
+    double F4[8];
+    form_F4(A, P.DT, F4);
+    for (int dd = 1; dd <= 3; ++dd) {
+      double G[5] = {0., 0., 0., 0., 0.};
+      if (x.has_nb(d, 2 * dd)) {
+        double A2[6];
+        coefA(x.nb(d, 2 * dd).c, dd, A2);
+        form_Fd(A[dd - 1], A2, G);
+      }
+      for (int k = 0; k < 5; ++k) F.MTF[(size_t)(5 * (dd - 1) + k) * Nc + c] = G[k];
+    }
+    int f[7];
+    cell_faces(d, x, f);
+    const double *T = F.f[4] + par * NF;
+    const double RDT = P.alpha * diffusion_source(d, g, T, x, f);
+    const double cold = F.c[3][c];
+    const double nw = cell_update(T, f, cold, F.co[3][c], (RDT + 0.), F4, P.w[3]);
+    F.c[3][c] = nw;
+    e[0] = errv(nw, cold, first);
+  }
+  block_max<1>(e, ctl->err[par] + 4);
+}
+
+// ---- K8: +xi face updates of T (nse.f90:1033-1088), cur -> next; the z-wall
+// values set by apply_zero_flux travel to the next half too
+__global__ void __launch_bounds__(BLK) k_T_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+  if (ctl->done) return;
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double e[1] = {0.};
+  if (c < d.Nc) {
+    const Cell x = Cell::of(d, c);
+    const size_t Nc = d.Nc, NF = d.NF;
+    const double *T = F.f[4] + par * NF;
+    double *Tn = F.f[4] + (1 - par) * NF;
+    for (int dd = 1; dd <= 3; ++dd) {
+      if (!x.has_nb(d, 2 * dd)) continue;
+      const Cell x2 = x.nb(d, 2 * dd);
+      double Fd[5];
+      for (int k = 0; k < 5; ++k) Fd[k] = F.MTF[(size_t)(5 * (dd - 1) + k) * Nc + c];
+      const int fo = x.face(d, 2 * dd);
+      const double nw = face_update(d, T, F.c[3], F.co[3], Fd, g.dg[(2 * (dd - 1)) * Nc + c],
+                                    g.dg[(2 * (dd - 1) + 1) * Nc + c], dd, x, x2, P.w[3]);
+      Tn[fo] = nw;
+      e[0] = nmax(e[0], errv(nw, T[fo], first));
+    }
+    if (x.k == 0) Tn[x.face(d, 5)] = T[x.face(d, 5)];
+    if (x.k == d.NZ - 1) Tn[x.face(d, 6)] = T[x.face(d, 6)];
+  }
+  block_max<1>(e, ctl->err[par] + 4);
+}
+
+// ---- K9: end of one pass (find_error's maxima, the do-while test of
+// nse.f90:129 and the max_iters guard)
+__global__ void k_iter_end(Ctrl *ctl, Phys P) {
+  if (ctl->done) return;
+  const int par = ctl->iter & 1;
+  double e[5];
+  bool finite = true;
+  for (int q = 0; q < 5; ++q) {
+    unsigned long long b = ctl->err[par][q];
+    if (q == 3 && P.dpdx_tolerance) b = ctl->err[par][5];
+    if (b >= 0x7FF0000000000000ull) finite = false;
+    e[q] = __longlong_as_double((long long)b);
+    if (ctl->first) e[q] = nmax(e[q], __longlong_as_double((long long)ctl->wall_floor[q]));
+    ctl->last_err[q] = e[q];
+  }
+  for (int q = 0; q < 8; ++q) ctl->err[1 - par][q] = 0ull;
+  ctl->iter += 1;
+  ctl->step_iters += 1;
+  ctl->first = 0;
+  bool busy = false;
+  for (int q = 0; q < 5; ++q) busy = busy || (e[q] > P.tol[q]);
+  if (!finite) {
+    ctl->done = 1;
+    ctl->status = -4;  // NIM_ERR_NONFINITE
+  } else if (!busy) {
+    ctl->done = 1;
+  } else if (P.max_iters > 0 && ctl->step_iters >= P.max_iters) {
+    ctl->done = 1;
+    ctl->status = -3;  // NIM_ERR_NOT_CONVERGED
+  }
+}
+
+// ====================================================== end of integrate
+// check_steady_state (nse.f90:1316-1332) + evaluate_D (nse.f90:2504-2537)
+__global__ void __launch_bounds__(BLK) k_after_integrate(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl, int nblk) {
+  const int par = parity(ctl);
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double m[2] = {0., 0.}, s[1] = {0.};
+  if (c < d.Nc) {
+    const Cell x = Cell::of(d, c);
+    const size_t NF = d.NF;
+    const double tdt = 2 * P.DT;
+    double mu = 0.;
+    for (int q = 0; q < 3; ++q) mu = nmax(mu, fabs(F.c[q][c] - F.co[q][c]) / tdt);
+    m[0] = mu;
+    m[1] = fabs(F.c[3][c] - F.co[3][c]) / tdt;
+    int f[7];
+    cell_faces(d, x, f);
+    double uf[7], vf[7], wf[7];
+    for (int k = 1; k <= 6; ++k) {
+      uf[k] = F.f[0][par * NF + f[k]];
+      vf[k] = F.f[1][par * NF + f[k]];
+      wf[k] = F.f[2][par * NF + f[k]];
+    }
+    const double invV = 1. / g.vol[c];
+    const double Dila = green_gauss(g, NF, invV, uf, f, 0) + green_gauss(g, NF, invV, vf, f, 1) +
+                        green_gauss(g, NF, invV, wf, f, 2);
+    F.dila[c] = Dila;
+    s[0] = Dila * Dila;
+  }
+  block_max<2>(m, ctl->red);
+  block_sum<1>(s, F.part, nblk);
+}
+
+// one block: fixed-order sum of the per-block partials
+__global__ void k_finish_sum(const double *part, int nblk, int nsum, double *out) {
+  __shared__ double sm[BLK];
+  for (int n = 0; n < nsum; ++n) {
+    double acc = 0.;
+    for (int b = threadIdx.x; b < nblk; b += BLK) acc = acc + part[(size_t)n * nblk + b];
+    sm[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = BLK / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) sm[threadIdx.x] = sm[threadIdx.x] + sm[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[n] = sm[0];
+    __syncthreads();
+  }
+}
+
+// update_time_step (nse.f90:1292-1313)
+__global__ void __launch_bounds__(BLK) k_update_time(Dims d, Fields F, Ctrl *ctl) {
+  const int par = parity(ctl);
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.Nc) return;
+  const Cell x = Cell::of(d, c);
+  for (int q = 0; q < 4; ++q) {
+    F.ct[q][c] = (F.co[q][c] + F.c[q][c]) / 2.;
+    F.co[q][c] = F.c[q][c];
+  }
+  int f[7];
+  cell_faces(d, x, f);
+  const double *p = F.f[3] + par * (size_t)d.NF;
+  F.mp[c] = (p[f[1]] + p[f[2]] + p[f[3]] + p[f[4]] + p[f[5]] + p[f[6]]) / 6.0;
+  F.dila_old[c] = F.dila[c];
+}
+
+// find_Nu2 (nse.f90:2699-2798): wall-normal one-sided dT/dn on the inner
+// (position 1) and outer (position 2) walls, area weighted.
+__global__ void __launch_bounds__(BLK) k_nusselt(Dims d, Geo g, Fields F, Ctrl *ctl, int nblk) {
+  const int par = parity(ctl);
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  double s[4] = {0., 0., 0., 0.};  // sum1, sumA1 (outer), sum2, sumA2 (inner)
+  const int nr = 2 * d.NT * d.NZ;
+  if (q < nr) {
+    const int b = 2 * d.plane + q;
+    const size_t NF = d.NF, NB = d.NBF;
+    const BFace B = bface(d, b);
+    const int in = (B.pos == 1) ? 2 : 1;
+    const Cell c2 = B.cell.nb(d, in), c3 = c2.nb(d, in);
+    const double *T = F.f[4] + par * NF;
+    const double *w = g.nuw;
+    const int f1 = B.cell.face(d, B.pos);
+    const double inner = -((w[b]) * T[f1]) + w[NB + b] * T[B.cell.face(d, in)] - w[2 * NB + b] * T[c2.face(d, in)] +
+                         w[3 * NB + b] * T[c3.face(d, in)];
+    const double dTdx = (B.pos == 1) ? -(inner) : inner;
+    const double A = g.area[f1];
+    if (B.pos == 1) {
+      s[2] = A * dTdx;
+      s[3] = A;
+    } else {
+      s[0] = A * dTdx;
+      s[1] = A;
+    }
+  }
+  block_sum<4>(s, F.part, nblk);
+}
+
+// max |value| of the Dirichlet walls per field (u, v, w, -, T): find_error
+// compares against zero-initialised *_old arrays on the first pass
+__global__ void k_wall_floor(Dims d, Geo g, Ctrl *ctl) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  double m[5] = {0., 0., 0., 0., 0.};
+  if (b < d.NBF) {
+    const BFace B = bface(d, b);
+    m[0] = fabs(g.bcval[b]);
+    m[1] = fabs(g.bcval[(size_t)d.NBF + b]);
+    m[2] = fabs(g.bcval[2 * (size_t)d.NBF + b]);
+    if (B.pos <= 2) m[4] = fabs(g.bcval[3 * (size_t)d.NBF + b]);  // r walls keep T; z walls are recomputed
+  }
+  block_max<5>(m, ctl->wall_floor);
+}
+
+}  // namespace nim

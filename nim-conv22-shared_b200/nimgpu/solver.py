@@ -1,0 +1,129 @@
+"""Python host mirror of the reference's solver interface over the C ABI.
+
+Method names follow the reference subroutines a Fortran host calls
+(solve_nse, nse.f90:23-85); each one is a single call into libnimgpu.so.
+There is no CPU path: without the CUDA library or a GPU the constructor
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from .mesh import Mesh, apply_temperature_noise
+
+
+def field_len(field: int, mesh: Mesh) -> int:
+    nf, nm, nb = mesh.nface, mesh.nmesh, mesh.nbcface
+    table = {
+        _abi.FACES_AREA: nf, _abi.FACES_NORMAL: 3 * nf, _abi.FACES_MID: 3 * nf,
+        _abi.FACES_TANGENTIAL: 3 * nf, _abi.FACES_BITANGENTIAL: 3 * nf,
+        _abi.MESHES_VOLUME: nm, _abi.MESHES_GIJ: 9 * nm, _abi.MESHES_XI_X: 9 * nm,
+        _abi.MESHES_G: 3 * nm, _abi.MESHES_GIJ_FACES: 54 * nm,
+        _abi.BCS_FACES_A: 5 * nb, _abi.BCS_FACES_AP: 8 * nb,
+        _abi.AA_PX: 15 * nm, _abi.AA_PY: 15 * nm, _abi.AA_PZ: 15 * nm,
+        _abi.M_F4: 8 * nm, _abi.M_F1: 5 * nm, _abi.M_F2: 5 * nm, _abi.M_F3: 5 * nm,
+    }
+    if field in table:
+        return table[field]
+    if field <= _abi.FACES_T:
+        return nf
+    if field <= _abi.MESHES_DILA:
+        return nm
+    raise ValueError(f"unknown field {field}")
+
+
+class NimSolver:
+    """One device-resident NIM context (include/nim_gpu.h)."""
+
+    def __init__(self, mesh: Mesh, params: _abi.Params):
+        self.lib = _abi.gpu_lib()
+        self.mesh = mesh
+        self.params = params
+        self._h = C.c_void_p()
+        _abi.check(self.lib.nim_gpu_create(C.byref(mesh.desc), C.byref(params), C.byref(self._h)),
+                   "nim_gpu_create")
+
+    # -- lifetime
+    def close(self):
+        if self._h:
+            self.lib.nim_gpu_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- the reference's call sites (nse.f90:34-73)
+    def initialize_nse(self):
+        """initialize_nse + apply_all_dirichlet_bcs (nse.f90:34-38)."""
+        _abi.check(self.lib.nim_gpu_init(self._h), "nim_gpu_init")
+
+    def calculate_velocity_nim_constants(self):
+        """calculate_velocity_nim_constants_formulation2 (nse.f90:52)."""
+        _abi.check(self.lib.nim_gpu_begin_step(self._h), "nim_gpu_begin_step")
+
+    def integrate_nse(self, raise_on_error: bool = True) -> _abi.StepStats:
+        """integrate_nse (nse.f90:57) with the max_iters guard."""
+        s = _abi.StepStats()
+        st = self.lib.nim_gpu_integrate(self._h, C.byref(s))
+        s.status = st
+        if raise_on_error:
+            _abi.check(st, "nim_gpu_integrate")
+        return s
+
+    def iterate(self, n: int) -> _abi.StepStats:
+        """Exactly n inner passes without the stop test."""
+        s = _abi.StepStats()
+        _abi.check(self.lib.nim_gpu_iterate(self._h, n, C.byref(s)), "nim_gpu_iterate")
+        return s
+
+    def update_time_step(self) -> _abi.StepStats:
+        """update_time_step + find_Nu2 (nse.f90:72-73)."""
+        s = _abi.StepStats()
+        _abi.check(self.lib.nim_gpu_end_step(self._h, C.byref(s)), "nim_gpu_end_step")
+        return s
+
+    def solve_nse(self, nsteps: int, raise_on_error: bool = True):
+        """nsteps of the time loop (nse.f90:47-75); returns per-step stats."""
+        arr = (_abi.StepStats * max(nsteps, 1))()
+        done = C.c_int32()
+        st = self.lib.nim_gpu_step(self._h, nsteps, arr, C.byref(done))
+        if raise_on_error:
+            _abi.check(st, "nim_gpu_step")
+        return [arr[i] for i in range(done.value)]
+
+    def synchronize(self):
+        _abi.check(self.lib.nim_gpu_synchronize(self._h), "nim_gpu_synchronize")
+
+    # -- host copies (write_data / write_restart / read_restart)
+    def download(self, field: int) -> np.ndarray:
+        n = field_len(field, self.mesh)
+        out = np.empty(n, dtype=np.float64)
+        _abi.check(self.lib.nim_gpu_download(self._h, field, out.ctypes.data_as(C.POINTER(C.c_double)), n),
+                   "nim_gpu_download")
+        return out
+
+    def upload(self, field: int, values: np.ndarray):
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        _abi.check(self.lib.nim_gpu_upload(self._h, field, a.ctypes.data_as(C.POINTER(C.c_double)), a.size),
+                   "nim_gpu_upload")
+
+    def get(self, field: int, n: int | None = None) -> np.ndarray:
+        return self.download(field)
+
+    def set(self, field: int, values: np.ndarray):
+        self.upload(field, values)
+
+    def add_temperature_noise(self, amp: float, seed: int):
+        apply_temperature_noise(self.get, self.set, self.mesh, amp, seed)

@@ -1,0 +1,55 @@
+/*
+ * nim_oracle.h -- CPU oracle for the NIM time advance (TEST INFRASTRUCTURE).
+ *
+ * A plain C++ restatement of the reference's live FP64 path (nse.f90,
+ * nim.f90, bc.f90, geometry.f90, curvilinear.f90, general.f90), used only by
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the
+ * checker.  Nothing in the product library calls it.
+ *
+ * Parity is unpinned: the reference ships no test, fixture or golden output
+ * and is Fortran, which this image cannot compile (no gfortran), so the
+ * oracle is pinned only by its own invariants (tests/test_oracle.py) and by
+ * the reference's structure it follows line by line.
+ *
+ * Two iteration schedules:
+ *   NIM_SCHED_SEQUENTIAL -- the reference's own order: one thread, cells in
+ *     number order, Gauss-Seidel inside every sweep (run.sh:2 pins
+ *     OMP_NUM_THREADS=1).  "faithful" mode.
+ *   NIM_SCHED_PARALLEL   -- the order the CUDA library uses: every sweep
+ *     reads the values from before the sweep (double-buffered faces).  Same
+ *     discrete fixed point, different path; used to check kernels step by
+ *     step.
+ */
+#ifndef NIM_ORACLE_H
+#define NIM_ORACLE_H
+#include <stdint.h>
+#include "nim_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { NIM_SCHED_SEQUENTIAL = 0, NIM_SCHED_PARALLEL = 1 };
+
+typedef struct nim_oracle nim_oracle;
+
+int nim_oracle_create(const nim_mesh_desc *mesh, const nim_params *params,
+                      int32_t schedule, int32_t threads, nim_oracle **out);
+int nim_oracle_init(nim_oracle *o);
+int nim_oracle_begin_step(nim_oracle *o);
+int nim_oracle_integrate(nim_oracle *o, nim_step_stats *stats);
+/* exactly n inner iterations, no convergence test; errors of the last one */
+int nim_oracle_iterate(nim_oracle *o, int32_t n, nim_step_stats *stats);
+int nim_oracle_end_step(nim_oracle *o, nim_step_stats *stats);
+int nim_oracle_step(nim_oracle *o, int32_t nsteps, nim_step_stats *per_step,
+                    int32_t *done);
+int nim_oracle_get(nim_oracle *o, int32_t field, double *out, int64_t n);
+int nim_oracle_set(nim_oracle *o, int32_t field, const double *in, int64_t n);
+/* max |R_C| seen by calculate_R_c_new in SEQUENTIAL mode (must be 0) */
+double nim_oracle_max_rc(nim_oracle *o);
+void nim_oracle_destroy(nim_oracle *o);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
