@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Benchmark of the NIM time advance: cell-iterations/s on the cylinder case.
+
+A step is one time step of the reference's solve_nse loop (nse.f90:47-75) on
+the 128x128x96 cylinder/hexagon mesh (Ra=1e5, Pr=0.71, dt=5e-4, FP64):
+calculate_velocity_nim_constants, the integrate_nse inner loop to the
+reference tolerances, update_time_step and find_Nu2.  The metric counts
+cells x inner iterations per second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun; each rank advances its own replica of the mesh
+(replicas only: no data crosses ranks) and the job value is the sum of all
+ranks' cell-iterations over the slowest rank's device time.
+
+--impl reference times the reference algorithm's CPU implementation (the
+oracle port of the Fortran, OpenMP threads as the reference uses them) on
+the host cores on the same workload, one inner iteration per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "nim-conv22-shared_b200"))
+
+import numpy as np  # noqa: E402
+
+CASE = "c2"
+METRIC = "NIM cell-iterations/s"
+UNIT = "cell-iterations/s"
+
+# Algorithmic HBM bytes of each kernel per cell and pass (FP64 doubles x 8):
+# the data the kernel must read and write once with structured connectivity
+# (faces counted as 3 per cell; geometry and coefficients as stored).
+KERNEL_BYTES_PER_CELL = {
+    "k_vel_cell": 8 * 53,   # faces p,u,v,w (12) T,T_old (2) area,normal,vol (13) G,g^ij (9) cells+old (6) M_F4 (8); write u,v,w (3)
+    "k_vel_face": 8 * 45,   # faces u,v,w (9) cells+old (6) M_F1..3 (15) dg (6); write faces (9)
+    "k_p_src": 8 * 39,      # faces u,v,w,T,p (15) area,normal,vol (13) G,g^ij (9); write dila,Rp (2)
+    "k_p_face": 8 * 52,     # faces p (3) Rp (1) AA used (39) dg (6); write faces p (3)
+    "k_T_cell": 8 * 54,     # cells+old u,v,w (6) xi (9) g^ij (9) gfd (6) faces T (3) G (3) T,T_old (2); write T, MT_F (16)
+    "k_T_face": 8 * 29,     # faces T (3) T,T_old (2) MT_F (15) dg (6); write faces T (3)
+}
+# per cell-iteration and per step, the survey's algorithmic model (FP64)
+SURVEY_BYTES_PER_CELL_ITER = 1880
+SURVEY_BYTES_PER_CELL_STEP = 776
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.idx), "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        try:
+            for line in Path(self.path).read_text().splitlines():
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        loaded = [s for s in sm if s > 0.3 * smax] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ------------------------------------------------------------ helpers
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def cpu_sample(case, threads: int, iters: int, schedule: int):
+    """Time `iters` inner iterations of the oracle (the reference's algorithm
+    on the CPU) on the same mesh; returns (cell-iterations/s, seconds)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import nimgpu
+    import oracle as O
+    mesh = nimgpu.Mesh(case.mesh_params())
+    o = O.Oracle(mesh, case.params(), schedule=schedule, threads=os.cpu_count() or 1)
+    o.init()  # geometry set-up on all cores, not timed
+    o.set_threads(threads)
+    nimgpu.apply_temperature_noise(o.get, o.set, mesh, case.noise, case.seed)
+    o.begin_step()
+    o.iterate(1)  # warm
+    t = time.perf_counter()
+    o.iterate(iters)
+    dt = time.perf_counter() - t
+    o.close()
+    return case.ncells * iters / dt, dt
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference algorithm on the host cores."""
+    if rank != 0:
+        return 0
+    from nimgpu import config
+    case = config.CASES[args.case]
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import nimgpu
+    import oracle as O
+    mesh = nimgpu.Mesh(case.mesh_params())
+    o = O.Oracle(mesh, case.params(), schedule=O.SEQUENTIAL, threads=threads)
+    o.init()
+    nimgpu.apply_temperature_noise(o.get, o.set, mesh, case.noise, case.seed)
+    o.begin_step()
+    for _ in range(args.warmup):
+        o.iterate(1)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        o.iterate(1)
+    dt = time.perf_counter() - t
+    value = case.ncells * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(case),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} inner iterations of step 1 on {args.case} "
+                                   f"({case.ncells} cells), reference cell order, OpenMP threads={threads}"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(case):
+    return {"workload": f"{case.name}: cylinder D=1 H=1, hexagon side 0.2, {case.n_theta}x{case.n_r}x{case.n_z} "
+                        f"O-grid (tanh 1.5), Ra={case.Ra:g} Pr={case.Pr:g} dt={case.dt:g}",
+            "cells": case.ncells, "Ra": case.Ra, "Pr": case.Pr, "dt": case.dt,
+            "parallelism": "replicas", "l2": "working set > L2 (126 MB): ~3 GB read per pass"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--case", default=CASE)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import nimgpu
+    from nimgpu import config, _abi
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+        pg = dist
+
+    case = config.CASES[args.case]
+    mesh = nimgpu.Mesh(case.mesh_params())
+    solver = nimgpu.NimSolver(mesh, case.params())
+    solver.initialize_nse()
+    solver.add_temperature_noise(case.noise, case.seed)
+    stream = torch.cuda.ExternalStream(solver.stream_handle)
+
+    for _ in range(max(args.warmup, 0)):
+        solver.solve_nse(1)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+
+    # ---------------- device-resident timed region
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = solver.launch_count()
+    ev0.record(stream)
+    stats = solver.solve_nse(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = solver.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    iters = sum(s.iters for s in stats)
+    cell_iters = case.ncells * iters
+    t_max = ms
+    total = cell_iters
+    if pg:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_max = float(t.item())
+        c = torch.tensor([float(cell_iters)], dtype=torch.float64, device="cuda")
+        pg.all_reduce(c, op=pg.ReduceOp.SUM)
+        total = float(c.item())
+    value = total / (t_max / 1e3)
+
+    # ---------------- end to end through the C ABI with host buffers: the
+    # host holds the state (read_restart / write_restart arrays) and every
+    # step uploads it, advances one step and downloads it again
+    up_fields = [_abi.FACES_U, _abi.FACES_V, _abi.FACES_W, _abi.FACES_P, _abi.FACES_T,
+                 _abi.MESHES_U, _abi.MESHES_V, _abi.MESHES_W, _abi.MESHES_T,
+                 _abi.MESHES_U_OLD, _abi.MESHES_V_OLD, _abi.MESHES_W_OLD, _abi.MESHES_T_OLD,
+                 _abi.MESHES_UT, _abi.MESHES_VT, _abi.MESHES_WT]
+    host = {f: torch.empty(nimgpu.field_len(f, mesh), dtype=torch.float64).pin_memory() for f in up_fields}
+    for f in up_fields:
+        host[f].numpy()[:] = solver.download(f)
+    h2d = sum(h.numel() * 8 for h in host.values())
+    d2h = h2d
+    e2e_steps = max(2, args.steps // 2)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_iters = 0
+    for _ in range(e2e_steps):
+        for f in up_fields:
+            solver.upload(f, host[f].numpy())
+        st = solver.solve_nse(1)
+        e2e_iters += sum(s.iters for s in st)
+        for f in up_fields:
+            host[f].numpy()[:] = solver.download(f)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_total = case.ncells * e2e_iters
+    if pg:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+        c = torch.tensor([float(e2e_total)], dtype=torch.float64, device="cuda")
+        pg.all_reduce(c, op=pg.ReduceOp.SUM)
+        e2e_total = float(c.item())
+    e2e_value = e2e_total / e2e_s
+
+    # ---------------- roofline of the dominant kernel (events per kernel)
+    prof = solver.profile_iterations(20)
+    peak, peak_kind = peaks()
+    shares = {k: v for k, v in prof.items() if v > 0}
+    tot = sum(shares.values())
+    dom = max(KERNEL_BYTES_PER_CELL, key=lambda k: prof.get(k, 0.0))
+    dom_ms = prof[dom]
+    achieved = KERNEL_BYTES_PER_CELL[dom] * case.ncells / (dom_ms / 1e3) / 1e9
+    iter_gbs = SURVEY_BYTES_PER_CELL_ITER * cell_iters / (ms / 1e3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, dt = cpu_sample(case, threads=1, iters=4, schedule=0)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"4 inner iterations of step 1 on {args.case} ({case.ncells} cells), "
+                         f"reference cell order, 1 thread ({dt:.1f} s)"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded mesh and T noise)",
+        "config": workload_config(case),
+        "iterations": iters, "iters_per_step": iters / max(len(stats), 1),
+        "hbm_gbs_iteration": iter_gbs,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "bytes_per_launch": KERNEL_BYTES_PER_CELL[dom] * case.ncells,
+                     "kernel_ms": dom_ms,
+                     "shares": {k: round(v / tot, 4) for k, v in shares.items()}},
+        "cpu_baseline": cpu,
+        "gpu_launches": launches,
+        "clocks": clk,
+        "nu_inner_last": stats[-1].nu_inner if stats else None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

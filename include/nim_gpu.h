@@ -204,6 +204,18 @@ int nim_gpu_step(nim_ctx *ctx, int32_t nsteps, nim_step_stats *per_step,
 int nim_gpu_download(nim_ctx *ctx, nim_field field, double *host, int64_t n);
 int nim_gpu_upload(nim_ctx *ctx, nim_field field, const double *host, int64_t n);
 
+/* Diagnostics and timing hooks (no counterpart in the reference).
+   nim_gpu_stream: the cudaStream_t every call of the context queues work on,
+   so a caller can record CUDA events on it.
+   nim_gpu_launch_count: kernels launched by the context since creation.
+   nim_gpu_profile_iterations: n inner passes launched one kernel at a time
+   with CUDA events around each; ms[k] receives the mean duration of kernel
+   k (names from nim_gpu_kernel_name); returns the number of kernels. */
+void *nim_gpu_stream(nim_ctx *ctx);
+int64_t nim_gpu_launch_count(nim_ctx *ctx);
+int nim_gpu_profile_iterations(nim_ctx *ctx, int32_t n, double *ms, int32_t cap);
+const char *nim_gpu_kernel_name(int32_t k);
+
 /* Block until all work queued on the context's stream has finished. */
 int nim_gpu_synchronize(nim_ctx *ctx);
 

@@ -58,6 +58,8 @@ struct nim_ctx {
   double TI = 0;
   int last_iters = 0;
   double host_sums[8] = {0};
+  long long launches = 0;    // kernels queued since creation
+  int kernels_per_iter = 0;
 };
 
 namespace {
@@ -190,6 +192,8 @@ int launch_iteration(nim_ctx *x) {
   k_T_face<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
   CK(cudaGetLastError());
+  x->kernels_per_iter = x->phys.dpdx_tolerance ? 11 : 10;
+  x->launches += x->kernels_per_iter;
   return NIM_OK;
 }
 
@@ -199,6 +203,7 @@ int build_graph(nim_ctx *x, int iters) {
     x->graph = nullptr;
   }
   cudaGraph_t g = nullptr;
+  const long long before = x->launches;
   CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
   for (int k = 0; k < iters; ++k) {
     const int st = launch_iteration(x);
@@ -209,6 +214,7 @@ int build_graph(nim_ctx *x, int iters) {
     }
   }
   CK(cudaStreamEndCapture(x->stream, &g));
+  x->launches = before;
   cudaError_t e = cudaGraphInstantiate(&x->graph, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return NIM_ERR_CUDA;
@@ -480,6 +486,7 @@ extern "C" int nim_gpu_begin_step(nim_ctx *x) {
   k_vel_coef_A<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->g, x->F, x->phys);
   k_vel_coef_F<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->F, x->phys);
   CK(cudaGetLastError());
+  x->launches += 3;
   x->in_step = true;
   return NIM_OK;
 }
@@ -529,6 +536,7 @@ extern "C" int nim_gpu_integrate(nim_ctx *x, nim_step_stats *s) {
   for (;;) {
     for (int k = 0; k < ahead; ++k) CK(cudaGraphLaunch(x->graph, x->stream));
     launched += (long long)ahead * G;
+    x->launches += (long long)ahead * G * x->kernels_per_iter;
     TRY(read_ctrl(x));
     if (x->ctl_host->done) break;
     if (launched >= cap) {
@@ -541,6 +549,7 @@ extern "C" int nim_gpu_integrate(nim_ctx *x, nim_step_stats *s) {
   k_after_integrate<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->g, x->F, x->phys, x->ctl, x->nblk_c);
   k_finish_sum<<<1, BLK, 0, x->stream>>>(x->F.part, x->nblk_c, 1, x->sums);
   CK(cudaGetLastError());
+  x->launches += 2;
   CK(cudaMemcpyAsync(x->host_sums, x->sums, sizeof(double), cudaMemcpyDeviceToHost, x->stream));
   TRY(read_ctrl(x));
   x->last_iters = x->ctl_host->step_iters;
@@ -563,6 +572,7 @@ extern "C" int nim_gpu_end_step(nim_ctx *x, nim_step_stats *s) {
   k_nusselt<<<gn, BLK, 0, x->stream>>>(d, x->g, x->F, x->ctl, gn);
   k_finish_sum<<<1, BLK, 0, x->stream>>>(x->F.part, gn, 4, x->sums);
   CK(cudaGetLastError());
+  x->launches += 3;
   CK(cudaMemcpyAsync(x->host_sums, x->sums, 4 * sizeof(double), cudaMemcpyDeviceToHost, x->stream));
   CK(cudaStreamSynchronize(x->stream));
   const int32_t step_done = x->STEP;
@@ -663,4 +673,66 @@ extern "C" void nim_gpu_destroy(nim_ctx *x) {
   if (x->ctl_host) cudaFreeHost(x->ctl_host);
   if (x->stream) cudaStreamDestroy(x->stream);
   delete x;
+}
+
+extern "C" void *nim_gpu_stream(nim_ctx *x) { return x ? (void *)x->stream : nullptr; }
+extern "C" int64_t nim_gpu_launch_count(nim_ctx *x) { return x ? x->launches : -1; }
+
+static const char *kKernelNames[] = {"k_vel_cell", "k_vel_face", "k_p_src",    "k_p_bc",  "k_p_bc_copy", "k_p_face",
+                                     "k_p_dpdx",   "k_zero_flux", "k_T_cell", "k_T_face", "k_iter_end"};
+extern "C" const char *nim_gpu_kernel_name(int32_t k) {
+  return (k >= 0 && k < (int32_t)(sizeof(kKernelNames) / sizeof(kKernelNames[0]))) ? kKernelNames[k] : "";
+}
+
+extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int32_t cap) {
+  const int NK = 11;
+  if (!x || n <= 0 || !ms || cap < NK) return NIM_ERR_BAD_ARG;
+  if (!x->initialized) return NIM_ERR_STATE;
+  const Dims &d = x->d;
+  cudaStream_t s = x->stream;
+  cudaEvent_t ev[NK + 1];
+  for (int k = 0; k <= NK; ++k) CK(cudaEventCreate(&ev[k]));
+  double acc[NK] = {0};
+  const Phys keep = x->phys;
+  x->phys.max_iters = 0;
+  for (int q = 0; q < 5; ++q) x->phys.tol[q] = -1.0;
+  k_step_reset<<<1, 1, 0, s>>>(x->ctl);
+  const int gc = x->nblk_c, gb = x->nblk_b;
+  for (int it = 0; it < n; ++it) {
+    CK(cudaEventRecord(ev[0], s));
+    k_vel_cell<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    CK(cudaEventRecord(ev[1], s));
+    k_vel_face<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    CK(cudaEventRecord(ev[2], s));
+    k_p_src<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    CK(cudaEventRecord(ev[3], s));
+    k_p_bc<<<gb, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    CK(cudaEventRecord(ev[4], s));
+    k_p_bc_copy<<<gb, BLK, 0, s>>>(d, x->F, x->ctl);
+    CK(cudaEventRecord(ev[5], s));
+    k_p_face<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    CK(cudaEventRecord(ev[6], s));
+    if (x->phys.dpdx_tolerance) k_p_dpdx<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+    CK(cudaEventRecord(ev[7], s));
+    k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+    CK(cudaEventRecord(ev[8], s));
+    k_T_cell<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    CK(cudaEventRecord(ev[9], s));
+    k_T_face<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    CK(cudaEventRecord(ev[10], s));
+    k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
+    CK(cudaEventRecord(ev[11], s));
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(ev[11]));
+    for (int k = 0; k < NK; ++k) {
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+      acc[k] += t;
+    }
+    x->launches += x->phys.dpdx_tolerance ? 11 : 10;
+  }
+  x->phys = keep;
+  for (int k = 0; k <= NK; ++k) cudaEventDestroy(ev[k]);
+  for (int k = 0; k < NK; ++k) ms[k] = acc[k] / n;
+  return NK;
 }

@@ -157,6 +157,14 @@ def gpu_lib() -> C.CDLL:
         lib.nim_gpu_destroy.restype = None
         lib.nim_gpu_strerror.argtypes = [C.c_int]
         lib.nim_gpu_strerror.restype = C.c_char_p
+        lib.nim_gpu_stream.argtypes = [vp]
+        lib.nim_gpu_stream.restype = vp
+        lib.nim_gpu_launch_count.argtypes = [vp]
+        lib.nim_gpu_launch_count.restype = C.c_int64
+        lib.nim_gpu_profile_iterations.argtypes = [vp, C.c_int32, C.POINTER(C.c_double), C.c_int32]
+        lib.nim_gpu_profile_iterations.restype = C.c_int
+        lib.nim_gpu_kernel_name.argtypes = [C.c_int32]
+        lib.nim_gpu_kernel_name.restype = C.c_char_p
         _gpu = lib
     return _gpu
 

@@ -130,6 +130,8 @@ CASES = {
     "c2": Case("c2", 128, 128, 96, Ra=1e5, Pr=0.71, dt=5e-4, steps=2000),
     "c3": Case("c3", 256, 256, 192, Ra=1e6, Pr=0.71, dt=2.5e-4, steps=1000),
     "c5": Case("c5", 64, 64, 48, Ra=1e5, Pr=0.71, dt=1e-3, steps=500),
+    # profiling size: per-kernel working set above the 126 MB L2, ~1.3 GB held
+    "p1": Case("p1", 96, 96, 64, Ra=1e5, Pr=0.71, dt=5e-4, steps=10),
 }
 
 

@@ -103,6 +103,23 @@ class NimSolver:
             _abi.check(st, "nim_gpu_step")
         return [arr[i] for i in range(done.value)]
 
+    # -- timing hooks
+    @property
+    def stream_handle(self) -> int:
+        """cudaStream_t of the context (for events on the launching stream)."""
+        return int(self.lib.nim_gpu_stream(self._h) or 0)
+
+    def launch_count(self) -> int:
+        return int(self.lib.nim_gpu_launch_count(self._h))
+
+    def profile_iterations(self, n: int) -> dict:
+        """Mean device time (ms) of each kernel over n un-graphed passes."""
+        ms = (C.c_double * 32)()
+        nk = self.lib.nim_gpu_profile_iterations(self._h, n, ms, 32)
+        if nk < 0:
+            _abi.check(nk, "nim_gpu_profile_iterations")
+        return {self.lib.nim_gpu_kernel_name(k).decode(): ms[k] for k in range(nk)}
+
     def synchronize(self):
         _abi.check(self.lib.nim_gpu_synchronize(self._h), "nim_gpu_synchronize")
 

@@ -218,6 +218,7 @@ struct nim_oracle {
 
   // geometry
   std::vector<Map> maps;  // 1-based
+  std::vector<int64_t> face_owner;  // highest cell number sharing each face
   V1 volume, G1, G2, G3, faces_area;
   M33 gij, xi_x;
   M336 gf;  // meshes_gij_faces
@@ -310,6 +311,7 @@ void cell_geometry(nim_oracle &o, int64_t m) {
     const int t1 = (d == 0) ? 1 : 0;        // first tangent
     const int t2 = (d == 2) ? 1 : 2;        // second tangent
     const int32_t f = o.F(fn, m);
+    if (o.face_owner[f] != m) continue;  // a later cell overwrites this face
     const double sn = std::sqrt(C.gij[d][d]);
     const double s1 = std::sqrt(C.g_ij[t1][t1]);
     const double s2 = std::sqrt(C.g_ij[t2][t2]);
@@ -343,9 +345,10 @@ void cell_geometry(nim_oracle &o, int64_t m) {
       return Int;
     };
     const int32_t f = o.F(fn, m);
-    o.faces_area(f) = integ(dS);
+    const double area = integ(dS);  // this cell's faces_area(f), read back at geometry.f90:484-492
+    if (o.face_owner[f] == m) o.faces_area(f) = area;
     for (int r = 0; r < 3; ++r)
-      for (int c = 0; c < 3; ++c) o.gf(r + 1, c + 1, fn, m) = integ(K[r][c]) / o.faces_area(f);
+      for (int c = 0; c < 3; ++c) o.gf(r + 1, c + 1, fn, m) = integ(K[r][c]) / area;
   }
   // convection_diffusion_constants_mesh_i, geometry.f90:500-632
   {
@@ -1129,7 +1132,13 @@ extern "C" int nim_oracle_init(nim_oracle *o) {
   o->STEP = 1;
 #pragma omp parallel for schedule(static) num_threads(o->nthreads)
   for (int64_t i = 1; i <= o->NMESH; ++i) mapping_coefficients(*o, i);
-  // the shared-face writes resolve to the higher cell number (serial order)
+  // Shared faces get their geometry from both cells; in the reference's
+  // serial loop the higher cell number writes last and wins, so only that
+  // cell (face_owner) writes here and the loop can run in parallel.
+  o->face_owner.assign(o->NFACE + 1, 0);
+  for (int64_t i = 1; i <= o->NMESH; ++i)
+    for (int k = 1; k <= 6; ++k) o->face_owner[o->F(k, i)] = std::max<int64_t>(o->face_owner[o->F(k, i)], i);
+#pragma omp parallel for schedule(dynamic, 64) num_threads(o->nthreads)
   for (int64_t i = 1; i <= o->NMESH; ++i) cell_geometry(*o, i);
   pressure_bc_array(*o);
   pressure_constants(*o);
@@ -1385,3 +1394,14 @@ extern "C" int nim_oracle_set(nim_oracle *o, int32_t f, const double *in, int64_
 
 extern "C" double nim_oracle_max_rc(nim_oracle *o) { return o ? o->max_rc : -1.0; }
 extern "C" void nim_oracle_destroy(nim_oracle *o) { delete o; }
+
+extern "C" void nim_oracle_set_threads(nim_oracle *o, int32_t threads) {
+  if (o) o->nthreads = threads > 0 ? threads : 1;
+}
+
+// M_A(d,1:6) of nim.f90:181-287 for one direction (exposed for the
+// continuity test of the exact and series branches).
+extern "C" void nim_oracle_nim_coefficients(double u, double k, double gminus, double gplus, double v_limit,
+                                            double *A) {
+  nim_direction(u, k, gminus, gplus, v_limit, A);
+}

@@ -48,6 +48,11 @@ int nim_oracle_set(nim_oracle *o, int32_t field, const double *in, int64_t n);
 /* max |R_C| seen by calculate_R_c_new in SEQUENTIAL mode (must be 0) */
 double nim_oracle_max_rc(nim_oracle *o);
 void nim_oracle_destroy(nim_oracle *o);
+void nim_oracle_set_threads(nim_oracle *o, int32_t threads);
+/* M_A(d,1:6) of one direction: contravariant speed u, diffusivity k, face
+   metrics g_minus/g_plus, branch switch v_limit (nim.f90:181-287) */
+void nim_oracle_nim_coefficients(double u, double k, double gminus, double gplus, double v_limit,
+                                 double *A);
 
 #ifdef __cplusplus
 }

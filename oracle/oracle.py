@@ -53,6 +53,10 @@ def lib() -> C.CDLL:
         L.nim_oracle_max_rc.restype = C.c_double
         L.nim_oracle_destroy.argtypes = [vp]
         L.nim_oracle_destroy.restype = None
+        L.nim_oracle_set_threads.argtypes = [vp, C.c_int32]
+        L.nim_oracle_set_threads.restype = None
+        L.nim_oracle_nim_coefficients.argtypes = [C.c_double] * 5 + [C.POINTER(C.c_double)]
+        L.nim_oracle_nim_coefficients.restype = None
         _lib = L
     return _lib
 
@@ -118,5 +122,15 @@ class Oracle:
         _abi.check(lib().nim_oracle_set(self._h, field, a.ctypes.data_as(C.POINTER(C.c_double)), a.size),
                    "nim_oracle_set")
 
+    def set_threads(self, n: int):
+        lib().nim_oracle_set_threads(self._h, n)
+
     def max_rc(self) -> float:
         return lib().nim_oracle_max_rc(self._h)
+
+
+def nim_coefficients(u: float, k: float, gminus: float = 1.0, gplus: float = 1.0, v_limit: float = 1e-2):
+    """M_A(d,1:6) of one direction (nim.f90:181-287)."""
+    A = (C.c_double * 6)()
+    lib().nim_oracle_nim_coefficients(u, k, gminus, gplus, v_limit, A)
+    return np.array(A[:])
