@@ -320,7 +320,8 @@ def main():
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
                      "bytes_per_launch": KERNEL_BYTES_PER_CELL[dom] * case.ncells,
                      "kernel_ms": dom_ms,
-                     "shares": {k: round(v / tot, 4) for k, v in shares.items()}},
+                     "shares": {k: round(v / tot, 4) for k, v in shares.items()},
+                     "kernel_us": {k: round(1e3 * v, 2) for k, v in shares.items()}},
         "cpu_baseline": cpu,
         "gpu_launches": launches,
         "clocks": clk,

@@ -48,7 +48,8 @@ struct nim_ctx {
   int *perm = nullptr;       // reference face number - 1 -> structured face index
   double *scratch = nullptr; // gather/scatter staging [54*Nc or 3*NF]
   double *sums = nullptr;    // [8] outputs of k_finish_sum
-  int nblk_c = 0, nblk_b = 0;
+  int nblk_c = 0, nblk_b = 0, nblk_c3 = 0;
+  dim3 g3{1, 1, 1}, g8{1, 1, 1};  // patch grids: 32x4 (x3 threads) and 32x8 cells
   std::vector<void *> allocs;
   cudaGraphExec_t graph = nullptr;
   int graph_iters = 0;
@@ -180,16 +181,17 @@ int launch_iteration(nim_ctx *x) {
   const Dims &d = x->d;
   cudaStream_t s = x->stream;
   const int gc = x->nblk_c, gb = x->nblk_b;
-  k_vel_cell<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-  k_vel_face<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-  k_p_src<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  const dim3 g3 = x->g3, g8 = x->g8;
+  k_vel_cell<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_vel_face<<<x->nblk_c3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_p_bc<<<gb, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_p_bc_copy<<<gb, BLK, 0, s>>>(d, x->F, x->ctl);
-  k_p_face<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_p_face<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   if (x->phys.dpdx_tolerance) k_p_dpdx<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
   k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
-  k_T_cell<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-  k_T_face<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_T_cell<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_T_face<<<g8, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
   CK(cudaGetLastError());
   x->kernels_per_iter = x->phys.dpdx_tolerance ? 11 : 10;
@@ -370,6 +372,9 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
   x->gq = make_gauss();
   x->nblk_c = grid(d.Nc);
   x->nblk_b = grid(d.NBF);
+  x->nblk_c3 = (d.Nc + CB - 1) / CB;
+  x->g3 = dim3((d.NT + 31) / 32, (d.NR + 3) / 4, d.NZ);
+  x->g8 = dim3((d.NT + 31) / 32, (d.NR + 7) / 8, d.NZ);
   const size_t Nc = d.Nc, NF = d.NF, NB = d.NBF;
   Geo &g = x->g;
   TRY(dalloc(x, &g.vol, Nc));
@@ -698,27 +703,28 @@ extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int
   for (int q = 0; q < 5; ++q) x->phys.tol[q] = -1.0;
   k_step_reset<<<1, 1, 0, s>>>(x->ctl);
   const int gc = x->nblk_c, gb = x->nblk_b;
+  const dim3 g3 = x->g3, g8 = x->g8;
   for (int it = 0; it < n; ++it) {
     CK(cudaEventRecord(ev[0], s));
-    k_vel_cell<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_vel_cell<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[1], s));
-    k_vel_face<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_vel_face<<<x->nblk_c3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[2], s));
-    k_p_src<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[3], s));
     k_p_bc<<<gb, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[4], s));
     k_p_bc_copy<<<gb, BLK, 0, s>>>(d, x->F, x->ctl);
     CK(cudaEventRecord(ev[5], s));
-    k_p_face<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_p_face<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[6], s));
     if (x->phys.dpdx_tolerance) k_p_dpdx<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
     CK(cudaEventRecord(ev[7], s));
     k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
     CK(cudaEventRecord(ev[8], s));
-    k_T_cell<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_T_cell<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[9], s));
-    k_T_face<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_T_face<<<g8, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[10], s));
     k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
     CK(cudaEventRecord(ev[11], s));

@@ -94,29 +94,57 @@ struct Ctrl {
 };
 
 constexpr int BLK = 256;
+// kernels that spread one cell over three threads (component or direction)
+constexpr int CB = 128;            // cells per block
+constexpr int CB3 = 3 * CB;        // threads per block
 
 // ------------------------------------------------------------ reductions
 // Max of non-negative doubles through their bit patterns (IEEE order equals
 // integer order for x >= 0; NaN sorts above +Inf and is caught as non-finite).
+// NT = threads in the block (flattened).  Call red_init() first (it holds
+// the only barrier); block_max() is barrier-free: warps fold their maxima
+// into shared memory with atomics and the last warp to finish publishes the
+// block's maxima with one global atomic each.
+struct BlockRed {
+  unsigned long long m[8];
+  unsigned int count;
+};
 template <int N>
-__device__ __forceinline__ void block_max(const double (&v)[N], unsigned long long *dst) {
-  __shared__ unsigned long long sm[N][BLK / 32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int n = 0; n < N; ++n) {
-    unsigned long long b = (unsigned long long)__double_as_longlong(v[n]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const unsigned long long t = __shfl_xor_sync(0xffffffffu, b, o);
-      b = (t > b) ? t : b;
-    }
-    if (lane == 0) sm[n][warp] = b;
+__device__ __forceinline__ void red_init(BlockRed &r) {
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    for (int n = 0; n < N; ++n) r.m[n] = 0ull;
+    r.count = 0u;
   }
   __syncthreads();
-  if (threadIdx.x < N) {
-    unsigned long long m = 0;
-    for (int w = 0; w < BLK / 32; ++w) m = (sm[threadIdx.x][w] > m) ? sm[threadIdx.x][w] : m;
-    if (m) atomicMax(dst + threadIdx.x, m);
+}
+template <int N, int NT = BLK>
+__device__ __forceinline__ void block_max(BlockRed &r, const double (&v)[N], unsigned long long *dst) {
+  const int t = threadIdx.x + blockDim.x * threadIdx.y;
+  const int lane = t & 31;
+  unsigned long long b[N];
+#pragma unroll
+  for (int n = 0; n < N; ++n) {
+    b[n] = (unsigned long long)__double_as_longlong(v[n]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long u = __shfl_xor_sync(0xffffffffu, b[n], o);
+      b[n] = (u > b[n]) ? u : b[n];
+    }
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int n = 0; n < N; ++n)
+      if (b[n]) atomicMax(&r.m[n], b[n]);
+    __threadfence_block();
+    const unsigned int done = atomicAdd(&r.count, 1u);
+    if (done == NT / 32 - 1) {
+      __threadfence_block();
+#pragma unroll
+      for (int n = 0; n < N; ++n) {
+        const unsigned long long m = atomicAdd(&r.m[n], 0ull);
+        if (m) atomicMax(dst + n, m);
+      }
+    }
   }
 }
 
@@ -733,56 +761,72 @@ __device__ __forceinline__ double errv(double nw, double old, bool first) { retu
 // max that keeps a NaN (fmax would drop it and hide a blow-up)
 __device__ __forceinline__ double nmax(double a, double b) { return (b > a || b != b) ? b : a; }
 
+// Cell of this thread in a 3D launch over patches of 32 (theta) x R (r)
+// cells of one z-plane: grid (ceil(NT/32), ceil(NR/R), NZ), threadIdx.x
+// spans the patch (R = blockDim.x / 32).  No division by run-time sizes, and
+// the +-r neighbours of a cell mostly sit in the same block.
+__device__ __forceinline__ bool patch_cell(const Dims &d, Cell &x) {
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int j = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int k = blockIdx.z;
+  x = Cell::at(d, i, j, k);
+  return i < d.NT && j < d.NR;
+}
+
 // ---- K1: velocity sources + cell update (update_velocity_sources
 // nse.f90:199-211 with calculate_gforces 2484-2502, calculate_R_b 1562-1592,
 // calculate_R_D2 1628-1860; cell part of integrate_velocity_field_formulation2_i
 // 839-872).  R_C (calculate_R_c_new, 1393-1434) is identically zero.
-__global__ void __launch_bounds__(BLK) k_vel_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+// Block (CB, 3): threadIdx.y = velocity component.
+__global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<3>(red);
   const int par = parity(ctl);
   const bool first = ctl->first;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = threadIdx.y;
+  Cell x;
+  const bool act = patch_cell(d, x);
+  const int c = x.c;
   double e[3] = {0., 0., 0.};
-  if (c < d.Nc) {
-    const Cell x = Cell::of(d, c);
+  if (act) {
     const size_t Nc = d.Nc, NF = d.NF;
     int f[7];
     cell_faces(d, x, f);
     const double *fp = F.f[3] + par * NF;
-    const double bz = -(P.g_beta * 0.5 * (F.c[3][c] + F.co[3][c]));
     double pf[7];
     for (int k = 1; k <= 6; ++k) pf[k] = fp[f[k]];
     const double invV = 1. / g.vol[c];
-    const double RB[3] = {0. + P.inv_rho * green_gauss(g, NF, invV, pf, f, 0),
-                          0. + P.inv_rho * green_gauss(g, NF, invV, pf, f, 1),
-                          bz + P.inv_rho * green_gauss(g, NF, invV, pf, f, 2)};
+    const double base = (q == 2) ? -(P.g_beta * 0.5 * (F.c[3][c] + F.co[3][c])) : 0.;
+    const double RB = base + P.inv_rho * green_gauss(g, NF, invV, pf, f, q);
+    const double *fr = F.f[q] + par * NF;
+    const double RD = P.inv_Re * diffusion_source(d, g, fr, x, f);
     double F4[8];
     for (int k = 0; k < 8; ++k) F4[k] = F.MF4[(size_t)k * Nc + c];
-    for (int q = 0; q < 3; ++q) {
-      const double *fr = F.f[q] + par * NF;
-      const double RD = P.inv_Re * diffusion_source(d, g, fr, x, f);
-      const double B = (0. + RD + RB[q]);
-      const double cold = F.c[q][c];
-      const double nw = cell_update(fr, f, cold, F.co[q][c], B, F4, P.w[q]);
-      F.c[q][c] = nw;
-      e[q] = errv(nw, cold, first);
-    }
+    const double B = (0. + RD + RB);
+    const double cold = F.c[q][c];
+    const double nw = cell_update(fr, f, cold, F.co[q][c], B, F4, P.w[q]);
+    F.c[q][c] = nw;
+    e[q] = errv(nw, cold, first);
   }
-  block_max<3>(e, ctl->err[par]);
+  block_max<3, CB3>(red, e, ctl->err[par]);
 }
 
-// ---- K2: +xi face updates of u, v, w (nse.f90:878-1005)
-__global__ void __launch_bounds__(BLK) k_vel_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+// ---- K2: +xi face updates of u, v, w (nse.f90:878-1005).
+// Block (CB, 3): threadIdx.y = direction.
+__global__ void __launch_bounds__(CB3, 2) k_vel_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<3>(red);
   const int par = parity(ctl);
   const bool first = ctl->first;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int dd = threadIdx.y + 1;
+  const int c = blockIdx.x * CB + threadIdx.x;
   double e[3] = {0., 0., 0.};
   if (c < d.Nc) {
     const Cell x = Cell::of(d, c);
     const size_t Nc = d.Nc, NF = d.NF;
-    for (int dd = 1; dd <= 3; ++dd) {
-      if (!x.has_nb(d, 2 * dd)) continue;
+    if (x.has_nb(d, 2 * dd)) {
       const Cell x2 = x.nb(d, 2 * dd);
       double Fd[5];
       for (int k = 0; k < 5; ++k) Fd[k] = F.MF[(size_t)(5 * (dd - 1) + k) * Nc + c];
@@ -792,52 +836,78 @@ __global__ void __launch_bounds__(BLK) k_vel_face(Dims d, Geo g, Fields F, Phys 
         const double *fr = F.f[q] + par * NF;
         const double nw = face_update(d, fr, F.c[q], F.co[q], Fd, dg0, dg1, dd, x, x2, P.w[q]);
         F.f[q][(1 - par) * NF + fo] = nw;
-        e[q] = nmax(e[q], errv(nw, fr[fo], first));
+        e[q] = errv(nw, fr[fo], first);
       }
     }
   }
-  block_max<3>(e, ctl->err[par]);
+  block_max<3, CB3>(red, e, ctl->err[par]);
 }
 
 // ---- K3: pressure sources (calculate_R_b_p nse.f90:2362-2407,
-// calculate_R_D_p2 1863-1997)
-__global__ void __launch_bounds__(BLK) k_p_src(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+// calculate_R_D_p2 1863-1997).  Block (CB, 3): thread y forms the gradient of
+// velocity component y and two of the six cross derivatives of p (y = 1 also
+// d(bz)/dz); thread 0 combines them in the reference's order.
+__global__ void __launch_bounds__(CB3, 3) k_p_src(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
+  __shared__ double sh[3][3][CB];  // gradients of u, v, w
+  __shared__ double sX[3][2][CB];  // cross derivatives of p
+  __shared__ double sbz[CB];
   const int par = parity(ctl);
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.Nc) return;
-  const Cell x = Cell::of(d, c);
-  const size_t NF = d.NF;
+  const int q = threadIdx.y, tx = threadIdx.x;
+  Cell x;
+  const bool active = patch_cell(d, x);
+  const int c = x.c;
   int f[7];
-  cell_faces(d, x, f);
-  const double *fu = F.f[0] + (1 - par) * NF, *fv = F.f[1] + (1 - par) * NF, *fw = F.f[2] + (1 - par) * NF;
-  const double *fT = F.f[4] + par * NF, *fp = F.f[3] + par * NF;
-  double uf[7], vf[7], wf[7], bzf[7];
-  for (int k = 1; k <= 6; ++k) {
-    uf[k] = fu[f[k]];
-    vf[k] = fv[f[k]];
-    wf[k] = fw[f[k]];
-    bzf[k] = -(P.g_beta * (fT[f[k]]));
+  const size_t Nc = d.Nc, NF = d.NF;
+  const double *fp = F.f[3] + par * NF;
+  if (active) {
+    cell_faces(d, x, f);
+    const double invV = 1. / g.vol[c];
+    const double *fq = F.f[q] + (1 - par) * NF;
+    double vf[7];
+    for (int k = 1; k <= 6; ++k) vf[k] = fq[f[k]];
+    for (int cc = 0; cc < 3; ++cc) sh[q][cc][tx] = green_gauss(g, NF, invV, vf, f, cc);
+    if (q == 1) {
+      const double *fT = F.f[4] + par * NF;
+      double bzf[7];
+      for (int k = 1; k <= 6; ++k) bzf[k] = -(P.g_beta * (fT[f[k]]));
+      sbz[tx] = green_gauss(g, NF, invV, bzf, f, 2);
+    }
+    // y=0 pxy,pzy  y=1 pyx,pzx  y=2 pxz,pyz (calculate_R_D_p2 order)
+    const int e2 = (q == 0) ? 2 : (q == 1) ? 1 : 3;
+    const int fa = (q == 1) ? 4 : 2, fb = (q == 1) ? 3 : 1;
+    sX[q][0][tx] = 0.5 * (tangential(d, fp, x, fa, e2) - tangential(d, fp, x, fb, e2));
+    sX[q][1][tx] = (q == 2) ? 0.5 * (tangential(d, fp, x, 4, 3) - tangential(d, fp, x, 3, 3))
+                            : 0.5 * (tangential(d, fp, x, 6, e2) - tangential(d, fp, x, 5, e2));
   }
-  const double invV = 1. / g.vol[c];
-  const double du_dx = green_gauss(g, NF, invV, uf, f, 0), du_dy = green_gauss(g, NF, invV, uf, f, 1),
-               du_dz = green_gauss(g, NF, invV, uf, f, 2);
-  const double dv_dx = green_gauss(g, NF, invV, vf, f, 0), dv_dy = green_gauss(g, NF, invV, vf, f, 1),
-               dv_dz = green_gauss(g, NF, invV, vf, f, 2);
-  const double dw_dx = green_gauss(g, NF, invV, wf, f, 0), dw_dy = green_gauss(g, NF, invV, wf, f, 1),
-               dw_dz = green_gauss(g, NF, invV, wf, f, 2);
-  const double dbz_dz = green_gauss(g, NF, invV, bzf, f, 2);
-  const double Dila = du_dx + dv_dy + dw_dz;
-  F.dila[c] = Dila;
-  const double RBp = -(du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) -
-                     2.0 * (du_dy * dv_dx + dv_dz * dw_dy + dw_dx * du_dz) - dbz_dz + Dila / (2 * P.DT);
-  const double RDp = P.inv_rho * diffusion_source(d, g, fp, x, f);
-  F.Rp[c] = RDp + RBp;
+  __syncthreads();
+  if (active && q == 0) {
+    const double du_dx = sh[0][0][tx], du_dy = sh[0][1][tx], du_dz = sh[0][2][tx];
+    const double dv_dx = sh[1][0][tx], dv_dy = sh[1][1][tx], dv_dz = sh[1][2][tx];
+    const double dw_dx = sh[2][0][tx], dw_dy = sh[2][1][tx], dw_dz = sh[2][2][tx];
+    const double dbz_dz = sbz[tx];
+    const double Dila = du_dx + dv_dy + dw_dz;
+    F.dila[c] = Dila;
+    const double RBp = -(du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) -
+                       2.0 * (du_dy * dv_dx + dv_dz * dw_dy + dw_dx * du_dz) - dbz_dz + Dila / (2 * P.DT);
+    const double pxy = sX[0][0][tx], pzy = sX[0][1][tx], pyx = sX[1][0][tx], pzx = sX[1][1][tx];
+    const double pxz = sX[2][0][tx], pyz = sX[2][1][tx];
+    const double px = (fp[f[2]] - fp[f[1]]) / 2.;
+    const double py = (fp[f[4]] - fp[f[3]]) / 2.;
+    const double pz = (fp[f[6]] - fp[f[5]]) / 2.;
+    const double *Gv = g.G, *gij = g.gij;
+    const double RDp = P.inv_rho * (Gv[c] * px + Gv[Nc + c] * py + Gv[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy -
+                                    gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz - gij[2 * Nc + c] * pzx -
+                                    gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
+    F.Rp[c] = RDp + RBp;
+  }
 }
 
 // ---- K4: apply_pressure_bc (bc.f90:141-342), reading cur, writing next
 __global__ void __launch_bounds__(BLK) k_p_bc(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<1>(red);
   const int par = parity(ctl);
   const bool first = ctl->first;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -880,7 +950,7 @@ __global__ void __launch_bounds__(BLK) k_p_bc(Dims d, Geo g, Fields F, Phys P, C
     F.f[3][(1 - par) * NF + fw0] = nw;
     e[0] = errv(nw, pr[fw0], first);
   }
-  block_max<1>(e, ctl->err[par] + 3);
+  block_max<1>(red, e, ctl->err[par] + 3);
 }
 
 __global__ void k_p_bc_copy(Dims d, Fields F, Ctrl *ctl) {
@@ -893,26 +963,32 @@ __global__ void k_p_bc_copy(Dims d, Fields F, Ctrl *ctl) {
   F.f[3][par * (size_t)d.NF + f] = F.f[3][(1 - par) * (size_t)d.NF + f];
 }
 
-// ---- K5: integrate_pressure_field_i (nse.f90:1091-1289), cur -> next
-__global__ void __launch_bounds__(BLK) k_p_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+// (coefficient, face, cell) of the ten off-diagonal terms of the pressure
+// face update for the +r, +theta, +z face, in source order (nse.f90:1150-1285)
+__constant__ unsigned char kPTerms[3][10][3] = {
+    {{1, 1, 1}, {3, 2, 2}, {4, 3, 1}, {5, 4, 1}, {6, 3, 2}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
+    {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
+    {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {6, 4, 1}, {7, 3, 2}, {8, 4, 2}, {9, 5, 1}, {11, 6, 2}}};
+
+// ---- K5: integrate_pressure_field_i (nse.f90:1091-1289), cur -> next.
+// Block (CB, 3): threadIdx.y = direction.
+__global__ void __launch_bounds__(CB3, 3) k_p_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<1>(red);
   const int par = parity(ctl);
   const bool first = ctl->first;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int dd = threadIdx.y + 1;
+  Cell x;
+  const bool act = patch_cell(d, x);
+  const int c = x.c;
   double e[1] = {0.};
-  if (c < d.Nc) {
-    const Cell x = Cell::of(d, c);
+  if (act) {
     const size_t Nc = d.Nc, NF = d.NF;
     const double *pr = F.f[3] + par * NF;
-    // (coefficient, face, cell) of the ten off-diagonal terms, source order
-    const unsigned char tab[3][10][3] = {
-        {{1, 1, 1}, {3, 2, 2}, {4, 3, 1}, {5, 4, 1}, {6, 3, 2}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
-        {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
-        {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {6, 4, 1}, {7, 3, 2}, {8, 4, 2}, {9, 5, 1}, {11, 6, 2}}};
-    const int diag[3] = {2, 6, 10};
-#pragma unroll
-    for (int dd = 1; dd <= 3; ++dd) {
-      if (!x.has_nb(d, 2 * dd)) continue;
+    if (x.has_nb(d, 2 * dd)) {
+      const unsigned char(*tab)[10][3] = kPTerms;
+      const int diag = (dd == 1) ? 2 : (dd == 2) ? 6 : 10;
       const Cell n2 = x.nb(d, 2 * dd);
       const double *A = g.AA + (size_t)15 * (dd - 1) * Nc;
       const double B1 = (F.Rp[c]) * A[12 * Nc + c];
@@ -928,17 +1004,19 @@ __global__ void __launch_bounds__(BLK) k_p_face(Dims d, Geo g, Fields F, Phys P,
       }
       const int fo = x.face(d, 2 * dd);
       const double w = P.w_p;
-      const double nw = (1 - w) * pr[fo] + w / (A[(size_t)(diag[dd - 1] - 1) * Nc + c]) * (s + B1 + B2 + B3 + B4);
+      const double nw = (1 - w) * pr[fo] + w / (A[(size_t)(diag - 1) * Nc + c]) * (s + B1 + B2 + B3 + B4);
       F.f[3][(1 - par) * NF + fo] = nw;
-      e[0] = nmax(e[0], errv(nw, pr[fo], first));
+      e[0] = errv(nw, pr[fo], first);
     }
   }
-  block_max<1>(e, ctl->err[par] + 3);
+  block_max<1, CB3>(red, e, ctl->err[par] + 3);
 }
 
 // ---- K5b (is_dpdx_tolerance): cell pressure gradients (nse.f90:292-307)
 __global__ void __launch_bounds__(BLK) k_p_dpdx(Dims d, Geo g, Fields F, Ctrl *ctl) {
   if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<1>(red);
   const int par = parity(ctl);
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   double e[1] = {0.};
@@ -955,12 +1033,14 @@ __global__ void __launch_bounds__(BLK) k_p_dpdx(Dims d, Geo g, Fields F, Ctrl *c
       F.dpd[q * Nc + c] = v[q];
     }
   }
-  block_max<1>(e, ctl->err[par] + 5);
+  block_max<1>(red, e, ctl->err[par] + 5);
 }
 
 // ---- K6: apply_zero_flux (bc.f90:345-390) on the z walls, in place
 __global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, Geo g, Fields F, Ctrl *ctl) {
   if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<1>(red);
   const int par = parity(ctl);
   const bool first = ctl->first;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -977,63 +1057,97 @@ __global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, Geo g, Fields F, Ctrl
     e[0] = errv(nw, T[f1], first);
     T[f1] = nw;
   }
-  block_max<1>(e, ctl->err[par] + 4);
+  block_max<1>(red, e, ctl->err[par] + 4);
 }
 
 // ---- K7: calculate_temperature_nim_constants_formulation2 (nim.f90:334-502),
-// calculate_R_D_T (nse.f90:2000-2134) and the cell update of T (1017-1026)
-__global__ void __launch_bounds__(BLK) k_T_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+// calculate_R_D_T (nse.f90:2000-2134) and the cell update of T (1017-1026).
+// Block (CB, 3): thread y forms MT_A of direction y+1 for the cell and its
+// +neighbour (MT_F of that face) and two of the six cross derivatives;
+// thread 0 assembles MT_F4, R_D_T and the update in the reference's order.
+__global__ void __launch_bounds__(CB3, 2) k_T_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<1>(red);
+  __shared__ double sA[3][2][CB];   // MT_A(d,5), MT_A(d,6)
+  __shared__ double sX[3][2][CB];   // cross derivatives
   const int par = parity(ctl);
   const bool first = ctl->first;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = threadIdx.y, tx = threadIdx.x, dd = y + 1;
+  Cell x;
+  const bool active = patch_cell(d, x);
+  const int c = x.c;
   double e[1] = {0.};
-  if (c < d.Nc) {
-    const Cell x = Cell::of(d, c);
-    const size_t Nc = d.Nc, NF = d.NF;
-    auto coefA = [&](int cell, int dd, double A[6]) {
+  const size_t Nc = d.Nc, NF = d.NF;
+  const double *T = F.f[4] + par * NF;
+  if (active) {
+    auto coefA = [&](int cell, double A[6]) {
       const double ut = 0.5 * (F.c[0][cell] + F.co[0][cell]);
       const double vt = 0.5 * (F.c[1][cell] + F.co[1][cell]);
       const double wt = 0.5 * (F.c[2][cell] + F.co[2][cell]);
       const double u = contravariant(g.xi, Nc, cell, dd, ut, vt, wt);
-      nim_direction(u, g.gij[(size_t)(dd - 1 + 3 * (dd - 1)) * Nc + cell] * P.alpha, g.gfd[(2 * (dd - 1)) * Nc + cell],
-                    g.gfd[(2 * (dd - 1) + 1) * Nc + cell], P.v_limit, A);
+      nim_direction(u, g.gij[(size_t)(dd - 1 + 3 * (dd - 1)) * Nc + cell] * P.alpha,
+                    g.gfd[(2 * (dd - 1)) * Nc + cell], g.gfd[(2 * (dd - 1) + 1) * Nc + cell], P.v_limit, A);
     };
-    double A[3][6];
-    for (int dd = 1; dd <= 3; ++dd) coefA(c, dd, A[dd - 1]);
-    double F4[8];
-    form_F4(A, P.DT, F4);
-    for (int dd = 1; dd <= 3; ++dd) {
-      double G[5] = {0., 0., 0., 0., 0.};
-      if (x.has_nb(d, 2 * dd)) {
-        double A2[6];
-        coefA(x.nb(d, 2 * dd).c, dd, A2);
-        form_Fd(A[dd - 1], A2, G);
-      }
-      for (int k = 0; k < 5; ++k) F.MTF[(size_t)(5 * (dd - 1) + k) * Nc + c] = G[k];
+    double A[6];
+    coefA(c, A);
+    sA[y][0][tx] = A[4];
+    sA[y][1][tx] = A[5];
+    double G[5] = {0., 0., 0., 0., 0.};
+    if (x.has_nb(d, 2 * dd)) {
+      double A2[6];
+      coefA(x.nb(d, 2 * dd).c, A2);
+      form_Fd(A, A2, G);
     }
+    for (int k = 0; k < 5; ++k) F.MTF[(size_t)(5 * (dd - 1) + k) * Nc + c] = G[k];
+    // cross derivatives of calculate_R_D_T: y=0 pxy,pzy  y=1 pyx,pzx  y=2 pxz,pyz
+    const int e2 = (y == 0) ? 2 : (y == 1) ? 1 : 3;
+    const int fa = (y == 1) ? 4 : 2, fb = (y == 1) ? 3 : 1;
+    sX[y][0][tx] = 0.5 * (tangential(d, T, x, (y == 2) ? 2 : fa, e2) - tangential(d, T, x, (y == 2) ? 1 : fb, e2));
+    sX[y][1][tx] = (y == 2) ? 0.5 * (tangential(d, T, x, 4, 3) - tangential(d, T, x, 3, 3))
+                            : 0.5 * (tangential(d, T, x, 6, e2) - tangential(d, T, x, 5, e2));
+  }
+  __syncthreads();
+  if (active && y == 0) {
+    double Am[3][6];
+    for (int k = 0; k < 3; ++k) {
+      Am[k][4] = sA[k][0][tx];
+      Am[k][5] = sA[k][1][tx];
+    }
+    double F4[8];
+    form_F4(Am, P.DT, F4);
     int f[7];
     cell_faces(d, x, f);
-    const double *T = F.f[4] + par * NF;
-    const double RDT = P.alpha * diffusion_source(d, g, T, x, f);
+    const double pxy = sX[0][0][tx], pzy = sX[0][1][tx], pyx = sX[1][0][tx], pzx = sX[1][1][tx];
+    const double pxz = sX[2][0][tx], pyz = sX[2][1][tx];
+    const double px = (T[f[2]] - T[f[1]]) / 2.;
+    const double py = (T[f[4]] - T[f[3]]) / 2.;
+    const double pz = (T[f[6]] - T[f[5]]) / 2.;
+    const double *Gv = g.G, *gij = g.gij;
+    const double RDT = P.alpha * (Gv[c] * px + Gv[Nc + c] * py + Gv[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy -
+                                  gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz - gij[2 * Nc + c] * pzx -
+                                  gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
     const double cold = F.c[3][c];
     const double nw = cell_update(T, f, cold, F.co[3][c], (RDT + 0.), F4, P.w[3]);
     F.c[3][c] = nw;
     e[0] = errv(nw, cold, first);
   }
-  block_max<1>(e, ctl->err[par] + 4);
+  block_max<1, CB3>(red, e, ctl->err[par] + 4);
 }
 
 // ---- K8: +xi face updates of T (nse.f90:1033-1088), cur -> next; the z-wall
 // values set by apply_zero_flux travel to the next half too
-__global__ void __launch_bounds__(BLK) k_T_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+__global__ void __launch_bounds__(BLK, 4) k_T_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<1>(red);
   const int par = parity(ctl);
   const bool first = ctl->first;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  Cell x;
+  const bool act = patch_cell(d, x);
+  const int c = x.c;
   double e[1] = {0.};
-  if (c < d.Nc) {
-    const Cell x = Cell::of(d, c);
+  if (act) {
     const size_t Nc = d.Nc, NF = d.NF;
     const double *T = F.f[4] + par * NF;
     double *Tn = F.f[4] + (1 - par) * NF;
@@ -1051,7 +1165,7 @@ __global__ void __launch_bounds__(BLK) k_T_face(Dims d, Geo g, Fields F, Phys P,
     if (x.k == 0) Tn[x.face(d, 5)] = T[x.face(d, 5)];
     if (x.k == d.NZ - 1) Tn[x.face(d, 6)] = T[x.face(d, 6)];
   }
-  block_max<1>(e, ctl->err[par] + 4);
+  block_max<1>(red, e, ctl->err[par] + 4);
 }
 
 // ---- K9: end of one pass (find_error's maxima, the do-while test of
@@ -1089,6 +1203,8 @@ __global__ void k_iter_end(Ctrl *ctl, Phys P) {
 // ====================================================== end of integrate
 // check_steady_state (nse.f90:1316-1332) + evaluate_D (nse.f90:2504-2537)
 __global__ void __launch_bounds__(BLK) k_after_integrate(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl, int nblk) {
+  __shared__ BlockRed red;
+  red_init<2>(red);
   const int par = parity(ctl);
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   double m[2] = {0., 0.}, s[1] = {0.};
@@ -1114,7 +1230,7 @@ __global__ void __launch_bounds__(BLK) k_after_integrate(Dims d, Geo g, Fields F
     F.dila[c] = Dila;
     s[0] = Dila * Dila;
   }
-  block_max<2>(m, ctl->red);
+  block_max<2>(red, m, ctl->red);
   block_sum<1>(s, F.part, nblk);
 }
 
@@ -1186,6 +1302,8 @@ __global__ void __launch_bounds__(BLK) k_nusselt(Dims d, Geo g, Fields F, Ctrl *
 // max |value| of the Dirichlet walls per field (u, v, w, -, T): find_error
 // compares against zero-initialised *_old arrays on the first pass
 __global__ void k_wall_floor(Dims d, Geo g, Ctrl *ctl) {
+  __shared__ BlockRed red;
+  red_init<5>(red);
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   double m[5] = {0., 0., 0., 0., 0.};
   if (b < d.NBF) {
@@ -1195,7 +1313,7 @@ __global__ void k_wall_floor(Dims d, Geo g, Ctrl *ctl) {
     m[2] = fabs(g.bcval[2 * (size_t)d.NBF + b]);
     if (B.pos <= 2) m[4] = fabs(g.bcval[3 * (size_t)d.NBF + b]);  // r walls keep T; z walls are recomputed
   }
-  block_max<5>(m, ctl->wall_floor);
+  block_max<5>(red, m, ctl->wall_floor);
 }
 
 }  // namespace nim
