@@ -216,6 +216,25 @@ int64_t nim_gpu_launch_count(nim_ctx *ctx);
 int nim_gpu_profile_iterations(nim_ctx *ctx, int32_t n, double *ms, int32_t cap);
 const char *nim_gpu_kernel_name(int32_t k);
 
+/* Wall-face limit of nim_gpu_nusselt_noalloc: 2*n_theta*n_z inner plus
+   outer wall faces, i.e. 4096 blocks of 256 faces. */
+#define NIM_NOALLOC_MAX_WALL_FACES 1048576
+
+/* find_Nu2 without any device allocation.  No counterpart in the reference:
+   it serves hosts that cannot call cudaMalloc when they want the Nusselt
+   numbers, for instance because another allocator already holds all free
+   device memory or because the host forbids allocation once its time loop
+   has started.  It computes, from the context's current face temperatures,
+   out4[0..3] = Nu_outer, Nu_inner, outer wall area, inner wall area (the
+   values nim_gpu_end_step reports) into caller-owned host memory.  Its
+   scratch is one static device array of 4*4096+8 doubles per device, whose
+   address nim_gpu_create looks up once per device; every call reuses it and
+   leaves the last call's partial sums there, so calls that overlap on the
+   GPU (two contexts on one device at once) race.  Meshes with more than
+   NIM_NOALLOC_MAX_WALL_FACES wall faces are refused with NIM_ERR_BAD_ARG.
+   Synchronises the context's stream. */
+int nim_gpu_nusselt_noalloc(nim_ctx *ctx, double *out4);
+
 /* Block until all work queued on the context's stream has finished. */
 int nim_gpu_synchronize(nim_ctx *ctx);
 

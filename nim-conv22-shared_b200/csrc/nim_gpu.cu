@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -25,6 +26,18 @@ using namespace nim;
 namespace {
 
 const double MATH_PI = 3.14159265359;  // parameters.f90:31
+
+// Scratch of nim_gpu_nusselt_noalloc: per-block partial sums of the four
+// wall sums for up to kNoallocBlocks blocks, then the four final sums.
+// A file-scope device array: every GPU that loads the library holds it.
+constexpr int kNoallocBlocks = NIM_NOALLOC_MAX_WALL_FACES / 256;
+__device__ __align__(256) double g_noalloc_scratch[4 * kNoallocBlocks + 8];
+
+// Device address of g_noalloc_scratch per device (host code cannot use the
+// symbol itself: on the host it names a stand-in, not device memory).
+constexpr int kMaxDevices = 64;
+double *g_noalloc_ptr[kMaxDevices] = {nullptr};
+std::mutex g_noalloc_mutex;
 
 struct Buf {
   void *p = nullptr;
@@ -360,8 +373,19 @@ extern "C" const char *nim_gpu_strerror(int s) {
   }
 }
 
+static int noalloc_setup(int device) {
+  if (device < 0 || device >= kMaxDevices) return NIM_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_ptr[device]) return NIM_OK;
+  void *ptr = nullptr;
+  CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));  // the current device's copy
+  g_noalloc_ptr[device] = static_cast<double *>(ptr);
+  return NIM_OK;
+}
+
 static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) {
   CK(cudaGetDevice(&x->device));
+  TRY(noalloc_setup(x->device));
   CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
   x->d = make_dims(m->n_theta, m->n_r, m->n_z);
   const Dims &d = x->d;
@@ -741,4 +765,30 @@ extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int
   for (int k = 0; k <= NK; ++k) cudaEventDestroy(ev[k]);
   for (int k = 0; k < NK; ++k) ms[k] = acc[k] / n;
   return NK;
+}
+
+extern "C" int nim_gpu_nusselt_noalloc(nim_ctx *x, double *out4) {
+  if (!x || !out4) return NIM_ERR_BAD_ARG;
+  if (!x->initialized) return NIM_ERR_STATE;
+  const Dims &d = x->d;
+  const int nr = 2 * d.NT * d.NZ;
+  if (nr > NIM_NOALLOC_MAX_WALL_FACES) return NIM_ERR_BAD_ARG;
+  double *scratch = (x->device >= 0 && x->device < kMaxDevices) ? g_noalloc_ptr[x->device] : nullptr;
+  if (!scratch) return NIM_ERR_STATE;
+  CK(cudaSetDevice(x->device));
+  const int gn = grid(nr);
+  Fields F = x->F;
+  F.part = scratch;  // per-block partials into the static array
+  k_nusselt<<<gn, BLK, 0, x->stream>>>(d, x->g, F, x->ctl, gn);
+  k_finish_sum<<<1, BLK, 0, x->stream>>>(scratch, gn, 4, scratch + 4 * kNoallocBlocks);
+  CK(cudaGetLastError());
+  x->launches += 2;
+  double sums[4];
+  CK(cudaMemcpyAsync(sums, scratch + 4 * kNoallocBlocks, sizeof(sums), cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  out4[0] = -(sums[0] / sums[1] * x->params.R_o);
+  out4[1] = -(sums[2] / sums[3] * x->params.R_i);
+  out4[2] = sums[1];
+  out4[3] = sums[3];
+  return NIM_OK;
 }

@@ -165,6 +165,8 @@ def gpu_lib() -> C.CDLL:
         lib.nim_gpu_profile_iterations.restype = C.c_int
         lib.nim_gpu_kernel_name.argtypes = [C.c_int32]
         lib.nim_gpu_kernel_name.restype = C.c_char_p
+        lib.nim_gpu_nusselt_noalloc.argtypes = [vp, C.POINTER(C.c_double)]
+        lib.nim_gpu_nusselt_noalloc.restype = C.c_int
         _gpu = lib
     return _gpu
 
