@@ -132,7 +132,8 @@ def test_reference_case_two_steps():
         # path: agreement to the tolerance's scale
         assert abs(a.nu_inner - c.nu_inner) <= 1e-4 * abs(c.nu_inner)
     # exp() of CUDA and of glibc differ in the last bit for some arguments and
-    # M_A(.,5) amplifies that by ~1/Pe^2 near |Pe| = v_limit
+    # the exponential form of M_A(.,5) amplifies that by ~12/|Pe|^3 near
+    # |Pe| = v_limit
     compare(gpu, par, STATE, 1e-9, "reference case")
 
 
