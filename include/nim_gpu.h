@@ -136,8 +136,15 @@ typedef struct nim_params {
                            (is_check_steady_state, nse.f90:60-69)              */
   int32_t dpdx_tolerance; /* 1: err_p from pressure gradients (is_dpdx_tolerance,
                            nse.f90:292-307)                                     */
-  int32_t reserved;
+  int32_t schedule;     /* NIM_SCHEDULE_PARALLEL (0): every sweep reads the
+                           values from before the sweep (fastest);
+                           NIM_SCHEDULE_REFERENCE (1): the Gauss-Seidel sweeps
+                           run in the reference's cell-number order
+                           (run.sh:2, one OpenMP thread), reproducing its
+                           iterates                                          */
 } nim_params;
+
+enum { NIM_SCHEDULE_PARALLEL = 0, NIM_SCHEDULE_REFERENCE = 1 };
 
 /* Statistics of one time step (the values the reference prints at
    nse.f90:169-171 and nse.f90:2793-2794, returned instead of printed). */

@@ -7,6 +7,8 @@
 //   nim_gpu_end_step   update_time_step + find_Nu2 (nse.f90:72-73)
 // The inner loop runs as CUDA graphs of whole iterations; the stop test lives
 // on the device (k_iter_end) and the host only polls it between batches.
+// With NIM_SCHEDULE_REFERENCE the four Gauss-Seidel sweeps run as in-place
+// level-by-level sweeps (k_seq_*) that reproduce the reference's cell order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -74,6 +76,12 @@ struct nim_ctx {
   double host_sums[8] = {0};
   long long launches = 0;    // kernels queued since creation
   int kernels_per_iter = 0;
+  // reference-order schedule
+  bool seq = false;
+  int *order = nullptr, *lstart = nullptr;  // cells level by level, level starts
+  int nlev = 0;
+  int *border = nullptr, *blev = nullptr, *wlev = nullptr;  // wall faces, levels, per-wall level ranges
+  int coop_vel = 0, coop_p = 0, coop_T = 0;  // cooperative grid sizes
 };
 
 namespace {
@@ -189,13 +197,50 @@ Phys make_phys(const nim_params &p) {
   return P;
 }
 
+template <typename K>
+int launch_coop(K kern, int blocks, nim_ctx *x) {
+  Dims d = x->d;
+  Geo g = x->g;
+  Fields F = x->F;
+  Phys P = x->phys;
+  Ctrl *ctl = x->ctl;
+  const int *order = x->order, *lstart = x->lstart;
+  int nlev = x->nlev;
+  void *args[] = {&d, &g, &F, &P, &ctl, &order, &lstart, &nlev};
+  CK(cudaLaunchCooperativeKernel((const void *)kern, dim3(blocks), dim3(BLK), args, 0, x->stream));
+  return NIM_OK;
+}
+
+// one pass of integrate_nse's loop body in the reference's order: the source
+// kernels store their terms, the sweeps run level by level in place
+int launch_iteration_seq(nim_ctx *x) {
+  const Dims &d = x->d;
+  cudaStream_t s = x->stream;
+  k_vel_cell<true><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  TRY(launch_coop(k_seq_vel, x->coop_vel, x));
+  k_p_src<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_seq_pbc<<<2, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl, x->border, x->blev, x->wlev, 0);
+  k_seq_pbc<<<2, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl, x->border, x->blev, x->wlev, 2);
+  TRY(launch_coop(k_seq_p, x->coop_p, x));
+  if (x->phys.dpdx_tolerance) k_p_dpdx<<<x->nblk_c, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+  k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+  k_T_cell<true><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  TRY(launch_coop(k_seq_T, x->coop_T, x));
+  k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
+  CK(cudaGetLastError());
+  x->kernels_per_iter = x->phys.dpdx_tolerance ? 11 : 10;
+  x->launches += x->kernels_per_iter;
+  return NIM_OK;
+}
+
 // one pass of integrate_nse's loop body
 int launch_iteration(nim_ctx *x) {
+  if (x->seq) return launch_iteration_seq(x);
   const Dims &d = x->d;
   cudaStream_t s = x->stream;
   const int gc = x->nblk_c, gb = x->nblk_b;
   const dim3 g3 = x->g3, g8 = x->g8;
-  k_vel_cell<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_vel_cell<false><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_vel_face<<<x->nblk_c3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_p_bc<<<gb, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
@@ -203,7 +248,7 @@ int launch_iteration(nim_ctx *x) {
   k_p_face<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   if (x->phys.dpdx_tolerance) k_p_dpdx<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
   k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
-  k_T_cell<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_T_cell<false><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_T_face<<<g8, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
   CK(cudaGetLastError());
@@ -250,7 +295,10 @@ __global__ void k_step_reset(Ctrl *ctl) {
   for (int q = 0; q < 4; ++q) ctl->red[q] = 0ull;
 }
 
-__global__ void k_run_reset(Ctrl *ctl) {
+// pmask: 1 double-buffers the face fields (parallel schedule), 0 keeps one
+// half that the reference-order sweeps update in place
+__global__ void k_run_reset(Ctrl *ctl, int pmask) {
+  ctl->pmask = pmask;
   for (int p = 0; p < 2; ++p)
     for (int q = 0; q < 8; ++q) ctl->err[p][q] = 0ull;
   for (int q = 0; q < 8; ++q) ctl->wall_floor[q] = 0ull;
@@ -383,6 +431,80 @@ static int noalloc_setup(int device) {
   return NIM_OK;
 }
 
+// Level orders of the reference-order sweeps.  Cells: level i + 2j + 3k,
+// which every dependence of a sweep crosses in the direction of the cell
+// numbers (the argument is in nim_kernels.cuh).  Wall faces, in BC-list
+// order bottom, top, inner, outer: level i + 2j on bottom and top, i + 2k on
+// inner and outer.  Also the sweep buffers and the cooperative grid sizes.
+static int setup_levels(nim_ctx *x) {
+  const Dims &d = x->d;
+  const size_t Nc = d.Nc;
+  TRY(dalloc(x, &x->F.Bv, 3 * Nc));
+  TRY(dalloc(x, &x->F.MTF4, 8 * Nc));
+  TRY(dalloc(x, &x->F.RDT, Nc));
+  // counting sort of the cells by level
+  const int nlev = (d.NT - 1) + 2 * (d.NR - 1) + 3 * (d.NZ - 1) + 1;
+  std::vector<int> lstart(nlev + 1, 0), order(Nc), fill;
+  for (int c = 0; c < d.Nc; ++c) {
+    const Cell q = Cell::of(d, c);
+    ++lstart[q.i + 2 * q.j + 3 * q.k + 1];
+  }
+  int maxlev = 0;
+  for (int L = 0; L < nlev; ++L) {
+    maxlev = std::max(maxlev, lstart[L + 1]);
+    lstart[L + 1] += lstart[L];
+  }
+  fill.assign(lstart.begin(), lstart.end() - 1);
+  for (int c = 0; c < d.Nc; ++c) {
+    const Cell q = Cell::of(d, c);
+    order[fill[q.i + 2 * q.j + 3 * q.k]++] = c;
+  }
+  // wall faces: per wall, counting sort by the in-wall level
+  const int nb1 = d.NT * d.NR, nb3 = d.NT * d.NZ;
+  const int w0[4] = {0, nb1, 2 * nb1, 2 * nb1 + nb3}, wn[4] = {nb1, nb1, nb3, nb3};
+  const int wl[4] = {d.NT + 2 * (d.NR - 1), d.NT + 2 * (d.NR - 1), d.NT + 2 * (d.NZ - 1), d.NT + 2 * (d.NZ - 1)};
+  std::vector<int> border(d.NBF), blev(1, 0), wlev(1, 0);
+  int q = 0;
+  for (int w = 0; w < 4; ++w) {
+    std::vector<int> cnt(wl[w] + 1, 0);
+    for (int r = 0; r < wn[w]; ++r) ++cnt[r % d.NT + 2 * (r / d.NT) + 1];
+    for (int L = 0; L < wl[w]; ++L) cnt[L + 1] += cnt[L];
+    std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+    for (int r = 0; r < wn[w]; ++r) border[q + pos[r % d.NT + 2 * (r / d.NT)]++] = w0[w] + r;
+    for (int L = 1; L <= wl[w]; ++L) blev.push_back(q + cnt[L]);
+    q += wn[w];
+    wlev.push_back((int)blev.size() - 1);
+  }
+  x->nlev = nlev;
+  TRY(dalloc(x, &x->order, Nc));
+  TRY(dalloc(x, &x->lstart, (size_t)nlev + 1));
+  TRY(dalloc(x, &x->border, (size_t)d.NBF));
+  TRY(dalloc(x, &x->blev, blev.size()));
+  TRY(dalloc(x, &x->wlev, wlev.size()));
+  CK(cudaMemcpy(x->order, order.data(), sizeof(int) * Nc, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(x->lstart, lstart.data(), sizeof(int) * (nlev + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(x->border, border.data(), sizeof(int) * d.NBF, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(x->blev, blev.data(), sizeof(int) * blev.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(x->wlev, wlev.data(), sizeof(int) * wlev.size(), cudaMemcpyHostToDevice));
+  // cooperative grids: no more blocks than the widest level needs, and no
+  // more than can be resident at once (cudaLaunchCooperativeKernel rejects
+  // a larger grid rather than running it)
+  int sms = 0, coop = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device));
+  CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, x->device));
+  if (!coop) return NIM_ERR_CUDA;
+  const int want = std::max(1, (maxlev + BLK - 1) / BLK);
+  int per = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_seq_vel, BLK, 0));
+  x->coop_vel = std::max(1, std::min(want, per * sms));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_seq_p, BLK, 0));
+  x->coop_p = std::max(1, std::min(want, per * sms));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_seq_T, BLK, 0));
+  x->coop_T = std::max(1, std::min(want, per * sms));
+  if (x->coop_vel < 1 || x->coop_p < 1 || x->coop_T < 1) return NIM_ERR_CUDA;
+  return NIM_OK;
+}
+
 static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) {
   CK(cudaGetDevice(&x->device));
   TRY(noalloc_setup(x->device));
@@ -392,6 +514,7 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
   std::vector<int> perm;
   TRY(verify_mesh(m, d, perm));
   x->params = *p;
+  x->seq = (p->schedule == NIM_SCHEDULE_REFERENCE);
   x->phys = make_phys(*p);
   x->gq = make_gauss();
   x->nblk_c = grid(d.Nc);
@@ -445,6 +568,7 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
   TRY(dalloc(x, &x->scratch, std::max(54 * Nc, 3 * NF)));
   TRY(dalloc(x, &x->sums, 8));
   CK(cudaMallocHost(&x->ctl_host, sizeof(Ctrl)));
+  if (x->seq) TRY(setup_levels(x));
   CK(cudaMemcpyAsync(x->node_xyz, m->node_xyz, 3 * sizeof(double) * m->nnode, cudaMemcpyHostToDevice, x->stream));
   double bcv[25];
   for (int f = 0; f < 5; ++f)
@@ -462,6 +586,7 @@ extern "C" int nim_gpu_create(const nim_mesh_desc *m, const nim_params *p, nim_c
   if (m->n_theta < 6 || m->n_r < 3 || m->n_z < 3) return NIM_ERR_BAD_ARG;
   if ((int64_t)m->n_theta * m->n_r * m->n_z > (int64_t)INT32_MAX / 4) return NIM_ERR_BAD_ARG;
   if (!(p->DT > 0) || !(p->nu > 0) || !(p->alpha > 0) || !(p->rho > 0)) return NIM_ERR_BAD_ARG;
+  if (p->schedule != NIM_SCHEDULE_PARALLEL && p->schedule != NIM_SCHEDULE_REFERENCE) return NIM_ERR_BAD_ARG;
   *out = nullptr;
   nim_ctx *x = new (std::nothrow) nim_ctx();
   if (!x) return NIM_ERR_BAD_ARG;
@@ -479,7 +604,7 @@ extern "C" int nim_gpu_init(nim_ctx *x) {
   CK(cudaSetDevice(x->device));
   const Dims &d = x->d;
   cudaStream_t s = x->stream;
-  k_run_reset<<<1, 1, 0, s>>>(x->ctl);
+  k_run_reset<<<1, 1, 0, s>>>(x->ctl, x->seq ? 0 : 1);
   k_cell_geometry<<<x->nblk_c, BLK, 0, s>>>(d, x->gq, x->node_xyz, x->g);
   k_metric_derived<<<x->nblk_c, BLK, 0, s>>>(d, x->g);
   k_pressure_coeffs<<<x->nblk_c, BLK, 0, s>>>(d, x->g, x->params.rho);
@@ -554,8 +679,8 @@ extern "C" int nim_gpu_iterate(nim_ctx *x, int32_t n, nim_step_stats *s) {
 extern "C" int nim_gpu_integrate(nim_ctx *x, nim_step_stats *s) {
   if (!x) return NIM_ERR_BAD_ARG;
   if (!x->initialized || !x->in_step) return NIM_ERR_STATE;
-  const int G = 4;  // iterations per graph launch
-  if (!x->graph || x->graph_iters != G) TRY(build_graph(x, G));
+  const int G = 4;  // iterations per graph launch (per poll, reference order)
+  if (!x->seq && (!x->graph || x->graph_iters != G)) TRY(build_graph(x, G));
   // launch ahead by the previous step's count, then poll
   int ahead = std::max(1, (x->last_iters * 7 / 8) / G);
   // with max_iters <= 0 the device never stops on its own; bound the host loop
@@ -563,9 +688,13 @@ extern "C" int nim_gpu_integrate(nim_ctx *x, nim_step_stats *s) {
   long long launched = 0;
   bool capped = false;
   for (;;) {
-    for (int k = 0; k < ahead; ++k) CK(cudaGraphLaunch(x->graph, x->stream));
+    if (x->seq) {
+      for (int k = 0; k < ahead * G; ++k) TRY(launch_iteration(x));
+    } else {
+      for (int k = 0; k < ahead; ++k) CK(cudaGraphLaunch(x->graph, x->stream));
+      x->launches += (long long)ahead * G * x->kernels_per_iter;
+    }
     launched += (long long)ahead * G;
-    x->launches += (long long)ahead * G * x->kernels_per_iter;
     TRY(read_ctrl(x));
     if (x->ctl_host->done) break;
     if (launched >= cap) {
@@ -662,7 +791,7 @@ extern "C" int nim_gpu_download(nim_ctx *x, nim_field f, double *host, int64_t n
   if (!x->initialized) return NIM_ERR_STATE;
   TRY(read_ctrl(x));
   FieldView v;
-  TRY(field_view(x, f, x->ctl_host->iter & 1, v));
+  TRY(field_view(x, f, x->seq ? 0 : (x->ctl_host->iter & 1), v));
   const int64_t len = (int64_t)v.n * v.K;
   if (n < len) return NIM_ERR_BAD_ARG;
   k_gather<<<grid(v.n), BLK, 0, x->stream>>>(v.src, v.stride, v.K, v.face ? x->perm : nullptr, v.n, x->scratch);
@@ -677,7 +806,7 @@ extern "C" int nim_gpu_upload(nim_ctx *x, nim_field f, const double *host, int64
   if (!x->initialized) return NIM_ERR_STATE;
   TRY(read_ctrl(x));
   FieldView v;
-  TRY(field_view(x, f, x->ctl_host->iter & 1, v));
+  TRY(field_view(x, f, x->seq ? 0 : (x->ctl_host->iter & 1), v));
   if (!v.writable || v.K != 1) return NIM_ERR_BAD_ARG;
   if (n < v.n) return NIM_ERR_BAD_ARG;
   CK(cudaMemcpyAsync(x->scratch, host, sizeof(double) * v.n, cudaMemcpyHostToDevice, x->stream));
@@ -717,6 +846,7 @@ extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int
   const int NK = 11;
   if (!x || n <= 0 || !ms || cap < NK) return NIM_ERR_BAD_ARG;
   if (!x->initialized) return NIM_ERR_STATE;
+  if (x->seq) return NIM_ERR_STATE;  // times the parallel-schedule kernels
   const Dims &d = x->d;
   cudaStream_t s = x->stream;
   cudaEvent_t ev[NK + 1];
@@ -730,7 +860,7 @@ extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int
   const dim3 g3 = x->g3, g8 = x->g8;
   for (int it = 0; it < n; ++it) {
     CK(cudaEventRecord(ev[0], s));
-    k_vel_cell<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_vel_cell<false><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[1], s));
     k_vel_face<<<x->nblk_c3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[2], s));
@@ -746,7 +876,7 @@ extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int
     CK(cudaEventRecord(ev[7], s));
     k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
     CK(cudaEventRecord(ev[8], s));
-    k_T_cell<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_T_cell<false><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[9], s));
     k_T_face<<<g8, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[10], s));

@@ -23,6 +23,8 @@
 // Every sweep reads only values from before the sweep, so the result does not
 // depend on thread order.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "nim_common.cuh"
 
 namespace nim {
@@ -62,6 +64,10 @@ struct Fields {
   double *MF;      // [15][Nc]  M_F1..3(k) at 5(d-1)+k-1
   double *MTF;     // [15][Nc]  MT_F1..3
   double *dpd;     // [3][Nc]   dpdx_old, dpdy_old, dpdz_old
+  // reference-order schedule: sources stored before the ordered sweeps
+  double *Bv;      // [3][Nc]   R_C + R_D + R_B of u, v, w
+  double *MTF4;    // [8][Nc]   MT_F4
+  double *RDT;     // [Nc]      R_D_T
   double *part;    // [8][nblk] per-block partial sums
 };
 
@@ -85,7 +91,9 @@ struct Ctrl {
   int done;         // 1: current step's inner loop has stopped
   int status;       // NIM_OK / NIM_ERR_NOT_CONVERGED / NIM_ERR_NONFINITE
   int first;        // 1 until the first iteration after init has finished
-  int pad[3];
+  int pmask;        // 1: face arrays alternate halves each pass (parallel
+                    // schedule); 0: one half, updated in place (reference order)
+  int pad[2];
   double last_err[5];
   unsigned long long wall_floor[8];  // max |Dirichlet wall value| bits (find_error
                                      // compares with zero-initialised arrays once)
@@ -680,7 +688,28 @@ __global__ void __launch_bounds__(BLK) k_vel_coef_F(Dims d, Fields F, Phys P) {
 }
 
 // =========================================================== iteration
-__device__ __forceinline__ int parity(const Ctrl *ctl) { return ctl->iter & 1; }
+// Load policies: the parallel kernels read with plain (L1-cached) loads; the
+// reference-order sweeps read data that other SMs rewrote one level earlier,
+// so they load through L2 only (ld.global.cg).
+struct LdPlain {
+  __device__ __forceinline__ static double ld(const double *p, size_t i) { return p[i]; }
+};
+// Loads of values the same launch rewrites in place (the reference-order
+// sweeps): a relaxed GPU-scope load, not cached in L1 and ordered against
+// this thread's own stores (volatile asm with a memory clobber), so it sees
+// every store made before the last grid or block barrier and this thread's
+// own earlier stores.
+struct LdCoh {
+  __device__ __forceinline__ static double ld(const double *p, size_t i) {
+    double r;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(r) : "l"(p + i) : "memory");
+    return r;
+  }
+};
+
+__device__ __forceinline__ int parity(const Ctrl *ctl) { return ctl->iter & ctl->pmask; }
+// half holding the values a sweep earlier in this pass produced
+__device__ __forceinline__ int newhalf(const Ctrl *ctl) { return ctl->pmask ? 1 - parity(ctl) : parity(ctl); }
 
 // Green-Gauss derivative dphi_dx2/dy2/dz2 (nse.f90:2866-2903), component cc
 __device__ __forceinline__ double green_gauss(const Geo &g, size_t NF, double invV, const double phi[7],
@@ -693,17 +722,18 @@ __device__ __forceinline__ double green_gauss(const Geo &g, size_t NF, double in
 // Derivative of face field phi along local direction e on face fpos of cell
 // x: centred, or second-order one-sided at walls (the ni/nj/nk stencils of
 // calculate_R_D2, nse.f90:1635-1838; integrate_pressure_field_i; bc.f90).
+template <class Ld = LdPlain>
 __device__ __forceinline__ double tangential(const Dims &d, const double *__restrict__ phi, const Cell &x, int fpos,
                                              int e) {
   const bool lo = !x.has_nb(d, 2 * e - 1), hi = !x.has_nb(d, 2 * e);
   if (lo) {
     const Cell m2 = x.nb(d, 2 * e), m3 = m2.nb(d, 2 * e);
-    return (-(3 * phi[x.face(d, fpos)]) + 4 * phi[m2.face(d, fpos)] - phi[m3.face(d, fpos)]) / 4.;
+    return (-(3 * Ld::ld(phi, x.face(d, fpos))) + 4 * Ld::ld(phi, m2.face(d, fpos)) - Ld::ld(phi, m3.face(d, fpos))) / 4.;
   } else if (hi) {
     const Cell m1 = x.nb(d, 2 * e - 1), m3 = m1.nb(d, 2 * e - 1);
-    return (3 * phi[x.face(d, fpos)] - 4 * phi[m1.face(d, fpos)] + phi[m3.face(d, fpos)]) / 4.;
+    return (3 * Ld::ld(phi, x.face(d, fpos)) - 4 * Ld::ld(phi, m1.face(d, fpos)) + Ld::ld(phi, m3.face(d, fpos))) / 4.;
   }
-  return (phi[x.nb(d, 2 * e).face(d, fpos)] - phi[x.nb(d, 2 * e - 1).face(d, fpos)]) / 4.;
+  return (Ld::ld(phi, x.nb(d, 2 * e).face(d, fpos)) - Ld::ld(phi, x.nb(d, 2 * e - 1).face(d, fpos))) / 4.;
 }
 
 // G_i d_i phi - g^ij d_ij phi of calculate_R_D2 / R_D_p2 / R_D_T
@@ -736,25 +766,28 @@ __device__ __forceinline__ void cell_faces(const Dims &d, const Cell &x, int f[7
 }
 
 // Cell-average update (nse.f90:840-848; T: 1018-1026)
+template <class Ld = LdPlain>
 __device__ __forceinline__ double cell_update(const double *__restrict__ fr, const int f[7], double c, double cold,
                                               double B, const double F4[8], double w) {
   return (1 - w) * c +
-         (w / F4[0]) * (+F4[1] * cold + F4[2] * fr[f[1]] + F4[3] * fr[f[2]] + F4[4] * fr[f[3]] + F4[5] * fr[f[4]] +
-                        F4[6] * fr[f[5]] + F4[7] * fr[f[6]] + B);
+         (w / F4[0]) * (+F4[1] * cold + F4[2] * Ld::ld(fr, f[1]) + F4[3] * Ld::ld(fr, f[2]) +
+                        F4[4] * Ld::ld(fr, f[3]) + F4[5] * Ld::ld(fr, f[4]) + F4[6] * Ld::ld(fr, f[5]) +
+                        F4[7] * Ld::ld(fr, f[6]) + B);
 }
 
 // +xi_d face update (nse.f90:878-1005; T: 1033-1088)
+template <class Ld = LdPlain>
 __device__ __forceinline__ double face_update(const Dims &d, const double *__restrict__ fr, const double *__restrict__ cv,
                                               const double *__restrict__ co, const double Fd[5], double dg0,
                                               double dg1, int dd, const Cell &x, const Cell &x2, double w) {
   const int e1 = tr1(dd), e2 = tr2(dd);
-  const double B3 = (dg0) * (fr[x.face(d, 2 * e1)] - fr[x.face(d, 2 * e1 - 1)] + fr[x2.face(d, 2 * e1)] -
-                             fr[x2.face(d, 2 * e1 - 1)]) / 4.0;
-  const double B4 = (dg1) * (fr[x.face(d, 2 * e2)] - fr[x.face(d, 2 * e2 - 1)] + fr[x2.face(d, 2 * e2)] -
-                             fr[x2.face(d, 2 * e2 - 1)]) / 4.0;
-  return (1 - w) * fr[x.face(d, 2 * dd)] +
-         (w / Fd[0]) * (+Fd[1] * fr[x.face(d, 2 * dd - 1)] + Fd[2] * fr[x2.face(d, 2 * dd)] +
-                        Fd[3] * (cv[x.c] + co[x.c]) + Fd[4] * (cv[x2.c] + co[x2.c]) - B3 - B4);
+  const double B3 = (dg0) * (Ld::ld(fr, x.face(d, 2 * e1)) - Ld::ld(fr, x.face(d, 2 * e1 - 1)) +
+                             Ld::ld(fr, x2.face(d, 2 * e1)) - Ld::ld(fr, x2.face(d, 2 * e1 - 1))) / 4.0;
+  const double B4 = (dg1) * (Ld::ld(fr, x.face(d, 2 * e2)) - Ld::ld(fr, x.face(d, 2 * e2 - 1)) +
+                             Ld::ld(fr, x2.face(d, 2 * e2)) - Ld::ld(fr, x2.face(d, 2 * e2 - 1))) / 4.0;
+  return (1 - w) * Ld::ld(fr, x.face(d, 2 * dd)) +
+         (w / Fd[0]) * (+Fd[1] * Ld::ld(fr, x.face(d, 2 * dd - 1)) + Fd[2] * Ld::ld(fr, x2.face(d, 2 * dd)) +
+                        Fd[3] * (Ld::ld(cv, x.c) + co[x.c]) + Fd[4] * (Ld::ld(cv, x2.c) + co[x2.c]) - B3 - B4);
 }
 
 __device__ __forceinline__ double errv(double nw, double old, bool first) { return fabs(nw - (first ? 0.0 : old)); }
@@ -778,6 +811,9 @@ __device__ __forceinline__ bool patch_cell(const Dims &d, Cell &x) {
 // calculate_R_D2 1628-1860; cell part of integrate_velocity_field_formulation2_i
 // 839-872).  R_C (calculate_R_c_new, 1393-1434) is identically zero.
 // Block (CB, 3): threadIdx.y = velocity component.
+// SRC_ONLY (reference-order schedule): store R_C + R_D + R_B and leave the
+// update to k_seq_vel, as update_velocity_sources precedes the sweep.
+template <bool SRC_ONLY>
 __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
@@ -804,12 +840,16 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, Geo g, Fields F, Ph
     double F4[8];
     for (int k = 0; k < 8; ++k) F4[k] = F.MF4[(size_t)k * Nc + c];
     const double B = (0. + RD + RB);
-    const double cold = F.c[q][c];
-    const double nw = cell_update(fr, f, cold, F.co[q][c], B, F4, P.w[q]);
-    F.c[q][c] = nw;
-    e[q] = errv(nw, cold, first);
+    if (SRC_ONLY) {
+      F.Bv[(size_t)q * Nc + c] = B;
+    } else {
+      const double cold = F.c[q][c];
+      const double nw = cell_update(fr, f, cold, F.co[q][c], B, F4, P.w[q]);
+      F.c[q][c] = nw;
+      e[q] = errv(nw, cold, first);
+    }
   }
-  block_max<3, CB3>(red, e, ctl->err[par]);
+  if (!SRC_ONLY) block_max<3, CB3>(red, e, ctl->err[par]);
 }
 
 // ---- K2: +xi face updates of u, v, w (nse.f90:878-1005).
@@ -863,7 +903,7 @@ __global__ void __launch_bounds__(CB3, 3) k_p_src(Dims d, Geo g, Fields F, Phys 
   if (active) {
     cell_faces(d, x, f);
     const double invV = 1. / g.vol[c];
-    const double *fq = F.f[q] + (1 - par) * NF;
+    const double *fq = F.f[q] + newhalf(ctl) * NF;
     double vf[7];
     for (int k = 1; k <= 6; ++k) vf[k] = fq[f[k]];
     for (int cc = 0; cc < 3; ++cc) sh[q][cc][tx] = green_gauss(g, NF, invV, vf, f, cc);
@@ -903,50 +943,63 @@ __global__ void __launch_bounds__(CB3, 3) k_p_src(Dims d, Geo g, Fields F, Phys 
   }
 }
 
-// ---- K4: apply_pressure_bc (bc.f90:141-342), reading cur, writing next
+// ---- apply_pressure_bc for wall face b (bc.f90:148-339): the new value
+// from the pressures pr, the new velocities fu/fv/fwv and the temperatures fT
+template <class Ld>
+__device__ __forceinline__ double p_bc_value(const Dims &d, const Geo &g, const Fields &F, const Phys &P,
+                                             const double *pr, const double *fu, const double *fv, const double *fwv,
+                                             const double *fT, int b) {
+  const size_t NF = d.NF, NB = d.NBF;
+  const BFace B = bface(d, b);
+  const Cell M1 = B.cell;
+  const int pos = B.pos;
+  const int fw0 = M1.face(d, pos);
+  const double n[3] = {g.normal[fw0], g.normal[NF + fw0], g.normal[2 * NF + fw0]};
+  const double bvec[3] = {0., 0., -(P.g_beta * (fT[fw0]))};
+  const double b_n = dot3(bvec, n);
+  double vn[6];
+  for (int j = 1; j <= 5; ++j) {
+    const int pt = g.bcpts[(j - 1) * NB + b];
+    const double v[3] = {fu[pt], fv[pt], fwv[pt]};
+    vn[j] = dot3(v, n);
+  }
+  const double *a = g.bca;
+  const double d2udn2 = -(a[b] * vn[1]) - a[NB + b] * vn[2] - a[2 * NB + b] * vn[3] - a[3 * NB + b] * vn[4] -
+                        a[4 * NB + b] * vn[5];
+  const int dd = (pos + 1) / 2;
+  const double B2 = tangential<Ld>(d, pr, M1, pos, tr1(dd)) * g.bcg[b];
+  const double B3 = tangential<Ld>(d, pr, M1, pos, tr2(dd)) * g.bcg[NB + b];
+  const double *ap = g.bcap;
+  const double B1 = ap[7 * NB + b] * (F.Rp[M1.c]);
+  double s = 0.0;
+  bool firstterm = true;
+  for (int k = 1; k <= 6; ++k) {
+    if (k == pos) continue;
+    const double t = ap[(k - 1) * NB + b] * Ld::ld(pr, M1.face(d, k));
+    s = firstterm ? -t : s - t;
+    firstterm = false;
+  }
+  const double w = P.w_p2;
+  return (1 - w) * Ld::ld(pr, fw0) +
+         w / (ap[(pos - 1) * NB + b]) * (s + B1 - B2 - B3 + (P.nu * P.rho * d2udn2 - b_n * P.rho));
+}
+
+// ---- K4: apply_pressure_bc, every wall face from the values before the pass
 __global__ void __launch_bounds__(BLK) k_p_bc(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
-  const int par = parity(ctl);
+  const int par = parity(ctl), nh = newhalf(ctl);
   const bool first = ctl->first;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   double e[1] = {0.};
   if (b < d.NBF) {
-    const size_t NF = d.NF, NB = d.NBF;
-    const BFace B = bface(d, b);
-    const Cell M1 = B.cell;
-    const int pos = B.pos;
-    const int fw0 = M1.face(d, pos);
+    const size_t NF = d.NF;
     const double *pr = F.f[3] + par * NF;
-    const double *fu = F.f[0] + (1 - par) * NF, *fv = F.f[1] + (1 - par) * NF, *fwv = F.f[2] + (1 - par) * NF;
-    const double n[3] = {g.normal[fw0], g.normal[NF + fw0], g.normal[2 * NF + fw0]};
-    const double bvec[3] = {0., 0., -(P.g_beta * (F.f[4][par * NF + fw0]))};
-    const double b_n = dot3(bvec, n);
-    double vn[6];
-    for (int j = 1; j <= 5; ++j) {
-      const int pt = g.bcpts[(j - 1) * NB + b];
-      const double v[3] = {fu[pt], fv[pt], fwv[pt]};
-      vn[j] = dot3(v, n);
-    }
-    const double *a = g.bca;
-    const double d2udn2 = -(a[b] * vn[1]) - a[NB + b] * vn[2] - a[2 * NB + b] * vn[3] - a[3 * NB + b] * vn[4] -
-                          a[4 * NB + b] * vn[5];
-    const int dd = (pos + 1) / 2;
-    const double B2 = tangential(d, pr, M1, pos, tr1(dd)) * g.bcg[b];
-    const double B3 = tangential(d, pr, M1, pos, tr2(dd)) * g.bcg[NB + b];
-    const double *ap = g.bcap;
-    const double B1 = ap[7 * NB + b] * (F.Rp[M1.c]);
-    double s = 0.0;
-    bool firstterm = true;
-    for (int k = 1; k <= 6; ++k) {
-      if (k == pos) continue;
-      const double t = ap[(k - 1) * NB + b] * pr[M1.face(d, k)];
-      s = firstterm ? -t : s - t;
-      firstterm = false;
-    }
-    const double w = P.w_p2;
-    const double nw = (1 - w) * pr[fw0] + w / (ap[(pos - 1) * NB + b]) * (s + B1 - B2 - B3 + (P.nu * P.rho * d2udn2 - b_n * P.rho));
+    const double nw = p_bc_value<LdPlain>(d, g, F, P, pr, F.f[0] + nh * NF, F.f[1] + nh * NF, F.f[2] + nh * NF,
+                                          F.f[4] + par * NF, b);
+    const BFace B = bface(d, b);
+    const int fw0 = B.cell.face(d, B.pos);
     F.f[3][(1 - par) * NF + fw0] = nw;
     e[0] = errv(nw, pr[fw0], first);
   }
@@ -970,7 +1023,34 @@ __constant__ unsigned char kPTerms[3][10][3] = {
     {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
     {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {6, 4, 1}, {7, 3, 2}, {8, 4, 2}, {9, 5, 1}, {11, 6, 2}}};
 
-// ---- K5: integrate_pressure_field_i (nse.f90:1091-1289), cur -> next.
+// ---- integrate_pressure_field_i for the +xi_dd face of cell x
+// (nse.f90:1091-1289): the new value from the pressures pr
+template <class Ld>
+__device__ __forceinline__ double p_face_value(const Dims &d, const Geo &g, const Fields &F, const Phys &P,
+                                               const double *pr, const Cell &x, int dd) {
+  const size_t Nc = d.Nc;
+  const int c = x.c;
+  const unsigned char(*tab)[10][3] = kPTerms;
+  const int diag = (dd == 1) ? 2 : (dd == 2) ? 6 : 10;
+  const Cell n2 = x.nb(d, 2 * dd);
+  const double *A = g.AA + (size_t)15 * (dd - 1) * Nc;
+  const double B1 = (F.Rp[c]) * A[12 * Nc + c];
+  const double B2 = (F.Rp[n2.c]) * A[14 * Nc + c];
+  const double B3 = (g.dg[(2 * (dd - 1)) * Nc + c]) * tangential<Ld>(d, pr, x, 2 * dd, tr1(dd));
+  const double B4 = (g.dg[(2 * (dd - 1) + 1) * Nc + c]) * tangential<Ld>(d, pr, x, 2 * dd, tr2(dd));
+  double s = 0.0;
+#pragma unroll
+  for (int t = 0; t < 10; ++t) {
+    const Cell &cl = (tab[dd - 1][t][2] == 1) ? x : n2;
+    const double term = A[(size_t)(tab[dd - 1][t][0] - 1) * Nc + c] * Ld::ld(pr, cl.face(d, tab[dd - 1][t][1]));
+    s = (t == 0) ? -term : s - term;
+  }
+  const int fo = x.face(d, 2 * dd);
+  const double w = P.w_p;
+  return (1 - w) * Ld::ld(pr, fo) + w / (A[(size_t)(diag - 1) * Nc + c]) * (s + B1 + B2 + B3 + B4);
+}
+
+// ---- K5: integrate_pressure_field_i, cur -> next.
 // Block (CB, 3): threadIdx.y = direction.
 __global__ void __launch_bounds__(CB3, 3) k_p_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
@@ -981,33 +1061,14 @@ __global__ void __launch_bounds__(CB3, 3) k_p_face(Dims d, Geo g, Fields F, Phys
   const int dd = threadIdx.y + 1;
   Cell x;
   const bool act = patch_cell(d, x);
-  const int c = x.c;
   double e[1] = {0.};
-  if (act) {
-    const size_t Nc = d.Nc, NF = d.NF;
+  if (act && x.has_nb(d, 2 * dd)) {
+    const size_t NF = d.NF;
     const double *pr = F.f[3] + par * NF;
-    if (x.has_nb(d, 2 * dd)) {
-      const unsigned char(*tab)[10][3] = kPTerms;
-      const int diag = (dd == 1) ? 2 : (dd == 2) ? 6 : 10;
-      const Cell n2 = x.nb(d, 2 * dd);
-      const double *A = g.AA + (size_t)15 * (dd - 1) * Nc;
-      const double B1 = (F.Rp[c]) * A[12 * Nc + c];
-      const double B2 = (F.Rp[n2.c]) * A[14 * Nc + c];
-      const double B3 = (g.dg[(2 * (dd - 1)) * Nc + c]) * tangential(d, pr, x, 2 * dd, tr1(dd));
-      const double B4 = (g.dg[(2 * (dd - 1) + 1) * Nc + c]) * tangential(d, pr, x, 2 * dd, tr2(dd));
-      double s = 0.0;
-#pragma unroll
-      for (int t = 0; t < 10; ++t) {
-        const Cell &cl = (tab[dd - 1][t][2] == 1) ? x : n2;
-        const double term = A[(size_t)(tab[dd - 1][t][0] - 1) * Nc + c] * pr[cl.face(d, tab[dd - 1][t][1])];
-        s = (t == 0) ? -term : s - term;
-      }
-      const int fo = x.face(d, 2 * dd);
-      const double w = P.w_p;
-      const double nw = (1 - w) * pr[fo] + w / (A[(size_t)(diag - 1) * Nc + c]) * (s + B1 + B2 + B3 + B4);
-      F.f[3][(1 - par) * NF + fo] = nw;
-      e[0] = errv(nw, pr[fo], first);
-    }
+    const double nw = p_face_value<LdPlain>(d, g, F, P, pr, x, dd);
+    const int fo = x.face(d, 2 * dd);
+    F.f[3][(1 - par) * NF + fo] = nw;
+    e[0] = errv(nw, pr[fo], first);
   }
   block_max<1, CB3>(red, e, ctl->err[par] + 3);
 }
@@ -1025,7 +1086,7 @@ __global__ void __launch_bounds__(BLK) k_p_dpdx(Dims d, Geo g, Fields F, Ctrl *c
     const size_t Nc = d.Nc, NF = d.NF;
     int f[7];
     cell_faces(d, x, f);
-    const double *p = F.f[3] + (1 - par) * NF;
+    const double *p = F.f[3] + newhalf(ctl) * NF;
     const double v[3] = {(p[f[2]] - p[f[1]]) / 2. * g.xi[0 * Nc + c], (p[f[4]] - p[f[3]]) / 2. * g.xi[4 * Nc + c],
                          (p[f[6]] - p[f[5]]) / 2. * g.xi[8 * Nc + c]};
     for (int q = 0; q < 3; ++q) {
@@ -1065,6 +1126,9 @@ __global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, Geo g, Fields F, Ctrl
 // Block (CB, 3): thread y forms MT_A of direction y+1 for the cell and its
 // +neighbour (MT_F of that face) and two of the six cross derivatives;
 // thread 0 assembles MT_F4, R_D_T and the update in the reference's order.
+// SRC_ONLY (reference-order schedule): store MT_F4 and R_D_T and leave the
+// update to k_seq_T.
+template <bool SRC_ONLY>
 __global__ void __launch_bounds__(CB3, 2) k_T_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
@@ -1127,12 +1191,17 @@ __global__ void __launch_bounds__(CB3, 2) k_T_cell(Dims d, Geo g, Fields F, Phys
     const double RDT = P.alpha * (Gv[c] * px + Gv[Nc + c] * py + Gv[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy -
                                   gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz - gij[2 * Nc + c] * pzx -
                                   gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
-    const double cold = F.c[3][c];
-    const double nw = cell_update(T, f, cold, F.co[3][c], (RDT + 0.), F4, P.w[3]);
-    F.c[3][c] = nw;
-    e[0] = errv(nw, cold, first);
+    if (SRC_ONLY) {
+      for (int k = 0; k < 8; ++k) F.MTF4[(size_t)k * Nc + c] = F4[k];
+      F.RDT[c] = RDT;
+    } else {
+      const double cold = F.c[3][c];
+      const double nw = cell_update(T, f, cold, F.co[3][c], (RDT + 0.), F4, P.w[3]);
+      F.c[3][c] = nw;
+      e[0] = errv(nw, cold, first);
+    }
   }
-  block_max<1, CB3>(red, e, ctl->err[par] + 4);
+  if (!SRC_ONLY) block_max<1, CB3>(red, e, ctl->err[par] + 4);
 }
 
 // ---- K8: +xi face updates of T (nse.f90:1033-1088), cur -> next; the z-wall
@@ -1172,7 +1241,7 @@ __global__ void __launch_bounds__(BLK, 4) k_T_face(Dims d, Geo g, Fields F, Phys
 // nse.f90:129 and the max_iters guard)
 __global__ void k_iter_end(Ctrl *ctl, Phys P) {
   if (ctl->done) return;
-  const int par = ctl->iter & 1;
+  const int par = ctl->iter & ctl->pmask;
   double e[5];
   bool finite = true;
   for (int q = 0; q < 5; ++q) {
@@ -1183,7 +1252,10 @@ __global__ void k_iter_end(Ctrl *ctl, Phys P) {
     if (ctl->first) e[q] = nmax(e[q], __longlong_as_double((long long)ctl->wall_floor[q]));
     ctl->last_err[q] = e[q];
   }
-  for (int q = 0; q < 8; ++q) ctl->err[1 - par][q] = 0ull;
+  // clear the slot the next pass accumulates into (the other one with
+  // double-buffered faces, this one with in-place sweeps)
+  const int nxt = (ctl->iter + 1) & ctl->pmask;
+  for (int q = 0; q < 8; ++q) ctl->err[nxt][q] = 0ull;
   ctl->iter += 1;
   ctl->step_iters += 1;
   ctl->first = 0;
@@ -1198,6 +1270,179 @@ __global__ void k_iter_end(Ctrl *ctl, Phys P) {
     ctl->done = 1;
     ctl->status = -3;  // NIM_ERR_NOT_CONVERGED
   }
+}
+
+// ============================================ reference-order sweeps
+// The reference runs every Gauss-Seidel sweep over cells in number order
+// (one OpenMP thread, run.sh:2).  A cell's update reads values of the cells
+// (di,dj,dk) in {(+-1,0,0),(0,+-1,0),(0,0,+-1),(0,0,+-2),(0,+-2,0),(+1,-1,0),
+// (+1,0,-1),(0,+1,-1),(-1,+1,0),(-1,0,+1),(0,-1,+1)} and no other cell's.
+// Ordering cells by the level t = i + 2j + 3k puts every such neighbour with
+// a smaller number on a lower level and every larger one on a higher level,
+// the theta seam included, so sweeping level by level, in
+// place, with a grid-wide barrier between levels reproduces the reference's
+// iterates exactly.  order[] lists the cells level by level, lstart[] the
+// level boundaries.
+
+// velocity sweep (integrate_velocity_field_formulation2_i, nse.f90:831-1006)
+__global__ void __launch_bounds__(BLK) k_seq_vel(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl,
+                                                 const int *__restrict__ order, const int *__restrict__ lstart,
+                                                 int nlev) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<3>(red);
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const size_t Nc = d.Nc, NF = d.NF;
+  double e[3] = {0., 0., 0.};
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  double *fr[3] = {F.f[0] + par * NF, F.f[1] + par * NF, F.f[2] + par * NF};
+  for (int L = 0; L < nlev; ++L) {
+    for (int q = lstart[L] + tid; q < lstart[L + 1]; q += nth) {
+      const int c = order[q];
+      const Cell x = Cell::of(d, c);
+      int f[7];
+      cell_faces(d, x, f);
+      double F4[8];
+      for (int k = 0; k < 8; ++k) F4[k] = F.MF4[(size_t)k * Nc + c];
+      for (int v = 0; v < 3; ++v) {
+        const double cold = LdCoh::ld(F.c[v], c);
+        const double nw = cell_update<LdCoh>(fr[v], f, cold, F.co[v][c], F.Bv[(size_t)v * Nc + c], F4, P.w[v]);
+        F.c[v][c] = nw;
+        e[v] = nmax(e[v], errv(nw, cold, first));
+      }
+      for (int dd = 1; dd <= 3; ++dd) {
+        if (!x.has_nb(d, 2 * dd)) continue;
+        const Cell x2 = x.nb(d, 2 * dd);
+        double Fd[5];
+        for (int k = 0; k < 5; ++k) Fd[k] = F.MF[(size_t)(5 * (dd - 1) + k) * Nc + c];
+        const double dg0 = g.dg[(2 * (dd - 1)) * Nc + c], dg1 = g.dg[(2 * (dd - 1) + 1) * Nc + c];
+        const int fo = x.face(d, 2 * dd);
+        for (int v = 0; v < 3; ++v) {
+          const double old = LdCoh::ld(fr[v], fo);
+          const double nw = face_update<LdCoh>(d, fr[v], F.c[v], F.co[v], Fd, dg0, dg1, dd, x, x2, P.w[v]);
+          fr[v][fo] = nw;
+          e[v] = nmax(e[v], errv(nw, old, first));
+        }
+      }
+    }
+    grid.sync();
+  }
+  block_max<3>(red, e, ctl->err[par]);
+}
+
+// pressure sweep (integrate_pressure_field_i, nse.f90:1091-1289)
+__global__ void __launch_bounds__(BLK) k_seq_p(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl,
+                                               const int *__restrict__ order, const int *__restrict__ lstart,
+                                               int nlev) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<1>(red);
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const size_t NF = d.NF;
+  double e[1] = {0.};
+  double *pr = F.f[3] + par * NF;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (int L = 0; L < nlev; ++L) {
+    for (int q = lstart[L] + tid; q < lstart[L + 1]; q += nth) {
+      const Cell x = Cell::of(d, order[q]);
+      for (int dd = 1; dd <= 3; ++dd) {
+        if (!x.has_nb(d, 2 * dd)) continue;
+        const int fo = x.face(d, 2 * dd);
+        const double old = LdCoh::ld(pr, fo);
+        const double nw = p_face_value<LdCoh>(d, g, F, P, pr, x, dd);
+        pr[fo] = nw;
+        e[0] = nmax(e[0], errv(nw, old, first));
+      }
+    }
+    grid.sync();
+  }
+  block_max<1>(red, e, ctl->err[par] + 3);
+}
+
+// temperature sweep (integrate_temperature_field_formulation2_i, nse.f90:1009-1089)
+__global__ void __launch_bounds__(BLK) k_seq_T(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl,
+                                               const int *__restrict__ order, const int *__restrict__ lstart,
+                                               int nlev) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<1>(red);
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const size_t Nc = d.Nc, NF = d.NF;
+  double e[1] = {0.};
+  double *T = F.f[4] + par * NF;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (int L = 0; L < nlev; ++L) {
+    for (int q = lstart[L] + tid; q < lstart[L + 1]; q += nth) {
+      const int c = order[q];
+      const Cell x = Cell::of(d, c);
+      int f[7];
+      cell_faces(d, x, f);
+      double F4[8];
+      for (int k = 0; k < 8; ++k) F4[k] = F.MTF4[(size_t)k * Nc + c];
+      const double cold = LdCoh::ld(F.c[3], c);
+      const double nw = cell_update<LdCoh>(T, f, cold, F.co[3][c], (F.RDT[c] + 0.), F4, P.w[3]);
+      F.c[3][c] = nw;
+      e[0] = nmax(e[0], errv(nw, cold, first));
+      for (int dd = 1; dd <= 3; ++dd) {
+        if (!x.has_nb(d, 2 * dd)) continue;
+        const Cell x2 = x.nb(d, 2 * dd);
+        double Fd[5];
+        for (int k = 0; k < 5; ++k) Fd[k] = F.MTF[(size_t)(5 * (dd - 1) + k) * Nc + c];
+        const int fo = x.face(d, 2 * dd);
+        const double old = LdCoh::ld(T, fo);
+        const double nwf = face_update<LdCoh>(d, T, F.c[3], F.co[3], Fd, g.dg[(2 * (dd - 1)) * Nc + c],
+                                             g.dg[(2 * (dd - 1) + 1) * Nc + c], dd, x, x2, P.w[3]);
+        T[fo] = nwf;
+        e[0] = nmax(e[0], errv(nwf, old, first));
+      }
+    }
+    grid.sync();
+  }
+  block_max<1>(red, e, ctl->err[par] + 4);
+}
+
+// apply_pressure_bc in the reference's BC-list order (bc.f90:148-340).  Within
+// one wall a face reads its in-wall neighbours (+-1, +-2 along the wall), so
+// levels t = (in-wall theta index) + 2 (other in-wall index) reproduce the
+// order; bottom and top do not read each other, inner and outer read bottom
+// and top only, so one block per wall runs {bottom, top} and then
+// {inner, outer}.  border[] lists BC-list indices wall by wall and level by
+// level; wlev[w] .. wlev[w+1] are wall w's entries of blev[].
+__global__ void __launch_bounds__(BLK) k_seq_pbc(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl,
+                                                 const int *__restrict__ border, const int *__restrict__ blev,
+                                                 const int *__restrict__ wlev, int wall0) {
+  if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<1>(red);
+  const int par = parity(ctl), nh = newhalf(ctl);
+  const bool first = ctl->first;
+  const size_t NF = d.NF;
+  double e[1] = {0.};
+  double *pr = F.f[3] + par * NF;
+  const int w = wall0 + blockIdx.x;
+  for (int L = wlev[w]; L < wlev[w + 1]; ++L) {
+    for (int q = blev[L] + threadIdx.x; q < blev[L + 1]; q += blockDim.x) {
+      const int b = border[q];
+      const BFace B = bface(d, b);
+      const int fw0 = B.cell.face(d, B.pos);
+      const double old = LdCoh::ld(pr, fw0);
+      const double nw = p_bc_value<LdCoh>(d, g, F, P, pr, F.f[0] + nh * NF, F.f[1] + nh * NF, F.f[2] + nh * NF,
+                                            F.f[4] + par * NF, b);
+      pr[fw0] = nw;
+      e[0] = nmax(e[0], errv(nw, old, first));
+    }
+    __syncthreads();
+  }
+  block_max<1>(red, e, ctl->err[par] + 3);
 }
 
 // ====================================================== end of integrate

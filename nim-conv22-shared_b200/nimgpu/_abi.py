@@ -35,6 +35,7 @@ AA_PX, AA_PY, AA_PZ = 44, 45, 46
 M_F4, M_F1, M_F2, M_F3 = 48, 49, 50, 51
 
 CLUSTER_NONE, CLUSTER_POWER, CLUSTER_TANH = 0, 1, 2
+SCHEDULE_PARALLEL, SCHEDULE_REFERENCE = 0, 1
 
 
 class MeshDesc(C.Structure):
@@ -66,7 +67,7 @@ class Params(C.Structure):
         ("R_i", C.c_double), ("R_o", C.c_double),
         ("bc_value", (C.c_double * NIM_NBC) * 5),
         ("max_iters", C.c_int32), ("check_steady", C.c_int32),
-        ("dpdx_tolerance", C.c_int32), ("reserved", C.c_int32),
+        ("dpdx_tolerance", C.c_int32), ("schedule", C.c_int32),
     ]
 
 

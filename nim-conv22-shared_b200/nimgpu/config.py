@@ -53,6 +53,7 @@ def reference_params(**over) -> _abi.Params:
     p.max_iters = 100000
     p.check_steady = 1
     p.dpdx_tolerance = 0
+    p.schedule = _abi.SCHEDULE_PARALLEL
     for k, v in over.items():
         setattr(p, k, v)
     return p

@@ -239,6 +239,9 @@ struct nim_oracle {
   VK<8> MF4, MTF4;
   // parallel-schedule scratch
   V1 snap, pb_new;
+  // Gauss-Seidel visiting orders (1-based cell numbers, BC-list indices):
+  // number order for SEQUENTIAL, the level order for LEVELS
+  std::vector<int64_t> cord, bord;
 
   double err[5] = {0, 0, 0, 0, 0};
   double Dilatation = 0, dudt_max = 0, dTdt_max = 0;
@@ -727,7 +730,7 @@ void velocity_sources(nim_oracle &o) {
   const double gb = o.P.g_beta;
   for (int64_t i = 1; i <= N; ++i) o.bz(i) = -(gb * 0.5 * (o.Txyz(i) + o.Told(i)));
   for (int64_t f = 1; f <= o.NFACE; ++f) o.fbz(f) = -(gb * (o.fT(f)));
-  const bool check_rc = (o.sched == NIM_SCHED_SEQUENTIAL);
+  const bool check_rc = (o.sched != NIM_SCHED_PARALLEL);
   double mrc = o.max_rc;
 #pragma omp parallel for schedule(static) num_threads(o.nthreads) reduction(max : mrc)
   for (int64_t i = 1; i <= N; ++i) {
@@ -937,7 +940,7 @@ void find_error(nim_oracle &o) {
 void iteration(nim_oracle &o) {
   const int64_t N = o.NMESH;
   const int nt = o.nthreads;
-  const bool seq = (o.sched == NIM_SCHED_SEQUENTIAL);
+  const bool seq = (o.sched != NIM_SCHED_PARALLEL);
   V1 *vf[3] = {&o.fu, &o.fv, &o.fw};
   V1 *vc[3] = {&o.uxyz, &o.vxyz, &o.wxyz};
   V1 *vo[3] = {&o.uold, &o.vold, &o.wold};
@@ -951,7 +954,8 @@ void iteration(nim_oracle &o) {
   velocity_sources(o);
   if (seq) {
 #pragma omp parallel for schedule(static) num_threads(nt)
-    for (int64_t i = 1; i <= N; ++i) {
+    for (int64_t q = 0; q < N; ++q) {
+      const int64_t i = o.cord[q];
       for (int k = 0; k < 3; ++k) {
         const double B = (0. + (*RD[k])(i) + (*RB[k])(i));  // R_C = 0
         (*vc[k])(i) = cell_update(o, *vf[k], (*vc[k])(i), (*vo[k])(i), B, o.MF4, i, wv[k]);
@@ -979,10 +983,13 @@ void iteration(nim_oracle &o) {
   // ---- pressure
   pressure_sources(o);
   if (seq) {
-    for (int64_t b = 1; b <= o.NBF; ++b) o.fp(o.F(o.BCpos[b], o.BCm[b])) = pressure_bc_face(o, o.fp, b);
+    for (int64_t q = 0; q < o.NBF; ++q) {
+      const int64_t b = o.bord[q];
+      o.fp(o.F(o.BCpos[b], o.BCm[b])) = pressure_bc_face(o, o.fp, b);
+    }
 #pragma omp parallel for schedule(static) num_threads(nt)
-    for (int64_t n = 1; n <= N; ++n)
-      for (int d = 1; d <= 3; ++d)
+    for (int64_t q = 0; q < N; ++q)
+      for (int d = 1, n = (int)o.cord[q]; d <= 3; ++d)
         if (o.faces_BC[o.F(2 * d, n)] == 1) o.fp(o.F(2 * d, n)) = pressure_face(o, o.fp, d, n);
   } else {
     for (int64_t b = 1; b <= o.NBF; ++b) o.pb_new(b) = pressure_bc_face(o, o.fp, b);
@@ -1000,7 +1007,8 @@ void iteration(nim_oracle &o) {
   for (int64_t i = 1; i <= N; ++i) o.RDT(i) = o.P.alpha * diffusion_source(o, o.fT, i);
   if (seq) {
 #pragma omp parallel for schedule(static) num_threads(nt)
-    for (int64_t i = 1; i <= N; ++i) {
+    for (int64_t q = 0; q < N; ++q) {
+      const int64_t i = o.cord[q];
       o.Txyz(i) = cell_update(o, o.fT, o.Txyz(i), o.Told(i), (o.RDT(i) + 0.), o.MTF4, i, o.P.w_T);
       for (int d = 1; d <= 3; ++d)
         if (o.NB(2 * d, i) != 0) o.fT(o.F(2 * d, i)) = face_update(o, o.fT, o.Txyz, o.Told, *MTF[d - 1], d, i, o.P.w_T);
@@ -1060,6 +1068,45 @@ void fill_integrate_stats(const nim_oracle &o, nim_step_stats *s, int iters) {
   s->dTdt_max = o.dTdt_max;
 }
 
+// The visiting orders of the Gauss-Seidel sweeps.  SEQUENTIAL: cell number
+// and BC-list order, as the reference's loops run.  LEVELS: cells by the level
+// i + 2j + 3k (theta, r, z indices of the structured numbering) and wall faces
+// by i + 2j (bottom, top) or i + 2k (inner, outer), the order the CUDA
+// library's reference-order sweeps follow; inside a level the numbers run
+// downwards and the walls come as top, bottom, outer, inner, so that any
+// dependence between faces or cells the level order treats as independent
+// changes the result.
+void visiting_orders(nim_oracle &o, int NT, int NR, int NZ) {
+  const int64_t N = o.NMESH, NB = o.NBF;
+  o.cord.resize(N);
+  o.bord.resize(NB);
+  for (int64_t q = 0; q < N; ++q) o.cord[q] = q + 1;
+  for (int64_t q = 0; q < NB; ++q) o.bord[q] = q + 1;
+  if (o.sched != NIM_SCHED_LEVELS) return;
+  auto by_level = [](std::vector<std::pair<int64_t, int64_t>> &v) {
+    std::sort(v.begin(), v.end(), [](const auto &a, const auto &b) {
+      return a.first != b.first ? a.first < b.first : a.second > b.second;
+    });
+  };
+  std::vector<std::pair<int64_t, int64_t>> v;
+  for (int64_t c = 0; c < N; ++c) {
+    const int64_t i = c % NT, j = (c / NT) % NR, k = c / ((int64_t)NT * NR);
+    v.push_back({i + 2 * j + 3 * k, c + 1});
+  }
+  by_level(v);
+  for (int64_t q = 0; q < N; ++q) o.cord[q] = v[q].second;
+  const int64_t nb1 = (int64_t)NT * NR, nb3 = (int64_t)NT * NZ;
+  const int64_t w0[4] = {nb1, 0, 2 * nb1 + nb3, 2 * nb1};  // top, bottom, outer, inner
+  const int64_t wn[4] = {nb1, nb1, nb3, nb3};
+  int64_t q = 0;
+  for (int w = 0; w < 4; ++w) {
+    v.clear();
+    for (int64_t r = 0; r < wn[w]; ++r) v.push_back({r % NT + 2 * (r / NT), w0[w] + r + 1});
+    by_level(v);
+    for (const auto &e : v) o.bord[q++] = e.second;
+  }
+}
+
 }  // namespace
 
 // ================================================================ C API
@@ -1117,6 +1164,7 @@ extern "C" int nim_oracle_create(const nim_mesh_desc *m, const nim_params *p, in
   for (V1 *v : {&o->fu, &o->fv, &o->fw, &o->fp, &o->fT, &o->fuo, &o->fvo, &o->fwo, &o->fpo, &o->fTo, &o->fbz})
     v->alloc(NF);
   o->pb_new.alloc(NB);
+  visiting_orders(*o, m->n_theta, m->n_r, m->n_z);
   o->MA.alloc(N); o->MTA.alloc(N);
   o->MF1.alloc(N); o->MF2.alloc(N); o->MF3.alloc(N); o->MTF1.alloc(N); o->MTF2.alloc(N); o->MTF3.alloc(N);
   o->MF4.alloc(N); o->MTF4.alloc(N);

@@ -19,6 +19,10 @@
  *     reads the values from before the sweep (double-buffered faces).  Same
  *     discrete fixed point, different path; used to check kernels step by
  *     step.
+ *   NIM_SCHED_LEVELS     -- SEQUENTIAL's arithmetic with cells visited by
+ *     the level i + 2j + 3k and wall faces by their in-wall level, the order
+ *     of the library's reference-order sweeps.  Equal to SEQUENTIAL bit for
+ *     bit when that order respects every dependence of the sweeps.
  */
 #ifndef NIM_ORACLE_H
 #define NIM_ORACLE_H
@@ -29,7 +33,7 @@
 extern "C" {
 #endif
 
-enum { NIM_SCHED_SEQUENTIAL = 0, NIM_SCHED_PARALLEL = 1 };
+enum { NIM_SCHED_SEQUENTIAL = 0, NIM_SCHED_PARALLEL = 1, NIM_SCHED_LEVELS = 2 };
 
 typedef struct nim_oracle nim_oracle;
 

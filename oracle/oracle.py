@@ -20,6 +20,7 @@ from nimgpu import _abi  # noqa: E402
 
 SEQUENTIAL = 0
 PARALLEL = 1
+LEVELS = 2        # SEQUENTIAL arithmetic, cells and wall faces in level order
 _lib = None
 
 

@@ -72,4 +72,10 @@ def test_argument_errors_without_device(gpu_lib):
     assert gpu_lib.nim_gpu_create(None, None, C.byref(h)) == _abi.NIM_ERR_BAD_ARG
     assert gpu_lib.nim_gpu_init(None) == _abi.NIM_ERR_BAD_ARG
     assert gpu_lib.nim_gpu_step(None, 1, None, None) == _abi.NIM_ERR_BAD_ARG
+    # an unknown schedule is refused before any device call
+    import nimgpu
+    mesh = nimgpu.Mesh(config.small_case().mesh_params())
+    desc = mesh.make_desc()
+    p = config.small_case().params(schedule=7)
+    assert gpu_lib.nim_gpu_create(C.byref(desc), C.byref(p), C.byref(h)) == _abi.NIM_ERR_BAD_ARG
     assert gpu_lib.nim_gpu_strerror(_abi.NIM_ERR_NOT_CONVERGED).decode().startswith("inner iteration")
