@@ -198,7 +198,7 @@ Phys make_phys(const nim_params &p) {
 }
 
 template <typename K>
-int launch_coop(K kern, int blocks, nim_ctx *x) {
+int launch_coop(K kern, int blocks, dim3 block, nim_ctx *x) {
   Dims d = x->d;
   Geo g = x->g;
   Fields F = x->F;
@@ -207,7 +207,7 @@ int launch_coop(K kern, int blocks, nim_ctx *x) {
   const int *order = x->order, *lstart = x->lstart;
   int nlev = x->nlev;
   void *args[] = {&d, &g, &F, &P, &ctl, &order, &lstart, &nlev};
-  CK(cudaLaunchCooperativeKernel((const void *)kern, dim3(blocks), dim3(BLK), args, 0, x->stream));
+  CK(cudaLaunchCooperativeKernel((const void *)kern, dim3(blocks), block, args, 0, x->stream));
   return NIM_OK;
 }
 
@@ -217,15 +217,15 @@ int launch_iteration_seq(nim_ctx *x) {
   const Dims &d = x->d;
   cudaStream_t s = x->stream;
   k_vel_cell<true><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-  TRY(launch_coop(k_seq_vel, x->coop_vel, x));
+  TRY(launch_coop(k_seq_vel, x->coop_vel, dim3(CB, 3), x));
   k_p_src<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_seq_pbc<<<2, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl, x->border, x->blev, x->wlev, 0);
   k_seq_pbc<<<2, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl, x->border, x->blev, x->wlev, 2);
-  TRY(launch_coop(k_seq_p, x->coop_p, x));
+  TRY(launch_coop(k_seq_p, x->coop_p, dim3(BLK), x));
   if (x->phys.dpdx_tolerance) k_p_dpdx<<<x->nblk_c, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
   k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
   k_T_cell<true><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-  TRY(launch_coop(k_seq_T, x->coop_T, x));
+  TRY(launch_coop(k_seq_T, x->coop_T, dim3(BLK), x));
   k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
   CK(cudaGetLastError());
   x->kernels_per_iter = x->phys.dpdx_tolerance ? 11 : 10;
@@ -495,8 +495,8 @@ static int setup_levels(nim_ctx *x) {
   if (!coop) return NIM_ERR_CUDA;
   const int want = std::max(1, (maxlev + BLK - 1) / BLK);
   int per = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_seq_vel, BLK, 0));
-  x->coop_vel = std::max(1, std::min(want, per * sms));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_seq_vel, CB3, 0));
+  x->coop_vel = std::max(1, std::min((maxlev + CB - 1) / CB, per * sms));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_seq_p, BLK, 0));
   x->coop_p = std::max(1, std::min(want, per * sms));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_seq_T, BLK, 0));

@@ -694,18 +694,17 @@ __global__ void __launch_bounds__(BLK) k_vel_coef_F(Dims d, Fields F, Phys P) {
 struct LdPlain {
   __device__ __forceinline__ static double ld(const double *p, size_t i) { return p[i]; }
 };
-// Loads of values the same launch rewrites in place (the reference-order
-// sweeps): a relaxed GPU-scope load, not cached in L1 and ordered against
-// this thread's own stores (volatile asm with a memory clobber), so it sees
-// every store made before the last grid or block barrier and this thread's
-// own earlier stores.
+// Loads and stores of values the same launch rewrites in place (the
+// reference-order sweeps) go through volatile: never the non-coherent
+// read-only path, never merged, and kept in program order against each
+// other, so a thread sees its own earlier stores and every store made before
+// the last grid or block barrier.  Other loads stay free to be scheduled.
 struct LdCoh {
   __device__ __forceinline__ static double ld(const double *p, size_t i) {
-    double r;
-    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(r) : "l"(p + i) : "memory");
-    return r;
+    return *(const volatile double *)(p + i);
   }
 };
+__device__ __forceinline__ void st_coh(double *p, size_t i, double v) { *(volatile double *)(p + i) = v; }
 
 __device__ __forceinline__ int parity(const Ctrl *ctl) { return ctl->iter & ctl->pmask; }
 // half holding the values a sweep earlier in this pass produced
@@ -775,11 +774,12 @@ __device__ __forceinline__ double cell_update(const double *__restrict__ fr, con
                         F4[7] * Ld::ld(fr, f[6]) + B);
 }
 
-// +xi_d face update (nse.f90:878-1005; T: 1033-1088)
+// +xi_d face update (nse.f90:878-1005; T: 1033-1088); cx, cx2 the cell
+// values of x and of its +xi_d neighbour x2
 template <class Ld = LdPlain>
-__device__ __forceinline__ double face_update(const Dims &d, const double *__restrict__ fr, const double *__restrict__ cv,
-                                              const double *__restrict__ co, const double Fd[5], double dg0,
-                                              double dg1, int dd, const Cell &x, const Cell &x2, double w) {
+__device__ __forceinline__ double face_update_cv(const Dims &d, const double *__restrict__ fr, double cx, double cx2,
+                                                 const double *__restrict__ co, const double Fd[5], double dg0,
+                                                 double dg1, int dd, const Cell &x, const Cell &x2, double w) {
   const int e1 = tr1(dd), e2 = tr2(dd);
   const double B3 = (dg0) * (Ld::ld(fr, x.face(d, 2 * e1)) - Ld::ld(fr, x.face(d, 2 * e1 - 1)) +
                              Ld::ld(fr, x2.face(d, 2 * e1)) - Ld::ld(fr, x2.face(d, 2 * e1 - 1))) / 4.0;
@@ -787,7 +787,13 @@ __device__ __forceinline__ double face_update(const Dims &d, const double *__res
                              Ld::ld(fr, x2.face(d, 2 * e2)) - Ld::ld(fr, x2.face(d, 2 * e2 - 1))) / 4.0;
   return (1 - w) * Ld::ld(fr, x.face(d, 2 * dd)) +
          (w / Fd[0]) * (+Fd[1] * Ld::ld(fr, x.face(d, 2 * dd - 1)) + Fd[2] * Ld::ld(fr, x2.face(d, 2 * dd)) +
-                        Fd[3] * (Ld::ld(cv, x.c) + co[x.c]) + Fd[4] * (Ld::ld(cv, x2.c) + co[x2.c]) - B3 - B4);
+                        Fd[3] * (cx + co[x.c]) + Fd[4] * (cx2 + co[x2.c]) - B3 - B4);
+}
+template <class Ld = LdPlain>
+__device__ __forceinline__ double face_update(const Dims &d, const double *__restrict__ fr, const double *__restrict__ cv,
+                                              const double *__restrict__ co, const double Fd[5], double dg0,
+                                              double dg1, int dd, const Cell &x, const Cell &x2, double w) {
+  return face_update_cv<Ld>(d, fr, Ld::ld(cv, x.c), Ld::ld(cv, x2.c), co, Fd, dg0, dg1, dd, x, x2, w);
 }
 
 __device__ __forceinline__ double errv(double nw, double old, bool first) { return fabs(nw - (first ? 0.0 : old)); }
@@ -1284,8 +1290,10 @@ __global__ void k_iter_end(Ctrl *ctl, Phys P) {
 // iterates exactly.  order[] lists the cells level by level, lstart[] the
 // level boundaries.
 
-// velocity sweep (integrate_velocity_field_formulation2_i, nse.f90:831-1006)
-__global__ void __launch_bounds__(BLK) k_seq_vel(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl,
+// velocity sweep (integrate_velocity_field_formulation2_i, nse.f90:831-1006).
+// Block (CB, 3): threadIdx.y = component; the three components of a cell
+// touch disjoint data, so they run side by side.
+__global__ void __launch_bounds__(CB3) k_seq_vel(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl,
                                                  const int *__restrict__ order, const int *__restrict__ lstart,
                                                  int nlev) {
   namespace cg = cooperative_groups;
@@ -1296,9 +1304,12 @@ __global__ void __launch_bounds__(BLK) k_seq_vel(Dims d, Geo g, Fields F, Phys P
   const int par = parity(ctl);
   const bool first = ctl->first;
   const size_t Nc = d.Nc, NF = d.NF;
+  const int v = threadIdx.y;
   double e[3] = {0., 0., 0.};
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-  double *fr[3] = {F.f[0] + par * NF, F.f[1] + par * NF, F.f[2] + par * NF};
+  const int tid = blockIdx.x * CB + threadIdx.x, nth = gridDim.x * CB;
+  double *fr = F.f[v] + par * NF;
+  double *cv = F.c[v];
+  const double *co = F.co[v];
   for (int L = 0; L < nlev; ++L) {
     for (int q = lstart[L] + tid; q < lstart[L + 1]; q += nth) {
       const int c = order[q];
@@ -1307,30 +1318,27 @@ __global__ void __launch_bounds__(BLK) k_seq_vel(Dims d, Geo g, Fields F, Phys P
       cell_faces(d, x, f);
       double F4[8];
       for (int k = 0; k < 8; ++k) F4[k] = F.MF4[(size_t)k * Nc + c];
-      for (int v = 0; v < 3; ++v) {
-        const double cold = LdCoh::ld(F.c[v], c);
-        const double nw = cell_update<LdCoh>(fr[v], f, cold, F.co[v][c], F.Bv[(size_t)v * Nc + c], F4, P.w[v]);
-        F.c[v][c] = nw;
-        e[v] = nmax(e[v], errv(nw, cold, first));
-      }
+      const double cold = LdCoh::ld(cv, c);
+      const double nw = cell_update<LdCoh>(fr, f, cold, co[c], F.Bv[(size_t)v * Nc + c], F4, P.w[v]);
+      st_coh(cv, c, nw);
+      e[v] = nmax(e[v], errv(nw, cold, first));
       for (int dd = 1; dd <= 3; ++dd) {
         if (!x.has_nb(d, 2 * dd)) continue;
         const Cell x2 = x.nb(d, 2 * dd);
         double Fd[5];
         for (int k = 0; k < 5; ++k) Fd[k] = F.MF[(size_t)(5 * (dd - 1) + k) * Nc + c];
-        const double dg0 = g.dg[(2 * (dd - 1)) * Nc + c], dg1 = g.dg[(2 * (dd - 1) + 1) * Nc + c];
         const int fo = x.face(d, 2 * dd);
-        for (int v = 0; v < 3; ++v) {
-          const double old = LdCoh::ld(fr[v], fo);
-          const double nw = face_update<LdCoh>(d, fr[v], F.c[v], F.co[v], Fd, dg0, dg1, dd, x, x2, P.w[v]);
-          fr[v][fo] = nw;
-          e[v] = nmax(e[v], errv(nw, old, first));
-        }
+        const double old = LdCoh::ld(fr, fo);
+        const double nf = face_update_cv<LdCoh>(d, fr, nw, LdCoh::ld(cv, x2.c), co, Fd,
+                                                g.dg[(2 * (dd - 1)) * Nc + c], g.dg[(2 * (dd - 1) + 1) * Nc + c], dd,
+                                                x, x2, P.w[v]);
+        st_coh(fr, fo, nf);
+        e[v] = nmax(e[v], errv(nf, old, first));
       }
     }
     grid.sync();
   }
-  block_max<3>(red, e, ctl->err[par]);
+  block_max<3, CB3>(red, e, ctl->err[par]);
 }
 
 // pressure sweep (integrate_pressure_field_i, nse.f90:1091-1289)
@@ -1356,7 +1364,7 @@ __global__ void __launch_bounds__(BLK) k_seq_p(Dims d, Geo g, Fields F, Phys P, 
         const int fo = x.face(d, 2 * dd);
         const double old = LdCoh::ld(pr, fo);
         const double nw = p_face_value<LdCoh>(d, g, F, P, pr, x, dd);
-        pr[fo] = nw;
+        st_coh(pr, fo, nw);
         e[0] = nmax(e[0], errv(nw, old, first));
       }
     }
@@ -1390,7 +1398,7 @@ __global__ void __launch_bounds__(BLK) k_seq_T(Dims d, Geo g, Fields F, Phys P, 
       for (int k = 0; k < 8; ++k) F4[k] = F.MTF4[(size_t)k * Nc + c];
       const double cold = LdCoh::ld(F.c[3], c);
       const double nw = cell_update<LdCoh>(T, f, cold, F.co[3][c], (F.RDT[c] + 0.), F4, P.w[3]);
-      F.c[3][c] = nw;
+      st_coh(F.c[3], c, nw);
       e[0] = nmax(e[0], errv(nw, cold, first));
       for (int dd = 1; dd <= 3; ++dd) {
         if (!x.has_nb(d, 2 * dd)) continue;
@@ -1399,9 +1407,10 @@ __global__ void __launch_bounds__(BLK) k_seq_T(Dims d, Geo g, Fields F, Phys P, 
         for (int k = 0; k < 5; ++k) Fd[k] = F.MTF[(size_t)(5 * (dd - 1) + k) * Nc + c];
         const int fo = x.face(d, 2 * dd);
         const double old = LdCoh::ld(T, fo);
-        const double nwf = face_update<LdCoh>(d, T, F.c[3], F.co[3], Fd, g.dg[(2 * (dd - 1)) * Nc + c],
-                                             g.dg[(2 * (dd - 1) + 1) * Nc + c], dd, x, x2, P.w[3]);
-        T[fo] = nwf;
+        const double nwf = face_update_cv<LdCoh>(d, T, nw, LdCoh::ld(F.c[3], x2.c), F.co[3], Fd,
+                                                g.dg[(2 * (dd - 1)) * Nc + c], g.dg[(2 * (dd - 1) + 1) * Nc + c], dd,
+                                                x, x2, P.w[3]);
+        st_coh(T, fo, nwf);
         e[0] = nmax(e[0], errv(nwf, old, first));
       }
     }
@@ -1437,7 +1446,7 @@ __global__ void __launch_bounds__(BLK) k_seq_pbc(Dims d, Geo g, Fields F, Phys P
       const double old = LdCoh::ld(pr, fw0);
       const double nw = p_bc_value<LdCoh>(d, g, F, P, pr, F.f[0] + nh * NF, F.f[1] + nh * NF, F.f[2] + nh * NF,
                                             F.f[4] + par * NF, b);
-      pr[fw0] = nw;
+      st_coh(pr, fw0, nw);
       e[0] = nmax(e[0], errv(nw, old, first));
     }
     __syncthreads();
