@@ -224,11 +224,12 @@ int launch_iteration_seq(nim_ctx *x) {
   TRY(launch_coop(k_seq_p, x->coop_p, dim3(BLK), x));
   if (x->phys.dpdx_tolerance) k_p_dpdx<<<x->nblk_c, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
   k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+  k_T_coef<<<dim3(3, x->nblk_c), BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_T_cell<true><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   TRY(launch_coop(k_seq_T, x->coop_T, dim3(BLK), x));
   k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
   CK(cudaGetLastError());
-  x->kernels_per_iter = x->phys.dpdx_tolerance ? 11 : 10;
+  x->kernels_per_iter = x->phys.dpdx_tolerance ? 12 : 11;
   x->launches += x->kernels_per_iter;
   return NIM_OK;
 }
@@ -241,18 +242,19 @@ int launch_iteration(nim_ctx *x) {
   const int gc = x->nblk_c, gb = x->nblk_b;
   const dim3 g3 = x->g3, g8 = x->g8;
   k_vel_cell<false><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-  k_vel_face<<<x->nblk_c3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_p_bc<<<gb, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_p_bc_copy<<<gb, BLK, 0, s>>>(d, x->F, x->ctl);
   k_p_face<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   if (x->phys.dpdx_tolerance) k_p_dpdx<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
   k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
-  k_T_cell<false><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_T_coef<<<dim3(3, x->nblk_c), BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_T_cell<false><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_T_face<<<g8, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
   CK(cudaGetLastError());
-  x->kernels_per_iter = x->phys.dpdx_tolerance ? 11 : 10;
+  x->kernels_per_iter = x->phys.dpdx_tolerance ? 12 : 11;
   x->launches += x->kernels_per_iter;
   return NIM_OK;
 }
@@ -559,6 +561,7 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
   TRY(dalloc(x, &F.MF4, 8 * Nc));
   TRY(dalloc(x, &F.MF, 15 * Nc));
   TRY(dalloc(x, &F.MTF, 15 * Nc));
+  TRY(dalloc(x, &F.MTA, 18 * Nc));
   TRY(dalloc(x, &F.dpd, 3 * Nc));
   TRY(dalloc(x, &F.part, 8 * (size_t)std::max(x->nblk_c, grid(2 * d.NT * d.NZ))));
   TRY(dalloc(x, &x->ctl, 1));
@@ -836,14 +839,15 @@ extern "C" void nim_gpu_destroy(nim_ctx *x) {
 extern "C" void *nim_gpu_stream(nim_ctx *x) { return x ? (void *)x->stream : nullptr; }
 extern "C" int64_t nim_gpu_launch_count(nim_ctx *x) { return x ? x->launches : -1; }
 
-static const char *kKernelNames[] = {"k_vel_cell", "k_vel_face", "k_p_src",    "k_p_bc",  "k_p_bc_copy", "k_p_face",
-                                     "k_p_dpdx",   "k_zero_flux", "k_T_cell", "k_T_face", "k_iter_end"};
+static const char *kKernelNames[] = {"k_vel_cell", "k_vel_face", "k_p_src",  "k_p_bc",   "k_p_bc_copy",
+                                     "k_p_face",   "k_p_dpdx",   "k_zero_flux", "k_T_coef", "k_T_cell",
+                                     "k_T_face",   "k_iter_end"};
 extern "C" const char *nim_gpu_kernel_name(int32_t k) {
   return (k >= 0 && k < (int32_t)(sizeof(kKernelNames) / sizeof(kKernelNames[0]))) ? kKernelNames[k] : "";
 }
 
 extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int32_t cap) {
-  const int NK = 11;
+  const int NK = 12;
   if (!x || n <= 0 || !ms || cap < NK) return NIM_ERR_BAD_ARG;
   if (!x->initialized) return NIM_ERR_STATE;
   if (x->seq) return NIM_ERR_STATE;  // times the parallel-schedule kernels
@@ -862,7 +866,7 @@ extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int
     CK(cudaEventRecord(ev[0], s));
     k_vel_cell<false><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[1], s));
-    k_vel_face<<<x->nblk_c3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[2], s));
     k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[3], s));
@@ -876,20 +880,22 @@ extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int
     CK(cudaEventRecord(ev[7], s));
     k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
     CK(cudaEventRecord(ev[8], s));
-    k_T_cell<false><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_T_coef<<<dim3(3, x->nblk_c), BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[9], s));
-    k_T_face<<<g8, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_T_cell<false><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[10], s));
-    k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
+    k_T_face<<<g8, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[11], s));
+    k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
+    CK(cudaEventRecord(ev[12], s));
     CK(cudaGetLastError());
-    CK(cudaEventSynchronize(ev[11]));
+    CK(cudaEventSynchronize(ev[12]));
     for (int k = 0; k < NK; ++k) {
       float t = 0.f;
       CK(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
       acc[k] += t;
     }
-    x->launches += x->phys.dpdx_tolerance ? 11 : 10;
+    x->launches += x->phys.dpdx_tolerance ? 12 : 11;
   }
   x->phys = keep;
   for (int k = 0; k <= NK; ++k) cudaEventDestroy(ev[k]);

@@ -63,6 +63,7 @@ struct Fields {
   double *MF4;     // [8][Nc]
   double *MF;      // [15][Nc]  M_F1..3(k) at 5(d-1)+k-1
   double *MTF;     // [15][Nc]  MT_F1..3
+  double *MTA;     // [18][Nc]  MT_A(q, d) at 3(q-1) + d-1
   double *dpd;     // [3][Nc]   dpdx_old, dpdy_old, dpdz_old
   // reference-order schedule: sources stored before the ordered sweeps
   double *Bv;      // [3][Nc]   R_C + R_D + R_B of u, v, w
@@ -710,6 +711,20 @@ __device__ __forceinline__ int parity(const Ctrl *ctl) { return ctl->iter & ctl-
 // half holding the values a sweep earlier in this pass produced
 __device__ __forceinline__ int newhalf(const Ctrl *ctl) { return ctl->pmask ? 1 - parity(ctl) : parity(ctl); }
 
+// fn(IC<y + 1>{}) for a warp-uniform y in 0..2: the direction (or component)
+// becomes a compile-time constant, so every face/neighbour selection on it
+// folds away instead of running as integer code per thread
+template <int V>
+struct IC {
+  static constexpr int value = V;
+};
+template <class Fn>
+__device__ __forceinline__ void by_dir(int y, Fn &&fn) {
+  if (y == 0) fn(IC<1>{});
+  else if (y == 1) fn(IC<2>{});
+  else fn(IC<3>{});
+}
+
 // Green-Gauss derivative dphi_dx2/dy2/dz2 (nse.f90:2866-2903), component cc
 __device__ __forceinline__ double green_gauss(const Geo &g, size_t NF, double invV, const double phi[7],
                                               const int f[7], int cc) {
@@ -866,25 +881,28 @@ __global__ void __launch_bounds__(CB3, 2) k_vel_face(Dims d, Geo g, Fields F, Ph
   red_init<3>(red);
   const int par = parity(ctl);
   const bool first = ctl->first;
-  const int dd = threadIdx.y + 1;
-  const int c = blockIdx.x * CB + threadIdx.x;
+  Cell x;
+  const bool act = patch_cell(d, x);
+  const int c = x.c;
   double e[3] = {0., 0., 0.};
-  if (c < d.Nc) {
-    const Cell x = Cell::of(d, c);
+  if (act) {
     const size_t Nc = d.Nc, NF = d.NF;
-    if (x.has_nb(d, 2 * dd)) {
+    by_dir(threadIdx.y, [&](auto D) {
+      constexpr int dd = decltype(D)::value;
+      if (!x.has_nb(d, 2 * dd)) return;
       const Cell x2 = x.nb(d, 2 * dd);
       double Fd[5];
       for (int k = 0; k < 5; ++k) Fd[k] = F.MF[(size_t)(5 * (dd - 1) + k) * Nc + c];
       const double dg0 = g.dg[(2 * (dd - 1)) * Nc + c], dg1 = g.dg[(2 * (dd - 1) + 1) * Nc + c];
       const int fo = x.face(d, 2 * dd);
+#pragma unroll
       for (int q = 0; q < 3; ++q) {
         const double *fr = F.f[q] + par * NF;
         const double nw = face_update(d, fr, F.c[q], F.co[q], Fd, dg0, dg1, dd, x, x2, P.w[q]);
         F.f[q][(1 - par) * NF + fo] = nw;
         e[q] = errv(nw, fr[fo], first);
       }
-    }
+    });
   }
   block_max<3, CB3>(red, e, ctl->err[par]);
 }
@@ -908,23 +926,27 @@ __global__ void __launch_bounds__(CB3, 3) k_p_src(Dims d, Geo g, Fields F, Phys 
   const double *fp = F.f[3] + par * NF;
   if (active) {
     cell_faces(d, x, f);
-    const double invV = 1. / g.vol[c];
-    const double *fq = F.f[q] + newhalf(ctl) * NF;
-    double vf[7];
-    for (int k = 1; k <= 6; ++k) vf[k] = fq[f[k]];
-    for (int cc = 0; cc < 3; ++cc) sh[q][cc][tx] = green_gauss(g, NF, invV, vf, f, cc);
-    if (q == 1) {
-      const double *fT = F.f[4] + par * NF;
-      double bzf[7];
-      for (int k = 1; k <= 6; ++k) bzf[k] = -(P.g_beta * (fT[f[k]]));
-      sbz[tx] = green_gauss(g, NF, invV, bzf, f, 2);
-    }
-    // y=0 pxy,pzy  y=1 pyx,pzx  y=2 pxz,pyz (calculate_R_D_p2 order)
-    const int e2 = (q == 0) ? 2 : (q == 1) ? 1 : 3;
-    const int fa = (q == 1) ? 4 : 2, fb = (q == 1) ? 3 : 1;
-    sX[q][0][tx] = 0.5 * (tangential(d, fp, x, fa, e2) - tangential(d, fp, x, fb, e2));
-    sX[q][1][tx] = (q == 2) ? 0.5 * (tangential(d, fp, x, 4, 3) - tangential(d, fp, x, 3, 3))
-                            : 0.5 * (tangential(d, fp, x, 6, e2) - tangential(d, fp, x, 5, e2));
+    by_dir(threadIdx.y, [&](auto Q) {
+      constexpr int q = decltype(Q)::value - 1;
+      const double invV = 1. / g.vol[c];
+      const double *fq = F.f[q] + newhalf(ctl) * NF;
+      double vf[7];
+      for (int k = 1; k <= 6; ++k) vf[k] = fq[f[k]];
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) sh[q][cc][tx] = green_gauss(g, NF, invV, vf, f, cc);
+      if (q == 1) {
+        const double *fT = F.f[4] + par * NF;
+        double bzf[7];
+        for (int k = 1; k <= 6; ++k) bzf[k] = -(P.g_beta * (fT[f[k]]));
+        sbz[tx] = green_gauss(g, NF, invV, bzf, f, 2);
+      }
+      // y=0 pxy,pzy  y=1 pyx,pzx  y=2 pxz,pyz (calculate_R_D_p2 order)
+      constexpr int e2 = (q == 0) ? 2 : (q == 1) ? 1 : 3;
+      constexpr int fa = (q == 1) ? 4 : 2, fb = (q == 1) ? 3 : 1;
+      sX[q][0][tx] = 0.5 * (tangential(d, fp, x, fa, e2) - tangential(d, fp, x, fb, e2));
+      sX[q][1][tx] = (q == 2) ? 0.5 * (tangential(d, fp, x, 4, 3) - tangential(d, fp, x, 3, 3))
+                              : 0.5 * (tangential(d, fp, x, 6, e2) - tangential(d, fp, x, 5, e2));
+    });
   }
   __syncthreads();
   if (active && q == 0) {
@@ -1023,11 +1045,21 @@ __global__ void k_p_bc_copy(Dims d, Fields F, Ctrl *ctl) {
 }
 
 // (coefficient, face, cell) of the ten off-diagonal terms of the pressure
-// face update for the +r, +theta, +z face, in source order (nse.f90:1150-1285)
-__constant__ unsigned char kPTerms[3][10][3] = {
-    {{1, 1, 1}, {3, 2, 2}, {4, 3, 1}, {5, 4, 1}, {6, 3, 2}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
-    {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
-    {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {6, 4, 1}, {7, 3, 2}, {8, 4, 2}, {9, 5, 1}, {11, 6, 2}}};
+// face update for the +r, +theta, +z face (dd = 1, 2, 3), in source order
+// (nse.f90:1150-1285), packed as coefficient | face << 4 | cell << 7.  A
+// constexpr switch: with dd and t known at compile time it folds to
+// constants.
+__host__ __device__ constexpr int p_term(int dd, int t) {
+  switch (10 * dd + t) {
+    case 10: return 1 | 1 << 4 | 1 << 7; case 11: return 3 | 2 << 4 | 2 << 7; case 12: return 4 | 3 << 4 | 1 << 7; case 13: return 5 | 4 << 4 | 1 << 7; case 14: return 6 | 3 << 4 | 2 << 7;
+    case 15: return 7 | 4 << 4 | 2 << 7; case 16: return 8 | 5 << 4 | 1 << 7; case 17: return 9 | 6 << 4 | 1 << 7; case 18: return 10 | 5 << 4 | 2 << 7; case 19: return 11 | 6 << 4 | 2 << 7;
+    case 20: return 1 | 1 << 4 | 1 << 7; case 21: return 2 | 2 << 4 | 1 << 7; case 22: return 3 | 1 << 4 | 2 << 7; case 23: return 4 | 2 << 4 | 2 << 7; case 24: return 5 | 3 << 4 | 1 << 7;
+    case 25: return 7 | 4 << 4 | 2 << 7; case 26: return 8 | 5 << 4 | 1 << 7; case 27: return 9 | 6 << 4 | 1 << 7; case 28: return 10 | 5 << 4 | 2 << 7; case 29: return 11 | 6 << 4 | 2 << 7;
+    case 30: return 1 | 1 << 4 | 1 << 7; case 31: return 2 | 2 << 4 | 1 << 7; case 32: return 3 | 1 << 4 | 2 << 7; case 33: return 4 | 2 << 4 | 2 << 7; case 34: return 5 | 3 << 4 | 1 << 7;
+    case 35: return 6 | 4 << 4 | 1 << 7; case 36: return 7 | 3 << 4 | 2 << 7; case 37: return 8 | 4 << 4 | 2 << 7; case 38: return 9 | 5 << 4 | 1 << 7; case 39: return 11 | 6 << 4 | 2 << 7;
+    default: return 0;
+  }
+}
 
 // ---- integrate_pressure_field_i for the +xi_dd face of cell x
 // (nse.f90:1091-1289): the new value from the pressures pr
@@ -1036,7 +1068,6 @@ __device__ __forceinline__ double p_face_value(const Dims &d, const Geo &g, cons
                                                const double *pr, const Cell &x, int dd) {
   const size_t Nc = d.Nc;
   const int c = x.c;
-  const unsigned char(*tab)[10][3] = kPTerms;
   const int diag = (dd == 1) ? 2 : (dd == 2) ? 6 : 10;
   const Cell n2 = x.nb(d, 2 * dd);
   const double *A = g.AA + (size_t)15 * (dd - 1) * Nc;
@@ -1047,8 +1078,9 @@ __device__ __forceinline__ double p_face_value(const Dims &d, const Geo &g, cons
   double s = 0.0;
 #pragma unroll
   for (int t = 0; t < 10; ++t) {
-    const Cell &cl = (tab[dd - 1][t][2] == 1) ? x : n2;
-    const double term = A[(size_t)(tab[dd - 1][t][0] - 1) * Nc + c] * Ld::ld(pr, cl.face(d, tab[dd - 1][t][1]));
+    const int pt = p_term(dd, t), coef = pt & 15, fpos = (pt >> 4) & 7, cell = pt >> 7;
+    const Cell &cl = (cell == 1) ? x : n2;
+    const double term = A[(size_t)(coef - 1) * Nc + c] * Ld::ld(pr, cl.face(d, fpos));
     s = (t == 0) ? -term : s - term;
   }
   const int fo = x.face(d, 2 * dd);
@@ -1064,17 +1096,20 @@ __global__ void __launch_bounds__(CB3, 3) k_p_face(Dims d, Geo g, Fields F, Phys
   red_init<1>(red);
   const int par = parity(ctl);
   const bool first = ctl->first;
-  const int dd = threadIdx.y + 1;
   Cell x;
   const bool act = patch_cell(d, x);
   double e[1] = {0.};
-  if (act && x.has_nb(d, 2 * dd)) {
-    const size_t NF = d.NF;
-    const double *pr = F.f[3] + par * NF;
-    const double nw = p_face_value<LdPlain>(d, g, F, P, pr, x, dd);
-    const int fo = x.face(d, 2 * dd);
-    F.f[3][(1 - par) * NF + fo] = nw;
-    e[0] = errv(nw, pr[fo], first);
+  if (act) {
+    by_dir(threadIdx.y, [&](auto D) {
+      constexpr int dd = decltype(D)::value;
+      if (!x.has_nb(d, 2 * dd)) return;
+      const size_t NF = d.NF;
+      const double *pr = F.f[3] + par * NF;
+      const double nw = p_face_value<LdPlain>(d, g, F, P, pr, x, dd);
+      const int fo = x.face(d, 2 * dd);
+      F.f[3][(1 - par) * NF + fo] = nw;
+      e[0] = errv(nw, pr[fo], first);
+    });
   }
   block_max<1, CB3>(red, e, ctl->err[par] + 3);
 }
@@ -1127,62 +1162,81 @@ __global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, Geo g, Fields F, Ctrl
   block_max<1>(red, e, ctl->err[par] + 4);
 }
 
-// ---- K7: calculate_temperature_nim_constants_formulation2 (nim.f90:334-502),
-// calculate_R_D_T (nse.f90:2000-2134) and the cell update of T (1017-1026).
-// Block (CB, 3): thread y forms MT_A of direction y+1 for the cell and its
-// +neighbour (MT_F of that face) and two of the six cross derivatives;
-// thread 0 assembles MT_F4, R_D_T and the update in the reference's order.
+// ---- K7a: calculate_temperature_nim_constants_formulation2, first part
+// (nim.f90:334-464): MT_A(1:6) of every cell and direction, from the cell
+// velocities of this pass.  One thread per (direction, cell) and no
+// barriers: the divisions of the NIM series make this the one
+// instruction-bound piece of the pass, and every warp can issue.
+// Grid (3, ceil(Nc/BLK)): blockIdx.x is the direction, so the three
+// directions of the same cells run side by side and share their loads.
+__global__ void __launch_bounds__(BLK, 3) k_T_coef(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+  if (ctl->done) return;
+  const int c = blockIdx.y * BLK + threadIdx.x;
+  if (c >= d.Nc) return;
+  const int dd = blockIdx.x + 1;
+  const size_t Nc = d.Nc;
+  const double ut = 0.5 * (F.c[0][c] + F.co[0][c]);
+  const double vt = 0.5 * (F.c[1][c] + F.co[1][c]);
+  const double wt = 0.5 * (F.c[2][c] + F.co[2][c]);
+  const double u = contravariant(g.xi, Nc, c, dd, ut, vt, wt);
+  double A[6];
+  nim_direction(u, g.gij[(size_t)(dd - 1 + 3 * (dd - 1)) * Nc + c] * P.alpha, g.gfd[(2 * (dd - 1)) * Nc + c],
+                g.gfd[(2 * (dd - 1) + 1) * Nc + c], P.v_limit, A);
+  for (int q = 0; q < 6; ++q) F.MTA[(size_t)(3 * q + dd - 1) * Nc + c] = A[q];
+}
+
+// ---- K7b: the rest of calculate_temperature_nim_constants_formulation2
+// (MT_F4, MT_F1..3, nim.f90:466-500), calculate_R_D_T (nse.f90:2000-2134)
+// and the cell update of T (1017-1026).  Block (CB, 3): thread y forms MT_F
+// of direction y+1 from MT_A of the cell and of its +neighbour, and two of
+// the six cross derivatives; thread 0 assembles MT_F4, R_D_T and the update
+// in the reference's order.
 // SRC_ONLY (reference-order schedule): store MT_F4 and R_D_T and leave the
 // update to k_seq_T.
 template <bool SRC_ONLY>
-__global__ void __launch_bounds__(CB3, 2) k_T_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+__global__ void __launch_bounds__(CB3, 3) k_T_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
-  __shared__ double sA[3][2][CB];   // MT_A(d,5), MT_A(d,6)
   __shared__ double sX[3][2][CB];   // cross derivatives
   const int par = parity(ctl);
   const bool first = ctl->first;
-  const int y = threadIdx.y, tx = threadIdx.x, dd = y + 1;
+  const int tx = threadIdx.x;
   Cell x;
   const bool active = patch_cell(d, x);
   const int c = x.c;
   double e[1] = {0.};
   const size_t Nc = d.Nc, NF = d.NF;
   const double *T = F.f[4] + par * NF;
-  if (active) {
-    auto coefA = [&](int cell, double A[6]) {
-      const double ut = 0.5 * (F.c[0][cell] + F.co[0][cell]);
-      const double vt = 0.5 * (F.c[1][cell] + F.co[1][cell]);
-      const double wt = 0.5 * (F.c[2][cell] + F.co[2][cell]);
-      const double u = contravariant(g.xi, Nc, cell, dd, ut, vt, wt);
-      nim_direction(u, g.gij[(size_t)(dd - 1 + 3 * (dd - 1)) * Nc + cell] * P.alpha,
-                    g.gfd[(2 * (dd - 1)) * Nc + cell], g.gfd[(2 * (dd - 1) + 1) * Nc + cell], P.v_limit, A);
-    };
-    double A[6];
-    coefA(c, A);
-    sA[y][0][tx] = A[4];
-    sA[y][1][tx] = A[5];
+  if (active) by_dir(threadIdx.y, [&](auto D) {
+    constexpr int dd = decltype(D)::value, y = dd - 1;
+    const double *MA = F.MTA + (size_t)y * Nc;  // MT_A(q, dd) at MA[3q Nc]
     double G[5] = {0., 0., 0., 0., 0.};
     if (x.has_nb(d, 2 * dd)) {
-      double A2[6];
-      coefA(x.nb(d, 2 * dd).c, A2);
+      const int c2 = x.nb(d, 2 * dd).c;
+      double A[6], A2[6];
+      for (int q = 0; q < 6; ++q) A[q] = MA[3 * q * Nc + c];
+      A2[0] = A2[2] = 0.;  // not used by form_Fd
+      A2[1] = MA[3 * Nc + c2];
+      A2[3] = MA[9 * Nc + c2];
+      A2[4] = MA[12 * Nc + c2];
+      A2[5] = MA[15 * Nc + c2];
       form_Fd(A, A2, G);
     }
     for (int k = 0; k < 5; ++k) F.MTF[(size_t)(5 * (dd - 1) + k) * Nc + c] = G[k];
     // cross derivatives of calculate_R_D_T: y=0 pxy,pzy  y=1 pyx,pzx  y=2 pxz,pyz
-    const int e2 = (y == 0) ? 2 : (y == 1) ? 1 : 3;
-    const int fa = (y == 1) ? 4 : 2, fb = (y == 1) ? 3 : 1;
+    constexpr int e2 = (y == 0) ? 2 : (y == 1) ? 1 : 3;
+    constexpr int fa = (y == 1) ? 4 : 2, fb = (y == 1) ? 3 : 1;
     sX[y][0][tx] = 0.5 * (tangential(d, T, x, (y == 2) ? 2 : fa, e2) - tangential(d, T, x, (y == 2) ? 1 : fb, e2));
     sX[y][1][tx] = (y == 2) ? 0.5 * (tangential(d, T, x, 4, 3) - tangential(d, T, x, 3, 3))
                             : 0.5 * (tangential(d, T, x, 6, e2) - tangential(d, T, x, 5, e2));
-  }
+  });
   __syncthreads();
-  if (active && y == 0) {
+  if (active && threadIdx.y == 0) {
     double Am[3][6];
     for (int k = 0; k < 3; ++k) {
-      Am[k][4] = sA[k][0][tx];
-      Am[k][5] = sA[k][1][tx];
+      Am[k][4] = F.MTA[(size_t)(12 + k) * Nc + c];
+      Am[k][5] = F.MTA[(size_t)(15 + k) * Nc + c];
     }
     double F4[8];
     form_F4(Am, P.DT, F4);
@@ -1322,6 +1376,7 @@ __global__ void __launch_bounds__(CB3) k_seq_vel(Dims d, Geo g, Fields F, Phys P
       const double nw = cell_update<LdCoh>(fr, f, cold, co[c], F.Bv[(size_t)v * Nc + c], F4, P.w[v]);
       st_coh(cv, c, nw);
       e[v] = nmax(e[v], errv(nw, cold, first));
+#pragma unroll
       for (int dd = 1; dd <= 3; ++dd) {
         if (!x.has_nb(d, 2 * dd)) continue;
         const Cell x2 = x.nb(d, 2 * dd);
@@ -1359,6 +1414,7 @@ __global__ void __launch_bounds__(BLK) k_seq_p(Dims d, Geo g, Fields F, Phys P, 
   for (int L = 0; L < nlev; ++L) {
     for (int q = lstart[L] + tid; q < lstart[L + 1]; q += nth) {
       const Cell x = Cell::of(d, order[q]);
+#pragma unroll
       for (int dd = 1; dd <= 3; ++dd) {
         if (!x.has_nb(d, 2 * dd)) continue;
         const int fo = x.face(d, 2 * dd);
@@ -1400,6 +1456,7 @@ __global__ void __launch_bounds__(BLK) k_seq_T(Dims d, Geo g, Fields F, Phys P, 
       const double nw = cell_update<LdCoh>(T, f, cold, F.co[3][c], (F.RDT[c] + 0.), F4, P.w[3]);
       st_coh(F.c[3], c, nw);
       e[0] = nmax(e[0], errv(nw, cold, first));
+#pragma unroll
       for (int dd = 1; dd <= 3; ++dd) {
         if (!x.has_nb(d, 2 * dd)) continue;
         const Cell x2 = x.nb(d, 2 * dd);
