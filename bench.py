@@ -46,7 +46,8 @@ KERNEL_BYTES_PER_CELL = {
     "k_vel_face": 8 * 45,   # faces u,v,w (9) cells+old (6) M_F1..3 (15) dg (6); write faces (9)
     "k_p_src": 8 * 39,      # faces u,v,w,T,p (15) area,normal,vol (13) G,g^ij (9); write dila,Rp (2)
     "k_p_face": 8 * 52,     # faces p (3) Rp (1) AA used (39) dg (6); write faces p (3)
-    "k_T_cell": 8 * 54,     # cells+old u,v,w (6) xi (9) g^ij (9) gfd (6) faces T (3) G (3) T,T_old (2); write T, MT_F (16)
+    "k_T_coef": 8 * 42,     # cells+old u,v,w (6) xi (9) g^ij diagonal (3) gfd (6); write MT_A (18)
+    "k_T_cell": 8 * 48,     # MT_A (18) faces T (3) G (3) g^ij (6) T,T_old (2); write T, MT_F (16)
     "k_T_face": 8 * 29,     # faces T (3) T,T_old (2) MT_F (15) dg (6); write faces T (3)
 }
 # per cell-iteration and per step, the survey's algorithmic model (FP64)

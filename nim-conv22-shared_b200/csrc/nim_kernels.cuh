@@ -1199,6 +1199,8 @@ __global__ void __launch_bounds__(CB3, 3) k_T_cell(Dims d, Geo g, Fields F, Phys
   __shared__ BlockRed red;
   red_init<1>(red);
   __shared__ double sX[3][2][CB];   // cross derivatives
+  __shared__ double sF4[8][CB];     // MT_F4, formed by thread 1
+  __shared__ double sG[CB];         // G1 dT/dx + G2 dT/dy + G3 dT/dz, by thread 2
   const int par = parity(ctl);
   const bool first = ctl->first;
   const int tx = threadIdx.x;
@@ -1208,6 +1210,8 @@ __global__ void __launch_bounds__(CB3, 3) k_T_cell(Dims d, Geo g, Fields F, Phys
   double e[1] = {0.};
   const size_t Nc = d.Nc, NF = d.NF;
   const double *T = F.f[4] + par * NF;
+  int f[7];
+  cell_faces(d, x, f);
   if (active) by_dir(threadIdx.y, [&](auto D) {
     constexpr int dd = decltype(D)::value, y = dd - 1;
     const double *MA = F.MTA + (size_t)y * Nc;  // MT_A(q, dd) at MA[3q Nc]
@@ -1230,27 +1234,31 @@ __global__ void __launch_bounds__(CB3, 3) k_T_cell(Dims d, Geo g, Fields F, Phys
     sX[y][0][tx] = 0.5 * (tangential(d, T, x, (y == 2) ? 2 : fa, e2) - tangential(d, T, x, (y == 2) ? 1 : fb, e2));
     sX[y][1][tx] = (y == 2) ? 0.5 * (tangential(d, T, x, 4, 3) - tangential(d, T, x, 3, 3))
                             : 0.5 * (tangential(d, T, x, 6, e2) - tangential(d, T, x, 5, e2));
+    if (y == 1) {  // MT_F4 (nim.f90:466-475)
+      double Am[3][6];
+      for (int k = 0; k < 3; ++k) {
+        Am[k][4] = F.MTA[(size_t)(12 + k) * Nc + c];
+        Am[k][5] = F.MTA[(size_t)(15 + k) * Nc + c];
+      }
+      double F4[8];
+      form_F4(Am, P.DT, F4);
+      for (int k = 0; k < 8; ++k) sF4[k][tx] = F4[k];
+    } else if (y == 2) {  // the leading G_i d_i T terms of R_D_T, in source order
+      const double px = (T[f[2]] - T[f[1]]) / 2.;
+      const double py = (T[f[4]] - T[f[3]]) / 2.;
+      const double pz = (T[f[6]] - T[f[5]]) / 2.;
+      sG[tx] = g.G[c] * px + g.G[Nc + c] * py + g.G[2 * Nc + c] * pz;
+    }
   });
   __syncthreads();
   if (active && threadIdx.y == 0) {
-    double Am[3][6];
-    for (int k = 0; k < 3; ++k) {
-      Am[k][4] = F.MTA[(size_t)(12 + k) * Nc + c];
-      Am[k][5] = F.MTA[(size_t)(15 + k) * Nc + c];
-    }
     double F4[8];
-    form_F4(Am, P.DT, F4);
-    int f[7];
-    cell_faces(d, x, f);
+    for (int k = 0; k < 8; ++k) F4[k] = sF4[k][tx];
     const double pxy = sX[0][0][tx], pzy = sX[0][1][tx], pyx = sX[1][0][tx], pzx = sX[1][1][tx];
     const double pxz = sX[2][0][tx], pyz = sX[2][1][tx];
-    const double px = (T[f[2]] - T[f[1]]) / 2.;
-    const double py = (T[f[4]] - T[f[3]]) / 2.;
-    const double pz = (T[f[6]] - T[f[5]]) / 2.;
-    const double *Gv = g.G, *gij = g.gij;
-    const double RDT = P.alpha * (Gv[c] * px + Gv[Nc + c] * py + Gv[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy -
-                                  gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz - gij[2 * Nc + c] * pzx -
-                                  gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
+    const double *gij = g.gij;
+    const double RDT = P.alpha * (sG[tx] - gij[3 * Nc + c] * pxy - gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz -
+                                  gij[2 * Nc + c] * pzx - gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
     if (SRC_ONLY) {
       for (int k = 0; k < 8; ++k) F.MTF4[(size_t)k * Nc + c] = F4[k];
       F.RDT[c] = RDT;
