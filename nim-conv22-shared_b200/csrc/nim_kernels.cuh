@@ -875,7 +875,7 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, Geo g, Fields F, Ph
 
 // ---- K2: +xi face updates of u, v, w (nse.f90:878-1005).
 // Block (CB, 3): threadIdx.y = direction.
-__global__ void __launch_bounds__(CB3, 2) k_vel_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+__global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<3>(red);
@@ -911,7 +911,7 @@ __global__ void __launch_bounds__(CB3, 2) k_vel_face(Dims d, Geo g, Fields F, Ph
 // calculate_R_D_p2 1863-1997).  Block (CB, 3): thread y forms the gradient of
 // velocity component y and two of the six cross derivatives of p (y = 1 also
 // d(bz)/dz); thread 0 combines them in the reference's order.
-__global__ void __launch_bounds__(CB3, 3) k_p_src(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+__global__ void __launch_bounds__(CB3, 4) k_p_src(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ double sh[3][3][CB];  // gradients of u, v, w
   __shared__ double sX[3][2][CB];  // cross derivatives of p
@@ -1090,7 +1090,7 @@ __device__ __forceinline__ double p_face_value(const Dims &d, const Geo &g, cons
 
 // ---- K5: integrate_pressure_field_i, cur -> next.
 // Block (CB, 3): threadIdx.y = direction.
-__global__ void __launch_bounds__(CB3, 3) k_p_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+__global__ void __launch_bounds__(CB3, 5) k_p_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
@@ -1169,7 +1169,7 @@ __global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, Geo g, Fields F, Ctrl
 // instruction-bound piece of the pass, and every warp can issue.
 // Grid (3, ceil(Nc/BLK)): blockIdx.x is the direction, so the three
 // directions of the same cells run side by side and share their loads.
-__global__ void __launch_bounds__(BLK, 3) k_T_coef(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+__global__ void __launch_bounds__(BLK, 4) k_T_coef(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   const int c = blockIdx.y * BLK + threadIdx.x;
   if (c >= d.Nc) return;
@@ -1194,7 +1194,7 @@ __global__ void __launch_bounds__(BLK, 3) k_T_coef(Dims d, Geo g, Fields F, Phys
 // SRC_ONLY (reference-order schedule): store MT_F4 and R_D_T and leave the
 // update to k_seq_T.
 template <bool SRC_ONLY>
-__global__ void __launch_bounds__(CB3, 3) k_T_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+__global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
