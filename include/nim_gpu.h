@@ -68,6 +68,7 @@ typedef enum nim_field {
   NIM_FIELD_MESHES_TT = 16,  /* meshes_Txyzt            */
   NIM_FIELD_MESHES_P = 17,   /* meshes_p (face mean, nse.f90:1307)        */
   NIM_FIELD_MESHES_DILA = 18,/* meshes_dila (evaluate_D, nse.f90:2530)    */
+  NIM_FIELD_MESHES_DILA_OLD = 19, /* meshes_dila_old (write_restart, restart.f90:37) */
   /* init-time geometry (read-only; download only) */
   NIM_FIELD_MESHES_VOLUME = 32,  /* meshes_volume(NMESH)                  */
   NIM_FIELD_FACES_AREA = 33,     /* faces_area(NFACE)                     */
@@ -210,6 +211,30 @@ int nim_gpu_step(nim_ctx *ctx, int32_t nsteps, nim_step_stats *per_step,
    n = number of doubles the host buffer holds. */
 int nim_gpu_download(nim_ctx *ctx, nim_field field, double *host, int64_t n);
 int nim_gpu_upload(nim_ctx *ctx, nim_field field, const double *host, int64_t n);
+
+/* Output sets packed on the device, copied to the host while the time loop
+   goes on.  They replace the host-side array walks of write_data and
+   write_restart; the files themselves (Silo, Fortran unformatted) stay with
+   the host.
+   NIM_OUTPUT_PLOT    write_data's zone variables (postprocess.f90:92-103):
+                      REAL(.,4) of meshes_uxyzt, meshes_vxyzt, meshes_wxyzt,
+                      meshes_p, meshes_Txyzt, meshes_dila, 6 x NMESH floats.
+   NIM_OUTPUT_RESTART write_restart's arrays after TI and STEP
+                      (restart.f90:24-37): faces_u, faces_v, faces_w,
+                      faces_p, faces_T (5 x NFACE), meshes_uxyz, vxyz, wxyz,
+                      Txyz, meshes_uxyz_old .. Txyz_old, meshes_dila_old
+                      (9 x NMESH), doubles.
+   nim_gpu_output_begin packs the set as it stands after the work already
+   queued and starts the copy into host (bytes >= nim_gpu_output_bytes; use
+   page-locked memory for the copy to overlap) on a copy stream of its own;
+   later calls may advance the state at once.  The packed snapshot is not
+   touched by them.  *ticket names the copy for nim_gpu_output_wait, which
+   returns once host holds it.  Beginning a set again while its previous
+   copy is still running orders the new packing after that copy. */
+typedef enum nim_output_set { NIM_OUTPUT_PLOT = 0, NIM_OUTPUT_RESTART = 1 } nim_output_set;
+int64_t nim_gpu_output_bytes(nim_ctx *ctx, int32_t set);
+int nim_gpu_output_begin(nim_ctx *ctx, int32_t set, void *host, int64_t bytes, int32_t *ticket);
+int nim_gpu_output_wait(nim_ctx *ctx, int32_t ticket);
 
 /* Diagnostics and timing hooks (no counterpart in the reference).
    nim_gpu_stream: the cudaStream_t every call of the context queues work on,

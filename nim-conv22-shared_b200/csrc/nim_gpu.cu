@@ -82,6 +82,13 @@ struct nim_ctx {
   int nlev = 0;
   int *border = nullptr, *blev = nullptr, *wlev = nullptr;  // wall faces, levels, per-wall level ranges
   int coop_vel = 0, coop_p = 0, coop_T = 0;  // cooperative grid sizes
+  // output sets (nim_gpu_output_begin): device staging, copy stream, events
+  cudaStream_t copy_stream = nullptr;
+  struct Output {
+    void *stage = nullptr;
+    cudaEvent_t packed = nullptr, copied = nullptr;
+    int gen = 0;
+  } out[2];
 };
 
 namespace {
@@ -328,6 +335,38 @@ __global__ void k_scatter(const double *__restrict__ src, const int *__restrict_
   if (dst1) dst1[s] = src[i];
 }
 
+// write_data's zone variables as REAL(.,4) (postprocess.f90:92-103)
+__global__ void k_pack_plot(Dims d, Fields F, float *__restrict__ dst) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.Nc) return;
+  const size_t Nc = d.Nc;
+  dst[c] = (float)F.ct[0][c];
+  dst[Nc + c] = (float)F.ct[1][c];
+  dst[2 * Nc + c] = (float)F.ct[2][c];
+  dst[3 * Nc + c] = (float)F.mp[c];
+  dst[4 * Nc + c] = (float)F.ct[3][c];
+  dst[5 * Nc + c] = (float)F.dila[c];
+}
+
+// write_restart's arrays (restart.f90:24-37): five face fields of the
+// current half in reference face order, then nine cell fields
+__global__ void k_pack_restart(Dims d, Fields F, const int *__restrict__ perm, const Ctrl *ctl,
+                               double *__restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t NF = d.NF, Nc = d.Nc;
+  const int par = ctl->iter & ctl->pmask;
+  if (i < d.NF) {
+    const int s = perm[i];
+    for (int q = 0; q < 5; ++q) dst[q * NF + i] = F.f[q][par * NF + s];
+  }
+  if (i < d.Nc) {
+    double *o = dst + 5 * NF;
+    for (int q = 0; q < 4; ++q) o[q * Nc + i] = F.c[q][i];
+    for (int q = 0; q < 4; ++q) o[(4 + q) * Nc + i] = F.co[q][i];
+    o[8 * Nc + i] = F.dila_old[i];
+  }
+}
+
 struct FieldView {
   const double *src = nullptr;
   double *dst1 = nullptr;  // second half (face fields)
@@ -358,6 +397,7 @@ int field_view(nim_ctx *x, nim_field f, int par, FieldView &v) {
       cellf(x->F.ct[(int)f - 13]); return NIM_OK;
     case NIM_FIELD_MESHES_P: cellf(x->F.mp); return NIM_OK;
     case NIM_FIELD_MESHES_DILA: cellf(x->F.dila); return NIM_OK;
+    case NIM_FIELD_MESHES_DILA_OLD: cellf(x->F.dila_old); return NIM_OK;
     default: break;
   }
   v.writable = false;
@@ -511,6 +551,7 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
   CK(cudaGetDevice(&x->device));
   TRY(noalloc_setup(x->device));
   CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&x->copy_stream, cudaStreamNonBlocking));
   x->d = make_dims(m->n_theta, m->n_r, m->n_z);
   const Dims &d = x->d;
   std::vector<int> perm;
@@ -622,6 +663,7 @@ extern "C" int nim_gpu_init(nim_ctx *x) {
   }
   CK(cudaMemsetAsync(x->F.dpd, 0, 3 * Nc * sizeof(double), s));
   CK(cudaMemsetAsync(x->F.dila, 0, Nc * sizeof(double), s));
+  CK(cudaMemsetAsync(x->F.dila_old, 0, Nc * sizeof(double), s));
   CK(cudaMemsetAsync(x->F.mp, 0, Nc * sizeof(double), s));
   k_apply_dirichlet<<<x->nblk_b, BLK, 0, s>>>(d, x->g, x->F);
   k_wall_floor<<<x->nblk_b, BLK, 0, s>>>(d, x->g, x->ctl);
@@ -820,6 +862,57 @@ extern "C" int nim_gpu_upload(nim_ctx *x, nim_field f, const double *host, int64
   return NIM_OK;
 }
 
+extern "C" int64_t nim_gpu_output_bytes(nim_ctx *x, int32_t set) {
+  if (!x) return NIM_ERR_BAD_ARG;
+  const int64_t Nc = x->d.Nc, NF = x->d.NF;
+  switch (set) {
+    case NIM_OUTPUT_PLOT: return 6 * Nc * (int64_t)sizeof(float);
+    case NIM_OUTPUT_RESTART: return (5 * NF + 9 * Nc) * (int64_t)sizeof(double);
+    default: return NIM_ERR_BAD_ARG;
+  }
+}
+
+extern "C" int nim_gpu_output_begin(nim_ctx *x, int32_t set, void *host, int64_t bytes, int32_t *ticket) {
+  if (!x || !host || !ticket) return NIM_ERR_BAD_ARG;
+  const int64_t need = nim_gpu_output_bytes(x, set);
+  if (need < 0 || bytes < need) return NIM_ERR_BAD_ARG;
+  if (!x->initialized) return NIM_ERR_STATE;
+  CK(cudaSetDevice(x->device));
+  nim_ctx::Output &o = x->out[set];
+  if (!o.stage) {
+    CK(cudaMalloc(&o.stage, need));
+    x->allocs.push_back(o.stage);
+    CK(cudaEventCreateWithFlags(&o.packed, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&o.copied, cudaEventDisableTiming));
+  } else {
+    CK(cudaStreamWaitEvent(x->stream, o.copied, 0));  // the previous copy has left the staging buffer
+  }
+  const Dims &d = x->d;
+  if (set == NIM_OUTPUT_PLOT)
+    k_pack_plot<<<grid(d.Nc), BLK, 0, x->stream>>>(d, x->F, static_cast<float *>(o.stage));
+  else
+    k_pack_restart<<<grid(std::max(d.NF, d.Nc)), BLK, 0, x->stream>>>(d, x->F, x->perm, x->ctl,
+                                                                      static_cast<double *>(o.stage));
+  CK(cudaGetLastError());
+  x->launches += 1;
+  CK(cudaEventRecord(o.packed, x->stream));
+  CK(cudaStreamWaitEvent(x->copy_stream, o.packed, 0));
+  CK(cudaMemcpyAsync(host, o.stage, need, cudaMemcpyDeviceToHost, x->copy_stream));
+  CK(cudaEventRecord(o.copied, x->copy_stream));
+  o.gen = (o.gen + 1) & 0x3fffffff;
+  *ticket = (o.gen << 1) | set;
+  return NIM_OK;
+}
+
+extern "C" int nim_gpu_output_wait(nim_ctx *x, int32_t ticket) {
+  if (!x || ticket < 0) return NIM_ERR_BAD_ARG;
+  const int set = ticket & 1, gen = ticket >> 1;
+  nim_ctx::Output &o = x->out[set];
+  if (!o.copied || gen != o.gen) return NIM_ERR_STATE;  // unknown, or overtaken by a later begin
+  CK(cudaEventSynchronize(o.copied));
+  return NIM_OK;
+}
+
 extern "C" int nim_gpu_synchronize(nim_ctx *x) {
   if (!x) return NIM_ERR_BAD_ARG;
   CK(cudaStreamSynchronize(x->stream));
@@ -829,9 +922,15 @@ extern "C" int nim_gpu_synchronize(nim_ctx *x) {
 extern "C" void nim_gpu_destroy(nim_ctx *x) {
   if (!x) return;
   if (x->stream) cudaStreamSynchronize(x->stream);
+  if (x->copy_stream) cudaStreamSynchronize(x->copy_stream);  // copies still reading staging
   if (x->graph) cudaGraphExecDestroy(x->graph);
   for (void *p : x->allocs) cudaFree(p);
   if (x->ctl_host) cudaFreeHost(x->ctl_host);
+  for (auto &o : x->out) {
+    if (o.packed) cudaEventDestroy(o.packed);
+    if (o.copied) cudaEventDestroy(o.copied);
+  }
+  if (x->copy_stream) cudaStreamDestroy(x->copy_stream);
   if (x->stream) cudaStreamDestroy(x->stream);
   delete x;
 }

@@ -27,7 +27,7 @@ FACES_U, FACES_V, FACES_W, FACES_P, FACES_T = 0, 1, 2, 3, 4
 MESHES_U, MESHES_V, MESHES_W, MESHES_T = 5, 6, 7, 8
 MESHES_U_OLD, MESHES_V_OLD, MESHES_W_OLD, MESHES_T_OLD = 9, 10, 11, 12
 MESHES_UT, MESHES_VT, MESHES_WT, MESHES_TT = 13, 14, 15, 16
-MESHES_P, MESHES_DILA = 17, 18
+MESHES_P, MESHES_DILA, MESHES_DILA_OLD = 17, 18, 19
 MESHES_VOLUME, FACES_AREA, FACES_NORMAL, FACES_MID = 32, 33, 34, 35
 MESHES_GIJ, MESHES_XI_X, MESHES_G, MESHES_GIJ_FACES = 36, 37, 38, 39
 FACES_TANGENTIAL, FACES_BITANGENTIAL, BCS_FACES_A, BCS_FACES_AP = 40, 41, 42, 43
@@ -36,6 +36,7 @@ M_F4, M_F1, M_F2, M_F3 = 48, 49, 50, 51
 
 CLUSTER_NONE, CLUSTER_POWER, CLUSTER_TANH = 0, 1, 2
 SCHEDULE_PARALLEL, SCHEDULE_REFERENCE = 0, 1
+OUTPUT_PLOT, OUTPUT_RESTART = 0, 1   # nim_output_set
 
 
 class MeshDesc(C.Structure):
@@ -154,6 +155,12 @@ def gpu_lib() -> C.CDLL:
         lib.nim_gpu_download.restype = C.c_int
         lib.nim_gpu_upload.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.c_int64]
         lib.nim_gpu_upload.restype = C.c_int
+        lib.nim_gpu_output_bytes.argtypes = [vp, C.c_int32]
+        lib.nim_gpu_output_bytes.restype = C.c_int64
+        lib.nim_gpu_output_begin.argtypes = [vp, C.c_int32, vp, C.c_int64, C.POINTER(C.c_int32)]
+        lib.nim_gpu_output_begin.restype = C.c_int
+        lib.nim_gpu_output_wait.argtypes = [vp, C.c_int32]
+        lib.nim_gpu_output_wait.restype = C.c_int
         lib.nim_gpu_destroy.argtypes = [vp]
         lib.nim_gpu_destroy.restype = None
         lib.nim_gpu_strerror.argtypes = [C.c_int]

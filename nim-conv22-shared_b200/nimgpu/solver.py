@@ -30,7 +30,7 @@ def field_len(field: int, mesh: Mesh) -> int:
         return table[field]
     if field <= _abi.FACES_T:
         return nf
-    if field <= _abi.MESHES_DILA:
+    if field <= _abi.MESHES_DILA_OLD:
         return nm
     raise ValueError(f"unknown field {field}")
 
@@ -135,6 +135,30 @@ class NimSolver:
         a = np.ascontiguousarray(values, dtype=np.float64)
         _abi.check(self.lib.nim_gpu_upload(self._h, field, a.ctypes.data_as(C.POINTER(C.c_double)), a.size),
                    "nim_gpu_upload")
+
+    # -- output sets packed on the device (write_data / write_restart)
+    def output_array(self, which: int) -> np.ndarray:
+        """A host array shaped for one output set: float32 (6, NMESH) for
+        OUTPUT_PLOT, float64 (5 NFACE + 9 NMESH,) for OUTPUT_RESTART."""
+        n = int(self.lib.nim_gpu_output_bytes(self._h, which))
+        if n < 0:
+            _abi.check(n, "nim_gpu_output_bytes")
+        if which == _abi.OUTPUT_PLOT:
+            return np.empty((6, self.mesh.nmesh), dtype=np.float32)
+        return np.empty(n // 8, dtype=np.float64)
+
+    def output_begin(self, which: int, out: np.ndarray) -> int:
+        """Pack the set on the device and start copying it into out (keep
+        out alive and untouched until output_wait); returns the ticket."""
+        if not out.flags.c_contiguous:
+            raise ValueError("output buffer must be contiguous")
+        t = C.c_int32()
+        _abi.check(self.lib.nim_gpu_output_begin(self._h, which, C.c_void_p(out.ctypes.data), out.nbytes,
+                                                 C.byref(t)), "nim_gpu_output_begin")
+        return t.value
+
+    def output_wait(self, ticket: int):
+        _abi.check(self.lib.nim_gpu_output_wait(self._h, ticket), "nim_gpu_output_wait")
 
     def get(self, field: int, n: int | None = None) -> np.ndarray:
         return self.download(field)
