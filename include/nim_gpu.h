@@ -143,6 +143,12 @@ typedef struct nim_params {
                            run in the reference's cell-number order
                            (run.sh:2, one OpenMP thread), reproducing its
                            iterates                                          */
+  int32_t formulation;  /* nim_formulation (parameters.f90:194): 2 (default),
+                           or 1 for the velocity NIM constants and sweep of
+                           calculate_velocity_nim_constants (nim.f90:17-157)
+                           and integrate_velocity_field_i (nse.f90:330-828);
+                           pressure and temperature are the same in both   */
+  int32_t reserved;     /* 0 */
 } nim_params;
 
 enum { NIM_SCHEDULE_PARALLEL = 0, NIM_SCHEDULE_REFERENCE = 1 };

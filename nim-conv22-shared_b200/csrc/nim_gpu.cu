@@ -448,6 +448,7 @@ extern "C" void nim_params_reference(nim_params *p) {
   p->max_iters = 100000;
   p->check_steady = 1;
   p->dpdx_tolerance = 0;
+  p->formulation = 2;  // parameters.f90:194
 }
 
 extern "C" const char *nim_gpu_strerror(int s) {

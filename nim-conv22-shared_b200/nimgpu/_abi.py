@@ -68,7 +68,8 @@ class Params(C.Structure):
         ("R_i", C.c_double), ("R_o", C.c_double),
         ("bc_value", (C.c_double * NIM_NBC) * 5),
         ("max_iters", C.c_int32), ("check_steady", C.c_int32),
-        ("dpdx_tolerance", C.c_int32), ("schedule", C.c_int32),
+        ("dpdx_tolerance", C.c_int32), ("schedule", C.c_int32), ("formulation", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

@@ -54,6 +54,7 @@ def reference_params(**over) -> _abi.Params:
     p.check_steady = 1
     p.dpdx_tolerance = 0
     p.schedule = _abi.SCHEDULE_PARALLEL
+    p.formulation = 2            # parameters.f90:194
     for k, v in over.items():
         setattr(p, k, v)
     return p

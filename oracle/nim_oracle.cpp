@@ -237,6 +237,9 @@ struct nim_oracle {
   M36 MA, MTA;
   VK<5> MF1, MF2, MF3, MTF1, MTF2, MTF3;
   VK<8> MF4, MTF4;
+  // formulation 1 (nim_formulation = 1): a_t(9), AA_vx/vy/vz(15)
+  VK<9> at;
+  VK<15> AAvx, AAvy, AAvz;
   // parallel-schedule scratch
   V1 snap, pb_new;
   // Gauss-Seidel visiting orders (1-based cell numbers, BC-list indices):
@@ -683,6 +686,178 @@ void temperature_constants(nim_oracle &o) {
   // BCs_faces_aT (nim.f90:509-549) only feeds the uncalled find_Nu.
 }
 
+// --------------------------------------------------------- formulation 1
+// B_nim, C_nim, G_nim, H_nim, I_nim, J_nim (nim.f90:758-875) of one
+// direction, a = 1, for contravariant speed u, diffusivity F and cell Peclet
+// number Re = 2u/F.  condition() (nim.f90:748-756): series when |Re| <
+// v_limit, exponential form otherwise.  G_nim and H_nim assign P twice in
+// their exponential branch; the second assignment is the one that counts.
+struct Nim1 {
+  double B, C, G, H, I, J;
+  bool series;
+};
+Nim1 nim1_direction(double u, double F, double Re, double v_limit) {
+  const double a = 1.;
+  Nim1 r;
+  r.series = std::fabs(Re) < v_limit;
+  if (r.series) {
+    const Pw U(u), K(F);
+    r.B = 0;
+    r.C = -(a * a / (3. * F)) + (U[2]) / (45. * K[3]) - (2 * U[4]) / (945. * K[5]) + -((U[6]) / (4725. * K[7])) -
+          (2 * U[8]) / (93555. * K[9]) + -((1382 * U[10]) / (6.38512875e8 * K[11]));
+    r.G = 1 / (2. * a) + u / (2. * F) + (U[2]) / (6. * K[2]) - (U[4]) / (90. * K[4]) + -((U[6]) / (945. * K[6])) -
+          (U[8]) / (9450. * K[8]) + (U[10]) / (93555. * K[10]);
+    r.H = a / F + (u) / (3. * K[2]) - (U[3]) / (45. * K[4]) + (2 * U[5]) / (945. * K[6]) -
+          -((U[7]) / (4725. * K[8])) + (2 * U[9]) / (93555. * K[10]);
+    r.I = 1 / (2. * a) - u / (2. * F) + (U[2]) / (6. * K[2]) - (U[4]) / (90. * K[4]) + -((U[6]) / (945. * K[6])) -
+          (U[8]) / (9450. * K[8]) + (U[10]) / (93555. * K[10]);
+    r.J = -(a / F) + (u) / (3. * K[2]) - (U[3]) / (45. * K[4]) + -((2 * U[5]) / (945. * K[6])) -
+          (U[7]) / (4725. * K[8]) + -((2 * U[9]) / (93555. * K[10]));
+  } else {
+    const double e = std::exp(Re);
+    r.B = 1. / u * (1. / Re - 1. / (e - 1.));
+    r.C = (-(1. / u) + 2. * r.B) * a;
+    r.G = u / F / (1. - 1. / e);
+    r.H = 2. * a / F / (1. - 1. / e) - 1. / u;
+    r.I = u / (F * (e - 1.));
+    r.J = 2. * a / (F * (e - 1.)) - 1. / u;
+  }
+  return r;
+}
+// E_nim, F_nim (nim.f90:787-815) with D = Det
+inline double nim1_E(const Nim1 &r, double u, double F, double D) {
+  const double a = 1.;
+  if (r.series) {
+    const Pw U(u), K(F);
+    return D / 2. + (a * D * u) / (6. * F) - (D * U[3]) / (90. * K[3]) + (D * U[5]) / (945. * K[5]) -
+           -((D * U[7]) / (9450. * K[7])) + (D * U[9]) / (93555. * K[9]);
+  }
+  return D * (1 - r.B * u);
+}
+inline double nim1_F(const Nim1 &r, double u, double F, double D) {
+  const double a = 1.;
+  if (r.series) {
+    const Pw U(u), K(F);
+    return D / 2. - (a * D * u) / (6. * F) + (D * U[3]) / (90. * K[3]) - (D * U[5]) / (945. * K[5]) +
+           -((D * U[7]) / (9450. * K[7])) - (D * U[9]) / (93555. * K[9]);
+  }
+  return D * (r.B * u);
+}
+
+// calculate_velocity_nim_constants (nim.f90:17-157): a_t and AA_vx/vy/vz
+void velocity_constants_f1(nim_oracle &o) {
+  const int64_t N = o.NMESH;
+  VK<3> CC, EE, FF, GG, HH, II, JJ;
+  V1 Det;
+  CC.alloc(N); EE.alloc(N); FF.alloc(N); GG.alloc(N); HH.alloc(N); II.alloc(N); JJ.alloc(N); Det.alloc(N);
+#pragma omp parallel for schedule(static) num_threads(o.nthreads)
+  for (int64_t i = 1; i <= N; ++i) {
+    o.mu(i) = o.ut(i) * o.xi_x(1, 1, i) + o.vt(i) * o.xi_x(1, 2, i) + o.wt(i) * o.xi_x(1, 3, i);
+    o.mv(i) = o.ut(i) * o.xi_x(2, 1, i) + o.vt(i) * o.xi_x(2, 2, i) + o.wt(i) * o.xi_x(2, 3, i);
+    o.mw(i) = o.ut(i) * o.xi_x(3, 1, i) + o.vt(i) * o.xi_x(3, 2, i) + o.wt(i) * o.xi_x(3, 3, i);
+    const double uc[3] = {o.mu(i), o.mv(i), o.mw(i)};
+    double K[3], Re[3];
+    Nim1 r[3];
+    for (int d = 1; d <= 3; ++d) {
+      K[d - 1] = o.gij(d, d, i) * o.P.nu;
+      Re[d - 1] = 2 * uc[d - 1] / K[d - 1];
+    }
+    for (int d = 1; d <= 3; ++d) {
+      r[d - 1] = nim1_direction(uc[d - 1], K[d - 1], Re[d - 1], o.P.v_limit);
+      CC(d, i) = r[d - 1].C;
+      GG(d, i) = r[d - 1].G;
+      HH(d, i) = r[d - 1].H;
+      II(d, i) = r[d - 1].I;
+      JJ(d, i) = r[d - 1].J;
+    }
+    Det(i) = 1. / (CC(1, i) * CC(2, i) + CC(2, i) * CC(3, i) + CC(1, i) * CC(3, i));
+    for (int d = 1; d <= 3; ++d) {
+      EE(d, i) = nim1_E(r[d - 1], uc[d - 1], K[d - 1], Det(i));
+      FF(d, i) = nim1_F(r[d - 1], uc[d - 1], K[d - 1], Det(i));
+    }
+  }
+  const double DT = o.P.DT;
+#pragma omp parallel for schedule(static) num_threads(o.nthreads)
+  for (int64_t i = 1; i <= N; ++i) {
+    auto C = [&](int d, int64_t n) { return CC(d, n); };
+    auto E = [&](int d, int64_t n) { return EE(d, n); };
+    auto Fv = [&](int d, int64_t n) { return FF(d, n); };
+    if (o.NB(2, i) != 0) {  // face 2 (nim.f90:87-104)
+      const int64_t i2 = o.NB(2, i);
+      const double g2 = o.gf(1, 1, 2, i), g1 = o.gf(1, 1, 1, i2);
+      VK<15> &A = o.AAvx;
+      A(1, i) = -(GG(1, i) + (C(2, i) + C(3, i)) * E(1, i) * HH(1, i)) * g2;
+      A(2, i) = (GG(1, i) - (C(2, i) + C(3, i)) * Fv(1, i) * HH(1, i)) * g2 +
+                (II(1, i2) + (C(2, i2) + C(3, i2)) * E(1, i2) * JJ(1, i2)) * g1;
+      A(3, i) = -(II(1, i2) - (C(2, i2) + C(3, i2)) * Fv(1, i2) * JJ(1, i2)) * g1;
+      A(4, i) = C(3, i) * E(2, i) * HH(1, i) * g2;
+      A(5, i) = C(3, i) * Fv(2, i) * HH(1, i) * g2;
+      A(6, i) = -C(3, i2) * E(2, i2) * JJ(1, i2) * g1;
+      A(7, i) = -C(3, i2) * Fv(2, i2) * JJ(1, i2) * g1;
+      A(8, i) = C(2, i) * E(3, i) * HH(1, i) * g2;
+      A(9, i) = C(2, i) * Fv(3, i) * HH(1, i) * g2;
+      A(10, i) = -C(2, i2) * E(3, i2) * JJ(1, i2) * g1;
+      A(11, i) = -C(2, i2) * Fv(3, i2) * JJ(1, i2) * g1;
+      A(12, i) = C(2, i) * C(3, i) * Det(i) * HH(1, i) * g2 / (2 * DT);
+      A(13, i) = -C(2, i) * C(3, i) * Det(i) * HH(1, i) * g2 / (2 * DT);
+      A(14, i) = -C(2, i2) * C(3, i2) * Det(i2) * JJ(1, i2) * g1 / (2 * DT);
+      A(15, i) = C(2, i2) * C(3, i2) * Det(i2) * JJ(1, i2) * g1 / (2 * DT);
+    }
+    if (o.NB(4, i) != 0) {  // face 4 (nim.f90:107-124)
+      const int64_t i2 = o.NB(4, i);
+      const double g4 = o.gf(2, 2, 4, i), g3 = o.gf(2, 2, 3, i2);
+      VK<15> &A = o.AAvy;
+      A(1, i) = C(3, i) * E(1, i) * HH(2, i) * g4;
+      A(2, i) = C(3, i) * Fv(1, i) * HH(2, i) * g4;
+      A(3, i) = -C(3, i2) * E(1, i2) * JJ(2, i2) * g3;
+      A(4, i) = -C(3, i2) * Fv(1, i2) * JJ(2, i2) * g3;
+      A(5, i) = -(GG(2, i) + (C(1, i) + C(3, i)) * E(2, i) * HH(2, i)) * g4;
+      A(6, i) = (GG(2, i) - (C(1, i) + C(3, i)) * Fv(2, i) * HH(2, i)) * g4 +
+                (II(2, i2) + (C(1, i2) + C(3, i2)) * E(2, i2) * JJ(2, i2)) * g3;
+      A(7, i) = -(II(2, i2) - (C(1, i2) + C(3, i2)) * Fv(2, i2) * JJ(2, i2)) * g3;
+      A(8, i) = C(1, i) * E(3, i) * HH(2, i) * g4;
+      A(9, i) = C(1, i) * Fv(3, i) * HH(2, i) * g4;
+      A(10, i) = -C(1, i2) * E(3, i2) * JJ(2, i2) * g3;
+      A(11, i) = -C(1, i2) * Fv(3, i2) * JJ(2, i2) * g3;
+      A(12, i) = C(1, i) * C(3, i) * Det(i) * HH(2, i) * g4 / (2 * DT);
+      A(13, i) = -C(1, i) * C(3, i) * Det(i) * HH(2, i) * g4 / (2 * DT);
+      A(14, i) = -C(1, i2) * C(3, i2) * Det(i2) * JJ(2, i2) * g3 / (2 * DT);
+      A(15, i) = C(1, i2) * C(3, i2) * Det(i2) * JJ(2, i2) * g3 / (2 * DT);
+    }
+    if (o.NB(6, i) != 0) {  // face 6 (nim.f90:126-143)
+      const int64_t i2 = o.NB(6, i);
+      const double g6 = o.gf(3, 3, 6, i), g5 = o.gf(3, 3, 5, i2);
+      VK<15> &A = o.AAvz;
+      A(1, i) = C(2, i) * E(1, i) * HH(3, i) * g6;
+      A(2, i) = C(2, i) * Fv(1, i) * HH(3, i) * g6;
+      A(3, i) = -C(2, i2) * E(1, i2) * JJ(3, i2) * g5;
+      A(4, i) = -C(2, i2) * Fv(1, i2) * JJ(3, i2) * g5;
+      A(5, i) = C(1, i) * E(2, i) * HH(3, i) * g6;
+      A(6, i) = C(1, i) * Fv(2, i) * HH(3, i) * g6;
+      A(7, i) = -C(1, i2) * E(2, i2) * JJ(3, i2) * g5;
+      A(8, i) = -C(1, i2) * Fv(2, i2) * JJ(3, i2) * g5;
+      A(9, i) = -(GG(3, i) + (C(1, i) + C(2, i)) * E(3, i) * HH(3, i)) * g6;
+      A(10, i) = (GG(3, i) - (C(1, i) + C(2, i)) * Fv(3, i) * HH(3, i)) * g6 +
+                 (II(3, i2) + (C(1, i2) + C(2, i2)) * E(3, i2) * JJ(3, i2)) * g5;
+      A(11, i) = -(II(3, i2) - (C(1, i2) + C(2, i2)) * Fv(3, i2) * JJ(3, i2)) * g5;
+      A(12, i) = C(1, i) * C(2, i) * Det(i) * HH(3, i) * g6 / (2 * DT);
+      A(13, i) = -C(1, i) * C(2, i) * Det(i) * HH(3, i) * g6 / (2 * DT);
+      A(14, i) = -C(1, i2) * C(2, i2) * Det(i2) * JJ(3, i2) * g5 / (2 * DT);
+      A(15, i) = C(1, i2) * C(2, i2) * Det(i2) * JJ(3, i2) * g5 / (2 * DT);
+    }
+    // a_t, nim.f90:146-154
+    o.at(1, i) = 2 * E(1, i) / Det(i) - 2 * (C(2, i) + C(3, i)) * C(1, i) * E(1, i);
+    o.at(2, i) = 2 * Fv(1, i) / Det(i) - 2 * (C(2, i) + C(3, i)) * C(1, i) * Fv(1, i);
+    o.at(3, i) = 2 * E(2, i) * C(1, i) * C(3, i);
+    o.at(4, i) = 2 * Fv(2, i) * C(1, i) * C(3, i);
+    o.at(5, i) = 2 * E(3, i) * C(1, i) * C(2, i);
+    o.at(6, i) = 2 * Fv(3, i) * C(1, i) * C(2, i);
+    o.at(7, i) = 2 * C(1, i) * C(2, i) * C(3, i) * Det(i);
+    o.at(8, i) = -o.at(7, i) / (2 * DT) - 1;
+    o.at(9, i) = o.at(7, i) / (2 * DT) - 1;
+  }
+}
+
 // ---------------------------------------------------------------- sources
 // Green-Gauss derivative dphi_dx2/dy2/dz2 (nse.f90:2866-2903), component c.
 inline double green_gauss(const nim_oracle &o, const double *phi, const int32_t *nf, int64_t i, int c) {
@@ -782,6 +957,47 @@ inline double face_update(const nim_oracle &o, const V1 &fr, const V1 &c, const 
   return (1 - w) * fr(o.F(2 * d, i)) +
          (w / Fd(1, i)) * (+Fd(2, i) * fr(o.F(2 * d - 1, i)) + Fd(3, i) * fr(o.F(2 * d, i2)) +
                            Fd(4, i) * (c(i) + cold(i)) + Fd(5, i) * (c(i2) + cold(i2)) - B3 - B4);
+}
+
+// Formulation 1 cell update of one velocity component (integrate_velocity_
+// field_i, nse.f90:341-352); R = R_C + R_D + R_B of the cell.
+inline double cell_update_f1(const nim_oracle &o, const V1 &f, double c, double cold, double R, int64_t i,
+                             double w) {
+  const VK<9> &a = o.at;
+  const double Bij = a(7, i) * R;
+  return (1 - w) * c + w * (-(a(1, i) * f(o.F(1, i))) - a(2, i) * f(o.F(2, i)) - a(3, i) * f(o.F(3, i)) -
+                            a(4, i) * f(o.F(4, i)) - a(5, i) * f(o.F(5, i)) - a(6, i) * f(o.F(6, i)) -
+                            a(8, i) * cold - Bij) /
+                           (a(9, i));
+}
+
+// Formulation 1 update of the +d face of cell n1 (nse.f90:378-826): the
+// pressure sweep's ten face terms with AA_v, the two cell time terms, the
+// R sums of both cells and the tangential cross terms B3, B4 (the centred
+// B3/B4 the source computes first are overwritten before use).
+inline double face_update_f1(const nim_oracle &o, const V1 &fr, const V1 &c, const V1 &cold, const V1 &RD,
+                             const V1 &RB, int d, int64_t n1, double w) {
+  const int64_t n2 = o.NB(2 * d, n1);
+  const VK<15> &A = (d == 1) ? o.AAvx : (d == 2) ? o.AAvy : o.AAvz;
+  const int e1 = (d == 1) ? 2 : 1, e2 = (d == 3) ? 2 : 3;
+  const double DT = o.P.DT;
+  const double B1 = (0. + RD(n1) + RB(n1)) * A(13, n1) * 2 * DT;
+  const double B2 = (0. + RD(n2) + RB(n2)) * A(15, n1) * 2 * DT;
+  const double B3 = (o.gf(d, e1, 2 * d - 1, n2) - o.gf(d, e1, 2 * d, n1)) * tangential(o, fr, n1, 2 * d, e1);
+  const double B4 = (o.gf(d, e2, 2 * d - 1, n2) - o.gf(d, e2, 2 * d, n1)) * tangential(o, fr, n1, 2 * d, e2);
+  static const int tab[3][10][3] = {
+      {{1, 1, 1}, {3, 2, 2}, {4, 3, 1}, {5, 4, 1}, {6, 3, 2}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
+      {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
+      {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {6, 4, 1}, {7, 3, 2}, {8, 4, 2}, {9, 5, 1}, {11, 6, 2}}};
+  static const int diag[3] = {2, 6, 10};
+  double s = 0.0;
+  for (int t = 0; t < 10; ++t) {
+    const int64_t cell = (tab[d - 1][t][2] == 1) ? n1 : n2;
+    const double term = A(tab[d - 1][t][0], n1) * fr(o.F(tab[d - 1][t][1], cell));
+    s = (t == 0) ? -term : s - term;
+  }
+  s = s - A(12, n1) * (c(n1) - cold(n1)) - A(14, n1) * (c(n2) - cold(n2));
+  return (1 - w) * fr(o.F(2 * d, n1)) + w / (A(diag[d - 1], n1)) * (s + B1 + B2 + B3 + B4);
 }
 
 // calculate_R_b_p (nse.f90:2362-2407) + calculate_R_D_p2 (nse.f90:1863-1997)
@@ -952,31 +1168,34 @@ void iteration(nim_oracle &o) {
 
   // ---- velocity
   velocity_sources(o);
+  const bool f1 = (o.P.formulation == 1);
+  auto vcell = [&](int k, int64_t i) {
+    const double B = (0. + (*RD[k])(i) + (*RB[k])(i));  // R_C = 0
+    return f1 ? cell_update_f1(o, *vf[k], (*vc[k])(i), (*vo[k])(i), B, i, wv[k])
+              : cell_update(o, *vf[k], (*vc[k])(i), (*vo[k])(i), B, o.MF4, i, wv[k]);
+  };
+  auto vface = [&](int k, const V1 &fr, int d, int64_t i) {
+    return f1 ? face_update_f1(o, fr, *vc[k], *vo[k], *RD[k], *RB[k], d, i, wv[k])
+              : face_update(o, fr, *vc[k], *vo[k], *MF[d - 1], d, i, wv[k]);
+  };
   if (seq) {
 #pragma omp parallel for schedule(static) num_threads(nt)
     for (int64_t q = 0; q < N; ++q) {
       const int64_t i = o.cord[q];
-      for (int k = 0; k < 3; ++k) {
-        const double B = (0. + (*RD[k])(i) + (*RB[k])(i));  // R_C = 0
-        (*vc[k])(i) = cell_update(o, *vf[k], (*vc[k])(i), (*vo[k])(i), B, o.MF4, i, wv[k]);
-      }
+      for (int k = 0; k < 3; ++k) (*vc[k])(i) = vcell(k, i);
       for (int d = 1; d <= 3; ++d) {
         if (o.NB(2 * d, i) == 0) continue;
-        for (int k = 0; k < 3; ++k)
-          (*vf[k])(o.F(2 * d, i)) = face_update(o, *vf[k], *vc[k], *vo[k], *MF[d - 1], d, i, wv[k]);
+        for (int k = 0; k < 3; ++k) (*vf[k])(o.F(2 * d, i)) = vface(k, *vf[k], d, i);
       }
     }
   } else {
     for (int64_t i = 1; i <= N; ++i)
-      for (int k = 0; k < 3; ++k) {
-        const double B = (0. + (*RD[k])(i) + (*RB[k])(i));
-        (*vc[k])(i) = cell_update(o, *vf[k], (*vc[k])(i), (*vo[k])(i), B, o.MF4, i, wv[k]);
-      }
+      for (int k = 0; k < 3; ++k) (*vc[k])(i) = vcell(k, i);
     for (int k = 0; k < 3; ++k) {
       o.snap.d = vf[k]->d;
       for (int64_t i = 1; i <= N; ++i)
         for (int d = 1; d <= 3; ++d)
-          if (o.NB(2 * d, i) != 0) (*vf[k])(o.F(2 * d, i)) = face_update(o, o.snap, *vc[k], *vo[k], *MF[d - 1], d, i, wv[k]);
+          if (o.NB(2 * d, i) != 0) (*vf[k])(o.F(2 * d, i)) = vface(k, o.snap, d, i);
     }
   }
 
@@ -1114,6 +1333,7 @@ extern "C" int nim_oracle_create(const nim_mesh_desc *m, const nim_params *p, in
                                  int32_t threads, nim_oracle **out) {
   if (!m || !p || !out) return NIM_ERR_BAD_ARG;
   if (m->nmesh <= 0 || m->nface <= 0 || m->nnode <= 0 || m->nbcface <= 0) return NIM_ERR_BAD_ARG;
+  if (p->formulation != 1 && p->formulation != 2) return NIM_ERR_BAD_ARG;
   auto *o = new nim_oracle();
   o->sched = schedule;
   o->nthreads = threads > 0 ? threads : 1;
@@ -1168,6 +1388,9 @@ extern "C" int nim_oracle_create(const nim_mesh_desc *m, const nim_params *p, in
   o->MA.alloc(N); o->MTA.alloc(N);
   o->MF1.alloc(N); o->MF2.alloc(N); o->MF3.alloc(N); o->MTF1.alloc(N); o->MTF2.alloc(N); o->MTF3.alloc(N);
   o->MF4.alloc(N); o->MTF4.alloc(N);
+  if (p->formulation == 1) {
+    o->at.alloc(N); o->AAvx.alloc(N); o->AAvy.alloc(N); o->AAvz.alloc(N);
+  }
   *out = o;
   return NIM_OK;
 }
@@ -1206,7 +1429,10 @@ extern "C" int nim_oracle_init(nim_oracle *o) {
 
 extern "C" int nim_oracle_begin_step(nim_oracle *o) {
   if (!o || !o->initialized) return NIM_ERR_STATE;
-  velocity_constants(*o);
+  if (o->P.formulation == 1)
+    velocity_constants_f1(*o);
+  else
+    velocity_constants(*o);
   return NIM_OK;
 }
 
@@ -1452,4 +1678,16 @@ extern "C" void nim_oracle_set_threads(nim_oracle *o, int32_t threads) {
 extern "C" void nim_oracle_nim_coefficients(double u, double k, double gminus, double gplus, double v_limit,
                                             double *A) {
   nim_direction(u, k, gminus, gplus, v_limit, A);
+}
+
+extern "C" void nim_oracle_nim1_coefficients(double u, double F, double D, double v_limit, double *out) {
+  const Nim1 r = nim1_direction(u, F, 2 * u / F, v_limit);
+  out[0] = r.B;
+  out[1] = r.C;
+  out[2] = nim1_E(r, u, F, D);
+  out[3] = nim1_F(r, u, F, D);
+  out[4] = r.G;
+  out[5] = r.H;
+  out[6] = r.I;
+  out[7] = r.J;
 }

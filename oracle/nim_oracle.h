@@ -57,6 +57,9 @@ void nim_oracle_set_threads(nim_oracle *o, int32_t threads);
    metrics g_minus/g_plus, branch switch v_limit (nim.f90:181-287) */
 void nim_oracle_nim_coefficients(double u, double k, double gminus, double gplus, double v_limit,
                                  double *A);
+/* formulation 1: B, C, E, F, G, H, I, J_nim of one direction (nim.f90:758-875)
+   for speed u, diffusivity F and Det = D */
+void nim_oracle_nim1_coefficients(double u, double F, double D, double v_limit, double *out);
 
 #ifdef __cplusplus
 }

@@ -130,6 +130,13 @@ class Oracle:
         return lib().nim_oracle_max_rc(self._h)
 
 
+def nim1_coefficients(u: float, F: float, D: float, v_limit: float = 1e-2):
+    """Formulation 1: B, C, E, F, G, H, I, J_nim of one direction (nim.f90:758-875)."""
+    out = (C.c_double * 8)()
+    lib().nim_oracle_nim1_coefficients(C.c_double(u), C.c_double(F), C.c_double(D), C.c_double(v_limit), out)
+    return np.array(out[:])
+
+
 def nim_coefficients(u: float, k: float, gminus: float = 1.0, gplus: float = 1.0, v_limit: float = 1e-2):
     """M_A(d,1:6) of one direction (nim.f90:181-287)."""
     A = (C.c_double * 6)()

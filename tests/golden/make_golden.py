@@ -61,6 +61,9 @@ def main():
     ]
     sc = config.small_case(16, 6, 6)
     cases.append(run("tanh_16x6x6", sc.mesh_params(), sc.params(), 3, noise=(sc.noise, sc.seed)))
+    # nim_formulation = 1 (nim.f90:17-157, nse.f90:330-828)
+    cases.append(run("formulation1_16x6x6", sc.mesh_params(), sc.params(formulation=1), 3,
+                     noise=(sc.noise, sc.seed)))
     (HERE / "oracle_golden.json").write_text(json.dumps(cases, indent=1))
     print("wrote", HERE / "oracle_golden.json")
 

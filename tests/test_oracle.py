@@ -24,6 +24,8 @@ def _case(name):
     if name.startswith("reference"):
         return config.reference_mesh(), config.reference_params(), None
     sc = config.small_case(16, 6, 6)
+    if name.startswith("formulation1"):
+        return sc.mesh_params(), sc.params(formulation=1), (sc.noise, sc.seed)
     return sc.mesh_params(), sc.params(), (sc.noise, sc.seed)
 
 
@@ -99,6 +101,23 @@ def test_nim_series_and_exact_branches_agree(Re):
     assert np.all(np.abs(series - exact) <= tol * np.abs(exact))
 
 
+@pytest.mark.parametrize("Re", [-0.05, -0.01, -0.003, 0.003, 0.01, 0.05])
+def test_formulation1_series_and_exact_branches_agree(Re):
+    """nim.f90:758-875: C, E, F, G, H, I, J_nim in their series and
+    exponential forms agree where condition() switches between them, up to
+    the exponential form's cancellation (C: ~eps/|Re|^3; the others
+    ~eps/Re^2) and the series' truncation.  B_nim is 0 in the series branch
+    by definition and enters only the exponential forms."""
+    eps = 2.2e-16
+    F, D = 0.37, -1.7
+    u = Re * F / 2
+    series = O.nim1_coefficients(u, F, D, v_limit=1e300)[1:]
+    exact = O.nim1_coefficients(u, F, D, v_limit=0.0)[1:]
+    tol = np.full(7, 1e-12 + 200 * eps / Re ** 2 + 100 * abs(Re) ** 9)
+    tol[0] += 10 * eps / abs(Re) ** 3
+    assert np.all(np.abs(series - exact) <= tol * np.abs(exact))
+
+
 def test_pressure_system_has_constant_null_space():
     """The pressure equations are of pure-Neumann type: a constant shift of
     all face pressures solves the homogeneous system (sum of the 11 face
@@ -115,14 +134,15 @@ def test_pressure_system_has_constant_null_space():
     assert np.all(np.abs(ap.sum(1)) <= 1e-12 * np.abs(ap).sum(1))
 
 
-def test_conduction_limit_nusselt():
+@pytest.mark.parametrize("formulation", [2, 1])
+def test_conduction_limit_nusselt(formulation):
     """Concentric annulus (no hexagon), negligible buoyancy: both wall
     Nusselt numbers tend to 1/ln(R_o/R_i).  The inner wall shows the time
     element's odd/even oscillation at this large step, so two steps are
     averaged."""
     mp = config.reference_mesh(n_theta=18, n_r=6, n_z=3, R_i=0.5, R_o=1.0, L=1.0, cluster=0, hexagon=0)
     mesh = nimgpu.Mesh(mp)
-    p = config.reference_params(Ra=1.0, Pr=1.0, DT=0.05, R_i=0.5, R_o=1.0)
+    p = config.reference_params(Ra=1.0, Pr=1.0, DT=0.05, R_i=0.5, R_o=1.0, formulation=formulation)
     o = O.Oracle(mesh, p)
     o.init()
     st, recs = o.step(40)
@@ -157,8 +177,9 @@ def test_both_orders_reach_the_same_fixed_point():
     assert np.abs(ca - cb).max() <= 1e-10 * np.abs(cb).max()
 
 
-@pytest.mark.parametrize("dims", [(12, 6, 6), (16, 5, 7), (6, 4, 4), (7, 3, 9)])
-def test_level_order_reproduces_reference_order(dims):
+@pytest.mark.parametrize("dims,formulation", [((12, 6, 6), 2), ((16, 5, 7), 2), ((6, 4, 4), 2), ((7, 3, 9), 2),
+                                              ((12, 6, 6), 1), ((7, 3, 9), 1)])
+def test_level_order_reproduces_reference_order(dims, formulation):
     """The CUDA library's reference-order schedule sweeps cells by the level
     i + 2j + 3k and wall faces by their in-wall level.  The oracle's LEVELS
     order visits them that way (numbers descending inside a level, walls top
@@ -169,7 +190,7 @@ def test_level_order_reproduces_reference_order(dims):
     mesh = nimgpu.Mesh(case.mesh_params())
     out = []
     for sched in (O.SEQUENTIAL, O.LEVELS):
-        o = O.Oracle(mesh, case.params(), schedule=sched)
+        o = O.Oracle(mesh, case.params(formulation=formulation), schedule=sched)
         o.init()
         nimgpu.apply_temperature_noise(o.get, o.set, mesh, case.noise, case.seed)
         st, recs = o.step(2)
