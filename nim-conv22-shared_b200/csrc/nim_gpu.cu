@@ -201,7 +201,21 @@ Phys make_phys(const nim_params &p) {
   P.inv_rho = 1 / p.rho;
   P.max_iters = p.max_iters;
   P.dpdx_tolerance = p.dpdx_tolerance;
+  P.formulation = p.formulation;
   return P;
+}
+
+// the velocity sources + cell kernel and the face kernel of the context's
+// formulation (parallel schedule)
+void launch_vel(nim_ctx *x, cudaStream_t s) {
+  const Dims &d = x->d;
+  if (x->phys.formulation == 1) {
+    k_vel_cell<false, 1><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_vel1_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  } else {
+    k_vel_cell<false, 2><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  }
 }
 
 template <typename K>
@@ -223,8 +237,13 @@ int launch_coop(K kern, int blocks, dim3 block, nim_ctx *x) {
 int launch_iteration_seq(nim_ctx *x) {
   const Dims &d = x->d;
   cudaStream_t s = x->stream;
-  k_vel_cell<true><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-  TRY(launch_coop(k_seq_vel, x->coop_vel, dim3(CB, 3), x));
+  if (x->phys.formulation == 1) {
+    k_vel_cell<true, 1><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    TRY(launch_coop(k_seq_vel<1>, x->coop_vel, dim3(CB, 3), x));
+  } else {
+    k_vel_cell<true, 2><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    TRY(launch_coop(k_seq_vel<2>, x->coop_vel, dim3(CB, 3), x));
+  }
   k_p_src<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_seq_pbc<<<2, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl, x->border, x->blev, x->wlev, 0);
   k_seq_pbc<<<2, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl, x->border, x->blev, x->wlev, 2);
@@ -248,8 +267,7 @@ int launch_iteration(nim_ctx *x) {
   cudaStream_t s = x->stream;
   const int gc = x->nblk_c, gb = x->nblk_b;
   const dim3 g3 = x->g3, g8 = x->g8;
-  k_vel_cell<false><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-  k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  launch_vel(x, s);
   k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_p_bc<<<gb, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
   k_p_bc_copy<<<gb, BLK, 0, s>>>(d, x->F, x->ctl);
@@ -482,7 +500,6 @@ static int noalloc_setup(int device) {
 static int setup_levels(nim_ctx *x) {
   const Dims &d = x->d;
   const size_t Nc = d.Nc;
-  TRY(dalloc(x, &x->F.Bv, 3 * Nc));
   TRY(dalloc(x, &x->F.MTF4, 8 * Nc));
   TRY(dalloc(x, &x->F.RDT, Nc));
   // counting sort of the cells by level
@@ -538,7 +555,10 @@ static int setup_levels(nim_ctx *x) {
   if (!coop) return NIM_ERR_CUDA;
   const int want = std::max(1, (maxlev + BLK - 1) / BLK);
   int per = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_seq_vel, CB3, 0));
+  if (x->phys.formulation == 1)
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_seq_vel<1>, CB3, 0));
+  else
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_seq_vel<2>, CB3, 0));
   x->coop_vel = std::max(1, std::min((maxlev + CB - 1) / CB, per * sms));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_seq_p, BLK, 0));
   x->coop_p = std::max(1, std::min(want, per * sms));
@@ -604,6 +624,12 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
   TRY(dalloc(x, &F.MF, 15 * Nc));
   TRY(dalloc(x, &F.MTF, 15 * Nc));
   TRY(dalloc(x, &F.MTA, 18 * Nc));
+  if (x->seq || p->formulation == 1) TRY(dalloc(x, &F.Bv, 3 * Nc));
+  if (p->formulation == 1) {
+    TRY(dalloc(x, &F.N1, 22 * Nc));
+    TRY(dalloc(x, &F.AT, 9 * Nc));
+    TRY(dalloc(x, &F.AAv, 45 * Nc));
+  }
   TRY(dalloc(x, &F.dpd, 3 * Nc));
   TRY(dalloc(x, &F.part, 8 * (size_t)std::max(x->nblk_c, grid(2 * d.NT * d.NZ))));
   TRY(dalloc(x, &x->ctl, 1));
@@ -632,6 +658,7 @@ extern "C" int nim_gpu_create(const nim_mesh_desc *m, const nim_params *p, nim_c
   if ((int64_t)m->n_theta * m->n_r * m->n_z > (int64_t)INT32_MAX / 4) return NIM_ERR_BAD_ARG;
   if (!(p->DT > 0) || !(p->nu > 0) || !(p->alpha > 0) || !(p->rho > 0)) return NIM_ERR_BAD_ARG;
   if (p->schedule != NIM_SCHEDULE_PARALLEL && p->schedule != NIM_SCHEDULE_REFERENCE) return NIM_ERR_BAD_ARG;
+  if (p->formulation != 1 && p->formulation != 2) return NIM_ERR_BAD_ARG;
   *out = nullptr;
   nim_ctx *x = new (std::nothrow) nim_ctx();
   if (!x) return NIM_ERR_BAD_ARG;
@@ -683,8 +710,13 @@ extern "C" int nim_gpu_begin_step(nim_ctx *x) {
   if (!x->initialized) return NIM_ERR_STATE;
   const Dims &d = x->d;
   k_step_reset<<<1, 1, 0, x->stream>>>(x->ctl);
-  k_vel_coef_A<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->g, x->F, x->phys);
-  k_vel_coef_F<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->F, x->phys);
+  if (x->phys.formulation == 1) {  // calculate_velocity_nim_constants (nim.f90:17-157)
+    k_vel1_coef_A<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->g, x->F, x->phys);
+    k_vel1_coef_F<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->g, x->F, x->phys);
+  } else {
+    k_vel_coef_A<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->g, x->F, x->phys);
+    k_vel_coef_F<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->F, x->phys);
+  }
   CK(cudaGetLastError());
   x->launches += 3;
   x->in_step = true;
@@ -964,9 +996,15 @@ extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int
   const dim3 g3 = x->g3, g8 = x->g8;
   for (int it = 0; it < n; ++it) {
     CK(cudaEventRecord(ev[0], s));
-    k_vel_cell<false><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-    CK(cudaEventRecord(ev[1], s));
-    k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    if (x->phys.formulation == 1) {
+      k_vel_cell<false, 1><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+      CK(cudaEventRecord(ev[1], s));
+      k_vel1_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    } else {
+      k_vel_cell<false, 2><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+      CK(cudaEventRecord(ev[1], s));
+      k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    }
     CK(cudaEventRecord(ev[2], s));
     k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
     CK(cudaEventRecord(ev[3], s));

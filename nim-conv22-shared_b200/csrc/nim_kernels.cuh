@@ -69,6 +69,10 @@ struct Fields {
   double *Bv;      // [3][Nc]   R_C + R_D + R_B of u, v, w
   double *MTF4;    // [8][Nc]   MT_F4
   double *RDT;     // [Nc]      R_D_T
+  // formulation 1 (nim_formulation = 1)
+  double *N1;      // [22][Nc]  CC, EE, FF, GG, HH, II, JJ (3 each), Det (per step)
+  double *AT;      // [9][Nc]   a_t
+  double *AAv;     // [45][Nc]  AA_vx, AA_vy, AA_vz (15 each)
   double *part;    // [8][nblk] per-block partial sums
 };
 
@@ -81,6 +85,7 @@ struct Phys {
   double inv_Re;   // 1/Re with Re = 1/nu (parameters.f90:172, nse.f90:1852)
   double inv_rho;  // 1/rho
   int max_iters, dpdx_tolerance;
+  int formulation; // nim_formulation: 1 or 2
 };
 
 // Control block in device memory; k_iter_end is its only writer during an
@@ -688,10 +693,196 @@ __global__ void __launch_bounds__(BLK) k_vel_coef_F(Dims d, Fields F, Phys P) {
   }
 }
 
+// ====================================================== formulation 1
+// B_nim, C_nim, G_nim, H_nim, I_nim, J_nim (nim.f90:748-875) of one
+// direction, a = 1, for contravariant speed u, diffusivity F and cell Peclet
+// number Re = 2u/F: series when |Re| < v_limit (condition, nim.f90:748-756),
+// exponential form otherwise.  G_nim and H_nim assign P twice in their
+// exponential branch; the second assignment is the one that counts.
+struct Nim1 {
+  double B, C, G, H, I, J;
+  bool series;
+};
+__device__ __forceinline__ Nim1 nim1_direction(double u, double F, double Re, double v_limit) {
+  const double a = 1.;
+  Nim1 r;
+  r.series = fabs(Re) < v_limit;
+  if (r.series) {
+    const Pw U(u), K(F);
+    r.B = 0;
+    r.C = -(a * a / (3. * F)) + (U[2]) / (45. * K[3]) - (2 * U[4]) / (945. * K[5]) + -((U[6]) / (4725. * K[7])) -
+          (2 * U[8]) / (93555. * K[9]) + -((1382 * U[10]) / (6.38512875e8 * K[11]));
+    r.G = 1 / (2. * a) + u / (2. * F) + (U[2]) / (6. * K[2]) - (U[4]) / (90. * K[4]) + -((U[6]) / (945. * K[6])) -
+          (U[8]) / (9450. * K[8]) + (U[10]) / (93555. * K[10]);
+    r.H = a / F + (u) / (3. * K[2]) - (U[3]) / (45. * K[4]) + (2 * U[5]) / (945. * K[6]) -
+          -((U[7]) / (4725. * K[8])) + (2 * U[9]) / (93555. * K[10]);
+    r.I = 1 / (2. * a) - u / (2. * F) + (U[2]) / (6. * K[2]) - (U[4]) / (90. * K[4]) + -((U[6]) / (945. * K[6])) -
+          (U[8]) / (9450. * K[8]) + (U[10]) / (93555. * K[10]);
+    r.J = -(a / F) + (u) / (3. * K[2]) - (U[3]) / (45. * K[4]) + -((2 * U[5]) / (945. * K[6])) -
+          (U[7]) / (4725. * K[8]) + -((2 * U[9]) / (93555. * K[10]));
+  } else {
+    const double e = exp(Re);
+    r.B = 1. / u * (1. / Re - 1. / (e - 1.));
+    r.C = (-(1. / u) + 2. * r.B) * a;
+    r.G = u / F / (1. - 1. / e);
+    r.H = 2. * a / F / (1. - 1. / e) - 1. / u;
+    r.I = u / (F * (e - 1.));
+    r.J = 2. * a / (F * (e - 1.)) - 1. / u;
+  }
+  return r;
+}
+// E_nim and F_nim (nim.f90:787-815) with D = Det
+__device__ __forceinline__ double nim1_E(const Nim1 &r, double u, double F, double D) {
+  const double a = 1.;
+  if (r.series) {
+    const Pw U(u), K(F);
+    return D / 2. + (a * D * u) / (6. * F) - (D * U[3]) / (90. * K[3]) + (D * U[5]) / (945. * K[5]) -
+           -((D * U[7]) / (9450. * K[7])) + (D * U[9]) / (93555. * K[9]);
+  }
+  return D * (1 - r.B * u);
+}
+__device__ __forceinline__ double nim1_F(const Nim1 &r, double u, double F, double D) {
+  const double a = 1.;
+  if (r.series) {
+    const Pw U(u), K(F);
+    return D / 2. - (a * D * u) / (6. * F) + (D * U[3]) / (90. * K[3]) - (D * U[5]) / (945. * K[5]) +
+           -((D * U[7]) / (9450. * K[7])) - (D * U[9]) / (93555. * K[9]);
+  }
+  return D * (r.B * u);
+}
+
+// calculate_velocity_nim_constants, first loop (nim.f90:29-83): CC .. JJ
+// and Det of every cell, then a_t (nim.f90:146-154), which needs only them.
+__global__ void __launch_bounds__(BLK) k_vel1_coef_A(Dims d, Geo g, Fields F, Phys P) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.Nc) return;
+  const size_t Nc = d.Nc;
+  const double ut = F.ct[0][c], vt = F.ct[1][c], wt = F.ct[2][c];
+  double uc[3], K[3], Re[3];
+  for (int dd = 1; dd <= 3; ++dd) {
+    uc[dd - 1] = contravariant(g.xi, Nc, c, dd, ut, vt, wt);
+    K[dd - 1] = g.gij[(size_t)(dd - 1 + 3 * (dd - 1)) * Nc + c] * P.nu;
+    Re[dd - 1] = 2 * uc[dd - 1] / K[dd - 1];
+  }
+  Nim1 r[3];
+  double C[3], E[3], Fv[3];
+  for (int k = 0; k < 3; ++k) {
+    r[k] = nim1_direction(uc[k], K[k], Re[k], P.v_limit);
+    C[k] = r[k].C;
+  }
+  const double Det = 1. / (C[0] * C[1] + C[1] * C[2] + C[0] * C[2]);
+  for (int k = 0; k < 3; ++k) {
+    E[k] = nim1_E(r[k], uc[k], K[k], Det);
+    Fv[k] = nim1_F(r[k], uc[k], K[k], Det);
+    F.N1[(size_t)(0 + k) * Nc + c] = C[k];
+    F.N1[(size_t)(3 + k) * Nc + c] = E[k];
+    F.N1[(size_t)(6 + k) * Nc + c] = Fv[k];
+    F.N1[(size_t)(9 + k) * Nc + c] = r[k].G;
+    F.N1[(size_t)(12 + k) * Nc + c] = r[k].H;
+    F.N1[(size_t)(15 + k) * Nc + c] = r[k].I;
+    F.N1[(size_t)(18 + k) * Nc + c] = r[k].J;
+  }
+  F.N1[(size_t)21 * Nc + c] = Det;
+  const double DT = P.DT;
+  double at[9];
+  at[0] = 2 * E[0] / Det - 2 * (C[1] + C[2]) * C[0] * E[0];
+  at[1] = 2 * Fv[0] / Det - 2 * (C[1] + C[2]) * C[0] * Fv[0];
+  at[2] = 2 * E[1] * C[0] * C[2];
+  at[3] = 2 * Fv[1] * C[0] * C[2];
+  at[4] = 2 * E[2] * C[0] * C[1];
+  at[5] = 2 * Fv[2] * C[0] * C[1];
+  at[6] = 2 * C[0] * C[1] * C[2] * Det;
+  at[7] = -at[6] / (2 * DT) - 1;
+  at[8] = at[6] / (2 * DT) - 1;
+  for (int k = 0; k < 9; ++k) F.AT[(size_t)k * Nc + c] = at[k];
+}
+
+// calculate_velocity_nim_constants, second loop (nim.f90:85-143): AA_vx,
+// AA_vy, AA_vz of the +r, +theta, +z faces from the cell and its neighbour.
+__global__ void __launch_bounds__(BLK) k_vel1_coef_F(Dims d, Geo g, Fields F, Phys P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Nc) return;
+  const Cell x = Cell::of(d, i);
+  const size_t Nc = d.Nc;
+  const double DT = P.DT;
+  auto C = [&](int k, int n) { return F.N1[(size_t)(k - 1) * Nc + n]; };
+  auto E = [&](int k, int n) { return F.N1[(size_t)(2 + k) * Nc + n]; };
+  auto Fv = [&](int k, int n) { return F.N1[(size_t)(5 + k) * Nc + n]; };
+  auto GG = [&](int k, int n) { return F.N1[(size_t)(8 + k) * Nc + n]; };
+  auto HH = [&](int k, int n) { return F.N1[(size_t)(11 + k) * Nc + n]; };
+  auto II = [&](int k, int n) { return F.N1[(size_t)(14 + k) * Nc + n]; };
+  auto JJ = [&](int k, int n) { return F.N1[(size_t)(17 + k) * Nc + n]; };
+  auto Det = [&](int n) { return F.N1[(size_t)21 * Nc + n]; };
+  double A[16];
+  if (x.has_nb(d, 2)) {  // face 2 (nim.f90:87-104)
+    const int i2 = x.nb(d, 2).c;
+    const double g2 = g.gfd[1 * Nc + i], g1 = g.gfd[0 * Nc + i2];
+    A[1] = -(GG(1, i) + (C(2, i) + C(3, i)) * E(1, i) * HH(1, i)) * g2;
+    A[2] = (GG(1, i) - (C(2, i) + C(3, i)) * Fv(1, i) * HH(1, i)) * g2 +
+           (II(1, i2) + (C(2, i2) + C(3, i2)) * E(1, i2) * JJ(1, i2)) * g1;
+    A[3] = -(II(1, i2) - (C(2, i2) + C(3, i2)) * Fv(1, i2) * JJ(1, i2)) * g1;
+    A[4] = C(3, i) * E(2, i) * HH(1, i) * g2;
+    A[5] = C(3, i) * Fv(2, i) * HH(1, i) * g2;
+    A[6] = -C(3, i2) * E(2, i2) * JJ(1, i2) * g1;
+    A[7] = -C(3, i2) * Fv(2, i2) * JJ(1, i2) * g1;
+    A[8] = C(2, i) * E(3, i) * HH(1, i) * g2;
+    A[9] = C(2, i) * Fv(3, i) * HH(1, i) * g2;
+    A[10] = -C(2, i2) * E(3, i2) * JJ(1, i2) * g1;
+    A[11] = -C(2, i2) * Fv(3, i2) * JJ(1, i2) * g1;
+    A[12] = C(2, i) * C(3, i) * Det(i) * HH(1, i) * g2 / (2 * DT);
+    A[13] = -C(2, i) * C(3, i) * Det(i) * HH(1, i) * g2 / (2 * DT);
+    A[14] = -C(2, i2) * C(3, i2) * Det(i2) * JJ(1, i2) * g1 / (2 * DT);
+    A[15] = C(2, i2) * C(3, i2) * Det(i2) * JJ(1, i2) * g1 / (2 * DT);
+    for (int k = 1; k <= 15; ++k) F.AAv[(size_t)(k - 1) * Nc + i] = A[k];
+  }
+  if (x.has_nb(d, 4)) {  // face 4 (nim.f90:107-124)
+    const int i2 = x.nb(d, 4).c;
+    const double g4 = g.gfd[3 * Nc + i], g3 = g.gfd[2 * Nc + i2];
+    A[1] = C(3, i) * E(1, i) * HH(2, i) * g4;
+    A[2] = C(3, i) * Fv(1, i) * HH(2, i) * g4;
+    A[3] = -C(3, i2) * E(1, i2) * JJ(2, i2) * g3;
+    A[4] = -C(3, i2) * Fv(1, i2) * JJ(2, i2) * g3;
+    A[5] = -(GG(2, i) + (C(1, i) + C(3, i)) * E(2, i) * HH(2, i)) * g4;
+    A[6] = (GG(2, i) - (C(1, i) + C(3, i)) * Fv(2, i) * HH(2, i)) * g4 +
+           (II(2, i2) + (C(1, i2) + C(3, i2)) * E(2, i2) * JJ(2, i2)) * g3;
+    A[7] = -(II(2, i2) - (C(1, i2) + C(3, i2)) * Fv(2, i2) * JJ(2, i2)) * g3;
+    A[8] = C(1, i) * E(3, i) * HH(2, i) * g4;
+    A[9] = C(1, i) * Fv(3, i) * HH(2, i) * g4;
+    A[10] = -C(1, i2) * E(3, i2) * JJ(2, i2) * g3;
+    A[11] = -C(1, i2) * Fv(3, i2) * JJ(2, i2) * g3;
+    A[12] = C(1, i) * C(3, i) * Det(i) * HH(2, i) * g4 / (2 * DT);
+    A[13] = -C(1, i) * C(3, i) * Det(i) * HH(2, i) * g4 / (2 * DT);
+    A[14] = -C(1, i2) * C(3, i2) * Det(i2) * JJ(2, i2) * g3 / (2 * DT);
+    A[15] = C(1, i2) * C(3, i2) * Det(i2) * JJ(2, i2) * g3 / (2 * DT);
+    for (int k = 1; k <= 15; ++k) F.AAv[(size_t)(14 + k) * Nc + i] = A[k];
+  }
+  if (x.has_nb(d, 6)) {  // face 6 (nim.f90:126-143)
+    const int i2 = x.nb(d, 6).c;
+    const double g6 = g.gfd[5 * Nc + i], g5 = g.gfd[4 * Nc + i2];
+    A[1] = C(2, i) * E(1, i) * HH(3, i) * g6;
+    A[2] = C(2, i) * Fv(1, i) * HH(3, i) * g6;
+    A[3] = -C(2, i2) * E(1, i2) * JJ(3, i2) * g5;
+    A[4] = -C(2, i2) * Fv(1, i2) * JJ(3, i2) * g5;
+    A[5] = C(1, i) * E(2, i) * HH(3, i) * g6;
+    A[6] = C(1, i) * Fv(2, i) * HH(3, i) * g6;
+    A[7] = -C(1, i2) * E(2, i2) * JJ(3, i2) * g5;
+    A[8] = -C(1, i2) * Fv(2, i2) * JJ(3, i2) * g5;
+    A[9] = -(GG(3, i) + (C(1, i) + C(2, i)) * E(3, i) * HH(3, i)) * g6;
+    A[10] = (GG(3, i) - (C(1, i) + C(2, i)) * Fv(3, i) * HH(3, i)) * g6 +
+            (II(3, i2) + (C(1, i2) + C(2, i2)) * E(3, i2) * JJ(3, i2)) * g5;
+    A[11] = -(II(3, i2) - (C(1, i2) + C(2, i2)) * Fv(3, i2) * JJ(3, i2)) * g5;
+    A[12] = C(1, i) * C(2, i) * Det(i) * HH(3, i) * g6 / (2 * DT);
+    A[13] = -C(1, i) * C(2, i) * Det(i) * HH(3, i) * g6 / (2 * DT);
+    A[14] = -C(1, i2) * C(2, i2) * Det(i2) * JJ(3, i2) * g5 / (2 * DT);
+    A[15] = C(1, i2) * C(2, i2) * Det(i2) * JJ(3, i2) * g5 / (2 * DT);
+    for (int k = 1; k <= 15; ++k) F.AAv[(size_t)(29 + k) * Nc + i] = A[k];
+  }
+}
+
 // =========================================================== iteration
 // Load policies: the parallel kernels read with plain (L1-cached) loads; the
-// reference-order sweeps read data that other SMs rewrote one level earlier,
-// so they load through L2 only (ld.global.cg).
+// reference-order sweeps read data that other SMs rewrote one level earlier
+// (LdCoh below).
 struct LdPlain {
   __device__ __forceinline__ static double ld(const double *p, size_t i) { return p[i]; }
 };
@@ -811,6 +1002,18 @@ __device__ __forceinline__ double face_update(const Dims &d, const double *__res
   return face_update_cv<Ld>(d, fr, Ld::ld(cv, x.c), Ld::ld(cv, x2.c), co, Fd, dg0, dg1, dd, x, x2, w);
 }
 
+// Formulation 1 cell update of one velocity component (integrate_velocity_
+// field_i, nse.f90:341-352); R = R_C + R_D + R_B of the cell, at = a_t(1:9).
+template <class Ld = LdPlain>
+__device__ __forceinline__ double cell_update_f1(const double *__restrict__ fr, const int f[7], double c, double cold,
+                                                 double R, const double at[9], double w) {
+  const double Bij = at[6] * R;
+  return (1 - w) * c + w * (-(at[0] * Ld::ld(fr, f[1])) - at[1] * Ld::ld(fr, f[2]) - at[2] * Ld::ld(fr, f[3]) -
+                            at[3] * Ld::ld(fr, f[4]) - at[4] * Ld::ld(fr, f[5]) - at[5] * Ld::ld(fr, f[6]) -
+                            at[7] * cold - Bij) /
+                           (at[8]);
+}
+
 __device__ __forceinline__ double errv(double nw, double old, bool first) { return fabs(nw - (first ? 0.0 : old)); }
 // max that keeps a NaN (fmax would drop it and hide a blow-up)
 __device__ __forceinline__ double nmax(double a, double b) { return (b > a || b != b) ? b : a; }
@@ -834,7 +1037,10 @@ __device__ __forceinline__ bool patch_cell(const Dims &d, Cell &x) {
 // Block (CB, 3): threadIdx.y = velocity component.
 // SRC_ONLY (reference-order schedule): store R_C + R_D + R_B and leave the
 // update to k_seq_vel, as update_velocity_sources precedes the sweep.
-template <bool SRC_ONLY>
+// FORM 1 (nim_formulation = 1): the a_t cell update of integrate_velocity_
+// field_i (nse.f90:341-378); the R sums are stored too, for the face sweep
+// reads them at both cells of a face.
+template <bool SRC_ONLY, int FORM>
 __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
@@ -858,14 +1064,20 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, Geo g, Fields F, Ph
     const double RB = base + P.inv_rho * green_gauss(g, NF, invV, pf, f, q);
     const double *fr = F.f[q] + par * NF;
     const double RD = P.inv_Re * diffusion_source(d, g, fr, x, f);
-    double F4[8];
-    for (int k = 0; k < 8; ++k) F4[k] = F.MF4[(size_t)k * Nc + c];
     const double B = (0. + RD + RB);
-    if (SRC_ONLY) {
-      F.Bv[(size_t)q * Nc + c] = B;
-    } else {
+    if (SRC_ONLY || FORM == 1) F.Bv[(size_t)q * Nc + c] = B;
+    if (!SRC_ONLY) {
       const double cold = F.c[q][c];
-      const double nw = cell_update(fr, f, cold, F.co[q][c], B, F4, P.w[q]);
+      double nw;
+      if (FORM == 1) {
+        double at[9];
+        for (int k = 0; k < 9; ++k) at[k] = F.AT[(size_t)k * Nc + c];
+        nw = cell_update_f1(fr, f, cold, F.co[q][c], B, at, P.w[q]);
+      } else {
+        double F4[8];
+        for (int k = 0; k < 8; ++k) F4[k] = F.MF4[(size_t)k * Nc + c];
+        nw = cell_update(fr, f, cold, F.co[q][c], B, F4, P.w[q]);
+      }
       F.c[q][c] = nw;
       e[q] = errv(nw, cold, first);
     }
@@ -1086,6 +1298,66 @@ __device__ __forceinline__ double p_face_value(const Dims &d, const Geo &g, cons
   const int fo = x.face(d, 2 * dd);
   const double w = P.w_p;
   return (1 - w) * Ld::ld(pr, fo) + w / (A[(size_t)(diag - 1) * Nc + c]) * (s + B1 + B2 + B3 + B4);
+}
+
+// ---- integrate_velocity_field_i for the +xi_dd face of cell x, one
+// component (nse.f90:378-826): the pressure sweep's ten face terms with
+// AA_v, the two cell time terms, the R sums Bq of both cells and the
+// tangential cross terms (the centred B3/B4 the source forms first are
+// overwritten before use).  fr faces, cv / co cells and old cells.
+template <class Ld>
+__device__ __forceinline__ double v1_face_value(const Dims &d, const Geo &g, const Fields &F, const Phys &P,
+                                                const double *fr, const double *cv, const double *co,
+                                                const double *Bq, const Cell &x, int dd, double w) {
+  const size_t Nc = d.Nc;
+  const int c = x.c;
+  const Cell n2 = x.nb(d, 2 * dd);
+  const double *A = F.AAv + (size_t)15 * (dd - 1) * Nc;
+  const double B1 = Bq[c] * A[12 * Nc + c] * 2 * P.DT;
+  const double B2 = Bq[n2.c] * A[14 * Nc + c] * 2 * P.DT;
+  const double B3 = (g.dg[(2 * (dd - 1)) * Nc + c]) * tangential<Ld>(d, fr, x, 2 * dd, tr1(dd));
+  const double B4 = (g.dg[(2 * (dd - 1) + 1) * Nc + c]) * tangential<Ld>(d, fr, x, 2 * dd, tr2(dd));
+  double s = 0.0;
+#pragma unroll
+  for (int t = 0; t < 10; ++t) {
+    const int pt = p_term(dd, t), coef = pt & 15, fpos = (pt >> 4) & 7, cell = pt >> 7;
+    const Cell &cl = (cell == 1) ? x : n2;
+    const double term = A[(size_t)(coef - 1) * Nc + c] * Ld::ld(fr, cl.face(d, fpos));
+    s = (t == 0) ? -term : s - term;
+  }
+  s = s - A[11 * Nc + c] * (Ld::ld(cv, c) - co[c]) - A[13 * Nc + c] * (Ld::ld(cv, n2.c) - co[n2.c]);
+  const int diag = (dd == 1) ? 2 : (dd == 2) ? 6 : 10;
+  return (1 - w) * Ld::ld(fr, x.face(d, 2 * dd)) + w / (A[(size_t)(diag - 1) * Nc + c]) * (s + B1 + B2 + B3 + B4);
+}
+
+// ---- K2 of formulation 1: +xi face updates of u, v, w (nse.f90:378-826),
+// cur -> next.  Block (CB, 3): threadIdx.y = direction.
+__global__ void __launch_bounds__(CB3, 2) k_vel1_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+  if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<3>(red);
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  Cell x;
+  const bool act = patch_cell(d, x);
+  double e[3] = {0., 0., 0.};
+  if (act) {
+    const size_t Nc = d.Nc, NF = d.NF;
+    by_dir(threadIdx.y, [&](auto D) {
+      constexpr int dd = decltype(D)::value;
+      if (!x.has_nb(d, 2 * dd)) return;
+      const int fo = x.face(d, 2 * dd);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const double *fr = F.f[q] + par * NF;
+        const double nw =
+            v1_face_value<LdPlain>(d, g, F, P, fr, F.c[q], F.co[q], F.Bv + (size_t)q * Nc, x, dd, P.w[q]);
+        F.f[q][(1 - par) * NF + fo] = nw;
+        e[q] = errv(nw, fr[fo], first);
+      }
+    });
+  }
+  block_max<3, CB3>(red, e, ctl->err[par]);
 }
 
 // ---- K5: integrate_pressure_field_i, cur -> next.
@@ -1352,9 +1624,11 @@ __global__ void k_iter_end(Ctrl *ctl, Phys P) {
 // iterates exactly.  order[] lists the cells level by level, lstart[] the
 // level boundaries.
 
-// velocity sweep (integrate_velocity_field_formulation2_i, nse.f90:831-1006).
-// Block (CB, 3): threadIdx.y = component; the three components of a cell
-// touch disjoint data, so they run side by side.
+// velocity sweep (integrate_velocity_field_formulation2_i, nse.f90:831-1006;
+// FORM 1: integrate_velocity_field_i, nse.f90:330-828).  Block (CB, 3):
+// threadIdx.y = component; the three components of a cell touch disjoint
+// data, so they run side by side.
+template <int FORM>
 __global__ void __launch_bounds__(CB3) k_seq_vel(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl,
                                                  const int *__restrict__ order, const int *__restrict__ lstart,
                                                  int nlev) {
@@ -1378,23 +1652,34 @@ __global__ void __launch_bounds__(CB3) k_seq_vel(Dims d, Geo g, Fields F, Phys P
       const Cell x = Cell::of(d, c);
       int f[7];
       cell_faces(d, x, f);
-      double F4[8];
-      for (int k = 0; k < 8; ++k) F4[k] = F.MF4[(size_t)k * Nc + c];
       const double cold = LdCoh::ld(cv, c);
-      const double nw = cell_update<LdCoh>(fr, f, cold, co[c], F.Bv[(size_t)v * Nc + c], F4, P.w[v]);
+      double nw;
+      if (FORM == 1) {
+        double at[9];
+        for (int k = 0; k < 9; ++k) at[k] = F.AT[(size_t)k * Nc + c];
+        nw = cell_update_f1<LdCoh>(fr, f, cold, co[c], F.Bv[(size_t)v * Nc + c], at, P.w[v]);
+      } else {
+        double F4[8];
+        for (int k = 0; k < 8; ++k) F4[k] = F.MF4[(size_t)k * Nc + c];
+        nw = cell_update<LdCoh>(fr, f, cold, co[c], F.Bv[(size_t)v * Nc + c], F4, P.w[v]);
+      }
       st_coh(cv, c, nw);
       e[v] = nmax(e[v], errv(nw, cold, first));
 #pragma unroll
       for (int dd = 1; dd <= 3; ++dd) {
         if (!x.has_nb(d, 2 * dd)) continue;
         const Cell x2 = x.nb(d, 2 * dd);
-        double Fd[5];
-        for (int k = 0; k < 5; ++k) Fd[k] = F.MF[(size_t)(5 * (dd - 1) + k) * Nc + c];
         const int fo = x.face(d, 2 * dd);
         const double old = LdCoh::ld(fr, fo);
-        const double nf = face_update_cv<LdCoh>(d, fr, nw, LdCoh::ld(cv, x2.c), co, Fd,
-                                                g.dg[(2 * (dd - 1)) * Nc + c], g.dg[(2 * (dd - 1) + 1) * Nc + c], dd,
-                                                x, x2, P.w[v]);
+        double nf;
+        if (FORM == 1) {
+          nf = v1_face_value<LdCoh>(d, g, F, P, fr, cv, co, F.Bv + (size_t)v * Nc, x, dd, P.w[v]);
+        } else {
+          double Fd[5];
+          for (int k = 0; k < 5; ++k) Fd[k] = F.MF[(size_t)(5 * (dd - 1) + k) * Nc + c];
+          nf = face_update_cv<LdCoh>(d, fr, nw, LdCoh::ld(cv, x2.c), co, Fd, g.dg[(2 * (dd - 1)) * Nc + c],
+                                     g.dg[(2 * (dd - 1) + 1) * Nc + c], dd, x, x2, P.w[v]);
+        }
         st_coh(fr, fo, nf);
         e[v] = nmax(e[v], errv(nf, old, first));
       }
