@@ -50,6 +50,12 @@ KERNEL_BYTES_PER_CELL = {
     "k_T_cell": 8 * 48,     # MT_A (18) faces T (3) G (3) g^ij (6) T,T_old (2); write T, MT_F (16)
     "k_T_face": 8 * 29,     # faces T (3) T,T_old (2) MT_F (15) dg (6); write faces T (3)
 }
+# DRAM bytes per cell and launch that ncu measured (dram__bytes_read.sum +
+# dram__bytes_write.sum) on the 96x96x64 case, profiles/sweep_kernels_96x96x64.md;
+# traffic grows with the cells, so roofline.traffic scales these to the run's mesh
+NCU_DRAM_BYTES_PER_CELL = {
+    "k_vel_cell": 424.3, "k_vel_face": 343.1, "k_p_src": 320.3, "k_T_coef": 273.3, "k_T_cell": 337.6,
+}
 # per cell-iteration and per step, the survey's algorithmic model (FP64)
 SURVEY_BYTES_PER_CELL_ITER = 1880
 SURVEY_BYTES_PER_CELL_STEP = 776
@@ -318,7 +324,10 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": (NCU_DRAM_BYTES_PER_CELL[dom] * case.ncells if dom in NCU_DRAM_BYTES_PER_CELL
+                                 else None),
+                     "traffic_source": "ncu dram bytes on the 96x96x64 case, scaled by cells",
                      "bytes_per_launch": KERNEL_BYTES_PER_CELL[dom] * case.ncells,
                      "kernel_ms": dom_ms,
                      "shares": {k: round(v / tot, 4) for k, v in shares.items()},
