@@ -51,14 +51,15 @@ KERNEL_BYTES_PER_CELL = {
     "k_T_face": 8 * 29,     # faces T (3) T,T_old (2) MT_F (15) dg (6); write faces T (3)
 }
 # DRAM bytes per cell and launch that ncu measured (dram__bytes_read.sum +
-# dram__bytes_write.sum) on the 96x96x64 case, profiles/sweep_kernels_96x96x64.md;
+# dram__bytes_write.sum, one --set full capture of the 96x96x64 case);
 # traffic grows with the cells, so roofline.traffic scales these to the run's mesh
 NCU_DRAM_BYTES_PER_CELL = {
     "k_vel_cell": 424.3, "k_vel_face": 343.1, "k_p_src": 320.3, "k_T_coef": 273.3, "k_T_cell": 337.6,
 }
-# per cell-iteration and per step, the survey's algorithmic model (FP64)
-SURVEY_BYTES_PER_CELL_ITER = 1880
-SURVEY_BYTES_PER_CELL_STEP = 776
+# algorithmic bytes per cell-iteration and per cell-step of the whole pass
+# (FP64, every array read and written once, implicit connectivity)
+ALGO_BYTES_PER_CELL_ITER = 1880
+ALGO_BYTES_PER_CELL_STEP = 776
 
 
 def peaks():
@@ -305,7 +306,7 @@ def main():
     dom = max(KERNEL_BYTES_PER_CELL, key=lambda k: prof.get(k, 0.0))
     dom_ms = prof[dom]
     achieved = KERNEL_BYTES_PER_CELL[dom] * case.ncells / (dom_ms / 1e3) / 1e9
-    iter_gbs = SURVEY_BYTES_PER_CELL_ITER * cell_iters / (ms / 1e3) / 1e9
+    iter_gbs = ALGO_BYTES_PER_CELL_ITER * cell_iters / (ms / 1e3) / 1e9
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -6,7 +6,7 @@
  * integral method by calling argument-less subroutines that work on module
  * globals (src/parameters.f90:222-292).  This header replaces those calls
  * with plain-C entry points taking pointers and sizes; a Fortran host binds
- * them with iso_c_binding (the interface block is in INTEGRATION.md).
+ * them with iso_c_binding through a bind(C) interface block.
  *
  * Conventions
  *   - Every entry point returns an int status: NIM_OK (0) or a negative
