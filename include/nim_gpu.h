@@ -147,7 +147,11 @@ typedef struct nim_params {
                            or 1 for the velocity NIM constants and sweep of
                            calculate_velocity_nim_constants (nim.f90:17-157)
                            and integrate_velocity_field_i (nse.f90:330-828);
-                           pressure and temperature are the same in both   */
+                           pressure and temperature are the same in both.
+                           Formulation 1's inner loop converges in the
+                           reference's Gauss-Seidel order but can diverge
+                           under NIM_SCHEDULE_PARALLEL on coarse meshes:
+                           pair it with NIM_SCHEDULE_REFERENCE            */
   int32_t reserved;     /* 0 */
 } nim_params;
 
@@ -211,6 +215,19 @@ int nim_gpu_end_step(nim_ctx *ctx, nim_step_stats *stats);
    *done (may be NULL) receives the number of steps advanced. */
 int nim_gpu_step(nim_ctx *ctx, int32_t nsteps, nim_step_stats *per_step,
                  int32_t *done);
+
+/* nim_gpu_step for n independent contexts (enclosures of any size and
+   parameters, on one device) advanced together.  No counterpart in the
+   reference, which runs one enclosure per process.  One host thread keeps
+   every context's stream fed and polls their progress, so the kernels of
+   all instances share the GPU; per instance the work and its order are
+   exactly nim_gpu_step's, so results are bit-identical to running the
+   instances one at a time.  per (may be NULL) receives n*nsteps records,
+   row i*nsteps + s for step s of instance i; done (may be NULL) receives
+   the steps each instance advanced (an instance stops early on an error or
+   the steady test).  Returns the first error any instance met, else
+   NIM_OK. */
+int nim_batch_step(int32_t n, nim_ctx *const *ctx, int32_t nsteps, nim_step_stats *per, int32_t *done);
 
 /* Copy a field to/from host memory in the reference layout (for
    write_data / write_restart / read_restart, postprocess.f90, restart.f90).

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "nim_gpu.h"
@@ -82,6 +83,14 @@ struct nim_ctx {
   int nlev = 0;
   int *border = nullptr, *blev = nullptr, *wlev = nullptr;  // wall faces, levels, per-wall level ranges
   int coop_vel = 0, coop_p = 0, coop_T = 0;  // cooperative grid sizes
+  // a time step driven without blocking (the synchronous calls and
+  // nim_batch_step share it): graph launches so far, the cap, the event that
+  // marks the last control-block (or sums) copy
+  struct Run {
+    long long launched = 0, cap = 0;
+    bool capped = false;
+    cudaEvent_t ev = nullptr;
+  } run;
   // output sets (nim_gpu_output_begin): device staging, copy stream, events
   cudaStream_t copy_stream = nullptr;
   struct Output {
@@ -573,6 +582,7 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
   TRY(noalloc_setup(x->device));
   CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&x->copy_stream, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&x->run.ev, cudaEventDisableTiming));
   x->d = make_dims(m->n_theta, m->n_r, m->n_z);
   const Dims &d = x->d;
   std::vector<int> perm;
@@ -754,32 +764,50 @@ extern "C" int nim_gpu_iterate(nim_ctx *x, int32_t n, nim_step_stats *s) {
   return x->ctl_host->status;
 }
 
-extern "C" int nim_gpu_integrate(nim_ctx *x, nim_step_stats *s) {
-  if (!x) return NIM_ERR_BAD_ARG;
-  if (!x->initialized || !x->in_step) return NIM_ERR_STATE;
-  const int G = 4;  // iterations per graph launch (per poll, reference order)
+// ---- the inner loop and the step end as non-blocking pieces.  Each piece
+// queues work on the context's stream and ends with an event (run.ev) the
+// caller waits for (cudaEventSynchronize) or polls (cudaEventQuery).
+namespace {
+const int kGraphIters = 4;  // iterations per graph launch (per poll, reference order)
+
+int ctrl_async(nim_ctx *x) {
+  CK(cudaMemcpyAsync(x->ctl_host, x->ctl, sizeof(Ctrl), cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaEventRecord(x->run.ev, x->stream));
+  return NIM_OK;
+}
+
+int iterations_launch(nim_ctx *x, int batches) {
+  const int G = kGraphIters;
+  if (x->seq) {
+    for (int k = 0; k < batches * G; ++k) TRY(launch_iteration(x));
+  } else {
+    for (int k = 0; k < batches; ++k) CK(cudaGraphLaunch(x->graph, x->stream));
+    x->launches += (long long)batches * G * x->kernels_per_iter;
+  }
+  x->run.launched += (long long)batches * G;
+  return ctrl_async(x);
+}
+
+// integrate_nse, first batch: launch ahead by the previous step's count
+int integrate_start(nim_ctx *x) {
+  const int G = kGraphIters;
   if (!x->seq && (!x->graph || x->graph_iters != G)) TRY(build_graph(x, G));
-  // launch ahead by the previous step's count, then poll
-  int ahead = std::max(1, (x->last_iters * 7 / 8) / G);
   // with max_iters <= 0 the device never stops on its own; bound the host loop
-  const long long cap = (x->params.max_iters > 0) ? (long long)x->params.max_iters + G : 100000000LL;
-  long long launched = 0;
-  bool capped = false;
-  for (;;) {
-    if (x->seq) {
-      for (int k = 0; k < ahead * G; ++k) TRY(launch_iteration(x));
-    } else {
-      for (int k = 0; k < ahead; ++k) CK(cudaGraphLaunch(x->graph, x->stream));
-      x->launches += (long long)ahead * G * x->kernels_per_iter;
+  x->run.cap = (x->params.max_iters > 0) ? (long long)x->params.max_iters + G : 100000000LL;
+  x->run.launched = 0;
+  x->run.capped = false;
+  return iterations_launch(x, std::max(1, (x->last_iters * 7 / 8) / G));
+}
+
+// after run.ev: 1 = more iterations queued; 0 = the loop has stopped and
+// the end-of-loop reductions are queued (wait for run.ev again)
+int integrate_advance(nim_ctx *x) {
+  if (!x->ctl_host->done) {
+    if (x->run.launched < x->run.cap) {
+      TRY(iterations_launch(x, 1));
+      return 1;
     }
-    launched += (long long)ahead * G;
-    TRY(read_ctrl(x));
-    if (x->ctl_host->done) break;
-    if (launched >= cap) {
-      capped = true;
-      break;
-    }
-    ahead = 1;
+    x->run.capped = true;
   }
   const Dims &d = x->d;
   k_after_integrate<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->g, x->F, x->phys, x->ctl, x->nblk_c);
@@ -787,9 +815,14 @@ extern "C" int nim_gpu_integrate(nim_ctx *x, nim_step_stats *s) {
   CK(cudaGetLastError());
   x->launches += 2;
   CK(cudaMemcpyAsync(x->host_sums, x->sums, sizeof(double), cudaMemcpyDeviceToHost, x->stream));
-  TRY(read_ctrl(x));
+  TRY(ctrl_async(x));
+  return 0;
+}
+
+int integrate_finish(nim_ctx *x, nim_step_stats *s) {
+  const Dims &d = x->d;
   x->last_iters = x->ctl_host->step_iters;
-  if (capped && x->ctl_host->status == NIM_OK) x->ctl_host->status = NIM_ERR_NOT_CONVERGED;
+  if (x->run.capped && x->ctl_host->status == NIM_OK) x->ctl_host->status = NIM_ERR_NOT_CONVERGED;
   if (s) {
     fill_iter_stats(x, s);
     s->dilatation = std::sqrt(x->host_sums[0] / d.Nc);
@@ -799,9 +832,8 @@ extern "C" int nim_gpu_integrate(nim_ctx *x, nim_step_stats *s) {
   return x->ctl_host->status;
 }
 
-extern "C" int nim_gpu_end_step(nim_ctx *x, nim_step_stats *s) {
-  if (!x) return NIM_ERR_BAD_ARG;
-  if (!x->initialized || !x->in_step) return NIM_ERR_STATE;
+// update_time_step + find_Nu2 (nse.f90:72-73), queued
+int end_start(nim_ctx *x) {
   const Dims &d = x->d;
   const int nr = 2 * d.NT * d.NZ, gn = grid(nr);
   k_update_time<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->F, x->ctl);
@@ -810,7 +842,11 @@ extern "C" int nim_gpu_end_step(nim_ctx *x, nim_step_stats *s) {
   CK(cudaGetLastError());
   x->launches += 3;
   CK(cudaMemcpyAsync(x->host_sums, x->sums, 4 * sizeof(double), cudaMemcpyDeviceToHost, x->stream));
-  CK(cudaStreamSynchronize(x->stream));
+  CK(cudaEventRecord(x->run.ev, x->stream));
+  return NIM_OK;
+}
+
+void end_finish(nim_ctx *x, nim_step_stats *s) {
   const int32_t step_done = x->STEP;
   x->STEP = x->STEP + 1;                 // nse.f90:1295
   x->TI = x->TI + 2 * x->params.DT;      // nse.f90:1296
@@ -824,6 +860,34 @@ extern "C" int nim_gpu_end_step(nim_ctx *x, nim_step_stats *s) {
     s->area_inner = sumA2;
     s->time = x->TI;
   }
+}
+
+// the steady-state exit of the time loop (nse.f90:60-69)
+bool steady_exit(const nim_ctx *x, const nim_step_stats &rec) {
+  return x->params.check_steady && rec.dudt_max < x->params.dudt_epsilon && rec.dTdt_max < x->params.dudt_epsilon;
+}
+}  // namespace
+
+extern "C" int nim_gpu_integrate(nim_ctx *x, nim_step_stats *s) {
+  if (!x) return NIM_ERR_BAD_ARG;
+  if (!x->initialized || !x->in_step) return NIM_ERR_STATE;
+  TRY(integrate_start(x));
+  for (;;) {
+    CK(cudaEventSynchronize(x->run.ev));
+    const int r = integrate_advance(x);
+    if (r < 0) return r;
+    if (r == 0) break;
+  }
+  CK(cudaEventSynchronize(x->run.ev));
+  return integrate_finish(x, s);
+}
+
+extern "C" int nim_gpu_end_step(nim_ctx *x, nim_step_stats *s) {
+  if (!x) return NIM_ERR_BAD_ARG;
+  if (!x->initialized || !x->in_step) return NIM_ERR_STATE;
+  TRY(end_start(x));
+  CK(cudaEventSynchronize(x->run.ev));
+  end_finish(x, s);
   return NIM_OK;
 }
 
@@ -845,7 +909,7 @@ extern "C" int nim_gpu_step(nim_ctx *x, int32_t nsteps, nim_step_stats *per, int
       break;
     }
     // steady-state exit of the time loop (nse.f90:60-69)
-    if (x->params.check_steady && rec.dudt_max < x->params.dudt_epsilon && rec.dTdt_max < x->params.dudt_epsilon) {
+    if (steady_exit(x, rec)) {
       rec.steady = 1;
       x->in_step = false;
       if (per) per[k] = rec;
@@ -862,6 +926,84 @@ extern "C" int nim_gpu_step(nim_ctx *x, int32_t nsteps, nim_step_stats *per, int
   }
   if (done) *done = k;
   return st;
+}
+
+// nim_gpu_step for several contexts at once: one host thread keeps every
+// context's stream fed, polling their events instead of waiting on any, so
+// the kernels of all instances share the GPU.  Per instance the calls and
+// their order are exactly nim_gpu_step's.
+extern "C" int nim_batch_step(int32_t n, nim_ctx *const *ctx, int32_t nsteps, nim_step_stats *per, int32_t *done) {
+  if (n <= 0 || !ctx || nsteps < 0) return NIM_ERR_BAD_ARG;
+  for (int32_t i = 0; i < n; ++i) {
+    if (!ctx[i]) return NIM_ERR_BAD_ARG;
+    if (!ctx[i]->initialized || ctx[i]->in_step) return NIM_ERR_STATE;
+    if (ctx[i]->device != ctx[0]->device) return NIM_ERR_BAD_ARG;
+    for (int32_t j = 0; j < i; ++j)
+      if (ctx[j] == ctx[i]) return NIM_ERR_BAD_ARG;
+  }
+  if (done)
+    for (int32_t i = 0; i < n; ++i) done[i] = 0;
+  if (nsteps == 0) return NIM_OK;
+  CK(cudaSetDevice(ctx[0]->device));
+  enum { ITER, AFTER, END, FINISHED };
+  std::vector<int> phase(n, ITER), k(n, 0);
+  std::vector<nim_step_stats> rec(n);
+  int first_error = NIM_OK;
+  auto start_step = [&](int32_t i) -> int {
+    std::memset(&rec[i], 0, sizeof(nim_step_stats));
+    TRY(nim_gpu_begin_step(ctx[i]));
+    phase[i] = ITER;
+    return integrate_start(ctx[i]);
+  };
+  auto finish = [&](int32_t i, int st) -> int {
+    if (per) per[(size_t)i * nsteps + k[i]] = rec[i];
+    ++k[i];
+    if (done) done[i] = k[i];
+    if (st != NIM_OK && first_error == NIM_OK) first_error = st;
+    if (st != NIM_OK || rec[i].steady || k[i] == nsteps) {
+      phase[i] = FINISHED;
+      return NIM_OK;
+    }
+    return start_step(i);
+  };
+  for (int32_t i = 0; i < n; ++i) TRY(start_step(i));
+  int left = n;
+  while (left > 0) {
+    bool moved = false;
+    for (int32_t i = 0; i < n; ++i) {
+      nim_ctx *x = ctx[i];
+      if (phase[i] == FINISHED) continue;
+      const cudaError_t q = cudaEventQuery(x->run.ev);
+      if (q == cudaErrorNotReady) continue;
+      CK(q);
+      moved = true;
+      if (phase[i] == ITER) {
+        const int r = integrate_advance(x);
+        if (r < 0) return r;
+        if (r == 0) phase[i] = AFTER;
+      } else if (phase[i] == AFTER) {
+        const int st = integrate_finish(x, &rec[i]);
+        rec[i].status = st;
+        if (st != NIM_OK) {
+          x->in_step = false;
+          TRY(finish(i, st));
+        } else if (steady_exit(x, rec[i])) {
+          rec[i].steady = 1;
+          x->in_step = false;
+          TRY(finish(i, NIM_OK));
+        } else {
+          TRY(end_start(x));
+          phase[i] = END;
+        }
+      } else {  // END
+        end_finish(x, &rec[i]);
+        TRY(finish(i, NIM_OK));
+      }
+      if (phase[i] == FINISHED) --left;
+    }
+    if (!moved) std::this_thread::yield();
+  }
+  return first_error;
 }
 
 extern "C" int nim_gpu_download(nim_ctx *x, nim_field f, double *host, int64_t n) {
@@ -964,6 +1106,7 @@ extern "C" void nim_gpu_destroy(nim_ctx *x) {
     if (o.copied) cudaEventDestroy(o.copied);
   }
   if (x->copy_stream) cudaStreamDestroy(x->copy_stream);
+  if (x->run.ev) cudaEventDestroy(x->run.ev);
   if (x->stream) cudaStreamDestroy(x->stream);
   delete x;
 }

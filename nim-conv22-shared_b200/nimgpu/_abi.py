@@ -156,6 +156,9 @@ def gpu_lib() -> C.CDLL:
         lib.nim_gpu_download.restype = C.c_int
         lib.nim_gpu_upload.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.c_int64]
         lib.nim_gpu_upload.restype = C.c_int
+        lib.nim_batch_step.argtypes = [C.c_int32, C.POINTER(vp), C.c_int32, C.POINTER(StepStats),
+                                       C.POINTER(C.c_int32)]
+        lib.nim_batch_step.restype = C.c_int
         lib.nim_gpu_output_bytes.argtypes = [vp, C.c_int32]
         lib.nim_gpu_output_bytes.restype = C.c_int64
         lib.nim_gpu_output_begin.argtypes = [vp, C.c_int32, vp, C.c_int64, C.POINTER(C.c_int32)]

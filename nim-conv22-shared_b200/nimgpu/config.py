@@ -139,3 +139,21 @@ CASES = {
 
 def small_case(n_theta=12, n_r=6, n_z=6, Ra=1e4, Pr=0.71, dt=1e-3, steps=5, **kw) -> Case:
     return Case("small", n_theta, n_r, n_z, Ra=Ra, Pr=Pr, dt=dt, steps=steps, **kw)
+
+
+def batch_cases(n: int = 64, seed: int = 2024, a_min: int = 24, a_max: int = 64) -> list[Case]:
+    """The seeded batch of independent enclosures: cylinder D=1, H=1 with a
+    coaxial hexagonal prism of side U[0.1, 0.3]; a x a x round(0.75 a)
+    cells with a uniform in [a_min, a_max]; Ra log-uniform in [1e3, 1e6];
+    Pr from {0.71, 7.0}; dt = 1e-3; seeded 1e-6 T noise per instance."""
+    import random
+    rng = random.Random(seed)
+    out = []
+    for q in range(n):
+        a = rng.randint(a_min, a_max)
+        side = rng.uniform(0.1, 0.3)
+        Ra = 10.0 ** rng.uniform(3.0, 6.0)
+        Pr = rng.choice((0.71, 7.0))
+        out.append(Case(f"batch{q}", a, a, max(3, round(0.75 * a)), Ra=Ra, Pr=Pr, dt=1e-3, steps=500,
+                        R_i=side, R_o=0.5, L=1.0, seed=seed + q))
+    return out

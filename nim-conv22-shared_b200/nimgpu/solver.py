@@ -168,3 +168,17 @@ class NimSolver:
 
     def add_temperature_noise(self, amp: float, seed: int):
         apply_temperature_noise(self.get, self.set, self.mesh, amp, seed)
+
+
+def batch_step(solvers, nsteps: int, raise_on_error: bool = True):
+    """nim_batch_step: advance several NimSolvers (one device) by nsteps
+    together; returns per-solver lists of step records."""
+    n = len(solvers)
+    lib = _abi.gpu_lib()
+    handles = (C.c_void_p * n)(*[s._h.value for s in solvers])
+    per = (_abi.StepStats * max(n * nsteps, 1))()
+    done = (C.c_int32 * n)()
+    st = lib.nim_batch_step(n, handles, nsteps, per, done)
+    if raise_on_error:
+        _abi.check(st, "nim_batch_step")
+    return [[per[i * nsteps + k] for k in range(done[i])] for i in range(n)]
