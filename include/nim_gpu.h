@@ -216,6 +216,13 @@ int nim_gpu_end_step(nim_ctx *ctx, nim_step_stats *stats);
 int nim_gpu_step(nim_ctx *ctx, int32_t nsteps, nim_step_stats *per_step,
                  int32_t *done);
 
+/* Inner iterations per CUDA-graph launch of nim_gpu_integrate (1..256,
+   default 4; no counterpart in the reference).  The device stops the loop
+   itself at convergence, so the results never depend on it; larger values
+   mean fewer host round trips per step (at most n-1 empty iterations are
+   launched after convergence).  Tuning knob for nim_batch_step. */
+int nim_gpu_set_graph_iters(nim_ctx *ctx, int32_t n);
+
 /* nim_gpu_step for n independent contexts (enclosures of any size and
    parameters, on one device) advanced together.  No counterpart in the
    reference, which runs one enclosure per process.  One host thread keeps

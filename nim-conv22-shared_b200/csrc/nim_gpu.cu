@@ -69,6 +69,7 @@ struct nim_ctx {
   std::vector<void *> allocs;
   cudaGraphExec_t graph = nullptr;
   int graph_iters = 0;
+  int graph_G = 4;  // inner iterations per graph launch (nim_gpu_set_graph_iters)
   bool initialized = false;
   bool in_step = false;
   int32_t STEP = 0;
@@ -768,8 +769,6 @@ extern "C" int nim_gpu_iterate(nim_ctx *x, int32_t n, nim_step_stats *s) {
 // queues work on the context's stream and ends with an event (run.ev) the
 // caller waits for (cudaEventSynchronize) or polls (cudaEventQuery).
 namespace {
-const int kGraphIters = 4;  // iterations per graph launch (per poll, reference order)
-
 int ctrl_async(nim_ctx *x) {
   CK(cudaMemcpyAsync(x->ctl_host, x->ctl, sizeof(Ctrl), cudaMemcpyDeviceToHost, x->stream));
   CK(cudaEventRecord(x->run.ev, x->stream));
@@ -777,7 +776,7 @@ int ctrl_async(nim_ctx *x) {
 }
 
 int iterations_launch(nim_ctx *x, int batches) {
-  const int G = kGraphIters;
+  const int G = x->graph_G;
   if (x->seq) {
     for (int k = 0; k < batches * G; ++k) TRY(launch_iteration(x));
   } else {
@@ -790,7 +789,7 @@ int iterations_launch(nim_ctx *x, int batches) {
 
 // integrate_nse, first batch: launch ahead by the previous step's count
 int integrate_start(nim_ctx *x) {
-  const int G = kGraphIters;
+  const int G = x->graph_G;
   if (!x->seq && (!x->graph || x->graph_iters != G)) TRY(build_graph(x, G));
   // with max_iters <= 0 the device never stops on its own; bound the host loop
   x->run.cap = (x->params.max_iters > 0) ? (long long)x->params.max_iters + G : 100000000LL;
@@ -867,6 +866,13 @@ bool steady_exit(const nim_ctx *x, const nim_step_stats &rec) {
   return x->params.check_steady && rec.dudt_max < x->params.dudt_epsilon && rec.dTdt_max < x->params.dudt_epsilon;
 }
 }  // namespace
+
+extern "C" int nim_gpu_set_graph_iters(nim_ctx *x, int32_t n) {
+  if (!x || n < 1 || n > 256) return NIM_ERR_BAD_ARG;
+  if (x->in_step) return NIM_ERR_STATE;
+  x->graph_G = n;  // the graph is rebuilt at the next integrate
+  return NIM_OK;
+}
 
 extern "C" int nim_gpu_integrate(nim_ctx *x, nim_step_stats *s) {
   if (!x) return NIM_ERR_BAD_ARG;

@@ -4,7 +4,7 @@ include/nim_gpu.h.  The Python layer only marshals arrays."""
 from . import _abi, config
 from ._abi import NimError, StepStats, Params, MeshParams
 from .mesh import Mesh, temperature_noise, apply_temperature_noise
-from .solver import NimSolver, batch_step, field_len
+from .solver import NimSolver, autotune_batch, batch_step, field_len
 
 __all__ = ["_abi", "config", "NimError", "StepStats", "Params", "MeshParams", "Mesh",
-           "temperature_noise", "apply_temperature_noise", "NimSolver", "batch_step", "field_len"]
+           "temperature_noise", "apply_temperature_noise", "NimSolver", "autotune_batch", "batch_step", "field_len"]

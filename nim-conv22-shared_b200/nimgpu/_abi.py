@@ -156,6 +156,8 @@ def gpu_lib() -> C.CDLL:
         lib.nim_gpu_download.restype = C.c_int
         lib.nim_gpu_upload.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.c_int64]
         lib.nim_gpu_upload.restype = C.c_int
+        lib.nim_gpu_set_graph_iters.argtypes = [vp, C.c_int32]
+        lib.nim_gpu_set_graph_iters.restype = C.c_int
         lib.nim_batch_step.argtypes = [C.c_int32, C.POINTER(vp), C.c_int32, C.POINTER(StepStats),
                                        C.POINTER(C.c_int32)]
         lib.nim_batch_step.restype = C.c_int

@@ -157,6 +157,10 @@ class NimSolver:
                                                  C.byref(t)), "nim_gpu_output_begin")
         return t.value
 
+    def set_graph_iters(self, n: int):
+        """Inner iterations per graph launch (results do not depend on it)."""
+        _abi.check(self.lib.nim_gpu_set_graph_iters(self._h, n), "nim_gpu_set_graph_iters")
+
     def output_wait(self, ticket: int):
         _abi.check(self.lib.nim_gpu_output_wait(self._h, ticket), "nim_gpu_output_wait")
 
@@ -182,3 +186,27 @@ def batch_step(solvers, nsteps: int, raise_on_error: bool = True):
     if raise_on_error:
         _abi.check(st, "nim_batch_step")
     return [[per[i * nsteps + k] for k in range(done[i])] for i in range(n)]
+
+
+def autotune_batch(solvers, candidates=(4, 8, 16, 32), steps_each: int = 1):
+    """Pick the graph length of a batch by measurement: advance the batch
+    steps_each steps with each candidate (these are real steps of the run:
+    the iterates do not depend on the graph length) and keep the fastest
+    per cell-iteration.  Returns (best, {candidate: seconds per
+    cell-iteration}, records of the steps taken)."""
+    import time
+    timing, recs_all = {}, []
+    cells = [s.mesh.nmesh for s in solvers]
+    for g in candidates:
+        for s in solvers:
+            s.set_graph_iters(g)
+        t0 = time.perf_counter()
+        recs = batch_step(solvers, steps_each)
+        dt = time.perf_counter() - t0
+        work = sum(c * sum(r.iters for r in rr) for c, rr in zip(cells, recs))
+        timing[g] = dt / max(work, 1)
+        recs_all.append(recs)
+    best = min(timing, key=timing.get)
+    for s in solvers:
+        s.set_graph_iters(best)
+    return best, timing, recs_all

@@ -70,3 +70,27 @@ def test_batch_arguments():
     h = (C.c_void_p * 2)(s._h.value, s._h.value)
     assert lib.nim_batch_step(2, h, 1, None, None) == _abi.NIM_ERR_BAD_ARG  # the same context twice
     s.close()
+
+
+def test_graph_length_does_not_change_results():
+    case = config.small_case(16, 5, 7)
+    outs = []
+    for g in (1, 4, 32):
+        s = make(case)
+        s.set_graph_iters(g)
+        recs = s.solve_nse(2)
+        outs.append(([r.iters for r in recs], [s.download(f) for f in STATE]))
+        s.close()
+    for it, fields in outs[1:]:
+        assert it == outs[0][0]
+        for a, b in zip(fields, outs[0][1]):
+            assert np.array_equal(a, b)
+
+
+def test_autotune_picks_a_candidate():
+    cases = config.batch_cases(3, seed=5, a_min=8, a_max=12)
+    solvers = [make(c) for c in cases]
+    best, timing, recs = nimgpu.autotune_batch(solvers, candidates=(2, 8), steps_each=1)
+    assert best in (2, 8) and set(timing) == {2, 8} and len(recs) == 2
+    for s in solvers:
+        s.close()
