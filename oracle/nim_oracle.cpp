@@ -1189,10 +1189,15 @@ void iteration(nim_oracle &o) {
       }
     }
   } else {
+    // every parallel-schedule loop reads only values from before the loop,
+    // so its threads write disjoint entries and the result is thread-count
+    // independent
+#pragma omp parallel for schedule(static) num_threads(nt)
     for (int64_t i = 1; i <= N; ++i)
       for (int k = 0; k < 3; ++k) (*vc[k])(i) = vcell(k, i);
     for (int k = 0; k < 3; ++k) {
       o.snap.d = vf[k]->d;
+#pragma omp parallel for schedule(static) num_threads(nt)
       for (int64_t i = 1; i <= N; ++i)
         for (int d = 1; d <= 3; ++d)
           if (o.NB(2 * d, i) != 0) (*vf[k])(o.F(2 * d, i)) = vface(k, o.snap, d, i);
@@ -1211,9 +1216,11 @@ void iteration(nim_oracle &o) {
       for (int d = 1, n = (int)o.cord[q]; d <= 3; ++d)
         if (o.faces_BC[o.F(2 * d, n)] == 1) o.fp(o.F(2 * d, n)) = pressure_face(o, o.fp, d, n);
   } else {
+#pragma omp parallel for schedule(static) num_threads(nt)
     for (int64_t b = 1; b <= o.NBF; ++b) o.pb_new(b) = pressure_bc_face(o, o.fp, b);
     for (int64_t b = 1; b <= o.NBF; ++b) o.fp(o.F(o.BCpos[b], o.BCm[b])) = o.pb_new(b);
     o.snap.d = o.fp.d;
+#pragma omp parallel for schedule(static) num_threads(nt)
     for (int64_t n = 1; n <= N; ++n)
       for (int d = 1; d <= 3; ++d)
         if (o.faces_BC[o.F(2 * d, n)] == 1) o.fp(o.F(2 * d, n)) = pressure_face(o, o.snap, d, n);
@@ -1233,9 +1240,11 @@ void iteration(nim_oracle &o) {
         if (o.NB(2 * d, i) != 0) o.fT(o.F(2 * d, i)) = face_update(o, o.fT, o.Txyz, o.Told, *MTF[d - 1], d, i, o.P.w_T);
     }
   } else {
+#pragma omp parallel for schedule(static) num_threads(nt)
     for (int64_t i = 1; i <= N; ++i)
       o.Txyz(i) = cell_update(o, o.fT, o.Txyz(i), o.Told(i), (o.RDT(i) + 0.), o.MTF4, i, o.P.w_T);
     o.snap.d = o.fT.d;
+#pragma omp parallel for schedule(static) num_threads(nt)
     for (int64_t i = 1; i <= N; ++i)
       for (int d = 1; d <= 3; ++d)
         if (o.NB(2 * d, i) != 0) o.fT(o.F(2 * d, i)) = face_update(o, o.snap, o.Txyz, o.Told, *MTF[d - 1], d, i, o.P.w_T);
