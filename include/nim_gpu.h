@@ -270,13 +270,14 @@ int nim_gpu_output_wait(nim_ctx *ctx, int32_t ticket);
    nim_gpu_stream: the cudaStream_t every call of the context queues work on,
    so a caller can record CUDA events on it.
    nim_gpu_launch_count: kernels launched by the context since creation.
-   nim_gpu_profile_iterations: n inner passes launched one kernel at a time
-   with CUDA events around each; ms[k] receives the mean duration of kernel
-   k (names from nim_gpu_kernel_name); returns the number of kernels. */
+   nim_gpu_profile_iterations: n inner passes of the context's schedule and
+   formulation, launched one kernel at a time with a CUDA event after each;
+   ms[k] receives the mean time of launch group k (its name from
+   nim_gpu_profile_name), at most cap of them; returns their number. */
 void *nim_gpu_stream(nim_ctx *ctx);
 int64_t nim_gpu_launch_count(nim_ctx *ctx);
 int nim_gpu_profile_iterations(nim_ctx *ctx, int32_t n, double *ms, int32_t cap);
-const char *nim_gpu_kernel_name(int32_t k);
+const char *nim_gpu_profile_name(nim_ctx *ctx, int32_t k);
 
 /* Wall-face limit of nim_gpu_nusselt_noalloc: 2*n_theta*n_z inner plus
    outer wall faces, i.e. 4096 blocks of 256 faces. */

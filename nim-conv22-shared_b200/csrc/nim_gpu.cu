@@ -17,6 +17,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -84,6 +85,14 @@ struct nim_ctx {
   int nlev = 0;
   int *border = nullptr, *blev = nullptr, *wlev = nullptr;  // wall faces, levels, per-wall level ranges
   int coop_vel = 0, coop_p = 0, coop_T = 0;  // cooperative grid sizes
+  // nim_gpu_profile_iterations: while set, every kernel launch of an
+  // iteration is followed by an event and its name
+  struct Marks {
+    std::vector<cudaEvent_t> ev;
+    std::vector<const char *> name;
+    size_t used = 0;
+  } *marks = nullptr;
+  std::vector<std::string> prof_names;  // names of the last profile
   // a time step driven without blocking (the synchronous calls and
   // nim_batch_step share it): graph launches so far, the cap, the event that
   // marks the last control-block (or sums) copy
@@ -215,17 +224,37 @@ Phys make_phys(const nim_params &p) {
   return P;
 }
 
+// after a kernel launch: an event named for it, when profiling
+int mark(nim_ctx *x, const char *name) {
+  nim_ctx::Marks *m = x->marks;
+  if (!m) return NIM_OK;
+  if (m->used == m->ev.size()) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    m->ev.push_back(e);
+    m->name.push_back(nullptr);
+  }
+  m->name[m->used] = name;
+  CK(cudaEventRecord(m->ev[m->used++], x->stream));
+  return NIM_OK;
+}
+
 // the velocity sources + cell kernel and the face kernel of the context's
 // formulation (parallel schedule)
-void launch_vel(nim_ctx *x, cudaStream_t s) {
+int launch_vel(nim_ctx *x, cudaStream_t s) {
   const Dims &d = x->d;
   if (x->phys.formulation == 1) {
     k_vel_cell<false, 1><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    TRY(mark(x, "k_vel_cell"));
     k_vel1_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    TRY(mark(x, "k_vel1_face"));
   } else {
     k_vel_cell<false, 2><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    TRY(mark(x, "k_vel_cell"));
     k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    TRY(mark(x, "k_vel_face"));
   }
+  return NIM_OK;
 }
 
 template <typename K>
@@ -249,21 +278,35 @@ int launch_iteration_seq(nim_ctx *x) {
   cudaStream_t s = x->stream;
   if (x->phys.formulation == 1) {
     k_vel_cell<true, 1><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    TRY(mark(x, "k_vel_cell(src)"));
     TRY(launch_coop(k_seq_vel<1>, x->coop_vel, dim3(CB, 3), x));
   } else {
     k_vel_cell<true, 2><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    TRY(mark(x, "k_vel_cell(src)"));
     TRY(launch_coop(k_seq_vel<2>, x->coop_vel, dim3(CB, 3), x));
   }
+  TRY(mark(x, "k_seq_vel"));
   k_p_src<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  TRY(mark(x, "k_p_src"));
   k_seq_pbc<<<2, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl, x->border, x->blev, x->wlev, 0);
   k_seq_pbc<<<2, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl, x->border, x->blev, x->wlev, 2);
+  TRY(mark(x, "k_seq_pbc"));
   TRY(launch_coop(k_seq_p, x->coop_p, dim3(BLK), x));
-  if (x->phys.dpdx_tolerance) k_p_dpdx<<<x->nblk_c, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+  TRY(mark(x, "k_seq_p"));
+  if (x->phys.dpdx_tolerance) {
+    k_p_dpdx<<<x->nblk_c, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+    TRY(mark(x, "k_p_dpdx"));
+  }
   k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+  TRY(mark(x, "k_zero_flux"));
   k_T_coef<<<dim3(3, x->nblk_c), BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  TRY(mark(x, "k_T_coef"));
   k_T_cell<true><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  TRY(mark(x, "k_T_cell(src)"));
   TRY(launch_coop(k_seq_T, x->coop_T, dim3(BLK), x));
+  TRY(mark(x, "k_seq_T"));
   k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
+  TRY(mark(x, "k_iter_end"));
   CK(cudaGetLastError());
   x->kernels_per_iter = x->phys.dpdx_tolerance ? 12 : 11;
   x->launches += x->kernels_per_iter;
@@ -277,17 +320,29 @@ int launch_iteration(nim_ctx *x) {
   cudaStream_t s = x->stream;
   const int gc = x->nblk_c, gb = x->nblk_b;
   const dim3 g3 = x->g3, g8 = x->g8;
-  launch_vel(x, s);
+  TRY(launch_vel(x, s));
   k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  TRY(mark(x, "k_p_src"));
   k_p_bc<<<gb, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  TRY(mark(x, "k_p_bc"));
   k_p_bc_copy<<<gb, BLK, 0, s>>>(d, x->F, x->ctl);
+  TRY(mark(x, "k_p_bc_copy"));
   k_p_face<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-  if (x->phys.dpdx_tolerance) k_p_dpdx<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+  TRY(mark(x, "k_p_face"));
+  if (x->phys.dpdx_tolerance) {
+    k_p_dpdx<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+    TRY(mark(x, "k_p_dpdx"));
+  }
   k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+  TRY(mark(x, "k_zero_flux"));
   k_T_coef<<<dim3(3, x->nblk_c), BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  TRY(mark(x, "k_T_coef"));
   k_T_cell<false><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  TRY(mark(x, "k_T_cell"));
   k_T_face<<<g8, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  TRY(mark(x, "k_T_face"));
   k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
+  TRY(mark(x, "k_iter_end"));
   CK(cudaGetLastError());
   x->kernels_per_iter = x->phys.dpdx_tolerance ? 12 : 11;
   x->launches += x->kernels_per_iter;
@@ -1120,74 +1175,58 @@ extern "C" void nim_gpu_destroy(nim_ctx *x) {
 extern "C" void *nim_gpu_stream(nim_ctx *x) { return x ? (void *)x->stream : nullptr; }
 extern "C" int64_t nim_gpu_launch_count(nim_ctx *x) { return x ? x->launches : -1; }
 
-static const char *kKernelNames[] = {"k_vel_cell", "k_vel_face", "k_p_src",  "k_p_bc",   "k_p_bc_copy",
-                                     "k_p_face",   "k_p_dpdx",   "k_zero_flux", "k_T_coef", "k_T_cell",
-                                     "k_T_face",   "k_iter_end"};
-extern "C" const char *nim_gpu_kernel_name(int32_t k) {
-  return (k >= 0 && k < (int32_t)(sizeof(kKernelNames) / sizeof(kKernelNames[0]))) ? kKernelNames[k] : "";
-}
-
 extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int32_t cap) {
-  const int NK = 12;
-  if (!x || n <= 0 || !ms || cap < NK) return NIM_ERR_BAD_ARG;
+  if (!x || n <= 0 || !ms || cap <= 0) return NIM_ERR_BAD_ARG;
   if (!x->initialized) return NIM_ERR_STATE;
-  if (x->seq) return NIM_ERR_STATE;  // times the parallel-schedule kernels
-  const Dims &d = x->d;
   cudaStream_t s = x->stream;
-  cudaEvent_t ev[NK + 1];
-  for (int k = 0; k <= NK; ++k) CK(cudaEventCreate(&ev[k]));
-  double acc[NK] = {0};
   const Phys keep = x->phys;
   x->phys.max_iters = 0;
   for (int q = 0; q < 5; ++q) x->phys.tol[q] = -1.0;
-  k_step_reset<<<1, 1, 0, s>>>(x->ctl);
-  const int gc = x->nblk_c, gb = x->nblk_b;
-  const dim3 g3 = x->g3, g8 = x->g8;
-  for (int it = 0; it < n; ++it) {
-    CK(cudaEventRecord(ev[0], s));
-    if (x->phys.formulation == 1) {
-      k_vel_cell<false, 1><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-      CK(cudaEventRecord(ev[1], s));
-      k_vel1_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-    } else {
-      k_vel_cell<false, 2><<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-      CK(cudaEventRecord(ev[1], s));
-      k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  nim_ctx::Marks marks;
+  cudaEvent_t start = nullptr;
+  std::vector<double> acc;
+  std::vector<const char *> names;
+  int st = NIM_OK;
+  if (cudaEventCreate(&start) != cudaSuccess) st = NIM_ERR_CUDA;
+  if (st == NIM_OK) {
+    k_step_reset<<<1, 1, 0, s>>>(x->ctl);
+    x->marks = &marks;
+    for (int it = 0; it < n && st == NIM_OK; ++it) {
+      marks.used = 0;
+      if (cudaEventRecord(start, s) != cudaSuccess) {
+        st = NIM_ERR_CUDA;
+        break;
+      }
+      st = launch_iteration(x);
+      if (st != NIM_OK) break;
+      if (cudaEventSynchronize(marks.ev[marks.used - 1]) != cudaSuccess) {
+        st = NIM_ERR_CUDA;
+        break;
+      }
+      if (it == 0) {
+        names.assign(marks.name.begin(), marks.name.begin() + marks.used);
+        acc.assign(marks.used, 0.0);
+      }
+      for (size_t k = 0; k < marks.used && k < acc.size(); ++k) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, k ? marks.ev[k - 1] : start, marks.ev[k]);
+        acc[k] += t;
+      }
     }
-    CK(cudaEventRecord(ev[2], s));
-    k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-    CK(cudaEventRecord(ev[3], s));
-    k_p_bc<<<gb, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-    CK(cudaEventRecord(ev[4], s));
-    k_p_bc_copy<<<gb, BLK, 0, s>>>(d, x->F, x->ctl);
-    CK(cudaEventRecord(ev[5], s));
-    k_p_face<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-    CK(cudaEventRecord(ev[6], s));
-    if (x->phys.dpdx_tolerance) k_p_dpdx<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
-    CK(cudaEventRecord(ev[7], s));
-    k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
-    CK(cudaEventRecord(ev[8], s));
-    k_T_coef<<<dim3(3, x->nblk_c), BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-    CK(cudaEventRecord(ev[9], s));
-    k_T_cell<false><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-    CK(cudaEventRecord(ev[10], s));
-    k_T_face<<<g8, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
-    CK(cudaEventRecord(ev[11], s));
-    k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
-    CK(cudaEventRecord(ev[12], s));
-    CK(cudaGetLastError());
-    CK(cudaEventSynchronize(ev[12]));
-    for (int k = 0; k < NK; ++k) {
-      float t = 0.f;
-      CK(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
-      acc[k] += t;
-    }
-    x->launches += x->phys.dpdx_tolerance ? 12 : 11;
+    x->marks = nullptr;
   }
   x->phys = keep;
-  for (int k = 0; k <= NK; ++k) cudaEventDestroy(ev[k]);
-  for (int k = 0; k < NK; ++k) ms[k] = acc[k] / n;
-  return NK;
+  for (cudaEvent_t e : marks.ev) cudaEventDestroy(e);
+  if (start) cudaEventDestroy(start);
+  if (st != NIM_OK) return st;
+  const int nk = std::min((int)acc.size(), (int)cap);
+  x->prof_names.assign(names.begin(), names.begin() + nk);
+  for (int k = 0; k < nk; ++k) ms[k] = acc[k] / n;
+  return nk;
+}
+
+extern "C" const char *nim_gpu_profile_name(nim_ctx *x, int32_t k) {
+  return (x && k >= 0 && k < (int32_t)x->prof_names.size()) ? x->prof_names[k].c_str() : "";
 }
 
 extern "C" int nim_gpu_nusselt_noalloc(nim_ctx *x, double *out4) {

@@ -177,8 +177,8 @@ def gpu_lib() -> C.CDLL:
         lib.nim_gpu_launch_count.restype = C.c_int64
         lib.nim_gpu_profile_iterations.argtypes = [vp, C.c_int32, C.POINTER(C.c_double), C.c_int32]
         lib.nim_gpu_profile_iterations.restype = C.c_int
-        lib.nim_gpu_kernel_name.argtypes = [C.c_int32]
-        lib.nim_gpu_kernel_name.restype = C.c_char_p
+        lib.nim_gpu_profile_name.argtypes = [vp, C.c_int32]
+        lib.nim_gpu_profile_name.restype = C.c_char_p
         lib.nim_gpu_nusselt_noalloc.argtypes = [vp, C.POINTER(C.c_double)]
         lib.nim_gpu_nusselt_noalloc.restype = C.c_int
         _gpu = lib

@@ -113,12 +113,13 @@ class NimSolver:
         return int(self.lib.nim_gpu_launch_count(self._h))
 
     def profile_iterations(self, n: int) -> dict:
-        """Mean device time (ms) of each kernel over n un-graphed passes."""
+        """Mean device time (ms) of each kernel (launch group) over n
+        un-graphed passes of the context's schedule."""
         ms = (C.c_double * 32)()
         nk = self.lib.nim_gpu_profile_iterations(self._h, n, ms, 32)
         if nk < 0:
             _abi.check(nk, "nim_gpu_profile_iterations")
-        return {self.lib.nim_gpu_kernel_name(k).decode(): ms[k] for k in range(nk)}
+        return {self.lib.nim_gpu_profile_name(self._h, k).decode(): ms[k] for k in range(nk)}
 
     def synchronize(self):
         _abi.check(self.lib.nim_gpu_synchronize(self._h), "nim_gpu_synchronize")

@@ -121,10 +121,11 @@ def test_reference_order_runs_are_deterministic_and_roundtrip():
         assert np.array_equal(a, b)
 
 
-def test_reference_order_refuses_kernel_profile():
+def test_reference_order_kernel_profile():
     case = config.small_case()
     _, gpu, _ = pair(case.mesh_params(), case.params())
-    with pytest.raises(nimgpu.NimError) as e:
-        gpu.profile_iterations(2)
-    assert e.value.status == _abi.NIM_ERR_STATE
+    prof = gpu.profile_iterations(2)
+    assert list(prof) == ["k_vel_cell(src)", "k_seq_vel", "k_p_src", "k_seq_pbc", "k_seq_p", "k_zero_flux",
+                          "k_T_coef", "k_T_cell(src)", "k_seq_T", "k_iter_end"]
+    assert all(v > 0 for v in prof.values())
     gpu.close()
