@@ -161,6 +161,21 @@ def cpu_sample(case, threads: int, iters: int, schedule: int):
     return case.ncells * iters / dt, dt
 
 
+def combine_ranks(pg, t, work, device="cuda"):
+    """Replicas on N ranks: the job takes as long as its slowest rank and
+    does the sum of the ranks' work.  pg is torch.distributed (or None for
+    one rank); device is where the reduction tensors live (cuda for nccl,
+    cpu for gloo)."""
+    if pg is None:
+        return t, work
+    import torch
+    tt = torch.tensor([float(t)], dtype=torch.float64, device=device)
+    pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+    ww = torch.tensor([float(work)], dtype=torch.float64, device=device)
+    pg.all_reduce(ww, op=pg.ReduceOp.SUM)
+    return float(tt.item()), float(ww.item())
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference algorithm on the host cores."""
     if rank != 0:
@@ -328,15 +343,7 @@ def main():
     ms = ev0.elapsed_time(ev1)
     iters = sum(s.iters for s in stats)
     cell_iters = case.ncells * iters
-    t_max = ms
-    total = cell_iters
-    if pg:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_max = float(t.item())
-        c = torch.tensor([float(cell_iters)], dtype=torch.float64, device="cuda")
-        pg.all_reduce(c, op=pg.ReduceOp.SUM)
-        total = float(c.item())
+    t_max, total = combine_ranks(pg, ms, cell_iters)
     value = total / (t_max / 1e3)
 
     # ---------------- end to end through the C ABI with host buffers: the
@@ -367,13 +374,7 @@ def main():
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e_total = case.ncells * e2e_iters
-    if pg:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
-        c = torch.tensor([float(e2e_total)], dtype=torch.float64, device="cuda")
-        pg.all_reduce(c, op=pg.ReduceOp.SUM)
-        e2e_total = float(c.item())
+    e2e_s, e2e_total = combine_ranks(pg, e2e_s, e2e_total)
     e2e_value = e2e_total / e2e_s
 
     # ---------------- roofline of the dominant kernel (events per kernel)
