@@ -56,6 +56,10 @@ KERNEL_BYTES_PER_CELL = {
     "k_T_coef": 8 * 42,     # cells+old u,v,w (6) xi (9) g^ij diagonal (3) gfd (6); write MT_A (18)
     "k_T_cell": 8 * 48,     # MT_A (18) faces T (3) G (3) g^ij (6) T,T_old (2); write T, MT_F (16)
     "k_T_face": 8 * 29,     # faces T (3) T,T_old (2) MT_F (15) dg (6); write faces T (3)
+    # the reference-order sweeps (--schedule reference), in place
+    "k_seq_vel": 8 * 59,    # cells+old u,v,w (6) faces u,v,w (9) M_F4 (8) R sums (3) M_F1..3 (15) dg (6); write cells, faces (12)
+    "k_seq_p": 8 * 52,      # faces p (3) R_p (1) AA used (39) dg (6); write faces p (3)
+    "k_seq_T": 8 * 39,      # T,T_old (2) faces T (3) MT_F4 (8) R_D_T (1) MT_F (15) dg (6); write T, faces (4)
 }
 # DRAM bytes per cell and launch that ncu measured (dram__bytes_read.sum +
 # dram__bytes_write.sum, one --set full capture of the 96x96x64 case);
@@ -296,6 +300,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--case", default=CASE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--schedule", default="parallel", choices=["parallel", "reference"],
+                    help="reference: the Gauss-Seidel sweeps in the reference's cell order (its iterates)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -317,7 +323,8 @@ def main():
 
     case = config.CASES[args.case]
     mesh = nimgpu.Mesh(case.mesh_params())
-    solver = nimgpu.NimSolver(mesh, case.params())
+    sched = _abi.SCHEDULE_REFERENCE if args.schedule == "reference" else _abi.SCHEDULE_PARALLEL
+    solver = nimgpu.NimSolver(mesh, case.params(schedule=sched))
     solver.initialize_nse()
     solver.add_temperature_noise(case.noise, case.seed)
     stream = torch.cuda.ExternalStream(solver.stream_handle)
@@ -382,7 +389,7 @@ def main():
     peak, peak_kind = peaks()
     shares = {k: v for k, v in prof.items() if v > 0}
     tot = sum(shares.values())
-    dom = max(KERNEL_BYTES_PER_CELL, key=lambda k: prof.get(k, 0.0))
+    dom = max((k for k in KERNEL_BYTES_PER_CELL if k in prof), key=lambda k: prof[k])
     dom_ms = prof[dom]
     achieved = KERNEL_BYTES_PER_CELL[dom] * case.ncells / (dom_ms / 1e3) / 1e9
     iter_gbs = ALGO_BYTES_PER_CELL_ITER * cell_iters / (ms / 1e3) / 1e9
@@ -398,7 +405,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / max(args.steps, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded mesh and T noise)",
-        "config": workload_config(case),
+        "config": dict(workload_config(case), schedule=args.schedule),
         "iterations": iters, "iters_per_step": iters / max(len(stats), 1),
         "hbm_gbs_iteration": iter_gbs,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
