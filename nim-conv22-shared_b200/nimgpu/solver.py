@@ -125,9 +125,15 @@ class NimSolver:
         _abi.check(self.lib.nim_gpu_synchronize(self._h), "nim_gpu_synchronize")
 
     # -- host copies (write_data / write_restart / read_restart)
-    def download(self, field: int) -> np.ndarray:
+    def download(self, field: int, out: np.ndarray | None = None) -> np.ndarray:
+        """The field in the reference layout, into out when given (a
+        contiguous float64 array, e.g. a view of page-locked memory, which
+        the copy then lands in directly), else into a new array."""
         n = field_len(field, self.mesh)
-        out = np.empty(n, dtype=np.float64)
+        if out is None:
+            out = np.empty(n, dtype=np.float64)
+        elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size < n:
+            raise ValueError("out must be a contiguous float64 array of at least the field's length")
         _abi.check(self.lib.nim_gpu_download(self._h, field, out.ctypes.data_as(C.POINTER(C.c_double)), n),
                    "nim_gpu_download")
         return out

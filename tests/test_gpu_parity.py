@@ -195,6 +195,8 @@ def test_download_upload_roundtrip():
         v = rng.standard_normal(nimgpu.field_len(f, mesh))
         gpu.upload(f, v)
         assert np.array_equal(gpu.download(f), v)
+        out = np.full(v.size, np.nan)
+        assert gpu.download(f, out=out) is out and np.array_equal(out, v)
 
 
 def test_runs_are_bitwise_deterministic():
