@@ -20,6 +20,12 @@ the host cores on the same workload, one inner iteration per step.
 --case batch times the batched extension instead: 64 seeded enclosures of
 uneven size (a x a x 0.75a cells, a in [24, 64]) and Ra, Pr advanced
 together by nim_batch_step, against the same 64 cases run one at a time.
+
+On one GPU the line also carries "mixed": the same steps from the same
+start with nim_params.precision = NIM_PRECISION_MIXED (FP32 passes, then
+FP64 passes to the reference's stop test), its throughput, its roofline and
+its per-step Nusselt and final field errors against the FP64 run.
+--precision mixed makes the mixed path the headline arm instead.
 """
 from __future__ import annotations
 
@@ -228,10 +234,11 @@ def run_batch(args, rank, world, local):
     nim_batch_step, against the same cases one at a time (nim_gpu_step per
     instance).  Wall clock between device-wide synchronisations: the batch
     spans 64 streams and its host-side scheduling is part of what is
-    measured."""
+    measured.  With --precision mixed the batch runs the mixed path and the
+    one-at-a-time baseline stays FP64."""
     import torch
     import nimgpu
-    from nimgpu import config
+    from nimgpu import config, _abi
 
     torch.cuda.set_device(local)
     if world > 1 and rank != 0:
@@ -239,10 +246,12 @@ def run_batch(args, rank, world, local):
     cases = config.batch_cases(64)
     steps = max(args.steps // 5, 1)
 
-    def build():
+    prec = _abi.PRECISION_MIXED if args.precision == "mixed" else _abi.PRECISION_FP64
+
+    def build(precision):
         out = []
         for c in cases:
-            s = nimgpu.NimSolver(nimgpu.Mesh(c.mesh_params()), c.params())
+            s = nimgpu.NimSolver(nimgpu.Mesh(c.mesh_params()), c.params(precision=precision))
             s.initialize_nse()
             s.add_temperature_noise(c.noise, c.seed)
             out.append(s)
@@ -251,7 +260,7 @@ def run_batch(args, rank, world, local):
     def cells_iters(recs_per_instance):
         return sum(c.ncells * sum(r.iters for r in recs) for c, recs in zip(cases, recs_per_instance))
 
-    solvers = build()
+    solvers = build(prec)
     # warm-up steps double as the autotuner's trials of the graph length
     best_g, tune, _ = nimgpu.autotune_batch(solvers, candidates=(4, 8, 16, 32), steps_each=1)
     torch.cuda.synchronize()
@@ -261,7 +270,7 @@ def run_batch(args, rank, world, local):
     tb = time.perf_counter() - t0
     for s in solvers:
         s.close()
-    solvers = build()
+    solvers = build(_abi.PRECISION_FP64)
     for s in solvers:
         s.solve_nse(4)  # the batch's warm-up / tuning steps
     torch.cuda.synchronize()
@@ -273,23 +282,81 @@ def run_batch(args, rank, world, local):
         s.close()
     vb, v1 = cells_iters(recs_b) / tb, cells_iters(recs_1) / t1
     same = [[r.iters for r in a] == [r.iters for r in b] for a, b in zip(recs_b, recs_1)]
+    nu_err = max(abs(a[-1].nu_inner - b[-1].nu_inner) / abs(b[-1].nu_inner) for a, b in zip(recs_b, recs_1))
     line = {
         "metric": METRIC, "value": vb, "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": max(args.warmup, 1),
         "ms_per_step": 1e3 * tb / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "warmup_note": "4 warm-up steps, one per autotuner candidate",
-        "dtype": "f64", "data": "synthetic (seeded meshes, physics and T noise)",
+        "dtype": "f64" if prec == _abi.PRECISION_FP64 else "f32+f64", "precision": args.precision,
+        "data": "synthetic (seeded meshes, physics and T noise)",
         "config": {"workload": "batch: 64 cylinder enclosures D=1 H=1, hexagon side U[0.1,0.3], "
                                "a x a x round(0.75a) cells, a in [24,64], Ra log-uniform [1e3,1e6], "
                                "Pr in {0.71, 7.0}, dt=1e-3",
                    "cells": sum(c.ncells for c in cases), "instances": len(cases),
                    "timing": "wall clock between device synchronisations"},
-        "one_at_a_time": {"value": v1, "unit": UNIT, "ms_per_step": 1e3 * t1 / steps},
+        "one_at_a_time": {"value": v1, "unit": UNIT, "ms_per_step": 1e3 * t1 / steps, "precision": "fp64"},
+        "nu_inner_rel_err_vs_one_at_a_time": nu_err,
         "batch_speedup": vb / v1,
         "autotune": {"graph_iters": best_g, "ns_per_cell_iteration": {str(k): 1e9 * v for k, v in tune.items()}},
         "same_iterations_as_one_at_a_time": all(same),
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+MIXED_FIELDS = (0, 1, 2, 3, 4, 5, 6, 7, 8)  # faces u,v,w,p,T; cells u,v,w,T (nim_field)
+
+
+def run_mixed(case, mesh, args, fp64_stats, fp64_fields, fp64_value, fp64_ms_step, peak, peak_kind):
+    """The FP64 run's steps again, from the same start, with the mixed
+    path: device-timed throughput of the same K steps, the Nusselt history
+    and final fields against the FP64 run, and the FP32 kernels' roofline."""
+    import torch
+    import nimgpu
+    from nimgpu import _abi
+    s = nimgpu.NimSolver(mesh, case.params(precision=_abi.PRECISION_MIXED))
+    s.initialize_nse()
+    s.add_temperature_noise(case.noise, case.seed)
+    stream = torch.cuda.ExternalStream(s.stream_handle)
+    recs = []
+    for _ in range(max(args.warmup, 0)):
+        recs += s.solve_nse(1)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    timed = s.solve_nse(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    recs += timed
+    iters = sum(r.iters for r in timed)
+    value = case.ncells * iters / (ms / 1e3)
+    nu = [max(abs(a.nu_inner - b.nu_inner) / abs(b.nu_inner), abs(a.nu_outer - b.nu_outer) / abs(b.nu_outer))
+          for a, b in zip(recs, fp64_stats)]
+    err = {}
+    for f in MIXED_FIELDS:
+        a, b = s.download(f), fp64_fields[f]
+        name = ["faces_u", "faces_v", "faces_w", "faces_p", "faces_T", "meshes_u", "meshes_v", "meshes_w",
+                "meshes_T"][f]
+        err[name] = {"max_rel": float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)),
+                     "l2_rel": float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))}
+    prof = s.profile_iterations(20)
+    dom = max((k for k in KERNEL_BYTES_PER_CELL if k in prof), key=lambda k: prof[k])
+    achieved = KERNEL_BYTES_PER_CELL[dom] / 2 * case.ncells / (prof[dom] / 1e3) / 1e9
+    s.close()
+    return {
+        "value": value, "unit": UNIT, "ms_per_step": ms / max(args.steps, 1), "iterations": iters,
+        "iters_fp32": sum(r.iters_fp32 for r in timed), "speedup_vs_fp64": value / fp64_value,
+        "step_time_speedup_vs_fp64": fp64_ms_step / (ms / max(args.steps, 1)),
+        "dtype": "f32 storage of the swept arrays, f64 arithmetic, reductions and refinement",
+        "nu_rel_err_max": max(nu) if nu else None, "nu_rel_err_per_step": nu,
+        "field_err_final": err,
+        "tolerances": "reference (tol_u,v,w,T 1e-6, tol_p 5e-3): both runs stop once a pass changes every "
+                      "field by less than its tolerance",
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "kernel_us": {k: round(1e3 * v, 2) for k, v in prof.items() if v > 0}},
+    }
 
 
 def main():
@@ -302,6 +369,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--schedule", default="parallel", choices=["parallel", "reference"],
                     help="reference: the Gauss-Seidel sweeps in the reference's cell order (its iterates)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="mixed: FP32 passes over a float mirror, then FP64 passes (nim_params.precision)")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -324,13 +394,15 @@ def main():
     case = config.CASES[args.case]
     mesh = nimgpu.Mesh(case.mesh_params())
     sched = _abi.SCHEDULE_REFERENCE if args.schedule == "reference" else _abi.SCHEDULE_PARALLEL
-    solver = nimgpu.NimSolver(mesh, case.params(schedule=sched))
+    prec = _abi.PRECISION_MIXED if args.precision == "mixed" else _abi.PRECISION_FP64
+    solver = nimgpu.NimSolver(mesh, case.params(schedule=sched, precision=prec))
     solver.initialize_nse()
     solver.add_temperature_noise(case.noise, case.seed)
     stream = torch.cuda.ExternalStream(solver.stream_handle)
 
+    warm_stats = []
     for _ in range(max(args.warmup, 0)):
-        solver.solve_nse(1)
+        warm_stats += solver.solve_nse(1)
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
@@ -352,6 +424,9 @@ def main():
     cell_iters = case.ncells * iters
     t_max, total = combine_ranks(pg, ms, cell_iters)
     value = total / (t_max / 1e3)
+    want_mixed = (world == 1 and prec == _abi.PRECISION_FP64 and sched == _abi.SCHEDULE_PARALLEL
+                  and not args.no_mixed)
+    fp64_fields = {f: solver.download(f) for f in MIXED_FIELDS} if want_mixed else None
 
     # ---------------- end to end through the C ABI with host buffers: the
     # host holds the state (read_restart / write_restart arrays) and every
@@ -391,8 +466,14 @@ def main():
     tot = sum(shares.values())
     dom = max((k for k in KERNEL_BYTES_PER_CELL if k in prof), key=lambda k: prof[k])
     dom_ms = prof[dom]
-    achieved = KERNEL_BYTES_PER_CELL[dom] * case.ncells / (dom_ms / 1e3) / 1e9
+    width = 4 if prec == _abi.PRECISION_MIXED else 8  # profile_iterations runs FP32 passes when mixed
+    achieved = KERNEL_BYTES_PER_CELL[dom] * width / 8 * case.ncells / (dom_ms / 1e3) / 1e9
     iter_gbs = ALGO_BYTES_PER_CELL_ITER * cell_iters / (ms / 1e3) / 1e9
+
+    mixed = None
+    if want_mixed:
+        mixed = run_mixed(case, mesh, args, warm_stats + list(stats), fp64_fields, value, ms / max(args.steps, 1),
+                          peak, peak_kind)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -404,8 +485,9 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / max(args.steps, 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded mesh and T noise)",
-        "config": dict(workload_config(case), schedule=args.schedule),
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == _abi.PRECISION_FP64 else "f32+f64",
+        "data": "synthetic (seeded mesh and T noise)",
+        "config": dict(workload_config(case), schedule=args.schedule, precision=args.precision),
         "iterations": iters, "iters_per_step": iters / max(len(stats), 1),
         "hbm_gbs_iteration": iter_gbs,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -415,7 +497,7 @@ def main():
                      "traffic": (NCU_DRAM_BYTES_PER_CELL[dom] * case.ncells if dom in NCU_DRAM_BYTES_PER_CELL
                                  else None),
                      "traffic_source": "ncu dram bytes on the 96x96x64 case, scaled by cells",
-                     "bytes_per_launch": KERNEL_BYTES_PER_CELL[dom] * case.ncells,
+                     "bytes_per_launch": KERNEL_BYTES_PER_CELL[dom] * width / 8 * case.ncells,
                      "kernel_ms": dom_ms,
                      "shares": {k: round(v / tot, 4) for k, v in shares.items()},
                      "kernel_us": {k: round(1e3 * v, 2) for k, v in shares.items()}},
@@ -423,6 +505,8 @@ def main():
         "gpu_launches": launches,
         "clocks": clk,
         "nu_inner_last": stats[-1].nu_inner if stats else None,
+        "iters_fp32": sum(s.iters_fp32 for s in stats),
+        "mixed": mixed,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

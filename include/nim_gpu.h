@@ -152,10 +152,25 @@ typedef struct nim_params {
                            reference's Gauss-Seidel order but can diverge
                            under NIM_SCHEDULE_PARALLEL on coarse meshes:
                            pair it with NIM_SCHEDULE_REFERENCE            */
-  int32_t reserved;     /* 0 */
+  int32_t precision;    /* NIM_PRECISION_FP64 (0): every pass in FP64, as the
+                           reference; NIM_PRECISION_MIXED (1): each step's
+                           inner loop first sweeps a float copy of the
+                           fields, NIM constants and geometry (arithmetic
+                           in double registers, maxima of the stored
+                           changes in double) until the tolerances hold or
+                           8 passes in a row bring no new smallest change
+                           to a field above its tolerance; the iterate is
+                           then widened and FP64 passes run until the
+                           reference's test holds.  Per-step work, the
+                           reductions and the Nusselt integrals stay FP64.
+                           max_iters bounds both phases together.
+                           Parallel schedule and formulation 2 only
+                           (NIM_ERR_BAD_ARG otherwise); nim_gpu_iterate
+                           always runs FP64 passes                        */
 } nim_params;
 
 enum { NIM_SCHEDULE_PARALLEL = 0, NIM_SCHEDULE_REFERENCE = 1 };
+enum { NIM_PRECISION_FP64 = 0, NIM_PRECISION_MIXED = 1 };
 
 /* Statistics of one time step (the values the reference prints at
    nse.f90:169-171 and nse.f90:2793-2794, returned instead of printed). */
@@ -171,6 +186,8 @@ typedef struct nim_step_stats {
   double time;          /* TI after update_time_step                         */
   int32_t steady;       /* 1 if the steady-state test fired at this step     */
   int32_t status;       /* NIM_OK or an error of this step                   */
+  int32_t iters_fp32;   /* of iters, the FP32 passes (NIM_PRECISION_MIXED)   */
+  int32_t pad;
 } nim_step_stats;
 
 typedef struct nim_ctx nim_ctx;
@@ -271,7 +288,9 @@ int nim_gpu_output_wait(nim_ctx *ctx, int32_t ticket);
    so a caller can record CUDA events on it.
    nim_gpu_launch_count: kernels launched by the context since creation.
    nim_gpu_profile_iterations: n inner passes of the context's schedule and
-   formulation, launched one kernel at a time with a CUDA event after each;
+   formulation (with NIM_PRECISION_MIXED: FP32 passes over the narrowed
+   iterate, leaving the FP64 fields as they were), launched one kernel at a
+   time with a CUDA event after each;
    ms[k] receives the mean time of launch group k (its name from
    nim_gpu_profile_name), at most cap of them; returns their number. */
 void *nim_gpu_stream(nim_ctx *ctx);

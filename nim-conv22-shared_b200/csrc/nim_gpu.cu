@@ -9,6 +9,9 @@
 // on the device (k_iter_end) and the host only polls it between batches.
 // With NIM_SCHEDULE_REFERENCE the four Gauss-Seidel sweeps run as in-place
 // level-by-level sweeps (k_seq_*) that reproduce the reference's cell order.
+// With NIM_PRECISION_MIXED each step's inner loop runs first as FP32 passes
+// over a float mirror of the arrays the pass touches, then as FP64 passes
+// from the widened FP32 iterate until the reference's stop test holds.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -93,6 +96,16 @@ struct nim_ctx {
     size_t used = 0;
   } *marks = nullptr;
   std::vector<std::string> prof_names;  // names of the last profile
+  // mixed precision: the FP32 mirror of every array a parallel pass reads or
+  // writes, the graph of FP32 passes, the phase of the current step (1: FP32
+  // passes queued, 2: FP64 passes) and the last step's pass count per phase
+  bool mixed = false;
+  GeoT<float> g32{};
+  FieldsT<float> F32{};
+  cudaGraphExec_t graph32 = nullptr;
+  int graph32_iters = 0;
+  int phase = 0;
+  int last_lowp = 0, last_hi = 0;
   // a time step driven without blocking (the synchronous calls and
   // nim_batch_step share it): graph launches so far, the cap, the event that
   // marks the last control-block (or sums) copy
@@ -240,18 +253,19 @@ int mark(nim_ctx *x, const char *name) {
 }
 
 // the velocity sources + cell kernel and the face kernel of the context's
-// formulation (parallel schedule)
-int launch_vel(nim_ctx *x, cudaStream_t s) {
+// formulation (parallel schedule), over arrays of storage type R
+template <class R>
+int launch_vel(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F) {
   const Dims &d = x->d;
   if (x->phys.formulation == 1) {
-    k_vel_cell<false, 1><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_vel_cell<false, 1><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
     TRY(mark(x, "k_vel_cell"));
-    k_vel1_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_vel1_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
     TRY(mark(x, "k_vel1_face"));
   } else {
-    k_vel_cell<false, 2><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_vel_cell<false, 2><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
     TRY(mark(x, "k_vel_cell"));
-    k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+    k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
     TRY(mark(x, "k_vel_face"));
   }
   return NIM_OK;
@@ -305,7 +319,7 @@ int launch_iteration_seq(nim_ctx *x) {
   TRY(mark(x, "k_T_cell(src)"));
   TRY(launch_coop(k_seq_T, x->coop_T, dim3(BLK), x));
   TRY(mark(x, "k_seq_T"));
-  k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
+  k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys, 0);
   TRY(mark(x, "k_iter_end"));
   CK(cudaGetLastError());
   x->kernels_per_iter = x->phys.dpdx_tolerance ? 12 : 11;
@@ -313,35 +327,35 @@ int launch_iteration_seq(nim_ctx *x) {
   return NIM_OK;
 }
 
-// one pass of integrate_nse's loop body
-int launch_iteration(nim_ctx *x) {
-  if (x->seq) return launch_iteration_seq(x);
+// one pass of the parallel schedule over arrays of storage type R
+template <class R>
+int launch_parallel(nim_ctx *x, const GeoT<R> &g, const FieldsT<R> &F, int lowp) {
   const Dims &d = x->d;
   cudaStream_t s = x->stream;
   const int gc = x->nblk_c, gb = x->nblk_b;
   const dim3 g3 = x->g3, g8 = x->g8;
-  TRY(launch_vel(x, s));
-  k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  TRY(launch_vel(x, s, g, F));
+  k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_p_src"));
-  k_p_bc<<<gb, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_p_bc<<<gb, BLK, 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_p_bc"));
-  k_p_bc_copy<<<gb, BLK, 0, s>>>(d, x->F, x->ctl);
+  k_p_bc_copy<<<gb, BLK, 0, s>>>(d, F, x->ctl);
   TRY(mark(x, "k_p_bc_copy"));
-  k_p_face<<<g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_p_face<<<g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_p_face"));
   if (x->phys.dpdx_tolerance) {
-    k_p_dpdx<<<gc, BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+    k_p_dpdx<<<gc, BLK, 0, s>>>(d, g, F, x->ctl);
     TRY(mark(x, "k_p_dpdx"));
   }
-  k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, x->g, x->F, x->ctl);
+  k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, g, F, x->ctl);
   TRY(mark(x, "k_zero_flux"));
-  k_T_coef<<<dim3(3, x->nblk_c), BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_T_coef<<<dim3(3, x->nblk_c), BLK, 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_T_coef"));
-  k_T_cell<false><<<x->g3, dim3(CB, 3), 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_T_cell<false><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_T_cell"));
-  k_T_face<<<g8, BLK, 0, s>>>(d, x->g, x->F, x->phys, x->ctl);
+  k_T_face<<<g8, BLK, 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_T_face"));
-  k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys);
+  k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys, lowp);
   TRY(mark(x, "k_iter_end"));
   CK(cudaGetLastError());
   x->kernels_per_iter = x->phys.dpdx_tolerance ? 12 : 11;
@@ -349,16 +363,24 @@ int launch_iteration(nim_ctx *x) {
   return NIM_OK;
 }
 
-int build_graph(nim_ctx *x, int iters) {
-  if (x->graph) {
-    cudaGraphExecDestroy(x->graph);
-    x->graph = nullptr;
+// one pass of integrate_nse's loop body; lowp: over the FP32 mirror, and
+// with stall_rule the pass ends the FP32 phase once the changes stop falling
+int launch_iteration(nim_ctx *x, bool lowp = false, bool stall_rule = true) {
+  if (x->seq) return launch_iteration_seq(x);
+  return lowp ? launch_parallel(x, x->g32, x->F32, stall_rule ? 1 : 0) : launch_parallel(x, x->g, x->F, 0);
+}
+
+int build_graph(nim_ctx *x, int iters, bool lowp = false) {
+  cudaGraphExec_t &exec = lowp ? x->graph32 : x->graph;
+  if (exec) {
+    cudaGraphExecDestroy(exec);
+    exec = nullptr;
   }
   cudaGraph_t g = nullptr;
   const long long before = x->launches;
   CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
   for (int k = 0; k < iters; ++k) {
-    const int st = launch_iteration(x);
+    const int st = launch_iteration(x, lowp);
     if (st != NIM_OK) {
       cudaStreamEndCapture(x->stream, &g);
       if (g) cudaGraphDestroy(g);
@@ -367,11 +389,89 @@ int build_graph(nim_ctx *x, int iters) {
   }
   CK(cudaStreamEndCapture(x->stream, &g));
   x->launches = before;
-  cudaError_t e = cudaGraphInstantiate(&x->graph, g, 0);
+  cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return NIM_ERR_CUDA;
-  x->graph_iters = iters;
+  (lowp ? x->graph32_iters : x->graph_iters) = iters;
   return NIM_OK;
+}
+
+// ---- the FP32 mirror of a mixed-precision context
+struct Cvt {
+  CvtList L{};
+  int k = 0;
+  long long nmax = 0;
+  template <class S, class D>
+  void add(const S *src, D *dst, size_t n) {
+    L.src[k] = src;
+    L.dst[k] = dst;
+    L.n[k] = (long long)n;
+    nmax = std::max(nmax, (long long)n);
+    ++k;
+  }
+};
+template <class S, class D>
+int run_cvt(nim_ctx *x, const Cvt &c) {
+  if (c.k == 0) return NIM_OK;
+  if (c.k > CvtList::kMax) return NIM_ERR_BAD_ARG;
+  const long long blocks = std::min<long long>((c.nmax + BLK - 1) / BLK, 148LL * 8);
+  k_convert<S, D><<<dim3((unsigned)std::max(1LL, blocks), c.k), BLK, 0, x->stream>>>(c.L);
+  CK(cudaGetLastError());
+  x->launches += 1;
+  return NIM_OK;
+}
+
+// geometry (once, after nim_gpu_init's metric kernels)
+int mirror_geometry(nim_ctx *x) {
+  const Dims &d = x->d;
+  const size_t Nc = d.Nc, NF = d.NF, NB = d.NBF;
+  const Geo &g = x->g;
+  GeoT<float> &h = x->g32;
+  Cvt c;
+  c.add(g.vol, h.vol, Nc);
+  c.add(g.G, h.G, 3 * Nc);
+  c.add(g.gij, h.gij, 9 * Nc);
+  c.add(g.xi, h.xi, 9 * Nc);
+  c.add(g.gfd, h.gfd, 6 * Nc);
+  c.add(g.dg, h.dg, 6 * Nc);
+  c.add(g.area, h.area, NF);
+  c.add(g.normal, h.normal, 3 * NF);
+  c.add(g.AA, h.AA, 45 * Nc);
+  c.add(g.bca, h.bca, 5 * NB);
+  c.add(g.bcap, h.bcap, 8 * NB);
+  c.add(g.bcg, h.bcg, 2 * NB);
+  c.add(g.zf, h.zf, 4 * NB);
+  return run_cvt<double, float>(x, c);
+}
+
+// velocity NIM constants (every step, after nim_gpu_begin_step's kernels)
+int mirror_step_coefficients(nim_ctx *x) {
+  const size_t Nc = x->d.Nc;
+  Cvt c;
+  c.add(x->F.MF4, x->F32.MF4, 8 * Nc);
+  c.add(x->F.MF, x->F32.MF, 15 * Nc);
+  return run_cvt<double, float>(x, c);
+}
+
+// the iterate: both halves of the face fields (wall values live in both),
+// cell fields, old cell fields, dpdx_old; dir 0 narrows, 1 widens (the old
+// cell fields only narrow: the passes do not write them)
+int mirror_state(nim_ctx *x, int dir) {
+  const size_t Nc = x->d.Nc, NF = x->d.NF;
+  const Fields &F = x->F;
+  const FieldsT<float> &H = x->F32;
+  Cvt c;
+  if (dir == 0) {
+    for (int q = 0; q < 5; ++q) c.add(F.f[q], H.f[q], 2 * NF);
+    for (int q = 0; q < 4; ++q) c.add(F.c[q], H.c[q], Nc);
+    for (int q = 0; q < 4; ++q) c.add(F.co[q], H.co[q], Nc);
+    c.add(F.dpd, H.dpd, 3 * Nc);
+    return run_cvt<double, float>(x, c);
+  }
+  for (int q = 0; q < 5; ++q) c.add(H.f[q], F.f[q], 2 * NF);
+  for (int q = 0; q < 4; ++q) c.add(H.c[q], F.c[q], Nc);
+  c.add(H.dpd, F.dpd, 3 * Nc);
+  return run_cvt<float, double>(x, c);
 }
 
 int read_ctrl(nim_ctx *x) {
@@ -697,6 +797,37 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
     TRY(dalloc(x, &F.AAv, 45 * Nc));
   }
   TRY(dalloc(x, &F.dpd, 3 * Nc));
+  x->mixed = (p->precision == NIM_PRECISION_MIXED);
+  if (x->mixed) {
+    GeoT<float> &h = x->g32;
+    TRY(dalloc(x, &h.vol, Nc));
+    TRY(dalloc(x, &h.G, 3 * Nc));
+    TRY(dalloc(x, &h.gij, 9 * Nc));
+    TRY(dalloc(x, &h.xi, 9 * Nc));
+    TRY(dalloc(x, &h.gfd, 6 * Nc));
+    TRY(dalloc(x, &h.dg, 6 * Nc));
+    TRY(dalloc(x, &h.area, NF));
+    TRY(dalloc(x, &h.normal, 3 * NF));
+    TRY(dalloc(x, &h.AA, 45 * Nc));
+    h.bcpts = g.bcpts;  // integer: shared with the FP64 side
+    TRY(dalloc(x, &h.bca, 5 * NB));
+    TRY(dalloc(x, &h.bcap, 8 * NB));
+    TRY(dalloc(x, &h.bcg, 2 * NB));
+    TRY(dalloc(x, &h.zf, 4 * NB));
+    FieldsT<float> &H = x->F32;
+    for (int q = 0; q < 5; ++q) TRY(dalloc(x, &H.f[q], 2 * NF));
+    for (int q = 0; q < 4; ++q) {
+      TRY(dalloc(x, &H.c[q], Nc));
+      TRY(dalloc(x, &H.co[q], Nc));
+    }
+    TRY(dalloc(x, &H.dila, Nc));
+    TRY(dalloc(x, &H.Rp, Nc));
+    TRY(dalloc(x, &H.MF4, 8 * Nc));
+    TRY(dalloc(x, &H.MF, 15 * Nc));
+    TRY(dalloc(x, &H.MTF, 15 * Nc));
+    TRY(dalloc(x, &H.MTA, 18 * Nc));
+    TRY(dalloc(x, &H.dpd, 3 * Nc));
+  }
   TRY(dalloc(x, &F.part, 8 * (size_t)std::max(x->nblk_c, grid(2 * d.NT * d.NZ))));
   TRY(dalloc(x, &x->ctl, 1));
   TRY(dalloc(x, &x->node_xyz, 3 * (size_t)m->nnode));
@@ -725,6 +856,10 @@ extern "C" int nim_gpu_create(const nim_mesh_desc *m, const nim_params *p, nim_c
   if (!(p->DT > 0) || !(p->nu > 0) || !(p->alpha > 0) || !(p->rho > 0)) return NIM_ERR_BAD_ARG;
   if (p->schedule != NIM_SCHEDULE_PARALLEL && p->schedule != NIM_SCHEDULE_REFERENCE) return NIM_ERR_BAD_ARG;
   if (p->formulation != 1 && p->formulation != 2) return NIM_ERR_BAD_ARG;
+  if (p->precision != NIM_PRECISION_FP64 && p->precision != NIM_PRECISION_MIXED) return NIM_ERR_BAD_ARG;
+  // the FP32 phase exists for the parallel schedule of formulation 2
+  if (p->precision == NIM_PRECISION_MIXED && (p->schedule != NIM_SCHEDULE_PARALLEL || p->formulation != 2))
+    return NIM_ERR_BAD_ARG;
   *out = nullptr;
   nim_ctx *x = new (std::nothrow) nim_ctx();
   if (!x) return NIM_ERR_BAD_ARG;
@@ -762,12 +897,14 @@ extern "C" int nim_gpu_init(nim_ctx *x) {
   k_apply_dirichlet<<<x->nblk_b, BLK, 0, s>>>(d, x->g, x->F);
   k_wall_floor<<<x->nblk_b, BLK, 0, s>>>(d, x->g, x->ctl);
   CK(cudaGetLastError());
+  if (x->mixed) TRY(mirror_geometry(x));
   CK(cudaStreamSynchronize(s));
   x->TI = x->params.DT;  // nse.f90:31
   x->STEP = 1;           // nse.f90:32
   x->initialized = true;
   x->in_step = false;
   x->last_iters = 0;
+  x->last_lowp = x->last_hi = 0;
   return NIM_OK;
 }
 
@@ -785,6 +922,7 @@ extern "C" int nim_gpu_begin_step(nim_ctx *x) {
   }
   CK(cudaGetLastError());
   x->launches += 3;
+  if (x->mixed) TRY(mirror_step_coefficients(x));
   x->in_step = true;
   return NIM_OK;
 }
@@ -800,6 +938,7 @@ static int fill_iter_stats(nim_ctx *x, nim_step_stats *s) {
   s->err_p = c.last_err[3];
   s->err_T = c.last_err[4];
   s->status = c.status;
+  s->iters_fp32 = x->mixed ? c.lowp_iters : 0;
   return NIM_OK;
 }
 
@@ -835,7 +974,8 @@ int iterations_launch(nim_ctx *x, int batches) {
   if (x->seq) {
     for (int k = 0; k < batches * G; ++k) TRY(launch_iteration(x));
   } else {
-    for (int k = 0; k < batches; ++k) CK(cudaGraphLaunch(x->graph, x->stream));
+    cudaGraphExec_t graph = (x->phase == 1) ? x->graph32 : x->graph;
+    for (int k = 0; k < batches; ++k) CK(cudaGraphLaunch(graph, x->stream));
     x->launches += (long long)batches * G * x->kernels_per_iter;
   }
   x->run.launched += (long long)batches * G;
@@ -846,10 +986,20 @@ int iterations_launch(nim_ctx *x, int batches) {
 int integrate_start(nim_ctx *x) {
   const int G = x->graph_G;
   if (!x->seq && (!x->graph || x->graph_iters != G)) TRY(build_graph(x, G));
+  if (x->mixed && (!x->graph32 || x->graph32_iters != G)) TRY(build_graph(x, G, true));
   // with max_iters <= 0 the device never stops on its own; bound the host loop
-  x->run.cap = (x->params.max_iters > 0) ? (long long)x->params.max_iters + G : 100000000LL;
+  x->run.cap = (x->params.max_iters > 0) ? (long long)x->params.max_iters + 2 * G : 100000000LL;
   x->run.launched = 0;
   x->run.capped = false;
+  if (x->mixed) {  // FP32 phase from the narrowed FP64 iterate
+    TRY(mirror_state(x, 0));
+    k_lowp_begin<<<1, 1, 0, x->stream>>>(x->ctl);
+    CK(cudaGetLastError());
+    x->launches += 1;
+    x->phase = 1;
+    return iterations_launch(x, std::max(1, (x->last_lowp * 7 / 8) / G));
+  }
+  x->phase = 0;
   return iterations_launch(x, std::max(1, (x->last_iters * 7 / 8) / G));
 }
 
@@ -862,6 +1012,15 @@ int integrate_advance(nim_ctx *x) {
       return 1;
     }
     x->run.capped = true;
+  } else if (x->phase == 1 && x->ctl_host->status == NIM_OK) {
+    // FP32 phase over: widen its iterate, FP64 passes to the reference's test
+    TRY(mirror_state(x, 1));
+    k_lowp_end<<<1, 1, 0, x->stream>>>(x->ctl);
+    CK(cudaGetLastError());
+    x->launches += 1;
+    x->phase = 2;
+    TRY(iterations_launch(x, std::max(1, (x->last_hi * 7 / 8) / x->graph_G)));
+    return 1;
   }
   const Dims &d = x->d;
   k_after_integrate<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->g, x->F, x->phys, x->ctl, x->nblk_c);
@@ -876,6 +1035,11 @@ int integrate_advance(nim_ctx *x) {
 int integrate_finish(nim_ctx *x, nim_step_stats *s) {
   const Dims &d = x->d;
   x->last_iters = x->ctl_host->step_iters;
+  if (x->mixed) {
+    x->last_lowp = x->ctl_host->lowp_iters;
+    x->last_hi = x->ctl_host->step_iters - x->ctl_host->lowp_iters;
+  }
+  x->phase = 0;
   if (x->run.capped && x->ctl_host->status == NIM_OK) x->ctl_host->status = NIM_ERR_NOT_CONVERGED;
   if (s) {
     fill_iter_stats(x, s);
@@ -1160,6 +1324,7 @@ extern "C" void nim_gpu_destroy(nim_ctx *x) {
   if (x->stream) cudaStreamSynchronize(x->stream);
   if (x->copy_stream) cudaStreamSynchronize(x->copy_stream);  // copies still reading staging
   if (x->graph) cudaGraphExecDestroy(x->graph);
+  if (x->graph32) cudaGraphExecDestroy(x->graph32);
   for (void *p : x->allocs) cudaFree(p);
   if (x->ctl_host) cudaFreeHost(x->ctl_host);
   for (auto &o : x->out) {
@@ -1190,6 +1355,7 @@ extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int
   if (cudaEventCreate(&start) != cudaSuccess) st = NIM_ERR_CUDA;
   if (st == NIM_OK) {
     k_step_reset<<<1, 1, 0, s>>>(x->ctl);
+    if (x->mixed) st = mirror_state(x, 0);  // FP32 passes over the narrowed iterate
     x->marks = &marks;
     for (int it = 0; it < n && st == NIM_OK; ++it) {
       marks.used = 0;
@@ -1197,7 +1363,7 @@ extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int
         st = NIM_ERR_CUDA;
         break;
       }
-      st = launch_iteration(x);
+      st = launch_iteration(x, x->mixed, false);  // every pass runs: no stop test
       if (st != NIM_OK) break;
       if (cudaEventSynchronize(marks.ev[marks.used - 1]) != cudaSuccess) {
         st = NIM_ERR_CUDA;

@@ -1,4 +1,4 @@
-// Device kernels of the NIM time advance (FP64 path).
+// Device kernels of the NIM time advance.
 //
 // Each kernel restates one or more reference routines; the file:line of the
 // routine is given at the kernel.  Arithmetic follows the reference's
@@ -30,51 +30,58 @@
 namespace nim {
 
 // ------------------------------------------------------------ device state
-struct Geo {
-  double *vol;     // [Nc]
-  double *G;       // [3][Nc]   G1, G2, G3
-  double *gij;     // [9][Nc]   meshes_gij(a,b) at a-1+3(b-1)
-  double *xi;      // [9][Nc]   meshes_xi_x(a,b) at a-1+3(b-1)
-  double *gf;      // [54][Nc]  meshes_gij_faces(a,b,f) at a-1+3(b-1)+9(f-1)
-  double *gfd;     // [6][Nc]   gf(d,d,2d-1), gf(d,d,2d) at 2(d-1)+{0,1}
-  double *dg;      // [6][Nc]   gf(d,e,2d-1,i2)-gf(d,e,2d,i), e=tr1,tr2 at 2(d-1)+{0,1}
-  double *area;    // [NF]
-  double *normal;  // [3][NF]
-  double *mid;     // [3][NF]
-  double *tang;    // [3][NF]
-  double *bitang;  // [3][NF]
-  double *AA;      // [45][Nc]  AA_px/py/pz(k) at 15(d-1)+k-1
+// Geometry and field arrays, by storage type R: double for the FP64 path;
+// float for the mirror the mixed-precision inner loop sweeps (every array the
+// parallel iteration reads or writes, arithmetic still in double registers).
+template <class R>
+struct GeoT {
+  R *vol;     // [Nc]
+  R *G;       // [3][Nc]   G1, G2, G3
+  R *gij;     // [9][Nc]   meshes_gij(a,b) at a-1+3(b-1)
+  R *xi;      // [9][Nc]   meshes_xi_x(a,b) at a-1+3(b-1)
+  R *gf;      // [54][Nc]  meshes_gij_faces(a,b,f) at a-1+3(b-1)+9(f-1)
+  R *gfd;     // [6][Nc]   gf(d,d,2d-1), gf(d,d,2d) at 2(d-1)+{0,1}
+  R *dg;      // [6][Nc]   gf(d,e,2d-1,i2)-gf(d,e,2d,i), e=tr1,tr2 at 2(d-1)+{0,1}
+  R *area;    // [NF]
+  R *normal;  // [3][NF]
+  R *mid;     // [3][NF]
+  R *tang;    // [3][NF]
+  R *bitang;  // [3][NF]
+  R *AA;      // [45][Nc]  AA_px/py/pz(k) at 15(d-1)+k-1
   int *bcpts;      // [5][NBF]  BCs_faces_points as structured face indices
-  double *bca;     // [5][NBF]  BCs_faces_a(1:5)
-  double *bcap;    // [8][NBF]  BCs_faces_ap(1:8)
-  double *bcg;     // [2][NBF]  gij_faces factors of B2, B3 in apply_pressure_bc
-  double *zf;      // [4][NBF]  zero-flux weights (B, C, D, A) for z walls
-  double *nuw;     // [4][NBF]  find_Nu2 weights (A, B, C, D) for r walls
-  double *bcval;   // [4][NBF]  Dirichlet face values of u, v, w, T
+  R *bca;     // [5][NBF]  BCs_faces_a(1:5)
+  R *bcap;    // [8][NBF]  BCs_faces_ap(1:8)
+  R *bcg;     // [2][NBF]  gij_faces factors of B2, B3 in apply_pressure_bc
+  R *zf;      // [4][NBF]  zero-flux weights (B, C, D, A) for z walls
+  R *nuw;     // [4][NBF]  find_Nu2 weights (A, B, C, D) for r walls
+  R *bcval;   // [4][NBF]  Dirichlet face values of u, v, w, T
 };
+using Geo = GeoT<double>;
 
-struct Fields {
-  double *f[5];    // faces u, v, w, p, T: each [2][NF]
-  double *c[4];    // cells u, v, w, T (meshes_*xyz)
-  double *co[4];   // meshes_*xyz_old
-  double *ct[4];   // meshes_*xyzt
-  double *mp, *dila, *dila_old, *Rp;
-  double *MA;      // [18][Nc] velocity M_A (per step scratch)
-  double *MF4;     // [8][Nc]
-  double *MF;      // [15][Nc]  M_F1..3(k) at 5(d-1)+k-1
-  double *MTF;     // [15][Nc]  MT_F1..3
-  double *MTA;     // [18][Nc]  MT_A(q, d) at 3(q-1) + d-1
-  double *dpd;     // [3][Nc]   dpdx_old, dpdy_old, dpdz_old
+template <class R>
+struct FieldsT {
+  R *f[5];    // faces u, v, w, p, T: each [2][NF]
+  R *c[4];    // cells u, v, w, T (meshes_*xyz)
+  R *co[4];   // meshes_*xyz_old
+  R *ct[4];   // meshes_*xyzt
+  R *mp, *dila, *dila_old, *Rp;
+  R *MA;      // [18][Nc] velocity M_A (per step scratch)
+  R *MF4;     // [8][Nc]
+  R *MF;      // [15][Nc]  M_F1..3(k) at 5(d-1)+k-1
+  R *MTF;     // [15][Nc]  MT_F1..3
+  R *MTA;     // [18][Nc]  MT_A(q, d) at 3(q-1) + d-1
+  R *dpd;     // [3][Nc]   dpdx_old, dpdy_old, dpdz_old
   // reference-order schedule: sources stored before the ordered sweeps
-  double *Bv;      // [3][Nc]   R_C + R_D + R_B of u, v, w
-  double *MTF4;    // [8][Nc]   MT_F4
-  double *RDT;     // [Nc]      R_D_T
+  R *Bv;      // [3][Nc]   R_C + R_D + R_B of u, v, w
+  R *MTF4;    // [8][Nc]   MT_F4
+  R *RDT;     // [Nc]      R_D_T
   // formulation 1 (nim_formulation = 1)
-  double *N1;      // [22][Nc]  CC, EE, FF, GG, HH, II, JJ (3 each), Det (per step)
-  double *AT;      // [9][Nc]   a_t
-  double *AAv;     // [45][Nc]  AA_vx, AA_vy, AA_vz (15 each)
-  double *part;    // [8][nblk] per-block partial sums
+  R *N1;      // [22][Nc]  CC, EE, FF, GG, HH, II, JJ (3 each), Det (per step)
+  R *AT;      // [9][Nc]   a_t
+  R *AAv;     // [45][Nc]  AA_vx, AA_vy, AA_vz (15 each)
+  double *part;  // [8][nblk] per-block partial sums (FP64 always)
 };
+using Fields = FieldsT<double>;
 
 struct Phys {
   double DT, nu, alpha, rho, g_beta;
@@ -105,7 +112,16 @@ struct Ctrl {
                                      // compares with zero-initialised arrays once)
   unsigned long long red[4];  // dudt, dTdt maxima (after integrate)
   double dilatation, nu_outer, nu_inner, area_outer, area_inner;
+  // FP32 phase of a mixed-precision step: passes run, the smallest maximum
+  // change seen per field, passes since a field still above its tolerance
+  // last reached a new smallest change
+  int lowp_iters, stall;
+  double best[5];
 };
+
+// FP32 passes without progress after which a mixed-precision step hands over
+// to FP64 (the FP32 iterate has reached its rounding floor)
+constexpr int kLowpStall = 8;
 
 constexpr int BLK = 256;
 // kernels that spread one cell over three threads (component or direction)
@@ -631,7 +647,8 @@ __device__ __forceinline__ void nim_direction(double u, double k, double gminus,
 }
 
 // contravariant component dd (1..3) of a Cartesian velocity in cell c
-__device__ __forceinline__ double contravariant(const double *xi, size_t Nc, int c, int dd, double u, double v, double w) {
+template <class R>
+__device__ __forceinline__ double contravariant(const R *xi, size_t Nc, int c, int dd, double u, double v, double w) {
   return u * xi[(size_t)(dd - 1 + 0) * Nc + c] + v * xi[(size_t)(dd - 1 + 3) * Nc + c] + w * xi[(size_t)(dd - 1 + 6) * Nc + c];
 }
 
@@ -884,7 +901,8 @@ __global__ void __launch_bounds__(BLK) k_vel1_coef_F(Dims d, Geo g, Fields F, Ph
 // reference-order sweeps read data that other SMs rewrote one level earlier
 // (LdCoh below).
 struct LdPlain {
-  __device__ __forceinline__ static double ld(const double *p, size_t i) { return p[i]; }
+  template <class T>
+  __device__ __forceinline__ static double ld(const T *p, size_t i) { return p[i]; }
 };
 // Loads and stores of values the same launch rewrites in place (the
 // reference-order sweeps) go through volatile: never the non-coherent
@@ -892,11 +910,17 @@ struct LdPlain {
 // other, so a thread sees its own earlier stores and every store made before
 // the last grid or block barrier.  Other loads stay free to be scheduled.
 struct LdCoh {
-  __device__ __forceinline__ static double ld(const double *p, size_t i) {
-    return *(const volatile double *)(p + i);
+  template <class T>
+  __device__ __forceinline__ static double ld(const T *p, size_t i) {
+    return *(const volatile T *)(p + i);
   }
 };
 __device__ __forceinline__ void st_coh(double *p, size_t i, double v) { *(volatile double *)(p + i) = v; }
+
+// a new value as the storage type R keeps it: the change find_error
+// measures is that of the stored field (identity for double)
+template <class R>
+__device__ __forceinline__ double stored(double v) { return (double)(R)v; }
 
 __device__ __forceinline__ int parity(const Ctrl *ctl) { return ctl->iter & ctl->pmask; }
 // half holding the values a sweep earlier in this pass produced
@@ -917,9 +941,10 @@ __device__ __forceinline__ void by_dir(int y, Fn &&fn) {
 }
 
 // Green-Gauss derivative dphi_dx2/dy2/dz2 (nse.f90:2866-2903), component cc
-__device__ __forceinline__ double green_gauss(const Geo &g, size_t NF, double invV, const double phi[7],
+template <class R>
+__device__ __forceinline__ double green_gauss(const GeoT<R> &g, size_t NF, double invV, const double phi[7],
                                               const int f[7], int cc) {
-  const double *A = g.area, *n = g.normal + cc * NF;
+  const R *A = g.area, *n = g.normal + cc * NF;
   return invV * (phi[2] * A[f[2]] * (n[f[2]]) - phi[1] * A[f[1]] * (n[f[1]]) + phi[4] * A[f[4]] * (n[f[4]]) -
                  phi[3] * A[f[3]] * (n[f[3]]) + phi[6] * A[f[6]] * (n[f[6]]) - phi[5] * A[f[5]] * (n[f[5]]));
 }
@@ -927,8 +952,8 @@ __device__ __forceinline__ double green_gauss(const Geo &g, size_t NF, double in
 // Derivative of face field phi along local direction e on face fpos of cell
 // x: centred, or second-order one-sided at walls (the ni/nj/nk stencils of
 // calculate_R_D2, nse.f90:1635-1838; integrate_pressure_field_i; bc.f90).
-template <class Ld = LdPlain>
-__device__ __forceinline__ double tangential(const Dims &d, const double *__restrict__ phi, const Cell &x, int fpos,
+template <class Ld = LdPlain, class R>
+__device__ __forceinline__ double tangential(const Dims &d, const R *__restrict__ phi, const Cell &x, int fpos,
                                              int e) {
   const bool lo = !x.has_nb(d, 2 * e - 1), hi = !x.has_nb(d, 2 * e);
   if (lo) {
@@ -943,7 +968,8 @@ __device__ __forceinline__ double tangential(const Dims &d, const double *__rest
 
 // G_i d_i phi - g^ij d_ij phi of calculate_R_D2 / R_D_p2 / R_D_T
 // (nse.f90:1852-1859, 1995-1996, 2132-2133), before the coefficient.
-__device__ __forceinline__ double diffusion_source(const Dims &d, const Geo &g, const double *__restrict__ phi,
+template <class R>
+__device__ __forceinline__ double diffusion_source(const Dims &d, const GeoT<R> &g, const R *__restrict__ phi,
                                                    const Cell &x, const int f[7]) {
   const size_t Nc = d.Nc;
   const int c = x.c;
@@ -956,7 +982,7 @@ __device__ __forceinline__ double diffusion_source(const Dims &d, const Geo &g, 
   const double px = (phi[f[2]] - phi[f[1]]) / 2.;
   const double py = (phi[f[4]] - phi[f[3]]) / 2.;
   const double pz = (phi[f[6]] - phi[f[5]]) / 2.;
-  const double *G = g.G, *gij = g.gij;
+  const R *G = g.G, *gij = g.gij;
   return (G[c] * px + G[Nc + c] * py + G[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy - gij[1 * Nc + c] * pyx -
           gij[6 * Nc + c] * pxz - gij[2 * Nc + c] * pzx - gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
 }
@@ -971,8 +997,8 @@ __device__ __forceinline__ void cell_faces(const Dims &d, const Cell &x, int f[7
 }
 
 // Cell-average update (nse.f90:840-848; T: 1018-1026)
-template <class Ld = LdPlain>
-__device__ __forceinline__ double cell_update(const double *__restrict__ fr, const int f[7], double c, double cold,
+template <class Ld = LdPlain, class R>
+__device__ __forceinline__ double cell_update(const R *__restrict__ fr, const int f[7], double c, double cold,
                                               double B, const double F4[8], double w) {
   return (1 - w) * c +
          (w / F4[0]) * (+F4[1] * cold + F4[2] * Ld::ld(fr, f[1]) + F4[3] * Ld::ld(fr, f[2]) +
@@ -982,9 +1008,9 @@ __device__ __forceinline__ double cell_update(const double *__restrict__ fr, con
 
 // +xi_d face update (nse.f90:878-1005; T: 1033-1088); cx, cx2 the cell
 // values of x and of its +xi_d neighbour x2
-template <class Ld = LdPlain>
-__device__ __forceinline__ double face_update_cv(const Dims &d, const double *__restrict__ fr, double cx, double cx2,
-                                                 const double *__restrict__ co, const double Fd[5], double dg0,
+template <class Ld = LdPlain, class R>
+__device__ __forceinline__ double face_update_cv(const Dims &d, const R *__restrict__ fr, double cx, double cx2,
+                                                 const R *__restrict__ co, const double Fd[5], double dg0,
                                                  double dg1, int dd, const Cell &x, const Cell &x2, double w) {
   const int e1 = tr1(dd), e2 = tr2(dd);
   const double B3 = (dg0) * (Ld::ld(fr, x.face(d, 2 * e1)) - Ld::ld(fr, x.face(d, 2 * e1 - 1)) +
@@ -995,19 +1021,19 @@ __device__ __forceinline__ double face_update_cv(const Dims &d, const double *__
          (w / Fd[0]) * (+Fd[1] * Ld::ld(fr, x.face(d, 2 * dd - 1)) + Fd[2] * Ld::ld(fr, x2.face(d, 2 * dd)) +
                         Fd[3] * (cx + co[x.c]) + Fd[4] * (cx2 + co[x2.c]) - B3 - B4);
 }
-template <class Ld = LdPlain>
-__device__ __forceinline__ double face_update(const Dims &d, const double *__restrict__ fr, const double *__restrict__ cv,
-                                              const double *__restrict__ co, const double Fd[5], double dg0,
+template <class Ld = LdPlain, class R>
+__device__ __forceinline__ double face_update(const Dims &d, const R *__restrict__ fr, const R *__restrict__ cv,
+                                              const R *__restrict__ co, const double Fd[5], double dg0,
                                               double dg1, int dd, const Cell &x, const Cell &x2, double w) {
   return face_update_cv<Ld>(d, fr, Ld::ld(cv, x.c), Ld::ld(cv, x2.c), co, Fd, dg0, dg1, dd, x, x2, w);
 }
 
 // Formulation 1 cell update of one velocity component (integrate_velocity_
-// field_i, nse.f90:341-352); R = R_C + R_D + R_B of the cell, at = a_t(1:9).
-template <class Ld = LdPlain>
-__device__ __forceinline__ double cell_update_f1(const double *__restrict__ fr, const int f[7], double c, double cold,
-                                                 double R, const double at[9], double w) {
-  const double Bij = at[6] * R;
+// field_i, nse.f90:341-352); Rs = R_C + R_D + R_B of the cell, at = a_t(1:9).
+template <class Ld = LdPlain, class R>
+__device__ __forceinline__ double cell_update_f1(const R *__restrict__ fr, const int f[7], double c, double cold,
+                                                 double Rs, const double at[9], double w) {
+  const double Bij = at[6] * Rs;
   return (1 - w) * c + w * (-(at[0] * Ld::ld(fr, f[1])) - at[1] * Ld::ld(fr, f[2]) - at[2] * Ld::ld(fr, f[3]) -
                             at[3] * Ld::ld(fr, f[4]) - at[4] * Ld::ld(fr, f[5]) - at[5] * Ld::ld(fr, f[6]) -
                             at[7] * cold - Bij) /
@@ -1040,8 +1066,8 @@ __device__ __forceinline__ bool patch_cell(const Dims &d, Cell &x) {
 // FORM 1 (nim_formulation = 1): the a_t cell update of integrate_velocity_
 // field_i (nse.f90:341-378); the R sums are stored too, for the face sweep
 // reads them at both cells of a face.
-template <bool SRC_ONLY, int FORM>
-__global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+template <bool SRC_ONLY, int FORM, class R>
+__global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<3>(red);
@@ -1056,13 +1082,13 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, Geo g, Fields F, Ph
     const size_t Nc = d.Nc, NF = d.NF;
     int f[7];
     cell_faces(d, x, f);
-    const double *fp = F.f[3] + par * NF;
+    const R *fp = F.f[3] + par * NF;
     double pf[7];
     for (int k = 1; k <= 6; ++k) pf[k] = fp[f[k]];
     const double invV = 1. / g.vol[c];
     const double base = (q == 2) ? -(P.g_beta * 0.5 * (F.c[3][c] + F.co[3][c])) : 0.;
     const double RB = base + P.inv_rho * green_gauss(g, NF, invV, pf, f, q);
-    const double *fr = F.f[q] + par * NF;
+    const R *fr = F.f[q] + par * NF;
     const double RD = P.inv_Re * diffusion_source(d, g, fr, x, f);
     const double B = (0. + RD + RB);
     if (SRC_ONLY || FORM == 1) F.Bv[(size_t)q * Nc + c] = B;
@@ -1072,11 +1098,11 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, Geo g, Fields F, Ph
       if (FORM == 1) {
         double at[9];
         for (int k = 0; k < 9; ++k) at[k] = F.AT[(size_t)k * Nc + c];
-        nw = cell_update_f1(fr, f, cold, F.co[q][c], B, at, P.w[q]);
+        nw = stored<R>(cell_update_f1(fr, f, cold, F.co[q][c], B, at, P.w[q]));
       } else {
         double F4[8];
         for (int k = 0; k < 8; ++k) F4[k] = F.MF4[(size_t)k * Nc + c];
-        nw = cell_update(fr, f, cold, F.co[q][c], B, F4, P.w[q]);
+        nw = stored<R>(cell_update(fr, f, cold, F.co[q][c], B, F4, P.w[q]));
       }
       F.c[q][c] = nw;
       e[q] = errv(nw, cold, first);
@@ -1087,7 +1113,8 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, Geo g, Fields F, Ph
 
 // ---- K2: +xi face updates of u, v, w (nse.f90:878-1005).
 // Block (CB, 3): threadIdx.y = direction.
-__global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+template <class R>
+__global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<3>(red);
@@ -1109,8 +1136,8 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, Geo g, Fields F, Ph
       const int fo = x.face(d, 2 * dd);
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
-        const double *fr = F.f[q] + par * NF;
-        const double nw = face_update(d, fr, F.c[q], F.co[q], Fd, dg0, dg1, dd, x, x2, P.w[q]);
+        const R *fr = F.f[q] + par * NF;
+        const double nw = stored<R>(face_update(d, fr, F.c[q], F.co[q], Fd, dg0, dg1, dd, x, x2, P.w[q]));
         F.f[q][(1 - par) * NF + fo] = nw;
         e[q] = errv(nw, fr[fo], first);
       }
@@ -1123,7 +1150,8 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, Geo g, Fields F, Ph
 // calculate_R_D_p2 1863-1997).  Block (CB, 3): thread y forms the gradient of
 // velocity component y and two of the six cross derivatives of p (y = 1 also
 // d(bz)/dz); thread 0 combines them in the reference's order.
-__global__ void __launch_bounds__(CB3, 4) k_p_src(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+template <class R>
+__global__ void __launch_bounds__(CB3, 4) k_p_src(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ double sh[3][3][CB];  // gradients of u, v, w
   __shared__ double sX[3][2][CB];  // cross derivatives of p
@@ -1135,19 +1163,19 @@ __global__ void __launch_bounds__(CB3, 4) k_p_src(Dims d, Geo g, Fields F, Phys 
   const int c = x.c;
   int f[7];
   const size_t Nc = d.Nc, NF = d.NF;
-  const double *fp = F.f[3] + par * NF;
+  const R *fp = F.f[3] + par * NF;
   if (active) {
     cell_faces(d, x, f);
     by_dir(threadIdx.y, [&](auto Q) {
       constexpr int q = decltype(Q)::value - 1;
       const double invV = 1. / g.vol[c];
-      const double *fq = F.f[q] + newhalf(ctl) * NF;
+      const R *fq = F.f[q] + newhalf(ctl) * NF;
       double vf[7];
       for (int k = 1; k <= 6; ++k) vf[k] = fq[f[k]];
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) sh[q][cc][tx] = green_gauss(g, NF, invV, vf, f, cc);
       if (q == 1) {
-        const double *fT = F.f[4] + par * NF;
+        const R *fT = F.f[4] + par * NF;
         double bzf[7];
         for (int k = 1; k <= 6; ++k) bzf[k] = -(P.g_beta * (fT[f[k]]));
         sbz[tx] = green_gauss(g, NF, invV, bzf, f, 2);
@@ -1175,7 +1203,7 @@ __global__ void __launch_bounds__(CB3, 4) k_p_src(Dims d, Geo g, Fields F, Phys 
     const double px = (fp[f[2]] - fp[f[1]]) / 2.;
     const double py = (fp[f[4]] - fp[f[3]]) / 2.;
     const double pz = (fp[f[6]] - fp[f[5]]) / 2.;
-    const double *Gv = g.G, *gij = g.gij;
+    const R *Gv = g.G, *gij = g.gij;
     const double RDp = P.inv_rho * (Gv[c] * px + Gv[Nc + c] * py + Gv[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy -
                                     gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz - gij[2 * Nc + c] * pzx -
                                     gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
@@ -1185,10 +1213,10 @@ __global__ void __launch_bounds__(CB3, 4) k_p_src(Dims d, Geo g, Fields F, Phys 
 
 // ---- apply_pressure_bc for wall face b (bc.f90:148-339): the new value
 // from the pressures pr, the new velocities fu/fv/fwv and the temperatures fT
-template <class Ld>
-__device__ __forceinline__ double p_bc_value(const Dims &d, const Geo &g, const Fields &F, const Phys &P,
-                                             const double *pr, const double *fu, const double *fv, const double *fwv,
-                                             const double *fT, int b) {
+template <class Ld, class R>
+__device__ __forceinline__ double p_bc_value(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P,
+                                             const R *pr, const R *fu, const R *fv, const R *fwv, const R *fT,
+                                             int b) {
   const size_t NF = d.NF, NB = d.NBF;
   const BFace B = bface(d, b);
   const Cell M1 = B.cell;
@@ -1203,13 +1231,13 @@ __device__ __forceinline__ double p_bc_value(const Dims &d, const Geo &g, const 
     const double v[3] = {fu[pt], fv[pt], fwv[pt]};
     vn[j] = dot3(v, n);
   }
-  const double *a = g.bca;
+  const R *a = g.bca;
   const double d2udn2 = -(a[b] * vn[1]) - a[NB + b] * vn[2] - a[2 * NB + b] * vn[3] - a[3 * NB + b] * vn[4] -
                         a[4 * NB + b] * vn[5];
   const int dd = (pos + 1) / 2;
   const double B2 = tangential<Ld>(d, pr, M1, pos, tr1(dd)) * g.bcg[b];
   const double B3 = tangential<Ld>(d, pr, M1, pos, tr2(dd)) * g.bcg[NB + b];
-  const double *ap = g.bcap;
+  const R *ap = g.bcap;
   const double B1 = ap[7 * NB + b] * (F.Rp[M1.c]);
   double s = 0.0;
   bool firstterm = true;
@@ -1225,7 +1253,8 @@ __device__ __forceinline__ double p_bc_value(const Dims &d, const Geo &g, const 
 }
 
 // ---- K4: apply_pressure_bc, every wall face from the values before the pass
-__global__ void __launch_bounds__(BLK) k_p_bc(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+template <class R>
+__global__ void __launch_bounds__(BLK) k_p_bc(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
@@ -1235,9 +1264,9 @@ __global__ void __launch_bounds__(BLK) k_p_bc(Dims d, Geo g, Fields F, Phys P, C
   double e[1] = {0.};
   if (b < d.NBF) {
     const size_t NF = d.NF;
-    const double *pr = F.f[3] + par * NF;
-    const double nw = p_bc_value<LdPlain>(d, g, F, P, pr, F.f[0] + nh * NF, F.f[1] + nh * NF, F.f[2] + nh * NF,
-                                          F.f[4] + par * NF, b);
+    const R *pr = F.f[3] + par * NF;
+    const double nw = stored<R>(p_bc_value<LdPlain>(d, g, F, P, pr, F.f[0] + nh * NF, F.f[1] + nh * NF,
+                                                    F.f[2] + nh * NF, F.f[4] + par * NF, b));
     const BFace B = bface(d, b);
     const int fw0 = B.cell.face(d, B.pos);
     F.f[3][(1 - par) * NF + fw0] = nw;
@@ -1246,7 +1275,8 @@ __global__ void __launch_bounds__(BLK) k_p_bc(Dims d, Geo g, Fields F, Phys P, C
   block_max<1>(red, e, ctl->err[par] + 3);
 }
 
-__global__ void k_p_bc_copy(Dims d, Fields F, Ctrl *ctl) {
+template <class R>
+__global__ void k_p_bc_copy(Dims d, FieldsT<R> F, Ctrl *ctl) {
   if (ctl->done) return;
   const int par = parity(ctl);
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1275,14 +1305,14 @@ __host__ __device__ constexpr int p_term(int dd, int t) {
 
 // ---- integrate_pressure_field_i for the +xi_dd face of cell x
 // (nse.f90:1091-1289): the new value from the pressures pr
-template <class Ld>
-__device__ __forceinline__ double p_face_value(const Dims &d, const Geo &g, const Fields &F, const Phys &P,
-                                               const double *pr, const Cell &x, int dd) {
+template <class Ld, class R>
+__device__ __forceinline__ double p_face_value(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P,
+                                               const R *pr, const Cell &x, int dd) {
   const size_t Nc = d.Nc;
   const int c = x.c;
   const int diag = (dd == 1) ? 2 : (dd == 2) ? 6 : 10;
   const Cell n2 = x.nb(d, 2 * dd);
-  const double *A = g.AA + (size_t)15 * (dd - 1) * Nc;
+  const R *A = g.AA + (size_t)15 * (dd - 1) * Nc;
   const double B1 = (F.Rp[c]) * A[12 * Nc + c];
   const double B2 = (F.Rp[n2.c]) * A[14 * Nc + c];
   const double B3 = (g.dg[(2 * (dd - 1)) * Nc + c]) * tangential<Ld>(d, pr, x, 2 * dd, tr1(dd));
@@ -1305,14 +1335,14 @@ __device__ __forceinline__ double p_face_value(const Dims &d, const Geo &g, cons
 // AA_v, the two cell time terms, the R sums Bq of both cells and the
 // tangential cross terms (the centred B3/B4 the source forms first are
 // overwritten before use).  fr faces, cv / co cells and old cells.
-template <class Ld>
-__device__ __forceinline__ double v1_face_value(const Dims &d, const Geo &g, const Fields &F, const Phys &P,
-                                                const double *fr, const double *cv, const double *co,
-                                                const double *Bq, const Cell &x, int dd, double w) {
+template <class Ld, class R>
+__device__ __forceinline__ double v1_face_value(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P,
+                                                const R *fr, const R *cv, const R *co, const R *Bq, const Cell &x,
+                                                int dd, double w) {
   const size_t Nc = d.Nc;
   const int c = x.c;
   const Cell n2 = x.nb(d, 2 * dd);
-  const double *A = F.AAv + (size_t)15 * (dd - 1) * Nc;
+  const R *A = F.AAv + (size_t)15 * (dd - 1) * Nc;
   const double B1 = Bq[c] * A[12 * Nc + c] * 2 * P.DT;
   const double B2 = Bq[n2.c] * A[14 * Nc + c] * 2 * P.DT;
   const double B3 = (g.dg[(2 * (dd - 1)) * Nc + c]) * tangential<Ld>(d, fr, x, 2 * dd, tr1(dd));
@@ -1332,7 +1362,8 @@ __device__ __forceinline__ double v1_face_value(const Dims &d, const Geo &g, con
 
 // ---- K2 of formulation 1: +xi face updates of u, v, w (nse.f90:378-826),
 // cur -> next.  Block (CB, 3): threadIdx.y = direction.
-__global__ void __launch_bounds__(CB3, 2) k_vel1_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+template <class R>
+__global__ void __launch_bounds__(CB3, 2) k_vel1_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<3>(red);
@@ -1349,9 +1380,9 @@ __global__ void __launch_bounds__(CB3, 2) k_vel1_face(Dims d, Geo g, Fields F, P
       const int fo = x.face(d, 2 * dd);
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
-        const double *fr = F.f[q] + par * NF;
-        const double nw =
-            v1_face_value<LdPlain>(d, g, F, P, fr, F.c[q], F.co[q], F.Bv + (size_t)q * Nc, x, dd, P.w[q]);
+        const R *fr = F.f[q] + par * NF;
+        const double nw = stored<R>(
+            v1_face_value<LdPlain>(d, g, F, P, fr, F.c[q], F.co[q], F.Bv + (size_t)q * Nc, x, dd, P.w[q]));
         F.f[q][(1 - par) * NF + fo] = nw;
         e[q] = errv(nw, fr[fo], first);
       }
@@ -1362,7 +1393,8 @@ __global__ void __launch_bounds__(CB3, 2) k_vel1_face(Dims d, Geo g, Fields F, P
 
 // ---- K5: integrate_pressure_field_i, cur -> next.
 // Block (CB, 3): threadIdx.y = direction.
-__global__ void __launch_bounds__(CB3, 5) k_p_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+template <class R>
+__global__ void __launch_bounds__(CB3, 5) k_p_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
@@ -1376,8 +1408,8 @@ __global__ void __launch_bounds__(CB3, 5) k_p_face(Dims d, Geo g, Fields F, Phys
       constexpr int dd = decltype(D)::value;
       if (!x.has_nb(d, 2 * dd)) return;
       const size_t NF = d.NF;
-      const double *pr = F.f[3] + par * NF;
-      const double nw = p_face_value<LdPlain>(d, g, F, P, pr, x, dd);
+      const R *pr = F.f[3] + par * NF;
+      const double nw = stored<R>(p_face_value<LdPlain>(d, g, F, P, pr, x, dd));
       const int fo = x.face(d, 2 * dd);
       F.f[3][(1 - par) * NF + fo] = nw;
       e[0] = errv(nw, pr[fo], first);
@@ -1387,7 +1419,8 @@ __global__ void __launch_bounds__(CB3, 5) k_p_face(Dims d, Geo g, Fields F, Phys
 }
 
 // ---- K5b (is_dpdx_tolerance): cell pressure gradients (nse.f90:292-307)
-__global__ void __launch_bounds__(BLK) k_p_dpdx(Dims d, Geo g, Fields F, Ctrl *ctl) {
+template <class R>
+__global__ void __launch_bounds__(BLK) k_p_dpdx(Dims d, GeoT<R> g, FieldsT<R> F, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
@@ -1399,9 +1432,10 @@ __global__ void __launch_bounds__(BLK) k_p_dpdx(Dims d, Geo g, Fields F, Ctrl *c
     const size_t Nc = d.Nc, NF = d.NF;
     int f[7];
     cell_faces(d, x, f);
-    const double *p = F.f[3] + newhalf(ctl) * NF;
-    const double v[3] = {(p[f[2]] - p[f[1]]) / 2. * g.xi[0 * Nc + c], (p[f[4]] - p[f[3]]) / 2. * g.xi[4 * Nc + c],
-                         (p[f[6]] - p[f[5]]) / 2. * g.xi[8 * Nc + c]};
+    const R *p = F.f[3] + newhalf(ctl) * NF;
+    const double v[3] = {stored<R>((p[f[2]] - p[f[1]]) / 2. * g.xi[0 * Nc + c]),
+                         stored<R>((p[f[4]] - p[f[3]]) / 2. * g.xi[4 * Nc + c]),
+                         stored<R>((p[f[6]] - p[f[5]]) / 2. * g.xi[8 * Nc + c])};
     for (int q = 0; q < 3; ++q) {
       e[0] = nmax(e[0], fabs(v[q] - F.dpd[q * Nc + c]));
       F.dpd[q * Nc + c] = v[q];
@@ -1411,7 +1445,8 @@ __global__ void __launch_bounds__(BLK) k_p_dpdx(Dims d, Geo g, Fields F, Ctrl *c
 }
 
 // ---- K6: apply_zero_flux (bc.f90:345-390) on the z walls, in place
-__global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, Geo g, Fields F, Ctrl *ctl) {
+template <class R>
+__global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, GeoT<R> g, FieldsT<R> F, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
@@ -1424,10 +1459,10 @@ __global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, Geo g, Fields F, Ctrl
     const BFace B = bface(d, b);
     const int in = (B.pos == 5) ? 6 : 5;
     const Cell c2 = B.cell.nb(d, in), c3 = c2.nb(d, in);
-    double *T = F.f[4] + par * NF;
+    R *T = F.f[4] + par * NF;
     const int f1 = B.cell.face(d, B.pos);
-    const double nw = (+g.zf[NB + b] * T[B.cell.face(d, in)] - g.zf[2 * NB + b] * T[c2.face(d, in)] +
-                       g.zf[3 * NB + b] * T[c3.face(d, in)]) / g.zf[b];
+    const double nw = stored<R>((+g.zf[NB + b] * T[B.cell.face(d, in)] - g.zf[2 * NB + b] * T[c2.face(d, in)] +
+                                 g.zf[3 * NB + b] * T[c3.face(d, in)]) / g.zf[b]);
     e[0] = errv(nw, T[f1], first);
     T[f1] = nw;
   }
@@ -1441,7 +1476,8 @@ __global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, Geo g, Fields F, Ctrl
 // instruction-bound piece of the pass, and every warp can issue.
 // Grid (3, ceil(Nc/BLK)): blockIdx.x is the direction, so the three
 // directions of the same cells run side by side and share their loads.
-__global__ void __launch_bounds__(BLK, 4) k_T_coef(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+template <class R>
+__global__ void __launch_bounds__(BLK, 4) k_T_coef(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   const int c = blockIdx.y * BLK + threadIdx.x;
   if (c >= d.Nc) return;
@@ -1465,8 +1501,8 @@ __global__ void __launch_bounds__(BLK, 4) k_T_coef(Dims d, Geo g, Fields F, Phys
 // in the reference's order.
 // SRC_ONLY (reference-order schedule): store MT_F4 and R_D_T and leave the
 // update to k_seq_T.
-template <bool SRC_ONLY>
-__global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+template <bool SRC_ONLY, class R>
+__global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
@@ -1481,12 +1517,12 @@ __global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, Geo g, Fields F, Phys
   const int c = x.c;
   double e[1] = {0.};
   const size_t Nc = d.Nc, NF = d.NF;
-  const double *T = F.f[4] + par * NF;
+  const R *T = F.f[4] + par * NF;
   int f[7];
   cell_faces(d, x, f);
   if (active) by_dir(threadIdx.y, [&](auto D) {
     constexpr int dd = decltype(D)::value, y = dd - 1;
-    const double *MA = F.MTA + (size_t)y * Nc;  // MT_A(q, dd) at MA[3q Nc]
+    const R *MA = F.MTA + (size_t)y * Nc;  // MT_A(q, dd) at MA[3q Nc]
     double G[5] = {0., 0., 0., 0., 0.};
     if (x.has_nb(d, 2 * dd)) {
       const int c2 = x.nb(d, 2 * dd).c;
@@ -1528,7 +1564,7 @@ __global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, Geo g, Fields F, Phys
     for (int k = 0; k < 8; ++k) F4[k] = sF4[k][tx];
     const double pxy = sX[0][0][tx], pzy = sX[0][1][tx], pyx = sX[1][0][tx], pzx = sX[1][1][tx];
     const double pxz = sX[2][0][tx], pyz = sX[2][1][tx];
-    const double *gij = g.gij;
+    const R *gij = g.gij;
     const double RDT = P.alpha * (sG[tx] - gij[3 * Nc + c] * pxy - gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz -
                                   gij[2 * Nc + c] * pzx - gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
     if (SRC_ONLY) {
@@ -1536,7 +1572,7 @@ __global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, Geo g, Fields F, Phys
       F.RDT[c] = RDT;
     } else {
       const double cold = F.c[3][c];
-      const double nw = cell_update(T, f, cold, F.co[3][c], (RDT + 0.), F4, P.w[3]);
+      const double nw = stored<R>(cell_update(T, f, cold, F.co[3][c], (RDT + 0.), F4, P.w[3]));
       F.c[3][c] = nw;
       e[0] = errv(nw, cold, first);
     }
@@ -1546,7 +1582,8 @@ __global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, Geo g, Fields F, Phys
 
 // ---- K8: +xi face updates of T (nse.f90:1033-1088), cur -> next; the z-wall
 // values set by apply_zero_flux travel to the next half too
-__global__ void __launch_bounds__(BLK, 4) k_T_face(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl) {
+template <class R>
+__global__ void __launch_bounds__(BLK, 4) k_T_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
@@ -1558,16 +1595,16 @@ __global__ void __launch_bounds__(BLK, 4) k_T_face(Dims d, Geo g, Fields F, Phys
   double e[1] = {0.};
   if (act) {
     const size_t Nc = d.Nc, NF = d.NF;
-    const double *T = F.f[4] + par * NF;
-    double *Tn = F.f[4] + (1 - par) * NF;
+    const R *T = F.f[4] + par * NF;
+    R *Tn = F.f[4] + (1 - par) * NF;
     for (int dd = 1; dd <= 3; ++dd) {
       if (!x.has_nb(d, 2 * dd)) continue;
       const Cell x2 = x.nb(d, 2 * dd);
       double Fd[5];
       for (int k = 0; k < 5; ++k) Fd[k] = F.MTF[(size_t)(5 * (dd - 1) + k) * Nc + c];
       const int fo = x.face(d, 2 * dd);
-      const double nw = face_update(d, T, F.c[3], F.co[3], Fd, g.dg[(2 * (dd - 1)) * Nc + c],
-                                    g.dg[(2 * (dd - 1) + 1) * Nc + c], dd, x, x2, P.w[3]);
+      const double nw = stored<R>(face_update(d, T, F.c[3], F.co[3], Fd, g.dg[(2 * (dd - 1)) * Nc + c],
+                                              g.dg[(2 * (dd - 1) + 1) * Nc + c], dd, x, x2, P.w[3]));
       Tn[fo] = nw;
       e[0] = nmax(e[0], errv(nw, T[fo], first));
     }
@@ -1578,8 +1615,13 @@ __global__ void __launch_bounds__(BLK, 4) k_T_face(Dims d, Geo g, Fields F, Phys
 }
 
 // ---- K9: end of one pass (find_error's maxima, the do-while test of
-// nse.f90:129 and the max_iters guard)
-__global__ void k_iter_end(Ctrl *ctl, Phys P) {
+// nse.f90:129 and the max_iters guard).  lowp: a pass of the FP32 phase of a
+// mixed-precision step, which ends (done, status untouched) when every field
+// meets its tolerance or when kLowpStall passes in a row brought no field
+// that is still above its tolerance to a new smallest change; the FP64
+// passes that follow apply the reference's test.  max_iters bounds both
+// phases together.
+__global__ void k_iter_end(Ctrl *ctl, Phys P, int lowp) {
   if (ctl->done) return;
   const int par = ctl->iter & ctl->pmask;
   double e[5];
@@ -1601,6 +1643,25 @@ __global__ void k_iter_end(Ctrl *ctl, Phys P) {
   ctl->first = 0;
   bool busy = false;
   for (int q = 0; q < 5; ++q) busy = busy || (e[q] > P.tol[q]);
+  if (lowp) {
+    ctl->lowp_iters += 1;
+    bool progress = false;
+    for (int q = 0; q < 5; ++q) {
+      if (e[q] > P.tol[q] && e[q] < ctl->best[q]) progress = true;
+      if (e[q] < ctl->best[q]) ctl->best[q] = e[q];
+    }
+    ctl->stall = progress ? 0 : ctl->stall + 1;
+    if (!finite) {
+      ctl->done = 1;
+      ctl->status = -4;  // NIM_ERR_NONFINITE
+    } else if (!busy || ctl->stall >= kLowpStall) {
+      ctl->done = 1;
+    } else if (P.max_iters > 0 && ctl->step_iters >= P.max_iters) {
+      ctl->done = 1;
+      ctl->status = -3;  // NIM_ERR_NOT_CONVERGED
+    }
+    return;
+  }
   if (!finite) {
     ctl->done = 1;
     ctl->status = -4;  // NIM_ERR_NONFINITE
@@ -1610,6 +1671,35 @@ __global__ void k_iter_end(Ctrl *ctl, Phys P) {
     ctl->done = 1;
     ctl->status = -3;  // NIM_ERR_NOT_CONVERGED
   }
+}
+
+// start of the FP32 phase of a mixed-precision step (after k_step_reset)
+__global__ void k_lowp_begin(Ctrl *ctl) {
+  ctl->lowp_iters = 0;
+  ctl->stall = 0;
+  for (int q = 0; q < 5; ++q) ctl->best[q] = __longlong_as_double(0x7FF0000000000000ll);  // +inf
+}
+
+// FP32 phase over, FP64 passes next (not after a non-finite stop)
+__global__ void k_lowp_end(Ctrl *ctl) {
+  if (ctl->status == 0) ctl->done = 0;
+}
+
+// Conversions between the FP64 arrays and their FP32 mirror: entry
+// blockIdx.y of the list, grid-stride over its elements
+struct CvtList {
+  static constexpr int kMax = 32;
+  const void *src[kMax];
+  void *dst[kMax];
+  long long n[kMax];
+};
+template <class S, class D>
+__global__ void __launch_bounds__(BLK) k_convert(CvtList L) {
+  const S *__restrict__ src = static_cast<const S *>(L.src[blockIdx.y]);
+  D *__restrict__ dst = static_cast<D *>(L.dst[blockIdx.y]);
+  const long long n = L.n[blockIdx.y];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (D)src[i];
 }
 
 // ============================================ reference-order sweeps

@@ -36,6 +36,7 @@ M_F4, M_F1, M_F2, M_F3 = 48, 49, 50, 51
 
 CLUSTER_NONE, CLUSTER_POWER, CLUSTER_TANH = 0, 1, 2
 SCHEDULE_PARALLEL, SCHEDULE_REFERENCE = 0, 1
+PRECISION_FP64, PRECISION_MIXED = 0, 1
 OUTPUT_PLOT, OUTPUT_RESTART = 0, 1   # nim_output_set
 
 
@@ -69,7 +70,7 @@ class Params(C.Structure):
         ("bc_value", (C.c_double * NIM_NBC) * 5),
         ("max_iters", C.c_int32), ("check_steady", C.c_int32),
         ("dpdx_tolerance", C.c_int32), ("schedule", C.c_int32), ("formulation", C.c_int32),
-        ("reserved", C.c_int32),
+        ("precision", C.c_int32),
     ]
 
 
@@ -82,6 +83,7 @@ class StepStats(C.Structure):
         ("nu_outer", C.c_double), ("nu_inner", C.c_double),
         ("area_outer", C.c_double), ("area_inner", C.c_double),
         ("time", C.c_double), ("steady", C.c_int32), ("status", C.c_int32),
+        ("iters_fp32", C.c_int32), ("pad", C.c_int32),
     ]
 
     def as_dict(self) -> dict:

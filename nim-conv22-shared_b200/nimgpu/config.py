@@ -55,6 +55,7 @@ def reference_params(**over) -> _abi.Params:
     p.dpdx_tolerance = 0
     p.schedule = _abi.SCHEDULE_PARALLEL
     p.formulation = 2            # parameters.f90:194
+    p.precision = _abi.PRECISION_FP64
     for k, v in over.items():
         setattr(p, k, v)
     return p
