@@ -12,16 +12,19 @@
 // With NIM_PRECISION_MIXED each step's inner loop runs first as FP32 passes
 // over a float mirror of the arrays the pass touches, then as FP64 passes
 // from the widened FP32 iterate until the reference's stop test holds.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "nim_gpu.h"
@@ -100,6 +103,11 @@ struct nim_ctx {
   // writes, the graph of FP32 passes, the phase of the current step (1: FP32
   // passes queued, 2: FP64 passes) and the last step's pass count per phase
   bool mixed = false;
+  // k_vel_face_tile (TMA-staged z-marching face sweep): whether it runs, its
+  // z-chunk length and its tensor maps, one set per storage type
+  bool bulk = false;
+  int tile_kc = 0;
+  VelFaceMaps vmap64{}, vmap32{};
   GeoT<float> g32{};
   FieldsT<float> F32{};
   cudaGraphExec_t graph32 = nullptr;
@@ -265,8 +273,15 @@ int launch_vel(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F
   } else {
     k_vel_cell<false, 2><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
     TRY(mark(x, "k_vel_cell"));
-    k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
-    TRY(mark(x, "k_vel_face"));
+    if (x->bulk) {
+      const dim3 gt((d.NT + 31) / 32, (d.NR + VT_R - 1) / VT_R, (d.NZ + x->tile_kc - 1) / x->tile_kc);
+      const VelFaceMaps &M = std::is_same<R, double>::value ? x->vmap64 : x->vmap32;
+      k_vel_face_tile<R><<<gt, dim3(VT_T, 3), VtLayout<R>::bytes, s>>>(d, g, F, x->phys, x->ctl, x->tile_kc, M);
+      TRY(mark(x, "k_vel_face_tile"));
+    } else {
+      k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+      TRY(mark(x, "k_vel_face"));
+    }
   }
   return NIM_OK;
 }
@@ -733,6 +748,91 @@ static int setup_levels(nim_ctx *x) {
   return NIM_OK;
 }
 
+// ---- tensor maps of k_vel_face_tile (cuTensorMapEncodeTiled through the
+// runtime's driver entry point: no link against the driver library)
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+  });
+  return fn;
+}
+
+// rank-dimensional map of a dense array starting at base: dims[0] fastest,
+// strides of dims 1.. in elements, box in elements; out-of-range elements
+// of a box read as zero
+template <class R>
+static bool encode_map(CUtensorMap *map, const R *base, int rank, const uint64_t *dims, const uint64_t *strides,
+                       const uint32_t *box) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  cuuint64_t gd[5], gs[4];
+  cuuint32_t bx[5], es[5];
+  for (int i = 0; i < rank; ++i) {
+    gd[i] = dims[i];
+    bx[i] = box[i];
+    es[i] = 1;
+  }
+  for (int i = 0; i + 1 < rank; ++i) gs[i] = strides[i] * sizeof(R);
+  const CUtensorMapDataType t = sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  return fn(map, t, (cuuint32_t)rank, const_cast<R *>(base), gd, gs, bx, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <class R>
+static bool encode_vel_face_maps(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, VelFaceMaps &M) {
+  const uint64_t NT = d.NT, NR = d.NR, NZ = d.NZ, NF = d.NF, Nc = d.Nc;
+  bool ok = true;
+  for (int q = 0; q < 3; ++q) {
+    const uint64_t dr[4] = {NT, NR + 1, NZ, 2}, sr[3] = {NT, NT * (NR + 1), NF};
+    const uint32_t br[4] = {(uint32_t)VtLayout<R>::W, VT_R + 2, 1, 1};
+    ok = ok && encode_map(&M.rf[q], F.f[q], 4, dr, sr, br);
+    const uint64_t dt[4] = {NT, NR, NZ, 2}, dz[4] = {NT, NR, NZ + 1, 2}, st[3] = {NT, NT * NR, NF};
+    const uint32_t bt[4] = {(uint32_t)VtLayout<R>::W, VT_R + 1, 1, 1};
+    ok = ok && encode_map(&M.tf[q], F.f[q] + d.offT, 4, dt, st, bt);
+    ok = ok && encode_map(&M.zf[q], F.f[q] + d.offZ, 4, dz, st, bt);
+    const uint64_t dc[3] = {NT, NR, NZ}, sc[2] = {NT, NT * NR};
+    const uint32_t bc[3] = {(uint32_t)VtLayout<R>::W, VT_R + 1, 1};
+    ok = ok && encode_map(&M.cv[q], F.c[q], 3, dc, sc, bc);
+    ok = ok && encode_map(&M.co[q], F.co[q], 3, dc, sc, bc);
+  }
+  const uint64_t dm[4] = {NT, NR, NZ, 15}, dgd[4] = {NT, NR, NZ, 6}, sm[3] = {NT, NT * NR, Nc};
+  const uint32_t bm[4] = {32, VT_R, 1, 15}, bg[4] = {32, VT_R, 1, 6};
+  ok = ok && encode_map(&M.mf, F.MF, 4, dm, sm, bm);
+  ok = ok && encode_map(&M.dg, g.dg, 4, dgd, sm, bg);
+  return ok;
+}
+
+// The +xi face sweep of u, v, w runs as k_vel_face_tile when n_theta is a
+// multiple of 4 (16-byte box rows), at most 256, and the mesh gives at least
+// one block per SM; the z-chunk length aims at about six waves of blocks with
+// chunks of at least 8 planes.  NIM_FACE_SWEEP=tile or =gather in the
+// environment forces the choice (tile still needs the n_theta conditions).
+static int choose_face_sweep(nim_ctx *x) {
+  const Dims &d = x->d;
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device));
+  const int tiles = ((d.NT + 31) / 32) * ((d.NR + VT_R - 1) / VT_R);
+  const int want = (6 * sms + tiles - 1) / tiles;
+  const int nch = std::max(1, std::min(want, d.NZ / 8));
+  x->tile_kc = (d.NZ + nch - 1) / nch;
+  const int blocks = tiles * ((d.NZ + x->tile_kc - 1) / x->tile_kc);
+  const bool shape = (d.NT % 4 == 0) && d.NT <= 256;
+  const char *env = std::getenv("NIM_FACE_SWEEP");
+  const std::string force = env ? env : "";
+  x->bulk = shape && !x->seq && (force == "tile" || (force != "gather" && blocks >= sms));
+  return NIM_OK;
+}
+
 static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) {
   CK(cudaGetDevice(&x->device));
   TRY(noalloc_setup(x->device));
@@ -745,6 +845,7 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
   TRY(verify_mesh(m, d, perm));
   x->params = *p;
   x->seq = (p->schedule == NIM_SCHEDULE_REFERENCE);
+  TRY(choose_face_sweep(x));
   x->phys = make_phys(*p);
   x->gq = make_gauss();
   x->nblk_c = grid(d.Nc);
@@ -836,6 +937,16 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
   TRY(dalloc(x, &x->scratch, std::max(54 * Nc, 3 * NF)));
   TRY(dalloc(x, &x->sums, 8));
   CK(cudaMallocHost(&x->ctl_host, sizeof(Ctrl)));
+  if (x->bulk && !x->seq) {
+    x->bulk = encode_vel_face_maps(d, x->g, x->F, x->vmap64) &&
+              (!x->mixed || encode_vel_face_maps(d, x->g32, x->F32, x->vmap32));
+    if (x->bulk) {
+      CK(cudaFuncSetAttribute(k_vel_face_tile<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)VtLayout<double>::bytes));
+      CK(cudaFuncSetAttribute(k_vel_face_tile<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)VtLayout<float>::bytes));
+    }
+  }
   if (x->seq) TRY(setup_levels(x));
   CK(cudaMemcpyAsync(x->node_xyz, m->node_xyz, 3 * sizeof(double) * m->nnode, cudaMemcpyHostToDevice, x->stream));
   double bcv[25];

@@ -11,6 +11,8 @@
 //   k_vel_cell   calculate_gforces + calculate_R_b + calculate_R_D2 + the
 //                cell-average update of u,v,w                (in place)
 //   k_vel_face   +xi face updates of u,v,w                    (cur -> next)
+//                (k_vel_face_tile on large meshes: the same sweep with its
+//                operands staged in shared memory by TMA boxes)
 //   k_p_src      calculate_R_b_p + calculate_R_D_p2           (-> Rp, dila)
 //   k_p_bc       apply_pressure_bc                            (cur -> next, walls)
 //   k_p_bc_copy  new wall values into cur
@@ -24,6 +26,7 @@
 // depend on thread order.
 #pragma once
 #include <cooperative_groups.h>
+#include <cuda.h>  // CUtensorMap (the maps are encoded by the host)
 
 #include "nim_common.cuh"
 
@@ -1006,20 +1009,27 @@ __device__ __forceinline__ double cell_update(const R *__restrict__ fr, const in
                         F4[7] * Ld::ld(fr, f[6]) + B);
 }
 
-// +xi_d face update (nse.f90:878-1005; T: 1033-1088); cx, cx2 the cell
-// values of x and of its +xi_d neighbour x2
+// +xi_d face update (nse.f90:878-1005; T: 1033-1088) from the face values
+// fx(pos) of cell x and fx2(pos) of its +xi_d neighbour x2, their cell
+// values cx, cx2 and old cell values ox, ox2
+template <class FX, class FX2>
+__device__ __forceinline__ double face_update_vals(FX &&fx, FX2 &&fx2, double cx, double cx2, double ox, double ox2,
+                                                   const double Fd[5], double dg0, double dg1, int dd, double w) {
+  const int e1 = tr1(dd), e2 = tr2(dd);
+  const double B3 = (dg0) * (fx(2 * e1) - fx(2 * e1 - 1) + fx2(2 * e1) - fx2(2 * e1 - 1)) / 4.0;
+  const double B4 = (dg1) * (fx(2 * e2) - fx(2 * e2 - 1) + fx2(2 * e2) - fx2(2 * e2 - 1)) / 4.0;
+  return (1 - w) * fx(2 * dd) +
+         (w / Fd[0]) * (+Fd[1] * fx(2 * dd - 1) + Fd[2] * fx2(2 * dd) + Fd[3] * (cx + ox) + Fd[4] * (cx2 + ox2) -
+                        B3 - B4);
+}
+// the same from the face array fr; cx, cx2 the cell values of x and x2
 template <class Ld = LdPlain, class R>
 __device__ __forceinline__ double face_update_cv(const Dims &d, const R *__restrict__ fr, double cx, double cx2,
                                                  const R *__restrict__ co, const double Fd[5], double dg0,
                                                  double dg1, int dd, const Cell &x, const Cell &x2, double w) {
-  const int e1 = tr1(dd), e2 = tr2(dd);
-  const double B3 = (dg0) * (Ld::ld(fr, x.face(d, 2 * e1)) - Ld::ld(fr, x.face(d, 2 * e1 - 1)) +
-                             Ld::ld(fr, x2.face(d, 2 * e1)) - Ld::ld(fr, x2.face(d, 2 * e1 - 1))) / 4.0;
-  const double B4 = (dg1) * (Ld::ld(fr, x.face(d, 2 * e2)) - Ld::ld(fr, x.face(d, 2 * e2 - 1)) +
-                             Ld::ld(fr, x2.face(d, 2 * e2)) - Ld::ld(fr, x2.face(d, 2 * e2 - 1))) / 4.0;
-  return (1 - w) * Ld::ld(fr, x.face(d, 2 * dd)) +
-         (w / Fd[0]) * (+Fd[1] * Ld::ld(fr, x.face(d, 2 * dd - 1)) + Fd[2] * Ld::ld(fr, x2.face(d, 2 * dd)) +
-                        Fd[3] * (cx + co[x.c]) + Fd[4] * (cx2 + co[x2.c]) - B3 - B4);
+  return face_update_vals([&](int pos) { return Ld::ld(fr, x.face(d, pos)); },
+                          [&](int pos) { return Ld::ld(fr, x2.face(d, pos)); }, cx, cx2, (double)co[x.c],
+                          (double)co[x2.c], Fd, dg0, dg1, dd, w);
 }
 template <class Ld = LdPlain, class R>
 __device__ __forceinline__ double face_update(const Dims &d, const R *__restrict__ fr, const R *__restrict__ cv,
@@ -1038,6 +1048,46 @@ __device__ __forceinline__ double cell_update_f1(const R *__restrict__ fr, const
                             at[3] * Ld::ld(fr, f[4]) - at[4] * Ld::ld(fr, f[5]) - at[5] * Ld::ld(fr, f[6]) -
                             at[7] * cold - Bij) /
                            (at[8]);
+}
+
+// ---- bulk copies into shared memory: cp.async.bulk rows whose completion
+// is counted in bytes on an mbarrier (phase 0, one arrival: the thread that
+// posts the byte count).  Every wait is bounded; a wait that runs out marks
+// the step NIM_ERR_TIMEOUT and stopped, then waits (bounded) once more so
+// that no copy lands in shared memory after the block has left.
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// dst and src 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+constexpr int kWaitTries = 1 << 22;  // each try suspends for a hardware-chosen slice
+__device__ __noinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, Ctrl *ctl) {
+  for (int n = 0; n < kWaitTries; ++n)
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicCAS(&ctl->status, 0, -5);  // NIM_ERR_TIMEOUT
+  *(volatile int *)&ctl->done = 1;
+  for (int n = 0; n < kWaitTries; ++n)
+    if (mbar_try_wait(bar, parity)) break;
+  return false;
 }
 
 __device__ __forceinline__ double errv(double nw, double old, bool first) { return fabs(nw - (first ? 0.0 : old)); }
@@ -1144,6 +1194,254 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, GeoT<R> g, FieldsT<
     });
   }
   block_max<3, CB3>(red, e, ctl->err[par]);
+}
+
+// ---- K2, z-marching form: the same face updates, one block per patch of
+// 32 theta x VT_R r cells marching up a chunk of kc z-planes.  Every value
+// the updates read arrives in shared memory by TMA box loads
+// (cp.async.bulk.tensor, completion counted in bytes on an mbarrier per
+// buffer): per plane p, for each velocity component, the r, theta and z
+// (level p) faces of the current half and the cell and old-cell values as
+// W x (VT_R + 1 or 2) boxes (the theta halo: columns i0+32, i0+33; at the
+// seam those two columns are fetched with plain loads and written in after
+// the box lands), in a ring of VT_S planes; and per plane the patch's
+// M_F1..3 and metric-difference rows as one 32 x VT_R x 21 box pair in a
+// ring of two.  Plane k is computed from ring planes k, k+1, k+2 while the
+// block's other resident neighbour on the SM computes; k+3 is issued once
+// plane k is done.  The arithmetic is k_vel_face's
+// (face_update_vals): the results are identical.
+// Needs n_theta % 4 == 0 and n_theta <= 256 (box rows of 16-byte multiples).
+constexpr int VT_R = 4;         // r rows of cells per patch
+constexpr int VT_T = 32 * VT_R;  // cells per patch = blockDim.x (blockDim.y = 3 directions)
+constexpr int VT_S = 3;          // plane ring depth (FP64: 109 KB with the coefficient ring)
+constexpr int VT_MINB = 2;       // resident blocks per SM the launch bounds ask for
+
+// tensor maps of one storage type, encoded by the host: per component the
+// r / theta / z parts of the face array as {NT, rows, planes, half}, the
+// cell and old-cell arrays as {NT, NR, NZ}, M_F1..3 and the metric
+// differences as {NT, NR, NZ, rows}
+struct VelFaceMaps {
+  CUtensorMap rf[3], tf[3], zf[3], cv[3], co[3], mf, dg;
+};
+
+// shared-memory layout (elements of R; every box starts on 128 bytes)
+template <class R>
+struct VtLayout {
+  // staged columns: 32 cells + the 2-column halo, rounded to 16-byte box rows
+  static constexpr int W = sizeof(R) == 8 ? 34 : 36;
+  static constexpr int up(int bytes) { return (bytes + 127) / 128 * 128 / (int)sizeof(R); }
+  static constexpr int RF = up((VT_R + 2) * W * (int)sizeof(R));  // r-face box region
+  static constexpr int C5 = up((VT_R + 1) * W * (int)sizeof(R));  // theta / z / cell box region
+  static constexpr int Q = RF + 4 * C5;                              // one component
+  static constexpr int PLANE = 3 * Q;
+  static constexpr int MF = 15 * VT_R * 32, DG = 6 * VT_R * 32, COEF = MF + DG;
+  static constexpr int BARS = VT_S * PLANE + 2 * COEF;  // element offset of the mbarriers
+  // + 128: the kernel rounds the dynamic shared-memory base up to 128 bytes
+  static constexpr size_t bytes = (size_t)BARS * sizeof(R) + (VT_S + 2) * sizeof(unsigned long long) + 128;
+  static constexpr unsigned plane_tx = 3u * ((VT_R + 2) + 4 * (VT_R + 1)) * W * sizeof(R);
+  static constexpr unsigned zlevel_tx = 3u * (VT_R + 1) * W * sizeof(R);
+  static constexpr unsigned coef_tx = (unsigned)(COEF * sizeof(R));
+};
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z,
+                                            unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int x, int y, int z, int w,
+                                            unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// plane bundle p (one thread): levels p of the z faces and, for p < NZ, the
+// r and theta faces and the cell values of plane p
+template <class R>
+__device__ void vt_issue_plane(const VelFaceMaps &M, R *slot, unsigned long long *bar, int i0, int j0, int p,
+                               int par, int NZ) {
+  using L = VtLayout<R>;
+  const bool cells = p < NZ;
+  mbar_expect_tx(bar, cells ? L::plane_tx : L::zlevel_tx);
+  for (int q = 0; q < 3; ++q) {
+    R *b = slot + q * L::Q;
+    tma_load_4d(b + L::RF + L::C5, &M.zf[q], i0, j0, p, par, bar);
+    if (!cells) continue;
+    tma_load_4d(b, &M.rf[q], i0, j0, p, par, bar);
+    tma_load_4d(b + L::RF, &M.tf[q], i0, j0, p, par, bar);
+    tma_load_3d(b + L::RF + 2 * L::C5, &M.cv[q], i0, j0, p, bar);
+    tma_load_3d(b + L::RF + 3 * L::C5, &M.co[q], i0, j0, p, bar);
+  }
+}
+template <class R>
+__device__ void vt_issue_coef(const VelFaceMaps &M, R *coef, unsigned long long *bar, int i0, int j0, int p) {
+  using L = VtLayout<R>;
+  mbar_expect_tx(bar, L::coef_tx);
+  tma_load_4d(coef, &M.mf, i0, j0, p, 0, bar);
+  tma_load_4d(coef + L::MF, &M.dg, i0, j0, p, 0, bar);
+}
+
+// the theta-seam columns of plane bundle p: value u (< 3 x 2 x row slots) of the
+// patch at the seam, global source and ring position; false if u names a
+// row outside the mesh or an array the bundle does not hold
+template <class R>
+__device__ __forceinline__ bool vt_seam(const Dims &d, const FieldsT<R> &F, int par, int i0, int j0, int ncell, int p,
+                                        int u, const R *&src, int &dst) {
+  using L = VtLayout<R>;
+  constexpr int per_q = 2 * (VT_R + 2 + 4 * (VT_R + 1));  // 2 columns x row slots
+  const int q = u / per_q, r = u - q * per_q, col = r & 1, k = r >> 1;
+  int kind, row;
+  if (k < VT_R + 2) {
+    kind = 0;
+    row = k;
+  } else {
+    kind = 1 + (k - (VT_R + 2)) / (VT_R + 1);
+    row = (k - (VT_R + 2)) % (VT_R + 1);
+  }
+  const int j = j0 + row;
+  if (kind == 0 ? j > d.NR : j > d.NR - 1) return false;
+  if (p >= d.NZ && kind != 2) return false;  // top level: z faces only
+  const size_t NT = d.NT, NR = d.NR;
+  const R *fq = F.f[q] + (size_t)par * d.NF;
+  switch (kind) {
+    case 0: src = fq + NT * (j + (NR + 1) * p) + col; break;
+    case 1: src = fq + d.offT + NT * (j + NR * p) + col; break;
+    case 2: src = fq + d.offZ + NT * (j + NR * p) + col; break;
+    case 3: src = F.c[q] + NT * (j + NR * p) + col; break;
+    default: src = F.co[q] + NT * (j + NR * p) + col; break;
+  }
+  const int base = q * L::Q + (kind == 0 ? 0 : L::RF + (kind - 1) * L::C5);
+  dst = base + row * L::W + ncell + col;
+  return true;
+}
+
+template <class R>
+__global__ void __launch_bounds__(3 * VT_T, VT_MINB)
+    k_vel_face_tile(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl, int kc, const __grid_constant__ VelFaceMaps M) {
+  using L = VtLayout<R>;
+  if (ctl->done) return;
+  extern __shared__ __align__(128) unsigned char vt_raw[];
+  R *ring = reinterpret_cast<R *>(vt_raw + ((128u - (smem_u32(vt_raw) & 127u)) & 127u));
+  R *coefs = ring + VT_S * L::PLANE;
+  unsigned long long *bar_pl = reinterpret_cast<unsigned long long *>(ring + L::BARS);
+  unsigned long long *bar_cf = bar_pl + VT_S;
+  __shared__ BlockRed red;
+  const int tid = threadIdx.x + VT_T * threadIdx.y;
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * VT_R;
+  const int ncell = min(32, d.NT - i0);
+  const bool seam = d.NT - i0 <= 32;  // columns ncell, ncell+1 wrap to theta 0, 1
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int kb = blockIdx.z * kc, ke = min(kb + kc, d.NZ);
+  const int nplanes = min(ke + 2, d.NZ + 1) - kb;  // plane bundles kb .. kb+nplanes-1
+  const int ncoef = ke - kb;
+  if (tid == 0) {
+    for (int s = 0; s < VT_S + 2; ++s) mbar_init(&bar_pl[s], 1);
+  }
+  red_init<3>(red);  // barrier: the mbarriers exist before any copy
+  if (tid == 0) {
+    for (int l = 0; l < VT_S && l < nplanes; ++l)
+      vt_issue_plane(M, ring + l * L::PLANE, &bar_pl[l], i0, j0, kb + l, par, d.NZ);
+    for (int l = 0; l < 2 && l < ncoef; ++l) vt_issue_coef(M, coefs + l * L::COEF, &bar_cf[l], i0, j0, kb + l);
+  }
+  const int ii = threadIdx.x & 31, jj = threadIdx.x >> 5;
+  const bool act = ii < ncell && j0 + jj < d.NR;
+  const size_t NF = d.NF;
+  double e[3] = {0., 0., 0.};
+  bool ok = true;
+  for (int l = 0; l < ncoef; ++l) {
+    const int k = kb + l;
+    // bundles that become readable now: 0, 1, 2 at the start, then l + 2
+    const int m0 = (l == 0) ? 0 : l + 2, m1 = min(l + 2, nplanes - 1);
+    R seamv[3];
+    int seamd[3];
+    bool have[3] = {false, false, false};
+    if (seam && tid < 3 * 2 * (VT_R + 2 + 4 * (VT_R + 1))) {
+      for (int m = m0; m <= m1; ++m) {
+        const R *src;
+        int dst;
+        if (vt_seam(d, F, par, i0, j0, ncell, kb + m, tid, src, dst)) {
+          have[m - m0] = true;
+          seamv[m - m0] = *src;
+          seamd[m - m0] = (m % VT_S) * L::PLANE + dst;
+        }
+      }
+    }
+    bool mine = true;
+    for (int m = m0; m <= m1; ++m) mine = mine && mbar_wait(&bar_pl[m % VT_S], (m / VT_S) & 1, ctl);
+    mine = mine && mbar_wait(&bar_cf[l & 1], (l >> 1) & 1, ctl);
+    if (mine && seam) {
+      for (int n = 0; n < 3; ++n)
+        if (have[n]) ring[seamd[n]] = seamv[n];
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // before later boxes into this slot
+    }
+    if (!__syncthreads_and(mine)) {  // the same decision in every thread
+      ok = false;
+      break;
+    }
+    if (act) {
+      const Cell x = Cell::at(d, i0 + ii, j0 + jj, k);
+      const R *P0 = ring + (l % VT_S) * L::PLANE, *P1 = ring + ((l + 1) % VT_S) * L::PLANE;
+      const R *P2 = ring + ((l + 2) % VT_S) * L::PLANE;
+      const R *C = coefs + (l & 1) * L::COEF;
+      by_dir(threadIdx.y, [&](auto D) {
+        constexpr int dd = decltype(D)::value;
+        if (!x.has_nb(d, 2 * dd)) return;
+        double Fd[5];
+        for (int kq = 0; kq < 5; ++kq) Fd[kq] = C[(5 * (dd - 1) + kq) * VT_R * 32 + jj * 32 + ii];
+        const double dg0 = C[L::MF + (2 * (dd - 1)) * VT_R * 32 + jj * 32 + ii];
+        const double dg1 = C[L::MF + (2 * (dd - 1) + 1) * VT_R * 32 + jj * 32 + ii];
+        // x2 = x + e_dd sits at (ii + di, jj + dj) of plane Q0
+        constexpr int di = (dd == 2), dj = (dd == 1);
+        const R *Q0 = (dd == 3) ? P1 : P0, *Q1 = (dd == 3) ? P2 : P1;
+        const int fo = x.face(d, 2 * dd);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          // face pos of the cell at (a, b) of plane A (B: the plane above)
+          auto face = [&](const R *A, const R *B, int a, int b, int pos) -> double {
+            const R *qa = A + q * L::Q, *qb = B + q * L::Q;
+            switch (pos) {
+              case 1: return qa[b * L::W + a];
+              case 2: return qa[(b + 1) * L::W + a];
+              case 3: return qa[L::RF + b * L::W + a];
+              case 4: return qa[L::RF + b * L::W + a + 1];
+              case 5: return qa[L::RF + L::C5 + b * L::W + a];
+              default: return qb[L::RF + L::C5 + b * L::W + a];
+            }
+          };
+          auto fx = [&](int pos) { return face(P0, P1, ii, jj, pos); };
+          auto fx2 = [&](int pos) { return face(Q0, Q1, ii + di, jj + dj, pos); };
+          const R *cq0 = P0 + q * L::Q + L::RF + 2 * L::C5, *cq2 = Q0 + q * L::Q + L::RF + 2 * L::C5;
+          const double nw = stored<R>(face_update_vals(
+              fx, fx2, cq0[jj * L::W + ii], cq2[(jj + dj) * L::W + ii + di], cq0[L::C5 + jj * L::W + ii],
+              cq2[L::C5 + (jj + dj) * L::W + ii + di], Fd, dg0, dg1, dd, P.w[q]));
+          F.f[q][(1 - par) * NF + fo] = nw;
+          e[q] = nmax(e[q], errv(nw, fx(2 * dd), first));
+        }
+      });
+    }
+    __syncthreads();  // every thread is done with ring plane l and coefficient buffer l & 1
+    if (tid == 0) {
+      if (l + VT_S < nplanes)
+        vt_issue_plane(M, ring + (l % VT_S) * L::PLANE, &bar_pl[l % VT_S], i0, j0, kb + l + VT_S, par, d.NZ);
+      if (l + 2 < ncoef) vt_issue_coef(M, coefs + (l & 1) * L::COEF, &bar_cf[l & 1], i0, j0, kb + l + 2);
+    }
+  }
+  if (!ok) {
+    // a wait ran out: let the copies already issued land (bounded) before
+    // the block leaves; waiting on both parities covers the pending phase
+    for (int s = 0; s < VT_S + 2; ++s) {
+      mbar_wait(&bar_pl[s], 0, ctl);
+      mbar_wait(&bar_pl[s], 1, ctl);
+    }
+    return;
+  }
+  block_max<3, 3 * VT_T>(red, e, ctl->err[par]);
 }
 
 // ---- K3: pressure sources (calculate_R_b_p nse.f90:2362-2407,

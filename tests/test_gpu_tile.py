@@ -1,0 +1,133 @@
+"""k_vel_face_tile: the +xi face sweep of u, v, w staged in shared memory by
+TMA boxes, marching up z in chunks.  It replaces k_vel_face when n_theta is a
+multiple of 4 (at most 256) and the mesh fills the GPU with blocks;
+NIM_FACE_SWEEP=tile forces it on the small meshes here.  Both restate
+nse.f90:878-1005 with the same arithmetic, so the passes match the CPU
+oracle's parallel schedule to round-off.  The meshes below reach every edge
+of the tiling: several z-chunks and the top level, theta tiles that read
+real halo columns and a seam tile of fewer than 32 cells, and patches cut
+short in r."""
+import numpy as np
+import pytest
+
+import nimgpu
+from nimgpu import _abi, config
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def force_tile(monkeypatch):
+    monkeypatch.setenv("NIM_FACE_SWEEP", "tile")
+
+
+STATE = [
+    _abi.FACES_U, _abi.FACES_V, _abi.FACES_W, _abi.FACES_P, _abi.FACES_T,
+    _abi.MESHES_U, _abi.MESHES_V, _abi.MESHES_W, _abi.MESHES_T,
+]
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def pair(dims, **over):
+    case = config.small_case(*dims)
+    mesh = nimgpu.Mesh(case.mesh_params())
+    p = case.params(**over)
+    gpu = nimgpu.NimSolver(mesh, p)
+    gpu.initialize_nse()
+    gpu.add_temperature_noise(case.noise, case.seed)
+    ref = O.Oracle(mesh, p, schedule=O.PARALLEL)
+    ref.init()
+    nimgpu.apply_temperature_noise(ref.get, ref.set, mesh, case.noise, case.seed)
+    return gpu, ref
+
+
+@pytest.mark.parametrize("dims", [(40, 6, 30), (12, 5, 13), (36, 9, 12), (64, 4, 25)])
+def test_tiled_passes_match_parallel_oracle(dims):
+    gpu, ref = pair(dims)
+    assert "k_vel_face_tile" in gpu.profile_iterations(1)
+    gpu.close()
+    gpu, ref = pair(dims)
+    gpu.calculate_velocity_nim_constants()
+    ref.begin_step()
+    sg, so = gpu.iterate(3), ref.iterate(3)
+    for k in ("err_u", "err_v", "err_w", "err_p", "err_T"):
+        a, b = getattr(sg, k), getattr(so, k)
+        assert abs(a - b) <= 1e-9 * max(abs(b), 1e-30) + 1e-300, (k, a, b)
+    for f in STATE:
+        a = gpu.download(f)
+        b = ref.get(f, a.size)
+        if f == _abi.FACES_P:
+            a, b = a - a.mean(), b - b.mean()
+        assert rel(a, b) <= 1e-12, f
+    gpu.close()
+
+
+def test_tiled_steps_match_parallel_oracle():
+    gpu, ref = pair((40, 6, 14))
+    sg = gpu.solve_nse(2)
+    _, so = ref.step(2)
+    assert [a.iters for a in sg] == [b.iters for b in so]
+    for a, b in zip(sg, so):
+        assert abs(a.nu_inner - b.nu_inner) <= 1e-10 * abs(b.nu_inner)
+    gpu.close()
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+def test_tile_and_gather_forms_are_bitwise_equal(monkeypatch, precision):
+    """Same arithmetic on the same stored values: whole steps agree to the
+    bit in FP64 and in the mixed path's FP32 passes."""
+    case = config.small_case(40, 6, 26, steps=2)
+    outs = []
+    for form in ("gather", "tile"):
+        monkeypatch.setenv("NIM_FACE_SWEEP", form)
+        s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()), case.params(precision=precision))
+        s.initialize_nse()
+        s.add_temperature_noise(case.noise, case.seed)
+        recs = s.solve_nse(2)
+        outs.append(([(r.iters, r.iters_fp32, r.nu_inner) for r in recs], [s.download(f) for f in STATE]))
+        assert ("k_vel_face_tile" if form == "tile" else "k_vel_face") in s.profile_iterations(1)
+        s.close()
+    assert outs[0][0] == outs[1][0]
+    for a, b in zip(outs[0][1], outs[1][1]):
+        assert np.array_equal(a, b)
+
+
+def test_automatic_choice(monkeypatch):
+    """Without the override: the tile form on a mesh with enough patches,
+    the gather form on one that cannot fill the GPU."""
+    monkeypatch.delenv("NIM_FACE_SWEEP")
+    for dims, name in (((128, 64, 32), "k_vel_face_tile"), ((48, 48, 32), "k_vel_face")):
+        case = config.small_case(*dims)
+        s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()), case.params())
+        s.initialize_nse()
+        assert name in s.profile_iterations(1)
+        s.close()
+
+
+def test_kernel_choice_follows_n_theta():
+    for nt, name in ((16, "k_vel_face_tile"), (18, "k_vel_face")):
+        case = config.small_case(nt, 5, 6)
+        s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()), case.params())
+        s.initialize_nse()
+        prof = s.profile_iterations(1)
+        assert name in prof and all(k in ("k_vel_face", "k_vel_face_tile") or not k.startswith("k_vel_face")
+                                    for k in prof)
+        assert ("k_vel_face" in prof) != ("k_vel_face_tile" in prof)
+        s.close()
+
+
+def test_plain_face_kernel_matches_parallel_oracle():
+    """n_theta = 18 (not a multiple of 4) keeps the gather form."""
+    gpu, ref = pair((18, 6, 7))
+    gpu.calculate_velocity_nim_constants()
+    ref.begin_step()
+    gpu.iterate(3)
+    ref.iterate(3)
+    for f in (_abi.FACES_U, _abi.FACES_W, _abi.FACES_T):
+        a = gpu.download(f)
+        assert rel(a, ref.get(f, a.size)) <= 1e-12
+    gpu.close()
