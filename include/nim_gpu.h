@@ -196,7 +196,11 @@ typedef struct nim_ctx nim_ctx;
 void nim_params_reference(nim_params *p);
 
 /* Copy the mesh and parameters to the device.  Replaces the module-global
-   allocation of parameters.f90:222-292.  *out receives the context. */
+   allocation of parameters.f90:222-292.  *out receives the context.
+   The +xi face sweep of u, v, w runs in its TMA-staged form when n_theta is
+   a multiple of 4, at most 256, and the mesh gives at least one block per
+   SM, else in its gather form (the results are identical);
+   NIM_FACE_SWEEP=tile or =gather in the environment overrides the choice. */
 int nim_gpu_create(const nim_mesh_desc *mesh, const nim_params *params,
                    nim_ctx **out);
 
@@ -287,12 +291,12 @@ int nim_gpu_output_wait(nim_ctx *ctx, int32_t ticket);
    nim_gpu_stream: the cudaStream_t every call of the context queues work on,
    so a caller can record CUDA events on it.
    nim_gpu_launch_count: kernels launched by the context since creation.
-   nim_gpu_profile_iterations: n inner passes of the context's schedule and
-   formulation (with NIM_PRECISION_MIXED: FP32 passes over the narrowed
-   iterate, leaving the FP64 fields as they were), launched one kernel at a
-   time with a CUDA event after each;
-   ms[k] receives the mean time of launch group k (its name from
-   nim_gpu_profile_name), at most cap of them; returns their number. */
+   nim_gpu_profile_iterations: n + 1 inner passes of the context's schedule
+   and formulation (with NIM_PRECISION_MIXED: FP32 passes over the narrowed
+   iterate, leaving the FP64 fields as they were), queued back to back with
+   a CUDA event after each kernel; ms[k] receives the mean time of launch
+   group k over the last n passes (its name from nim_gpu_profile_name), at
+   most cap of them; returns their number. */
 void *nim_gpu_stream(nim_ctx *ctx);
 int64_t nim_gpu_launch_count(nim_ctx *ctx);
 int nim_gpu_profile_iterations(nim_ctx *ctx, int32_t n, double *ms, int32_t cap);

@@ -1458,43 +1458,40 @@ extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int
   const Phys keep = x->phys;
   x->phys.max_iters = 0;
   for (int q = 0; q < 5; ++q) x->phys.tol[q] = -1.0;
+  // n + 1 passes queued back to back with an event after every kernel, one
+  // wait at the end: no host gap inside the timed passes; the first pass
+  // (which starts on an idle stream) is not counted
   nim_ctx::Marks marks;
-  cudaEvent_t start = nullptr;
   std::vector<double> acc;
   std::vector<const char *> names;
   int st = NIM_OK;
-  if (cudaEventCreate(&start) != cudaSuccess) st = NIM_ERR_CUDA;
-  if (st == NIM_OK) {
+  {
     k_step_reset<<<1, 1, 0, s>>>(x->ctl);
     if (x->mixed) st = mirror_state(x, 0);  // FP32 passes over the narrowed iterate
     x->marks = &marks;
-    for (int it = 0; it < n && st == NIM_OK; ++it) {
-      marks.used = 0;
-      if (cudaEventRecord(start, s) != cudaSuccess) {
-        st = NIM_ERR_CUDA;
-        break;
-      }
+    std::vector<size_t> pass_end;
+    for (int it = 0; it <= n && st == NIM_OK; ++it) {
       st = launch_iteration(x, x->mixed, false);  // every pass runs: no stop test
-      if (st != NIM_OK) break;
-      if (cudaEventSynchronize(marks.ev[marks.used - 1]) != cudaSuccess) {
-        st = NIM_ERR_CUDA;
-        break;
-      }
-      if (it == 0) {
-        names.assign(marks.name.begin(), marks.name.begin() + marks.used);
-        acc.assign(marks.used, 0.0);
-      }
-      for (size_t k = 0; k < marks.used && k < acc.size(); ++k) {
-        float t = 0.f;
-        cudaEventElapsedTime(&t, k ? marks.ev[k - 1] : start, marks.ev[k]);
-        acc[k] += t;
-      }
+      pass_end.push_back(marks.used);
     }
     x->marks = nullptr;
+    if (st == NIM_OK && cudaEventSynchronize(marks.ev[marks.used - 1]) != cudaSuccess) st = NIM_ERR_CUDA;
+    if (st == NIM_OK) {
+      const size_t K = pass_end[0];
+      names.assign(marks.name.begin(), marks.name.begin() + K);
+      acc.assign(K, 0.0);
+      for (int it = 1; it <= n; ++it) {
+        const size_t b0 = pass_end[it - 1];
+        for (size_t k = 0; k < K; ++k) {
+          float t = 0.f;
+          cudaEventElapsedTime(&t, marks.ev[b0 + k - 1], marks.ev[b0 + k]);
+          acc[k] += t;
+        }
+      }
+    }
   }
   x->phys = keep;
   for (cudaEvent_t e : marks.ev) cudaEventDestroy(e);
-  if (start) cudaEventDestroy(start);
   if (st != NIM_OK) return st;
   const int nk = std::min((int)acc.size(), (int)cap);
   x->prof_names.assign(names.begin(), names.begin() + nk);
