@@ -200,7 +200,10 @@ void nim_params_reference(nim_params *p);
    The +xi face sweep of u, v, w runs in its TMA-staged form when n_theta is
    a multiple of 4, at most 256, and the mesh gives at least one block per
    SM, else in its gather form (the results are identical);
-   NIM_FACE_SWEEP=tile or =gather in the environment overrides the choice. */
+   NIM_FACE_SWEEP=tile or =gather in the environment overrides the choice.
+   NIM_CELL_SWEEP=tile selects the TMA-staged form of the u, v, w source and
+   cell sweep under the same n_theta conditions (formulation 2; identical
+   results, not faster at the benchmark sizes, so off by default). */
 int nim_gpu_create(const nim_mesh_desc *mesh, const nim_params *params,
                    nim_ctx **out);
 

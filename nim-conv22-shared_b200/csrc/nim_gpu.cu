@@ -108,6 +108,9 @@ struct nim_ctx {
   bool bulk = false;
   int tile_kc = 0;
   VelFaceMaps vmap64{}, vmap32{};
+  // k_vel_cell_tile (TMA-staged cell sweep of u, v, w, formulation 2)
+  bool cell_tile = false;
+  VelCellMaps cmap64{}, cmap32{};
   GeoT<float> g32{};
   FieldsT<float> F32{};
   cudaGraphExec_t graph32 = nullptr;
@@ -271,8 +274,15 @@ int launch_vel(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F
     k_vel1_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
     TRY(mark(x, "k_vel1_face"));
   } else {
-    k_vel_cell<false, 2><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
-    TRY(mark(x, "k_vel_cell"));
+    if (x->cell_tile) {
+      const dim3 gt((d.NT + 31) / 32, (d.NR + CT_R - 1) / CT_R, (d.NZ + x->tile_kc - 1) / x->tile_kc);
+      const VelCellMaps &M = std::is_same<R, double>::value ? x->cmap64 : x->cmap32;
+      k_vel_cell_tile<R><<<gt, dim3(CT_T, 3), CtLayout<R>::bytes, s>>>(d, g, F, x->phys, x->ctl, x->tile_kc, M);
+      TRY(mark(x, "k_vel_cell_tile"));
+    } else {
+      k_vel_cell<false, 2><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+      TRY(mark(x, "k_vel_cell"));
+    }
     if (x->bulk) {
       const dim3 gt((d.NT + 31) / 32, (d.NR + VT_R - 1) / VT_R, (d.NZ + x->tile_kc - 1) / x->tile_kc);
       const VelFaceMaps &M = std::is_same<R, double>::value ? x->vmap64 : x->vmap32;
@@ -812,11 +822,29 @@ static bool encode_vel_face_maps(const Dims &d, const GeoT<R> &g, const FieldsT<
   return ok;
 }
 
+template <class R>
+static bool encode_vel_cell_maps(const Dims &d, const FieldsT<R> &F, VelCellMaps &M) {
+  const uint64_t NT = d.NT, NR = d.NR, NZ = d.NZ, NF = d.NF;
+  bool ok = true;
+  for (int q = 0; q < 3; ++q) {
+    const uint64_t dr[4] = {NT, NR + 1, NZ, 2}, sr[3] = {NT, NT * (NR + 1), NF};
+    const uint64_t dt[4] = {NT, NR, NZ, 2}, dz[4] = {NT, NR, NZ + 1, 2}, st[3] = {NT, NT * NR, NF};
+    const uint32_t br[4] = {(uint32_t)CtLayout<R>::W, CT_R + 1, 1, 1};
+    const uint32_t bt[4] = {(uint32_t)CtLayout<R>::W, CT_R + 4, 1, 1};
+    ok = ok && encode_map(&M.rf[q], F.f[q], 4, dr, sr, br);
+    ok = ok && encode_map(&M.tf[q], F.f[q] + d.offT, 4, dt, st, bt);
+    ok = ok && encode_map(&M.zf[q], F.f[q] + d.offZ, 4, dz, st, bt);
+  }
+  return ok;
+}
+
 // The +xi face sweep of u, v, w runs as k_vel_face_tile when n_theta is a
 // multiple of 4 (16-byte box rows), at most 256, and the mesh gives at least
 // one block per SM; the z-chunk length aims at about six waves of blocks with
 // chunks of at least 8 planes.  NIM_FACE_SWEEP=tile or =gather in the
 // environment forces the choice (tile still needs the n_theta conditions).
+// NIM_CELL_SWEEP=tile selects k_vel_cell_tile under the same conditions
+// (formulation 2).
 static int choose_face_sweep(nim_ctx *x) {
   const Dims &d = x->d;
   int sms = 0;
@@ -830,6 +858,11 @@ static int choose_face_sweep(nim_ctx *x) {
   const char *env = std::getenv("NIM_FACE_SWEEP");
   const std::string force = env ? env : "";
   x->bulk = shape && !x->seq && (force == "tile" || (force != "gather" && blocks >= sms));
+  // the staged cell sweep only on request: its u, v, w faces are a sixth of
+  // k_vel_cell's bytes, and the two 110 KB blocks per SM it needs leave the
+  // direct loads of the rest with fewer warps than the gather form has
+  const char *envc = std::getenv("NIM_CELL_SWEEP");
+  x->cell_tile = shape && !x->seq && x->params.formulation == 2 && envc && std::string(envc) == "tile";
   return NIM_OK;
 }
 
@@ -937,6 +970,16 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
   TRY(dalloc(x, &x->scratch, std::max(54 * Nc, 3 * NF)));
   TRY(dalloc(x, &x->sums, 8));
   CK(cudaMallocHost(&x->ctl_host, sizeof(Ctrl)));
+  if (x->cell_tile) {
+    x->cell_tile = encode_vel_cell_maps(d, x->F, x->cmap64) &&
+                   (!x->mixed || encode_vel_cell_maps(d, x->F32, x->cmap32));
+    if (x->cell_tile) {
+      CK(cudaFuncSetAttribute(k_vel_cell_tile<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)CtLayout<double>::bytes));
+      CK(cudaFuncSetAttribute(k_vel_cell_tile<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)CtLayout<float>::bytes));
+    }
+  }
   if (x->bulk && !x->seq) {
     x->bulk = encode_vel_face_maps(d, x->g, x->F, x->vmap64) &&
               (!x->mixed || encode_vel_face_maps(d, x->g32, x->F32, x->vmap32));

@@ -1444,6 +1444,241 @@ __global__ void __launch_bounds__(3 * VT_T, VT_MINB)
   block_max<3, 3 * VT_T>(red, e, ctl->err[par]);
 }
 
+// ---- K1, tiled form (parallel schedule, formulation 2): k_vel_cell with the
+// face values of u, v, w its stencils read staged in shared memory by TMA
+// boxes.  One block per patch of 32 theta x CT_R r cells marches up a chunk
+// of z-planes; per plane p, for each component, three boxes of W columns
+// from i0-OFF (OFF = 16 bytes of elements, so the box's x coordinate stays
+// 16-byte aligned; the theta halo on both sides): r faces, rows j0 .. j0+CT_R;
+// theta faces and z faces of level p, rows j0-2 .. j0+CT_R+1 (the two-cell
+// one-sided wall stencils in r).  A ring of CT_S bundles holds planes k-2 ..
+// k+2 (the one-sided stencils in z) and one in flight.  Pressure faces,
+// geometry, M_F4 and the cell values stay direct loads (each read once).
+// The theta-seam columns (theta NT-1 left of the first patch, theta 0 right
+// of the last) are fetched with plain loads and written in after the box
+// lands.  The arithmetic is k_vel_cell's, term for term.
+constexpr int CT_R = 4;          // r rows of cells per patch
+constexpr int CT_T = 32 * CT_R;  // cells per patch = blockDim.x (blockDim.y = 3 components)
+constexpr int CT_S = 6;          // bundle ring depth
+constexpr int CT_MINB = 2;       // resident blocks per SM the launch bounds ask for
+
+struct VelCellMaps {
+  CUtensorMap rf[3], tf[3], zf[3];
+};
+
+template <class R>
+struct CtLayout {
+  static constexpr int OFF = 16 / (int)sizeof(R);                  // columns left of i0 (2 or 4)
+  static constexpr int W = (32 + OFF + 2 + 3) / 4 * 4;             // 36 (double) or 40 (float) columns
+  static constexpr int up(int bytes) { return (bytes + 127) / 128 * 128 / (int)sizeof(R); }
+  static constexpr int RF = up((CT_R + 1) * W * (int)sizeof(R));  // r-face box region
+  static constexpr int TZ = up((CT_R + 4) * W * (int)sizeof(R));  // theta / z box region
+  static constexpr int Q = RF + 2 * TZ;                             // one component
+  static constexpr int BUNDLE = 3 * Q;
+  static constexpr int BARS = CT_S * BUNDLE;
+  static constexpr size_t bytes = (size_t)BARS * sizeof(R) + CT_S * sizeof(unsigned long long) + 128;
+  static constexpr unsigned full_tx = 3u * ((CT_R + 1) + 2 * (CT_R + 4)) * W * sizeof(R);
+  static constexpr unsigned top_tx = 3u * (CT_R + 4) * W * sizeof(R);  // z level NZ only
+  static constexpr int SEAM_L = 3 * ((CT_R + 1) + (CT_R + 4));          // r and z rows, column OFF-1
+  static constexpr int SEAM_R = 3 * ((CT_R + 1) + 2 * (CT_R + 4));      // r, theta, z rows, column ncell+OFF
+};
+
+template <class R>
+__device__ void ct_issue(const VelCellMaps &M, R *slot, unsigned long long *bar, int i0, int j0, int p, int par,
+                         int NZ) {
+  using L = CtLayout<R>;
+  const bool cells = p < NZ;
+  mbar_expect_tx(bar, cells ? L::full_tx : L::top_tx);
+  for (int q = 0; q < 3; ++q) {
+    R *b = slot + q * L::Q;
+    tma_load_4d(b + L::RF + L::TZ, &M.zf[q], i0 - L::OFF, j0 - 2, p, par, bar);
+    if (!cells) continue;
+    tma_load_4d(b, &M.rf[q], i0 - L::OFF, j0, p, par, bar);
+    tma_load_4d(b + L::RF, &M.tf[q], i0 - L::OFF, j0 - 2, p, par, bar);
+  }
+}
+
+// seam value u of bundle p: global source and position in the bundle;
+// false if u names nothing (no seam on that side, a row outside the mesh,
+// or an array the bundle does not hold)
+template <class R>
+__device__ __forceinline__ bool ct_seam(const Dims &d, const FieldsT<R> &F, int par, int i0, int j0, int ncell,
+                                        bool left, bool right, int p, int u, const R *&src, int &dst) {
+  using L = CtLayout<R>;
+  int q, r, kind, col, ti;  // kind 0 r faces, 1 theta faces, 2 z faces
+  if (u < L::SEAM_L) {
+    if (!left) return false;
+    q = u / (L::SEAM_L / 3);
+    r = u - q * (L::SEAM_L / 3);
+    kind = (r < CT_R + 1) ? 0 : 2;
+    if (kind == 2) r -= CT_R + 1;
+    col = L::OFF - 1;
+    ti = d.NT - 1;
+  } else {
+    if (!right) return false;
+    u -= L::SEAM_L;
+    q = u / (L::SEAM_R / 3);
+    r = u - q * (L::SEAM_R / 3);
+    if (r < CT_R + 1) {
+      kind = 0;
+    } else if (r < CT_R + 1 + CT_R + 4) {
+      kind = 1;
+      r -= CT_R + 1;
+    } else {
+      kind = 2;
+      r -= CT_R + 1 + CT_R + 4;
+    }
+    col = ncell + L::OFF;
+    ti = 0;
+  }
+  const int j = (kind == 0) ? j0 + r : j0 - 2 + r;
+  if (kind == 0 ? (j > d.NR) : (j < 0 || j > d.NR - 1)) return false;
+  if (p >= d.NZ && kind != 2) return false;
+  const size_t NT = d.NT, NR = d.NR;
+  const R *fq = F.f[q] + (size_t)par * d.NF;
+  switch (kind) {
+    case 0: src = fq + NT * (j + (NR + 1) * p) + ti; break;
+    case 1: src = fq + d.offT + NT * (j + NR * p) + ti; break;
+    default: src = fq + d.offZ + NT * (j + NR * p) + ti; break;
+  }
+  dst = q * L::Q + (kind == 0 ? 0 : kind == 1 ? L::RF : L::RF + L::TZ) + r * L::W + col;
+  return true;
+}
+
+template <class R>
+__global__ void __launch_bounds__(3 * CT_T, CT_MINB)
+    k_vel_cell_tile(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl, int kc, const __grid_constant__ VelCellMaps M) {
+  using L = CtLayout<R>;
+  if (ctl->done) return;
+  extern __shared__ __align__(128) unsigned char ct_raw[];
+  R *ring = reinterpret_cast<R *>(ct_raw + ((128u - (smem_u32(ct_raw) & 127u)) & 127u));
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(ring + L::BARS);
+  __shared__ BlockRed red;
+  const int tid = threadIdx.x + CT_T * threadIdx.y;
+  const int q = threadIdx.y;
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * CT_R;
+  const int ncell = min(32, d.NT - i0);
+  const bool left = (i0 == 0), right = (d.NT - i0 <= 32);
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int kb = blockIdx.z * kc, ke = min(kb + kc, d.NZ);
+  const int P0 = max(kb - 2, 0), P1 = min(ke + 1, d.NZ);  // bundles P0 .. P1
+  const int nb = P1 - P0 + 1;
+  if (tid == 0)
+    for (int s = 0; s < CT_S; ++s) mbar_init(&bar[s], 1);
+  red_init<3>(red);  // barrier: the mbarriers exist before any copy
+  int issued = 0;    // bundles issued so far (the same count in every thread)
+  for (; issued < nb && issued < CT_S; ++issued)
+    if (tid == 0) ct_issue(M, ring + issued * L::BUNDLE, &bar[issued], i0, j0, P0 + issued, par, d.NZ);
+  const int ii = threadIdx.x & 31, jj = threadIdx.x >> 5;
+  const bool act = ii < ncell && j0 + jj < d.NR;
+  const size_t Nc = d.Nc, NF = d.NF;
+  double e[3] = {0., 0., 0.};
+  bool ok = true;
+  int waited = 0;  // bundles 0 .. waited-1 have landed
+  for (int k = kb; k < ke; ++k) {
+    const int need = min(k + 2, d.NZ) - P0;  // highest bundle plane k reads
+    // seam values of the bundles that become readable now (at most 5)
+    R seamv[5];
+    int seamd[5];
+    bool have[5] = {false, false, false, false, false};
+    if ((left || right) && tid < L::SEAM_L + L::SEAM_R) {
+      for (int b = waited; b <= need; ++b) {
+        const R *src;
+        int dst;
+        if (ct_seam(d, F, par, i0, j0, ncell, left, right, P0 + b, tid, src, dst)) {
+          have[b - waited] = true;
+          seamv[b - waited] = *src;
+          seamd[b - waited] = (b % CT_S) * L::BUNDLE + dst;
+        }
+      }
+    }
+    bool mine = true;
+    for (int b = waited; b <= need; ++b) mine = mine && mbar_wait(&bar[b % CT_S], (b / CT_S) & 1, ctl);
+    if (mine && (left || right)) {
+      for (int n = 0; n < 5; ++n)
+        if (have[n]) ring[seamd[n]] = seamv[n];
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // before later boxes into these slots
+    }
+    waited = need + 1;
+    if (!__syncthreads_and(mine)) {  // the same decision in every thread
+      ok = false;
+      break;
+    }
+    if (act) {
+      const Cell x = Cell::at(d, i0 + ii, j0 + jj, k);
+      const int c = x.c;
+      int f[7];
+      cell_faces(d, x, f);
+      const R *fp = F.f[3] + par * NF;
+      double pf[7];
+      for (int m = 1; m <= 6; ++m) pf[m] = fp[f[m]];
+      const double invV = 1. / g.vol[c];
+      const double base = (q == 2) ? -(P.g_beta * 0.5 * (F.c[3][c] + F.co[3][c])) : 0.;
+      const double RB = base + P.inv_rho * green_gauss(g, NF, invV, pf, f, q);
+      // face pos of the cell (di, dj, dk) away, component q, from the ring
+      auto fv = [&](int pos, int di, int dj, int dk) -> double {
+        const int pb = k + dk + (pos == 6 ? 1 : 0) - P0;
+        const R *b = ring + (pb % CT_S) * L::BUNDLE + q * L::Q;
+        const int col = ii + di + L::OFF + (pos == 4 ? 1 : 0);
+        switch (pos) {
+          case 1: return b[(jj + dj) * L::W + col];
+          case 2: return b[(jj + dj + 1) * L::W + col];
+          case 3:
+          case 4: return b[L::RF + (jj + dj + 2) * L::W + col];
+          default: return b[L::RF + L::TZ + (jj + dj + 2) * L::W + col];
+        }
+      };
+      // tangential(): centred, or one-sided at the walls, along e
+      auto tng = [&](int pos, int e) -> double {
+        auto at = [&](int s) { return fv(pos, e == 2 ? s : 0, e == 1 ? s : 0, e == 3 ? s : 0); };
+        const bool lo = !x.has_nb(d, 2 * e - 1), hi = !x.has_nb(d, 2 * e);
+        if (lo) return (-(3 * at(0)) + 4 * at(1) - at(2)) / 4.;
+        if (hi) return (3 * at(0) - 4 * at(-1) + at(-2)) / 4.;
+        return (at(1) - at(-1)) / 4.;
+      };
+      const double pxy = 0.5 * (tng(2, 2) - tng(1, 2));
+      const double pzy = 0.5 * (tng(6, 2) - tng(5, 2));
+      const double pyx = 0.5 * (tng(4, 1) - tng(3, 1));
+      const double pzx = 0.5 * (tng(6, 1) - tng(5, 1));
+      const double pxz = 0.5 * (tng(2, 3) - tng(1, 3));
+      const double pyz = 0.5 * (tng(4, 3) - tng(3, 3));
+      R fr[7];  // the stored values: the differences below are taken in R, as in diffusion_source
+      for (int m = 1; m <= 6; ++m) fr[m] = (R)fv(m, 0, 0, 0);
+      const double px = (fr[2] - fr[1]) / 2.;
+      const double py = (fr[4] - fr[3]) / 2.;
+      const double pz = (fr[6] - fr[5]) / 2.;
+      const R *G = g.G, *gij = g.gij;
+      const double RD =
+          P.inv_Re * (G[c] * px + G[Nc + c] * py + G[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy -
+                      gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz - gij[2 * Nc + c] * pzx - gij[7 * Nc + c] * pyz -
+                      gij[5 * Nc + c] * pzy);
+      const double B = (0. + RD + RB);
+      const double cv = F.c[q][c], cold = F.co[q][c], w = P.w[q];
+      double F4[8];
+      for (int m = 0; m < 8; ++m) F4[m] = F.MF4[(size_t)m * Nc + c];
+      const double nw = stored<R>((1 - w) * cv + (w / F4[0]) * (+F4[1] * cold + F4[2] * fr[1] + F4[3] * fr[2] +
+                                                                  F4[4] * fr[3] + F4[5] * fr[4] + F4[6] * fr[5] +
+                                                                  F4[7] * fr[6] + B));
+      F.c[q][c] = nw;
+      e[q] = nmax(e[q], errv(nw, cv, first));
+    }
+    __syncthreads();  // every thread is done with the bundles plane k+1 no longer reads
+    const int low = max(k + 1 - 2, 0) - P0;  // lowest bundle plane k+1 reads
+    for (; issued < nb && issued - CT_S < low; ++issued)
+      if (tid == 0)
+        ct_issue(M, ring + (issued % CT_S) * L::BUNDLE, &bar[issued % CT_S], i0, j0, P0 + issued, par, d.NZ);
+  }
+  if (!ok) {
+    for (int s = 0; s < CT_S; ++s) {  // bounded: let the copies in flight land
+      mbar_wait(&bar[s], 0, ctl);
+      mbar_wait(&bar[s], 1, ctl);
+    }
+    return;
+  }
+  block_max<3, 3 * CT_T>(red, e, ctl->err[par]);
+}
+
 // ---- K3: pressure sources (calculate_R_b_p nse.f90:2362-2407,
 // calculate_R_D_p2 1863-1997).  Block (CB, 3): thread y forms the gradient of
 // velocity component y and two of the six cross derivatives of p (y = 1 also

@@ -1,12 +1,16 @@
-"""k_vel_face_tile: the +xi face sweep of u, v, w staged in shared memory by
-TMA boxes, marching up z in chunks.  It replaces k_vel_face when n_theta is a
-multiple of 4 (at most 256) and the mesh fills the GPU with blocks;
-NIM_FACE_SWEEP=tile forces it on the small meshes here.  Both restate
-nse.f90:878-1005 with the same arithmetic, so the passes match the CPU
-oracle's parallel schedule to round-off.  The meshes below reach every edge
-of the tiling: several z-chunks and the top level, theta tiles that read
-real halo columns and a seam tile of fewer than 32 cells, and patches cut
-short in r."""
+"""The TMA-staged sweeps of u, v, w: k_vel_face_tile (+xi face updates,
+nse.f90:878-1005) and k_vel_cell_tile (sources and cell update,
+nse.f90:199-211, 839-872), which march up z in chunks with their face
+operands staged in shared memory by TMA boxes.  They replace k_vel_face and
+k_vel_cell when n_theta is a multiple of 4 (at most 256): the face sweep by
+itself when the mesh fills the GPU with blocks, the cell sweep on request
+(NIM_CELL_SWEEP=tile); NIM_FACE_SWEEP=tile forces the face sweep on the
+small meshes here.  Each restates its gather twin with the same
+arithmetic, so the passes match the CPU oracle's parallel schedule to
+round-off and the two forms agree to the bit.  The meshes below reach every
+edge of the tiling: several z-chunks, both z walls and the top level, theta
+tiles that read real halo columns, seam tiles on both sides (one of fewer
+than 32 cells), and patches cut short in r."""
 import numpy as np
 import pytest
 
@@ -20,6 +24,7 @@ pytestmark = pytest.mark.gpu
 @pytest.fixture(autouse=True)
 def force_tile(monkeypatch):
     monkeypatch.setenv("NIM_FACE_SWEEP", "tile")
+    monkeypatch.setenv("NIM_CELL_SWEEP", "tile")
 
 
 STATE = [
@@ -48,7 +53,8 @@ def pair(dims, **over):
 @pytest.mark.parametrize("dims", [(40, 6, 30), (12, 5, 13), (36, 9, 12), (64, 4, 25)])
 def test_tiled_passes_match_parallel_oracle(dims):
     gpu, ref = pair(dims)
-    assert "k_vel_face_tile" in gpu.profile_iterations(1)
+    prof = gpu.profile_iterations(1)
+    assert "k_vel_face_tile" in prof and "k_vel_cell_tile" in prof
     gpu.close()
     gpu, ref = pair(dims)
     gpu.calculate_velocity_nim_constants()
@@ -84,12 +90,15 @@ def test_tile_and_gather_forms_are_bitwise_equal(monkeypatch, precision):
     outs = []
     for form in ("gather", "tile"):
         monkeypatch.setenv("NIM_FACE_SWEEP", form)
+        monkeypatch.setenv("NIM_CELL_SWEEP", form)
         s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()), case.params(precision=precision))
         s.initialize_nse()
         s.add_temperature_noise(case.noise, case.seed)
         recs = s.solve_nse(2)
         outs.append(([(r.iters, r.iters_fp32, r.nu_inner) for r in recs], [s.download(f) for f in STATE]))
-        assert ("k_vel_face_tile" if form == "tile" else "k_vel_face") in s.profile_iterations(1)
+        prof = s.profile_iterations(1)
+        suffix = "_tile" if form == "tile" else ""
+        assert "k_vel_face" + suffix in prof and "k_vel_cell" + suffix in prof
         s.close()
     assert outs[0][0] == outs[1][0]
     for a, b in zip(outs[0][1], outs[1][1]):
@@ -100,24 +109,36 @@ def test_automatic_choice(monkeypatch):
     """Without the override: the tile form on a mesh with enough patches,
     the gather form on one that cannot fill the GPU."""
     monkeypatch.delenv("NIM_FACE_SWEEP")
-    for dims, name in (((128, 64, 32), "k_vel_face_tile"), ((48, 48, 32), "k_vel_face")):
+    monkeypatch.delenv("NIM_CELL_SWEEP")
+    for dims, suffix in (((128, 64, 32), "_tile"), ((48, 48, 32), "")):
         case = config.small_case(*dims)
         s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()), case.params())
         s.initialize_nse()
-        assert name in s.profile_iterations(1)
+        prof = s.profile_iterations(1)
+        assert "k_vel_face" + suffix in prof and "k_vel_cell" in prof  # the cell sweep only on request
         s.close()
 
 
 def test_kernel_choice_follows_n_theta():
-    for nt, name in ((16, "k_vel_face_tile"), (18, "k_vel_face")):
+    for nt, suffix in ((16, "_tile"), (18, "")):
         case = config.small_case(nt, 5, 6)
         s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()), case.params())
         s.initialize_nse()
         prof = s.profile_iterations(1)
-        assert name in prof and all(k in ("k_vel_face", "k_vel_face_tile") or not k.startswith("k_vel_face")
-                                    for k in prof)
-        assert ("k_vel_face" in prof) != ("k_vel_face_tile" in prof)
+        for sweep in ("k_vel_face", "k_vel_cell"):
+            assert sweep + suffix in prof
+            assert (sweep in prof) != (sweep + "_tile" in prof)
         s.close()
+
+
+def test_formulation_one_keeps_the_gather_cell_sweep():
+    case = config.small_case(16, 5, 6)
+    s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()),
+                         case.params(formulation=1, schedule=_abi.SCHEDULE_PARALLEL))
+    s.initialize_nse()
+    prof = s.profile_iterations(1)
+    assert "k_vel_cell" in prof and "k_vel_cell_tile" not in prof
+    s.close()
 
 
 def test_plain_face_kernel_matches_parallel_oracle():
