@@ -1214,7 +1214,8 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, GeoT<R> g, FieldsT<
 constexpr int VT_R = 4;         // r rows of cells per patch
 constexpr int VT_T = 32 * VT_R;  // cells per patch = blockDim.x (blockDim.y = 3 directions)
 constexpr int VT_S = 3;          // plane ring depth (FP64: 109 KB with the coefficient ring)
-constexpr int VT_MINB = 2;       // resident blocks per SM the launch bounds ask for
+constexpr int VT_MINB = 2;       // resident blocks per SM the launch bounds ask for (FP64;
+                                 // float: 3, its 57 KB ring allows it)
 
 // tensor maps of one storage type, encoded by the host: per component the
 // r / theta / z parts of the face array as {NT, rows, planes, half}, the
@@ -1321,7 +1322,7 @@ __device__ __forceinline__ bool vt_seam(const Dims &d, const FieldsT<R> &F, int 
 }
 
 template <class R>
-__global__ void __launch_bounds__(3 * VT_T, VT_MINB)
+__global__ void __launch_bounds__(3 * VT_T, sizeof(R) == 8 ? VT_MINB : 3)
     k_vel_face_tile(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl, int kc, const __grid_constant__ VelFaceMaps M) {
   using L = VtLayout<R>;
   if (ctl->done) return;
