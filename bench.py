@@ -70,11 +70,14 @@ KERNEL_BYTES_PER_CELL = {
     "k_seq_T": 8 * 39,      # T,T_old (2) faces T (3) MT_F4 (8) R_D_T (1) MT_F (15) dg (6); write T, faces (4)
 }
 # DRAM bytes per cell and launch that ncu measured (dram__bytes_read.sum +
-# dram__bytes_write.sum, one --set full capture of the 96x96x64 case);
-# traffic grows with the cells, so roofline.traffic scales these to the run's mesh
+# dram__bytes_write.sum, one --set full capture each); traffic grows with the
+# cells, so roofline.traffic scales these to the run's mesh
 NCU_DRAM_BYTES_PER_CELL = {
     "k_vel_cell": 424.3, "k_vel_face": 343.1, "k_p_src": 320.3, "k_T_coef": 273.3, "k_T_cell": 337.6,
+    "k_vel_face_tile": 361.4,
 }
+NCU_CAPTURE = {k: "96x96x64" for k in NCU_DRAM_BYTES_PER_CELL}
+NCU_CAPTURE["k_vel_face_tile"] = "128x128x96"
 # algorithmic bytes per cell-iteration and per cell-step of the whole pass
 # (FP64, every array read and written once, implicit connectivity)
 ALGO_BYTES_PER_CELL_ITER = 1880
@@ -498,7 +501,8 @@ def main():
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": (NCU_DRAM_BYTES_PER_CELL[dom] * case.ncells if dom in NCU_DRAM_BYTES_PER_CELL
                                  else None),
-                     "traffic_source": "ncu dram bytes on the 96x96x64 case, scaled by cells",
+                     "traffic_source": (f"ncu dram bytes on the {NCU_CAPTURE[dom]} case, scaled by cells"
+                                        if dom in NCU_CAPTURE else None),
                      "bytes_per_launch": KERNEL_BYTES_PER_CELL[dom] * width / 8 * case.ncells,
                      "kernel_ms": dom_ms,
                      "shares": {k: round(v / tot, 4) for k, v in shares.items()},
