@@ -73,11 +73,11 @@ KERNEL_BYTES_PER_CELL = {
 # dram__bytes_write.sum, one --set full capture each); traffic grows with the
 # cells, so roofline.traffic scales these to the run's mesh
 NCU_DRAM_BYTES_PER_CELL = {
-    "k_vel_cell": 424.3, "k_vel_face": 343.1, "k_p_src": 320.3, "k_T_coef": 273.3, "k_T_cell": 337.6,
-    "k_vel_face_tile": 361.4,
+    "k_vel_cell": 425.2, "k_p_src": 324.4, "k_p_face": 420.2, "k_T_coef": 317.0, "k_T_cell": 389.6,
+    "k_T_face": 227.3, "k_vel_face_tile": 361.4, "k_vel_face": 343.1,
 }
-NCU_CAPTURE = {k: "96x96x64" for k in NCU_DRAM_BYTES_PER_CELL}
-NCU_CAPTURE["k_vel_face_tile"] = "128x128x96"
+NCU_CAPTURE = {k: "128x128x96" for k in NCU_DRAM_BYTES_PER_CELL}
+NCU_CAPTURE["k_vel_face"] = "96x96x64"
 # algorithmic bytes per cell-iteration and per cell-step of the whole pass
 # (FP64, every array read and written once, implicit connectivity)
 ALGO_BYTES_PER_CELL_ITER = 1880
