@@ -59,6 +59,7 @@ KERNEL_BYTES_PER_CELL = {
     "k_vel_face": 8 * 45,   # faces u,v,w (9) cells+old (6) M_F1..3 (15) dg (6); write faces (9)
     "k_vel_face_tile": 8 * 45,  # the same sweep staged by TMA boxes (same algorithmic bytes)
     "k_vel_cell_tile": 8 * 53,  # k_vel_cell with its u, v, w faces staged by TMA boxes
+    "k_vel_cell2": 8 * 53,  # k_vel_cell on cell pairs with paired loads (same algorithmic bytes)
     "k_p_src": 8 * 39,      # faces u,v,w,T,p (15) area,normal,vol (13) G,g^ij (9); write dila,Rp (2)
     "k_p_face": 8 * 52,     # faces p (3) Rp (1) AA used (39) dg (6); write faces p (3)
     "k_T_coef": 8 * 42,     # cells+old u,v,w (6) xi (9) g^ij diagonal (3) gfd (6); write MT_A (18)

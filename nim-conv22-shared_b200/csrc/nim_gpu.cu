@@ -110,6 +110,7 @@ struct nim_ctx {
   VelFaceMaps vmap64{}, vmap32{};
   // k_vel_cell_tile (TMA-staged cell sweep of u, v, w, formulation 2)
   bool cell_tile = false;
+  bool cell_pair = false;  // k_vel_cell2: two theta-adjacent cells per thread
   VelCellMaps cmap64{}, cmap32{};
   GeoT<float> g32{};
   FieldsT<float> F32{};
@@ -279,6 +280,10 @@ int launch_vel(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F
       const VelCellMaps &M = std::is_same<R, double>::value ? x->cmap64 : x->cmap32;
       k_vel_cell_tile<R><<<gt, dim3(CT_T, 3), CtLayout<R>::bytes, s>>>(d, g, F, x->phys, x->ctl, x->tile_kc, M);
       TRY(mark(x, "k_vel_cell_tile"));
+    } else if (x->cell_pair) {
+      const dim3 gp((d.NT + 63) / 64, (d.NR + 3) / 4, d.NZ);
+      k_vel_cell2<<<gp, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+      TRY(mark(x, "k_vel_cell2"));
     } else {
       k_vel_cell<false, 2><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
       TRY(mark(x, "k_vel_cell"));
@@ -843,8 +848,10 @@ static bool encode_vel_cell_maps(const Dims &d, const FieldsT<R> &F, VelCellMaps
 // one block per SM; the z-chunk length aims at about six waves of blocks with
 // chunks of at least 8 planes.  NIM_FACE_SWEEP=tile or =gather in the
 // environment forces the choice (tile still needs the n_theta conditions).
-// NIM_CELL_SWEEP=tile selects k_vel_cell_tile under the same conditions
-// (formulation 2).
+// The source and cell sweep of u, v, w (formulation 2) runs as k_vel_cell2
+// (two theta-adjacent cells per thread, paired loads) when n_theta is even;
+// NIM_CELL_SWEEP=gather forces k_vel_cell, =tile k_vel_cell_tile (under the
+// tile's n_theta conditions).
 static int choose_face_sweep(nim_ctx *x) {
   const Dims &d = x->d;
   int sms = 0;
@@ -862,7 +869,10 @@ static int choose_face_sweep(nim_ctx *x) {
   // k_vel_cell's bytes, and the two 110 KB blocks per SM it needs leave the
   // direct loads of the rest with fewer warps than the gather form has
   const char *envc = std::getenv("NIM_CELL_SWEEP");
-  x->cell_tile = shape && !x->seq && x->params.formulation == 2 && envc && std::string(envc) == "tile";
+  const std::string cell = envc ? envc : "";
+  x->cell_tile = shape && !x->seq && x->params.formulation == 2 && cell == "tile";
+  // the paired-load form whenever n_theta is even, unless another is asked for
+  x->cell_pair = !x->cell_tile && d.NT % 2 == 0 && !x->seq && x->params.formulation == 2 && cell != "gather";
   return NIM_OK;
 }
 

@@ -127,6 +127,7 @@ struct Ctrl {
 constexpr int kLowpStall = 8;
 
 constexpr int BLK = 256;
+constexpr int VC2_MINB = 3;  // resident blocks per SM asked of k_vel_cell2 (56 registers)
 // kernels that spread one cell over three threads (component or direction)
 constexpr int CB = 128;            // cells per block
 constexpr int CB3 = 3 * CB;        // threads per block
@@ -1159,6 +1160,230 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, GeoT<R> g, FieldsT<
     }
   }
   if (!SRC_ONLY) block_max<3, CB3>(red, e, ctl->err[par]);
+}
+
+// ---- K1, vectorised form (parallel schedule, formulation 2): k_vel_cell
+// with each thread on two theta-adjacent cells (i even, i+1) of one
+// component, so that nearly every load brings both cells' values at once
+// (16 bytes in FP64): the cell arrays, the r and z faces, and the theta faces
+// at i and i+1 (the +theta face of cell i is the -theta face of cell i+1).
+// Only the faces at i-1 and i+2 that the theta stencils reach, and the
+// +theta face of cell i+1, are single loads: ~70 load instructions for two
+// cells instead of ~120.  The two cells advance together term by term, in
+// each sum's source order, so the arithmetic is k_vel_cell's to the bit.
+// Needs n_theta even; block (CB, 3) over patches of 64 x CB/32 cells.
+template <class R>
+struct Pair2;
+template <>
+struct Pair2<double> {
+  using T = double2;
+};
+template <>
+struct Pair2<float> {
+  using T = float2;
+};
+// p[i], p[i+1] for an even element index i (a 2 x sizeof(R)-aligned pair)
+template <class R>
+__device__ __forceinline__ void ld2(const R *__restrict__ p, size_t i, R &a, R &b) {
+  const typename Pair2<R>::T v = *reinterpret_cast<const typename Pair2<R>::T *>(p + i);
+  a = v.x;
+  b = v.y;
+}
+// tangential() from the values: v0 at the cell, vp1 / vp2 one / two cells
+// along +e, vm1 / vm2 along -e (only those the branch reads are used)
+__device__ __forceinline__ double tang_vals(bool lo, bool hi, double v0, double vp1, double vp2, double vm1,
+                                            double vm2) {
+  if (lo) return (-(3 * v0) + 4 * vp1 - vp2) / 4.;
+  if (hi) return (3 * v0 - 4 * vm1 + vm2) / 4.;
+  return (vp1 - vm1) / 4.;
+}
+
+template <class R>
+__global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<3>(red);
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int q = threadIdx.y;
+  const int i = blockIdx.x * 64 + 2 * (threadIdx.x & 31);
+  const int j = blockIdx.y * (CB / 32) + (threadIdx.x >> 5);
+  const int k = blockIdx.z;
+  double e[3] = {0., 0., 0.};
+  if (i < d.NT && j < d.NR) {
+    const size_t Nc = d.Nc, NF = d.NF, NT = d.NT, NR = d.NR, pl = d.plane;
+    const size_t c = (size_t)i + NT * (j + NR * k);  // cell i; the pair's second cell is c + 1
+    const int im1 = (i == 0) ? d.NT - 1 : i - 1, ip2 = (i + 2 >= d.NT) ? i + 2 - d.NT : i + 2;
+    // face m of cell i at fi[m]; of cell i+1 at fi[m] + 1, except face 4: f4b
+    const size_t f1 = c + NT * k;
+    const size_t fi[7] = {0, f1, f1 + NT, d.offT + c, d.offT + c + 1, d.offZ + c, d.offZ + c + pl};
+    const size_t f4b = d.offT + c - i + ip2;
+    // face m of both cells from array a (pairs; faces 3 and 4 share one pair)
+    auto face2 = [&](const R *a, int m, R &v0, R &v1) {
+      if (m == 4) {
+        v0 = a[fi[3] + 1];
+        v1 = a[f4b];
+      } else {
+        ld2(a, fi[m], v0, v1);
+      }
+    };
+    // RB = base + 1/rho * green_gauss (component q): the sum term by term in
+    // source order (faces 2, 1, 4, 3, 6, 5) for both cells
+    const R *pp = F.f[3] + par * NF, *nq = g.normal + q * NF;
+    double gs0 = 0., gs1 = 0.;
+    {
+      const int order[6] = {2, 1, 4, 3, 6, 5};
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        const int m = order[t];
+        R p0, p1, a0, a1, n0, n1;
+        face2(pp, m, p0, p1);
+        face2(g.area, m, a0, a1);
+        face2(nq, m, n0, n1);
+        const double t0 = (double)p0 * a0 * (n0), t1 = (double)p1 * a1 * (n1);
+        if (t == 0) {
+          gs0 = t0;
+          gs1 = t1;
+        } else if (t & 1) {
+          gs0 = gs0 - t0;
+          gs1 = gs1 - t1;
+        } else {
+          gs0 = gs0 + t0;
+          gs1 = gs1 + t1;
+        }
+      }
+    }
+    double RB0, RB1;
+    {
+      R v0, v1;
+      ld2(g.vol, c, v0, v1);
+      double base0 = 0., base1 = 0.;
+      if (q == 2) {
+        R t0, t1, o0, o1;
+        ld2(F.c[3], c, t0, t1);
+        ld2(F.co[3], c, o0, o1);
+        base0 = -(P.g_beta * 0.5 * (t0 + o0));
+        base1 = -(P.g_beta * 0.5 * (t1 + o1));
+      }
+      const double invV0 = 1. / v0, invV1 = 1. / v1;
+      RB0 = base0 + P.inv_rho * (invV0 * gs0);
+      RB1 = base1 + P.inv_rho * (invV1 * gs1);
+    }
+    // own faces of component q (stored values)
+    const R *fr = F.f[q] + par * NF;
+    R o0[7], o1[7];
+    for (int m = 1; m <= 6; ++m) face2(fr, m, o0[m], o1[m]);
+    // rows / planes a and b: the -e,+e neighbours (centred), +1,+2 (lo) or -1,-2 (hi)
+    auto along = [&](bool lo, bool hi, double v0, double va, double vb) {
+      return lo ? tang_vals(true, false, v0, va, vb, 0., 0.)
+                : hi ? tang_vals(false, true, v0, 0., 0., va, vb) : tang_vals(false, false, v0, vb, 0., va, 0.);
+    };
+    // theta: centred; r faces (rows j, j+1) and z faces (levels k, k+1) at theta i-1, i+2
+    double pxy0, pxy1, pzy0, pzy1;
+    {
+      const size_t rrow = NT * (j + (NR + 1) * k), zlev = d.offZ + NT * (j + NR * k);
+      const double r_m1 = fr[rrow + im1], r_p2 = fr[rrow + ip2];
+      const double r1_m1 = fr[rrow + NT + im1], r1_p2 = fr[rrow + NT + ip2];
+      pxy0 = 0.5 * (((double)o1[2] - r1_m1) / 4. - ((double)o1[1] - r_m1) / 4.);
+      pxy1 = 0.5 * ((r1_p2 - (double)o0[2]) / 4. - (r_p2 - (double)o0[1]) / 4.);
+      const double z_m1 = fr[zlev + im1], z_p2 = fr[zlev + ip2];
+      const double z1_m1 = fr[zlev + pl + im1], z1_p2 = fr[zlev + pl + ip2];
+      pzy0 = 0.5 * (((double)o1[6] - z1_m1) / 4. - ((double)o1[5] - z_m1) / 4.);
+      pzy1 = 0.5 * ((z1_p2 - (double)o0[6]) / 4. - (z_p2 - (double)o0[5]) / 4.);
+    }
+    // r: theta faces and z faces of rows a, b
+    const bool rlo = (j == 0), rhi = (j == d.NR - 1);
+    const int ra = rlo ? j + 1 : j - 1, rb = rlo ? j + 2 : (rhi ? j - 2 : j + 1);
+    double pyx0, pyx1, pzx0, pzx1;
+    {
+      const size_t tra = d.offT + NT * (ra + NR * k), trb = d.offT + NT * (rb + NR * k);
+      R a0, a1, b0, b1;
+      ld2(fr, tra + i, a0, a1);
+      ld2(fr, trb + i, b0, b1);
+      const R a2 = fr[tra + ip2], b2 = fr[trb + ip2];
+      pyx0 = 0.5 * (along(rlo, rhi, o0[4], a1, b1) - along(rlo, rhi, o0[3], a0, b0));
+      pyx1 = 0.5 * (along(rlo, rhi, o1[4], a2, b2) - along(rlo, rhi, o1[3], a1, b1));
+      const size_t zra = d.offZ + NT * (ra + NR * k), zrb = d.offZ + NT * (rb + NR * k);
+      R za0, za1, zb0, zb1, zA0, zA1, zB0, zB1;
+      ld2(fr, zra + i, za0, za1);
+      ld2(fr, zrb + i, zb0, zb1);
+      ld2(fr, zra + pl + i, zA0, zA1);
+      ld2(fr, zrb + pl + i, zB0, zB1);
+      pzx0 = 0.5 * (along(rlo, rhi, o0[6], zA0, zB0) - along(rlo, rhi, o0[5], za0, zb0));
+      pzx1 = 0.5 * (along(rlo, rhi, o1[6], zA1, zB1) - along(rlo, rhi, o1[5], za1, zb1));
+    }
+    // z: r faces (rows j, j+1) and theta faces of planes a, b
+    const bool zlo = (k == 0), zhi = (k == d.NZ - 1);
+    const int ka = zlo ? k + 1 : k - 1, kb = zlo ? k + 2 : (zhi ? k - 2 : k + 1);
+    double pxz0, pxz1, pyz0, pyz1;
+    {
+      const size_t rka = NT * (j + (NR + 1) * ka), rkb = NT * (j + (NR + 1) * kb);
+      R pa0, pa1, pb0, pb1, pA0, pA1, pB0, pB1;
+      ld2(fr, rka + i, pa0, pa1);
+      ld2(fr, rkb + i, pb0, pb1);
+      ld2(fr, rka + NT + i, pA0, pA1);
+      ld2(fr, rkb + NT + i, pB0, pB1);
+      pxz0 = 0.5 * (along(zlo, zhi, o0[2], pA0, pB0) - along(zlo, zhi, o0[1], pa0, pb0));
+      pxz1 = 0.5 * (along(zlo, zhi, o1[2], pA1, pB1) - along(zlo, zhi, o1[1], pa1, pb1));
+      const size_t tka = d.offT + NT * (j + NR * ka), tkb = d.offT + NT * (j + NR * kb);
+      R a0, a1, b0, b1;
+      ld2(fr, tka + i, a0, a1);
+      ld2(fr, tkb + i, b0, b1);
+      const R a2 = fr[tka + ip2], b2 = fr[tkb + ip2];
+      pyz0 = 0.5 * (along(zlo, zhi, o0[4], a1, b1) - along(zlo, zhi, o0[3], a0, b0));
+      pyz1 = 0.5 * (along(zlo, zhi, o1[4], a2, b2) - along(zlo, zhi, o1[3], a1, b1));
+    }
+    // R_D: G_i d_i phi - g^ij d_ij phi, term by term in source order
+    double RD0, RD1;
+    {
+      const double px0 = (o0[2] - o0[1]) / 2., px1 = (o1[2] - o1[1]) / 2.;
+      const double py0 = (o0[4] - o0[3]) / 2., py1 = (o1[4] - o1[3]) / 2.;
+      const double pz0 = (o0[6] - o0[5]) / 2., pz1 = (o1[6] - o1[5]) / 2.;
+      R a0, a1;
+      ld2(g.G, c, a0, a1);
+      double s0 = a0 * px0, s1 = a1 * px1;
+      ld2(g.G + Nc, c, a0, a1);
+      s0 = s0 + a0 * py0;
+      s1 = s1 + a1 * py1;
+      ld2(g.G + 2 * Nc, c, a0, a1);
+      s0 = s0 + a0 * pz0;
+      s1 = s1 + a1 * pz1;
+      const int slot[6] = {3, 1, 6, 2, 7, 5};
+      const double d0[6] = {pxy0, pyx0, pxz0, pzx0, pyz0, pzy0}, d1[6] = {pxy1, pyx1, pxz1, pzx1, pyz1, pzy1};
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        ld2(g.gij + (size_t)slot[t] * Nc, c, a0, a1);
+        s0 = s0 - a0 * d0[t];
+        s1 = s1 - a1 * d1[t];
+      }
+      RD0 = P.inv_Re * s0;
+      RD1 = P.inv_Re * s1;
+    }
+    const double B0 = (0. + RD0 + RB0), B1 = (0. + RD1 + RB1);
+    // cell update (cell_update), term by term
+    R cv0, cv1, co0, co1, a0, a1;
+    ld2(F.c[q], c, cv0, cv1);
+    ld2(F.co[q], c, co0, co1);
+    const double w = P.w[q];
+    ld2(F.MF4, c, a0, a1);
+    const double F40 = a0, F41 = a1;
+    ld2(F.MF4 + Nc, c, a0, a1);
+    double s0 = +a0 * (double)co0, s1 = +a1 * (double)co1;
+#pragma unroll
+    for (int m = 2; m <= 7; ++m) {
+      ld2(F.MF4 + (size_t)m * Nc, c, a0, a1);
+      s0 = s0 + a0 * (double)o0[m - 1];
+      s1 = s1 + a1 * (double)o1[m - 1];
+    }
+    const double nw0 = stored<R>((1 - w) * (double)cv0 + (w / F40) * (s0 + B0));
+    const double nw1 = stored<R>((1 - w) * (double)cv1 + (w / F41) * (s1 + B1));
+    typename Pair2<R>::T out;
+    out.x = (R)nw0;
+    out.y = (R)nw1;
+    *reinterpret_cast<typename Pair2<R>::T *>(F.c[q] + c) = out;
+    e[q] = nmax(errv(nw0, cv0, first), errv(nw1, cv1, first));
+  }
+  block_max<3, CB3>(red, e, ctl->err[par]);
 }
 
 // ---- K2: +xi face updates of u, v, w (nse.f90:878-1005).

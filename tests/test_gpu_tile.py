@@ -105,6 +105,29 @@ def test_tile_and_gather_forms_are_bitwise_equal(monkeypatch, precision):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+@pytest.mark.parametrize("dims", [(40, 6, 26), (130, 5, 7)])
+def test_pair_and_gather_cell_sweeps_are_bitwise_equal(monkeypatch, precision, dims):
+    """k_vel_cell2 (two theta-adjacent cells per thread, paired loads)
+    against k_vel_cell: whole steps to the bit (theta seams, walls, a
+    partial 64-cell patch)."""
+    case = config.small_case(*dims, steps=2)
+    monkeypatch.setenv("NIM_FACE_SWEEP", "gather")
+    outs = []
+    for form in ("gather", "pair"):
+        monkeypatch.setenv("NIM_CELL_SWEEP", form)
+        s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()), case.params(precision=precision))
+        s.initialize_nse()
+        s.add_temperature_noise(case.noise, case.seed)
+        recs = s.solve_nse(2)
+        outs.append(([(r.iters, r.iters_fp32, r.nu_inner) for r in recs], [s.download(f) for f in STATE]))
+        assert ("k_vel_cell2" if form == "pair" else "k_vel_cell") in s.profile_iterations(1)
+        s.close()
+    assert outs[0][0] == outs[1][0]
+    for a, b in zip(outs[0][1], outs[1][1]):
+        assert np.array_equal(a, b)
+
+
 def test_automatic_choice(monkeypatch):
     """Without the override: the tile form on a mesh with enough patches,
     the gather form on one that cannot fill the GPU."""
@@ -115,19 +138,23 @@ def test_automatic_choice(monkeypatch):
         s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()), case.params())
         s.initialize_nse()
         prof = s.profile_iterations(1)
-        assert "k_vel_face" + suffix in prof and "k_vel_cell" in prof  # the cell sweep only on request
+        # the cell sweep: the paired-load form for even n_theta, the tile only on request
+        assert "k_vel_face" + suffix in prof and "k_vel_cell2" in prof
         s.close()
 
 
-def test_kernel_choice_follows_n_theta():
-    for nt, suffix in ((16, "_tile"), (18, "")):
+def test_kernel_choice_follows_n_theta(monkeypatch):
+    """With both tiles requested: n_theta = 16 gets them; 18 (not a multiple
+    of 4) keeps the gather face sweep and the paired cell sweep; 19 (odd)
+    the gather forms of both."""
+    for nt, face, cell in ((16, "k_vel_face_tile", "k_vel_cell_tile"), (18, "k_vel_face", "k_vel_cell2"),
+                           (19, "k_vel_face", "k_vel_cell")):
         case = config.small_case(nt, 5, 6)
         s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()), case.params())
         s.initialize_nse()
         prof = s.profile_iterations(1)
-        for sweep in ("k_vel_face", "k_vel_cell"):
-            assert sweep + suffix in prof
-            assert (sweep in prof) != (sweep + "_tile" in prof)
+        names = [k for k in prof if k.startswith("k_vel_")]
+        assert names == [cell, face], names
         s.close()
 
 
