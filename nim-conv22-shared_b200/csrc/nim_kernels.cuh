@@ -1278,87 +1278,87 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
       return lo ? tang_vals(true, false, v0, va, vb, 0., 0.)
                 : hi ? tang_vals(false, true, v0, 0., 0., va, vb) : tang_vals(false, false, v0, vb, 0., va, 0.);
     };
-    // theta: centred; r faces (rows j, j+1) and z faces (levels k, k+1) at theta i-1, i+2
-    double pxy0, pxy1, pzy0, pzy1;
-    {
-      const size_t rrow = NT * (j + (NR + 1) * k), zlev = d.offZ + NT * (j + NR * k);
-      const double r_m1 = fr[rrow + im1], r_p2 = fr[rrow + ip2];
-      const double r1_m1 = fr[rrow + NT + im1], r1_p2 = fr[rrow + NT + ip2];
-      pxy0 = 0.5 * (((double)o1[2] - r1_m1) / 4. - ((double)o1[1] - r_m1) / 4.);
-      pxy1 = 0.5 * ((r1_p2 - (double)o0[2]) / 4. - (r_p2 - (double)o0[1]) / 4.);
-      const double z_m1 = fr[zlev + im1], z_p2 = fr[zlev + ip2];
-      const double z1_m1 = fr[zlev + pl + im1], z1_p2 = fr[zlev + pl + ip2];
-      pzy0 = 0.5 * (((double)o1[6] - z1_m1) / 4. - ((double)o1[5] - z_m1) / 4.);
-      pzy1 = 0.5 * ((z1_p2 - (double)o0[6]) / 4. - (z_p2 - (double)o0[5]) / 4.);
-    }
-    // r: theta faces and z faces of rows a, b
+    // R_D: G_i d_i phi - g^ij d_ij phi, term by term in source order; each
+    // cross derivative is formed for both cells right before its term
     const bool rlo = (j == 0), rhi = (j == d.NR - 1);
     const int ra = rlo ? j + 1 : j - 1, rb = rlo ? j + 2 : (rhi ? j - 2 : j + 1);
-    double pyx0, pyx1, pzx0, pzx1;
-    {
-      const size_t tra = d.offT + NT * (ra + NR * k), trb = d.offT + NT * (rb + NR * k);
-      R a0, a1, b0, b1;
-      ld2(fr, tra + i, a0, a1);
-      ld2(fr, trb + i, b0, b1);
-      const R a2 = fr[tra + ip2], b2 = fr[trb + ip2];
-      pyx0 = 0.5 * (along(rlo, rhi, o0[4], a1, b1) - along(rlo, rhi, o0[3], a0, b0));
-      pyx1 = 0.5 * (along(rlo, rhi, o1[4], a2, b2) - along(rlo, rhi, o1[3], a1, b1));
-      const size_t zra = d.offZ + NT * (ra + NR * k), zrb = d.offZ + NT * (rb + NR * k);
-      R za0, za1, zb0, zb1, zA0, zA1, zB0, zB1;
-      ld2(fr, zra + i, za0, za1);
-      ld2(fr, zrb + i, zb0, zb1);
-      ld2(fr, zra + pl + i, zA0, zA1);
-      ld2(fr, zrb + pl + i, zB0, zB1);
-      pzx0 = 0.5 * (along(rlo, rhi, o0[6], zA0, zB0) - along(rlo, rhi, o0[5], za0, zb0));
-      pzx1 = 0.5 * (along(rlo, rhi, o1[6], zA1, zB1) - along(rlo, rhi, o1[5], za1, zb1));
-    }
-    // z: r faces (rows j, j+1) and theta faces of planes a, b
     const bool zlo = (k == 0), zhi = (k == d.NZ - 1);
     const int ka = zlo ? k + 1 : k - 1, kb = zlo ? k + 2 : (zhi ? k - 2 : k + 1);
-    double pxz0, pxz1, pyz0, pyz1;
-    {
-      const size_t rka = NT * (j + (NR + 1) * ka), rkb = NT * (j + (NR + 1) * kb);
-      R pa0, pa1, pb0, pb1, pA0, pA1, pB0, pB1;
-      ld2(fr, rka + i, pa0, pa1);
-      ld2(fr, rkb + i, pb0, pb1);
-      ld2(fr, rka + NT + i, pA0, pA1);
-      ld2(fr, rkb + NT + i, pB0, pB1);
-      pxz0 = 0.5 * (along(zlo, zhi, o0[2], pA0, pB0) - along(zlo, zhi, o0[1], pa0, pb0));
-      pxz1 = 0.5 * (along(zlo, zhi, o1[2], pA1, pB1) - along(zlo, zhi, o1[1], pa1, pb1));
-      const size_t tka = d.offT + NT * (j + NR * ka), tkb = d.offT + NT * (j + NR * kb);
-      R a0, a1, b0, b1;
-      ld2(fr, tka + i, a0, a1);
-      ld2(fr, tkb + i, b0, b1);
-      const R a2 = fr[tka + ip2], b2 = fr[tkb + ip2];
-      pyz0 = 0.5 * (along(zlo, zhi, o0[4], a1, b1) - along(zlo, zhi, o0[3], a0, b0));
-      pyz1 = 0.5 * (along(zlo, zhi, o1[4], a2, b2) - along(zlo, zhi, o1[3], a1, b1));
-    }
-    // R_D: G_i d_i phi - g^ij d_ij phi, term by term in source order
-    double RD0, RD1;
+    double s0, s1;
     {
       const double px0 = (o0[2] - o0[1]) / 2., px1 = (o1[2] - o1[1]) / 2.;
       const double py0 = (o0[4] - o0[3]) / 2., py1 = (o1[4] - o1[3]) / 2.;
       const double pz0 = (o0[6] - o0[5]) / 2., pz1 = (o1[6] - o1[5]) / 2.;
       R a0, a1;
       ld2(g.G, c, a0, a1);
-      double s0 = a0 * px0, s1 = a1 * px1;
+      s0 = a0 * px0;
+      s1 = a1 * px1;
       ld2(g.G + Nc, c, a0, a1);
       s0 = s0 + a0 * py0;
       s1 = s1 + a1 * py1;
       ld2(g.G + 2 * Nc, c, a0, a1);
       s0 = s0 + a0 * pz0;
       s1 = s1 + a1 * pz1;
-      const int slot[6] = {3, 1, 6, 2, 7, 5};
-      const double d0[6] = {pxy0, pyx0, pxz0, pzx0, pyz0, pzy0}, d1[6] = {pxy1, pyx1, pxz1, pzx1, pyz1, pzy1};
-#pragma unroll
-      for (int t = 0; t < 6; ++t) {
-        ld2(g.gij + (size_t)slot[t] * Nc, c, a0, a1);
-        s0 = s0 - a0 * d0[t];
-        s1 = s1 - a1 * d1[t];
-      }
-      RD0 = P.inv_Re * s0;
-      RD1 = P.inv_Re * s1;
     }
+    auto term = [&](int slot, double d0, double d1) {
+      R a0, a1;
+      ld2(g.gij + (size_t)slot * Nc, c, a0, a1);
+      s0 = s0 - a0 * d0;
+      s1 = s1 - a1 * d1;
+    };
+    {  // pxy: r faces (rows j, j+1) at theta i-1, i+2 (centred in theta)
+      const size_t rrow = NT * (j + (NR + 1) * k);
+      const double r_m1 = fr[rrow + im1], r_p2 = fr[rrow + ip2];
+      const double r1_m1 = fr[rrow + NT + im1], r1_p2 = fr[rrow + NT + ip2];
+      term(3, 0.5 * (((double)o1[2] - r1_m1) / 4. - ((double)o1[1] - r_m1) / 4.),
+           0.5 * ((r1_p2 - (double)o0[2]) / 4. - (r_p2 - (double)o0[1]) / 4.));
+    }
+    {  // pyx: theta faces of rows a, b
+      const size_t tra = d.offT + NT * (ra + NR * k), trb = d.offT + NT * (rb + NR * k);
+      R a0, a1, b0, b1;
+      ld2(fr, tra + i, a0, a1);
+      ld2(fr, trb + i, b0, b1);
+      const R a2 = fr[tra + ip2], b2 = fr[trb + ip2];
+      term(1, 0.5 * (along(rlo, rhi, o0[4], a1, b1) - along(rlo, rhi, o0[3], a0, b0)),
+           0.5 * (along(rlo, rhi, o1[4], a2, b2) - along(rlo, rhi, o1[3], a1, b1)));
+    }
+    {  // pxz: r faces (rows j, j+1) of planes a, b
+      const size_t rka = NT * (j + (NR + 1) * ka), rkb = NT * (j + (NR + 1) * kb);
+      R pa0, pa1, pb0, pb1, pA0, pA1, pB0, pB1;
+      ld2(fr, rka + i, pa0, pa1);
+      ld2(fr, rkb + i, pb0, pb1);
+      ld2(fr, rka + NT + i, pA0, pA1);
+      ld2(fr, rkb + NT + i, pB0, pB1);
+      term(6, 0.5 * (along(zlo, zhi, o0[2], pA0, pB0) - along(zlo, zhi, o0[1], pa0, pb0)),
+           0.5 * (along(zlo, zhi, o1[2], pA1, pB1) - along(zlo, zhi, o1[1], pa1, pb1)));
+    }
+    {  // pzx: z faces (levels k, k+1) of rows a, b
+      const size_t zra = d.offZ + NT * (ra + NR * k), zrb = d.offZ + NT * (rb + NR * k);
+      R za0, za1, zb0, zb1, zA0, zA1, zB0, zB1;
+      ld2(fr, zra + i, za0, za1);
+      ld2(fr, zrb + i, zb0, zb1);
+      ld2(fr, zra + pl + i, zA0, zA1);
+      ld2(fr, zrb + pl + i, zB0, zB1);
+      term(2, 0.5 * (along(rlo, rhi, o0[6], zA0, zB0) - along(rlo, rhi, o0[5], za0, zb0)),
+           0.5 * (along(rlo, rhi, o1[6], zA1, zB1) - along(rlo, rhi, o1[5], za1, zb1)));
+    }
+    {  // pyz: theta faces of planes a, b
+      const size_t tka = d.offT + NT * (j + NR * ka), tkb = d.offT + NT * (j + NR * kb);
+      R a0, a1, b0, b1;
+      ld2(fr, tka + i, a0, a1);
+      ld2(fr, tkb + i, b0, b1);
+      const R a2 = fr[tka + ip2], b2 = fr[tkb + ip2];
+      term(7, 0.5 * (along(zlo, zhi, o0[4], a1, b1) - along(zlo, zhi, o0[3], a0, b0)),
+           0.5 * (along(zlo, zhi, o1[4], a2, b2) - along(zlo, zhi, o1[3], a1, b1)));
+    }
+    {  // pzy: z faces (levels k, k+1) at theta i-1, i+2
+      const size_t zlev = d.offZ + NT * (j + NR * k);
+      const double z_m1 = fr[zlev + im1], z_p2 = fr[zlev + ip2];
+      const double z1_m1 = fr[zlev + pl + im1], z1_p2 = fr[zlev + pl + ip2];
+      term(5, 0.5 * (((double)o1[6] - z1_m1) / 4. - ((double)o1[5] - z_m1) / 4.),
+           0.5 * ((z1_p2 - (double)o0[6]) / 4. - (z_p2 - (double)o0[5]) / 4.));
+    }
+    const double RD0 = P.inv_Re * s0, RD1 = P.inv_Re * s1;
     const double B0 = (0. + RD0 + RB0), B1 = (0. + RD1 + RB1);
     // cell update (cell_update), term by term
     R cv0, cv1, co0, co1, a0, a1;
@@ -1368,15 +1368,15 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
     ld2(F.MF4, c, a0, a1);
     const double F40 = a0, F41 = a1;
     ld2(F.MF4 + Nc, c, a0, a1);
-    double s0 = +a0 * (double)co0, s1 = +a1 * (double)co1;
+    double u0 = +a0 * (double)co0, u1 = +a1 * (double)co1;
 #pragma unroll
     for (int m = 2; m <= 7; ++m) {
       ld2(F.MF4 + (size_t)m * Nc, c, a0, a1);
-      s0 = s0 + a0 * (double)o0[m - 1];
-      s1 = s1 + a1 * (double)o1[m - 1];
+      u0 = u0 + a0 * (double)o0[m - 1];
+      u1 = u1 + a1 * (double)o1[m - 1];
     }
-    const double nw0 = stored<R>((1 - w) * (double)cv0 + (w / F40) * (s0 + B0));
-    const double nw1 = stored<R>((1 - w) * (double)cv1 + (w / F41) * (s1 + B1));
+    const double nw0 = stored<R>((1 - w) * (double)cv0 + (w / F40) * (u0 + B0));
+    const double nw1 = stored<R>((1 - w) * (double)cv1 + (w / F41) * (u1 + B1));
     typename Pair2<R>::T out;
     out.x = (R)nw0;
     out.y = (R)nw1;
