@@ -201,9 +201,12 @@ void nim_params_reference(nim_params *p);
    a multiple of 4, at most 256, and the mesh gives at least one block per
    SM, else in its gather form (the results are identical);
    NIM_FACE_SWEEP=tile or =gather in the environment overrides the choice.
-   NIM_CELL_SWEEP=tile selects the TMA-staged form of the u, v, w source and
-   cell sweep under the same n_theta conditions (formulation 2; identical
-   results, not faster at the benchmark sizes, so off by default). */
+   The u, v, w source and cell sweep (formulation 2) runs on theta-adjacent
+   cell pairs with paired loads when n_theta is even, else one cell per
+   thread; NIM_CELL_SWEEP=gather forces the one-cell form, =tile a
+   TMA-staged form under the face sweep's n_theta conditions (not faster at
+   the benchmark sizes, so off by default).  All forms give identical
+   results. */
 int nim_gpu_create(const nim_mesh_desc *mesh, const nim_params *params,
                    nim_ctx **out);
 
