@@ -308,6 +308,13 @@ int64_t nim_gpu_launch_count(nim_ctx *ctx);
 int nim_gpu_profile_iterations(nim_ctx *ctx, int32_t n, double *ms, int32_t cap);
 const char *nim_gpu_profile_name(nim_ctx *ctx, int32_t k);
 
+/* Self-test of the bounded device waits (no counterpart in the reference):
+   runs the wait that the TMA-staged sweeps use on an mbarrier that no copy
+   will complete, at most `tries` (1..2^20) times, and returns the status the
+   device recorded (NIM_ERR_TIMEOUT when the bound works), then clears it;
+   the context stays usable.  Between steps only. */
+int nim_gpu_selftest_wait_timeout(nim_ctx *ctx, int32_t tries);
+
 /* Wall-face limit of nim_gpu_nusselt_noalloc: 2*n_theta*n_z inner plus
    outer wall faces, i.e. 4096 blocks of 256 faces. */
 #define NIM_NOALLOC_MAX_WALL_FACES 1048576

@@ -1552,6 +1552,20 @@ extern "C" int nim_gpu_profile_iterations(nim_ctx *x, int32_t n, double *ms, int
   return nk;
 }
 
+extern "C" int nim_gpu_selftest_wait_timeout(nim_ctx *x, int32_t tries) {
+  if (!x || tries < 1 || tries > (1 << 20)) return NIM_ERR_BAD_ARG;
+  if (!x->initialized || x->in_step) return NIM_ERR_STATE;
+  CK(cudaSetDevice(x->device));
+  k_step_reset<<<1, 1, 0, x->stream>>>(x->ctl);
+  k_wait_selftest<<<1, 1, 0, x->stream>>>(x->ctl, tries);
+  CK(cudaGetLastError());
+  TRY(read_ctrl(x));
+  const int seen = x->ctl_host->status;
+  k_step_reset<<<1, 1, 0, x->stream>>>(x->ctl);  // the context stays usable
+  TRY(read_ctrl(x));
+  return seen;
+}
+
 extern "C" const char *nim_gpu_profile_name(nim_ctx *x, int32_t k) {
   return (x && k >= 0 && k < (int32_t)x->prof_names.size()) ? x->prof_names[k].c_str() : "";
 }

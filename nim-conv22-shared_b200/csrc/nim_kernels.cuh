@@ -1081,14 +1081,26 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
   return ok != 0;
 }
 constexpr int kWaitTries = 1 << 22;  // each try suspends for a hardware-chosen slice
-__device__ __noinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, Ctrl *ctl) {
-  for (int n = 0; n < kWaitTries; ++n)
+__device__ __noinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, Ctrl *ctl,
+                                       int tries = kWaitTries) {
+  for (int n = 0; n < tries; ++n)
     if (mbar_try_wait(bar, parity)) return true;
   atomicCAS(&ctl->status, 0, -5);  // NIM_ERR_TIMEOUT
   *(volatile int *)&ctl->done = 1;
-  for (int n = 0; n < kWaitTries; ++n)
+  for (int n = 0; n < tries; ++n)
     if (mbar_try_wait(bar, parity)) break;
   return false;
+}
+
+// The timeout path of mbar_wait on the device, without a fault: one thread
+// posts 16 expected bytes that no copy will bring and waits at most `tries`
+// times; the step is then marked NIM_ERR_TIMEOUT and stopped.  No copy is in
+// flight, so nothing can land after the block leaves.
+__global__ void k_wait_selftest(Ctrl *ctl, int tries) {
+  __shared__ alignas(8) unsigned long long bar;
+  mbar_init(&bar, 1);
+  mbar_expect_tx(&bar, 16);
+  mbar_wait(&bar, 0, ctl, tries);
 }
 
 __device__ __forceinline__ double errv(double nw, double old, bool first) { return fabs(nw - (first ? 0.0 : old)); }
