@@ -198,7 +198,7 @@ void nim_params_reference(nim_params *p);
 /* Copy the mesh and parameters to the device.  Replaces the module-global
    allocation of parameters.f90:222-292.  *out receives the context.
    The +xi face sweep of u, v, w runs in its TMA-staged form when n_theta is
-   a multiple of 4, at most 256, and the mesh gives at least one block per
+   a multiple of 4, at most 256, and the mesh gives at least four blocks per
    SM, else in its gather form (the results are identical);
    NIM_FACE_SWEEP=tile or =gather in the environment overrides the choice.
    The u, v, w source and cell sweep (formulation 2) runs on theta-adjacent

@@ -844,8 +844,10 @@ static bool encode_vel_cell_maps(const Dims &d, const FieldsT<R> &F, VelCellMaps
 }
 
 // The +xi face sweep of u, v, w runs as k_vel_face_tile when n_theta is a
-// multiple of 4 (16-byte box rows), at most 256, and the mesh gives at least
-// one block per SM; the z-chunk length aims at about six waves of blocks with
+// multiple of 4 (16-byte box rows), at most 256, and the mesh by itself
+// gives at least four waves of blocks (fewer, and the 109 KB blocks cost
+// more than they save: at 96x96x64, and for the enclosures of a batch that
+// share the GPU); the z-chunk length aims at about six waves of blocks with
 // chunks of at least 8 planes.  NIM_FACE_SWEEP=tile or =gather in the
 // environment forces the choice (tile still needs the n_theta conditions).
 // The source and cell sweep of u, v, w (formulation 2) runs as k_vel_cell2
@@ -864,7 +866,7 @@ static int choose_face_sweep(nim_ctx *x) {
   const bool shape = (d.NT % 4 == 0) && d.NT <= 256;
   const char *env = std::getenv("NIM_FACE_SWEEP");
   const std::string force = env ? env : "";
-  x->bulk = shape && !x->seq && (force == "tile" || (force != "gather" && blocks >= sms));
+  x->bulk = shape && !x->seq && (force == "tile" || (force != "gather" && blocks >= 4 * sms));
   // the staged cell sweep only on request: its u, v, w faces are a sixth of
   // k_vel_cell's bytes, and the two 110 KB blocks per SM it needs leave the
   // direct loads of the rest with fewer warps than the gather form has

@@ -133,7 +133,7 @@ def test_automatic_choice(monkeypatch):
     the gather form on one that cannot fill the GPU."""
     monkeypatch.delenv("NIM_FACE_SWEEP")
     monkeypatch.delenv("NIM_CELL_SWEEP")
-    for dims, suffix in (((128, 64, 32), "_tile"), ((48, 48, 32), "")):
+    for dims, suffix in (((128, 128, 48), "_tile"), ((128, 64, 32), "")):
         case = config.small_case(*dims)
         s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()), case.params())
         s.initialize_nse()
