@@ -263,6 +263,53 @@ int nim_gpu_set_graph_iters(nim_ctx *ctx, int32_t n);
    NIM_OK. */
 int nim_batch_step(int32_t n, nim_ctx *const *ctx, int32_t nsteps, nim_step_stats *per, int32_t *done);
 
+/* ---- z-slab decomposition (no counterpart in the reference, which runs
+   one enclosure on one node).  The n_z cell planes split into nslab
+   contiguous slabs of n_z / nslab or one more planes (at least 2 each).
+   A slab's context holds its own planes and, on each side with a
+   neighbour slab, that neighbour's two nearest planes (the halo: the
+   farthest any stencil of an owned cell or face reaches in z away from
+   the physical walls).  find_error's maxima, check_steady_state, evaluate_D
+   and find_Nu2 cover only the owned planes.
+
+   nim_slab_layout: out4 = {first plane held, one past the last held, first
+   plane owned, one past the last owned}, global plane numbers.
+   NIM_ERR_BAD_ARG unless 1 <= nslab, 0 <= s < nslab, n_z / nslab >= 2. */
+int nim_slab_layout(int32_t n_z, int32_t nslab, int32_t s, int32_t *out4);
+
+/* The halo exchange of slab s with its neighbour below (side 0) or above
+   (side 1), as element spans (offset, count) into the slab context's own
+   arrays: {cells, r faces, theta faces, z faces}.  recv8: the halo planes
+   the neighbour owns; send8: the owned planes the neighbour holds as its
+   halo.  Every cell array carries span 0; every face array carries spans
+   1..3 in both of its halves (the face arrays alternate halves each
+   pass).  The send spans of slab s, side 1, and the receive spans of slab
+   s+1, side 0, have the same counts, and vice versa.  NIM_ERR_BAD_ARG on
+   a side without a neighbour. */
+int nim_slab_halo(int32_t n_theta, int32_t n_r, int32_t n_z, int32_t nslab, int32_t s, int32_t side,
+                  int64_t *recv8, int64_t *send8);
+
+/* nim_gpu_create for slab s of nslab of the mesh described by mesh (the
+   whole mesh's arrays, checked as nim_gpu_create checks them).  The
+   context is a cylinder of its held planes: nim_gpu_download/upload
+   address its cells and faces in the library's structured order (cell
+   i + n_theta*(j + n_r*k) with k the held plane from the slab's first;
+   faces in the r / theta / z blocks of that numbering).  Parallel
+   schedule, formulation 2, FP64 only (NIM_ERR_BAD_ARG otherwise). */
+int nim_gpu_create_slab(const nim_mesh_desc *mesh, const nim_params *params, int32_t nslab, int32_t s,
+                        nim_ctx **ctx);
+
+/* nim_gpu_step for the nslab = n slab contexts ctx[0..n) of one mesh on
+   one device (ctx[s] created as slab s of n, each initialised).  Each pass
+   runs its velocity, pressure and temperature parts on every slab, each
+   part followed by the halo exchange of the fields it changed
+   (device-to-device copies), then merges the maxima so every slab takes
+   the same convergence decision.  The fields of the owned planes are
+   bit-identical to a whole-mesh context's, with the same iteration counts;
+   dilatation and the Nusselt numbers are the group's sums (the summation
+   order differs).  per (may be NULL) receives nsteps group records. */
+int nim_slab_step(int32_t n, nim_ctx *const *ctx, int32_t nsteps, nim_step_stats *per, int32_t *done);
+
 /* Copy a field to/from host memory in the reference layout (for
    write_data / write_restart / read_restart, postprocess.f90, restart.f90).
    n = number of doubles the host buffer holds. */

@@ -25,6 +25,12 @@ struct Dims {
   int NF;           // faces
   int NBF;          // boundary faces (2*NT*NR + 2*NT*NZ)
   int plane;        // NT*NR
+  // cell planes [kown0, kown1) this context owns: the maxima of find_error,
+  // check_steady_state and the wall and dilatation sums cover only these.
+  // All planes, except in a z-slab, whose outer two planes on a side with a
+  // neighbour slab are halo copies of that neighbour's cells.
+  int kown0, kown1;
+  __host__ __device__ bool owns(int k) const { return k >= kown0 && k < kown1; }
 };
 
 struct Cell {
@@ -86,6 +92,8 @@ __host__ inline Dims make_dims(int NT, int NR, int NZ) {
   d.offZ = d.offT + d.Nc;
   d.NF = d.offZ + NT * NR * (NZ + 1);
   d.NBF = 2 * NT * NR + 2 * NT * NZ;
+  d.kown0 = 0;
+  d.kown1 = NZ;
   return d;
 }
 

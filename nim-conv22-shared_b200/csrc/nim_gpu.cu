@@ -118,6 +118,13 @@ struct nim_ctx {
   int graph32_iters = 0;
   int phase = 0;
   int last_lowp = 0, last_hi = 0;
+  // z-slab s of slab_count (nim_gpu_create_slab; slab_count 0: the whole
+  // mesh): global plane of local plane 0, and per side (0: the slab below,
+  // 1: above) whether it has a neighbour and the element spans of its halo
+  // exchange (nim_slab_halo)
+  int slab_count = 0, slab_index = 0, slab_lo = 0;
+  bool halo_ok[2] = {false, false};
+  int64_t halo_recv[2][8] = {}, halo_send[2][8] = {};
   // a time step driven without blocking (the synchronous calls and
   // nim_batch_step share it): graph launches so far, the cap, the event that
   // marks the last control-block (or sums) copy
@@ -282,7 +289,10 @@ int launch_vel(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F
       TRY(mark(x, "k_vel_cell_tile"));
     } else if (x->cell_pair) {
       const dim3 gp((d.NT + 63) / 64, (d.NR + 3) / 4, d.NZ);
-      k_vel_cell2<<<gp, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+      if (x->slab_count)
+        k_vel_cell2<R, true><<<gp, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+      else
+        k_vel_cell2<R><<<gp, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
       TRY(mark(x, "k_vel_cell2"));
     } else {
       k_vel_cell<false, 2><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
@@ -357,34 +367,48 @@ int launch_iteration_seq(nim_ctx *x) {
   return NIM_OK;
 }
 
-// one pass of the parallel schedule over arrays of storage type R
+// the pressure part of a parallel pass (nse.f90:150-156)
 template <class R>
-int launch_parallel(nim_ctx *x, const GeoT<R> &g, const FieldsT<R> &F, int lowp) {
+int launch_pressure(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F) {
   const Dims &d = x->d;
-  cudaStream_t s = x->stream;
-  const int gc = x->nblk_c, gb = x->nblk_b;
-  const dim3 g3 = x->g3, g8 = x->g8;
-  TRY(launch_vel(x, s, g, F));
+  const dim3 g3 = x->g3;
   k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_p_src"));
-  k_p_bc<<<gb, BLK, 0, s>>>(d, g, F, x->phys, x->ctl);
+  k_p_bc<<<x->nblk_b, BLK, 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_p_bc"));
-  k_p_bc_copy<<<gb, BLK, 0, s>>>(d, F, x->ctl);
+  k_p_bc_copy<<<x->nblk_b, BLK, 0, s>>>(d, F, x->ctl);
   TRY(mark(x, "k_p_bc_copy"));
   k_p_face<<<g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_p_face"));
   if (x->phys.dpdx_tolerance) {
-    k_p_dpdx<<<gc, BLK, 0, s>>>(d, g, F, x->ctl);
+    k_p_dpdx<<<x->nblk_c, BLK, 0, s>>>(d, g, F, x->ctl);
     TRY(mark(x, "k_p_dpdx"));
   }
+  return NIM_OK;
+}
+
+// the temperature part of a parallel pass (nse.f90:157-162)
+template <class R>
+int launch_temperature(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F) {
+  const Dims &d = x->d;
   k_zero_flux<<<grid(2 * d.plane), BLK, 0, s>>>(d, g, F, x->ctl);
   TRY(mark(x, "k_zero_flux"));
   k_T_coef<<<dim3(3, x->nblk_c), BLK, 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_T_coef"));
   k_T_cell<false><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_T_cell"));
-  k_T_face<<<g8, BLK, 0, s>>>(d, g, F, x->phys, x->ctl);
+  k_T_face<<<x->g8, BLK, 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_T_face"));
+  return NIM_OK;
+}
+
+// one pass of the parallel schedule over arrays of storage type R
+template <class R>
+int launch_parallel(nim_ctx *x, const GeoT<R> &g, const FieldsT<R> &F, int lowp) {
+  cudaStream_t s = x->stream;
+  TRY(launch_vel(x, s, g, F));
+  TRY(launch_pressure(x, s, g, F));
+  TRY(launch_temperature(x, s, g, F));
   k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys, lowp);
   TRY(mark(x, "k_iter_end"));
   CK(cudaGetLastError());
@@ -878,19 +902,89 @@ static int choose_face_sweep(nim_ctx *x) {
   return NIM_OK;
 }
 
-static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) {
+// ---- z-slabs: the cell planes split into nslab contiguous runs of at least
+// two planes; each slab's context also holds the two planes either side that
+// a neighbour owns (its halo): no stencil of an owned cell or of a face of
+// one reaches further (the two-cell chains exist only at the physical walls,
+// nse.f90:1638-1639, bc.f90:345-390).
+extern "C" int nim_slab_layout(int32_t n_z, int32_t nslab, int32_t s, int32_t *out4) {
+  if (!out4 || nslab < 1 || s < 0 || s >= nslab || n_z < 3 || n_z / nslab < 2) return NIM_ERR_BAD_ARG;
+  const int32_t base = n_z / nslab, rem = n_z % nslab;
+  const int32_t own_lo = s * base + std::min(s, rem);
+  const int32_t own_hi = own_lo + base + (s < rem ? 1 : 0);
+  out4[0] = std::max(0, own_lo - 2);
+  out4[1] = std::min(n_z, own_hi + 2);
+  out4[2] = own_lo;
+  out4[3] = own_hi;
+  return NIM_OK;
+}
+
+extern "C" int nim_slab_halo(int32_t n_theta, int32_t n_r, int32_t n_z, int32_t nslab, int32_t s, int32_t side,
+                             int64_t *recv8, int64_t *send8) {
+  int32_t lay[4];
+  if (!recv8 || !send8 || n_theta < 1 || n_r < 1 || (side != 0 && side != 1)) return NIM_ERR_BAD_ARG;
+  TRY(nim_slab_layout(n_z, nslab, s, lay));
+  if ((side == 0 && s == 0) || (side == 1 && s == nslab - 1)) return NIM_ERR_BAD_ARG;
+  const int64_t NT = n_theta, NR = n_r, NZl = lay[1] - lay[0], pl = NT * NR;
+  const int64_t offT = NT * (NR + 1) * NZl, offZ = offT + pl * NZl;
+  // planes [g0, g0 + 2) of the slab with the z faces g0 .. g0 + 2
+  auto spans = [&](int64_t g0, int64_t *o) {
+    const int64_t l0 = g0 - lay[0];
+    o[0] = l0 * pl;                o[1] = 2 * pl;
+    o[2] = NT * (NR + 1) * l0;     o[3] = 2 * NT * (NR + 1);
+    o[4] = offT + l0 * pl;         o[5] = 2 * pl;
+    o[6] = offZ + l0 * pl;         o[7] = 3 * pl;
+  };
+  if (side == 0) {
+    spans(lay[2] - 2, recv8);
+    spans(lay[2], send8);
+  } else {
+    spans(lay[3], recv8);
+    spans(lay[3] - 2, send8);
+  }
+  return NIM_OK;
+}
+
+// slab: null for the whole mesh, else {nslab, s}: the context holds z-slab s
+// of nslab (nim_slab_layout) with its halo planes
+static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x, const int32_t *slab = nullptr) {
   CK(cudaGetDevice(&x->device));
   TRY(noalloc_setup(x->device));
   CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&x->copy_stream, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&x->run.ev, cudaEventDisableTiming));
   x->d = make_dims(m->n_theta, m->n_r, m->n_z);
-  const Dims &d = x->d;
   std::vector<int> perm;
-  TRY(verify_mesh(m, d, perm));
+  TRY(verify_mesh(m, x->d, perm));
+  const double *node_xyz = m->node_xyz;
+  int64_t nnode = m->nnode;
+  if (slab) {
+    // the slab's planes as a cylinder of their own; its faces and cells in
+    // the library's structured order (the identity permutation)
+    int32_t lay[4];
+    TRY(nim_slab_layout(m->n_z, slab[0], slab[1], lay));
+    if (p->schedule == NIM_SCHEDULE_REFERENCE || p->formulation == 1 || p->precision == NIM_PRECISION_MIXED)
+      return NIM_ERR_BAD_ARG;
+    const int NT = m->n_theta, NR = m->n_r;
+    x->d = make_dims(NT, NR, lay[1] - lay[0]);
+    x->d.kown0 = lay[2] - lay[0];
+    x->d.kown1 = lay[3] - lay[0];
+    x->slab_count = slab[0];
+    x->slab_index = slab[1];
+    x->slab_lo = lay[0];
+    node_xyz += 3 * (size_t)NT * (NR + 1) * lay[0];
+    nnode = (int64_t)NT * (NR + 1) * (x->d.NZ + 1);
+    perm.resize(x->d.NF);
+    for (int f = 0; f < x->d.NF; ++f) perm[f] = f;
+    for (int side = 0; side < 2; ++side)
+      x->halo_ok[side] = nim_slab_halo(NT, NR, m->n_z, slab[0], slab[1], side, x->halo_recv[side],
+                                       x->halo_send[side]) == NIM_OK;
+  }
+  const Dims &d = x->d;
   x->params = *p;
   x->seq = (p->schedule == NIM_SCHEDULE_REFERENCE);
   TRY(choose_face_sweep(x));
+  if (slab) x->bulk = x->cell_tile = false;  // the gather forms: masked maxima
   x->phys = make_phys(*p);
   x->gq = make_gauss();
   x->nblk_c = grid(d.Nc);
@@ -976,7 +1070,7 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
   }
   TRY(dalloc(x, &F.part, 8 * (size_t)std::max(x->nblk_c, grid(2 * d.NT * d.NZ))));
   TRY(dalloc(x, &x->ctl, 1));
-  TRY(dalloc(x, &x->node_xyz, 3 * (size_t)m->nnode));
+  TRY(dalloc(x, &x->node_xyz, 3 * (size_t)nnode));
   TRY(dalloc(x, &x->bcv, 25));
   TRY(dalloc(x, &x->perm, NF));
   TRY(dalloc(x, &x->scratch, std::max(54 * Nc, 3 * NF)));
@@ -1003,7 +1097,7 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
     }
   }
   if (x->seq) TRY(setup_levels(x));
-  CK(cudaMemcpyAsync(x->node_xyz, m->node_xyz, 3 * sizeof(double) * m->nnode, cudaMemcpyHostToDevice, x->stream));
+  CK(cudaMemcpyAsync(x->node_xyz, node_xyz, 3 * sizeof(double) * nnode, cudaMemcpyHostToDevice, x->stream));
   double bcv[25];
   for (int f = 0; f < 5; ++f)
     for (int b = 0; b < 5; ++b) bcv[5 * f + b] = p->bc_value[f][b];
@@ -1013,7 +1107,7 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x) 
   return NIM_OK;
 }
 
-extern "C" int nim_gpu_create(const nim_mesh_desc *m, const nim_params *p, nim_ctx **out) {
+static int create_checked(const nim_mesh_desc *m, const nim_params *p, nim_ctx **out, const int32_t *slab) {
   if (!m || !p || !out || !m->node_xyz || !m->meshes_nodes || !m->meshes_faces || !m->meshes_neighbors ||
       !m->faces_bc || !m->bcs_faces || !m->bcs_faces_id || !m->bcs_faces_position || !m->bcs_faces_mesh_num)
     return NIM_ERR_BAD_ARG;
@@ -1029,13 +1123,23 @@ extern "C" int nim_gpu_create(const nim_mesh_desc *m, const nim_params *p, nim_c
   *out = nullptr;
   nim_ctx *x = new (std::nothrow) nim_ctx();
   if (!x) return NIM_ERR_BAD_ARG;
-  const int st = create_impl(m, p, x);
+  const int st = create_impl(m, p, x, slab);
   if (st != NIM_OK) {
     nim_gpu_destroy(x);
     return st;
   }
   *out = x;
   return NIM_OK;
+}
+
+extern "C" int nim_gpu_create(const nim_mesh_desc *m, const nim_params *p, nim_ctx **out) {
+  return create_checked(m, p, out, nullptr);
+}
+
+extern "C" int nim_gpu_create_slab(const nim_mesh_desc *m, const nim_params *p, int32_t nslab, int32_t s,
+                                   nim_ctx **out) {
+  const int32_t slab[2] = {nslab, s};
+  return create_checked(m, p, out, slab);
 }
 
 extern "C" int nim_gpu_init(nim_ctx *x) {
@@ -1395,6 +1499,243 @@ extern "C" int nim_batch_step(int32_t n, nim_ctx *const *ctx, int32_t nsteps, ni
     if (!moved) std::this_thread::yield();
   }
   return first_error;
+}
+
+// ---- a group of z-slabs on one device, advanced together (nim_slab_step)
+namespace {
+constexpr int kMaxSlabs = 16;
+struct CtlList {
+  Ctrl *c[kMaxSlabs];
+  int n;
+};
+
+// find_error's maxima and the Dirichlet wall floor over every slab of the
+// group, written back to each slab's control block before its k_iter_end:
+// one thread per slot, so reads and writes of a slot never race
+__global__ void k_slab_merge(CtlList L) {
+  const int q = threadIdx.x;
+  if (q >= 16 || L.c[0]->done) return;
+  const int par = L.c[0]->iter & L.c[0]->pmask;
+  unsigned long long m = 0ull;
+  for (int s = 0; s < L.n; ++s) {
+    const unsigned long long v = (q < 8) ? L.c[s]->err[par][q] : L.c[s]->wall_floor[q - 8];
+    m = (v > m) ? v : m;
+  }
+  for (int s = 0; s < L.n; ++s) {
+    if (q < 8)
+      L.c[s]->err[par][q] = m;
+    else
+      L.c[s]->wall_floor[q - 8] = m;
+  }
+}
+
+// which arrays a halo exchange carries: after the velocity, pressure and
+// temperature parts of a pass, or the whole state
+enum { kHaloV = 1, kHaloP = 2, kHaloT = 4, kHaloAll = 8 };
+
+// src's owned planes next to dst into dst's halo: each cell array over span
+// 0, each face array (both halves) over the r, theta and z spans 1..3
+int copy_halo(const nim_ctx *src, const int64_t *snd, const nim_ctx *dst, const int64_t *rcv, cudaStream_t st,
+              int what) {
+  const Fields &A = src->F, &B = dst->F;
+  std::vector<std::pair<const double *, double *>> cells, faces;
+  const bool all = (what & kHaloAll) != 0;
+  if (all || (what & kHaloV))
+    for (int q = 0; q < 3; ++q) {
+      cells.emplace_back(A.c[q], B.c[q]);
+      faces.emplace_back(A.f[q], B.f[q]);
+    }
+  if (all || (what & kHaloP)) faces.emplace_back(A.f[3], B.f[3]);
+  if (all || (what & kHaloT)) {
+    cells.emplace_back(A.c[3], B.c[3]);
+    faces.emplace_back(A.f[4], B.f[4]);
+  }
+  if (all) {
+    for (int q = 0; q < 4; ++q) {
+      cells.emplace_back(A.co[q], B.co[q]);
+      cells.emplace_back(A.ct[q], B.ct[q]);
+    }
+    cells.emplace_back(A.mp, B.mp);
+    cells.emplace_back(A.dila, B.dila);
+    cells.emplace_back(A.dila_old, B.dila_old);
+    for (int q = 0; q < 3; ++q) cells.emplace_back(A.dpd + (size_t)q * src->d.Nc, B.dpd + (size_t)q * dst->d.Nc);
+  }
+  for (int t = 0; t < 4; ++t)
+    if (snd[2 * t + 1] != rcv[2 * t + 1]) return NIM_ERR_BAD_ARG;
+  for (auto &c : cells)
+    CK(cudaMemcpyAsync(c.second + rcv[0], c.first + snd[0], sizeof(double) * snd[1], cudaMemcpyDeviceToDevice, st));
+  const size_t NFa = src->d.NF, NFb = dst->d.NF;
+  for (auto &f : faces)
+    for (int h = 0; h < 2; ++h)
+      for (int t = 1; t < 4; ++t)
+        CK(cudaMemcpyAsync(f.second + h * NFb + rcv[2 * t], f.first + h * NFa + snd[2 * t],
+                           sizeof(double) * snd[2 * t + 1], cudaMemcpyDeviceToDevice, st));
+  return NIM_OK;
+}
+
+int halo_exchange(nim_ctx *const *X, int n, cudaStream_t st, int what) {
+  for (int s = 0; s + 1 < n; ++s) {
+    TRY(copy_halo(X[s], X[s]->halo_send[1], X[s + 1], X[s + 1]->halo_recv[0], st, what));
+    TRY(copy_halo(X[s + 1], X[s + 1]->halo_send[0], X[s], X[s]->halo_recv[1], st, what));
+  }
+  return NIM_OK;
+}
+
+// G passes of integrate_nse's loop body over the whole group: each part of
+// the pass on every slab, then the halos it changed; the merged maxima,
+// then every slab's k_iter_end (which therefore all decide alike)
+int slab_pass_graph(nim_ctx *const *X, int n, int G, cudaGraphExec_t *exec) {
+  cudaStream_t st = X[0]->stream;
+  CtlList L{};
+  L.n = n;
+  for (int s = 0; s < n; ++s) L.c[s] = X[s]->ctl;
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  int rc = NIM_OK;
+  for (int it = 0; it < G && rc == NIM_OK; ++it) {
+    for (int s = 0; s < n && rc == NIM_OK; ++s) rc = launch_vel(X[s], st, X[s]->g, X[s]->F);
+    if (rc == NIM_OK) rc = halo_exchange(X, n, st, kHaloV);
+    for (int s = 0; s < n && rc == NIM_OK; ++s) rc = launch_pressure(X[s], st, X[s]->g, X[s]->F);
+    if (rc == NIM_OK) rc = halo_exchange(X, n, st, kHaloP);
+    for (int s = 0; s < n && rc == NIM_OK; ++s) rc = launch_temperature(X[s], st, X[s]->g, X[s]->F);
+    if (rc == NIM_OK) rc = halo_exchange(X, n, st, kHaloT);
+    if (rc == NIM_OK) {
+      k_slab_merge<<<1, 32, 0, st>>>(L);
+      for (int s = 0; s < n; ++s) k_iter_end<<<1, 1, 0, st>>>(X[s]->ctl, X[s]->phys, 0);
+    }
+  }
+  const cudaError_t ce = cudaStreamEndCapture(st, &g);
+  if (rc == NIM_OK && ce != cudaSuccess) rc = NIM_ERR_CUDA;
+  if (rc == NIM_OK && cudaGraphInstantiate(exec, g, 0) != cudaSuccess) rc = NIM_ERR_CUDA;
+  if (g) cudaGraphDestroy(g);
+  return rc;
+}
+
+// the step-end reductions of the group: sums[0..n) the dilatation sums,
+// red[0..1] the merged dudt / dTdt maxima
+int slab_after_integrate(nim_ctx *const *X, int n, cudaStream_t st, double &dsum, double &dudt, double &dTdt) {
+  for (int s = 0; s < n; ++s) {
+    nim_ctx *x = X[s];
+    k_after_integrate<<<x->nblk_c, BLK, 0, st>>>(x->d, x->g, x->F, x->phys, x->ctl, x->nblk_c);
+    k_finish_sum<<<1, BLK, 0, st>>>(x->F.part, x->nblk_c, 1, x->sums);
+    CK(cudaGetLastError());
+    x->launches += 2;
+    CK(cudaMemcpyAsync(x->host_sums, x->sums, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(x->ctl_host, x->ctl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  dsum = dudt = dTdt = 0.;
+  for (int s = 0; s < n; ++s) {
+    dsum += X[s]->host_sums[0];
+    dudt = std::max(dudt, bits_to_double(X[s]->ctl_host->red[0]));
+    dTdt = std::max(dTdt, bits_to_double(X[s]->ctl_host->red[1]));
+  }
+  return NIM_OK;
+}
+
+// update_time_step + find_Nu2 on every slab; sums4 = the group's wall sums
+int slab_end(nim_ctx *const *X, int n, cudaStream_t st, double *sums4) {
+  for (int s = 0; s < n; ++s) {
+    nim_ctx *x = X[s];
+    const Dims &d = x->d;
+    const int gn = grid(2 * d.NT * d.NZ);
+    k_update_time<<<x->nblk_c, BLK, 0, st>>>(d, x->F, x->ctl);
+    k_nusselt<<<gn, BLK, 0, st>>>(d, x->g, x->F, x->ctl, gn);
+    k_finish_sum<<<1, BLK, 0, st>>>(x->F.part, gn, 4, x->sums);
+    CK(cudaGetLastError());
+    x->launches += 3;
+    CK(cudaMemcpyAsync(x->host_sums, x->sums, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  for (int q = 0; q < 4; ++q) sums4[q] = 0.;
+  for (int s = 0; s < n; ++s)
+    for (int q = 0; q < 4; ++q) sums4[q] += X[s]->host_sums[q];
+  return NIM_OK;
+}
+
+int slab_step_impl(nim_ctx *const *X, int n, int32_t nsteps, nim_step_stats *per, int32_t *done,
+                   cudaGraphExec_t exec) {
+  nim_ctx *x0 = X[0];
+  cudaStream_t st = x0->stream;
+  const int G = x0->graph_G;
+  int64_t owned = 0;
+  for (int s = 0; s < n; ++s) owned += (int64_t)(X[s]->d.kown1 - X[s]->d.kown0) * X[s]->d.plane;
+  int32_t k = 0;
+  int status = NIM_OK;
+  for (; k < nsteps; ++k) {
+    nim_step_stats rec;
+    std::memset(&rec, 0, sizeof(rec));
+    for (int s = 0; s < n; ++s) TRY(nim_gpu_begin_step(X[s]));
+    for (int s = 0; s < n; ++s) CK(cudaStreamSynchronize(X[s]->stream));
+    const long long cap = (x0->params.max_iters > 0) ? (long long)x0->params.max_iters + 2 * G : 100000000LL;
+    long long launched = 0;
+    bool capped = false;
+    for (;;) {
+      CK(cudaGraphLaunch(exec, st));
+      launched += G;
+      for (int s = 0; s < n; ++s) X[s]->launches += (long long)G * (X[s]->phys.dpdx_tolerance ? 12 : 11);
+      CK(cudaMemcpyAsync(x0->ctl_host, x0->ctl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (x0->ctl_host->done) break;
+      if (launched >= cap) {
+        capped = true;
+        break;
+      }
+    }
+    double dsum, dudt, dTdt;
+    TRY(slab_after_integrate(X, n, st, dsum, dudt, dTdt));
+    for (int s = 0; s < n; ++s) X[s]->last_iters = X[s]->ctl_host->step_iters;
+    if (capped && x0->ctl_host->status == NIM_OK) x0->ctl_host->status = NIM_ERR_NOT_CONVERGED;
+    fill_iter_stats(x0, &rec);
+    rec.dilatation = std::sqrt(dsum / (double)owned);
+    rec.dudt_max = dudt;
+    rec.dTdt_max = dTdt;
+    status = rec.status;
+    if (status != NIM_OK || steady_exit(x0, rec)) {
+      if (status == NIM_OK) rec.steady = 1;
+      for (int s = 0; s < n; ++s) X[s]->in_step = false;
+      if (per) per[k] = rec;
+      ++k;
+      break;
+    }
+    double sums[4];
+    TRY(slab_end(X, n, st, sums));
+    for (int s = 0; s < n; ++s) end_finish(X[s], nullptr);
+    rec.step = x0->STEP - 1;
+    rec.nu_outer = -(sums[0] / sums[1] * x0->params.R_o);
+    rec.nu_inner = -(sums[2] / sums[3] * x0->params.R_i);
+    rec.area_outer = sums[1];
+    rec.area_inner = sums[3];
+    rec.time = x0->TI;
+    if (per) per[k] = rec;
+  }
+  if (done) *done = k;
+  return status;
+}
+}  // namespace
+
+extern "C" int nim_slab_step(int32_t n, nim_ctx *const *X, int32_t nsteps, nim_step_stats *per, int32_t *done) {
+  if (n < 1 || n > kMaxSlabs || !X || nsteps < 0) return NIM_ERR_BAD_ARG;
+  for (int32_t s = 0; s < n; ++s) {
+    if (!X[s] || X[s]->slab_count != n || X[s]->slab_index != s || X[s]->device != X[0]->device ||
+        X[s]->graph_G != X[0]->graph_G)
+      return NIM_ERR_BAD_ARG;
+    if (!X[s]->initialized || X[s]->in_step) return NIM_ERR_STATE;
+    // slabs of one mesh: same cross-section, owned planes end to end
+    if (X[s]->d.NT != X[0]->d.NT || X[s]->d.NR != X[0]->d.NR) return NIM_ERR_BAD_ARG;
+    if (s > 0 && X[s]->slab_lo + X[s]->d.kown0 != X[s - 1]->slab_lo + X[s - 1]->d.kown1) return NIM_ERR_BAD_ARG;
+  }
+  CK(cudaSetDevice(X[0]->device));
+  for (int32_t s = 0; s < n; ++s) CK(cudaStreamSynchronize(X[s]->stream));
+  // every halo from its owner: after nim_gpu_init, uploads or a previous call
+  TRY(halo_exchange(X, n, X[0]->stream, kHaloAll));
+  CK(cudaStreamSynchronize(X[0]->stream));
+  cudaGraphExec_t exec = nullptr;
+  TRY(slab_pass_graph(X, n, X[0]->graph_G, &exec));
+  const int st = slab_step_impl(X, n, nsteps, per, done, exec);
+  cudaStreamSynchronize(X[0]->stream);
+  cudaGraphExecDestroy(exec);
+  return st;
 }
 
 extern "C" int nim_gpu_download(nim_ctx *x, nim_field f, double *host, int64_t n) {

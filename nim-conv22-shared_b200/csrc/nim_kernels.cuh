@@ -1171,7 +1171,8 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, GeoT<R> g, FieldsT<
       e[q] = errv(nw, cold, first);
     }
   }
-  if (!SRC_ONLY) block_max<3, CB3>(red, e, ctl->err[par]);
+  // blocks of one z plane: a plane another slab owns adds nothing
+  if (!SRC_ONLY && d.owns(blockIdx.z)) block_max<3, CB3>(red, e, ctl->err[par]);
 }
 
 // ---- K1, vectorised form (parallel schedule, formulation 2): k_vel_cell
@@ -1210,7 +1211,10 @@ __device__ __forceinline__ double tang_vals(bool lo, bool hi, double v0, double 
   return (vp1 - vm1) / 4.;
 }
 
-template <class R>
+// SLAB: a z-slab context, whose maxima skip the planes a neighbour owns (a
+// separate instantiation: at this kernel's register bound the test alone
+// costs spills)
+template <class R, bool SLAB = false>
 __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
@@ -1395,7 +1399,7 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
     *reinterpret_cast<typename Pair2<R>::T *>(F.c[q] + c) = out;
     e[q] = nmax(errv(nw0, cv0, first), errv(nw1, cv1, first));
   }
-  block_max<3, CB3>(red, e, ctl->err[par]);
+  if (!SLAB || d.owns(k)) block_max<3, CB3>(red, e, ctl->err[par]);
 }
 
 // ---- K2: +xi face updates of u, v, w (nse.f90:878-1005).
@@ -1430,7 +1434,7 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, GeoT<R> g, FieldsT<
       }
     });
   }
-  block_max<3, CB3>(red, e, ctl->err[par]);
+  if (d.owns(blockIdx.z)) block_max<3, CB3>(red, e, ctl->err[par]);
 }
 
 // ---- K2, z-marching form: the same face updates, one block per patch of
@@ -2041,7 +2045,7 @@ __global__ void __launch_bounds__(BLK) k_p_bc(Dims d, GeoT<R> g, FieldsT<R> F, P
     const BFace B = bface(d, b);
     const int fw0 = B.cell.face(d, B.pos);
     F.f[3][(1 - par) * NF + fw0] = nw;
-    e[0] = errv(nw, pr[fw0], first);
+    e[0] = d.owns(B.cell.k) ? errv(nw, pr[fw0], first) : 0.;
   }
   block_max<1>(red, e, ctl->err[par] + 3);
 }
@@ -2159,7 +2163,7 @@ __global__ void __launch_bounds__(CB3, 2) k_vel1_face(Dims d, GeoT<R> g, FieldsT
       }
     });
   }
-  block_max<3, CB3>(red, e, ctl->err[par]);
+  if (d.owns(blockIdx.z)) block_max<3, CB3>(red, e, ctl->err[par]);
 }
 
 // ---- K5: integrate_pressure_field_i, cur -> next.
@@ -2186,7 +2190,7 @@ __global__ void __launch_bounds__(CB3, 5) k_p_face(Dims d, GeoT<R> g, FieldsT<R>
       e[0] = errv(nw, pr[fo], first);
     });
   }
-  block_max<1, CB3>(red, e, ctl->err[par] + 3);
+  if (d.owns(blockIdx.z)) block_max<1, CB3>(red, e, ctl->err[par] + 3);
 }
 
 // ---- K5b (is_dpdx_tolerance): cell pressure gradients (nse.f90:292-307)
@@ -2208,7 +2212,7 @@ __global__ void __launch_bounds__(BLK) k_p_dpdx(Dims d, GeoT<R> g, FieldsT<R> F,
                          stored<R>((p[f[4]] - p[f[3]]) / 2. * g.xi[4 * Nc + c]),
                          stored<R>((p[f[6]] - p[f[5]]) / 2. * g.xi[8 * Nc + c])};
     for (int q = 0; q < 3; ++q) {
-      e[0] = nmax(e[0], fabs(v[q] - F.dpd[q * Nc + c]));
+      if (d.owns(x.k)) e[0] = nmax(e[0], fabs(v[q] - F.dpd[q * Nc + c]));
       F.dpd[q * Nc + c] = v[q];
     }
   }
@@ -2234,7 +2238,7 @@ __global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, GeoT<R> g, FieldsT<R>
     const int f1 = B.cell.face(d, B.pos);
     const double nw = stored<R>((+g.zf[NB + b] * T[B.cell.face(d, in)] - g.zf[2 * NB + b] * T[c2.face(d, in)] +
                                  g.zf[3 * NB + b] * T[c3.face(d, in)]) / g.zf[b]);
-    e[0] = errv(nw, T[f1], first);
+    e[0] = d.owns(B.cell.k) ? errv(nw, T[f1], first) : 0.;
     T[f1] = nw;
   }
   block_max<1>(red, e, ctl->err[par] + 4);
@@ -2348,7 +2352,7 @@ __global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, GeoT<R> g, FieldsT<R>
       e[0] = errv(nw, cold, first);
     }
   }
-  if (!SRC_ONLY) block_max<1, CB3>(red, e, ctl->err[par] + 4);
+  if (!SRC_ONLY && d.owns(blockIdx.z)) block_max<1, CB3>(red, e, ctl->err[par] + 4);
 }
 
 // ---- K8: +xi face updates of T (nse.f90:1033-1088), cur -> next; the z-wall
@@ -2382,7 +2386,7 @@ __global__ void __launch_bounds__(BLK, 4) k_T_face(Dims d, GeoT<R> g, FieldsT<R>
     if (x.k == 0) Tn[x.face(d, 5)] = T[x.face(d, 5)];
     if (x.k == d.NZ - 1) Tn[x.face(d, 6)] = T[x.face(d, 6)];
   }
-  block_max<1>(red, e, ctl->err[par] + 4);
+  if (d.owns(blockIdx.z)) block_max<1>(red, e, ctl->err[par] + 4);
 }
 
 // ---- K9: end of one pass (find_error's maxima, the do-while test of
@@ -2694,6 +2698,7 @@ __global__ void __launch_bounds__(BLK) k_after_integrate(Dims d, Geo g, Fields F
                         green_gauss(g, NF, invV, wf, f, 2);
     F.dila[c] = Dila;
     s[0] = Dila * Dila;
+    if (!d.owns(x.k)) m[0] = m[1] = s[0] = 0.;
   }
   block_max<2>(red, m, ctl->red);
   block_sum<1>(s, F.part, nblk);
@@ -2760,6 +2765,7 @@ __global__ void __launch_bounds__(BLK) k_nusselt(Dims d, Geo g, Fields F, Ctrl *
       s[0] = A * dTdx;
       s[1] = A;
     }
+    if (!d.owns(B.cell.k)) s[0] = s[1] = s[2] = s[3] = 0.;
   }
   block_sum<4>(s, F.part, nblk);
 }

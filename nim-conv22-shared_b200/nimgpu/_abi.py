@@ -163,6 +163,16 @@ def gpu_lib() -> C.CDLL:
         lib.nim_batch_step.argtypes = [C.c_int32, C.POINTER(vp), C.c_int32, C.POINTER(StepStats),
                                        C.POINTER(C.c_int32)]
         lib.nim_batch_step.restype = C.c_int
+        lib.nim_slab_layout.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]
+        lib.nim_slab_layout.restype = C.c_int
+        lib.nim_slab_halo.argtypes = [C.c_int32] * 6 + [C.POINTER(C.c_int64)] * 2
+        lib.nim_slab_halo.restype = C.c_int
+        lib.nim_gpu_create_slab.argtypes = [C.POINTER(MeshDesc), C.POINTER(Params), C.c_int32, C.c_int32,
+                                            C.POINTER(vp)]
+        lib.nim_gpu_create_slab.restype = C.c_int
+        lib.nim_slab_step.argtypes = [C.c_int32, C.POINTER(vp), C.c_int32, C.POINTER(StepStats),
+                                      C.POINTER(C.c_int32)]
+        lib.nim_slab_step.restype = C.c_int
         lib.nim_gpu_output_bytes.argtypes = [vp, C.c_int32]
         lib.nim_gpu_output_bytes.restype = C.c_int64
         lib.nim_gpu_output_begin.argtypes = [vp, C.c_int32, vp, C.c_int64, C.POINTER(C.c_int32)]
