@@ -310,6 +310,48 @@ int nim_gpu_create_slab(const nim_mesh_desc *mesh, const nim_params *params, int
    order differs).  per (may be NULL) receives nsteps group records. */
 int nim_slab_step(int32_t n, nim_ctx *const *ctx, int32_t nsteps, nim_step_stats *per, int32_t *done);
 
+/* ---- the pieces of nim_slab_step for a host that moves the halos itself
+   (one process per GPU, each with one slab context).  Per step:
+   nim_gpu_begin_step; per pass: part 0, exchange of set 1, part 1,
+   exchange of set 2, part 2, exchange of set 4, max-reduction of the 24
+   words at nim_slab_maxima over all slabs, part 3; every few passes
+   nim_slab_loop_state until done; then nim_slab_after_loop (reduce: sum,
+   max, max) and, unless the step stops there, nim_slab_end_step (reduce:
+   sums).  Before the first step, and after any upload, exchange set 8.
+   Everything is queued on the context's stream (nim_gpu_stream); the
+   host's transport must be ordered on it too.
+
+   nim_slab_part: part 0 velocity (update_velocity_sources +
+   integrate_velocity_field), 1 pressure, 2 temperature, 3 the pass end
+   (find_error's test on the merged maxima). */
+int nim_slab_part(nim_ctx *ctx, int32_t part);
+
+/* Device arrays an exchange of set (bits: 1 velocity, 2 pressure, 4
+   temperature, 8 the whole state) carries, in a fixed order: ptr[i] and
+   face[i] (0: a cell array of the context's cells, exchanged over span 0 of
+   nim_slab_halo; 1: a face array of 2 x faces doubles, spans 1..3 in each
+   half).  Returns the count (at most 32), or NIM_ERR_BAD_ARG when cap is
+   too small. */
+int nim_slab_arrays(nim_ctx *ctx, int32_t set, void **ptr, int32_t *face, int32_t cap);
+
+/* Device address of the 24 uint64 words (bit patterns of non-negative
+   doubles) every slab must replace by their maximum over all slabs before
+   part 3: find_error's accumulators and the Dirichlet wall floor. */
+int nim_slab_maxima(nim_ctx *ctx, void **slots24);
+
+/* After the context's stream drains: state3 = {done, passes this step,
+   status}; err5 (may be NULL) = the last pass's maxima of u, v, w, p, T. */
+int nim_slab_loop_state(nim_ctx *ctx, int32_t *state3, double *err5);
+
+/* check_steady_state + evaluate_D over the owned planes: out3 = {sum of
+   squared dilatation, max dudt, max dTdt}. */
+int nim_slab_after_loop(nim_ctx *ctx, double *out3);
+
+/* update_time_step + find_Nu2 over the owned planes: out4 = {outer wall
+   sum of area x dT/dn, outer area, inner sum, inner area}; advances the
+   step counter and time. */
+int nim_slab_end_step(nim_ctx *ctx, double *out4);
+
 /* Copy a field to/from host memory in the reference layout (for
    write_data / write_restart / read_restart, postprocess.f90, restart.f90).
    n = number of doubles the host buffer holds. */

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -1533,43 +1534,58 @@ __global__ void k_slab_merge(CtlList L) {
 // temperature parts of a pass, or the whole state
 enum { kHaloV = 1, kHaloP = 2, kHaloT = 4, kHaloAll = 8 };
 
+// The device arrays an exchange of `what` carries, in a fixed order: each
+// a cell array (Nc doubles) or a face array (both halves, 2*NF doubles).
+struct HaloArray {
+  double *p;
+  bool face;
+};
+void halo_arrays(const nim_ctx *x, int what, std::vector<HaloArray> &out) {
+  const Fields &F = x->F;
+  const bool all = (what & kHaloAll) != 0;
+  out.clear();
+  if (all || (what & kHaloV))
+    for (int q = 0; q < 3; ++q) {
+      out.push_back({F.c[q], false});
+      out.push_back({F.f[q], true});
+    }
+  if (all || (what & kHaloP)) out.push_back({F.f[3], true});
+  if (all || (what & kHaloT)) {
+    out.push_back({F.c[3], false});
+    out.push_back({F.f[4], true});
+  }
+  if (all) {
+    for (int q = 0; q < 4; ++q) {
+      out.push_back({F.co[q], false});
+      out.push_back({F.ct[q], false});
+    }
+    out.push_back({F.mp, false});
+    out.push_back({F.dila, false});
+    out.push_back({F.dila_old, false});
+    for (int q = 0; q < 3; ++q) out.push_back({F.dpd + (size_t)q * x->d.Nc, false});
+  }
+}
+
 // src's owned planes next to dst into dst's halo: each cell array over span
 // 0, each face array (both halves) over the r, theta and z spans 1..3
 int copy_halo(const nim_ctx *src, const int64_t *snd, const nim_ctx *dst, const int64_t *rcv, cudaStream_t st,
               int what) {
-  const Fields &A = src->F, &B = dst->F;
-  std::vector<std::pair<const double *, double *>> cells, faces;
-  const bool all = (what & kHaloAll) != 0;
-  if (all || (what & kHaloV))
-    for (int q = 0; q < 3; ++q) {
-      cells.emplace_back(A.c[q], B.c[q]);
-      faces.emplace_back(A.f[q], B.f[q]);
-    }
-  if (all || (what & kHaloP)) faces.emplace_back(A.f[3], B.f[3]);
-  if (all || (what & kHaloT)) {
-    cells.emplace_back(A.c[3], B.c[3]);
-    faces.emplace_back(A.f[4], B.f[4]);
-  }
-  if (all) {
-    for (int q = 0; q < 4; ++q) {
-      cells.emplace_back(A.co[q], B.co[q]);
-      cells.emplace_back(A.ct[q], B.ct[q]);
-    }
-    cells.emplace_back(A.mp, B.mp);
-    cells.emplace_back(A.dila, B.dila);
-    cells.emplace_back(A.dila_old, B.dila_old);
-    for (int q = 0; q < 3; ++q) cells.emplace_back(A.dpd + (size_t)q * src->d.Nc, B.dpd + (size_t)q * dst->d.Nc);
-  }
   for (int t = 0; t < 4; ++t)
     if (snd[2 * t + 1] != rcv[2 * t + 1]) return NIM_ERR_BAD_ARG;
-  for (auto &c : cells)
-    CK(cudaMemcpyAsync(c.second + rcv[0], c.first + snd[0], sizeof(double) * snd[1], cudaMemcpyDeviceToDevice, st));
+  std::vector<HaloArray> A, B;
+  halo_arrays(src, what, A);
+  halo_arrays(dst, what, B);
   const size_t NFa = src->d.NF, NFb = dst->d.NF;
-  for (auto &f : faces)
+  for (size_t a = 0; a < A.size(); ++a) {
+    if (!A[a].face) {
+      CK(cudaMemcpyAsync(B[a].p + rcv[0], A[a].p + snd[0], sizeof(double) * snd[1], cudaMemcpyDeviceToDevice, st));
+      continue;
+    }
     for (int h = 0; h < 2; ++h)
       for (int t = 1; t < 4; ++t)
-        CK(cudaMemcpyAsync(f.second + h * NFb + rcv[2 * t], f.first + h * NFa + snd[2 * t],
+        CK(cudaMemcpyAsync(B[a].p + h * NFb + rcv[2 * t], A[a].p + h * NFa + snd[2 * t],
                            sizeof(double) * snd[2 * t + 1], cudaMemcpyDeviceToDevice, st));
+  }
   return NIM_OK;
 }
 
@@ -1736,6 +1752,75 @@ extern "C" int nim_slab_step(int32_t n, nim_ctx *const *X, int32_t nsteps, nim_s
   cudaStreamSynchronize(X[0]->stream);
   cudaGraphExecDestroy(exec);
   return st;
+}
+
+// ---- the pieces of a pass for a host that moves the halos itself (one
+// process per GPU: the exchange and the maxima reduction over its own
+// transport, on the context's stream, between the parts)
+extern "C" int nim_slab_part(nim_ctx *x, int32_t part) {
+  if (!x || part < 0 || part > 3) return NIM_ERR_BAD_ARG;
+  if (!x->initialized || !x->in_step) return NIM_ERR_STATE;
+  if (x->seq || x->mixed) return NIM_ERR_BAD_ARG;
+  CK(cudaSetDevice(x->device));
+  cudaStream_t s = x->stream;
+  switch (part) {
+    case 0: TRY(launch_vel(x, s, x->g, x->F)); break;
+    case 1: TRY(launch_pressure(x, s, x->g, x->F)); break;
+    case 2: TRY(launch_temperature(x, s, x->g, x->F)); break;
+    default: k_iter_end<<<1, 1, 0, s>>>(x->ctl, x->phys, 0);
+  }
+  CK(cudaGetLastError());
+  x->launches += (part == 3) ? 1 : 4;
+  return NIM_OK;
+}
+
+extern "C" int nim_slab_arrays(nim_ctx *x, int32_t set, void **ptr, int32_t *face, int32_t cap) {
+  if (!x || !ptr || !face || set < 1 || set > 15 || cap < 0) return NIM_ERR_BAD_ARG;
+  std::vector<HaloArray> v;
+  halo_arrays(x, set, v);
+  if ((int)v.size() > cap) return NIM_ERR_BAD_ARG;
+  for (size_t i = 0; i < v.size(); ++i) {
+    ptr[i] = v[i].p;
+    face[i] = v[i].face ? 1 : 0;
+  }
+  return (int)v.size();
+}
+
+extern "C" int nim_slab_maxima(nim_ctx *x, void **slots24) {
+  if (!x || !slots24) return NIM_ERR_BAD_ARG;
+  *slots24 = reinterpret_cast<char *>(x->ctl) + offsetof(Ctrl, err);
+  return NIM_OK;
+}
+
+extern "C" int nim_slab_loop_state(nim_ctx *x, int32_t *state3, double *err5) {
+  if (!x || !state3) return NIM_ERR_BAD_ARG;
+  CK(cudaSetDevice(x->device));
+  TRY(read_ctrl(x));
+  const Ctrl &c = *x->ctl_host;
+  state3[0] = c.done;
+  state3[1] = c.step_iters;
+  state3[2] = c.status;
+  if (err5)
+    for (int q = 0; q < 5; ++q) err5[q] = c.last_err[q];
+  return NIM_OK;
+}
+
+extern "C" int nim_slab_after_loop(nim_ctx *x, double *out3) {
+  if (!x || !out3) return NIM_ERR_BAD_ARG;
+  if (!x->initialized || !x->in_step) return NIM_ERR_STATE;
+  CK(cudaSetDevice(x->device));
+  TRY(slab_after_integrate(&x, 1, x->stream, out3[0], out3[1], out3[2]));
+  x->last_iters = x->ctl_host->step_iters;
+  return NIM_OK;
+}
+
+extern "C" int nim_slab_end_step(nim_ctx *x, double *out4) {
+  if (!x || !out4) return NIM_ERR_BAD_ARG;
+  if (!x->initialized || !x->in_step) return NIM_ERR_STATE;
+  CK(cudaSetDevice(x->device));
+  TRY(slab_end(&x, 1, x->stream, out4));
+  end_finish(x, nullptr);
+  return NIM_OK;
 }
 
 extern "C" int nim_gpu_download(nim_ctx *x, nim_field f, double *host, int64_t n) {

@@ -102,6 +102,9 @@ struct Phys {
 // iteration, the host reads it between batches.
 struct Ctrl {
   unsigned long long err[2][8];  // max-accumulators per parity: u,v,w,p,T,dpdx
+  unsigned long long wall_floor[8];  // max |Dirichlet wall value| bits (find_error
+                                     // compares with zero-initialised arrays once);
+                                     // with err: the 24 words z-slabs max-reduce
   int iter;         // iterations since init (parity source)
   int step_iters;   // iterations of the current step (cnt)
   int done;         // 1: current step's inner loop has stopped
@@ -111,8 +114,6 @@ struct Ctrl {
                     // schedule); 0: one half, updated in place (reference order)
   int pad[2];
   double last_err[5];
-  unsigned long long wall_floor[8];  // max |Dirichlet wall value| bits (find_error
-                                     // compares with zero-initialised arrays once)
   unsigned long long red[4];  // dudt, dTdt maxima (after integrate)
   double dilatation, nu_outer, nu_inner, area_outer, area_inner;
   // FP32 phase of a mixed-precision step: passes run, the smallest maximum

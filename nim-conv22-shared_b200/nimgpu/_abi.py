@@ -173,6 +173,18 @@ def gpu_lib() -> C.CDLL:
         lib.nim_slab_step.argtypes = [C.c_int32, C.POINTER(vp), C.c_int32, C.POINTER(StepStats),
                                       C.POINTER(C.c_int32)]
         lib.nim_slab_step.restype = C.c_int
+        lib.nim_slab_part.argtypes = [vp, C.c_int32]
+        lib.nim_slab_part.restype = C.c_int
+        lib.nim_slab_arrays.argtypes = [vp, C.c_int32, C.POINTER(vp), C.POINTER(C.c_int32), C.c_int32]
+        lib.nim_slab_arrays.restype = C.c_int
+        lib.nim_slab_maxima.argtypes = [vp, C.POINTER(vp)]
+        lib.nim_slab_maxima.restype = C.c_int
+        lib.nim_slab_loop_state.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+        lib.nim_slab_loop_state.restype = C.c_int
+        lib.nim_slab_after_loop.argtypes = [vp, C.POINTER(C.c_double)]
+        lib.nim_slab_after_loop.restype = C.c_int
+        lib.nim_slab_end_step.argtypes = [vp, C.POINTER(C.c_double)]
+        lib.nim_slab_end_step.restype = C.c_int
         lib.nim_gpu_output_bytes.argtypes = [vp, C.c_int32]
         lib.nim_gpu_output_bytes.restype = C.c_int64
         lib.nim_gpu_output_begin.argtypes = [vp, C.c_int32, vp, C.c_int64, C.POINTER(C.c_int32)]

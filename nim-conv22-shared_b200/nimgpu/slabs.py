@@ -12,6 +12,7 @@ the slabs and gather their owned planes back.
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import numpy as np
 
@@ -77,19 +78,20 @@ def slab_face_planes(mesh: Mesh, lo: int, hi: int):
     return glob, plane
 
 
-class SlabGroup:
-    """nslab z-slab contexts of one mesh on the current device, advanced
-    together (nim_slab_step).  Without the CUDA library or a GPU the
-    constructor raises."""
+class _Slabs:
+    """Slab contexts of one mesh held by this process (slab numbers in
+    `slabs`), with the host copies between the whole mesh's reference
+    layout and the slabs' structured layout."""
 
-    def __init__(self, mesh: Mesh, params: _abi.Params, nslab: int):
+    def __init__(self, mesh: Mesh, params: _abi.Params, nslab: int, slabs):
         self.lib = _abi.gpu_lib()
         self.mesh, self.params, self.nslab = mesh, params, nslab
-        self.layout = [slab_layout(mesh.n_z, nslab, s) for s in range(nslab)]
+        self.slabs = list(slabs)
+        self.layout = {s: slab_layout(mesh.n_z, nslab, s) for s in self.slabs}
         self._ref = structured_faces(mesh)
         self._h = []
         try:
-            for s in range(nslab):
+            for s in self.slabs:
                 h = C.c_void_p()
                 _abi.check(self.lib.nim_gpu_create_slab(C.byref(mesh.desc), C.byref(params), nslab, s, C.byref(h)),
                            "nim_gpu_create_slab")
@@ -97,6 +99,9 @@ class SlabGroup:
         except Exception:
             self.close()
             raise
+
+    def _handle(self, s: int):
+        return self._h[self.slabs.index(s)]
 
     # -- lifetime
     def close(self):
@@ -117,10 +122,85 @@ class SlabGroup:
         except Exception:
             pass
 
-    # -- the reference's call sites
     def initialize_nse(self):
         for h in self._h:
             _abi.check(self.lib.nim_gpu_init(h), "nim_gpu_init")
+
+    def set_graph_iters(self, n: int):
+        for h in self._h:
+            _abi.check(self.lib.nim_gpu_set_graph_iters(h, n), "nim_gpu_set_graph_iters")
+
+    # -- host copies in a slab's structured layout
+    def _sizes(self, s: int):
+        lo, hi = self.layout[s][:2]
+        return slab_sizes(self.mesh.n_theta, self.mesh.n_r, hi - lo)
+
+    def download(self, s: int, field: int) -> np.ndarray:
+        nc, nf = self._sizes(s)
+        out = np.empty(nf if field <= _abi.FACES_T else nc, dtype=np.float64)
+        _abi.check(self.lib.nim_gpu_download(self._handle(s), field, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                             out.size), "nim_gpu_download")
+        return out
+
+    def upload(self, s: int, field: int, values: np.ndarray):
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        _abi.check(self.lib.nim_gpu_upload(self._handle(s), field, a.ctypes.data_as(C.POINTER(C.c_double)), a.size),
+                   "nim_gpu_upload")
+
+    # -- whole-mesh arrays (reference layout) to and from the slabs
+    def scatter(self, field: int, values: np.ndarray):
+        """Upload the held part of a whole-mesh field to every slab here."""
+        pl = self.mesh.n_theta * self.mesh.n_r
+        for s in self.slabs:
+            lo, hi = self.layout[s][:2]
+            if field <= _abi.FACES_T:
+                glob, _ = slab_face_planes(self.mesh, lo, hi)
+                self.upload(s, field, values[self._ref[glob]])
+            else:
+                self.upload(s, field, values[lo * pl:hi * pl])
+
+    def gather(self, field: int) -> np.ndarray:
+        """A whole-mesh field in the reference layout from the owned planes
+        of the slabs here (NaN where another process's slab owns it)."""
+        m = self.mesh
+        pl = m.n_theta * m.n_r
+        if field > _abi.FACES_T:
+            out = np.full(m.nmesh, np.nan, dtype=np.float64)
+            for s in self.slabs:
+                lo, _, olo, ohi = self.layout[s]
+                out[olo * pl:ohi * pl] = self.download(s, field)[(olo - lo) * pl:(ohi - lo) * pl]
+            return out
+        out = np.full(m.nface, np.nan, dtype=np.float64)
+        for s in self.slabs:
+            lo, hi, olo, ohi = self.layout[s]
+            glob, plane = slab_face_planes(m, lo, hi)
+            top = ohi + (1 if s == self.nslab - 1 else 0)
+            keep = (plane >= olo) & (plane < top)
+            out[self._ref[glob[keep]]] = self.download(s, field)[keep]
+        return out
+
+    def add_temperature_noise(self, amp: float, seed: int):
+        """nimgpu.apply_temperature_noise for slabs: the whole mesh's seeded
+        noise added to every slab's held planes."""
+        if amp == 0.0:
+            return
+        cells, faces = temperature_noise(self.mesh, amp, seed)
+        pl = self.mesh.n_theta * self.mesh.n_r
+        for s in self.slabs:
+            lo, hi = self.layout[s][:2]
+            glob, _ = slab_face_planes(self.mesh, lo, hi)
+            self.upload(s, _abi.FACES_T, self.download(s, _abi.FACES_T) + faces[self._ref[glob]])
+            for fld in (_abi.MESHES_T, _abi.MESHES_T_OLD, _abi.MESHES_TT):
+                self.upload(s, fld, self.download(s, fld) + cells[lo * pl:hi * pl])
+
+
+class SlabGroup(_Slabs):
+    """All nslab z-slab contexts of one mesh on the current device, advanced
+    together (nim_slab_step).  Without the CUDA library or a GPU the
+    constructor raises."""
+
+    def __init__(self, mesh: Mesh, params: _abi.Params, nslab: int):
+        super().__init__(mesh, params, nslab, range(nslab))
 
     def solve_nse(self, nsteps: int, raise_on_error: bool = True):
         """nsteps of the time loop over the group; returns the group's
@@ -134,65 +214,165 @@ class SlabGroup:
             _abi.check(st, "nim_slab_step")
         return [per[k] for k in range(done.value)]
 
-    def set_graph_iters(self, n: int):
-        for h in self._h:
-            _abi.check(self.lib.nim_gpu_set_graph_iters(h, n), "nim_gpu_set_graph_iters")
 
-    # -- host copies in the slab's structured layout
-    def _sizes(self, s: int):
-        lo, hi = self.layout[s][:2]
-        return slab_sizes(self.mesh.n_theta, self.mesh.n_r, hi - lo)
+# exchange sets of nim_slab_arrays
+HALO_VELOCITY, HALO_PRESSURE, HALO_TEMPERATURE, HALO_STATE = 1, 2, 4, 8
 
-    def download(self, s: int, field: int) -> np.ndarray:
-        nc, nf = self._sizes(s)
-        out = np.empty(nf if field <= _abi.FACES_T else nc, dtype=np.float64)
-        _abi.check(self.lib.nim_gpu_download(self._h[s], field, out.ctypes.data_as(C.POINTER(C.c_double)), out.size),
-                   "nim_gpu_download")
-        return out
 
-    def upload(self, s: int, field: int, values: np.ndarray):
-        a = np.ascontiguousarray(values, dtype=np.float64)
-        _abi.check(self.lib.nim_gpu_upload(self._h[s], field, a.ctypes.data_as(C.POINTER(C.c_double)), a.size),
-                   "nim_gpu_upload")
+def halo_views(arrays, nf: int, plans: dict, rank: int):
+    """The transfers of one halo exchange of slab `rank`: per neighbour,
+    (peer rank, views to send, views to receive into), in one order both
+    sides generate alike.  arrays: (1-D tensor or array, is_face) pairs as
+    nim_slab_arrays lists them (face arrays hold both halves, 2*nf);
+    plans: {side: (recv spans, send spans)} of slab_halo."""
+    out = []
+    for side in (0, 1):
+        if side not in plans:
+            continue
+        recv, send = plans[side]
+        sv, rv = [], []
+        for a, face in arrays:
+            spans = [(h * nf, t) for h in (0, 1) for t in (1, 2, 3)] if face else [(0, 0)]
+            for base, t in spans:
+                (so, sn), (ro, rn) = send[t], recv[t]
+                if sn != rn:
+                    raise ValueError("exchange plans of neighbour slabs disagree")
+                sv.append(a[base + so:base + so + sn])
+                rv.append(a[base + ro:base + ro + rn])
+        out.append((rank - 1 if side == 0 else rank + 1, sv, rv))
+    return out
 
-    # -- whole-mesh arrays (reference layout) to and from the slabs
-    def scatter(self, field: int, values: np.ndarray):
-        """Upload the held part of a whole-mesh field to every slab."""
-        pl = self.mesh.n_theta * self.mesh.n_r
-        for s, (lo, hi, _, _) in enumerate(self.layout):
-            if field <= _abi.FACES_T:
-                glob, _ = slab_face_planes(self.mesh, lo, hi)
-                self.upload(s, field, values[self._ref[glob]])
-            else:
-                self.upload(s, field, values[lo * pl:hi * pl])
 
-    def gather(self, field: int) -> np.ndarray:
-        """A whole-mesh field in the reference layout from the slabs' owned
-        planes."""
-        m = self.mesh
-        pl = m.n_theta * m.n_r
-        if field > _abi.FACES_T:
-            out = np.empty(m.nmesh, dtype=np.float64)
-            for s, (lo, _, olo, ohi) in enumerate(self.layout):
-                out[olo * pl:ohi * pl] = self.download(s, field)[(olo - lo) * pl:(ohi - lo) * pl]
-            return out
-        out = np.full(m.nface, np.nan, dtype=np.float64)
-        for s, (lo, hi, olo, ohi) in enumerate(self.layout):
-            glob, plane = slab_face_planes(m, lo, hi)
-            top = ohi + (1 if s == self.nslab - 1 else 0)
-            keep = (plane >= olo) & (plane < top)
-            out[self._ref[glob[keep]]] = self.download(s, field)[keep]
-        return out
+def exchange_halos(arrays, nf: int, plans: dict, rank: int, group=None):
+    """One halo exchange over torch.distributed point-to-point operations
+    (NCCL for device tensors, ordered on the current CUDA stream; gloo for
+    host tensors): slab `rank` sends its planes next to each neighbour and
+    receives that neighbour's into its halo."""
+    import torch.distributed as dist
+    ops = []
+    for peer, sv, rv in halo_views(arrays, nf, plans, rank):
+        ops += [dist.P2POp(dist.isend, t, peer, group) for t in sv]
+        ops += [dist.P2POp(dist.irecv, t, peer, group) for t in rv]
+    if ops:
+        for w in dist.batch_isend_irecv(ops):
+            w.wait()
 
-    def add_temperature_noise(self, amp: float, seed: int):
-        """nimgpu.apply_temperature_noise for the group: the whole mesh's
-        seeded noise added to every slab's held planes."""
-        if amp == 0.0:
-            return
-        cells, faces = temperature_noise(self.mesh, amp, seed)
-        pl = self.mesh.n_theta * self.mesh.n_r
-        for s, (lo, hi, _, _) in enumerate(self.layout):
-            glob, _ = slab_face_planes(self.mesh, lo, hi)
-            self.upload(s, _abi.FACES_T, self.download(s, _abi.FACES_T) + faces[self._ref[glob]])
-            for fld in (_abi.MESHES_T, _abi.MESHES_T_OLD, _abi.MESHES_TT):
-                self.upload(s, fld, self.download(s, fld) + cells[lo * pl:hi * pl])
+
+def _device_tensor(ptr: int, n: int, typestr: str, device):
+    """A torch tensor over n elements of device memory the library owns."""
+    import torch
+
+    class _View:
+        pass
+
+    v = _View()
+    v.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (int(ptr), False),
+                                  "strides": None, "version": 3}
+    return torch.as_tensor(v, device=device)
+
+
+class SlabRank(_Slabs):
+    """This process's slab of a mesh split over the ranks of a
+    torch.distributed group, one GPU per rank (rank r holds slab r, bottom to
+    top).  solve_nse drives the pieces of nim_slab_step: each part of a pass
+    on the context's stream, then the halo exchange over the group
+    (exchange_halos), the maxima's all-reduce before every pass end, and the
+    step-end sums reduced over the group."""
+
+    def __init__(self, mesh: Mesh, params: _abi.Params, group=None):
+        import torch
+        import torch.distributed as dist
+        self._dist, self._group = dist, group
+        self.rank, self.world = dist.get_rank(group), dist.get_world_size(group)
+        super().__init__(mesh, params, self.world, [self.rank])
+        h = self._h[0]
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self.stream = torch.cuda.ExternalStream(int(self.lib.nim_gpu_stream(h)), device=self.device)
+        self.plans = {}
+        if self.rank > 0:
+            self.plans[0] = slab_halo(mesh.n_theta, mesh.n_r, mesh.n_z, self.world, self.rank, 0)
+        if self.rank < self.world - 1:
+            self.plans[1] = slab_halo(mesh.n_theta, mesh.n_r, mesh.n_z, self.world, self.rank, 1)
+        nc, self._nf = self._sizes(self.rank)
+        self._arrays = {}
+        for st in (HALO_VELOCITY, HALO_PRESSURE, HALO_TEMPERATURE, HALO_STATE):
+            ptr, face = (C.c_void_p * 32)(), (C.c_int32 * 32)()
+            n = self.lib.nim_slab_arrays(h, st, ptr, face, 32)
+            if n < 0:
+                _abi.check(n, "nim_slab_arrays")
+            self._arrays[st] = [(_device_tensor(ptr[i], 2 * self._nf if face[i] else nc, "<f8", self.device),
+                                 bool(face[i])) for i in range(n)]
+        slots = C.c_void_p()
+        _abi.check(self.lib.nim_slab_maxima(h, C.byref(slots)), "nim_slab_maxima")
+        self._maxima = _device_tensor(slots.value, 24, "<i8", self.device)
+        self._step, self._time = 1, params.DT
+
+    def close(self):
+        self._arrays, self._maxima = {}, None
+        super().close()
+
+    def _exchange(self, what: int):
+        import torch
+        if self.world > 1:
+            with torch.cuda.stream(self.stream):
+                exchange_halos(self._arrays[what], self._nf, self.plans, self.rank, self._group)
+
+    def _merge(self):
+        import torch
+        with torch.cuda.stream(self.stream):
+            self._dist.all_reduce(self._maxima, op=self._dist.ReduceOp.MAX, group=self._group)
+
+    def _reduce(self, values, op):
+        import torch
+        t = torch.tensor(values, dtype=torch.float64, device=self.device)
+        self._dist.all_reduce(t, op=op, group=self._group)
+        return t.tolist()
+
+    def initialize_nse(self):
+        super().initialize_nse()
+        self._step, self._time = 1, self.params.DT
+
+    def solve_nse(self, nsteps: int, passes_per_check: int = 4, raise_on_error: bool = True):
+        """nsteps of the time loop; every rank returns the same records."""
+        lib, h, R = self.lib, self._h[0], self._dist.ReduceOp
+        recs = []
+        self._exchange(HALO_STATE)
+        for _ in range(nsteps):
+            _abi.check(lib.nim_gpu_begin_step(h), "nim_gpu_begin_step")
+            state, err = (C.c_int32 * 3)(), (C.c_double * 5)()
+            while True:
+                for _ in range(passes_per_check):
+                    for part, what in ((0, HALO_VELOCITY), (1, HALO_PRESSURE), (2, HALO_TEMPERATURE)):
+                        _abi.check(lib.nim_slab_part(h, part), "nim_slab_part")
+                        self._exchange(what)
+                    self._merge()
+                    _abi.check(lib.nim_slab_part(h, 3), "nim_slab_part")
+                _abi.check(lib.nim_slab_loop_state(h, state, err), "nim_slab_loop_state")
+                if state[0]:
+                    break
+            a3 = (C.c_double * 3)()
+            _abi.check(lib.nim_slab_after_loop(h, a3), "nim_slab_after_loop")
+            (dsum,) = self._reduce([a3[0]], R.SUM)
+            dudt, dTdt = self._reduce([a3[1], a3[2]], R.MAX)
+            r = _abi.StepStats()
+            r.step, r.iters, r.status = self._step, state[1], state[2]
+            r.err_u, r.err_v, r.err_w, r.err_p, r.err_T = err
+            r.dilatation = math.sqrt(dsum / self.mesh.nmesh)
+            r.dudt_max, r.dTdt_max = dudt, dTdt
+            p = self.params
+            if r.status != _abi.NIM_OK or (p.check_steady and dudt < p.dudt_epsilon and dTdt < p.dudt_epsilon):
+                r.steady = int(r.status == _abi.NIM_OK)
+                recs.append(r)
+                break
+            s4 = (C.c_double * 4)()
+            _abi.check(lib.nim_slab_end_step(h, s4), "nim_slab_end_step")
+            sum1, sumA1, sum2, sumA2 = self._reduce(list(s4), R.SUM)
+            self._time = self._time + 2 * p.DT
+            r.nu_outer = -(sum1 / sumA1 * p.R_o)
+            r.nu_inner = -(sum2 / sumA2 * p.R_i)
+            r.area_outer, r.area_inner, r.time = sumA1, sumA2, self._time
+            self._step += 1
+            recs.append(r)
+        if raise_on_error and recs and recs[-1].status != _abi.NIM_OK:
+            _abi.check(recs[-1].status, "SlabRank.solve_nse")
+        return recs

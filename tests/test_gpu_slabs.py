@@ -70,3 +70,39 @@ def test_slab_group_checks_its_members():
         assert lib.nim_slab_step(2, wrong, 1, None, None) == _abi.NIM_ERR_BAD_ARG
         swapped = (C.c_void_p * n)(g._h[1].value, g._h[0].value, g._h[2].value)
         assert lib.nim_slab_step(n, swapped, 1, None, None) == _abi.NIM_ERR_BAD_ARG
+
+
+def test_slab_rank_single_process_equals_whole_mesh():
+    """SlabRank drives the pass part by part with the maxima all-reduced over
+    a one-rank NCCL group (no neighbour: the exchange is empty); the result
+    is the whole-mesh context's to the bit."""
+    import datetime
+    import os
+    import socket
+
+    import torch
+    import torch.distributed as dist
+    case = config.small_case(16, 12, 12, Ra=1e5, steps=3)
+    want_recs, want = whole(case, case.steps)
+    sock = socket.socket()
+    sock.bind(("127.0.0.1", 0))
+    port = sock.getsockname()[1]
+    sock.close()
+    os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        r = nimgpu.SlabRank(nimgpu.Mesh(case.mesh_params()), case.params(**CAP))
+        r.initialize_nse()
+        r.add_temperature_noise(case.noise, case.seed)
+        recs = r.solve_nse(case.steps)
+        assert [(x.step, x.iters, x.status) for x in recs] == [(w.step, w.iters, w.status) for w in want_recs]
+        for x, w in zip(recs, want_recs):
+            for a in ("err_u", "err_v", "err_w", "err_p", "err_T", "dudt_max", "dTdt_max", "time", "nu_inner",
+                      "nu_outer", "dilatation"):
+                assert getattr(x, a) == getattr(w, a), a
+        for f, w in zip(FIELDS, want):
+            assert np.array_equal(r.gather(f), w), f
+        r.close()
+    finally:
+        dist.destroy_process_group()
