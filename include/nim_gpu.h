@@ -295,7 +295,10 @@ int nim_slab_halo(int32_t n_theta, int32_t n_r, int32_t n_z, int32_t nslab, int3
    address its cells and faces in the library's structured order (cell
    i + n_theta*(j + n_r*k) with k the held plane from the slab's first;
    faces in the r / theta / z blocks of that numbering).  Parallel
-   schedule, formulation 2, FP64 only (NIM_ERR_BAD_ARG otherwise). */
+   schedule, formulation 2, FP64 only (NIM_ERR_BAD_ARG otherwise).  With
+   nslab > 1 the context advances only with its neighbours (nim_slab_step,
+   or the nim_slab_part pieces): nim_gpu_iterate, nim_gpu_integrate,
+   nim_gpu_step and nim_batch_step refuse it with NIM_ERR_BAD_ARG. */
 int nim_gpu_create_slab(const nim_mesh_desc *mesh, const nim_params *params, int32_t nslab, int32_t s,
                         nim_ctx **ctx);
 

@@ -1213,8 +1213,12 @@ static int fill_iter_stats(nim_ctx *x, nim_step_stats *s) {
   return NIM_OK;
 }
 
+// a slab of a split mesh advances only with its neighbours (nim_slab_step,
+// nim_slab_part): alone its halo would go stale
+static bool lone_slab(const nim_ctx *x) { return x->slab_count > 1; }
+
 extern "C" int nim_gpu_iterate(nim_ctx *x, int32_t n, nim_step_stats *s) {
-  if (!x || n < 0) return NIM_ERR_BAD_ARG;
+  if (!x || n < 0 || lone_slab(x)) return NIM_ERR_BAD_ARG;
   if (!x->initialized) return NIM_ERR_STATE;
   // fixed number of passes: keep the stop flag clear and the cap out of reach
   const Phys keep = x->phys;
@@ -1365,7 +1369,7 @@ extern "C" int nim_gpu_set_graph_iters(nim_ctx *x, int32_t n) {
 }
 
 extern "C" int nim_gpu_integrate(nim_ctx *x, nim_step_stats *s) {
-  if (!x) return NIM_ERR_BAD_ARG;
+  if (!x || lone_slab(x)) return NIM_ERR_BAD_ARG;
   if (!x->initialized || !x->in_step) return NIM_ERR_STATE;
   TRY(integrate_start(x));
   for (;;) {
@@ -1388,7 +1392,7 @@ extern "C" int nim_gpu_end_step(nim_ctx *x, nim_step_stats *s) {
 }
 
 extern "C" int nim_gpu_step(nim_ctx *x, int32_t nsteps, nim_step_stats *per, int32_t *done) {
-  if (!x || nsteps < 0) return NIM_ERR_BAD_ARG;
+  if (!x || nsteps < 0 || lone_slab(x)) return NIM_ERR_BAD_ARG;
   if (!x->initialized) return NIM_ERR_STATE;
   int32_t k = 0;
   int st = NIM_OK;
@@ -1431,7 +1435,7 @@ extern "C" int nim_gpu_step(nim_ctx *x, int32_t nsteps, nim_step_stats *per, int
 extern "C" int nim_batch_step(int32_t n, nim_ctx *const *ctx, int32_t nsteps, nim_step_stats *per, int32_t *done) {
   if (n <= 0 || !ctx || nsteps < 0) return NIM_ERR_BAD_ARG;
   for (int32_t i = 0; i < n; ++i) {
-    if (!ctx[i]) return NIM_ERR_BAD_ARG;
+    if (!ctx[i] || lone_slab(ctx[i])) return NIM_ERR_BAD_ARG;
     if (!ctx[i]->initialized || ctx[i]->in_step) return NIM_ERR_STATE;
     if (ctx[i]->device != ctx[0]->device) return NIM_ERR_BAD_ARG;
     for (int32_t j = 0; j < i; ++j)

@@ -70,6 +70,10 @@ def test_slab_group_checks_its_members():
         assert lib.nim_slab_step(2, wrong, 1, None, None) == _abi.NIM_ERR_BAD_ARG
         swapped = (C.c_void_p * n)(g._h[1].value, g._h[0].value, g._h[2].value)
         assert lib.nim_slab_step(n, swapped, 1, None, None) == _abi.NIM_ERR_BAD_ARG
+        # a slab alone would step with a stale halo
+        assert lib.nim_gpu_step(g._h[1], 1, None, None) == _abi.NIM_ERR_BAD_ARG
+        one = (C.c_void_p * 1)(g._h[0].value)
+        assert lib.nim_batch_step(1, one, 1, None, None) == _abi.NIM_ERR_BAD_ARG
 
 
 def test_slab_rank_single_process_equals_whole_mesh():
