@@ -281,7 +281,9 @@ int nim_slab_layout(int32_t n_z, int32_t nslab, int32_t s, int32_t *out4);
    (side 1), as element spans (offset, count) into the slab context's own
    arrays: {cells, r faces, theta faces, z faces}.  recv8: the halo planes
    the neighbour owns; send8: the owned planes the neighbour holds as its
-   halo.  Every cell array carries span 0; every face array carries spans
+   halo.  The z span is the two rows of axial faces beyond the cut face
+   (which both slabs compute), so no span an exchange writes is read by
+   it.  Every cell array carries span 0; every face array carries spans
    1..3 in both of its halves (the face arrays alternate halves each
    pass).  The send spans of slab s, side 1, and the receive spans of slab
    s+1, side 0, have the same counts, and vice versa.  NIM_ERR_BAD_ARG on

@@ -928,20 +928,23 @@ extern "C" int nim_slab_halo(int32_t n_theta, int32_t n_r, int32_t n_z, int32_t 
   if ((side == 0 && s == 0) || (side == 1 && s == nslab - 1)) return NIM_ERR_BAD_ARG;
   const int64_t NT = n_theta, NR = n_r, NZl = lay[1] - lay[0], pl = NT * NR;
   const int64_t offT = NT * (NR + 1) * NZl, offZ = offT + pl * NZl;
-  // planes [g0, g0 + 2) of the slab with the z faces g0 .. g0 + 2
-  auto spans = [&](int64_t g0, int64_t *o) {
+  // planes [g0, g0 + 2) of the slab with the z-face rows z0, z0 + 1.  The
+  // cut face between two slabs is left out: each computes it from its own
+  // first halo plane, so no span written in an exchange is read in it.
+  auto spans = [&](int64_t g0, int64_t z0, int64_t *o) {
     const int64_t l0 = g0 - lay[0];
     o[0] = l0 * pl;                o[1] = 2 * pl;
     o[2] = NT * (NR + 1) * l0;     o[3] = 2 * NT * (NR + 1);
     o[4] = offT + l0 * pl;         o[5] = 2 * pl;
-    o[6] = offZ + l0 * pl;         o[7] = 3 * pl;
+    o[6] = offZ + (z0 - lay[0]) * pl;  o[7] = 2 * pl;
   };
+  const int64_t olo = lay[2], ohi = lay[3];
   if (side == 0) {
-    spans(lay[2] - 2, recv8);
-    spans(lay[2], send8);
+    spans(olo - 2, olo - 2, recv8);  // rows olo-2 (the end face), olo-1
+    spans(olo, olo + 1, send8);      // the lower neighbour's rows past its cut
   } else {
-    spans(lay[3], recv8);
-    spans(lay[3] - 2, send8);
+    spans(ohi, ohi + 1, recv8);      // rows ohi+1, ohi+2 (the end face)
+    spans(ohi - 2, ohi - 2, send8);
   }
   return NIM_OK;
 }
@@ -1570,33 +1573,67 @@ void halo_arrays(const nim_ctx *x, int what, std::vector<HaloArray> &out) {
   }
 }
 
+// One launch copies up to kHaloJobs spans (blockIdx.y = span): every copy
+// of an exchange in a handful of launches instead of one memcpy per span.
+constexpr int kHaloJobs = 120;
+struct HaloJobs {
+  const double *src[kHaloJobs];
+  double *dst[kHaloJobs];
+  int n[kHaloJobs];
+};
+__global__ void __launch_bounds__(BLK) k_halo_copy(HaloJobs J) {
+  const int j = blockIdx.y;
+  const double *__restrict__ a = J.src[j];
+  double *__restrict__ b = J.dst[j];
+  for (int i = blockIdx.x * BLK + threadIdx.x; i < J.n[j]; i += gridDim.x * BLK) b[i] = a[i];
+}
+
 // src's owned planes next to dst into dst's halo: each cell array over span
 // 0, each face array (both halves) over the r, theta and z spans 1..3
-int copy_halo(const nim_ctx *src, const int64_t *snd, const nim_ctx *dst, const int64_t *rcv, cudaStream_t st,
-              int what) {
+int halo_jobs(const nim_ctx *src, const int64_t *snd, const nim_ctx *dst, const int64_t *rcv, int what,
+              std::vector<HaloJobs> &jobs, int &used) {
   for (int t = 0; t < 4; ++t)
     if (snd[2 * t + 1] != rcv[2 * t + 1]) return NIM_ERR_BAD_ARG;
   std::vector<HaloArray> A, B;
   halo_arrays(src, what, A);
   halo_arrays(dst, what, B);
   const size_t NFa = src->d.NF, NFb = dst->d.NF;
+  auto add = [&](const double *from, double *to, int64_t n) {
+    if (used == kHaloJobs || jobs.empty()) {
+      jobs.emplace_back();
+      used = 0;
+    }
+    HaloJobs &J = jobs.back();
+    J.src[used] = from;
+    J.dst[used] = to;
+    J.n[used] = (int)n;
+    ++used;
+  };
   for (size_t a = 0; a < A.size(); ++a) {
     if (!A[a].face) {
-      CK(cudaMemcpyAsync(B[a].p + rcv[0], A[a].p + snd[0], sizeof(double) * snd[1], cudaMemcpyDeviceToDevice, st));
+      add(A[a].p + snd[0], B[a].p + rcv[0], snd[1]);
       continue;
     }
     for (int h = 0; h < 2; ++h)
-      for (int t = 1; t < 4; ++t)
-        CK(cudaMemcpyAsync(B[a].p + h * NFb + rcv[2 * t], A[a].p + h * NFa + snd[2 * t],
-                           sizeof(double) * snd[2 * t + 1], cudaMemcpyDeviceToDevice, st));
+      for (int t = 1; t < 4; ++t) add(A[a].p + h * NFa + snd[2 * t], B[a].p + h * NFb + rcv[2 * t], snd[2 * t + 1]);
   }
   return NIM_OK;
 }
 
 int halo_exchange(nim_ctx *const *X, int n, cudaStream_t st, int what) {
+  std::vector<HaloJobs> jobs;
+  int used = 0;
+  int64_t longest = 0;
   for (int s = 0; s + 1 < n; ++s) {
-    TRY(copy_halo(X[s], X[s]->halo_send[1], X[s + 1], X[s + 1]->halo_recv[0], st, what));
-    TRY(copy_halo(X[s + 1], X[s + 1]->halo_send[0], X[s], X[s]->halo_recv[1], st, what));
+    TRY(halo_jobs(X[s], X[s]->halo_send[1], X[s + 1], X[s + 1]->halo_recv[0], what, jobs, used));
+    TRY(halo_jobs(X[s + 1], X[s + 1]->halo_send[0], X[s], X[s]->halo_recv[1], what, jobs, used));
+    for (int t = 0; t < 4; ++t) longest = std::max(longest, X[s]->halo_send[1][2 * t + 1]);
+  }
+  const int gx = (int)std::min<int64_t>((longest + BLK - 1) / BLK, 64);
+  for (size_t k = 0; k < jobs.size(); ++k) {
+    const int nj = (k + 1 == jobs.size()) ? used : kHaloJobs;
+    k_halo_copy<<<dim3(std::max(gx, 1), nj), BLK, 0, st>>>(jobs[k]);
+    CK(cudaGetLastError());
   }
   return NIM_OK;
 }
