@@ -339,6 +339,18 @@ int nim_slab_part(nim_ctx *ctx, int32_t part);
    too small. */
 int nim_slab_arrays(nim_ctx *ctx, int32_t set, void **ptr, int32_t *face, int32_t cap);
 
+/* One message per neighbour instead of one per span: nim_slab_pack gathers
+   the send spans of side `side` of every array of the set into the device
+   buffer buf (nim_slab_pack_doubles doubles, in nim_slab_arrays order, a
+   face array's first half then its second), nim_slab_unpack scatters a
+   neighbour's packed payload into the receive spans.  The send payload of
+   slab s, side 1, and the receive payload of slab s+1, side 0, have the
+   same length and order, and vice versa.  Both are queued on the
+   context's stream. */
+int64_t nim_slab_pack_doubles(nim_ctx *ctx, int32_t set, int32_t side);
+int nim_slab_pack(nim_ctx *ctx, int32_t set, int32_t side, void *buf);
+int nim_slab_unpack(nim_ctx *ctx, int32_t set, int32_t side, const void *buf);
+
 /* Device address of the 24 uint64 words (bit patterns of non-negative
    doubles) every slab must replace by their maximum over all slabs before
    part 3: find_error's accumulators and the Dirichlet wall floor. */

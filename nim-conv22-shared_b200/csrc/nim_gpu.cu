@@ -1827,6 +1827,79 @@ extern "C" int nim_slab_arrays(nim_ctx *x, int32_t set, void **ptr, int32_t *fac
   return (int)v.size();
 }
 
+namespace {
+// the spans of one side of an exchange of `what`, in payload order: each
+// array of halo_arrays, a cell array over span 0, a face array over spans
+// 1..3 of its first half then of its second
+int side_spans(const nim_ctx *x, int what, int side, bool send, std::vector<std::pair<double *, int64_t>> &out) {
+  if ((side != 0 && side != 1) || !x->halo_ok[side]) return NIM_ERR_BAD_ARG;
+  const int64_t *sp = send ? x->halo_send[side] : x->halo_recv[side];
+  std::vector<HaloArray> A;
+  halo_arrays(x, what, A);
+  out.clear();
+  const size_t NF = x->d.NF;
+  for (const HaloArray &a : A) {
+    if (!a.face) {
+      out.emplace_back(a.p + sp[0], sp[1]);
+      continue;
+    }
+    for (int h = 0; h < 2; ++h)
+      for (int t = 1; t < 4; ++t) out.emplace_back(a.p + h * NF + sp[2 * t], sp[2 * t + 1]);
+  }
+  return NIM_OK;
+}
+
+// pack (spans -> buf) or unpack (buf -> spans) on the context's stream
+int pack_side(nim_ctx *x, int what, int side, double *buf, bool pack) {
+  std::vector<std::pair<double *, int64_t>> sp;
+  TRY(side_spans(x, what, side, pack, sp));
+  std::vector<HaloJobs> jobs;
+  int64_t off = 0, longest = 0;
+  int used = 0;
+  for (auto &v : sp) {
+    if (used == kHaloJobs || jobs.empty()) {
+      jobs.emplace_back();
+      used = 0;
+    }
+    HaloJobs &J = jobs.back();
+    J.src[used] = pack ? v.first : buf + off;
+    J.dst[used] = pack ? buf + off : v.first;
+    J.n[used] = (int)v.second;
+    ++used;
+    off += v.second;
+    longest = std::max(longest, v.second);
+  }
+  CK(cudaSetDevice(x->device));
+  const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((longest + BLK - 1) / BLK, 64));
+  for (size_t k = 0; k < jobs.size(); ++k) {
+    const int nj = (k + 1 == jobs.size()) ? used : kHaloJobs;
+    k_halo_copy<<<dim3(gx, nj), BLK, 0, x->stream>>>(jobs[k]);
+    CK(cudaGetLastError());
+  }
+  x->launches += (long long)jobs.size();
+  return NIM_OK;
+}
+}  // namespace
+
+extern "C" int64_t nim_slab_pack_doubles(nim_ctx *x, int32_t set, int32_t side) {
+  if (!x || set < 1 || set > 15) return NIM_ERR_BAD_ARG;
+  std::vector<std::pair<double *, int64_t>> sp;
+  TRY(side_spans(x, set, side, true, sp));
+  int64_t n = 0;
+  for (auto &v : sp) n += v.second;
+  return n;
+}
+
+extern "C" int nim_slab_pack(nim_ctx *x, int32_t set, int32_t side, void *buf) {
+  if (!x || !buf || set < 1 || set > 15) return NIM_ERR_BAD_ARG;
+  return pack_side(x, set, side, static_cast<double *>(buf), true);
+}
+
+extern "C" int nim_slab_unpack(nim_ctx *x, int32_t set, int32_t side, const void *buf) {
+  if (!x || !buf || set < 1 || set > 15) return NIM_ERR_BAD_ARG;
+  return pack_side(x, set, side, const_cast<double *>(static_cast<const double *>(buf)), false);
+}
+
 extern "C" int nim_slab_maxima(nim_ctx *x, void **slots24) {
   if (!x || !slots24) return NIM_ERR_BAD_ARG;
   *slots24 = reinterpret_cast<char *>(x->ctl) + offsetof(Ctrl, err);

@@ -5,8 +5,8 @@ from . import _abi, config
 from ._abi import NimError, StepStats, Params, MeshParams
 from .mesh import Mesh, temperature_noise, apply_temperature_noise
 from .solver import NimSolver, autotune_batch, batch_step, field_len
-from .slabs import SlabGroup, SlabRank, exchange_halos, slab_halo, slab_layout
+from .slabs import SlabGroup, SlabRank, exchange_packed, slab_halo, slab_layout
 
 __all__ = ["_abi", "config", "NimError", "StepStats", "Params", "MeshParams", "Mesh",
            "temperature_noise", "apply_temperature_noise", "NimSolver", "autotune_batch", "batch_step", "field_len",
-           "SlabGroup", "SlabRank", "exchange_halos", "slab_halo", "slab_layout"]
+           "SlabGroup", "SlabRank", "exchange_packed", "slab_halo", "slab_layout"]

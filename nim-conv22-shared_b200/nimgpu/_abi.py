@@ -177,6 +177,12 @@ def gpu_lib() -> C.CDLL:
         lib.nim_slab_part.restype = C.c_int
         lib.nim_slab_arrays.argtypes = [vp, C.c_int32, C.POINTER(vp), C.POINTER(C.c_int32), C.c_int32]
         lib.nim_slab_arrays.restype = C.c_int
+        lib.nim_slab_pack_doubles.argtypes = [vp, C.c_int32, C.c_int32]
+        lib.nim_slab_pack_doubles.restype = C.c_int64
+        lib.nim_slab_pack.argtypes = [vp, C.c_int32, C.c_int32, vp]
+        lib.nim_slab_pack.restype = C.c_int
+        lib.nim_slab_unpack.argtypes = [vp, C.c_int32, C.c_int32, vp]
+        lib.nim_slab_unpack.restype = C.c_int
         lib.nim_slab_maxima.argtypes = [vp, C.POINTER(vp)]
         lib.nim_slab_maxima.restype = C.c_int
         lib.nim_slab_loop_state.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_double)]

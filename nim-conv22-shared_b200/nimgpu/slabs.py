@@ -219,40 +219,17 @@ class SlabGroup(_Slabs):
 HALO_VELOCITY, HALO_PRESSURE, HALO_TEMPERATURE, HALO_STATE = 1, 2, 4, 8
 
 
-def halo_views(arrays, nf: int, plans: dict, rank: int):
-    """The transfers of one halo exchange of slab `rank`: per neighbour,
-    (peer rank, views to send, views to receive into), in one order both
-    sides generate alike.  arrays: (1-D tensor or array, is_face) pairs as
-    nim_slab_arrays lists them (face arrays hold both halves, 2*nf);
-    plans: {side: (recv spans, send spans)} of slab_halo."""
-    out = []
-    for side in (0, 1):
-        if side not in plans:
-            continue
-        recv, send = plans[side]
-        sv, rv = [], []
-        for a, face in arrays:
-            spans = [(h * nf, t) for h in (0, 1) for t in (1, 2, 3)] if face else [(0, 0)]
-            for base, t in spans:
-                (so, sn), (ro, rn) = send[t], recv[t]
-                if sn != rn:
-                    raise ValueError("exchange plans of neighbour slabs disagree")
-                sv.append(a[base + so:base + so + sn])
-                rv.append(a[base + ro:base + ro + rn])
-        out.append((rank - 1 if side == 0 else rank + 1, sv, rv))
-    return out
-
-
-def exchange_halos(arrays, nf: int, plans: dict, rank: int, group=None):
-    """One halo exchange over torch.distributed point-to-point operations
-    (NCCL for device tensors, ordered on the current CUDA stream; gloo for
-    host tensors): slab `rank` sends its planes next to each neighbour and
-    receives that neighbour's into its halo."""
+def exchange_packed(send: dict, recv: dict, rank: int, group=None):
+    """One halo exchange over torch.distributed: per side with a neighbour
+    (0 below, 1 above), the packed payload send[side] goes to that
+    neighbour and its payload lands in recv[side] (NCCL for device tensors,
+    ordered on the current CUDA stream; gloo for host tensors)."""
     import torch.distributed as dist
     ops = []
-    for peer, sv, rv in halo_views(arrays, nf, plans, rank):
-        ops += [dist.P2POp(dist.isend, t, peer, group) for t in sv]
-        ops += [dist.P2POp(dist.irecv, t, peer, group) for t in rv]
+    for side in sorted(send):
+        peer = rank - 1 if side == 0 else rank + 1
+        ops.append(dist.P2POp(dist.isend, send[side], peer, group))
+        ops.append(dist.P2POp(dist.irecv, recv[side], peer, group))
     if ops:
         for w in dist.batch_isend_irecv(ops):
             w.wait()
@@ -275,8 +252,9 @@ class SlabRank(_Slabs):
     """This process's slab of a mesh split over the ranks of a
     torch.distributed group, one GPU per rank (rank r holds slab r, bottom to
     top).  solve_nse drives the pieces of nim_slab_step: each part of a pass
-    on the context's stream, then the halo exchange over the group
-    (exchange_halos), the maxima's all-reduce before every pass end, and the
+    on the context's stream, then the halo exchange over the group (packed
+    by nim_slab_pack, one message per neighbour: exchange_packed), the
+    maxima's all-reduce before every pass end, and the
     step-end sums reduced over the group."""
 
     def __init__(self, mesh: Mesh, params: _abi.Params, group=None):
@@ -293,29 +271,38 @@ class SlabRank(_Slabs):
             self.plans[0] = slab_halo(mesh.n_theta, mesh.n_r, mesh.n_z, self.world, self.rank, 0)
         if self.rank < self.world - 1:
             self.plans[1] = slab_halo(mesh.n_theta, mesh.n_r, mesh.n_z, self.world, self.rank, 1)
-        nc, self._nf = self._sizes(self.rank)
-        self._arrays = {}
+        # packed send / receive buffers per exchange set and side
+        self._send, self._recv = {}, {}
         for st in (HALO_VELOCITY, HALO_PRESSURE, HALO_TEMPERATURE, HALO_STATE):
-            ptr, face = (C.c_void_p * 32)(), (C.c_int32 * 32)()
-            n = self.lib.nim_slab_arrays(h, st, ptr, face, 32)
-            if n < 0:
-                _abi.check(n, "nim_slab_arrays")
-            self._arrays[st] = [(_device_tensor(ptr[i], 2 * self._nf if face[i] else nc, "<f8", self.device),
-                                 bool(face[i])) for i in range(n)]
+            self._send[st], self._recv[st] = {}, {}
+            for side in self.plans:
+                n = int(self.lib.nim_slab_pack_doubles(h, st, side))
+                if n < 0:
+                    _abi.check(n, "nim_slab_pack_doubles")
+                self._send[st][side] = torch.empty(n, dtype=torch.float64, device=self.device)
+                self._recv[st][side] = torch.empty(n, dtype=torch.float64, device=self.device)
         slots = C.c_void_p()
         _abi.check(self.lib.nim_slab_maxima(h, C.byref(slots)), "nim_slab_maxima")
         self._maxima = _device_tensor(slots.value, 24, "<i8", self.device)
         self._step, self._time = 1, params.DT
 
     def close(self):
-        self._arrays, self._maxima = {}, None
+        self._send, self._recv, self._maxima = {}, {}, None
         super().close()
 
     def _exchange(self, what: int):
+        """Pack each side on the context's stream, one message per
+        neighbour, unpack after it lands."""
         import torch
-        if self.world > 1:
-            with torch.cuda.stream(self.stream):
-                exchange_halos(self._arrays[what], self._nf, self.plans, self.rank, self._group)
+        if self.world == 1:
+            return
+        h, send, recv = self._h[0], self._send[what], self._recv[what]
+        for side, buf in send.items():
+            _abi.check(self.lib.nim_slab_pack(h, what, side, C.c_void_p(buf.data_ptr())), "nim_slab_pack")
+        with torch.cuda.stream(self.stream):
+            exchange_packed(send, recv, self.rank, self._group)
+        for side, buf in recv.items():
+            _abi.check(self.lib.nim_slab_unpack(h, what, side, C.c_void_p(buf.data_ptr())), "nim_slab_unpack")
 
     def _merge(self):
         import torch

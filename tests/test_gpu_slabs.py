@@ -110,3 +110,59 @@ def test_slab_rank_single_process_equals_whole_mesh():
         r.close()
     finally:
         dist.destroy_process_group()
+
+
+def test_pack_unpack_restores_halos():
+    """nim_slab_pack / nim_slab_unpack between the slabs of one device (no
+    collective): halos overwritten with junk, the whole state moved through
+    packed device buffers, every held plane again holds the whole mesh's
+    values (cells, and the faces of the current half)."""
+    import ctypes as C
+
+    import torch
+    from nimgpu.slabs import HALO_STATE, slab_face_planes, structured_faces
+    case = config.small_case(16, 12, 12, Ra=1e5)
+    mesh = nimgpu.Mesh(case.mesh_params())
+    ref = structured_faces(mesh)
+    pl = mesh.n_theta * mesh.n_r
+    offZ = mesh.n_theta * (mesh.n_r + 1) * mesh.n_z + pl * mesh.n_z
+    w = nimgpu.NimSolver(mesh, case.params())
+    w.initialize_nse()
+    w.add_temperature_noise(1e-3, 5)
+    cells_T, faces_T = w.download(_abi.MESHES_T), w.download(_abi.FACES_T)
+    w.close()
+    with nimgpu.SlabGroup(mesh, case.params(), 3) as g:
+        g.initialize_nse()
+        g.add_temperature_noise(1e-3, 5)
+        for s in g.slabs:
+            lo, hi, olo, ohi = g.layout[s]
+            c = g.download(s, _abi.MESHES_T)
+            for k in range(lo, hi):
+                if not olo <= k < ohi:
+                    c[(k - lo) * pl:(k - lo + 1) * pl] = -7.0
+            g.upload(s, _abi.MESHES_T, c)
+            glob, plane = slab_face_planes(mesh, lo, hi)
+            z = glob >= offZ
+            own = (plane >= olo) & (plane < ohi)
+            halo = np.where(z, ~(own | ((plane - 1 >= olo) & (plane - 1 < ohi))), ~own)
+            f = g.download(s, _abi.FACES_T)
+            f[halo] = -7.0
+            g.upload(s, _abi.FACES_T, f)
+        lib = g.lib
+        for s in range(g.nslab - 1):
+            for a, sa, b, sb in ((s, 1, s + 1, 0), (s + 1, 0, s, 1)):
+                ha, hb = g._handle(a), g._handle(b)
+                n = lib.nim_slab_pack_doubles(ha, HALO_STATE, sa)
+                assert n == lib.nim_slab_pack_doubles(hb, HALO_STATE, sb) > 0
+                buf = torch.empty(n, dtype=torch.float64, device="cuda")
+                torch.cuda.synchronize()
+                _abi.check(lib.nim_slab_pack(ha, HALO_STATE, sa, C.c_void_p(buf.data_ptr())), "nim_slab_pack")
+                _abi.check(lib.nim_gpu_synchronize(ha), "sync")
+                _abi.check(lib.nim_slab_unpack(hb, HALO_STATE, sb, C.c_void_p(buf.data_ptr())), "nim_slab_unpack")
+                _abi.check(lib.nim_gpu_synchronize(hb), "sync")
+        for s in g.slabs:
+            lo, hi = g.layout[s][:2]
+            assert np.array_equal(g.download(s, _abi.MESHES_T), cells_T[lo * pl:hi * pl])
+            glob, _ = slab_face_planes(mesh, lo, hi)
+            assert np.array_equal(g.download(s, _abi.FACES_T), faces_T[ref[glob]])
+        assert lib.nim_slab_pack_doubles(g._handle(0), HALO_STATE, 0) == _abi.NIM_ERR_BAD_ARG  # no slab below 0

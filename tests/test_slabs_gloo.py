@@ -1,9 +1,10 @@
-"""The halo exchange of z-slabs over torch.distributed (nimgpu.exchange_halos),
-run by 2 and 3 gloo ranks on the CPU: each rank holds one slab's arrays (a
-cell and a face array per field, both face halves) filled with their
-whole-mesh identity and its halo wiped; after one exchange every element
-is whole again.  The same function moves device arrays over NCCL between
-one process per GPU."""
+"""The halo exchange of z-slabs over torch.distributed
+(nimgpu.exchange_packed), run by 2 and 3 gloo ranks on the CPU: each rank
+holds one slab's arrays (a cell and a face array per field, both face
+halves) filled with their whole-mesh identity and its halo wiped, packs
+each side in the order nim_slab_pack uses, exchanges one message per
+neighbour and unpacks: every element is whole again.  The same function
+moves the device-packed payloads over NCCL between one process per GPU."""
 import os
 import socket
 import sys
@@ -59,7 +60,7 @@ def _rank(rank, world, port, dims, out):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     sys.path.insert(0, str(ROOT / "nim-conv22-shared_b200"))
-    from nimgpu.slabs import exchange_halos, slab_halo
+    from nimgpu.slabs import exchange_packed, slab_halo
     import datetime
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
@@ -70,7 +71,27 @@ def _rank(rank, world, port, dims, out):
             plans[0] = slab_halo(NT, NR, NZ, world, rank, 0)
         if rank < world - 1:
             plans[1] = slab_halo(NT, NR, NZ, world, rank, 1)
-        exchange_halos(have, nf, plans, rank)
+
+        def views(side, send):
+            # nim_slab_pack's order: each array; a face array's spans 1..3 of
+            # its first half, then of its second
+            recv_sp, send_sp = plans[side]
+            sp = send_sp if send else recv_sp
+            out = []
+            for a, face in have:
+                for base, t in ([(h * nf, t) for h in (0, 1) for t in (1, 2, 3)] if face else [(0, 0)]):
+                    o, n = sp[t]
+                    out.append(a[base + o:base + o + n])
+            return out
+
+        send = {side: torch.cat(views(side, True)) for side in plans}
+        recv = {side: torch.empty_like(send[side]) for side in plans}
+        exchange_packed(send, recv, rank)
+        for side in plans:
+            off = 0
+            for v in views(side, False):
+                v.copy_(recv[side][off:off + v.numel()])
+                off += v.numel()
         out[rank] = all(torch.equal(w, h) for (w, _), (h, _) in zip(want, have))
     finally:
         dist.destroy_process_group()
