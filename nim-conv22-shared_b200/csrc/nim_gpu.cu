@@ -1792,6 +1792,8 @@ extern "C" int nim_slab_step(int32_t n, nim_ctx *const *X, int32_t nsteps, nim_s
   const int st = slab_step_impl(X, n, nsteps, per, done, exec);
   cudaStreamSynchronize(X[0]->stream);
   cudaGraphExecDestroy(exec);
+  if (st != NIM_OK)  // a step left half done: the next call starts a new one
+    for (int32_t s = 0; s < n; ++s) X[s]->in_step = false;
   return st;
 }
 
