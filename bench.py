@@ -26,6 +26,11 @@ start with nim_params.precision = NIM_PRECISION_MIXED (FP32 passes, then
 FP64 passes to the reference's stop test), its throughput, its roofline and
 its per-step Nusselt and final field errors against the FP64 run.
 --precision mixed makes the mixed path the headline arm instead.
+
+It also carries "slabs": the same steps from the same start with the mesh
+split into two z-slabs on the one device (nim_slab_step: halo exchange after
+each part of every pass), their throughput against the whole mesh and
+whether iterations and final fields match the whole-mesh run exactly.
 """
 from __future__ import annotations
 
@@ -365,6 +370,36 @@ def run_mixed(case, mesh, args, fp64_stats, fp64_fields, fp64_value, fp64_ms_ste
     }
 
 
+def run_slabs(case, mesh, args, fp64_stats, fp64_fields, fp64_value, nslab=2):
+    """The FP64 run's steps again, from the same start, as nslab z-slabs of
+    the mesh on this device; wall clock around the synchronous group step
+    (its work spans the slabs' streams)."""
+    import nimgpu
+    g = nimgpu.SlabGroup(mesh, case.params(), nslab)
+    try:
+        g.initialize_nse()
+        g.add_temperature_noise(case.noise, case.seed)
+        recs = []
+        for _ in range(max(args.warmup, 0)):
+            recs += g.solve_nse(1)
+        t0 = time.perf_counter()
+        timed = g.solve_nse(args.steps)
+        dt = time.perf_counter() - t0
+        recs += timed
+        iters = sum(r.iters for r in timed)
+        value = case.ncells * iters / dt
+        same_iters = [r.iters for r in recs] == [r.iters for r in fp64_stats]
+        same_fields = (all(np.array_equal(g.gather(f), fp64_fields[f]) for f in MIXED_FIELDS)
+                       if fp64_fields is not None else None)
+        return {"slabs": nslab, "value": value, "unit": UNIT, "ms_per_step": 1e3 * dt / max(args.steps, 1),
+                "ratio_to_whole_mesh": value / fp64_value, "same_iterations": same_iters,
+                "fields_identical": same_fields,
+                "layout": [list(g.layout[s]) for s in g.slabs],
+                "timing": "wall clock around nim_slab_step (synchronous)"}
+    finally:
+        g.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -378,6 +413,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 passes over a float mirror, then FP64 passes (nim_params.precision)")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
+    ap.add_argument("--no-slabs", action="store_true", help="skip the two-slab comparison")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -432,7 +468,9 @@ def main():
     value = total / (t_max / 1e3)
     want_mixed = (world == 1 and prec == _abi.PRECISION_FP64 and sched == _abi.SCHEDULE_PARALLEL
                   and not args.no_mixed)
-    fp64_fields = {f: solver.download(f) for f in MIXED_FIELDS} if want_mixed else None
+    want_slabs = (world == 1 and prec == _abi.PRECISION_FP64 and sched == _abi.SCHEDULE_PARALLEL
+                  and not args.no_slabs and case.n_z // 2 >= 2)
+    fp64_fields = ({f: solver.download(f) for f in MIXED_FIELDS} if (want_mixed or want_slabs) else None)
 
     # ---------------- end to end through the C ABI with host buffers: the
     # host holds the state (read_restart / write_restart arrays) and every
@@ -481,6 +519,13 @@ def main():
         mixed = run_mixed(case, mesh, args, warm_stats + list(stats), fp64_fields, value, ms / max(args.steps, 1),
                           peak, peak_kind)
 
+    slabs = None
+    if want_slabs:
+        try:
+            slabs = run_slabs(case, mesh, args, warm_stats + list(stats), fp64_fields, value)
+        except Exception as exc:  # an extra measurement: report it, keep the line
+            slabs = {"error": repr(exc)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt = cpu_sample(case, threads=1, iters=4, schedule=0)
@@ -514,6 +559,7 @@ def main():
         "nu_inner_last": stats[-1].nu_inner if stats else None,
         "iters_fp32": sum(s.iters_fp32 for s in stats),
         "mixed": mixed,
+        "slabs": slabs,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
