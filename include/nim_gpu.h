@@ -437,7 +437,9 @@ int nim_gpu_selftest_wait_timeout(nim_ctx *ctx, int32_t tries);
    leaves the last call's partial sums there, so calls that overlap on the
    GPU (two contexts on one device at once) race.  Meshes with more than
    NIM_NOALLOC_MAX_WALL_FACES wall faces are refused with NIM_ERR_BAD_ARG.
-   Synchronises the context's stream. */
+   On a z-slab context the sums cover the slab's owned planes only (the
+   areas let a host combine slabs: Nu = sum of Nu_k * area_k / sum of
+   area_k per wall).  Synchronises the context's stream. */
 int nim_gpu_nusselt_noalloc(nim_ctx *ctx, double *out4);
 
 /* Block until all work queued on the context's stream has finished. */
