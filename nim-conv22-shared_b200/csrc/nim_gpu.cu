@@ -302,7 +302,10 @@ int launch_vel(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F
     if (x->bulk) {
       const dim3 gt((d.NT + 31) / 32, (d.NR + VT_R - 1) / VT_R, (d.NZ + x->tile_kc - 1) / x->tile_kc);
       const VelFaceMaps &M = std::is_same<R, double>::value ? x->vmap64 : x->vmap32;
-      k_vel_face_tile<R><<<gt, dim3(VT_T, 3), VtLayout<R>::bytes, s>>>(d, g, F, x->phys, x->ctl, x->tile_kc, M);
+      if (x->slab_count)
+        k_vel_face_tile<R, true><<<gt, dim3(VT_T, 3), VtLayout<R>::bytes, s>>>(d, g, F, x->phys, x->ctl, x->tile_kc, M);
+      else
+        k_vel_face_tile<R><<<gt, dim3(VT_T, 3), VtLayout<R>::bytes, s>>>(d, g, F, x->phys, x->ctl, x->tile_kc, M);
       TRY(mark(x, "k_vel_face_tile"));
     } else {
       k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
@@ -988,7 +991,7 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x, 
   x->params = *p;
   x->seq = (p->schedule == NIM_SCHEDULE_REFERENCE);
   TRY(choose_face_sweep(x));
-  if (slab) x->bulk = x->cell_tile = false;  // the gather forms: masked maxima
+  if (slab) x->cell_tile = false;  // its maxima are not masked per plane
   x->phys = make_phys(*p);
   x->gq = make_gauss();
   x->nblk_c = grid(d.Nc);
@@ -1097,6 +1100,10 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x, 
       CK(cudaFuncSetAttribute(k_vel_face_tile<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)VtLayout<double>::bytes));
       CK(cudaFuncSetAttribute(k_vel_face_tile<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)VtLayout<float>::bytes));
+      CK(cudaFuncSetAttribute(k_vel_face_tile<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)VtLayout<double>::bytes));
+      CK(cudaFuncSetAttribute(k_vel_face_tile<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)VtLayout<float>::bytes));
     }
   }

@@ -1563,7 +1563,8 @@ __device__ __forceinline__ bool vt_seam(const Dims &d, const FieldsT<R> &F, int 
   return true;
 }
 
-template <class R>
+// SLAB: a z-slab context, whose maxima skip the planes a neighbour owns
+template <class R, bool SLAB = false>
 __global__ void __launch_bounds__(3 * VT_T, sizeof(R) == 8 ? VT_MINB : 3)
     k_vel_face_tile(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl, int kc, const __grid_constant__ VelFaceMaps M) {
   using L = VtLayout<R>;
@@ -1664,7 +1665,7 @@ __global__ void __launch_bounds__(3 * VT_T, sizeof(R) == 8 ? VT_MINB : 3)
               fx, fx2, cq0[jj * L::W + ii], cq2[(jj + dj) * L::W + ii + di], cq0[L::C5 + jj * L::W + ii],
               cq2[L::C5 + (jj + dj) * L::W + ii + di], Fd, dg0, dg1, dd, P.w[q]));
           F.f[q][(1 - par) * NF + fo] = nw;
-          e[q] = nmax(e[q], errv(nw, fx(2 * dd), first));
+          if (!SLAB || d.owns(k)) e[q] = nmax(e[q], errv(nw, fx(2 * dd), first));
         }
       });
     }

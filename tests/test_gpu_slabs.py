@@ -166,3 +166,27 @@ def test_pack_unpack_restores_halos():
             glob, _ = slab_face_planes(mesh, lo, hi)
             assert np.array_equal(g.download(s, _abi.FACES_T), faces_T[ref[glob]])
         assert lib.nim_slab_pack_doubles(g._handle(0), HALO_STATE, 0) == _abi.NIM_ERR_BAD_ARG  # no slab below 0
+
+
+def test_slabs_with_tiled_face_sweep(monkeypatch):
+    """Slab contexts running the TMA-staged face sweep (its per-plane masked
+    maxima), forced on a small mesh: still the whole mesh's fields and
+    iteration counts."""
+    import ctypes as C
+    case = config.small_case(16, 12, 12, Ra=1e5, steps=3)
+    want_recs, want = whole(case, case.steps)
+    monkeypatch.setenv("NIM_FACE_SWEEP", "tile")
+    mesh = nimgpu.Mesh(case.mesh_params())
+    with nimgpu.SlabGroup(mesh, case.params(**CAP), 3) as g:
+        g.initialize_nse()
+        g.add_temperature_noise(case.noise, case.seed)
+        recs = g.solve_nse(case.steps)
+        assert [(r.iters, r.err_u, r.err_T) for r in recs] == [(w.iters, w.err_u, w.err_T) for w in want_recs]
+        for f, w in zip(FIELDS, want):
+            assert np.array_equal(g.gather(f), w), f
+        # the slabs did run the staged sweep
+        ms = (C.c_double * 32)()
+        h = g._handle(1)
+        nk = g.lib.nim_gpu_profile_iterations(h, 1, ms, 32)
+        assert nk > 0
+        assert "k_vel_face_tile" in [g.lib.nim_gpu_profile_name(h, k).decode() for k in range(nk)]
