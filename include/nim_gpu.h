@@ -421,6 +421,14 @@ const char *nim_gpu_profile_name(nim_ctx *ctx, int32_t k);
    the context stays usable.  Between steps only. */
 int nim_gpu_selftest_wait_timeout(nim_ctx *ctx, int32_t tries);
 
+/* Self-test of the device exp (no counterpart in the reference): y[i] =
+   the exp that the NIM coefficients use on the device, for n host values x
+   (n <= 2^28; the call allocates and frees its device buffers and runs on
+   the current device's default stream).  That exp restates glibc's
+   algorithm and must equal the host libm's exp bit for bit (the reference's
+   exponential NIM coefficients, nim.f90:190-194, call it). */
+int nim_gpu_selftest_exp(const double *x, double *y, int64_t n);
+
 /* Wall-face limit of nim_gpu_nusselt_noalloc: 2*n_theta*n_z inner plus
    outer wall faces, i.e. 4096 blocks of 256 faces. */
 #define NIM_NOALLOC_MAX_WALL_FACES 1048576
@@ -433,10 +441,16 @@ int nim_gpu_selftest_wait_timeout(nim_ctx *ctx, int32_t tries);
    out4[0..3] = Nu_outer, Nu_inner, outer wall area, inner wall area (the
    values nim_gpu_end_step reports) into caller-owned host memory.  Its
    scratch is one static device array of 4*4096+8 doubles per device, whose
-   address nim_gpu_create looks up once per device; every call reuses it and
-   leaves the last call's partial sums there, so calls that overlap on the
-   GPU (two contexts on one device at once) race.  Meshes with more than
-   NIM_NOALLOC_MAX_WALL_FACES wall faces are refused with NIM_ERR_BAD_ARG.
+   address is looked up with the context's device current, first by
+   nim_gpu_create and again on every call (a lookup, not an allocation, so
+   a device reset cannot leave a stale address behind); the first
+   nim_gpu_create on a device should therefore come before any stream
+   capture.  Every call reuses the array and leaves the last call's partial
+   sums there, so calls that overlap on the GPU (two contexts on one device
+   at once) race: the host must serialise them per device.  Between steps
+   only (NIM_ERR_STATE after nim_gpu_begin_step until nim_gpu_end_step).
+   Meshes with more than NIM_NOALLOC_MAX_WALL_FACES wall faces are refused
+   with NIM_ERR_BAD_ARG.
    On a z-slab context the sums cover the slab's owned planes only (the
    areas let a host combine slabs: Nu = sum of Nu_k * area_k / sum of
    area_k per wall).  Synchronises the context's stream. */

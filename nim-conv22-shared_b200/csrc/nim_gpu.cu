@@ -705,10 +705,15 @@ extern "C" const char *nim_gpu_strerror(int s) {
   }
 }
 
+// Looks up the device address of g_noalloc_scratch with `device` current.
+// nim_gpu_create calls it first (so the lookup, which may load the module,
+// happens before any stream capture) and nim_gpu_nusselt_noalloc again on
+// every call: after a device reset or a new primary context the module is
+// loaded afresh and an address kept from before would dangle.  The lookup
+// allocates nothing.
 static int noalloc_setup(int device) {
   if (device < 0 || device >= kMaxDevices) return NIM_ERR_BAD_ARG;
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (g_noalloc_ptr[device]) return NIM_OK;
   void *ptr = nullptr;
   CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));  // the current device's copy
   g_noalloc_ptr[device] = static_cast<double *>(ptr);
@@ -2117,19 +2122,40 @@ extern "C" int nim_gpu_selftest_wait_timeout(nim_ctx *x, int32_t tries) {
   return seen;
 }
 
+extern "C" int nim_gpu_selftest_exp(const double *x, double *y, int64_t n) {
+  if (n < 0 || (n > 0 && (!x || !y)) || n > (int64_t(1) << 28)) return NIM_ERR_BAD_ARG;
+  if (n == 0) return NIM_OK;
+  const size_t bytes = (size_t)n * sizeof(double);
+  double *dx = nullptr, *dy = nullptr;
+  int st = NIM_OK;
+  if (cudaMalloc(&dx, bytes) != cudaSuccess || cudaMalloc(&dy, bytes) != cudaSuccess) st = NIM_ERR_CUDA;
+  if (st == NIM_OK && cudaMemcpy(dx, x, bytes, cudaMemcpyHostToDevice) != cudaSuccess) st = NIM_ERR_CUDA;
+  if (st == NIM_OK) {
+    const int64_t blocks = std::min<int64_t>((n + BLK - 1) / BLK, 148 * 16);
+    k_exp_selftest<<<(unsigned)blocks, BLK>>>(dx, dy, n);
+    if (cudaGetLastError() != cudaSuccess || cudaMemcpy(y, dy, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+      st = NIM_ERR_CUDA;
+  }
+  cudaFree(dx);
+  cudaFree(dy);
+  return st;
+}
+
 extern "C" const char *nim_gpu_profile_name(nim_ctx *x, int32_t k) {
   return (x && k >= 0 && k < (int32_t)x->prof_names.size()) ? x->prof_names[k].c_str() : "";
 }
 
 extern "C" int nim_gpu_nusselt_noalloc(nim_ctx *x, double *out4) {
   if (!x || !out4) return NIM_ERR_BAD_ARG;
-  if (!x->initialized) return NIM_ERR_STATE;
+  // between steps only: inside a step the face temperatures are mid-iteration
+  if (!x->initialized || x->in_step) return NIM_ERR_STATE;
   const Dims &d = x->d;
   const int nr = 2 * d.NT * d.NZ;
   if (nr > NIM_NOALLOC_MAX_WALL_FACES) return NIM_ERR_BAD_ARG;
-  double *scratch = (x->device >= 0 && x->device < kMaxDevices) ? g_noalloc_ptr[x->device] : nullptr;
-  if (!scratch) return NIM_ERR_STATE;
   CK(cudaSetDevice(x->device));
+  TRY(noalloc_setup(x->device));
+  double *scratch = g_noalloc_ptr[x->device];
+  if (!scratch) return NIM_ERR_STATE;
   const int gn = grid(nr);
   Fields F = x->F;
   F.part = scratch;  // per-block partials into the static array

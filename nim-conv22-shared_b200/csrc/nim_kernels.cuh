@@ -2,8 +2,9 @@
 //
 // Each kernel restates one or more reference routines; the file:line of the
 // routine is given at the kernel.  Arithmetic follows the reference's
-// expression order (built with -fmad=false, IEEE division/sqrt) so every value
-// matches the CPU oracle's parallel schedule up to the last bit of exp().
+// expression order (built with -fmad=false, IEEE division/sqrt, and nim_exp,
+// which gives glibc's exp bit for bit) so every value matches the CPU
+// oracle's parallel schedule to the last bit.
 //
 // Iteration schedule (one pass of integrate_nse, nse.f90:131-160), parity
 // par = ctrl->iter & 1 selects the current half of every double-buffered face
@@ -29,6 +30,7 @@
 #include <cuda.h>  // CUtensorMap (the maps are encoded by the host)
 
 #include "nim_common.cuh"
+#include "nim_exp.cuh"
 
 namespace nim {
 
@@ -622,7 +624,7 @@ __device__ __forceinline__ void nim_direction(double u, double k, double gminus,
   const double a = 1.;
   const double Re = 2 * a * u / k;
   if (fabs(Re) > v_limit) {
-    const double e = exp(Re);
+    const double e = nim_exp(Re);
     A[0] = (2 * a / (k * (1. / e - 1.)) + 1. / u) * gplus;
     A[1] = (-(2 * a / (k * (1. - e))) - 1. / u) * gminus;
     A[2] = (u / (k * (1. / e - 1.))) * gplus;
@@ -743,7 +745,7 @@ __device__ __forceinline__ Nim1 nim1_direction(double u, double F, double Re, do
     r.J = -(a / F) + (u) / (3. * K[2]) - (U[3]) / (45. * K[4]) + -((2 * U[5]) / (945. * K[6])) -
           (U[7]) / (4725. * K[8]) + -((2 * U[9]) / (93555. * K[10]));
   } else {
-    const double e = exp(Re);
+    const double e = nim_exp(Re);
     r.B = 1. / u * (1. / Re - 1. / (e - 1.));
     r.C = (-(1. / u) + 2. * r.B) * a;
     r.G = u / F / (1. - 1. / e);
@@ -1102,6 +1104,12 @@ __global__ void k_wait_selftest(Ctrl *ctl, int tries) {
   mbar_init(&bar, 1);
   mbar_expect_tx(&bar, 16);
   mbar_wait(&bar, 0, ctl, tries);
+}
+
+// nim_exp over n arguments (self-test of the exp the NIM coefficients use)
+__global__ void k_exp_selftest(const double *x, double *y, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = nim_exp(x[i]);
 }
 
 __device__ __forceinline__ double errv(double nw, double old, bool first) { return fabs(nw - (first ? 0.0 : old)); }

@@ -190,3 +190,34 @@ def test_slabs_with_tiled_face_sweep(monkeypatch):
         nk = g.lib.nim_gpu_profile_iterations(h, 1, ms, 32)
         assert nk > 0
         assert "k_vel_face_tile" in [g.lib.nim_gpu_profile_name(h, k).decode() for k in range(nk)]
+
+
+def test_nusselt_noalloc_on_slabs_combines_to_whole_mesh():
+    """nim_gpu_nusselt_noalloc on a z-slab context sums over the slab's owned
+    planes only: the slabs' Nusselt numbers, weighted by their wall areas,
+    give the whole mesh's."""
+    import ctypes as C
+    case = config.small_case(16, 12, 12, Ra=1e5, steps=2)
+    want_recs, _ = whole(case, case.steps)
+    w = want_recs[-1]
+    mesh = nimgpu.Mesh(case.mesh_params())
+    with nimgpu.SlabGroup(mesh, case.params(**CAP), 2) as g:
+        g.initialize_nse()
+        g.add_temperature_noise(case.noise, case.seed)
+        g.solve_nse(case.steps)
+        parts = []
+        for s in g.slabs:
+            out = (C.c_double * 4)()
+            st = g.lib.nim_gpu_nusselt_noalloc(g._handle(s), out)
+            assert st == _abi.NIM_OK, _abi.strerror(st)
+            parts.append(list(out))
+    area_out = sum(p[2] for p in parts)
+    area_in = sum(p[3] for p in parts)
+    nu_out = sum(p[0] * p[2] for p in parts) / area_out
+    nu_in = sum(p[1] * p[3] for p in parts) / area_in
+    # each slab holds part of each wall, not all of it
+    assert all(0 < p[3] < w.area_inner for p in parts)
+    assert area_out == pytest.approx(w.area_outer, rel=1e-12)
+    assert area_in == pytest.approx(w.area_inner, rel=1e-12)
+    assert nu_out == pytest.approx(w.nu_outer, rel=1e-12)
+    assert nu_in == pytest.approx(w.nu_inner, rel=1e-12)

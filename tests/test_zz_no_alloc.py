@@ -48,4 +48,13 @@ def test_nusselt_noalloc_rejects_bad_arguments():
     assert lib.nim_gpu_nusselt_noalloc(solver._h, None) == _abi.NIM_ERR_BAD_ARG
     out = (C.c_double * 4)()
     assert lib.nim_gpu_nusselt_noalloc(solver._h, out) == _abi.NIM_ERR_STATE  # before init
+    solver.initialize_nse()
+    solver.calculate_velocity_nim_constants()
+    # inside a step the face temperatures are mid-iteration: refused
+    assert lib.nim_gpu_nusselt_noalloc(solver._h, out) == _abi.NIM_ERR_STATE
+    solver.integrate_nse()
+    assert lib.nim_gpu_nusselt_noalloc(solver._h, out) == _abi.NIM_ERR_STATE
+    ref = solver.update_time_step()
+    assert _noalloc(solver) == pytest.approx([ref.nu_outer, ref.nu_inner, ref.area_outer, ref.area_inner],
+                                             rel=1e-12, abs=1e-300)
     solver.close()
