@@ -166,13 +166,12 @@ def cpu_sample(case, threads: int, iters: int, schedule: int):
     """Time `iters` inner iterations of the oracle (the reference's algorithm
     on the CPU) on the same mesh; returns (cell-iterations/s, seconds)."""
     sys.path.insert(0, str(ROOT / "oracle"))
-    import nimgpu
     import oracle as O
-    mesh = nimgpu.Mesh(case.mesh_params())
+    mesh = O.OracleMesh(case.mesh_params())
     o = O.Oracle(mesh, case.params(), schedule=schedule, threads=os.cpu_count() or 1)
     o.init()  # geometry set-up on all cores, not timed
     o.set_threads(threads)
-    nimgpu.apply_temperature_noise(o.get, o.set, mesh, case.noise, case.seed)
+    o.add_temperature_noise(case.noise, case.seed)
     o.begin_step()
     o.iterate(1)  # warm
     t = time.perf_counter()
@@ -197,36 +196,63 @@ def combine_ranks(pg, t, work, device="cuda"):
     return float(tt.item()), float(ww.item())
 
 
+def host_cpu():
+    """Model name and logical CPU count of the host the CPU arms run on."""
+    model = None
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count()}
+
+
 def run_reference(args, rank, world):
-    """--impl reference: the reference algorithm on the host cores."""
+    """--impl reference: the reference algorithm (the oracle port of the
+    Fortran, the checker) on all host cores, with the oracle's own mesh
+    builder and noise (no product library is loaded).  The timed unit is
+    one inner pass of step 1 (the loop body nse.f90:131-160); the per-step
+    work (velocity NIM constants, update_time_step, find_Nu2) is timed
+    once on its own and reported beside it."""
     if rank != 0:
         return 0
-    from nimgpu import config
+    from nimgpu import config  # pure Python: case definitions only
     case = config.CASES[args.case]
     threads = os.cpu_count() or 1
     sys.path.insert(0, str(ROOT / "oracle"))
-    import nimgpu
     import oracle as O
-    mesh = nimgpu.Mesh(case.mesh_params())
+    mesh = O.OracleMesh(case.mesh_params())
     o = O.Oracle(mesh, case.params(), schedule=O.SEQUENTIAL, threads=threads)
     o.init()
-    nimgpu.apply_temperature_noise(o.get, o.set, mesh, case.noise, case.seed)
+    o.add_temperature_noise(case.noise, case.seed)
+    t = time.perf_counter()
     o.begin_step()
+    t_begin = time.perf_counter() - t
     for _ in range(args.warmup):
         o.iterate(1)
     t = time.perf_counter()
     for _ in range(args.steps):
         o.iterate(1)
     dt = time.perf_counter() - t
+    t = time.perf_counter()
+    o.end_step()
+    t_end = time.perf_counter() - t
+    o.close()
     value = case.ncells * args.steps / dt
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "timed_unit": "one inner pass (nse.f90:131-160) of step 1 per timed step",
+        "per_step_work_ms": 1e3 * (t_begin + t_end),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": workload_config(case),
+        "host_cpu": host_cpu(),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} inner iterations of step 1 on {args.case} "
-                                   f"({case.ncells} cells), reference cell order, OpenMP threads={threads}"},
+                         "sample": f"{args.steps} inner passes of step 1 on {args.case} "
+                                   f"({case.ncells} cells), reference cell order, OpenMP threads={threads}; "
+                                   f"per-step work {1e3 * (t_begin + t_end):.0f} ms timed apart"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -531,7 +557,7 @@ def main():
         v, dt = cpu_sample(case, threads=1, iters=4, schedule=0)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                "sample": f"4 inner iterations of step 1 on {args.case} ({case.ncells} cells), "
-                         f"reference cell order, 1 thread ({dt:.1f} s)"}
+                         f"reference cell order, 1 thread ({dt:.1f} s)", "host_cpu": host_cpu()}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -61,6 +61,16 @@ void nim_oracle_nim_coefficients(double u, double k, double gminus, double gplus
    for speed u, diffusivity F and Det = D */
 void nim_oracle_nim1_coefficients(double u, double F, double D, double v_limit, double *out);
 
+/* The oracle's own cylinder mesh (create_hollow + deform_nodes + the
+   renumbering of fill_global_geometry, followed loop by loop): fills
+   arrays sized as nim_mesh_sizes() gives, like nim_mesh_build(), without
+   the library's mesh builder.  0 or -1. */
+struct nim_mesh_params;
+int nim_oracle_mesh_build(const struct nim_mesh_params *p, double *node_xyz, int32_t *meshes_nodes,
+                          int32_t *meshes_faces, int32_t *meshes_neighbors, int32_t *faces_bc,
+                          int32_t *bcs_faces, int32_t *bcs_faces_id, int32_t *bcs_faces_position,
+                          int32_t *bcs_faces_mesh_num);
+
 #ifdef __cplusplus
 }
 #endif

@@ -56,10 +56,67 @@ def lib() -> C.CDLL:
         L.nim_oracle_destroy.restype = None
         L.nim_oracle_set_threads.argtypes = [vp, C.c_int32]
         L.nim_oracle_set_threads.restype = None
+        ip = C.POINTER(C.c_int32)
+        L.nim_oracle_mesh_build.argtypes = [C.POINTER(_abi.MeshParams), C.POINTER(C.c_double)] + [ip] * 8
+        L.nim_oracle_mesh_build.restype = C.c_int
         L.nim_oracle_nim_coefficients.argtypes = [C.c_double] * 5 + [C.POINTER(C.c_double)]
         L.nim_oracle_nim_coefficients.restype = None
         _lib = L
     return _lib
+
+
+class OracleMesh:
+    """The cylinder mesh built by the oracle's own restatement of the
+    reference's mesh set-up (nim_oracle_mesh_build), with the attributes of
+    nimgpu.Mesh; loads no product library."""
+
+    def __init__(self, mp: _abi.MeshParams):
+        n1, n2, n3 = mp.n_theta, mp.n_r, mp.n_z
+        self.params = mp
+        self.n_theta, self.n_r, self.n_z = n1, n2, n3
+        self.nnode = n1 * (n2 + 1) * (n3 + 1)          # parameters.f90:119
+        self.nmesh = n1 * n2 * n3
+        self.nface = 3 * n1 * n2 * n3 + n1 * n3 + n1 * n2  # parameters.f90:117
+        self.nbcface = 2 * n1 * n2 + 2 * n1 * n3
+        self.node_xyz = np.zeros((self.nnode, 3), dtype=np.float64)
+        self.meshes_nodes = np.zeros((self.nmesh, 8), dtype=np.int32)
+        self.meshes_faces = np.zeros((self.nmesh, 6), dtype=np.int32)
+        self.meshes_neighbors = np.zeros((self.nmesh, 6), dtype=np.int32)
+        self.faces_bc = np.zeros(self.nface, dtype=np.int32)
+        self.bcs_faces = np.zeros(self.nbcface, dtype=np.int32)
+        self.bcs_faces_id = np.zeros(self.nbcface, dtype=np.int32)
+        self.bcs_faces_position = np.zeros(self.nbcface, dtype=np.int32)
+        self.bcs_faces_mesh_num = np.zeros(self.nbcface, dtype=np.int32)
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))  # noqa: E731
+        st = lib().nim_oracle_mesh_build(
+            C.byref(mp), self.node_xyz.ctypes.data_as(C.POINTER(C.c_double)), ip(self.meshes_nodes),
+            ip(self.meshes_faces), ip(self.meshes_neighbors), ip(self.faces_bc), ip(self.bcs_faces),
+            ip(self.bcs_faces_id), ip(self.bcs_faces_position), ip(self.bcs_faces_mesh_num))
+        if st != 0:
+            raise ValueError("nim_oracle_mesh_build: bad mesh parameters")
+        d = _abi.MeshDesc()
+        d.n_theta, d.n_r, d.n_z = n1, n2, n3
+        d.nnode, d.nmesh, d.nface, d.nbcface = self.nnode, self.nmesh, self.nface, self.nbcface
+        d.node_xyz = self.node_xyz.ctypes.data_as(C.POINTER(C.c_double))
+        for name in ("meshes_nodes", "meshes_faces", "meshes_neighbors", "faces_bc", "bcs_faces", "bcs_faces_id",
+                     "bcs_faces_position", "bcs_faces_mesh_num"):
+            setattr(d, name, ip(getattr(self, name)))
+        self.desc = d
+
+    @property
+    def interior_faces(self) -> np.ndarray:
+        return self.faces_bc == 1
+
+
+def temperature_noise(mesh, amp: float, seed: int):
+    """The benchmark cases' seeded U(-amp, amp) initial-temperature noise,
+    one value per cell and per interior face (the same draws as the
+    library's host helper, so both sides start from the same state)."""
+    rng = np.random.default_rng(seed)
+    cells = rng.uniform(-amp, amp, size=mesh.nmesh)
+    faces = rng.uniform(-amp, amp, size=mesh.nface)
+    faces[~mesh.interior_faces] = 0.0
+    return cells, faces
 
 
 class Oracle:
@@ -122,6 +179,15 @@ class Oracle:
         a = np.ascontiguousarray(a, dtype=np.float64)
         _abi.check(lib().nim_oracle_set(self._h, field, a.ctypes.data_as(C.POINTER(C.c_double)), a.size),
                    "nim_oracle_set")
+
+    def add_temperature_noise(self, amp: float, seed: int):
+        """The seeded initial-temperature noise of the benchmark cases."""
+        if amp == 0.0:
+            return
+        cells, faces = temperature_noise(self.mesh, amp, seed)
+        self.set(_abi.FACES_T, self.get(_abi.FACES_T, self.mesh.nface) + faces)
+        for f in (_abi.MESHES_T, _abi.MESHES_T_OLD, _abi.MESHES_TT):
+            self.set(f, self.get(f, self.mesh.nmesh) + cells)
 
     def set_threads(self, n: int):
         lib().nim_oracle_set_threads(self._h, n)
