@@ -9,9 +9,15 @@ cells x inner iterations per second.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 runs under torchrun; each rank advances its own replica of the mesh
-(replicas only: no data crosses ranks) and the job value is the sum of all
-ranks' cell-iterations over the slowest rank's device time.
+N > 1 runs under torchrun with one GPU per rank and splits ONE enclosure
+over the ranks: the 256x256x192 cylinder (Ra=1e6, Pr=0.71, dt=2.5e-4) cut
+into N z-slabs (nimgpu.SlabRank: each rank holds its slab plus two halo
+planes per neighbour; after the velocity, pressure and temperature parts of
+every pass the halo planes move to the neighbours over NCCL, and the
+find_error maxima are all-reduced before each pass end).  Strong scaling:
+the job value is the mesh's cell-iterations over the slowest rank's device
+time.  --replicas instead gives every rank its own copy of the --case mesh
+(no data crosses ranks; the job value sums the ranks' work).
 
 --impl reference times the reference algorithm's CPU implementation (the
 oracle port of the Fortran, OpenMP threads as the reference uses them) on
@@ -266,6 +272,121 @@ def workload_config(case):
             "parallelism": "replicas", "l2": "working set > L2 (126 MB): ~3 GB read per pass"}
 
 
+SLAB_CASE = "c3"
+
+
+def run_slab_ranks(args, rank, world, local):
+    """--gpus N > 1: one enclosure split into N z-slabs, one per rank
+    (nimgpu.SlabRank over NCCL).  Every rank runs the same collective
+    sequence; the timed region is bracketed by a barrier and a device
+    synchronisation, and its length is the maximum over the ranks."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    import nimgpu
+    from nimgpu import config, _abi
+
+    torch.cuda.set_device(local)
+    if "MASTER_ADDR" not in os.environ:  # one rank without torchrun (--decompose at N=1)
+        import socket
+        sock = socket.socket()
+        sock.bind(("127.0.0.1", 0))
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(sock.getsockname()[1]), RANK="0",
+                          WORLD_SIZE="1")
+        sock.close()
+    dist.init_process_group("nccl", timeout=timedelta(seconds=180), device_id=torch.device("cuda", local))
+    case = config.CASES[args.case if args.case != CASE else SLAB_CASE]
+    mesh = nimgpu.Mesh(case.mesh_params())
+    r = nimgpu.SlabRank(mesh, case.params())
+    passes = 8
+    try:
+        r.initialize_nse()
+        r.add_temperature_noise(case.noise, case.seed)
+        h = r._h[0]
+        for _ in range(max(args.warmup, 0)):
+            r.solve_nse(1, passes_per_check=passes)
+        dist.barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = int(r.lib.nim_gpu_launch_count(h))
+        ev0.record(r.stream)
+        stats = r.solve_nse(args.steps, passes_per_check=passes)
+        ev1.record(r.stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        launches = int(r.lib.nim_gpu_launch_count(h)) - launches0
+        ms = ev0.elapsed_time(ev1)
+        iters = sum(x.iters for x in stats)
+        t_max, _ = combine_ranks(dist, ms, 0)
+        total = case.ncells * iters  # one mesh: every rank reports the same iterations
+        value = total / (t_max / 1e3)
+        launches_all = combine_ranks(dist, 0.0, launches)[1]
+
+        # end to end: every step each rank uploads its slab's restart arrays
+        # from page-locked host memory, advances one step and downloads them
+        fields = [_abi.FACES_U, _abi.FACES_V, _abi.FACES_W, _abi.FACES_P, _abi.FACES_T,
+                  _abi.MESHES_U, _abi.MESHES_V, _abi.MESHES_W, _abi.MESHES_T,
+                  _abi.MESHES_U_OLD, _abi.MESHES_V_OLD, _abi.MESHES_W_OLD, _abi.MESHES_T_OLD,
+                  _abi.MESHES_UT, _abi.MESHES_VT, _abi.MESHES_WT]
+        host = {f: torch.empty(r.field_size(rank, f), dtype=torch.float64).pin_memory() for f in fields}
+        for f in fields:
+            r.download(rank, f, out=host[f].numpy())
+        h2d = sum(x.numel() * 8 for x in host.values())
+        e2e_steps = max(2, args.steps // 2)
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_iters = 0
+        for _ in range(e2e_steps):
+            for f in fields:
+                r.upload(rank, f, host[f].numpy())
+            st = r.solve_nse(1, passes_per_check=passes)
+            e2e_iters += sum(x.iters for x in st)
+            for f in fields:
+                r.download(rank, f, out=host[f].numpy())
+        torch.cuda.synchronize()
+        e2e_s, h2d_all = combine_ranks(dist, time.perf_counter() - t0, h2d)
+        e2e_value = case.ncells * e2e_iters / e2e_s
+        peak, peak_kind = peaks()
+        per_gpu = ALGO_BYTES_PER_CELL_ITER * total / (t_max / 1e3) / 1e9 / world
+        nt, nr = mesh.n_theta, mesh.n_r
+        halo_doubles = ({name: int(r.lib.nim_slab_pack_doubles(h, st, 1 if rank == 0 else 0))
+                         for name, st in (("velocity", 1), ("pressure", 2), ("temperature", 4))}
+                        if world > 1 else {})
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / max(args.steps, 1), "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded mesh and T noise)",
+            "config": dict(workload_config(case), parallelism=f"z-slabs x{world} (NCCL halo exchange)",
+                           layout=[list(nimgpu.slab_layout(mesh.n_z, world, q)) for q in range(world)]),
+            "iterations": iters, "iters_per_step": iters / max(len(stats), 1),
+            "hbm_gbs_iteration_per_gpu": per_gpu,
+            "halo": {"doubles_per_neighbour_per_pass": halo_doubles,
+                     "bytes_sent_per_neighbour_per_pass": 8 * sum(halo_doubles.values()),
+                     "all_reduces_per_pass": 1, "all_reduce_words": 24, "plane_cells": nt * nr},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_all, "d2h_bytes_per_step": h2d_all,
+                    "steps": e2e_steps},
+            "roofline": {"bound": "hbm", "kernel": "whole pass, per GPU (algorithmic 1880 B per cell-iteration)",
+                         "achieved": per_gpu, "peak": peak, "unit": "GB/s", "frac": per_gpu / peak,
+                         "peak_source": peak_kind, "traffic": None},
+            "cpu_baseline": None,
+            "gpu_launches": launches_all,
+            "clocks": clk,
+            "nu_inner_last": stats[-1].nu_inner if stats else None,
+        }
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        r.close()
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def run_batch(args, rank, world, local):
     """The batched extension: 64 seeded enclosures advanced together by
     nim_batch_step, against the same cases one at a time (nim_gpu_step per
@@ -440,12 +561,18 @@ def main():
                     help="mixed: FP32 passes over a float mirror, then FP64 passes (nim_params.precision)")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
     ap.add_argument("--no-slabs", action="store_true", help="skip the two-slab comparison")
+    ap.add_argument("--replicas", action="store_true",
+                    help="N > 1: every rank advances its own copy of --case (no decomposition)")
+    ap.add_argument("--decompose", action="store_true",
+                    help="run the z-slab decomposition path even at N = 1 (one slab, one rank)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if args.case == "batch":
         return run_batch(args, rank, world, local)
+    if (world > 1 and not args.replicas) or args.decompose:
+        return run_slab_ranks(args, rank, world, local)
 
     import torch
     import nimgpu

@@ -20,20 +20,21 @@ from . import _abi
 from .mesh import Mesh, temperature_noise
 
 
-def slab_layout(n_z: int, nslab: int, s: int) -> tuple[int, int, int, int]:
+def slab_layout(n_z: int, nslab: int, s: int, lib=None) -> tuple[int, int, int, int]:
     """(first plane held, one past the last held, first owned, one past the
     last owned) of slab s, global plane numbers."""
     out = (C.c_int32 * 4)()
-    _abi.check(_abi.gpu_lib().nim_slab_layout(n_z, nslab, s, out), "nim_slab_layout")
+    _abi.check((lib or _abi.gpu_lib()).nim_slab_layout(n_z, nslab, s, out), "nim_slab_layout")
     return tuple(out)
 
 
-def slab_halo(n_theta: int, n_r: int, n_z: int, nslab: int, s: int, side: int):
+def slab_halo(n_theta: int, n_r: int, n_z: int, nslab: int, s: int, side: int, lib=None):
     """(recv, send) element spans of slab s's exchange with its neighbour
     below (side 0) or above (side 1): four (offset, count) pairs each, for
     the cells and the r, theta and z faces of the slab context's arrays."""
     recv, send = (C.c_int64 * 8)(), (C.c_int64 * 8)()
-    _abi.check(_abi.gpu_lib().nim_slab_halo(n_theta, n_r, n_z, nslab, s, side, recv, send), "nim_slab_halo")
+    _abi.check((lib or _abi.gpu_lib()).nim_slab_halo(n_theta, n_r, n_z, nslab, s, side, recv, send),
+               "nim_slab_halo")
     pairs = lambda a: [(a[2 * t], a[2 * t + 1]) for t in range(4)]
     return pairs(recv), pairs(send)
 
@@ -83,11 +84,11 @@ class _Slabs:
     `slabs`), with the host copies between the whole mesh's reference
     layout and the slabs' structured layout."""
 
-    def __init__(self, mesh: Mesh, params: _abi.Params, nslab: int, slabs):
-        self.lib = _abi.gpu_lib()
+    def __init__(self, mesh: Mesh, params: _abi.Params, nslab: int, slabs, lib=None):
+        self.lib = lib or _abi.gpu_lib()
         self.mesh, self.params, self.nslab = mesh, params, nslab
         self.slabs = list(slabs)
-        self.layout = {s: slab_layout(mesh.n_z, nslab, s) for s in self.slabs}
+        self.layout = {s: slab_layout(mesh.n_z, nslab, s, self.lib) for s in self.slabs}
         self._ref = structured_faces(mesh)
         self._h = []
         try:
@@ -135,9 +136,14 @@ class _Slabs:
         lo, hi = self.layout[s][:2]
         return slab_sizes(self.mesh.n_theta, self.mesh.n_r, hi - lo)
 
-    def download(self, s: int, field: int) -> np.ndarray:
+    def field_size(self, s: int, field: int) -> int:
+        """Doubles of `field` in slab s's context (its held planes)."""
         nc, nf = self._sizes(s)
-        out = np.empty(nf if field <= _abi.FACES_T else nc, dtype=np.float64)
+        return nf if field <= _abi.FACES_T else nc
+
+    def download(self, s: int, field: int, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.field_size(s, field), dtype=np.float64)
         _abi.check(self.lib.nim_gpu_download(self._handle(s), field, out.ctypes.data_as(C.POINTER(C.c_double)),
                                              out.size), "nim_gpu_download")
         return out
@@ -255,22 +261,30 @@ class SlabRank(_Slabs):
     on the context's stream, then the halo exchange over the group (packed
     by nim_slab_pack, one message per neighbour: exchange_packed), the
     maxima's all-reduce before every pass end, and the
-    step-end sums reduced over the group."""
+    step-end sums reduced over the group.
 
-    def __init__(self, mesh: Mesh, params: _abi.Params, group=None):
+    Every rank takes the same collective steps in the same order: the stop
+    decision of each pass comes from maxima all-reduced over the group, so
+    every rank reads the same `done` and leaves the loop after the same
+    pass.  `lib` and `device` exist for testing the control flow on the CPU
+    (a stand-in for the library's slab entry points and CPU tensors over a
+    gloo group); by default the CUDA library and the current GPU."""
+
+    def __init__(self, mesh: Mesh, params: _abi.Params, group=None, lib=None, device=None):
         import torch
         import torch.distributed as dist
         self._dist, self._group = dist, group
         self.rank, self.world = dist.get_rank(group), dist.get_world_size(group)
-        super().__init__(mesh, params, self.world, [self.rank])
+        super().__init__(mesh, params, self.world, [self.rank], lib=lib)
         h = self._h[0]
-        self.device = torch.device("cuda", torch.cuda.current_device())
-        self.stream = torch.cuda.ExternalStream(int(self.lib.nim_gpu_stream(h)), device=self.device)
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        self.stream = (torch.cuda.ExternalStream(int(self.lib.nim_gpu_stream(h)), device=self.device)
+                       if self.device.type == "cuda" else None)
         self.plans = {}
         if self.rank > 0:
-            self.plans[0] = slab_halo(mesh.n_theta, mesh.n_r, mesh.n_z, self.world, self.rank, 0)
+            self.plans[0] = slab_halo(mesh.n_theta, mesh.n_r, mesh.n_z, self.world, self.rank, 0, self.lib)
         if self.rank < self.world - 1:
-            self.plans[1] = slab_halo(mesh.n_theta, mesh.n_r, mesh.n_z, self.world, self.rank, 1)
+            self.plans[1] = slab_halo(mesh.n_theta, mesh.n_r, mesh.n_z, self.world, self.rank, 1, self.lib)
         # packed send / receive buffers per exchange set and side
         self._send, self._recv = {}, {}
         for st in (HALO_VELOCITY, HALO_PRESSURE, HALO_TEMPERATURE, HALO_STATE):
@@ -283,8 +297,16 @@ class SlabRank(_Slabs):
                 self._recv[st][side] = torch.empty(n, dtype=torch.float64, device=self.device)
         slots = C.c_void_p()
         _abi.check(self.lib.nim_slab_maxima(h, C.byref(slots)), "nim_slab_maxima")
-        self._maxima = _device_tensor(slots.value, 24, "<i8", self.device)
+        self._maxima = (_device_tensor(slots.value, 24, "<i8", self.device) if self.device.type == "cuda"
+                        else torch.frombuffer((C.c_int64 * 24).from_address(slots.value), dtype=torch.int64))
         self._step, self._time = 1, params.DT
+
+    def _on_stream(self):
+        """The context's stream as torch's current stream (CUDA), so the
+        collectives are ordered with the library's kernels."""
+        import contextlib
+        import torch
+        return torch.cuda.stream(self.stream) if self.stream is not None else contextlib.nullcontext()
 
     def close(self):
         self._send, self._recv, self._maxima = {}, {}, None
@@ -299,14 +321,13 @@ class SlabRank(_Slabs):
         h, send, recv = self._h[0], self._send[what], self._recv[what]
         for side, buf in send.items():
             _abi.check(self.lib.nim_slab_pack(h, what, side, C.c_void_p(buf.data_ptr())), "nim_slab_pack")
-        with torch.cuda.stream(self.stream):
+        with self._on_stream():
             exchange_packed(send, recv, self.rank, self._group)
         for side, buf in recv.items():
             _abi.check(self.lib.nim_slab_unpack(h, what, side, C.c_void_p(buf.data_ptr())), "nim_slab_unpack")
 
     def _merge(self):
-        import torch
-        with torch.cuda.stream(self.stream):
+        with self._on_stream():
             self._dist.all_reduce(self._maxima, op=self._dist.ReduceOp.MAX, group=self._group)
 
     def _reduce(self, values, op):
