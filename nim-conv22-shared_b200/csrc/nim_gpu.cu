@@ -199,6 +199,10 @@ int verify_mesh(const nim_mesh_desc *m, const Dims &d, std::vector<int> &perm) {
   const int NT = d.NT, NR = d.NR, NZ = d.NZ;
   if ((int64_t)NT * (NR + 1) * (NZ + 1) != m->nnode || d.Nc != m->nmesh || d.NF != m->nface || d.NBF != m->nbcface)
     return NIM_ERR_BAD_ARG;
+  // The sweep kernels index with 32-bit integers (fewer registers, so fewer
+  // spills); their largest offset is 19 x the cell count (MT_A, 18 rows).
+  // 2^31 / 20 = 107 M cells is beyond what one GPU's memory holds in FP64.
+  if ((int64_t)d.Nc * 20 >= (int64_t)INT32_MAX) return NIM_ERR_BAD_ARG;
   perm.assign(d.NF, -1);
   std::vector<char> seen(d.NF, 0);
   for (int c = 0; c < d.Nc; ++c) {

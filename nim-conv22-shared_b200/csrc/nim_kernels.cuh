@@ -655,8 +655,8 @@ __device__ __forceinline__ void nim_direction(double u, double k, double gminus,
 
 // contravariant component dd (1..3) of a Cartesian velocity in cell c
 template <class R>
-__device__ __forceinline__ double contravariant(const R *xi, size_t Nc, int c, int dd, double u, double v, double w) {
-  return u * xi[(size_t)(dd - 1 + 0) * Nc + c] + v * xi[(size_t)(dd - 1 + 3) * Nc + c] + w * xi[(size_t)(dd - 1 + 6) * Nc + c];
+__device__ __forceinline__ double contravariant(const R *xi, int Nc, int c, int dd, double u, double v, double w) {
+  return u * xi[(dd - 1 + 0) * Nc + c] + v * xi[(dd - 1 + 3) * Nc + c] + w * xi[(dd - 1 + 6) * Nc + c];
 }
 
 // calculate_velocity_nim_constants_formulation2, first pass (nim.f90:165-289)
@@ -1206,7 +1206,7 @@ struct Pair2<float> {
 };
 // p[i], p[i+1] for an even element index i (a 2 x sizeof(R)-aligned pair)
 template <class R>
-__device__ __forceinline__ void ld2(const R *__restrict__ p, size_t i, R &a, R &b) {
+__device__ __forceinline__ void ld2(const R *__restrict__ p, int i, R &a, R &b) {
   const typename Pair2<R>::T v = *reinterpret_cast<const typename Pair2<R>::T *>(p + i);
   a = v.x;
   b = v.y;
@@ -1220,6 +1220,10 @@ __device__ __forceinline__ double tang_vals(bool lo, bool hi, double v0, double 
   return (vp1 - vm1) / 4.;
 }
 
+// Index arithmetic here is 32-bit (its largest offset is 9 x the cell count;
+// nim_gpu_create refuses meshes for which 19 x the cell count would not fit
+// an int): 64-bit offsets took registers that the kernel's bound of 56
+// turned into spills (184 bytes against 108).
 // SLAB: a z-slab context, whose maxima skip the planes a neighbour owns (a
 // separate instantiation: at this kernel's register bound the test alone
 // costs spills)
@@ -1236,13 +1240,13 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
   const int k = blockIdx.z;
   double e[3] = {0., 0., 0.};
   if (i < d.NT && j < d.NR) {
-    const size_t Nc = d.Nc, NF = d.NF, NT = d.NT, NR = d.NR, pl = d.plane;
-    const size_t c = (size_t)i + NT * (j + NR * k);  // cell i; the pair's second cell is c + 1
+    const int Nc = d.Nc, NF = d.NF, NT = d.NT, NR = d.NR, pl = d.plane;
+    const int c = i + NT * (j + NR * k);  // cell i; the pair's second cell is c + 1
     const int im1 = (i == 0) ? d.NT - 1 : i - 1, ip2 = (i + 2 >= d.NT) ? i + 2 - d.NT : i + 2;
     // face m of cell i at fi[m]; of cell i+1 at fi[m] + 1, except face 4: f4b
-    const size_t f1 = c + NT * k;
-    const size_t fi[7] = {0, f1, f1 + NT, d.offT + c, d.offT + c + 1, d.offZ + c, d.offZ + c + pl};
-    const size_t f4b = d.offT + c - i + ip2;
+    const int f1 = c + NT * k;
+    const int fi[7] = {0, f1, f1 + NT, d.offT + c, d.offT + c + 1, d.offZ + c, d.offZ + c + pl};
+    const int f4b = d.offT + c - i + ip2;
     // face m of both cells from array a (pairs; faces 3 and 4 share one pair)
     auto face2 = [&](const R *a, int m, R &v0, R &v1) {
       if (m == 4) {
@@ -1327,19 +1331,19 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
     }
     auto term = [&](int slot, double d0, double d1) {
       R a0, a1;
-      ld2(g.gij + (size_t)slot * Nc, c, a0, a1);
+      ld2(g.gij + slot * Nc, c, a0, a1);
       s0 = s0 - a0 * d0;
       s1 = s1 - a1 * d1;
     };
     {  // pxy: r faces (rows j, j+1) at theta i-1, i+2 (centred in theta)
-      const size_t rrow = NT * (j + (NR + 1) * k);
+      const int rrow = NT * (j + (NR + 1) * k);
       const double r_m1 = fr[rrow + im1], r_p2 = fr[rrow + ip2];
       const double r1_m1 = fr[rrow + NT + im1], r1_p2 = fr[rrow + NT + ip2];
       term(3, 0.5 * (((double)o1[2] - r1_m1) / 4. - ((double)o1[1] - r_m1) / 4.),
            0.5 * ((r1_p2 - (double)o0[2]) / 4. - (r_p2 - (double)o0[1]) / 4.));
     }
     {  // pyx: theta faces of rows a, b
-      const size_t tra = d.offT + NT * (ra + NR * k), trb = d.offT + NT * (rb + NR * k);
+      const int tra = d.offT + NT * (ra + NR * k), trb = d.offT + NT * (rb + NR * k);
       R a0, a1, b0, b1;
       ld2(fr, tra + i, a0, a1);
       ld2(fr, trb + i, b0, b1);
@@ -1348,7 +1352,7 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
            0.5 * (along(rlo, rhi, o1[4], a2, b2) - along(rlo, rhi, o1[3], a1, b1)));
     }
     {  // pxz: r faces (rows j, j+1) of planes a, b
-      const size_t rka = NT * (j + (NR + 1) * ka), rkb = NT * (j + (NR + 1) * kb);
+      const int rka = NT * (j + (NR + 1) * ka), rkb = NT * (j + (NR + 1) * kb);
       R pa0, pa1, pb0, pb1, pA0, pA1, pB0, pB1;
       ld2(fr, rka + i, pa0, pa1);
       ld2(fr, rkb + i, pb0, pb1);
@@ -1358,7 +1362,7 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
            0.5 * (along(zlo, zhi, o1[2], pA1, pB1) - along(zlo, zhi, o1[1], pa1, pb1)));
     }
     {  // pzx: z faces (levels k, k+1) of rows a, b
-      const size_t zra = d.offZ + NT * (ra + NR * k), zrb = d.offZ + NT * (rb + NR * k);
+      const int zra = d.offZ + NT * (ra + NR * k), zrb = d.offZ + NT * (rb + NR * k);
       R za0, za1, zb0, zb1, zA0, zA1, zB0, zB1;
       ld2(fr, zra + i, za0, za1);
       ld2(fr, zrb + i, zb0, zb1);
@@ -1368,7 +1372,7 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
            0.5 * (along(rlo, rhi, o1[6], zA1, zB1) - along(rlo, rhi, o1[5], za1, zb1)));
     }
     {  // pyz: theta faces of planes a, b
-      const size_t tka = d.offT + NT * (j + NR * ka), tkb = d.offT + NT * (j + NR * kb);
+      const int tka = d.offT + NT * (j + NR * ka), tkb = d.offT + NT * (j + NR * kb);
       R a0, a1, b0, b1;
       ld2(fr, tka + i, a0, a1);
       ld2(fr, tkb + i, b0, b1);
@@ -1377,7 +1381,7 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
            0.5 * (along(zlo, zhi, o1[4], a2, b2) - along(zlo, zhi, o1[3], a1, b1)));
     }
     {  // pzy: z faces (levels k, k+1) at theta i-1, i+2
-      const size_t zlev = d.offZ + NT * (j + NR * k);
+      const int zlev = d.offZ + NT * (j + NR * k);
       const double z_m1 = fr[zlev + im1], z_p2 = fr[zlev + ip2];
       const double z1_m1 = fr[zlev + pl + im1], z1_p2 = fr[zlev + pl + ip2];
       term(5, 0.5 * (((double)o1[6] - z1_m1) / 4. - ((double)o1[5] - z_m1) / 4.),
@@ -1396,7 +1400,7 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
     double u0 = +a0 * (double)co0, u1 = +a1 * (double)co1;
 #pragma unroll
     for (int m = 2; m <= 7; ++m) {
-      ld2(F.MF4 + (size_t)m * Nc, c, a0, a1);
+      ld2(F.MF4 + m * Nc, c, a0, a1);
       u0 = u0 + a0 * (double)o0[m - 1];
       u1 = u1 + a1 * (double)o1[m - 1];
     }
@@ -2002,7 +2006,7 @@ template <class Ld, class R>
 __device__ __forceinline__ double p_bc_value(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P,
                                              const R *pr, const R *fu, const R *fv, const R *fwv, const R *fT,
                                              int b) {
-  const size_t NF = d.NF, NB = d.NBF;
+  const int NF = d.NF, NB = d.NBF;
   const BFace B = bface(d, b);
   const Cell M1 = B.cell;
   const int pos = B.pos;
@@ -2048,7 +2052,7 @@ __global__ void __launch_bounds__(BLK) k_p_bc(Dims d, GeoT<R> g, FieldsT<R> F, P
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   double e[1] = {0.};
   if (b < d.NBF) {
-    const size_t NF = d.NF;
+    const int NF = d.NF;
     const R *pr = F.f[3] + par * NF;
     const double nw = stored<R>(p_bc_value<LdPlain>(d, g, F, P, pr, F.f[0] + nh * NF, F.f[1] + nh * NF,
                                                     F.f[2] + nh * NF, F.f[4] + par * NF, b));
@@ -2068,7 +2072,7 @@ __global__ void k_p_bc_copy(Dims d, FieldsT<R> F, Ctrl *ctl) {
   if (b >= d.NBF) return;
   const BFace B = bface(d, b);
   const int f = B.cell.face(d, B.pos);
-  F.f[3][par * (size_t)d.NF + f] = F.f[3][(1 - par) * (size_t)d.NF + f];
+  F.f[3][par * d.NF + f] = F.f[3][(1 - par) * d.NF + f];
 }
 
 // (coefficient, face, cell) of the ten off-diagonal terms of the pressure
@@ -2240,7 +2244,7 @@ __global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, GeoT<R> g, FieldsT<R>
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   double e[1] = {0.};
   if (b < 2 * d.plane) {
-    const size_t NF = d.NF, NB = d.NBF;
+    const int NF = d.NF, NB = d.NBF;
     const BFace B = bface(d, b);
     const int in = (B.pos == 5) ? 6 : 5;
     const Cell c2 = B.cell.nb(d, in), c3 = c2.nb(d, in);
@@ -2267,15 +2271,15 @@ __global__ void __launch_bounds__(BLK, 4) k_T_coef(Dims d, GeoT<R> g, FieldsT<R>
   const int c = blockIdx.y * BLK + threadIdx.x;
   if (c >= d.Nc) return;
   const int dd = blockIdx.x + 1;
-  const size_t Nc = d.Nc;
+  const int Nc = d.Nc;
   const double ut = 0.5 * (F.c[0][c] + F.co[0][c]);
   const double vt = 0.5 * (F.c[1][c] + F.co[1][c]);
   const double wt = 0.5 * (F.c[2][c] + F.co[2][c]);
   const double u = contravariant(g.xi, Nc, c, dd, ut, vt, wt);
   double A[6];
-  nim_direction(u, g.gij[(size_t)(dd - 1 + 3 * (dd - 1)) * Nc + c] * P.alpha, g.gfd[(2 * (dd - 1)) * Nc + c],
+  nim_direction(u, g.gij[(dd - 1 + 3 * (dd - 1)) * Nc + c] * P.alpha, g.gfd[(2 * (dd - 1)) * Nc + c],
                 g.gfd[(2 * (dd - 1) + 1) * Nc + c], P.v_limit, A);
-  for (int q = 0; q < 6; ++q) F.MTA[(size_t)(3 * q + dd - 1) * Nc + c] = A[q];
+  for (int q = 0; q < 6; ++q) F.MTA[(3 * q + dd - 1) * Nc + c] = A[q];
 }
 
 // ---- K7b: the rest of calculate_temperature_nim_constants_formulation2
@@ -2379,14 +2383,14 @@ __global__ void __launch_bounds__(BLK, 4) k_T_face(Dims d, GeoT<R> g, FieldsT<R>
   const int c = x.c;
   double e[1] = {0.};
   if (act) {
-    const size_t Nc = d.Nc, NF = d.NF;
+    const int Nc = d.Nc, NF = d.NF;
     const R *T = F.f[4] + par * NF;
     R *Tn = F.f[4] + (1 - par) * NF;
     for (int dd = 1; dd <= 3; ++dd) {
       if (!x.has_nb(d, 2 * dd)) continue;
       const Cell x2 = x.nb(d, 2 * dd);
       double Fd[5];
-      for (int k = 0; k < 5; ++k) Fd[k] = F.MTF[(size_t)(5 * (dd - 1) + k) * Nc + c];
+      for (int k = 0; k < 5; ++k) Fd[k] = F.MTF[(5 * (dd - 1) + k) * Nc + c];
       const int fo = x.face(d, 2 * dd);
       const double nw = stored<R>(face_update(d, T, F.c[3], F.co[3], Fd, g.dg[(2 * (dd - 1)) * Nc + c],
                                               g.dg[(2 * (dd - 1) + 1) * Nc + c], dd, x, x2, P.w[3]));
