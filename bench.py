@@ -85,11 +85,12 @@ KERNEL_BYTES_PER_CELL = {
 # dram__bytes_write.sum, one --set full capture each); traffic grows with the
 # cells, so roofline.traffic scales these to the run's mesh
 NCU_DRAM_BYTES_PER_CELL = {
-    "k_vel_cell": 425.2, "k_p_src": 324.4, "k_p_face": 420.2, "k_T_coef": 317.0, "k_T_cell": 389.6,
-    "k_T_face": 227.3, "k_vel_face_tile": 361.4, "k_vel_face": 343.1, "k_vel_cell2": 500.4,
+    "k_vel_cell": 425.2, "k_p_src": 324.4, "k_p_face": 420.2, "k_T_coef": 276.9, "k_T_cell": 389.6,
+    "k_T_face": 227.3, "k_vel_face_tile": 361.4, "k_vel_face": 343.1, "k_vel_cell2": 441.0,
 }
 NCU_CAPTURE = {k: "128x128x96" for k in NCU_DRAM_BYTES_PER_CELL}
-NCU_CAPTURE["k_vel_face"] = "96x96x64"
+for _k in ("k_vel_face", "k_vel_cell2", "k_T_coef"):
+    NCU_CAPTURE[_k] = "96x96x64"
 # algorithmic bytes per cell-iteration and per cell-step of the whole pass
 # (FP64, every array read and written once, implicit connectivity)
 ALGO_BYTES_PER_CELL_ITER = 1880

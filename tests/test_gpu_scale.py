@@ -6,9 +6,9 @@ run on the CPU).
 * the parallel order (the kernels' order) on the 48x48x32 cylinder for all
   200 steps of its run and on the 128x128x96 cylinder for 20 steps: the same
   iteration count and the same find_error maxima every step, the fields
-  bit-identical to the oracle's at the recorded steps, and the Nusselt
-  numbers, dilatation and steady-state maxima to 1e-12 relative (the GPU
-  sums them in another order);
+  bit-identical to the oracle's at the recorded steps, the steady-state
+  maxima exactly, and the Nusselt numbers to 1e-12 and the dilatation to
+  1e-10 relative (the GPU sums them in another order);
 * the reference's own Gauss-Seidel order (NIM_SCHEDULE_REFERENCE) on the
   48x48x32 cylinder against the sequential oracle: the same per-step
   history and bit-identical fields.
@@ -32,8 +32,10 @@ FIELDS = {"faces_u": _abi.FACES_U, "faces_v": _abi.FACES_V, "faces_w": _abi.FACE
           "faces_T": _abi.FACES_T, "meshes_u": _abi.MESHES_U, "meshes_v": _abi.MESHES_V,
           "meshes_w": _abi.MESHES_W, "meshes_T": _abi.MESHES_T, "meshes_p": _abi.MESHES_P}
 EXACT = ("iters", "err_u", "err_v", "err_w", "err_p", "err_T", "dudt_max", "dTdt_max", "time")
-CLOSE = ("dilatation", "nu_outer", "nu_inner", "area_outer", "area_inner")
-RTOL = 1e-12
+# sums the device forms in another order than the oracle: the wall integrals
+# of find_Nu2 (a few thousand terms) to 1e-12; evaluate_D's root of a sum
+# of one squared residual per cell (1.6 M at 128x128x96) to 1e-10
+CLOSE = {"nu_outer": 1e-12, "nu_inner": 1e-12, "area_outer": 1e-12, "area_inner": 1e-12, "dilatation": 1e-10}
 
 
 def load(name):
@@ -70,9 +72,9 @@ def run_and_compare(golden: dict, schedule: int):
         assert r.status == _abi.NIM_OK, (s, _abi.strerror(r.status))
         for k in EXACT:
             assert getattr(r, k) == per[k][s - 1], (s, k, getattr(r, k), per[k][s - 1])
-        for k in CLOSE:
+        for k, rtol in CLOSE.items():
             want = per[k][s - 1]
-            assert abs(getattr(r, k) - want) <= RTOL * abs(want) + 1e-300, (s, k, getattr(r, k), want)
+            assert abs(getattr(r, k) - want) <= rtol * abs(want) + 1e-300, (s, k, getattr(r, k), want)
         if str(s) in golden["fields"]:
             check_fields(solver, golden["fields"][str(s)], s)
     solver.close()
