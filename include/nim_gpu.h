@@ -429,6 +429,17 @@ int nim_gpu_selftest_wait_timeout(nim_ctx *ctx, int32_t tries);
    exponential NIM coefficients, nim.f90:190-194, call it). */
 int nim_gpu_selftest_exp(const double *x, double *y, int64_t n);
 
+/* Self-test of the temperature's NIM coefficients of one direction
+   (nim.f90:334-464, with gminus = gplus = 1): A[6i + q] = coefficient q+1
+   for the contravariant velocity u[i] and diffusion coefficient k[i] > 0,
+   n <= 2^26.  precision NIM_PRECISION_FP64: the FP64 path's form (series
+   below |2u/k| = v_limit, exponential above, as the reference);
+   NIM_PRECISION_MIXED: the float form of the FP32 phase (no counterpart in
+   the reference), which must stay within a few 1e-7 of the FP64 values
+   relative.  Allocates and frees its device buffers; default stream. */
+int nim_gpu_selftest_nim_coef(const double *u, const double *k, int64_t n, int32_t precision, double v_limit,
+                              double *A);
+
 /* Wall-face limit of nim_gpu_nusselt_noalloc: 2*n_theta*n_z inner plus
    outer wall faces, i.e. 4096 blocks of 256 faces. */
 #define NIM_NOALLOC_MAX_WALL_FACES 1048576

@@ -2145,6 +2145,32 @@ extern "C" int nim_gpu_selftest_exp(const double *x, double *y, int64_t n) {
   return st;
 }
 
+extern "C" int nim_gpu_selftest_nim_coef(const double *u, const double *k, int64_t n, int32_t precision,
+                                         double v_limit, double *A) {
+  if (n < 0 || (n > 0 && (!u || !k || !A)) || n > (int64_t(1) << 26)) return NIM_ERR_BAD_ARG;
+  if (precision != NIM_PRECISION_FP64 && precision != NIM_PRECISION_MIXED) return NIM_ERR_BAD_ARG;
+  if (n == 0) return NIM_OK;
+  const size_t bytes = (size_t)n * sizeof(double);
+  double *du = nullptr, *dk = nullptr, *dA = nullptr;
+  int st = NIM_OK;
+  if (cudaMalloc(&du, bytes) != cudaSuccess || cudaMalloc(&dk, bytes) != cudaSuccess ||
+      cudaMalloc(&dA, 6 * bytes) != cudaSuccess)
+    st = NIM_ERR_CUDA;
+  if (st == NIM_OK && (cudaMemcpy(du, u, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+                       cudaMemcpy(dk, k, bytes, cudaMemcpyHostToDevice) != cudaSuccess))
+    st = NIM_ERR_CUDA;
+  if (st == NIM_OK) {
+    const int64_t blocks = std::min<int64_t>((n + BLK - 1) / BLK, 148 * 16);
+    k_nim_coef_selftest<<<(unsigned)blocks, BLK>>>(du, dk, dA, n, precision == NIM_PRECISION_MIXED, v_limit);
+    if (cudaGetLastError() != cudaSuccess || cudaMemcpy(A, dA, 6 * bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+      st = NIM_ERR_CUDA;
+  }
+  cudaFree(du);
+  cudaFree(dk);
+  cudaFree(dA);
+  return st;
+}
+
 extern "C" const char *nim_gpu_profile_name(nim_ctx *x, int32_t k) {
   return (x && k >= 0 && k < (int32_t)x->prof_names.size()) ? x->prof_names[k].c_str() : "";
 }

@@ -28,6 +28,7 @@
 #pragma once
 #include <cooperative_groups.h>
 #include <cuda.h>  // CUtensorMap (the maps are encoded by the host)
+#include <type_traits>
 
 #include "nim_common.cuh"
 #include "nim_exp.cuh"
@@ -74,7 +75,7 @@ struct FieldsT {
   R *MF4;     // [8][Nc]
   R *MF;      // [15][Nc]  M_F1..3(k) at 5(d-1)+k-1
   R *MTF;     // [15][Nc]  MT_F1..3
-  R *MTA;     // [18][Nc]  MT_A(q, d) at 3(q-1) + d-1
+  R *MTA;     // [18][Nc]  MT_A(q, d) at 3(q-1) + d-1 (float: 1/MT_A(5, d) at q = 5)
   R *dpd;     // [3][Nc]   dpdx_old, dpdy_old, dpdz_old
   // reference-order schedule: sources stored before the ordered sweeps
   R *Bv;      // [3][Nc]   R_C + R_D + R_B of u, v, w
@@ -653,6 +654,76 @@ __device__ __forceinline__ void nim_direction(double u, double k, double gminus,
   }
 }
 
+// The temperature's NIM coefficients in float for the FP32 phase.  With
+// x = 2u/k (the cell Reynolds number) every coefficient follows from
+// h(x) = (x/(e^x-1) - 1 + x/2)/x^2 = sum_{n>=1} B_2n x^(2n-2)/(2n)!:
+//   A0 = (-1 - 2xh)/k gplus    A1 = (-1 + 2xh)/k gminus
+//   A2 = -(1 + x/2 + x^2 h)/2 gplus   A3 = -(1 - x/2 + x^2 h)/2 gminus
+//   A4 = 4h/k                  A5 = 1/2 + xh
+// (the exact functions the exp form of nim_direction evaluates).  For
+// |x| <= 2 h is its Taylor series to x^14 (truncation below 1e-8); above,
+// the exp form, which has no cancellation there.  Both keep every
+// coefficient within ~1e-6 of the exact value (the FP64 forms lose ~1e-2 in
+// float near |x| = v_limit).
+__device__ __forceinline__ void nim_direction_f32(float u, float k, float gminus, float gplus, float A[6]) {
+  const float ik = 1.f / k;
+  const float x = 2.f * u * ik;
+  if (fabsf(x) <= 2.f) {
+    const float y = x * x;
+    float h = -3617.f / 10670622842880000.f;
+    h = fmaf(h, y, 1.f / 74724249600.f);
+    h = fmaf(h, y, -691.f / 1307674368000.f);
+    h = fmaf(h, y, 1.f / 47900160.f);
+    h = fmaf(h, y, -1.f / 1209600.f);
+    h = fmaf(h, y, 1.f / 30240.f);
+    h = fmaf(h, y, -1.f / 720.f);
+    h = fmaf(h, y, 1.f / 12.f);
+    const float xh = x * h, yh = y * h;
+    A[0] = (-1.f - 2.f * xh) * ik * gplus;
+    A[1] = (-1.f + 2.f * xh) * ik * gminus;
+    A[2] = -0.5f * (1.f + 0.5f * x + yh) * gplus;
+    A[3] = -0.5f * (1.f - 0.5f * x + yh) * gminus;
+    A[4] = 4.f * h * ik;
+    A[5] = 0.5f + xh;
+  } else {
+    const float e = expf(x), ie = 1.f / e;
+    A[0] = (2.f / (k * (ie - 1.f)) + 1.f / u) * gplus;
+    A[1] = (-(2.f / (k * (1.f - e))) - 1.f / u) * gminus;
+    A[2] = (u / (k * (ie - 1.f))) * gplus;
+    A[3] = (u / (k * (1.f - e))) * gminus;
+    if (x > 0) {
+      A[4] = (-k + u * (ie + 1.f) / (1.f - ie)) / (u * u);
+      A[5] = 1.f / (1.f - ie) - 1.f / x;
+    } else {
+      A[4] = (-k + u * (1.f + e) / (e - 1.f)) / (u * u);
+      A[5] = e / (e - 1.f) - 1.f / x;
+    }
+  }
+}
+
+__global__ void k_exp_selftest(const double *x, double *y, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = nim_exp(x[i]);
+}
+
+// the six NIM coefficients of one direction (gminus = gplus = 1) for n
+// (u, k) pairs: the FP64 form of the FP64 path or the float form of the
+// FP32 phase; A[6i + q]
+__global__ void k_nim_coef_selftest(const double *u, const double *k, double *A, int64_t n, int lowp,
+                                    double v_limit) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (lowp) {
+      float a[6];
+      nim_direction_f32((float)u[i], (float)k[i], 1.f, 1.f, a);
+      for (int q = 0; q < 6; ++q) A[6 * i + q] = a[q];
+    } else {
+      double a[6];
+      nim_direction(u[i], k[i], 1., 1., v_limit, a);
+      for (int q = 0; q < 6; ++q) A[6 * i + q] = a[q];
+    }
+  }
+}
+
 // contravariant component dd (1..3) of a Cartesian velocity in cell c
 template <class R>
 __device__ __forceinline__ double contravariant(const R *xi, int Nc, int c, int dd, double u, double v, double w) {
@@ -692,6 +763,26 @@ __device__ __forceinline__ void form_Fd(const double Ai[6], const double A2[6], 
   G[3] = Ai[0] / (2. * Ai[4]);
   G[4] = A2[1] / (2. * A2[4]);
   G[0] = G[1] + G[2] + 2. * G[3] + 2. * G[4];
+}
+
+// form_Fd and form_F4 with slot 4 holding 1/A4 (the float MT_A of the FP32
+// phase): the same terms with each division by A4 a multiplication
+__device__ __forceinline__ void form_Fd_rcp(const double Ai[6], const double A2[6], double G[5]) {
+  G[1] = Ai[2] - Ai[0] * Ai[5] * Ai[4];
+  G[2] = A2[3] - A2[1] * A2[4] + A2[1] * A2[5] * A2[4];
+  G[3] = 0.5 * Ai[0] * Ai[4];
+  G[4] = 0.5 * A2[1] * A2[4];
+  G[0] = G[1] + G[2] + 2. * G[3] + 2. * G[4];
+}
+__device__ __forceinline__ void form_F4_rcp(const double A[3][6], double DT, double F4[8]) {
+  F4[1] = 0.5 * (A[0][4] + A[1][4] + A[2][4] - 1. / DT);
+  F4[2] = -(A[0][5] * A[0][4]);
+  F4[3] = (A[0][5] - 1.) * A[0][4];
+  F4[4] = -(A[1][5] * A[1][4]);
+  F4[5] = (A[1][5] - 1.) * A[1][4];
+  F4[6] = -(A[2][5] * A[2][4]);
+  F4[7] = (A[2][5] - 1.) * A[2][4];
+  F4[0] = F4[1] + F4[2] + F4[3] + F4[4] + F4[5] + F4[6] + F4[7];
 }
 
 __global__ void __launch_bounds__(BLK) k_vel_coef_F(Dims d, Fields F, Phys P) {
@@ -1107,10 +1198,6 @@ __global__ void k_wait_selftest(Ctrl *ctl, int tries) {
 }
 
 // nim_exp over n arguments (self-test of the exp the NIM coefficients use)
-__global__ void k_exp_selftest(const double *x, double *y, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    y[i] = nim_exp(x[i]);
-}
 
 __device__ __forceinline__ double errv(double nw, double old, bool first) { return fabs(nw - (first ? 0.0 : old)); }
 // max that keeps a NaN (fmax would drop it and hide a blow-up)
@@ -2261,10 +2348,12 @@ __global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, GeoT<R> g, FieldsT<R>
 // ---- K7a: calculate_temperature_nim_constants_formulation2, first part
 // (nim.f90:334-464): MT_A(1:6) of every cell and direction, from the cell
 // velocities of this pass.  One thread per (direction, cell) and no
-// barriers: the divisions of the NIM series make this the one
+// barriers: in FP64 the divisions of the NIM series make this the one
 // instruction-bound piece of the pass, and every warp can issue.
 // Grid (3, ceil(Nc/BLK)): blockIdx.x is the direction, so the three
 // directions of the same cells run side by side and share their loads.
+// The float instantiation (the FP32 phase) computes in float with
+// nim_direction_f32, which makes it bound by its bytes.
 template <class R>
 __global__ void __launch_bounds__(BLK, 4) k_T_coef(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
@@ -2272,14 +2361,26 @@ __global__ void __launch_bounds__(BLK, 4) k_T_coef(Dims d, GeoT<R> g, FieldsT<R>
   if (c >= d.Nc) return;
   const int dd = blockIdx.x + 1;
   const int Nc = d.Nc;
-  const double ut = 0.5 * (F.c[0][c] + F.co[0][c]);
-  const double vt = 0.5 * (F.c[1][c] + F.co[1][c]);
-  const double wt = 0.5 * (F.c[2][c] + F.co[2][c]);
-  const double u = contravariant(g.xi, Nc, c, dd, ut, vt, wt);
-  double A[6];
-  nim_direction(u, g.gij[(dd - 1 + 3 * (dd - 1)) * Nc + c] * P.alpha, g.gfd[(2 * (dd - 1)) * Nc + c],
-                g.gfd[(2 * (dd - 1) + 1) * Nc + c], P.v_limit, A);
-  for (int q = 0; q < 6; ++q) F.MTA[(3 * q + dd - 1) * Nc + c] = A[q];
+  if constexpr (std::is_same<R, float>::value) {
+    const float ut = 0.5f * (F.c[0][c] + F.co[0][c]);
+    const float vt = 0.5f * (F.c[1][c] + F.co[1][c]);
+    const float wt = 0.5f * (F.c[2][c] + F.co[2][c]);
+    const float u = ut * g.xi[(dd - 1) * Nc + c] + vt * g.xi[(dd + 2) * Nc + c] + wt * g.xi[(dd + 5) * Nc + c];
+    float A[6];
+    nim_direction_f32(u, g.gij[(dd - 1 + 3 * (dd - 1)) * Nc + c] * (float)P.alpha, g.gfd[(2 * (dd - 1)) * Nc + c],
+                      g.gfd[(2 * (dd - 1) + 1) * Nc + c], A);
+    A[4] = 1.f / A[4];  // k_T_cell, the one reader, only divides by A4 (A4 = 4h/k > 0)
+    for (int q = 0; q < 6; ++q) F.MTA[(3 * q + dd - 1) * Nc + c] = A[q];
+  } else {
+    const double ut = 0.5 * (F.c[0][c] + F.co[0][c]);
+    const double vt = 0.5 * (F.c[1][c] + F.co[1][c]);
+    const double wt = 0.5 * (F.c[2][c] + F.co[2][c]);
+    const double u = contravariant(g.xi, Nc, c, dd, ut, vt, wt);
+    double A[6];
+    nim_direction(u, g.gij[(dd - 1 + 3 * (dd - 1)) * Nc + c] * P.alpha, g.gfd[(2 * (dd - 1)) * Nc + c],
+                  g.gfd[(2 * (dd - 1) + 1) * Nc + c], P.v_limit, A);
+    for (int q = 0; q < 6; ++q) F.MTA[(3 * q + dd - 1) * Nc + c] = A[q];
+  }
 }
 
 // ---- K7b: the rest of calculate_temperature_nim_constants_formulation2
@@ -2322,7 +2423,10 @@ __global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, GeoT<R> g, FieldsT<R>
       A2[3] = MA[9 * Nc + c2];
       A2[4] = MA[12 * Nc + c2];
       A2[5] = MA[15 * Nc + c2];
-      form_Fd(A, A2, G);
+      if constexpr (std::is_same<R, float>::value)
+        form_Fd_rcp(A, A2, G);
+      else
+        form_Fd(A, A2, G);
     }
     for (int k = 0; k < 5; ++k) F.MTF[(size_t)(5 * (dd - 1) + k) * Nc + c] = G[k];
     // cross derivatives of calculate_R_D_T: y=0 pxy,pzy  y=1 pyx,pzx  y=2 pxz,pyz
@@ -2338,7 +2442,10 @@ __global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, GeoT<R> g, FieldsT<R>
         Am[k][5] = F.MTA[(size_t)(15 + k) * Nc + c];
       }
       double F4[8];
-      form_F4(Am, P.DT, F4);
+      if constexpr (std::is_same<R, float>::value)
+        form_F4_rcp(Am, P.DT, F4);
+      else
+        form_F4(Am, P.DT, F4);
       for (int k = 0; k < 8; ++k) sF4[k][tx] = F4[k];
     } else if (y == 2) {  // the leading G_i d_i T terms of R_D_T, in source order
       const double px = (T[f[2]] - T[f[1]]) / 2.;

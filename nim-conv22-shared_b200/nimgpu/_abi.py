@@ -211,6 +211,9 @@ def gpu_lib() -> C.CDLL:
         lib.nim_gpu_profile_name.restype = C.c_char_p
         lib.nim_gpu_selftest_exp.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64]
         lib.nim_gpu_selftest_exp.restype = C.c_int
+        lib.nim_gpu_selftest_nim_coef.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64,
+                                                  C.c_int32, C.c_double, C.POINTER(C.c_double)]
+        lib.nim_gpu_selftest_nim_coef.restype = C.c_int
         lib.nim_gpu_selftest_wait_timeout.argtypes = [vp, C.c_int32]
         lib.nim_gpu_selftest_wait_timeout.restype = C.c_int
         lib.nim_gpu_nusselt_noalloc.argtypes = [vp, C.POINTER(C.c_double)]
