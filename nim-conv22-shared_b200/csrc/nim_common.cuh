@@ -166,7 +166,8 @@ __device__ __forceinline__ void inv3(const double a[3][3], double x[3][3]) {
   x[2][2] = s * (a[0][0] * a[1][1] - a[0][1] * a[1][0]);
 }
 
-__device__ __forceinline__ double dot3(const double *a, const double *b) {
+template <class V>
+__device__ __forceinline__ V dot3(const V *a, const V *b) {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
 }
 

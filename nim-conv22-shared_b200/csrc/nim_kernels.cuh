@@ -132,6 +132,13 @@ constexpr int kLowpStall = 8;
 
 constexpr int BLK = 256;
 constexpr int VC2_MINB = 3;  // resident blocks per SM asked of k_vel_cell2 (56 registers)
+// resident blocks per SM the float instantiations of the pass kernels ask
+// for: computing in float they need about half the FP64 registers
+constexpr int VC2_MINB_F = 3, PSRC_MINB_F = 4, PFACE_MINB_F = 5, TCELL_MINB_F = 5, TFACE_MINB_F = 4;
+template <class R>
+constexpr int minb(int fp64, int fp32) {
+  return sizeof(R) == 8 ? fp64 : fp32;
+}
 // kernels that spread one cell over three threads (component or direction)
 constexpr int CB = 128;            // cells per block
 constexpr int CB3 = 3 * CB;        // threads per block
@@ -767,21 +774,23 @@ __device__ __forceinline__ void form_Fd(const double Ai[6], const double A2[6], 
 
 // form_Fd and form_F4 with slot 4 holding 1/A4 (the float MT_A of the FP32
 // phase): the same terms with each division by A4 a multiplication
-__device__ __forceinline__ void form_Fd_rcp(const double Ai[6], const double A2[6], double G[5]) {
+template <class V>
+__device__ __forceinline__ void form_Fd_rcp(const V Ai[6], const V A2[6], V G[5]) {
   G[1] = Ai[2] - Ai[0] * Ai[5] * Ai[4];
   G[2] = A2[3] - A2[1] * A2[4] + A2[1] * A2[5] * A2[4];
-  G[3] = 0.5 * Ai[0] * Ai[4];
-  G[4] = 0.5 * A2[1] * A2[4];
-  G[0] = G[1] + G[2] + 2. * G[3] + 2. * G[4];
+  G[3] = V(0.5) * Ai[0] * Ai[4];
+  G[4] = V(0.5) * A2[1] * A2[4];
+  G[0] = G[1] + G[2] + V(2) * G[3] + V(2) * G[4];
 }
-__device__ __forceinline__ void form_F4_rcp(const double A[3][6], double DT, double F4[8]) {
-  F4[1] = 0.5 * (A[0][4] + A[1][4] + A[2][4] - 1. / DT);
+template <class V>
+__device__ __forceinline__ void form_F4_rcp(const V A[3][6], V DT, V F4[8]) {
+  F4[1] = V(0.5) * (A[0][4] + A[1][4] + A[2][4] - V(1) / DT);
   F4[2] = -(A[0][5] * A[0][4]);
-  F4[3] = (A[0][5] - 1.) * A[0][4];
+  F4[3] = (A[0][5] - V(1)) * A[0][4];
   F4[4] = -(A[1][5] * A[1][4]);
-  F4[5] = (A[1][5] - 1.) * A[1][4];
+  F4[5] = (A[1][5] - V(1)) * A[1][4];
   F4[6] = -(A[2][5] * A[2][4]);
-  F4[7] = (A[2][5] - 1.) * A[2][4];
+  F4[7] = (A[2][5] - V(1)) * A[2][4];
   F4[0] = F4[1] + F4[2] + F4[3] + F4[4] + F4[5] + F4[6] + F4[7];
 }
 
@@ -998,9 +1007,23 @@ __global__ void __launch_bounds__(BLK) k_vel1_coef_F(Dims d, Geo g, Fields F, Ph
 // Load policies: the parallel kernels read with plain (L1-cached) loads; the
 // reference-order sweeps read data that other SMs rewrote one level earlier
 // (LdCoh below).
+// Arithmetic type of a kernel over storage type R: double for the FP64
+// path, float for the float mirror of the FP32 phase (whose kernels compute
+// in float, with only the change maxima and reductions in double).
+template <class R>
+struct ArithOf {
+  using type = double;
+};
+template <>
+struct ArithOf<float> {
+  using type = float;
+};
+template <class R>
+using Ar = typename ArithOf<R>::type;
+
 struct LdPlain {
   template <class T>
-  __device__ __forceinline__ static double ld(const T *p, size_t i) { return p[i]; }
+  __device__ __forceinline__ static Ar<T> ld(const T *p, size_t i) { return p[i]; }
 };
 // Loads and stores of values the same launch rewrites in place (the
 // reference-order sweeps) go through volatile: never the non-coherent
@@ -1009,7 +1032,7 @@ struct LdPlain {
 // the last grid or block barrier.  Other loads stay free to be scheduled.
 struct LdCoh {
   template <class T>
-  __device__ __forceinline__ static double ld(const T *p, size_t i) {
+  __device__ __forceinline__ static Ar<T> ld(const T *p, size_t i) {
     return *(const volatile T *)(p + i);
   }
 };
@@ -1018,7 +1041,7 @@ __device__ __forceinline__ void st_coh(double *p, size_t i, double v) { *(volati
 // a new value as the storage type R keeps it: the change find_error
 // measures is that of the stored field (identity for double)
 template <class R>
-__device__ __forceinline__ double stored(double v) { return (double)(R)v; }
+__device__ __forceinline__ Ar<R> stored(Ar<R> v) { return (Ar<R>)(R)v; }
 
 __device__ __forceinline__ int parity(const Ctrl *ctl) { return ctl->iter & ctl->pmask; }
 // half holding the values a sweep earlier in this pass produced
@@ -1039,9 +1062,9 @@ __device__ __forceinline__ void by_dir(int y, Fn &&fn) {
 }
 
 // Green-Gauss derivative dphi_dx2/dy2/dz2 (nse.f90:2866-2903), component cc
-template <class R>
-__device__ __forceinline__ double green_gauss(const GeoT<R> &g, size_t NF, double invV, const double phi[7],
-                                              const int f[7], int cc) {
+// in the value type V of phi (the kernel's arithmetic type)
+template <class R, class V>
+__device__ __forceinline__ V green_gauss(const GeoT<R> &g, size_t NF, V invV, const V phi[7], const int f[7], int cc) {
   const R *A = g.area, *n = g.normal + cc * NF;
   return invV * (phi[2] * A[f[2]] * (n[f[2]]) - phi[1] * A[f[1]] * (n[f[1]]) + phi[4] * A[f[4]] * (n[f[4]]) -
                  phi[3] * A[f[3]] * (n[f[3]]) + phi[6] * A[f[6]] * (n[f[6]]) - phi[5] * A[f[5]] * (n[f[5]]));
@@ -1051,35 +1074,37 @@ __device__ __forceinline__ double green_gauss(const GeoT<R> &g, size_t NF, doubl
 // x: centred, or second-order one-sided at walls (the ni/nj/nk stencils of
 // calculate_R_D2, nse.f90:1635-1838; integrate_pressure_field_i; bc.f90).
 template <class Ld = LdPlain, class R>
-__device__ __forceinline__ double tangential(const Dims &d, const R *__restrict__ phi, const Cell &x, int fpos,
-                                             int e) {
+__device__ __forceinline__ Ar<R> tangential(const Dims &d, const R *__restrict__ phi, const Cell &x, int fpos,
+                                            int e) {
+  using A = Ar<R>;
   const bool lo = !x.has_nb(d, 2 * e - 1), hi = !x.has_nb(d, 2 * e);
   if (lo) {
     const Cell m2 = x.nb(d, 2 * e), m3 = m2.nb(d, 2 * e);
-    return (-(3 * Ld::ld(phi, x.face(d, fpos))) + 4 * Ld::ld(phi, m2.face(d, fpos)) - Ld::ld(phi, m3.face(d, fpos))) / 4.;
+    return (-(3 * Ld::ld(phi, x.face(d, fpos))) + 4 * Ld::ld(phi, m2.face(d, fpos)) - Ld::ld(phi, m3.face(d, fpos))) / A(4);
   } else if (hi) {
     const Cell m1 = x.nb(d, 2 * e - 1), m3 = m1.nb(d, 2 * e - 1);
-    return (3 * Ld::ld(phi, x.face(d, fpos)) - 4 * Ld::ld(phi, m1.face(d, fpos)) + Ld::ld(phi, m3.face(d, fpos))) / 4.;
+    return (3 * Ld::ld(phi, x.face(d, fpos)) - 4 * Ld::ld(phi, m1.face(d, fpos)) + Ld::ld(phi, m3.face(d, fpos))) / A(4);
   }
-  return (Ld::ld(phi, x.nb(d, 2 * e).face(d, fpos)) - Ld::ld(phi, x.nb(d, 2 * e - 1).face(d, fpos))) / 4.;
+  return (Ld::ld(phi, x.nb(d, 2 * e).face(d, fpos)) - Ld::ld(phi, x.nb(d, 2 * e - 1).face(d, fpos))) / A(4);
 }
 
 // G_i d_i phi - g^ij d_ij phi of calculate_R_D2 / R_D_p2 / R_D_T
 // (nse.f90:1852-1859, 1995-1996, 2132-2133), before the coefficient.
 template <class R>
-__device__ __forceinline__ double diffusion_source(const Dims &d, const GeoT<R> &g, const R *__restrict__ phi,
-                                                   const Cell &x, const int f[7]) {
+__device__ __forceinline__ Ar<R> diffusion_source(const Dims &d, const GeoT<R> &g, const R *__restrict__ phi,
+                                                  const Cell &x, const int f[7]) {
+  using V = Ar<R>;
   const size_t Nc = d.Nc;
   const int c = x.c;
-  const double pxy = 0.5 * (tangential(d, phi, x, 2, 2) - tangential(d, phi, x, 1, 2));
-  const double pzy = 0.5 * (tangential(d, phi, x, 6, 2) - tangential(d, phi, x, 5, 2));
-  const double pyx = 0.5 * (tangential(d, phi, x, 4, 1) - tangential(d, phi, x, 3, 1));
-  const double pzx = 0.5 * (tangential(d, phi, x, 6, 1) - tangential(d, phi, x, 5, 1));
-  const double pxz = 0.5 * (tangential(d, phi, x, 2, 3) - tangential(d, phi, x, 1, 3));
-  const double pyz = 0.5 * (tangential(d, phi, x, 4, 3) - tangential(d, phi, x, 3, 3));
-  const double px = (phi[f[2]] - phi[f[1]]) / 2.;
-  const double py = (phi[f[4]] - phi[f[3]]) / 2.;
-  const double pz = (phi[f[6]] - phi[f[5]]) / 2.;
+  const V pxy = V(0.5) * (tangential(d, phi, x, 2, 2) - tangential(d, phi, x, 1, 2));
+  const V pzy = V(0.5) * (tangential(d, phi, x, 6, 2) - tangential(d, phi, x, 5, 2));
+  const V pyx = V(0.5) * (tangential(d, phi, x, 4, 1) - tangential(d, phi, x, 3, 1));
+  const V pzx = V(0.5) * (tangential(d, phi, x, 6, 1) - tangential(d, phi, x, 5, 1));
+  const V pxz = V(0.5) * (tangential(d, phi, x, 2, 3) - tangential(d, phi, x, 1, 3));
+  const V pyz = V(0.5) * (tangential(d, phi, x, 4, 3) - tangential(d, phi, x, 3, 3));
+  const V px = (phi[f[2]] - phi[f[1]]) / V(2.);
+  const V py = (phi[f[4]] - phi[f[3]]) / V(2.);
+  const V pz = (phi[f[6]] - phi[f[5]]) / V(2.);
   const R *G = g.G, *gij = g.gij;
   return (G[c] * px + G[Nc + c] * py + G[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy - gij[1 * Nc + c] * pyx -
           gij[6 * Nc + c] * pxz - gij[2 * Nc + c] * pzx - gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
@@ -1096,8 +1121,8 @@ __device__ __forceinline__ void cell_faces(const Dims &d, const Cell &x, int f[7
 
 // Cell-average update (nse.f90:840-848; T: 1018-1026)
 template <class Ld = LdPlain, class R>
-__device__ __forceinline__ double cell_update(const R *__restrict__ fr, const int f[7], double c, double cold,
-                                              double B, const double F4[8], double w) {
+__device__ __forceinline__ Ar<R> cell_update(const R *__restrict__ fr, const int f[7], Ar<R> c, Ar<R> cold,
+                                             Ar<R> B, const Ar<R> F4[8], Ar<R> w) {
   return (1 - w) * c +
          (w / F4[0]) * (+F4[1] * cold + F4[2] * Ld::ld(fr, f[1]) + F4[3] * Ld::ld(fr, f[2]) +
                         F4[4] * Ld::ld(fr, f[3]) + F4[5] * Ld::ld(fr, f[4]) + F4[6] * Ld::ld(fr, f[5]) +
@@ -1107,38 +1132,38 @@ __device__ __forceinline__ double cell_update(const R *__restrict__ fr, const in
 // +xi_d face update (nse.f90:878-1005; T: 1033-1088) from the face values
 // fx(pos) of cell x and fx2(pos) of its +xi_d neighbour x2, their cell
 // values cx, cx2 and old cell values ox, ox2
-template <class FX, class FX2>
-__device__ __forceinline__ double face_update_vals(FX &&fx, FX2 &&fx2, double cx, double cx2, double ox, double ox2,
-                                                   const double Fd[5], double dg0, double dg1, int dd, double w) {
+template <class V, class FX, class FX2>
+__device__ __forceinline__ V face_update_vals(FX &&fx, FX2 &&fx2, V cx, V cx2, V ox, V ox2, const V Fd[5], V dg0,
+                                              V dg1, int dd, V w) {
   const int e1 = tr1(dd), e2 = tr2(dd);
-  const double B3 = (dg0) * (fx(2 * e1) - fx(2 * e1 - 1) + fx2(2 * e1) - fx2(2 * e1 - 1)) / 4.0;
-  const double B4 = (dg1) * (fx(2 * e2) - fx(2 * e2 - 1) + fx2(2 * e2) - fx2(2 * e2 - 1)) / 4.0;
+  const V B3 = (dg0) * (fx(2 * e1) - fx(2 * e1 - 1) + fx2(2 * e1) - fx2(2 * e1 - 1)) / V(4.0);
+  const V B4 = (dg1) * (fx(2 * e2) - fx(2 * e2 - 1) + fx2(2 * e2) - fx2(2 * e2 - 1)) / V(4.0);
   return (1 - w) * fx(2 * dd) +
          (w / Fd[0]) * (+Fd[1] * fx(2 * dd - 1) + Fd[2] * fx2(2 * dd) + Fd[3] * (cx + ox) + Fd[4] * (cx2 + ox2) -
                         B3 - B4);
 }
 // the same from the face array fr; cx, cx2 the cell values of x and x2
 template <class Ld = LdPlain, class R>
-__device__ __forceinline__ double face_update_cv(const Dims &d, const R *__restrict__ fr, double cx, double cx2,
-                                                 const R *__restrict__ co, const double Fd[5], double dg0,
-                                                 double dg1, int dd, const Cell &x, const Cell &x2, double w) {
-  return face_update_vals([&](int pos) { return Ld::ld(fr, x.face(d, pos)); },
-                          [&](int pos) { return Ld::ld(fr, x2.face(d, pos)); }, cx, cx2, (double)co[x.c],
-                          (double)co[x2.c], Fd, dg0, dg1, dd, w);
+__device__ __forceinline__ Ar<R> face_update_cv(const Dims &d, const R *__restrict__ fr, Ar<R> cx, Ar<R> cx2,
+                                                const R *__restrict__ co, const Ar<R> Fd[5], Ar<R> dg0, Ar<R> dg1,
+                                                int dd, const Cell &x, const Cell &x2, Ar<R> w) {
+  return face_update_vals<Ar<R>>([&](int pos) { return Ld::ld(fr, x.face(d, pos)); },
+                                 [&](int pos) { return Ld::ld(fr, x2.face(d, pos)); }, cx, cx2, (Ar<R>)co[x.c],
+                                 (Ar<R>)co[x2.c], Fd, dg0, dg1, dd, w);
 }
 template <class Ld = LdPlain, class R>
-__device__ __forceinline__ double face_update(const Dims &d, const R *__restrict__ fr, const R *__restrict__ cv,
-                                              const R *__restrict__ co, const double Fd[5], double dg0,
-                                              double dg1, int dd, const Cell &x, const Cell &x2, double w) {
+__device__ __forceinline__ Ar<R> face_update(const Dims &d, const R *__restrict__ fr, const R *__restrict__ cv,
+                                             const R *__restrict__ co, const Ar<R> Fd[5], Ar<R> dg0, Ar<R> dg1,
+                                             int dd, const Cell &x, const Cell &x2, Ar<R> w) {
   return face_update_cv<Ld>(d, fr, Ld::ld(cv, x.c), Ld::ld(cv, x2.c), co, Fd, dg0, dg1, dd, x, x2, w);
 }
 
 // Formulation 1 cell update of one velocity component (integrate_velocity_
 // field_i, nse.f90:341-352); Rs = R_C + R_D + R_B of the cell, at = a_t(1:9).
 template <class Ld = LdPlain, class R>
-__device__ __forceinline__ double cell_update_f1(const R *__restrict__ fr, const int f[7], double c, double cold,
-                                                 double Rs, const double at[9], double w) {
-  const double Bij = at[6] * Rs;
+__device__ __forceinline__ Ar<R> cell_update_f1(const R *__restrict__ fr, const int f[7], Ar<R> c, Ar<R> cold,
+                                                Ar<R> Rs, const Ar<R> at[9], Ar<R> w) {
+  const Ar<R> Bij = at[6] * Rs;
   return (1 - w) * c + w * (-(at[0] * Ld::ld(fr, f[1])) - at[1] * Ld::ld(fr, f[2]) - at[2] * Ld::ld(fr, f[3]) -
                             at[3] * Ld::ld(fr, f[4]) - at[4] * Ld::ld(fr, f[5]) - at[5] * Ld::ld(fr, f[6]) -
                             at[7] * cold - Bij) /
@@ -1227,6 +1252,7 @@ __device__ __forceinline__ bool patch_cell(const Dims &d, Cell &x) {
 // reads them at both cells of a face.
 template <bool SRC_ONLY, int FORM, class R>
 __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  using V = Ar<R>;
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<3>(red);
@@ -1242,26 +1268,26 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, GeoT<R> g, FieldsT<
     int f[7];
     cell_faces(d, x, f);
     const R *fp = F.f[3] + par * NF;
-    double pf[7];
+    V pf[7];
     for (int k = 1; k <= 6; ++k) pf[k] = fp[f[k]];
-    const double invV = 1. / g.vol[c];
-    const double base = (q == 2) ? -(P.g_beta * 0.5 * (F.c[3][c] + F.co[3][c])) : 0.;
-    const double RB = base + P.inv_rho * green_gauss(g, NF, invV, pf, f, q);
+    const V invV = V(1.) / g.vol[c];
+    const V base = (q == 2) ? -(V(P.g_beta) * V(0.5) * (F.c[3][c] + F.co[3][c])) : V(0.);
+    const V RB = base + V(P.inv_rho) * green_gauss(g, NF, invV, pf, f, q);
     const R *fr = F.f[q] + par * NF;
-    const double RD = P.inv_Re * diffusion_source(d, g, fr, x, f);
-    const double B = (0. + RD + RB);
+    const V RD = V(P.inv_Re) * diffusion_source(d, g, fr, x, f);
+    const V B = (V(0.) + RD + RB);
     if (SRC_ONLY || FORM == 1) F.Bv[(size_t)q * Nc + c] = B;
     if (!SRC_ONLY) {
-      const double cold = F.c[q][c];
-      double nw;
+      const V cold = F.c[q][c];
+      V nw;
       if (FORM == 1) {
-        double at[9];
+        V at[9];
         for (int k = 0; k < 9; ++k) at[k] = F.AT[(size_t)k * Nc + c];
-        nw = stored<R>(cell_update_f1(fr, f, cold, F.co[q][c], B, at, P.w[q]));
+        nw = stored<R>(cell_update_f1(fr, f, cold, F.co[q][c], B, at, V(P.w[q])));
       } else {
-        double F4[8];
+        V F4[8];
         for (int k = 0; k < 8; ++k) F4[k] = F.MF4[(size_t)k * Nc + c];
-        nw = stored<R>(cell_update(fr, f, cold, F.co[q][c], B, F4, P.w[q]));
+        nw = stored<R>(cell_update(fr, f, cold, F.co[q][c], B, F4, V(P.w[q])));
       }
       F.c[q][c] = nw;
       e[q] = errv(nw, cold, first);
@@ -1300,11 +1326,11 @@ __device__ __forceinline__ void ld2(const R *__restrict__ p, int i, R &a, R &b) 
 }
 // tangential() from the values: v0 at the cell, vp1 / vp2 one / two cells
 // along +e, vm1 / vm2 along -e (only those the branch reads are used)
-__device__ __forceinline__ double tang_vals(bool lo, bool hi, double v0, double vp1, double vp2, double vm1,
-                                            double vm2) {
-  if (lo) return (-(3 * v0) + 4 * vp1 - vp2) / 4.;
-  if (hi) return (3 * v0 - 4 * vm1 + vm2) / 4.;
-  return (vp1 - vm1) / 4.;
+template <class V>
+__device__ __forceinline__ V tang_vals(bool lo, bool hi, V v0, V vp1, V vp2, V vm1, V vm2) {
+  if (lo) return (-(3 * v0) + 4 * vp1 - vp2) / V(4.);
+  if (hi) return (3 * v0 - 4 * vm1 + vm2) / V(4.);
+  return (vp1 - vm1) / V(4.);
 }
 
 // Index arithmetic here is 32-bit (its largest offset is 9 x the cell count;
@@ -1315,7 +1341,8 @@ __device__ __forceinline__ double tang_vals(bool lo, bool hi, double v0, double 
 // separate instantiation: at this kernel's register bound the test alone
 // costs spills)
 template <class R, bool SLAB = false>
-__global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+__global__ void __launch_bounds__(CB3, minb<R>(VC2_MINB, VC2_MINB_F)) k_vel_cell2(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  using V = Ar<R>;
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<3>(red);
@@ -1346,7 +1373,7 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
     // RB = base + 1/rho * green_gauss (component q): the sum term by term in
     // source order (faces 2, 1, 4, 3, 6, 5) for both cells
     const R *pp = F.f[3] + par * NF, *nq = g.normal + q * NF;
-    double gs0 = 0., gs1 = 0.;
+    V gs0 = V(0.), gs1 = V(0.);
     {
       const int order[6] = {2, 1, 4, 3, 6, 5};
 #pragma unroll
@@ -1356,7 +1383,7 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
         face2(pp, m, p0, p1);
         face2(g.area, m, a0, a1);
         face2(nq, m, n0, n1);
-        const double t0 = (double)p0 * a0 * (n0), t1 = (double)p1 * a1 * (n1);
+        const V t0 = (V)p0 * a0 * (n0), t1 = (V)p1 * a1 * (n1);
         if (t == 0) {
           gs0 = t0;
           gs1 = t1;
@@ -1369,30 +1396,30 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
         }
       }
     }
-    double RB0, RB1;
+    V RB0, RB1;
     {
       R v0, v1;
       ld2(g.vol, c, v0, v1);
-      double base0 = 0., base1 = 0.;
+      V base0 = V(0.), base1 = V(0.);
       if (q == 2) {
         R t0, t1, o0, o1;
         ld2(F.c[3], c, t0, t1);
         ld2(F.co[3], c, o0, o1);
-        base0 = -(P.g_beta * 0.5 * (t0 + o0));
-        base1 = -(P.g_beta * 0.5 * (t1 + o1));
+        base0 = -(V(P.g_beta) * V(0.5) * (t0 + o0));
+        base1 = -(V(P.g_beta) * V(0.5) * (t1 + o1));
       }
-      const double invV0 = 1. / v0, invV1 = 1. / v1;
-      RB0 = base0 + P.inv_rho * (invV0 * gs0);
-      RB1 = base1 + P.inv_rho * (invV1 * gs1);
+      const V invV0 = V(1.) / v0, invV1 = V(1.) / v1;
+      RB0 = base0 + V(P.inv_rho) * (invV0 * gs0);
+      RB1 = base1 + V(P.inv_rho) * (invV1 * gs1);
     }
     // own faces of component q (stored values)
     const R *fr = F.f[q] + par * NF;
     R o0[7], o1[7];
     for (int m = 1; m <= 6; ++m) face2(fr, m, o0[m], o1[m]);
     // rows / planes a and b: the -e,+e neighbours (centred), +1,+2 (lo) or -1,-2 (hi)
-    auto along = [&](bool lo, bool hi, double v0, double va, double vb) {
-      return lo ? tang_vals(true, false, v0, va, vb, 0., 0.)
-                : hi ? tang_vals(false, true, v0, 0., 0., va, vb) : tang_vals(false, false, v0, vb, 0., va, 0.);
+    auto along = [&](bool lo, bool hi, V v0, V va, V vb) {
+      return lo ? tang_vals(true, false, v0, va, vb, V(0.), V(0.))
+                : hi ? tang_vals(false, true, v0, V(0.), V(0.), va, vb) : tang_vals(false, false, v0, vb, V(0.), va, V(0.));
     };
     // R_D: G_i d_i phi - g^ij d_ij phi, term by term in source order; each
     // cross derivative is formed for both cells right before its term
@@ -1400,11 +1427,11 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
     const int ra = rlo ? j + 1 : j - 1, rb = rlo ? j + 2 : (rhi ? j - 2 : j + 1);
     const bool zlo = (k == 0), zhi = (k == d.NZ - 1);
     const int ka = zlo ? k + 1 : k - 1, kb = zlo ? k + 2 : (zhi ? k - 2 : k + 1);
-    double s0, s1;
+    V s0, s1;
     {
-      const double px0 = (o0[2] - o0[1]) / 2., px1 = (o1[2] - o1[1]) / 2.;
-      const double py0 = (o0[4] - o0[3]) / 2., py1 = (o1[4] - o1[3]) / 2.;
-      const double pz0 = (o0[6] - o0[5]) / 2., pz1 = (o1[6] - o1[5]) / 2.;
+      const V px0 = (o0[2] - o0[1]) / V(2.), px1 = (o1[2] - o1[1]) / V(2.);
+      const V py0 = (o0[4] - o0[3]) / V(2.), py1 = (o1[4] - o1[3]) / V(2.);
+      const V pz0 = (o0[6] - o0[5]) / V(2.), pz1 = (o1[6] - o1[5]) / V(2.);
       R a0, a1;
       ld2(g.G, c, a0, a1);
       s0 = a0 * px0;
@@ -1416,7 +1443,7 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
       s0 = s0 + a0 * pz0;
       s1 = s1 + a1 * pz1;
     }
-    auto term = [&](int slot, double d0, double d1) {
+    auto term = [&](int slot, V d0, V d1) {
       R a0, a1;
       ld2(g.gij + slot * Nc, c, a0, a1);
       s0 = s0 - a0 * d0;
@@ -1424,10 +1451,10 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
     };
     {  // pxy: r faces (rows j, j+1) at theta i-1, i+2 (centred in theta)
       const int rrow = NT * (j + (NR + 1) * k);
-      const double r_m1 = fr[rrow + im1], r_p2 = fr[rrow + ip2];
-      const double r1_m1 = fr[rrow + NT + im1], r1_p2 = fr[rrow + NT + ip2];
-      term(3, 0.5 * (((double)o1[2] - r1_m1) / 4. - ((double)o1[1] - r_m1) / 4.),
-           0.5 * ((r1_p2 - (double)o0[2]) / 4. - (r_p2 - (double)o0[1]) / 4.));
+      const V r_m1 = fr[rrow + im1], r_p2 = fr[rrow + ip2];
+      const V r1_m1 = fr[rrow + NT + im1], r1_p2 = fr[rrow + NT + ip2];
+      term(3, V(0.5) * (((V)o1[2] - r1_m1) / V(4.) - ((V)o1[1] - r_m1) / V(4.)),
+           V(0.5) * ((r1_p2 - (V)o0[2]) / V(4.) - (r_p2 - (V)o0[1]) / V(4.)));
     }
     {  // pyx: theta faces of rows a, b
       const int tra = d.offT + NT * (ra + NR * k), trb = d.offT + NT * (rb + NR * k);
@@ -1435,8 +1462,8 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
       ld2(fr, tra + i, a0, a1);
       ld2(fr, trb + i, b0, b1);
       const R a2 = fr[tra + ip2], b2 = fr[trb + ip2];
-      term(1, 0.5 * (along(rlo, rhi, o0[4], a1, b1) - along(rlo, rhi, o0[3], a0, b0)),
-           0.5 * (along(rlo, rhi, o1[4], a2, b2) - along(rlo, rhi, o1[3], a1, b1)));
+      term(1, V(0.5) * (along(rlo, rhi, o0[4], a1, b1) - along(rlo, rhi, o0[3], a0, b0)),
+           V(0.5) * (along(rlo, rhi, o1[4], a2, b2) - along(rlo, rhi, o1[3], a1, b1)));
     }
     {  // pxz: r faces (rows j, j+1) of planes a, b
       const int rka = NT * (j + (NR + 1) * ka), rkb = NT * (j + (NR + 1) * kb);
@@ -1445,8 +1472,8 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
       ld2(fr, rkb + i, pb0, pb1);
       ld2(fr, rka + NT + i, pA0, pA1);
       ld2(fr, rkb + NT + i, pB0, pB1);
-      term(6, 0.5 * (along(zlo, zhi, o0[2], pA0, pB0) - along(zlo, zhi, o0[1], pa0, pb0)),
-           0.5 * (along(zlo, zhi, o1[2], pA1, pB1) - along(zlo, zhi, o1[1], pa1, pb1)));
+      term(6, V(0.5) * (along(zlo, zhi, o0[2], pA0, pB0) - along(zlo, zhi, o0[1], pa0, pb0)),
+           V(0.5) * (along(zlo, zhi, o1[2], pA1, pB1) - along(zlo, zhi, o1[1], pa1, pb1)));
     }
     {  // pzx: z faces (levels k, k+1) of rows a, b
       const int zra = d.offZ + NT * (ra + NR * k), zrb = d.offZ + NT * (rb + NR * k);
@@ -1455,8 +1482,8 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
       ld2(fr, zrb + i, zb0, zb1);
       ld2(fr, zra + pl + i, zA0, zA1);
       ld2(fr, zrb + pl + i, zB0, zB1);
-      term(2, 0.5 * (along(rlo, rhi, o0[6], zA0, zB0) - along(rlo, rhi, o0[5], za0, zb0)),
-           0.5 * (along(rlo, rhi, o1[6], zA1, zB1) - along(rlo, rhi, o1[5], za1, zb1)));
+      term(2, V(0.5) * (along(rlo, rhi, o0[6], zA0, zB0) - along(rlo, rhi, o0[5], za0, zb0)),
+           V(0.5) * (along(rlo, rhi, o1[6], zA1, zB1) - along(rlo, rhi, o1[5], za1, zb1)));
     }
     {  // pyz: theta faces of planes a, b
       const int tka = d.offT + NT * (j + NR * ka), tkb = d.offT + NT * (j + NR * kb);
@@ -1464,35 +1491,35 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
       ld2(fr, tka + i, a0, a1);
       ld2(fr, tkb + i, b0, b1);
       const R a2 = fr[tka + ip2], b2 = fr[tkb + ip2];
-      term(7, 0.5 * (along(zlo, zhi, o0[4], a1, b1) - along(zlo, zhi, o0[3], a0, b0)),
-           0.5 * (along(zlo, zhi, o1[4], a2, b2) - along(zlo, zhi, o1[3], a1, b1)));
+      term(7, V(0.5) * (along(zlo, zhi, o0[4], a1, b1) - along(zlo, zhi, o0[3], a0, b0)),
+           V(0.5) * (along(zlo, zhi, o1[4], a2, b2) - along(zlo, zhi, o1[3], a1, b1)));
     }
     {  // pzy: z faces (levels k, k+1) at theta i-1, i+2
       const int zlev = d.offZ + NT * (j + NR * k);
-      const double z_m1 = fr[zlev + im1], z_p2 = fr[zlev + ip2];
-      const double z1_m1 = fr[zlev + pl + im1], z1_p2 = fr[zlev + pl + ip2];
-      term(5, 0.5 * (((double)o1[6] - z1_m1) / 4. - ((double)o1[5] - z_m1) / 4.),
-           0.5 * ((z1_p2 - (double)o0[6]) / 4. - (z_p2 - (double)o0[5]) / 4.));
+      const V z_m1 = fr[zlev + im1], z_p2 = fr[zlev + ip2];
+      const V z1_m1 = fr[zlev + pl + im1], z1_p2 = fr[zlev + pl + ip2];
+      term(5, V(0.5) * (((V)o1[6] - z1_m1) / V(4.) - ((V)o1[5] - z_m1) / V(4.)),
+           V(0.5) * ((z1_p2 - (V)o0[6]) / V(4.) - (z_p2 - (V)o0[5]) / V(4.)));
     }
-    const double RD0 = P.inv_Re * s0, RD1 = P.inv_Re * s1;
-    const double B0 = (0. + RD0 + RB0), B1 = (0. + RD1 + RB1);
+    const V RD0 = V(P.inv_Re) * s0, RD1 = V(P.inv_Re) * s1;
+    const V B0 = (V(0.) + RD0 + RB0), B1 = (V(0.) + RD1 + RB1);
     // cell update (cell_update), term by term
     R cv0, cv1, co0, co1, a0, a1;
     ld2(F.c[q], c, cv0, cv1);
     ld2(F.co[q], c, co0, co1);
-    const double w = P.w[q];
+    const V w = V(P.w[q]);
     ld2(F.MF4, c, a0, a1);
-    const double F40 = a0, F41 = a1;
+    const V F40 = a0, F41 = a1;
     ld2(F.MF4 + Nc, c, a0, a1);
-    double u0 = +a0 * (double)co0, u1 = +a1 * (double)co1;
+    V u0 = +a0 * (V)co0, u1 = +a1 * (V)co1;
 #pragma unroll
     for (int m = 2; m <= 7; ++m) {
       ld2(F.MF4 + m * Nc, c, a0, a1);
-      u0 = u0 + a0 * (double)o0[m - 1];
-      u1 = u1 + a1 * (double)o1[m - 1];
+      u0 = u0 + a0 * (V)o0[m - 1];
+      u1 = u1 + a1 * (V)o1[m - 1];
     }
-    const double nw0 = stored<R>((1 - w) * (double)cv0 + (w / F40) * (u0 + B0));
-    const double nw1 = stored<R>((1 - w) * (double)cv1 + (w / F41) * (u1 + B1));
+    const V nw0 = stored<R>((1 - w) * (V)cv0 + (w / F40) * (u0 + B0));
+    const V nw1 = stored<R>((1 - w) * (V)cv1 + (w / F41) * (u1 + B1));
     typename Pair2<R>::T out;
     out.x = (R)nw0;
     out.y = (R)nw1;
@@ -1506,6 +1533,7 @@ __global__ void __launch_bounds__(CB3, VC2_MINB) k_vel_cell2(Dims d, GeoT<R> g, 
 // Block (CB, 3): threadIdx.y = direction.
 template <class R>
 __global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  using V = Ar<R>;
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<3>(red);
@@ -1521,14 +1549,14 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, GeoT<R> g, FieldsT<
       constexpr int dd = decltype(D)::value;
       if (!x.has_nb(d, 2 * dd)) return;
       const Cell x2 = x.nb(d, 2 * dd);
-      double Fd[5];
+      V Fd[5];
       for (int k = 0; k < 5; ++k) Fd[k] = F.MF[(size_t)(5 * (dd - 1) + k) * Nc + c];
-      const double dg0 = g.dg[(2 * (dd - 1)) * Nc + c], dg1 = g.dg[(2 * (dd - 1) + 1) * Nc + c];
+      const V dg0 = g.dg[(2 * (dd - 1)) * Nc + c], dg1 = g.dg[(2 * (dd - 1) + 1) * Nc + c];
       const int fo = x.face(d, 2 * dd);
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
         const R *fr = F.f[q] + par * NF;
-        const double nw = stored<R>(face_update(d, fr, F.c[q], F.co[q], Fd, dg0, dg1, dd, x, x2, P.w[q]));
+        const V nw = stored<R>(face_update(d, fr, F.c[q], F.co[q], Fd, dg0, dg1, dd, x, x2, V(P.w[q])));
         F.f[q][(1 - par) * NF + fo] = nw;
         e[q] = errv(nw, fr[fo], first);
       }
@@ -1555,8 +1583,8 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, GeoT<R> g, FieldsT<
 constexpr int VT_R = 4;         // r rows of cells per patch
 constexpr int VT_T = 32 * VT_R;  // cells per patch = blockDim.x (blockDim.y = 3 directions)
 constexpr int VT_S = 3;          // plane ring depth (FP64: 109 KB with the coefficient ring)
-constexpr int VT_MINB = 2;       // resident blocks per SM the launch bounds ask for (FP64;
-                                 // float: 3, its 57 KB ring allows it)
+constexpr int VT_MINB = 2;       // resident blocks per SM the launch bounds ask for (FP64)
+constexpr int VT_MINB_F = 3;     // float: its 57 KB ring allows 3
 
 // tensor maps of one storage type, encoded by the host: per component the
 // r / theta / z parts of the face array as {NT, rows, planes, half}, the
@@ -1664,8 +1692,9 @@ __device__ __forceinline__ bool vt_seam(const Dims &d, const FieldsT<R> &F, int 
 
 // SLAB: a z-slab context, whose maxima skip the planes a neighbour owns
 template <class R, bool SLAB = false>
-__global__ void __launch_bounds__(3 * VT_T, sizeof(R) == 8 ? VT_MINB : 3)
+__global__ void __launch_bounds__(3 * VT_T, minb<R>(VT_MINB, VT_MINB_F))
     k_vel_face_tile(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl, int kc, const __grid_constant__ VelFaceMaps M) {
+  using V = Ar<R>;
   using L = VtLayout<R>;
   if (ctl->done) return;
   extern __shared__ __align__(128) unsigned char vt_raw[];
@@ -1735,10 +1764,10 @@ __global__ void __launch_bounds__(3 * VT_T, sizeof(R) == 8 ? VT_MINB : 3)
       by_dir(threadIdx.y, [&](auto D) {
         constexpr int dd = decltype(D)::value;
         if (!x.has_nb(d, 2 * dd)) return;
-        double Fd[5];
+        V Fd[5];
         for (int kq = 0; kq < 5; ++kq) Fd[kq] = C[(5 * (dd - 1) + kq) * VT_R * 32 + jj * 32 + ii];
-        const double dg0 = C[L::MF + (2 * (dd - 1)) * VT_R * 32 + jj * 32 + ii];
-        const double dg1 = C[L::MF + (2 * (dd - 1) + 1) * VT_R * 32 + jj * 32 + ii];
+        const V dg0 = C[L::MF + (2 * (dd - 1)) * VT_R * 32 + jj * 32 + ii];
+        const V dg1 = C[L::MF + (2 * (dd - 1) + 1) * VT_R * 32 + jj * 32 + ii];
         // x2 = x + e_dd sits at (ii + di, jj + dj) of plane Q0
         constexpr int di = (dd == 2), dj = (dd == 1);
         const R *Q0 = (dd == 3) ? P1 : P0, *Q1 = (dd == 3) ? P2 : P1;
@@ -1746,7 +1775,7 @@ __global__ void __launch_bounds__(3 * VT_T, sizeof(R) == 8 ? VT_MINB : 3)
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
           // face pos of the cell at (a, b) of plane A (B: the plane above)
-          auto face = [&](const R *A, const R *B, int a, int b, int pos) -> double {
+          auto face = [&](const R *A, const R *B, int a, int b, int pos) -> V {
             const R *qa = A + q * L::Q, *qb = B + q * L::Q;
             switch (pos) {
               case 1: return qa[b * L::W + a];
@@ -1760,9 +1789,9 @@ __global__ void __launch_bounds__(3 * VT_T, sizeof(R) == 8 ? VT_MINB : 3)
           auto fx = [&](int pos) { return face(P0, P1, ii, jj, pos); };
           auto fx2 = [&](int pos) { return face(Q0, Q1, ii + di, jj + dj, pos); };
           const R *cq0 = P0 + q * L::Q + L::RF + 2 * L::C5, *cq2 = Q0 + q * L::Q + L::RF + 2 * L::C5;
-          const double nw = stored<R>(face_update_vals(
+          const V nw = stored<R>(face_update_vals(
               fx, fx2, cq0[jj * L::W + ii], cq2[(jj + dj) * L::W + ii + di], cq0[L::C5 + jj * L::W + ii],
-              cq2[L::C5 + (jj + dj) * L::W + ii + di], Fd, dg0, dg1, dd, P.w[q]));
+              cq2[L::C5 + (jj + dj) * L::W + ii + di], Fd, dg0, dg1, dd, V(P.w[q])));
           F.f[q][(1 - par) * NF + fo] = nw;
           if (!SLAB || d.owns(k)) e[q] = nmax(e[q], errv(nw, fx(2 * dd), first));
         }
@@ -1891,6 +1920,7 @@ __device__ __forceinline__ bool ct_seam(const Dims &d, const FieldsT<R> &F, int 
 template <class R>
 __global__ void __launch_bounds__(3 * CT_T, CT_MINB)
     k_vel_cell_tile(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl, int kc, const __grid_constant__ VelCellMaps M) {
+  using V = Ar<R>;
   using L = CtLayout<R>;
   if (ctl->done) return;
   extern __shared__ __align__(128) unsigned char ct_raw[];
@@ -1954,13 +1984,13 @@ __global__ void __launch_bounds__(3 * CT_T, CT_MINB)
       int f[7];
       cell_faces(d, x, f);
       const R *fp = F.f[3] + par * NF;
-      double pf[7];
+      V pf[7];
       for (int m = 1; m <= 6; ++m) pf[m] = fp[f[m]];
-      const double invV = 1. / g.vol[c];
-      const double base = (q == 2) ? -(P.g_beta * 0.5 * (F.c[3][c] + F.co[3][c])) : 0.;
-      const double RB = base + P.inv_rho * green_gauss(g, NF, invV, pf, f, q);
+      const V invV = V(1.) / g.vol[c];
+      const V base = (q == 2) ? -(V(P.g_beta) * V(0.5) * (F.c[3][c] + F.co[3][c])) : V(0.);
+      const V RB = base + V(P.inv_rho) * green_gauss(g, NF, invV, pf, f, q);
       // face pos of the cell (di, dj, dk) away, component q, from the ring
-      auto fv = [&](int pos, int di, int dj, int dk) -> double {
+      auto fv = [&](int pos, int di, int dj, int dk) -> V {
         const int pb = k + dk + (pos == 6 ? 1 : 0) - P0;
         const R *b = ring + (pb % CT_S) * L::BUNDLE + q * L::Q;
         const int col = ii + di + L::OFF + (pos == 4 ? 1 : 0);
@@ -1973,34 +2003,34 @@ __global__ void __launch_bounds__(3 * CT_T, CT_MINB)
         }
       };
       // tangential(): centred, or one-sided at the walls, along e
-      auto tng = [&](int pos, int e) -> double {
+      auto tng = [&](int pos, int e) -> V {
         auto at = [&](int s) { return fv(pos, e == 2 ? s : 0, e == 1 ? s : 0, e == 3 ? s : 0); };
         const bool lo = !x.has_nb(d, 2 * e - 1), hi = !x.has_nb(d, 2 * e);
-        if (lo) return (-(3 * at(0)) + 4 * at(1) - at(2)) / 4.;
-        if (hi) return (3 * at(0) - 4 * at(-1) + at(-2)) / 4.;
-        return (at(1) - at(-1)) / 4.;
+        if (lo) return (-(3 * at(0)) + 4 * at(1) - at(2)) / V(4.);
+        if (hi) return (3 * at(0) - 4 * at(-1) + at(-2)) / V(4.);
+        return (at(1) - at(-1)) / V(4.);
       };
-      const double pxy = 0.5 * (tng(2, 2) - tng(1, 2));
-      const double pzy = 0.5 * (tng(6, 2) - tng(5, 2));
-      const double pyx = 0.5 * (tng(4, 1) - tng(3, 1));
-      const double pzx = 0.5 * (tng(6, 1) - tng(5, 1));
-      const double pxz = 0.5 * (tng(2, 3) - tng(1, 3));
-      const double pyz = 0.5 * (tng(4, 3) - tng(3, 3));
+      const V pxy = V(0.5) * (tng(2, 2) - tng(1, 2));
+      const V pzy = V(0.5) * (tng(6, 2) - tng(5, 2));
+      const V pyx = V(0.5) * (tng(4, 1) - tng(3, 1));
+      const V pzx = V(0.5) * (tng(6, 1) - tng(5, 1));
+      const V pxz = V(0.5) * (tng(2, 3) - tng(1, 3));
+      const V pyz = V(0.5) * (tng(4, 3) - tng(3, 3));
       R fr[7];  // the stored values: the differences below are taken in R, as in diffusion_source
       for (int m = 1; m <= 6; ++m) fr[m] = (R)fv(m, 0, 0, 0);
-      const double px = (fr[2] - fr[1]) / 2.;
-      const double py = (fr[4] - fr[3]) / 2.;
-      const double pz = (fr[6] - fr[5]) / 2.;
+      const V px = (fr[2] - fr[1]) / V(2.);
+      const V py = (fr[4] - fr[3]) / V(2.);
+      const V pz = (fr[6] - fr[5]) / V(2.);
       const R *G = g.G, *gij = g.gij;
-      const double RD =
-          P.inv_Re * (G[c] * px + G[Nc + c] * py + G[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy -
+      const V RD =
+          V(P.inv_Re) * (G[c] * px + G[Nc + c] * py + G[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy -
                       gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz - gij[2 * Nc + c] * pzx - gij[7 * Nc + c] * pyz -
                       gij[5 * Nc + c] * pzy);
-      const double B = (0. + RD + RB);
-      const double cv = F.c[q][c], cold = F.co[q][c], w = P.w[q];
-      double F4[8];
+      const V B = (V(0.) + RD + RB);
+      const V cv = F.c[q][c], cold = F.co[q][c], w = V(P.w[q]);
+      V F4[8];
       for (int m = 0; m < 8; ++m) F4[m] = F.MF4[(size_t)m * Nc + c];
-      const double nw = stored<R>((1 - w) * cv + (w / F4[0]) * (+F4[1] * cold + F4[2] * fr[1] + F4[3] * fr[2] +
+      const V nw = stored<R>((1 - w) * cv + (w / F4[0]) * (+F4[1] * cold + F4[2] * fr[1] + F4[3] * fr[2] +
                                                                   F4[4] * fr[3] + F4[5] * fr[4] + F4[6] * fr[5] +
                                                                   F4[7] * fr[6] + B));
       F.c[q][c] = nw;
@@ -2027,11 +2057,12 @@ __global__ void __launch_bounds__(3 * CT_T, CT_MINB)
 // velocity component y and two of the six cross derivatives of p (y = 1 also
 // d(bz)/dz); thread 0 combines them in the reference's order.
 template <class R>
-__global__ void __launch_bounds__(CB3, 4) k_p_src(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+__global__ void __launch_bounds__(CB3, minb<R>(4, PSRC_MINB_F)) k_p_src(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
-  __shared__ double sh[3][3][CB];  // gradients of u, v, w
-  __shared__ double sX[3][2][CB];  // cross derivatives of p
-  __shared__ double sbz[CB];
+  using A = Ar<R>;
+  __shared__ A sh[3][3][CB];  // gradients of u, v, w
+  __shared__ A sX[3][2][CB];  // cross derivatives of p
+  __shared__ A sbz[CB];
   const int par = parity(ctl);
   const int q = threadIdx.y, tx = threadIdx.x;
   Cell x;
@@ -2044,43 +2075,43 @@ __global__ void __launch_bounds__(CB3, 4) k_p_src(Dims d, GeoT<R> g, FieldsT<R> 
     cell_faces(d, x, f);
     by_dir(threadIdx.y, [&](auto Q) {
       constexpr int q = decltype(Q)::value - 1;
-      const double invV = 1. / g.vol[c];
+      const A invV = A(1) / g.vol[c];
       const R *fq = F.f[q] + newhalf(ctl) * NF;
-      double vf[7];
+      A vf[7];
       for (int k = 1; k <= 6; ++k) vf[k] = fq[f[k]];
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) sh[q][cc][tx] = green_gauss(g, NF, invV, vf, f, cc);
       if (q == 1) {
         const R *fT = F.f[4] + par * NF;
-        double bzf[7];
-        for (int k = 1; k <= 6; ++k) bzf[k] = -(P.g_beta * (fT[f[k]]));
+        A bzf[7];
+        for (int k = 1; k <= 6; ++k) bzf[k] = -(A(P.g_beta) * (fT[f[k]]));
         sbz[tx] = green_gauss(g, NF, invV, bzf, f, 2);
       }
       // y=0 pxy,pzy  y=1 pyx,pzx  y=2 pxz,pyz (calculate_R_D_p2 order)
       constexpr int e2 = (q == 0) ? 2 : (q == 1) ? 1 : 3;
       constexpr int fa = (q == 1) ? 4 : 2, fb = (q == 1) ? 3 : 1;
-      sX[q][0][tx] = 0.5 * (tangential(d, fp, x, fa, e2) - tangential(d, fp, x, fb, e2));
-      sX[q][1][tx] = (q == 2) ? 0.5 * (tangential(d, fp, x, 4, 3) - tangential(d, fp, x, 3, 3))
-                              : 0.5 * (tangential(d, fp, x, 6, e2) - tangential(d, fp, x, 5, e2));
+      sX[q][0][tx] = A(0.5) * (tangential(d, fp, x, fa, e2) - tangential(d, fp, x, fb, e2));
+      sX[q][1][tx] = (q == 2) ? A(0.5) * (tangential(d, fp, x, 4, 3) - tangential(d, fp, x, 3, 3))
+                              : A(0.5) * (tangential(d, fp, x, 6, e2) - tangential(d, fp, x, 5, e2));
     });
   }
   __syncthreads();
   if (active && q == 0) {
-    const double du_dx = sh[0][0][tx], du_dy = sh[0][1][tx], du_dz = sh[0][2][tx];
-    const double dv_dx = sh[1][0][tx], dv_dy = sh[1][1][tx], dv_dz = sh[1][2][tx];
-    const double dw_dx = sh[2][0][tx], dw_dy = sh[2][1][tx], dw_dz = sh[2][2][tx];
-    const double dbz_dz = sbz[tx];
-    const double Dila = du_dx + dv_dy + dw_dz;
+    const A du_dx = sh[0][0][tx], du_dy = sh[0][1][tx], du_dz = sh[0][2][tx];
+    const A dv_dx = sh[1][0][tx], dv_dy = sh[1][1][tx], dv_dz = sh[1][2][tx];
+    const A dw_dx = sh[2][0][tx], dw_dy = sh[2][1][tx], dw_dz = sh[2][2][tx];
+    const A dbz_dz = sbz[tx];
+    const A Dila = du_dx + dv_dy + dw_dz;
     F.dila[c] = Dila;
-    const double RBp = -(du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) -
-                       2.0 * (du_dy * dv_dx + dv_dz * dw_dy + dw_dx * du_dz) - dbz_dz + Dila / (2 * P.DT);
-    const double pxy = sX[0][0][tx], pzy = sX[0][1][tx], pyx = sX[1][0][tx], pzx = sX[1][1][tx];
-    const double pxz = sX[2][0][tx], pyz = sX[2][1][tx];
-    const double px = (fp[f[2]] - fp[f[1]]) / 2.;
-    const double py = (fp[f[4]] - fp[f[3]]) / 2.;
-    const double pz = (fp[f[6]] - fp[f[5]]) / 2.;
+    const A RBp = -(du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) -
+                  A(2) * (du_dy * dv_dx + dv_dz * dw_dy + dw_dx * du_dz) - dbz_dz + Dila / (2 * A(P.DT));
+    const A pxy = sX[0][0][tx], pzy = sX[0][1][tx], pyx = sX[1][0][tx], pzx = sX[1][1][tx];
+    const A pxz = sX[2][0][tx], pyz = sX[2][1][tx];
+    const A px = (fp[f[2]] - fp[f[1]]) / A(2);
+    const A py = (fp[f[4]] - fp[f[3]]) / A(2);
+    const A pz = (fp[f[6]] - fp[f[5]]) / A(2);
     const R *Gv = g.G, *gij = g.gij;
-    const double RDp = P.inv_rho * (Gv[c] * px + Gv[Nc + c] * py + Gv[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy -
+    const A RDp = A(P.inv_rho) * (Gv[c] * px + Gv[Nc + c] * py + Gv[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy -
                                     gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz - gij[2 * Nc + c] * pzx -
                                     gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
     F.Rp[c] = RDp + RBp;
@@ -2090,42 +2121,43 @@ __global__ void __launch_bounds__(CB3, 4) k_p_src(Dims d, GeoT<R> g, FieldsT<R> 
 // ---- apply_pressure_bc for wall face b (bc.f90:148-339): the new value
 // from the pressures pr, the new velocities fu/fv/fwv and the temperatures fT
 template <class Ld, class R>
-__device__ __forceinline__ double p_bc_value(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P,
-                                             const R *pr, const R *fu, const R *fv, const R *fwv, const R *fT,
-                                             int b) {
+__device__ __forceinline__ Ar<R> p_bc_value(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P,
+                                            const R *pr, const R *fu, const R *fv, const R *fwv, const R *fT,
+                                            int b) {
+  using V = Ar<R>;
   const int NF = d.NF, NB = d.NBF;
   const BFace B = bface(d, b);
   const Cell M1 = B.cell;
   const int pos = B.pos;
   const int fw0 = M1.face(d, pos);
-  const double n[3] = {g.normal[fw0], g.normal[NF + fw0], g.normal[2 * NF + fw0]};
-  const double bvec[3] = {0., 0., -(P.g_beta * (fT[fw0]))};
-  const double b_n = dot3(bvec, n);
-  double vn[6];
+  const V n[3] = {g.normal[fw0], g.normal[NF + fw0], g.normal[2 * NF + fw0]};
+  const V bvec[3] = {V(0), V(0), -(V(P.g_beta) * (fT[fw0]))};
+  const V b_n = dot3(bvec, n);
+  V vn[6];
   for (int j = 1; j <= 5; ++j) {
     const int pt = g.bcpts[(j - 1) * NB + b];
-    const double v[3] = {fu[pt], fv[pt], fwv[pt]};
+    const V v[3] = {fu[pt], fv[pt], fwv[pt]};
     vn[j] = dot3(v, n);
   }
   const R *a = g.bca;
-  const double d2udn2 = -(a[b] * vn[1]) - a[NB + b] * vn[2] - a[2 * NB + b] * vn[3] - a[3 * NB + b] * vn[4] -
+  const V d2udn2 = -(a[b] * vn[1]) - a[NB + b] * vn[2] - a[2 * NB + b] * vn[3] - a[3 * NB + b] * vn[4] -
                         a[4 * NB + b] * vn[5];
   const int dd = (pos + 1) / 2;
-  const double B2 = tangential<Ld>(d, pr, M1, pos, tr1(dd)) * g.bcg[b];
-  const double B3 = tangential<Ld>(d, pr, M1, pos, tr2(dd)) * g.bcg[NB + b];
+  const V B2 = tangential<Ld>(d, pr, M1, pos, tr1(dd)) * g.bcg[b];
+  const V B3 = tangential<Ld>(d, pr, M1, pos, tr2(dd)) * g.bcg[NB + b];
   const R *ap = g.bcap;
-  const double B1 = ap[7 * NB + b] * (F.Rp[M1.c]);
-  double s = 0.0;
+  const V B1 = ap[7 * NB + b] * (F.Rp[M1.c]);
+  V s = 0.0;
   bool firstterm = true;
   for (int k = 1; k <= 6; ++k) {
     if (k == pos) continue;
-    const double t = ap[(k - 1) * NB + b] * Ld::ld(pr, M1.face(d, k));
+    const V t = ap[(k - 1) * NB + b] * Ld::ld(pr, M1.face(d, k));
     s = firstterm ? -t : s - t;
     firstterm = false;
   }
-  const double w = P.w_p2;
+  const V w = V(P.w_p2);
   return (1 - w) * Ld::ld(pr, fw0) +
-         w / (ap[(pos - 1) * NB + b]) * (s + B1 - B2 - B3 + (P.nu * P.rho * d2udn2 - b_n * P.rho));
+         w / (ap[(pos - 1) * NB + b]) * (s + B1 - B2 - B3 + (V(P.nu) * V(P.rho) * d2udn2 - b_n * V(P.rho)));
 }
 
 // ---- K4: apply_pressure_bc, every wall face from the values before the pass
@@ -2141,8 +2173,8 @@ __global__ void __launch_bounds__(BLK) k_p_bc(Dims d, GeoT<R> g, FieldsT<R> F, P
   if (b < d.NBF) {
     const int NF = d.NF;
     const R *pr = F.f[3] + par * NF;
-    const double nw = stored<R>(p_bc_value<LdPlain>(d, g, F, P, pr, F.f[0] + nh * NF, F.f[1] + nh * NF,
-                                                    F.f[2] + nh * NF, F.f[4] + par * NF, b));
+    const Ar<R> nw = stored<R>(p_bc_value<LdPlain>(d, g, F, P, pr, F.f[0] + nh * NF, F.f[1] + nh * NF,
+                                                   F.f[2] + nh * NF, F.f[4] + par * NF, b));
     const BFace B = bface(d, b);
     const int fw0 = B.cell.face(d, B.pos);
     F.f[3][(1 - par) * NF + fw0] = nw;
@@ -2182,27 +2214,28 @@ __host__ __device__ constexpr int p_term(int dd, int t) {
 // ---- integrate_pressure_field_i for the +xi_dd face of cell x
 // (nse.f90:1091-1289): the new value from the pressures pr
 template <class Ld, class R>
-__device__ __forceinline__ double p_face_value(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P,
-                                               const R *pr, const Cell &x, int dd) {
+__device__ __forceinline__ Ar<R> p_face_value(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P,
+                                              const R *pr, const Cell &x, int dd) {
+  using V = Ar<R>;
   const size_t Nc = d.Nc;
   const int c = x.c;
   const int diag = (dd == 1) ? 2 : (dd == 2) ? 6 : 10;
   const Cell n2 = x.nb(d, 2 * dd);
   const R *A = g.AA + (size_t)15 * (dd - 1) * Nc;
-  const double B1 = (F.Rp[c]) * A[12 * Nc + c];
-  const double B2 = (F.Rp[n2.c]) * A[14 * Nc + c];
-  const double B3 = (g.dg[(2 * (dd - 1)) * Nc + c]) * tangential<Ld>(d, pr, x, 2 * dd, tr1(dd));
-  const double B4 = (g.dg[(2 * (dd - 1) + 1) * Nc + c]) * tangential<Ld>(d, pr, x, 2 * dd, tr2(dd));
-  double s = 0.0;
+  const V B1 = (F.Rp[c]) * A[12 * Nc + c];
+  const V B2 = (F.Rp[n2.c]) * A[14 * Nc + c];
+  const V B3 = (g.dg[(2 * (dd - 1)) * Nc + c]) * tangential<Ld>(d, pr, x, 2 * dd, tr1(dd));
+  const V B4 = (g.dg[(2 * (dd - 1) + 1) * Nc + c]) * tangential<Ld>(d, pr, x, 2 * dd, tr2(dd));
+  V s = 0.0;
 #pragma unroll
   for (int t = 0; t < 10; ++t) {
     const int pt = p_term(dd, t), coef = pt & 15, fpos = (pt >> 4) & 7, cell = pt >> 7;
     const Cell &cl = (cell == 1) ? x : n2;
-    const double term = A[(size_t)(coef - 1) * Nc + c] * Ld::ld(pr, cl.face(d, fpos));
+    const V term = A[(size_t)(coef - 1) * Nc + c] * Ld::ld(pr, cl.face(d, fpos));
     s = (t == 0) ? -term : s - term;
   }
   const int fo = x.face(d, 2 * dd);
-  const double w = P.w_p;
+  const V w = V(P.w_p);
   return (1 - w) * Ld::ld(pr, fo) + w / (A[(size_t)(diag - 1) * Nc + c]) * (s + B1 + B2 + B3 + B4);
 }
 
@@ -2212,23 +2245,24 @@ __device__ __forceinline__ double p_face_value(const Dims &d, const GeoT<R> &g, 
 // tangential cross terms (the centred B3/B4 the source forms first are
 // overwritten before use).  fr faces, cv / co cells and old cells.
 template <class Ld, class R>
-__device__ __forceinline__ double v1_face_value(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P,
-                                                const R *fr, const R *cv, const R *co, const R *Bq, const Cell &x,
-                                                int dd, double w) {
+__device__ __forceinline__ Ar<R> v1_face_value(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P,
+                                               const R *fr, const R *cv, const R *co, const R *Bq, const Cell &x,
+                                               int dd, Ar<R> w) {
+  using V = Ar<R>;
   const size_t Nc = d.Nc;
   const int c = x.c;
   const Cell n2 = x.nb(d, 2 * dd);
   const R *A = F.AAv + (size_t)15 * (dd - 1) * Nc;
-  const double B1 = Bq[c] * A[12 * Nc + c] * 2 * P.DT;
-  const double B2 = Bq[n2.c] * A[14 * Nc + c] * 2 * P.DT;
-  const double B3 = (g.dg[(2 * (dd - 1)) * Nc + c]) * tangential<Ld>(d, fr, x, 2 * dd, tr1(dd));
-  const double B4 = (g.dg[(2 * (dd - 1) + 1) * Nc + c]) * tangential<Ld>(d, fr, x, 2 * dd, tr2(dd));
-  double s = 0.0;
+  const V B1 = Bq[c] * A[12 * Nc + c] * 2 * V(P.DT);
+  const V B2 = Bq[n2.c] * A[14 * Nc + c] * 2 * V(P.DT);
+  const V B3 = (g.dg[(2 * (dd - 1)) * Nc + c]) * tangential<Ld>(d, fr, x, 2 * dd, tr1(dd));
+  const V B4 = (g.dg[(2 * (dd - 1) + 1) * Nc + c]) * tangential<Ld>(d, fr, x, 2 * dd, tr2(dd));
+  V s = V(0.0);
 #pragma unroll
   for (int t = 0; t < 10; ++t) {
     const int pt = p_term(dd, t), coef = pt & 15, fpos = (pt >> 4) & 7, cell = pt >> 7;
     const Cell &cl = (cell == 1) ? x : n2;
-    const double term = A[(size_t)(coef - 1) * Nc + c] * Ld::ld(fr, cl.face(d, fpos));
+    const V term = A[(size_t)(coef - 1) * Nc + c] * Ld::ld(fr, cl.face(d, fpos));
     s = (t == 0) ? -term : s - term;
   }
   s = s - A[11 * Nc + c] * (Ld::ld(cv, c) - co[c]) - A[13 * Nc + c] * (Ld::ld(cv, n2.c) - co[n2.c]);
@@ -2240,6 +2274,7 @@ __device__ __forceinline__ double v1_face_value(const Dims &d, const GeoT<R> &g,
 // cur -> next.  Block (CB, 3): threadIdx.y = direction.
 template <class R>
 __global__ void __launch_bounds__(CB3, 2) k_vel1_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  using V = Ar<R>;
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<3>(red);
@@ -2257,8 +2292,8 @@ __global__ void __launch_bounds__(CB3, 2) k_vel1_face(Dims d, GeoT<R> g, FieldsT
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
         const R *fr = F.f[q] + par * NF;
-        const double nw = stored<R>(
-            v1_face_value<LdPlain>(d, g, F, P, fr, F.c[q], F.co[q], F.Bv + (size_t)q * Nc, x, dd, P.w[q]));
+        const V nw = stored<R>(
+            v1_face_value<LdPlain>(d, g, F, P, fr, F.c[q], F.co[q], F.Bv + (size_t)q * Nc, x, dd, V(P.w[q])));
         F.f[q][(1 - par) * NF + fo] = nw;
         e[q] = errv(nw, fr[fo], first);
       }
@@ -2270,7 +2305,7 @@ __global__ void __launch_bounds__(CB3, 2) k_vel1_face(Dims d, GeoT<R> g, FieldsT
 // ---- K5: integrate_pressure_field_i, cur -> next.
 // Block (CB, 3): threadIdx.y = direction.
 template <class R>
-__global__ void __launch_bounds__(CB3, 5) k_p_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+__global__ void __launch_bounds__(CB3, minb<R>(5, PFACE_MINB_F)) k_p_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
@@ -2285,7 +2320,7 @@ __global__ void __launch_bounds__(CB3, 5) k_p_face(Dims d, GeoT<R> g, FieldsT<R>
       if (!x.has_nb(d, 2 * dd)) return;
       const size_t NF = d.NF;
       const R *pr = F.f[3] + par * NF;
-      const double nw = stored<R>(p_face_value<LdPlain>(d, g, F, P, pr, x, dd));
+      const Ar<R> nw = stored<R>(p_face_value<LdPlain>(d, g, F, P, pr, x, dd));
       const int fo = x.face(d, 2 * dd);
       F.f[3][(1 - par) * NF + fo] = nw;
       e[0] = errv(nw, pr[fo], first);
@@ -2337,8 +2372,8 @@ __global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, GeoT<R> g, FieldsT<R>
     const Cell c2 = B.cell.nb(d, in), c3 = c2.nb(d, in);
     R *T = F.f[4] + par * NF;
     const int f1 = B.cell.face(d, B.pos);
-    const double nw = stored<R>((+g.zf[NB + b] * T[B.cell.face(d, in)] - g.zf[2 * NB + b] * T[c2.face(d, in)] +
-                                 g.zf[3 * NB + b] * T[c3.face(d, in)]) / g.zf[b]);
+    const Ar<R> nw = stored<R>((+g.zf[NB + b] * T[B.cell.face(d, in)] - g.zf[2 * NB + b] * T[c2.face(d, in)] +
+                                g.zf[3 * NB + b] * T[c3.face(d, in)]) / g.zf[b]);
     e[0] = d.owns(B.cell.k) ? errv(nw, T[f1], first) : 0.;
     T[f1] = nw;
   }
@@ -2392,13 +2427,14 @@ __global__ void __launch_bounds__(BLK, 4) k_T_coef(Dims d, GeoT<R> g, FieldsT<R>
 // SRC_ONLY (reference-order schedule): store MT_F4 and R_D_T and leave the
 // update to k_seq_T.
 template <bool SRC_ONLY, class R>
-__global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+__global__ void __launch_bounds__(CB3, minb<R>(5, TCELL_MINB_F)) k_T_cell(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  using V = Ar<R>;
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
-  __shared__ double sX[3][2][CB];   // cross derivatives
-  __shared__ double sF4[8][CB];     // MT_F4, formed by thread 1
-  __shared__ double sG[CB];         // G1 dT/dx + G2 dT/dy + G3 dT/dz, by thread 2
+  __shared__ V sX[3][2][CB];   // cross derivatives
+  __shared__ V sF4[8][CB];     // MT_F4, formed by thread 1
+  __shared__ V sG[CB];         // G1 dT/dx + G2 dT/dy + G3 dT/dz, by thread 2
   const int par = parity(ctl);
   const bool first = ctl->first;
   const int tx = threadIdx.x;
@@ -2413,12 +2449,12 @@ __global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, GeoT<R> g, FieldsT<R>
   if (active) by_dir(threadIdx.y, [&](auto D) {
     constexpr int dd = decltype(D)::value, y = dd - 1;
     const R *MA = F.MTA + (size_t)y * Nc;  // MT_A(q, dd) at MA[3q Nc]
-    double G[5] = {0., 0., 0., 0., 0.};
+    V G[5] = {V(0.), V(0.), V(0.), V(0.), V(0.)};
     if (x.has_nb(d, 2 * dd)) {
       const int c2 = x.nb(d, 2 * dd).c;
-      double A[6], A2[6];
+      V A[6], A2[6];
       for (int q = 0; q < 6; ++q) A[q] = MA[3 * q * Nc + c];
-      A2[0] = A2[2] = 0.;  // not used by form_Fd
+      A2[0] = A2[2] = V(0.);  // not used by form_Fd
       A2[1] = MA[3 * Nc + c2];
       A2[3] = MA[9 * Nc + c2];
       A2[4] = MA[12 * Nc + c2];
@@ -2432,43 +2468,43 @@ __global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, GeoT<R> g, FieldsT<R>
     // cross derivatives of calculate_R_D_T: y=0 pxy,pzy  y=1 pyx,pzx  y=2 pxz,pyz
     constexpr int e2 = (y == 0) ? 2 : (y == 1) ? 1 : 3;
     constexpr int fa = (y == 1) ? 4 : 2, fb = (y == 1) ? 3 : 1;
-    sX[y][0][tx] = 0.5 * (tangential(d, T, x, (y == 2) ? 2 : fa, e2) - tangential(d, T, x, (y == 2) ? 1 : fb, e2));
-    sX[y][1][tx] = (y == 2) ? 0.5 * (tangential(d, T, x, 4, 3) - tangential(d, T, x, 3, 3))
-                            : 0.5 * (tangential(d, T, x, 6, e2) - tangential(d, T, x, 5, e2));
+    sX[y][0][tx] = V(0.5) * (tangential(d, T, x, (y == 2) ? 2 : fa, e2) - tangential(d, T, x, (y == 2) ? 1 : fb, e2));
+    sX[y][1][tx] = (y == 2) ? V(0.5) * (tangential(d, T, x, 4, 3) - tangential(d, T, x, 3, 3))
+                            : V(0.5) * (tangential(d, T, x, 6, e2) - tangential(d, T, x, 5, e2));
     if (y == 1) {  // MT_F4 (nim.f90:466-475)
-      double Am[3][6];
+      V Am[3][6];
       for (int k = 0; k < 3; ++k) {
         Am[k][4] = F.MTA[(size_t)(12 + k) * Nc + c];
         Am[k][5] = F.MTA[(size_t)(15 + k) * Nc + c];
       }
-      double F4[8];
+      V F4[8];
       if constexpr (std::is_same<R, float>::value)
-        form_F4_rcp(Am, P.DT, F4);
+        form_F4_rcp(Am, V(P.DT), F4);
       else
-        form_F4(Am, P.DT, F4);
+        form_F4(Am, V(P.DT), F4);
       for (int k = 0; k < 8; ++k) sF4[k][tx] = F4[k];
     } else if (y == 2) {  // the leading G_i d_i T terms of R_D_T, in source order
-      const double px = (T[f[2]] - T[f[1]]) / 2.;
-      const double py = (T[f[4]] - T[f[3]]) / 2.;
-      const double pz = (T[f[6]] - T[f[5]]) / 2.;
+      const V px = (T[f[2]] - T[f[1]]) / V(2.);
+      const V py = (T[f[4]] - T[f[3]]) / V(2.);
+      const V pz = (T[f[6]] - T[f[5]]) / V(2.);
       sG[tx] = g.G[c] * px + g.G[Nc + c] * py + g.G[2 * Nc + c] * pz;
     }
   });
   __syncthreads();
   if (active && threadIdx.y == 0) {
-    double F4[8];
+    V F4[8];
     for (int k = 0; k < 8; ++k) F4[k] = sF4[k][tx];
-    const double pxy = sX[0][0][tx], pzy = sX[0][1][tx], pyx = sX[1][0][tx], pzx = sX[1][1][tx];
-    const double pxz = sX[2][0][tx], pyz = sX[2][1][tx];
+    const V pxy = sX[0][0][tx], pzy = sX[0][1][tx], pyx = sX[1][0][tx], pzx = sX[1][1][tx];
+    const V pxz = sX[2][0][tx], pyz = sX[2][1][tx];
     const R *gij = g.gij;
-    const double RDT = P.alpha * (sG[tx] - gij[3 * Nc + c] * pxy - gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz -
+    const V RDT = V(P.alpha) * (sG[tx] - gij[3 * Nc + c] * pxy - gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz -
                                   gij[2 * Nc + c] * pzx - gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
     if (SRC_ONLY) {
       for (int k = 0; k < 8; ++k) F.MTF4[(size_t)k * Nc + c] = F4[k];
       F.RDT[c] = RDT;
     } else {
-      const double cold = F.c[3][c];
-      const double nw = stored<R>(cell_update(T, f, cold, F.co[3][c], (RDT + 0.), F4, P.w[3]));
+      const V cold = F.c[3][c];
+      const V nw = stored<R>(cell_update(T, f, cold, F.co[3][c], (RDT + V(0.)), F4, V(P.w[3])));
       F.c[3][c] = nw;
       e[0] = errv(nw, cold, first);
     }
@@ -2479,7 +2515,8 @@ __global__ void __launch_bounds__(CB3, 5) k_T_cell(Dims d, GeoT<R> g, FieldsT<R>
 // ---- K8: +xi face updates of T (nse.f90:1033-1088), cur -> next; the z-wall
 // values set by apply_zero_flux travel to the next half too
 template <class R>
-__global__ void __launch_bounds__(BLK, 4) k_T_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+__global__ void __launch_bounds__(BLK, minb<R>(4, TFACE_MINB_F)) k_T_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  using V = Ar<R>;
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
@@ -2496,11 +2533,11 @@ __global__ void __launch_bounds__(BLK, 4) k_T_face(Dims d, GeoT<R> g, FieldsT<R>
     for (int dd = 1; dd <= 3; ++dd) {
       if (!x.has_nb(d, 2 * dd)) continue;
       const Cell x2 = x.nb(d, 2 * dd);
-      double Fd[5];
+      V Fd[5];
       for (int k = 0; k < 5; ++k) Fd[k] = F.MTF[(5 * (dd - 1) + k) * Nc + c];
       const int fo = x.face(d, 2 * dd);
-      const double nw = stored<R>(face_update(d, T, F.c[3], F.co[3], Fd, g.dg[(2 * (dd - 1)) * Nc + c],
-                                              g.dg[(2 * (dd - 1) + 1) * Nc + c], dd, x, x2, P.w[3]));
+      const V nw = stored<R>(face_update(d, T, F.c[3], F.co[3], Fd, g.dg[(2 * (dd - 1)) * Nc + c],
+                                              g.dg[(2 * (dd - 1) + 1) * Nc + c], dd, x, x2, V(P.w[3])));
       Tn[fo] = nw;
       e[0] = nmax(e[0], errv(nw, T[fo], first));
     }
