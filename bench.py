@@ -71,6 +71,7 @@ KERNEL_BYTES_PER_CELL = {
     "k_vel_face_tile": 8 * 45,  # the same sweep staged by TMA boxes (same algorithmic bytes)
     "k_vel_cell_tile": 8 * 53,  # k_vel_cell with its u, v, w faces staged by TMA boxes
     "k_vel_cell2": 8 * 53,  # k_vel_cell on cell pairs with paired loads (same algorithmic bytes)
+    "k_vel_cellN": 8 * 53,  # the float mirror's form: four cells a thread (same words; the mixed line halves them)
     "k_p_src": 8 * 39,      # faces u,v,w,T,p (15) area,normal,vol (13) G,g^ij (9); write dila,Rp (2)
     "k_p_face": 8 * 52,     # faces p (3) Rp (1) AA used (39) dg (6); write faces p (3)
     "k_T_coef": 8 * 42,     # cells+old u,v,w (6) xi (9) g^ij diagonal (3) gfd (6); write MT_A (18)
@@ -503,8 +504,9 @@ def run_mixed(case, mesh, args, fp64_stats, fp64_fields, fp64_value, fp64_ms_ste
     recs += timed
     iters = sum(r.iters for r in timed)
     value = case.ncells * iters / (ms / 1e3)
-    nu = [max(abs(a.nu_inner - b.nu_inner) / abs(b.nu_inner), abs(a.nu_outer - b.nu_outer) / abs(b.nu_outer))
-          for a, b in zip(recs, fp64_stats)]
+    nu_in = [abs(a.nu_inner - b.nu_inner) / abs(b.nu_inner) for a, b in zip(recs, fp64_stats)]
+    nu_out = [abs(a.nu_outer - b.nu_outer) / abs(b.nu_outer) for a, b in zip(recs, fp64_stats)]
+    nu = [max(a, b) for a, b in zip(nu_in, nu_out)]
     err = {}
     for f in MIXED_FIELDS:
         a, b = s.download(f), fp64_fields[f]
@@ -520,8 +522,12 @@ def run_mixed(case, mesh, args, fp64_stats, fp64_fields, fp64_value, fp64_ms_ste
         "value": value, "unit": UNIT, "ms_per_step": ms / max(args.steps, 1), "iterations": iters,
         "iters_fp32": sum(r.iters_fp32 for r in timed), "speedup_vs_fp64": value / fp64_value,
         "step_time_speedup_vs_fp64": fp64_ms_step / (ms / max(args.steps, 1)),
-        "dtype": "f32 storage of the swept arrays, f64 arithmetic, reductions and refinement",
+        "dtype": "FP32 phase: f32 storage and arithmetic of the swept arrays; f64 maxima, per-step work, "
+                 "reductions and refinement",
         "nu_rel_err_max": max(nu) if nu else None, "nu_rel_err_per_step": nu,
+        "nu_inner_rel_err_per_step": nu_in, "nu_outer_rel_err_per_step": nu_out,
+        "nu_fp64_per_step": [[b.nu_inner, b.nu_outer] for b in fp64_stats[:len(recs)]],
+        "nu_mixed_per_step": [[a.nu_inner, a.nu_outer] for a in recs],
         "field_err_final": err,
         "tolerances": ("reference (tol_u,v,w,T 1e-6, tol_p 5e-3): both runs stop once a pass changes every "
                        "field by less than its tolerance" if args.stop_tol is None else

@@ -155,9 +155,9 @@ typedef struct nim_params {
   int32_t precision;    /* NIM_PRECISION_FP64 (0): every pass in FP64, as the
                            reference; NIM_PRECISION_MIXED (1): each step's
                            inner loop first sweeps a float copy of the
-                           fields, NIM constants and geometry (arithmetic
-                           in double registers, maxima of the stored
-                           changes in double) until the tolerances hold or
+                           fields, NIM constants and geometry (float
+                           arithmetic, maxima of the stored changes in
+                           double) until the tolerances hold or
                            8 passes in a row bring no new smallest change
                            to a field above its tolerance; the iterate is
                            then widened and FP64 passes run until the

@@ -112,6 +112,7 @@ struct nim_ctx {
   // k_vel_cell_tile (TMA-staged cell sweep of u, v, w, formulation 2)
   bool cell_tile = false;
   bool cell_pair = false;  // k_vel_cell2: two theta-adjacent cells per thread
+  bool cell_quad = false;  // the float mirror's cell sweep as k_vel_cellN, four cells a thread
   VelCellMaps cmap64{}, cmap32{};
   GeoT<float> g32{};
   FieldsT<float> F32{};
@@ -292,6 +293,15 @@ int launch_vel(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F
       const VelCellMaps &M = std::is_same<R, double>::value ? x->cmap64 : x->cmap32;
       k_vel_cell_tile<R><<<gt, dim3(CT_T, 3), CtLayout<R>::bytes, s>>>(d, g, F, x->phys, x->ctl, x->tile_kc, M);
       TRY(mark(x, "k_vel_cell_tile"));
+    } else if (std::is_same<R, float>::value && x->cell_quad) {
+      if constexpr (std::is_same<R, float>::value) {
+        const dim3 gq((d.NT + 127) / 128, (d.NR + 3) / 4, d.NZ);
+        if (x->slab_count)
+          k_vel_cellN<R, 4, true><<<gq, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+        else
+          k_vel_cellN<R, 4><<<gq, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+        TRY(mark(x, "k_vel_cellN"));
+      }
     } else if (x->cell_pair) {
       const dim3 gp((d.NT + 63) / 64, (d.NR + 3) / 4, d.NZ);
       if (x->slab_count)
@@ -888,9 +898,11 @@ static bool encode_vel_cell_maps(const Dims &d, const FieldsT<R> &F, VelCellMaps
 // chunks of at least 8 planes.  NIM_FACE_SWEEP=tile or =gather in the
 // environment forces the choice (tile still needs the n_theta conditions).
 // The source and cell sweep of u, v, w (formulation 2) runs as k_vel_cell2
-// (two theta-adjacent cells per thread, paired loads) when n_theta is even;
-// NIM_CELL_SWEEP=gather forces k_vel_cell, =tile k_vel_cell_tile (under the
-// tile's n_theta conditions).
+// (two theta-adjacent cells per thread, paired loads) when n_theta is even,
+// and for the float mirror as k_vel_cellN (four cells a thread, float4
+// loads) when n_theta % 4 == 0; NIM_CELL_SWEEP=gather forces k_vel_cell,
+// =pair k_vel_cell2, =tile k_vel_cell_tile (under the tile's n_theta
+// conditions).
 static int choose_face_sweep(nim_ctx *x) {
   const Dims &d = x->d;
   int sms = 0;
@@ -910,8 +922,10 @@ static int choose_face_sweep(nim_ctx *x) {
   const char *envc = std::getenv("NIM_CELL_SWEEP");
   const std::string cell = envc ? envc : "";
   x->cell_tile = shape && !x->seq && x->params.formulation == 2 && cell == "tile";
-  // the paired-load form whenever n_theta is even, unless another is asked for
+  // the paired-load form whenever n_theta is even, unless another is asked for;
+  // the float mirror's sweeps four cells a thread when n_theta % 4 == 0
   x->cell_pair = !x->cell_tile && d.NT % 2 == 0 && !x->seq && x->params.formulation == 2 && cell != "gather";
+  x->cell_quad = x->cell_pair && d.NT % 4 == 0 && cell != "pair";
   return NIM_OK;
 }
 

@@ -38,7 +38,7 @@ namespace nim {
 // ------------------------------------------------------------ device state
 // Geometry and field arrays, by storage type R: double for the FP64 path;
 // float for the mirror the mixed-precision inner loop sweeps (every array the
-// parallel iteration reads or writes, arithmetic still in double registers).
+// parallel iteration reads or writes; its kernels compute in float, Ar<R>).
 template <class R>
 struct GeoT {
   R *vol;     // [Nc]
@@ -135,6 +135,7 @@ constexpr int VC2_MINB = 3;  // resident blocks per SM asked of k_vel_cell2 (56 
 // resident blocks per SM the float instantiations of the pass kernels ask
 // for: computing in float they need about half the FP64 registers
 constexpr int VC2_MINB_F = 3, PSRC_MINB_F = 4, PFACE_MINB_F = 5, TCELL_MINB_F = 5, TFACE_MINB_F = 4;
+constexpr int VCN_MINB = 2;  // k_vel_cellN (four float cells a thread)
 template <class R>
 constexpr int minb(int fp64, int fp32) {
   return sizeof(R) == 8 ? fp64 : fp32;
@@ -1525,6 +1526,266 @@ __global__ void __launch_bounds__(CB3, minb<R>(VC2_MINB, VC2_MINB_F)) k_vel_cell
     out.y = (R)nw1;
     *reinterpret_cast<typename Pair2<R>::T *>(F.c[q] + c) = out;
     e[q] = nmax(errv(nw0, cv0, first), errv(nw1, cv1, first));
+  }
+  if (!SLAB || d.owns(k)) block_max<3, CB3>(red, e, ctl->err[par]);
+}
+
+// ---- K1, NP cells per thread: k_vel_cell2's sweep over NP theta-adjacent
+// cells (i a multiple of NP), every value the NP cells share a row for in
+// one NP-wide vector load (float4 for the float mirror: 16 bytes a load,
+// as FP64's pairs): the cell arrays, the r and z faces, the theta faces at
+// i..i+NP-1 (the +theta face of cell p is the -theta face of cell p+1) and
+// the r- and z-stencil rows; single loads only for the theta-stencil ends
+// (i-1, i+NP) and the +theta face of the last cell.  Each cell's terms are
+// k_vel_cell's in its order.  Needs n_theta % NP == 0 (every vector
+// NP-aligned); block (CB, 3) over patches of 32 NP x CB/32 cells.
+template <class R, int NP>
+struct VecN;
+template <>
+struct VecN<float, 4> {
+  using T = float4;
+};
+template <>
+struct VecN<float, 2> {
+  using T = float2;
+};
+template <>
+struct VecN<double, 2> {
+  using T = double2;
+};
+template <class R, int NP>
+__device__ __forceinline__ void ldN(const R *__restrict__ p, int i, R (&v)[NP]) {
+  const typename VecN<R, NP>::T t = *reinterpret_cast<const typename VecN<R, NP>::T *>(p + i);
+  const R *e = reinterpret_cast<const R *>(&t);
+#pragma unroll
+  for (int q = 0; q < NP; ++q) v[q] = e[q];
+}
+template <class R, int NP>
+__device__ __forceinline__ void stN(R *__restrict__ p, int i, const R (&v)[NP]) {
+  typename VecN<R, NP>::T t;
+  R *e = reinterpret_cast<R *>(&t);
+#pragma unroll
+  for (int q = 0; q < NP; ++q) e[q] = v[q];
+  *reinterpret_cast<typename VecN<R, NP>::T *>(p + i) = t;
+}
+
+template <class R, int NP, bool SLAB = false>
+__global__ void __launch_bounds__(CB3, VCN_MINB) k_vel_cellN(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  using V = Ar<R>;
+  if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<3>(red);
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int q = threadIdx.y;
+  const int i = blockIdx.x * (32 * NP) + NP * (threadIdx.x & 31);
+  const int j = blockIdx.y * (CB / 32) + (threadIdx.x >> 5);
+  const int k = blockIdx.z;
+  double e[3] = {0., 0., 0.};
+  if (i < d.NT && j < d.NR) {
+    const int Nc = d.Nc, NF = d.NF, NT = d.NT, NR = d.NR, pl = d.plane;
+    const int c = i + NT * (j + NR * k);  // cell i; cell p of the group is c + p
+    const int im1 = (i == 0) ? NT - 1 : i - 1, ipn = (i + NP >= NT) ? i + NP - NT : i + NP;
+    const int f1 = c + NT * k;
+    const int fi[7] = {0, f1, f1 + NT, d.offT + c, d.offT + c + 1, d.offZ + c, d.offZ + c + pl};
+    const int f4b = d.offT + c - i + ipn;  // +theta face of the last cell
+    // face m of the NP cells from array a
+    auto faceN = [&](const R *a, int m, R (&v)[NP]) {
+      if (m == 4) {
+        R t[NP];
+        ldN<R, NP>(a, fi[3], t);
+#pragma unroll
+        for (int p = 0; p + 1 < NP; ++p) v[p] = t[p + 1];
+        v[NP - 1] = a[f4b];
+      } else {
+        ldN<R, NP>(a, fi[m], v);
+      }
+    };
+    // RB = base + 1/rho * green_gauss (component q), faces 2, 1, 4, 3, 6, 5
+    const R *pp = F.f[3] + par * NF, *nq = g.normal + q * NF;
+    V gs[NP];
+    {
+      const int order[6] = {2, 1, 4, 3, 6, 5};
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        const int m = order[t];
+        R pv[NP], av[NP], nv[NP];
+        faceN(pp, m, pv);
+        faceN(g.area, m, av);
+        faceN(nq, m, nv);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          const V tp = (V)pv[p] * av[p] * (nv[p]);
+          gs[p] = (t == 0) ? tp : (t & 1) ? gs[p] - tp : gs[p] + tp;
+        }
+      }
+    }
+    V RB[NP];
+    {
+      R vol[NP];
+      ldN<R, NP>(g.vol, c, vol);
+      V base[NP];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) base[p] = V(0.);
+      if (q == 2) {
+        R t[NP], o[NP];
+        ldN<R, NP>(F.c[3], c, t);
+        ldN<R, NP>(F.co[3], c, o);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) base[p] = -(V(P.g_beta) * V(0.5) * (t[p] + o[p]));
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) RB[p] = base[p] + V(P.inv_rho) * ((V(1.) / vol[p]) * gs[p]);
+    }
+    // own faces of component q (stored values)
+    const R *fr = F.f[q] + par * NF;
+    R o[7][NP];
+#pragma unroll
+    for (int m = 1; m <= 6; ++m) faceN(fr, m, o[m]);
+    auto along = [&](bool lo, bool hi, V v0, V va, V vb) {
+      return lo ? tang_vals(true, false, v0, va, vb, V(0.), V(0.))
+                : hi ? tang_vals(false, true, v0, V(0.), V(0.), va, vb) : tang_vals(false, false, v0, vb, V(0.), va, V(0.));
+    };
+    const bool rlo = (j == 0), rhi = (j == NR - 1);
+    const int ra = rlo ? j + 1 : j - 1, rb = rlo ? j + 2 : (rhi ? j - 2 : j + 1);
+    const bool zlo = (k == 0), zhi = (k == d.NZ - 1);
+    const int ka = zlo ? k + 1 : k - 1, kb = zlo ? k + 2 : (zhi ? k - 2 : k + 1);
+    V s[NP];
+    {
+      R a[NP];
+      ldN<R, NP>(g.G, c, a);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) s[p] = a[p] * ((o[2][p] - o[1][p]) / V(2.));
+      ldN<R, NP>(g.G + Nc, c, a);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) s[p] = s[p] + a[p] * ((o[4][p] - o[3][p]) / V(2.));
+      ldN<R, NP>(g.G + 2 * Nc, c, a);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) s[p] = s[p] + a[p] * ((o[6][p] - o[5][p]) / V(2.));
+    }
+    auto term = [&](int slot, const V (&dv)[NP]) {
+      R a[NP];
+      ldN<R, NP>(g.gij + slot * Nc, c, a);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) s[p] = s[p] - a[p] * dv[p];
+    };
+    {  // pxy: r faces (rows j, j+1) at theta i-1 .. i+NP (centred in theta)
+      const int rrow = NT * (j + (NR + 1) * k);
+      const V r_m1 = fr[rrow + im1], r_pn = fr[rrow + ipn];
+      const V r1_m1 = fr[rrow + NT + im1], r1_pn = fr[rrow + NT + ipn];
+      V dv[NP];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const V up2 = (p + 1 < NP) ? (V)o[2][p + 1] : r1_pn, um2 = (p > 0) ? (V)o[2][p - 1] : r1_m1;
+        const V up1 = (p + 1 < NP) ? (V)o[1][p + 1] : r_pn, um1 = (p > 0) ? (V)o[1][p - 1] : r_m1;
+        dv[p] = V(0.5) * ((up2 - um2) / V(4.) - (up1 - um1) / V(4.));
+      }
+      term(3, dv);
+    }
+    {  // pyx: theta faces of rows a, b
+      const int tra = d.offT + NT * (ra + NR * k), trb = d.offT + NT * (rb + NR * k);
+      R av[NP + 1], bv[NP + 1];
+      {
+        R t[NP];
+        ldN<R, NP>(fr, tra + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) av[p] = t[p];
+        ldN<R, NP>(fr, trb + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) bv[p] = t[p];
+        av[NP] = fr[tra + ipn];
+        bv[NP] = fr[trb + ipn];
+      }
+      V dv[NP];
+#pragma unroll
+      for (int p = 0; p < NP; ++p)
+        dv[p] = V(0.5) * (along(rlo, rhi, o[4][p], av[p + 1], bv[p + 1]) - along(rlo, rhi, o[3][p], av[p], bv[p]));
+      term(1, dv);
+    }
+    {  // pxz: r faces (rows j, j+1) of planes a, b
+      const int rka = NT * (j + (NR + 1) * ka), rkb = NT * (j + (NR + 1) * kb);
+      R pa[NP], pb[NP], pA[NP], pB[NP];
+      ldN<R, NP>(fr, rka + i, pa);
+      ldN<R, NP>(fr, rkb + i, pb);
+      ldN<R, NP>(fr, rka + NT + i, pA);
+      ldN<R, NP>(fr, rkb + NT + i, pB);
+      V dv[NP];
+#pragma unroll
+      for (int p = 0; p < NP; ++p)
+        dv[p] = V(0.5) * (along(zlo, zhi, o[2][p], pA[p], pB[p]) - along(zlo, zhi, o[1][p], pa[p], pb[p]));
+      term(6, dv);
+    }
+    {  // pzx: z faces (levels k, k+1) of rows a, b
+      const int zra = d.offZ + NT * (ra + NR * k), zrb = d.offZ + NT * (rb + NR * k);
+      R za[NP], zb[NP], zA[NP], zB[NP];
+      ldN<R, NP>(fr, zra + i, za);
+      ldN<R, NP>(fr, zrb + i, zb);
+      ldN<R, NP>(fr, zra + pl + i, zA);
+      ldN<R, NP>(fr, zrb + pl + i, zB);
+      V dv[NP];
+#pragma unroll
+      for (int p = 0; p < NP; ++p)
+        dv[p] = V(0.5) * (along(rlo, rhi, o[6][p], zA[p], zB[p]) - along(rlo, rhi, o[5][p], za[p], zb[p]));
+      term(2, dv);
+    }
+    {  // pyz: theta faces of planes a, b
+      const int tka = d.offT + NT * (j + NR * ka), tkb = d.offT + NT * (j + NR * kb);
+      R av[NP + 1], bv[NP + 1];
+      {
+        R t[NP];
+        ldN<R, NP>(fr, tka + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) av[p] = t[p];
+        ldN<R, NP>(fr, tkb + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) bv[p] = t[p];
+        av[NP] = fr[tka + ipn];
+        bv[NP] = fr[tkb + ipn];
+      }
+      V dv[NP];
+#pragma unroll
+      for (int p = 0; p < NP; ++p)
+        dv[p] = V(0.5) * (along(zlo, zhi, o[4][p], av[p + 1], bv[p + 1]) - along(zlo, zhi, o[3][p], av[p], bv[p]));
+      term(7, dv);
+    }
+    {  // pzy: z faces (levels k, k+1) at theta i-1 .. i+NP
+      const int zlev = d.offZ + NT * (j + NR * k);
+      const V z_m1 = fr[zlev + im1], z_pn = fr[zlev + ipn];
+      const V z1_m1 = fr[zlev + pl + im1], z1_pn = fr[zlev + pl + ipn];
+      V dv[NP];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const V up6 = (p + 1 < NP) ? (V)o[6][p + 1] : z1_pn, um6 = (p > 0) ? (V)o[6][p - 1] : z1_m1;
+        const V up5 = (p + 1 < NP) ? (V)o[5][p + 1] : z_pn, um5 = (p > 0) ? (V)o[5][p - 1] : z_m1;
+        dv[p] = V(0.5) * ((up6 - um6) / V(4.) - (up5 - um5) / V(4.));
+      }
+      term(5, dv);
+    }
+    // cell update (cell_update), term by term
+    R cv[NP], co[NP], a[NP], F40[NP];
+    ldN<R, NP>(F.c[q], c, cv);
+    ldN<R, NP>(F.co[q], c, co);
+    const V w = V(P.w[q]);
+    ldN<R, NP>(F.MF4, c, F40);
+    ldN<R, NP>(F.MF4 + Nc, c, a);
+    V u[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) u[p] = +a[p] * (V)co[p];
+#pragma unroll
+    for (int m = 2; m <= 7; ++m) {
+      ldN<R, NP>(F.MF4 + m * Nc, c, a);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) u[p] = u[p] + a[p] * (V)o[m - 1][p];
+    }
+    R out[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const V B = (V(0.) + V(P.inv_Re) * s[p] + RB[p]);
+      const V nw = stored<R>((1 - w) * (V)cv[p] + (w / F40[p]) * (u[p] + B));
+      out[p] = (R)nw;
+      e[q] = nmax(e[q], errv(nw, cv[p], first));
+    }
+    stN<R, NP>(F.c[q], c, out);
   }
   if (!SLAB || d.owns(k)) block_max<3, CB3>(red, e, ctl->err[par]);
 }
