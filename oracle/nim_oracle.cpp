@@ -19,23 +19,43 @@
 #ifdef _OPENMP
 #include <omp.h>
 #endif
+#ifdef NIM_ORACLE_TANGENT
+#include "nim_dual.h"
+#endif
+
+// The scalar of every value the time advance computes: real, or in the
+// tangent-linear build (nim_oracle_tl.cpp) a Dual carrying the value and its
+// derivative along the seeded direction.  The values are the same bits in
+// both builds.
+#ifdef NIM_ORACLE_TANGENT
+using real = nimtl::Dual;
+using nimtl::tan_of;
+using nimtl::val;
+#define nim_oracle nim_oracle_tl  // a type of its own in the tangent build
+#define NIM_ORACLE_FN(name) nim_oracle_tl_##name
+#else
+using real = double;
+inline double val(double a) { return a; }
+inline double tan_of(double) { return 0.0; }
+#define NIM_ORACLE_FN(name) nim_oracle_##name
+#endif
 
 namespace {
 
 // ------------------------------------------------------------------ arrays
 // 1-based vectors: a(i) with i = 1..n, and (K, n) column-major blocks.
 struct V1 {
-  std::vector<double> d;
+  std::vector<real> d;
   void alloc(int64_t n) { d.assign(n + 1, 0.0); }
-  double &operator()(int64_t i) { return d[i]; }
-  const double &operator()(int64_t i) const { return d[i]; }
+  real &operator()(int64_t i) { return d[i]; }
+  const real &operator()(int64_t i) const { return d[i]; }
 };
 template <int K>
 struct VK {
-  std::vector<double> d;
+  std::vector<real> d;
   void alloc(int64_t n) { d.assign((size_t)K * (n + 1), 0.0); }
-  double &operator()(int k, int64_t i) { return d[(size_t)K * i + (k - 1)]; }
-  const double &operator()(int k, int64_t i) const { return d[(size_t)K * i + (k - 1)]; }
+  real &operator()(int k, int64_t i) { return d[(size_t)K * i + (k - 1)]; }
+  const real &operator()(int k, int64_t i) const { return d[(size_t)K * i + (k - 1)]; }
 };
 template <int K>
 struct IK {
@@ -46,34 +66,34 @@ struct IK {
 };
 // (3,3,n) and (3,3,6,n) blocks
 struct M33 {
-  std::vector<double> d;
+  std::vector<real> d;
   void alloc(int64_t n) { d.assign((size_t)9 * (n + 1), 0.0); }
-  double &operator()(int a, int b, int64_t i) { return d[(size_t)9 * i + (a - 1) + 3 * (b - 1)]; }
-  const double &operator()(int a, int b, int64_t i) const { return d[(size_t)9 * i + (a - 1) + 3 * (b - 1)]; }
+  real &operator()(int a, int b, int64_t i) { return d[(size_t)9 * i + (a - 1) + 3 * (b - 1)]; }
+  const real &operator()(int a, int b, int64_t i) const { return d[(size_t)9 * i + (a - 1) + 3 * (b - 1)]; }
 };
 struct M336 {
-  std::vector<double> d;
+  std::vector<real> d;
   void alloc(int64_t n) { d.assign((size_t)54 * (n + 1), 0.0); }
-  double &operator()(int a, int b, int f, int64_t i) {
+  real &operator()(int a, int b, int f, int64_t i) {
     return d[(size_t)54 * i + (a - 1) + 3 * (b - 1) + 9 * (f - 1)];
   }
-  const double &operator()(int a, int b, int f, int64_t i) const {
+  const real &operator()(int a, int b, int f, int64_t i) const {
     return d[(size_t)54 * i + (a - 1) + 3 * (b - 1) + 9 * (f - 1)];
   }
 };
 struct M36 {  // (3,6,n)
-  std::vector<double> d;
+  std::vector<real> d;
   void alloc(int64_t n) { d.assign((size_t)18 * (n + 1), 0.0); }
-  double &operator()(int a, int b, int64_t i) { return d[(size_t)18 * i + (a - 1) + 3 * (b - 1)]; }
-  const double &operator()(int a, int b, int64_t i) const { return d[(size_t)18 * i + (a - 1) + 3 * (b - 1)]; }
+  real &operator()(int a, int b, int64_t i) { return d[(size_t)18 * i + (a - 1) + 3 * (b - 1)]; }
+  const real &operator()(int a, int b, int64_t i) const { return d[(size_t)18 * i + (a - 1) + 3 * (b - 1)]; }
 };
 
 // ------------------------------------------------------------- arithmetic
 // x**n for constant integer n the way gfortran expands it (gfc_conv_powi and
 // its powi_table: x^n = x^(n-t[n]) * x^t[n]).
 struct Pw {
-  double p[13];
-  explicit Pw(double x) {
+  real p[13];
+  explicit Pw(real x) {
     p[0] = 1.0;
     p[1] = x;
     p[2] = p[1] * p[1];
@@ -88,16 +108,16 @@ struct Pw {
     p[11] = p[5] * p[6];
     p[12] = p[6] * p[6];
   }
-  double operator[](int n) const { return p[n]; }
+  real operator[](int n) const { return p[n]; }
 };
 
 // det and inv3x3 of general.f90:840-857 on a 0-based 3x3 a[r][c].
-inline double det3(const double a[3][3]) {
+inline real det3(const real a[3][3]) {
   return a[0][0] * a[1][1] * a[2][2] + a[0][1] * a[1][2] * a[2][0] + a[0][2] * a[1][0] * a[2][1] -
          a[0][2] * a[1][1] * a[2][0] - a[0][1] * a[1][0] * a[2][2] - a[0][0] * a[1][2] * a[2][1];
 }
-inline void inv3(const double a[3][3], double x[3][3]) {
-  const double s = 1 / det3(a);
+inline void inv3(const real a[3][3], real x[3][3]) {
+  const real s = 1 / det3(a);
   x[0][0] = s * (a[1][1] * a[2][2] - a[2][1] * a[1][2]);
   x[0][1] = s * (a[0][2] * a[2][1] - a[0][1] * a[2][2]);
   x[0][2] = s * (a[0][1] * a[1][2] - a[0][2] * a[1][1]);
@@ -108,44 +128,44 @@ inline void inv3(const double a[3][3], double x[3][3]) {
   x[2][1] = s * (a[0][1] * a[2][0] - a[0][0] * a[2][1]);
   x[2][2] = s * (a[0][0] * a[1][1] - a[0][1] * a[1][0]);
 }
-inline double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline real dot3(const real *a, const real *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
 // 5-point Gauss-Legendre rule, parameters.f90:18-22
 struct Gauss {
-  double x[5], w[5];
+  real x[5], w[5];
   Gauss() {
-    x[0] = -(1. / 3. * std::sqrt(5. - 2. * std::sqrt(10. / 7.)));
-    x[1] = 1. / 3. * std::sqrt(5. - 2. * std::sqrt(10. / 7.));
+    x[0] = -(1. / 3. * sqrt(5. - 2. * sqrt(10. / 7.)));
+    x[1] = 1. / 3. * sqrt(5. - 2. * sqrt(10. / 7.));
     x[2] = 0.;
-    x[3] = -(1. / 3. * std::sqrt(5. + 2. * std::sqrt(10. / 7.)));
-    x[4] = 1. / 3. * std::sqrt(5. + 2. * std::sqrt(10. / 7.));
-    w[0] = (322. + 13. * std::sqrt(70.)) / 900.;
-    w[1] = (322. + 13. * std::sqrt(70.)) / 900.;
+    x[3] = -(1. / 3. * sqrt(5. + 2. * sqrt(10. / 7.)));
+    x[4] = 1. / 3. * sqrt(5. + 2. * sqrt(10. / 7.));
+    w[0] = (322. + 13. * sqrt(70.)) / 900.;
+    w[1] = (322. + 13. * sqrt(70.)) / 900.;
     w[2] = 128. / 225.;
-    w[3] = (322. - 13. * std::sqrt(70.)) / 900.;
-    w[4] = (322. - 13. * std::sqrt(70.)) / 900.;
+    w[3] = (322. - 13. * sqrt(70.)) / 900.;
+    w[4] = (322. - 13. * sqrt(70.)) / 900.;
   }
 };
 const Gauss GQ;
 
 // Trilinear map of one cell: mesh%C, %D, %E (create_mesh.f90:254-303).
 struct Map {
-  double C[8], D[8], E[8];
+  real C[8], D[8], E[8];
 };
 
 // type curvi3d filled by evaluate_curvilinear (curvilinear.f90:9-41).
 struct Curvi {
-  double x, y, z;
-  double jac[3][3];     // jacmat(r,c) = d x_c / d xi_r
-  double jacinv[3][3];  // inv3x3(jacmat)
-  double g_ij[3][3];    // covariant metric
-  double gij[3][3];     // contravariant metric
-  double gam[3][3][3];  // gamma_tensor
-  double detJ;
+  real x, y, z;
+  real jac[3][3];     // jacmat(r,c) = d x_c / d xi_r
+  real jacinv[3][3];  // inv3x3(jacmat)
+  real g_ij[3][3];    // covariant metric
+  real gij[3][3];     // contravariant metric
+  real gam[3][3][3];  // gamma_tensor
+  real detJ;
 };
 
-void evaluate_curvilinear(const Map &M, double x, double y, double z, Curvi &C) {
-  const double *Cc = M.C, *Dd = M.D, *Ee = M.E;
+void evaluate_curvilinear(const Map &M, real x, real y, real z, Curvi &C) {
+  const real *Cc = M.C, *Dd = M.D, *Ee = M.E;
   C.x = Cc[0] + Cc[1] * x + Cc[2] * y + Cc[3] * z + Cc[4] * x * y + Cc[5] * x * z + Cc[6] * y * z + Cc[7] * x * y * z;
   C.y = Dd[0] + Dd[1] * x + Dd[2] * y + Dd[3] * z + Dd[4] * x * y + Dd[5] * x * z + Dd[6] * y * z + Dd[7] * x * y * z;
   C.z = Ee[0] + Ee[1] * x + Ee[2] * y + Ee[3] * z + Ee[4] * x * y + Ee[5] * x * z + Ee[6] * y * z + Ee[7] * x * y * z;
@@ -161,7 +181,7 @@ void evaluate_curvilinear(const Map &M, double x, double y, double z, Curvi &C) 
   C.jac[2][2] = Ee[3] + Ee[5] * x + Ee[6] * y + Ee[7] * x * y;
   inv3(C.jac, C.jacinv);
   // g_a = jacmat(a,:) (covariant), g^a = jacinv(:,a) (contravariant)
-  double gl[3][3], gu[3][3];
+  real gl[3][3], gu[3][3];
   for (int a = 0; a < 3; ++a)
     for (int c = 0; c < 3; ++c) {
       gl[a][c] = C.jac[a][c];
@@ -173,11 +193,11 @@ void evaluate_curvilinear(const Map &M, double x, double y, double z, Curvi &C) 
       C.gij[a][b] = dot3(gu[a], gu[b]);
     }
   // find_gamma_tensor, curvilinear.f90:109-160
-  const double g1_2[3] = {Cc[4] + Cc[7] * z, Dd[4] + Dd[7] * z, Ee[4] + Ee[7] * z};
-  const double g1_3[3] = {Cc[5] + Cc[7] * y, Dd[5] + Dd[7] * y, Ee[5] + Ee[7] * y};
-  const double g2_3[3] = {Cc[6] + Cc[7] * x, Dd[6] + Dd[7] * x, Ee[6] + Ee[7] * x};
+  const real g1_2[3] = {Cc[4] + Cc[7] * z, Dd[4] + Dd[7] * z, Ee[4] + Ee[7] * z};
+  const real g1_3[3] = {Cc[5] + Cc[7] * y, Dd[5] + Dd[7] * y, Ee[5] + Ee[7] * y};
+  const real g2_3[3] = {Cc[6] + Cc[7] * x, Dd[6] + Dd[7] * x, Ee[6] + Ee[7] * x};
   for (int a = 0; a < 3; ++a) {
-    const double a12 = dot3(gu[a], g1_2), a13 = dot3(gu[a], g1_3), a23 = dot3(gu[a], g2_3);
+    const real a12 = dot3(gu[a], g1_2), a13 = dot3(gu[a], g1_3), a23 = dot3(gu[a], g2_3);
     C.gam[a][0][0] = 0.;
     C.gam[a][0][1] = a12;
     C.gam[a][0][2] = a13;
@@ -191,7 +211,7 @@ void evaluate_curvilinear(const Map &M, double x, double y, double z, Curvi &C) 
   C.detJ = det3(C.jac);
 }
 
-inline double sq(double x) { return x * x; }
+inline real sq(real x) { return x * x; }
 
 }  // namespace
 
@@ -201,15 +221,17 @@ struct nim_oracle {
   int nthreads = 1;
   nim_params P{};
   int64_t NMESH = 0, NFACE = 0, NNODE = 0, NBF = 0;
-  double Re = 0, inv_Re = 0;
+  real nu = 0, alpha = 0;  // P.nu, P.alpha: the tangent build seeds their derivatives
+  real Re = 0, inv_Re = 0;
   bool initialized = false;
   bool first_iteration = true;
   int32_t STEP = 0;
-  double TI = 0;
+  real TI = 0;
   double max_rc = 0;
+  double nu_tan[2] = {0, 0};  // derivatives of Nu_inner, Nu_outer at the last end_step
 
   // mesh (Fortran layout, 1-based)
-  std::vector<double> node_xyz;  // (3, NNODE) 0-based storage
+  std::vector<real> node_xyz;  // (3, NNODE) 0-based storage
   IK<8> mnodes;
   IK<6> mfaces, mnb;
   std::vector<int32_t> faces_BC;  // 1-based
@@ -246,8 +268,8 @@ struct nim_oracle {
   // number order for SEQUENTIAL, the level order for LEVELS
   std::vector<int64_t> cord, bord;
 
-  double err[5] = {0, 0, 0, 0, 0};
-  double Dilatation = 0, dudt_max = 0, dTdt_max = 0;
+  real err[5] = {0, 0, 0, 0, 0};
+  real Dilatation = 0, dudt_max = 0, dTdt_max = 0;
 
   // --------------------------------------------------------- helpers
   int32_t F(int pos, int64_t n) const { return mfaces(pos, n); }
@@ -259,14 +281,14 @@ namespace {
 // ====================================================== init-time geometry
 // mesh_calculate_mapping_coefficients, create_mesh.f90:254-303
 void mapping_coefficients(nim_oracle &o, int64_t m) {
-  double x[9], y[9], z[9];
+  real x[9], y[9], z[9];
   for (int i = 1; i <= 8; ++i) {
     const int64_t nd = o.mnodes(i, m) - 1;
     x[i] = o.node_xyz[3 * nd + 0];
     y[i] = o.node_xyz[3 * nd + 1];
     z[i] = o.node_xyz[3 * nd + 2];
   }
-  auto coef = [](const double *v, double *C) {
+  auto coef = [](const real *v, real *C) {
     C[0] = (v[7] + v[8] + v[5] + v[6] + v[3] + v[4] + v[1] + v[2]) / 8.;
     C[1] = (v[7] - v[8] - v[5] + v[6] + v[3] - v[4] - v[1] + v[2]) / 8.;
     C[2] = (v[7] + v[8] - v[5] - v[6] + v[3] + v[4] - v[1] - v[2]) / 8.;
@@ -282,8 +304,8 @@ void mapping_coefficients(nim_oracle &o, int64_t m) {
 }
 
 // The local coordinates of face fn's centre and of its Gauss points.
-inline void face_point(int fn, double a, double b, double &x, double &y, double &z) {
-  const double s = (fn % 2 == 1) ? -1.0 : 1.0;
+inline void face_point(int fn, real a, real b, real &x, real &y, real &z) {
+  const real s = (fn % 2 == 1) ? -1.0 : 1.0;
   if (fn <= 2) { x = s; y = a; z = b; }
   else if (fn <= 4) { x = a; y = s; z = b; }
   else { x = a; y = b; z = s; }
@@ -298,7 +320,7 @@ void cell_geometry(nim_oracle &o, int64_t m) {
   Curvi C;
   // volume_calculate, create_mesh.f90:306-322
   {
-    double Int = 0.;
+    real Int = 0.;
     for (int i = 0; i < 5; ++i)
       for (int j = 0; j < 5; ++j)
         for (int k = 0; k < 5; ++k) {
@@ -310,7 +332,7 @@ void cell_geometry(nim_oracle &o, int64_t m) {
   // find_normal, geometry.f90:76-190: unit contravariant normal, unit
   // covariant tangents and the centre point of every face.
   for (int fn = 1; fn <= 6; ++fn) {
-    double x, y, z;
+    real x, y, z;
     face_point(fn, 0.0, 0.0, x, y, z);
     evaluate_curvilinear(M, x, y, z, C);
     const int d = (fn - 1) / 2;             // normal direction 0..2
@@ -318,9 +340,9 @@ void cell_geometry(nim_oracle &o, int64_t m) {
     const int t2 = (d == 2) ? 1 : 2;        // second tangent
     const int32_t f = o.F(fn, m);
     if (o.face_owner[f] != m) continue;  // a later cell overwrites this face
-    const double sn = std::sqrt(C.gij[d][d]);
-    const double s1 = std::sqrt(C.g_ij[t1][t1]);
-    const double s2 = std::sqrt(C.g_ij[t2][t2]);
+    const real sn = sqrt(C.gij[d][d]);
+    const real s1 = sqrt(C.g_ij[t1][t1]);
+    const real s2 = sqrt(C.g_ij[t2][t2]);
     for (int c = 0; c < 3; ++c) {
       o.fnormal(c + 1, f) = C.jacinv[c][d] / sn;
       o.ftan(c + 1, f) = C.jac[t1][c] / s1;
@@ -334,40 +356,40 @@ void cell_geometry(nim_oracle &o, int64_t m) {
   // of each face that Gauss_integration2d_face keeps)
   for (int fn = 1; fn <= 6; ++fn) {
     const int d = (fn - 1) / 2;
-    double dS[5][5], K[3][3][5][5];
+    real dS[5][5], K[3][3][5][5];
     for (int a = 0; a < 5; ++a)
       for (int b = 0; b < 5; ++b) {
-        double x, y, z;
+        real x, y, z;
         face_point(fn, GQ.x[a], GQ.x[b], x, y, z);
         evaluate_curvilinear(M, x, y, z, C);
-        dS[a][b] = C.detJ * std::sqrt(C.gij[d][d]);
+        dS[a][b] = C.detJ * sqrt(C.gij[d][d]);
         for (int r = 0; r < 3; ++r)
-          for (int c = 0; c < 3; ++c) K[r][c][a][b] = C.gij[r][c] / std::sqrt(C.gij[r][r]) * dS[a][b];
+          for (int c = 0; c < 3; ++c) K[r][c][a][b] = C.gij[r][c] / sqrt(C.gij[r][r]) * dS[a][b];
       }
-    auto integ = [&](const double A[5][5]) {
-      double Int = 0.;
+    auto integ = [&](const real A[5][5]) {
+      real Int = 0.;
       for (int a = 0; a < 5; ++a)
         for (int b = 0; b < 5; ++b) Int = Int + GQ.w[a] * GQ.w[b] * A[a][b];
       return Int;
     };
     const int32_t f = o.F(fn, m);
-    const double area = integ(dS);  // this cell's faces_area(f), read back at geometry.f90:484-492
+    const real area = integ(dS);  // this cell's faces_area(f), read back at geometry.f90:484-492
     if (o.face_owner[f] == m) o.faces_area(f) = area;
     for (int r = 0; r < 3; ++r)
       for (int c = 0; c < 3; ++c) o.gf(r + 1, c + 1, fn, m) = integ(K[r][c]) / area;
   }
   // convection_diffusion_constants_mesh_i, geometry.f90:500-632
   {
-    double sG[3] = {0, 0, 0}, sK[3][3], sJ[3][3];
+    real sG[3] = {0, 0, 0}, sK[3][3], sJ[3][3];
     for (int r = 0; r < 3; ++r)
       for (int c = 0; c < 3; ++c) sK[r][c] = sJ[r][c] = 0.;
     for (int i = 0; i < 5; ++i)
       for (int j = 0; j < 5; ++j)
         for (int k = 0; k < 5; ++k) {
           evaluate_curvilinear(M, GQ.x[i], GQ.x[j], GQ.x[k], C);
-          const double w = GQ.w[i] * GQ.w[j] * GQ.w[k];
+          const real w = GQ.w[i] * GQ.w[j] * GQ.w[k];
           for (int a = 0; a < 3; ++a) {
-            const double Ga = (C.gam[a][0][1] * C.gij[0][1] + C.gam[a][1][0] * C.gij[1][0] +
+            const real Ga = (C.gam[a][0][1] * C.gij[0][1] + C.gam[a][1][0] * C.gij[1][0] +
                                C.gam[a][0][2] * C.gij[0][2] + C.gam[a][2][0] * C.gij[2][0] +
                                C.gam[a][1][2] * C.gij[1][2] + C.gam[a][2][1] * C.gij[2][1]);
             sG[a] = sG[a] + w * (Ga * C.detJ);
@@ -378,7 +400,7 @@ void cell_geometry(nim_oracle &o, int64_t m) {
               sJ[r][c] = sJ[r][c] + w * (C.jacinv[r][c] * C.detJ);
             }
         }
-    const double V = o.volume(m);
+    const real V = o.volume(m);
     o.G1(m) = sG[0] / V;
     o.G2(m) = sG[1] / V;
     o.G3(m) = sG[2] / V;
@@ -395,7 +417,7 @@ void cell_geometry(nim_oracle &o, int64_t m) {
 void pressure_bc_array(nim_oracle &o) {
   for (int64_t i = 1; i <= o.NBF; ++i) {
     const int32_t f0 = o.BCf[i];
-    const double *nv = &o.fnormal(1, f0), *tv = &o.ftan(1, f0), *sv = &o.fbitan(1, f0);
+    const real *nv = &o.fnormal(1, f0), *tv = &o.ftan(1, f0), *sv = &o.fbitan(1, f0);
     const int64_t M1 = o.BCm[i];
     const int pos = o.BCpos[i];
     int fn = 0;
@@ -413,21 +435,21 @@ void pressure_bc_array(nim_oracle &o) {
     o.BCpts(3, i) = o.F(fn, M2);
     o.BCpts(4, i) = o.F(fn, M3);
     o.BCpts(5, i) = o.F(fn, M4);
-    double n[6], t[6], s[6];
+    real n[6], t[6], s[6];
     for (int j = 1; j <= 5; ++j) {
-      double dvec[3];
+      real dvec[3];
       for (int c = 1; c <= 3; ++c) dvec[c - 1] = o.fmid(c, o.BCpts(j, i)) - o.fmid(c, o.BCpts(1, i));
       n[j] = dot3(dvec, nv);
       t[j] = dot3(dvec, tv);
       s[j] = dot3(dvec, sv);
     }
-    const double D =
+    const real D =
         (n[3] * s[4] * t[2] - n[3] * s[5] * t[2] - n[2] * s[4] * t[3] + n[2] * s[5] * t[3] - n[3] * s[2] * t[4] +
          n[2] * s[3] * t[4] - n[2] * s[5] * t[4] + n[3] * s[5] * t[4] + n[5] * s[3] * t[2] - n[5] * s[4] * t[2] -
          n[5] * s[2] * t[3] + n[5] * s[4] * t[3] + n[5] * s[2] * t[4] - n[5] * s[3] * t[4] + n[3] * s[2] * t[5] -
          n[2] * s[3] * t[5] + n[2] * s[4] * t[5] - n[3] * s[4] * t[5] +
          n[4] * (s[5] * t[2] + s[2] * t[3] - s[5] * t[3] - s[2] * t[5] + s[3] * (-t[2] + t[5])));
-    double a[21];
+    real a[21];
     a[2] = 2 * (-(n[5] * s[4] * t[3]) + n[4] * s[5] * t[3] + n[5] * s[3] * t[4] - n[3] * s[5] * t[4] -
                 n[4] * s[3] * t[5] + n[3] * s[4] * t[5]) / (sq(n[2]) * D);
     a[3] = 2 * (n[5] * s[4] * t[2] - n[4] * s[5] * t[2] - n[5] * s[2] * t[4] + n[2] * s[5] * t[4] +
@@ -452,12 +474,12 @@ void pressure_constants(nim_oracle &o) {
   Det.alloc(N);
   VK<3> CC, EE, FF, GG, HH, II, JJ;
   CC.alloc(N); EE.alloc(N); FF.alloc(N); GG.alloc(N); HH.alloc(N); II.alloc(N); JJ.alloc(N);
-  const double a = 1.;
+  const real a = 1.;
   for (int64_t i = 1; i <= N; ++i) {
-    double K[3];
+    real K[3];
     for (int d = 1; d <= 3; ++d) K[d - 1] = o.gij(d, d, i) / o.P.rho;
     for (int d = 1; d <= 3; ++d) {
-      const double Fk = K[d - 1];
+      const real Fk = K[d - 1];
       CC(d, i) = -(a * a / (3. * Fk));  // C_nim case(1), u = 0
       GG(d, i) = 1 / (2. * a);          // G_nim
       HH(d, i) = a / Fk;                // H_nim
@@ -473,8 +495,8 @@ void pressure_constants(nim_oracle &o) {
   for (int64_t i = 1; i <= N; ++i) {
     if (o.NB(2, i) != 0) {
       const int64_t i2 = o.NB(2, i);
-      const double g = o.gf(1, 1, 2, i), g2 = o.gf(1, 1, 1, i2);
-      double *A = &o.AApx(1, i);
+      const real g = o.gf(1, 1, 2, i), g2 = o.gf(1, 1, 1, i2);
+      real *A = &o.AApx(1, i);
       A[0] = -(GG(1, i) + (CC(2, i) + CC(3, i)) * EE(1, i) * HH(1, i)) * g;
       A[1] = (GG(1, i) - (CC(2, i) + CC(3, i)) * FF(1, i) * HH(1, i)) * g +
              (II(1, i2) + (CC(2, i2) + CC(3, i2)) * EE(1, i2) * JJ(1, i2)) * g2;
@@ -494,8 +516,8 @@ void pressure_constants(nim_oracle &o) {
     }
     if (o.NB(4, i) != 0) {
       const int64_t i2 = o.NB(4, i);
-      const double g = o.gf(2, 2, 4, i), g2 = o.gf(2, 2, 3, i2);
-      double *A = &o.AApy(1, i);
+      const real g = o.gf(2, 2, 4, i), g2 = o.gf(2, 2, 3, i2);
+      real *A = &o.AApy(1, i);
       A[0] = CC(3, i) * EE(1, i) * HH(2, i) * g;
       A[1] = CC(3, i) * FF(1, i) * HH(2, i) * g;
       A[2] = -(CC(3, i2) * EE(1, i2) * JJ(2, i2) * g2);
@@ -515,8 +537,8 @@ void pressure_constants(nim_oracle &o) {
     }
     if (o.NB(6, i) != 0) {
       const int64_t i2 = o.NB(6, i);
-      const double g = o.gf(3, 3, 6, i), g2 = o.gf(3, 3, 5, i2);
-      double *A = &o.AApz(1, i);
+      const real g = o.gf(3, 3, 6, i), g2 = o.gf(3, 3, 5, i2);
+      real *A = &o.AApz(1, i);
       A[0] = CC(2, i) * EE(1, i) * HH(3, i) * g;
       A[1] = CC(2, i) * FF(1, i) * HH(3, i) * g;
       A[2] = -(CC(2, i2) * EE(1, i2) * JJ(3, i2) * g2);
@@ -539,21 +561,21 @@ void pressure_constants(nim_oracle &o) {
   for (int64_t i = 1; i <= o.NBF; ++i) {
     const int64_t M = o.BCm[i];
     const int pos = o.BCpos[i];
-    double *ap = &o.BCap(1, i);
+    real *ap = &o.BCap(1, i);
     const int d = (pos + 1) / 2;                    // normal direction 1..3
     const int e1 = (d == 1) ? 2 : 1, e2 = (d == 3) ? 2 : 3;  // transverse
     const bool minus = (pos % 2 == 1);               // wall on the - side
-    const double g = o.gf(d, d, pos, M);
+    const real g = o.gf(d, d, pos, M);
     // - side walls use I/J (the "i2" role), + side walls G/H (the "i" role)
-    const double P0 = minus ? II(d, M) : GG(d, M);
-    const double Q = minus ? JJ(d, M) : HH(d, M);
-    const double cs = CC(e1, M) + CC(e2, M);
-    const double own_m = -(P0 + cs * EE(d, M) * Q) * g;
-    const double own_p = (P0 - cs * FF(d, M) * Q) * g;
-    double te1_m = CC(e2, M) * EE(e1, M) * Q * g, te1_p = CC(e2, M) * FF(e1, M) * Q * g;
-    double te2_m = CC(e1, M) * EE(e2, M) * Q * g, te2_p = CC(e1, M) * FF(e2, M) * Q * g;
-    double a7 = CC(e1, M) * CC(e2, M) * Det(M) * Q * g;
-    double a8 = -(CC(e1, M) * CC(e2, M) * Det(M) * Q * g);
+    const real P0 = minus ? II(d, M) : GG(d, M);
+    const real Q = minus ? JJ(d, M) : HH(d, M);
+    const real cs = CC(e1, M) + CC(e2, M);
+    const real own_m = -(P0 + cs * EE(d, M) * Q) * g;
+    const real own_p = (P0 - cs * FF(d, M) * Q) * g;
+    real te1_m = CC(e2, M) * EE(e1, M) * Q * g, te1_p = CC(e2, M) * FF(e1, M) * Q * g;
+    real te2_m = CC(e1, M) * EE(e2, M) * Q * g, te2_p = CC(e1, M) * FF(e2, M) * Q * g;
+    real a7 = CC(e1, M) * CC(e2, M) * Det(M) * Q * g;
+    real a8 = -(CC(e1, M) * CC(e2, M) * Det(M) * Q * g);
     // slots: 2d-1 / 2d own direction, 2e-1 / 2e transverse
     ap[2 * d - 2] = own_m;
     ap[2 * d - 1] = own_p;
@@ -568,19 +590,19 @@ void pressure_constants(nim_oracle &o) {
 
 // Face average of a constant boundary value c over face fn of cell M:
 // apply_dirichlet_bc_i, bc.f90:59-88 (c * dS integrated, over the area).
-double dirichlet_face_value(nim_oracle &o, int64_t M, int fn, double c) {
+real dirichlet_face_value(nim_oracle &o, int64_t M, int fn, real c) {
   const int d = (fn - 1) / 2;
   Curvi C;
-  double TT[5][5];
+  real TT[5][5];
   for (int i = 0; i < 5; ++i)
     for (int j = 0; j < 5; ++j) {
-      double x, y, z;
+      real x, y, z;
       face_point(fn, GQ.x[i], GQ.x[j], x, y, z);
       evaluate_curvilinear(o.maps[M], x, y, z, C);
-      const double dS = C.detJ * std::sqrt(C.gij[d][d]);
+      const real dS = C.detJ * sqrt(C.gij[d][d]);
       TT[i][j] = c * dS;
     }
-  double Int = 0.;
+  real Int = 0.;
   for (int i = 0; i < 5; ++i)
     for (int j = 0; j < 5; ++j) Int = Int + GQ.w[i] * GQ.w[j] * TT[i][j];
   return Int / o.faces_area(o.F(fn, M));
@@ -589,11 +611,11 @@ double dirichlet_face_value(nim_oracle &o, int64_t M, int fn, double c) {
 // ============================================================ per step
 // NIM coefficients of one direction for contravariant speed u and
 // diffusivity k (M_A(d,1:6) / MT_A(d,1:6), nim.f90:181-287 / 354-460).
-void nim_direction(double u, double k, double gminus, double gplus, double v_limit, double A[6]) {
-  const double a = 1.;
-  const double Re = 2 * a * u / k;
-  if (std::fabs(Re) > v_limit) {
-    const double e = std::exp(Re);
+void nim_direction(real u, real k, real gminus, real gplus, real v_limit, real A[6]) {
+  const real a = 1.;
+  const real Re = 2 * a * u / k;
+  if (fabs(Re) > v_limit) {
+    const real e = exp(Re);
     A[0] = (2 * a / (k * (1. / e - 1.)) + 1. / u) * gplus;
     A[1] = (-(2 * a / (k * (1. - e))) - 1. / u) * gminus;
     A[2] = (u / (k * (1. / e - 1.))) * gplus;
@@ -621,7 +643,7 @@ void nim_direction(double u, double k, double gminus, double gplus, double v_lim
 
 // M_F4 / M_F1..3 from M_A (nim.f90:293-328), shared by velocity and T.
 void form_F(nim_oracle &o, const M36 &A, VK<8> &F4, VK<5> &F1, VK<5> &F2, VK<5> &F3, int64_t i) {
-  const double DT = o.P.DT;
+  const real DT = o.P.DT;
   F4(2, i) = 0.5 * (1. / A(1, 5, i) + 1. / A(2, 5, i) + 1. / A(3, 5, i) - 1. / DT);
   F4(3, i) = -(A(1, 6, i) / A(1, 5, i));
   F4(4, i) = (A(1, 6, i) - 1.) / A(1, 5, i);
@@ -651,10 +673,10 @@ void velocity_constants(nim_oracle &o) {
     o.mu(i) = o.ut(i) * o.xi_x(1, 1, i) + o.vt(i) * o.xi_x(1, 2, i) + o.wt(i) * o.xi_x(1, 3, i);
     o.mv(i) = o.ut(i) * o.xi_x(2, 1, i) + o.vt(i) * o.xi_x(2, 2, i) + o.wt(i) * o.xi_x(2, 3, i);
     o.mw(i) = o.ut(i) * o.xi_x(3, 1, i) + o.vt(i) * o.xi_x(3, 2, i) + o.wt(i) * o.xi_x(3, 3, i);
-    const double c[3] = {o.mu(i), o.mv(i), o.mw(i)};
+    const real c[3] = {o.mu(i), o.mv(i), o.mw(i)};
     for (int d = 1; d <= 3; ++d) {
-      double A[6];
-      nim_direction(c[d - 1], o.gij(d, d, i) * o.P.nu, o.gf(d, d, 2 * d - 1, i), o.gf(d, d, 2 * d, i),
+      real A[6];
+      nim_direction(c[d - 1], o.gij(d, d, i) * o.nu, o.gf(d, d, 2 * d - 1, i), o.gf(d, d, 2 * d, i),
                     o.P.v_limit, A);
       for (int k = 0; k < 6; ++k) o.MA(d, k + 1, i) = A[k];
     }
@@ -668,15 +690,15 @@ void temperature_constants(nim_oracle &o) {
   const int64_t N = o.NMESH;
 #pragma omp parallel for schedule(static) num_threads(o.nthreads)
   for (int64_t i = 1; i <= N; ++i) {
-    const double ut = 0.5 * (o.uxyz(i) + o.uold(i));
-    const double vt = 0.5 * (o.vxyz(i) + o.vold(i));
-    const double wt = 0.5 * (o.wxyz(i) + o.wold(i));
-    const double c[3] = {ut * o.xi_x(1, 1, i) + vt * o.xi_x(1, 2, i) + wt * o.xi_x(1, 3, i),
+    const real ut = 0.5 * (o.uxyz(i) + o.uold(i));
+    const real vt = 0.5 * (o.vxyz(i) + o.vold(i));
+    const real wt = 0.5 * (o.wxyz(i) + o.wold(i));
+    const real c[3] = {ut * o.xi_x(1, 1, i) + vt * o.xi_x(1, 2, i) + wt * o.xi_x(1, 3, i),
                          ut * o.xi_x(2, 1, i) + vt * o.xi_x(2, 2, i) + wt * o.xi_x(2, 3, i),
                          ut * o.xi_x(3, 1, i) + vt * o.xi_x(3, 2, i) + wt * o.xi_x(3, 3, i)};
     for (int d = 1; d <= 3; ++d) {
-      double A[6];
-      nim_direction(c[d - 1], o.gij(d, d, i) * o.P.alpha, o.gf(d, d, 2 * d - 1, i), o.gf(d, d, 2 * d, i),
+      real A[6];
+      nim_direction(c[d - 1], o.gij(d, d, i) * o.alpha, o.gf(d, d, 2 * d - 1, i), o.gf(d, d, 2 * d, i),
                     o.P.v_limit, A);
       for (int k = 0; k < 6; ++k) o.MTA(d, k + 1, i) = A[k];
     }
@@ -693,13 +715,13 @@ void temperature_constants(nim_oracle &o) {
 // v_limit, exponential form otherwise.  G_nim and H_nim assign P twice in
 // their exponential branch; the second assignment is the one that counts.
 struct Nim1 {
-  double B, C, G, H, I, J;
+  real B, C, G, H, I, J;
   bool series;
 };
-Nim1 nim1_direction(double u, double F, double Re, double v_limit) {
-  const double a = 1.;
+Nim1 nim1_direction(real u, real F, real Re, real v_limit) {
+  const real a = 1.;
   Nim1 r;
-  r.series = std::fabs(Re) < v_limit;
+  r.series = fabs(Re) < v_limit;
   if (r.series) {
     const Pw U(u), K(F);
     r.B = 0;
@@ -714,7 +736,7 @@ Nim1 nim1_direction(double u, double F, double Re, double v_limit) {
     r.J = -(a / F) + (u) / (3. * K[2]) - (U[3]) / (45. * K[4]) + -((2 * U[5]) / (945. * K[6])) -
           (U[7]) / (4725. * K[8]) + -((2 * U[9]) / (93555. * K[10]));
   } else {
-    const double e = std::exp(Re);
+    const real e = exp(Re);
     r.B = 1. / u * (1. / Re - 1. / (e - 1.));
     r.C = (-(1. / u) + 2. * r.B) * a;
     r.G = u / F / (1. - 1. / e);
@@ -725,8 +747,8 @@ Nim1 nim1_direction(double u, double F, double Re, double v_limit) {
   return r;
 }
 // E_nim, F_nim (nim.f90:787-815) with D = Det
-inline double nim1_E(const Nim1 &r, double u, double F, double D) {
-  const double a = 1.;
+inline real nim1_E(const Nim1 &r, real u, real F, real D) {
+  const real a = 1.;
   if (r.series) {
     const Pw U(u), K(F);
     return D / 2. + (a * D * u) / (6. * F) - (D * U[3]) / (90. * K[3]) + (D * U[5]) / (945. * K[5]) -
@@ -734,8 +756,8 @@ inline double nim1_E(const Nim1 &r, double u, double F, double D) {
   }
   return D * (1 - r.B * u);
 }
-inline double nim1_F(const Nim1 &r, double u, double F, double D) {
-  const double a = 1.;
+inline real nim1_F(const Nim1 &r, real u, real F, real D) {
+  const real a = 1.;
   if (r.series) {
     const Pw U(u), K(F);
     return D / 2. - (a * D * u) / (6. * F) + (D * U[3]) / (90. * K[3]) - (D * U[5]) / (945. * K[5]) +
@@ -755,11 +777,11 @@ void velocity_constants_f1(nim_oracle &o) {
     o.mu(i) = o.ut(i) * o.xi_x(1, 1, i) + o.vt(i) * o.xi_x(1, 2, i) + o.wt(i) * o.xi_x(1, 3, i);
     o.mv(i) = o.ut(i) * o.xi_x(2, 1, i) + o.vt(i) * o.xi_x(2, 2, i) + o.wt(i) * o.xi_x(2, 3, i);
     o.mw(i) = o.ut(i) * o.xi_x(3, 1, i) + o.vt(i) * o.xi_x(3, 2, i) + o.wt(i) * o.xi_x(3, 3, i);
-    const double uc[3] = {o.mu(i), o.mv(i), o.mw(i)};
-    double K[3], Re[3];
+    const real uc[3] = {o.mu(i), o.mv(i), o.mw(i)};
+    real K[3], Re[3];
     Nim1 r[3];
     for (int d = 1; d <= 3; ++d) {
-      K[d - 1] = o.gij(d, d, i) * o.P.nu;
+      K[d - 1] = o.gij(d, d, i) * o.nu;
       Re[d - 1] = 2 * uc[d - 1] / K[d - 1];
     }
     for (int d = 1; d <= 3; ++d) {
@@ -776,7 +798,7 @@ void velocity_constants_f1(nim_oracle &o) {
       FF(d, i) = nim1_F(r[d - 1], uc[d - 1], K[d - 1], Det(i));
     }
   }
-  const double DT = o.P.DT;
+  const real DT = o.P.DT;
 #pragma omp parallel for schedule(static) num_threads(o.nthreads)
   for (int64_t i = 1; i <= N; ++i) {
     auto C = [&](int d, int64_t n) { return CC(d, n); };
@@ -784,7 +806,7 @@ void velocity_constants_f1(nim_oracle &o) {
     auto Fv = [&](int d, int64_t n) { return FF(d, n); };
     if (o.NB(2, i) != 0) {  // face 2 (nim.f90:87-104)
       const int64_t i2 = o.NB(2, i);
-      const double g2 = o.gf(1, 1, 2, i), g1 = o.gf(1, 1, 1, i2);
+      const real g2 = o.gf(1, 1, 2, i), g1 = o.gf(1, 1, 1, i2);
       VK<15> &A = o.AAvx;
       A(1, i) = -(GG(1, i) + (C(2, i) + C(3, i)) * E(1, i) * HH(1, i)) * g2;
       A(2, i) = (GG(1, i) - (C(2, i) + C(3, i)) * Fv(1, i) * HH(1, i)) * g2 +
@@ -805,7 +827,7 @@ void velocity_constants_f1(nim_oracle &o) {
     }
     if (o.NB(4, i) != 0) {  // face 4 (nim.f90:107-124)
       const int64_t i2 = o.NB(4, i);
-      const double g4 = o.gf(2, 2, 4, i), g3 = o.gf(2, 2, 3, i2);
+      const real g4 = o.gf(2, 2, 4, i), g3 = o.gf(2, 2, 3, i2);
       VK<15> &A = o.AAvy;
       A(1, i) = C(3, i) * E(1, i) * HH(2, i) * g4;
       A(2, i) = C(3, i) * Fv(1, i) * HH(2, i) * g4;
@@ -826,7 +848,7 @@ void velocity_constants_f1(nim_oracle &o) {
     }
     if (o.NB(6, i) != 0) {  // face 6 (nim.f90:126-143)
       const int64_t i2 = o.NB(6, i);
-      const double g6 = o.gf(3, 3, 6, i), g5 = o.gf(3, 3, 5, i2);
+      const real g6 = o.gf(3, 3, 6, i), g5 = o.gf(3, 3, 5, i2);
       VK<15> &A = o.AAvz;
       A(1, i) = C(2, i) * E(1, i) * HH(3, i) * g6;
       A(2, i) = C(2, i) * Fv(1, i) * HH(3, i) * g6;
@@ -860,7 +882,7 @@ void velocity_constants_f1(nim_oracle &o) {
 
 // ---------------------------------------------------------------- sources
 // Green-Gauss derivative dphi_dx2/dy2/dz2 (nse.f90:2866-2903), component c.
-inline double green_gauss(const nim_oracle &o, const double *phi, const int32_t *nf, int64_t i, int c) {
+inline real green_gauss(const nim_oracle &o, const real *phi, const int32_t *nf, int64_t i, int c) {
   return 1. / o.volume(i) *
          (phi[2] * o.faces_area(nf[2]) * (o.fnormal(c, nf[2])) - phi[1] * o.faces_area(nf[1]) * (o.fnormal(c, nf[1])) +
           phi[4] * o.faces_area(nf[4]) * (o.fnormal(c, nf[4])) - phi[3] * o.faces_area(nf[3]) * (o.fnormal(c, nf[3])) +
@@ -870,7 +892,7 @@ inline double green_gauss(const nim_oracle &o, const double *phi, const int32_t 
 // Derivative along local direction e of face field phi on face position fpos
 // of cell n, centred or one-sided at walls (the nj/ni/nk stencils of
 // calculate_R_D2, nse.f90:1635-1838, and of the pressure sweep).
-inline double tangential(const nim_oracle &o, const V1 &phi, int64_t n, int fpos, int e) {
+inline real tangential(const nim_oracle &o, const V1 &phi, int64_t n, int fpos, int e) {
   const int64_t m1 = o.NB(2 * e - 1, n), m2 = o.NB(2 * e, n);
   if (m1 == 0) {
     const int64_t m3 = o.NB(2 * e, m2);
@@ -884,16 +906,16 @@ inline double tangential(const nim_oracle &o, const V1 &phi, int64_t n, int fpos
 
 // Cross-derivative diffusion source (calculate_R_D2 / R_D_p2 / R_D_T):
 // G_i d_i phi - g^ij d_ij phi, before the 1/Re, 1/rho or alpha factor.
-inline double diffusion_source(const nim_oracle &o, const V1 &phi, int64_t n) {
-  const double pxy = 0.5 * (tangential(o, phi, n, 2, 2) - tangential(o, phi, n, 1, 2));
-  const double pzy = 0.5 * (tangential(o, phi, n, 6, 2) - tangential(o, phi, n, 5, 2));
-  const double pyx = 0.5 * (tangential(o, phi, n, 4, 1) - tangential(o, phi, n, 3, 1));
-  const double pzx = 0.5 * (tangential(o, phi, n, 6, 1) - tangential(o, phi, n, 5, 1));
-  const double pxz = 0.5 * (tangential(o, phi, n, 2, 3) - tangential(o, phi, n, 1, 3));
-  const double pyz = 0.5 * (tangential(o, phi, n, 4, 3) - tangential(o, phi, n, 3, 3));
-  const double px = (phi(o.F(2, n)) - phi(o.F(1, n))) / 2.;
-  const double py = (phi(o.F(4, n)) - phi(o.F(3, n))) / 2.;
-  const double pz = (phi(o.F(6, n)) - phi(o.F(5, n))) / 2.;
+inline real diffusion_source(const nim_oracle &o, const V1 &phi, int64_t n) {
+  const real pxy = 0.5 * (tangential(o, phi, n, 2, 2) - tangential(o, phi, n, 1, 2));
+  const real pzy = 0.5 * (tangential(o, phi, n, 6, 2) - tangential(o, phi, n, 5, 2));
+  const real pyx = 0.5 * (tangential(o, phi, n, 4, 1) - tangential(o, phi, n, 3, 1));
+  const real pzx = 0.5 * (tangential(o, phi, n, 6, 1) - tangential(o, phi, n, 5, 1));
+  const real pxz = 0.5 * (tangential(o, phi, n, 2, 3) - tangential(o, phi, n, 1, 3));
+  const real pyz = 0.5 * (tangential(o, phi, n, 4, 3) - tangential(o, phi, n, 3, 3));
+  const real px = (phi(o.F(2, n)) - phi(o.F(1, n))) / 2.;
+  const real py = (phi(o.F(4, n)) - phi(o.F(3, n))) / 2.;
+  const real pz = (phi(o.F(6, n)) - phi(o.F(5, n))) / 2.;
   return (o.G1(n) * px + o.G2(n) * py + o.G3(n) * pz - o.gij(1, 2, n) * pxy - o.gij(2, 1, n) * pyx -
           o.gij(1, 3, n) * pxz - o.gij(3, 1, n) * pzx - o.gij(2, 3, n) * pyz - o.gij(3, 2, n) * pzy);
 }
@@ -902,7 +924,7 @@ inline double diffusion_source(const nim_oracle &o, const V1 &phi, int64_t n) {
 // calculate_R_c_new, calculate_R_D2 for every cell.
 void velocity_sources(nim_oracle &o) {
   const int64_t N = o.NMESH;
-  const double gb = o.P.g_beta;
+  const real gb = o.P.g_beta;
   for (int64_t i = 1; i <= N; ++i) o.bz(i) = -(gb * 0.5 * (o.Txyz(i) + o.Told(i)));
   for (int64_t f = 1; f <= o.NFACE; ++f) o.fbz(f) = -(gb * (o.fT(f)));
   const bool check_rc = (o.sched != NIM_SCHED_PARALLEL);
@@ -911,9 +933,9 @@ void velocity_sources(nim_oracle &o) {
   for (int64_t i = 1; i <= N; ++i) {
     int32_t nf[7];
     for (int k = 1; k <= 6; ++k) nf[k] = o.F(k, i);
-    double pf[7];
+    real pf[7];
     for (int k = 1; k <= 6; ++k) pf[k] = o.fp(nf[k]);
-    const double dpx = green_gauss(o, pf, nf, i, 1), dpy = green_gauss(o, pf, nf, i, 2),
+    const real dpx = green_gauss(o, pf, nf, i, 1), dpy = green_gauss(o, pf, nf, i, 2),
                  dpz = green_gauss(o, pf, nf, i, 3);
     o.RBu(i) = 0. + 1 / o.P.rho * dpx;  // meshes_bx = 0
     o.RBv(i) = 0. + 1 / o.P.rho * dpy;  // meshes_by = 0
@@ -921,11 +943,11 @@ void velocity_sources(nim_oracle &o) {
     if (check_rc) {
       // calculate_R_c_new, nse.f90:1393-1434: (meshes_u - uc) is the same
       // expression on the same values, so R_C is zero; verify it.
-      const double uc = o.ut(i) * o.xi_x(1, 1, i) + o.vt(i) * o.xi_x(1, 2, i) + o.wt(i) * o.xi_x(1, 3, i);
-      const double vc = o.ut(i) * o.xi_x(2, 1, i) + o.vt(i) * o.xi_x(2, 2, i) + o.wt(i) * o.xi_x(2, 3, i);
-      const double wc = o.ut(i) * o.xi_x(3, 1, i) + o.vt(i) * o.xi_x(3, 2, i) + o.wt(i) * o.xi_x(3, 3, i);
-      const double r = std::fabs(o.mu(i) - uc) + std::fabs(o.mv(i) - vc) + std::fabs(o.mw(i) - wc);
-      mrc = std::max(mrc, r);
+      const real uc = o.ut(i) * o.xi_x(1, 1, i) + o.vt(i) * o.xi_x(1, 2, i) + o.wt(i) * o.xi_x(1, 3, i);
+      const real vc = o.ut(i) * o.xi_x(2, 1, i) + o.vt(i) * o.xi_x(2, 2, i) + o.wt(i) * o.xi_x(2, 3, i);
+      const real wc = o.ut(i) * o.xi_x(3, 1, i) + o.vt(i) * o.xi_x(3, 2, i) + o.wt(i) * o.xi_x(3, 3, i);
+      const real r = fabs(o.mu(i) - uc) + fabs(o.mv(i) - vc) + fabs(o.mw(i) - wc);
+      mrc = std::max(mrc, val(r));
     }
     o.RDu(i) = o.inv_Re * diffusion_source(o, o.fu, i);
     o.RDv(i) = o.inv_Re * diffusion_source(o, o.fv, i);
@@ -936,8 +958,8 @@ void velocity_sources(nim_oracle &o) {
 
 // Cell-average update of one field (integrate_velocity_field_formulation2_i
 // nse.f90:839-872, temperature nse.f90:1017-1026).
-inline double cell_update(const nim_oracle &o, const V1 &f, double c, double cold, double B,
-                          const VK<8> &F4, int64_t i, double w) {
+inline real cell_update(const nim_oracle &o, const V1 &f, real c, real cold, real B,
+                          const VK<8> &F4, int64_t i, real w) {
   return (1 - w) * c +
          (w / F4(1, i)) * (+F4(2, i) * cold + F4(3, i) * f(o.F(1, i)) + F4(4, i) * f(o.F(2, i)) +
                            F4(5, i) * f(o.F(3, i)) + F4(6, i) * f(o.F(4, i)) + F4(7, i) * f(o.F(5, i)) +
@@ -946,13 +968,13 @@ inline double cell_update(const nim_oracle &o, const V1 &f, double c, double col
 
 // Update of the +d face of cell i (nse.f90:878-1005, 1033-1088).  fr is read,
 // the result is returned; the caller stores it.
-inline double face_update(const nim_oracle &o, const V1 &fr, const V1 &c, const V1 &cold,
-                          const VK<5> &Fd, int d, int64_t i, double w) {
+inline real face_update(const nim_oracle &o, const V1 &fr, const V1 &c, const V1 &cold,
+                          const VK<5> &Fd, int d, int64_t i, real w) {
   const int64_t i2 = o.NB(2 * d, i);
   const int e1 = (d == 1) ? 2 : 1, e2 = (d == 3) ? 2 : 3;
-  const double B3 = (o.gf(d, e1, 2 * d - 1, i2) - o.gf(d, e1, 2 * d, i)) *
+  const real B3 = (o.gf(d, e1, 2 * d - 1, i2) - o.gf(d, e1, 2 * d, i)) *
                     (fr(o.F(2 * e1, i)) - fr(o.F(2 * e1 - 1, i)) + fr(o.F(2 * e1, i2)) - fr(o.F(2 * e1 - 1, i2))) / 4.0;
-  const double B4 = (o.gf(d, e2, 2 * d - 1, i2) - o.gf(d, e2, 2 * d, i)) *
+  const real B4 = (o.gf(d, e2, 2 * d - 1, i2) - o.gf(d, e2, 2 * d, i)) *
                     (fr(o.F(2 * e2, i)) - fr(o.F(2 * e2 - 1, i)) + fr(o.F(2 * e2, i2)) - fr(o.F(2 * e2 - 1, i2))) / 4.0;
   return (1 - w) * fr(o.F(2 * d, i)) +
          (w / Fd(1, i)) * (+Fd(2, i) * fr(o.F(2 * d - 1, i)) + Fd(3, i) * fr(o.F(2 * d, i2)) +
@@ -961,10 +983,10 @@ inline double face_update(const nim_oracle &o, const V1 &fr, const V1 &c, const 
 
 // Formulation 1 cell update of one velocity component (integrate_velocity_
 // field_i, nse.f90:341-352); R = R_C + R_D + R_B of the cell.
-inline double cell_update_f1(const nim_oracle &o, const V1 &f, double c, double cold, double R, int64_t i,
-                             double w) {
+inline real cell_update_f1(const nim_oracle &o, const V1 &f, real c, real cold, real R, int64_t i,
+                             real w) {
   const VK<9> &a = o.at;
-  const double Bij = a(7, i) * R;
+  const real Bij = a(7, i) * R;
   return (1 - w) * c + w * (-(a(1, i) * f(o.F(1, i))) - a(2, i) * f(o.F(2, i)) - a(3, i) * f(o.F(3, i)) -
                             a(4, i) * f(o.F(4, i)) - a(5, i) * f(o.F(5, i)) - a(6, i) * f(o.F(6, i)) -
                             a(8, i) * cold - Bij) /
@@ -975,25 +997,25 @@ inline double cell_update_f1(const nim_oracle &o, const V1 &f, double c, double 
 // pressure sweep's ten face terms with AA_v, the two cell time terms, the
 // R sums of both cells and the tangential cross terms B3, B4 (the centred
 // B3/B4 the source computes first are overwritten before use).
-inline double face_update_f1(const nim_oracle &o, const V1 &fr, const V1 &c, const V1 &cold, const V1 &RD,
-                             const V1 &RB, int d, int64_t n1, double w) {
+inline real face_update_f1(const nim_oracle &o, const V1 &fr, const V1 &c, const V1 &cold, const V1 &RD,
+                             const V1 &RB, int d, int64_t n1, real w) {
   const int64_t n2 = o.NB(2 * d, n1);
   const VK<15> &A = (d == 1) ? o.AAvx : (d == 2) ? o.AAvy : o.AAvz;
   const int e1 = (d == 1) ? 2 : 1, e2 = (d == 3) ? 2 : 3;
-  const double DT = o.P.DT;
-  const double B1 = (0. + RD(n1) + RB(n1)) * A(13, n1) * 2 * DT;
-  const double B2 = (0. + RD(n2) + RB(n2)) * A(15, n1) * 2 * DT;
-  const double B3 = (o.gf(d, e1, 2 * d - 1, n2) - o.gf(d, e1, 2 * d, n1)) * tangential(o, fr, n1, 2 * d, e1);
-  const double B4 = (o.gf(d, e2, 2 * d - 1, n2) - o.gf(d, e2, 2 * d, n1)) * tangential(o, fr, n1, 2 * d, e2);
+  const real DT = o.P.DT;
+  const real B1 = (0. + RD(n1) + RB(n1)) * A(13, n1) * 2 * DT;
+  const real B2 = (0. + RD(n2) + RB(n2)) * A(15, n1) * 2 * DT;
+  const real B3 = (o.gf(d, e1, 2 * d - 1, n2) - o.gf(d, e1, 2 * d, n1)) * tangential(o, fr, n1, 2 * d, e1);
+  const real B4 = (o.gf(d, e2, 2 * d - 1, n2) - o.gf(d, e2, 2 * d, n1)) * tangential(o, fr, n1, 2 * d, e2);
   static const int tab[3][10][3] = {
       {{1, 1, 1}, {3, 2, 2}, {4, 3, 1}, {5, 4, 1}, {6, 3, 2}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
       {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
       {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {6, 4, 1}, {7, 3, 2}, {8, 4, 2}, {9, 5, 1}, {11, 6, 2}}};
   static const int diag[3] = {2, 6, 10};
-  double s = 0.0;
+  real s = 0.0;
   for (int t = 0; t < 10; ++t) {
     const int64_t cell = (tab[d - 1][t][2] == 1) ? n1 : n2;
-    const double term = A(tab[d - 1][t][0], n1) * fr(o.F(tab[d - 1][t][1], cell));
+    const real term = A(tab[d - 1][t][0], n1) * fr(o.F(tab[d - 1][t][1], cell));
     s = (t == 0) ? -term : s - term;
   }
   s = s - A(12, n1) * (c(n1) - cold(n1)) - A(14, n1) * (c(n2) - cold(n2));
@@ -1003,26 +1025,26 @@ inline double face_update_f1(const nim_oracle &o, const V1 &fr, const V1 &c, con
 // calculate_R_b_p (nse.f90:2362-2407) + calculate_R_D_p2 (nse.f90:1863-1997)
 void pressure_sources(nim_oracle &o) {
   const int64_t N = o.NMESH;
-  const double DT = o.P.DT;
+  const real DT = o.P.DT;
 #pragma omp parallel for schedule(static) num_threads(o.nthreads)
   for (int64_t n = 1; n <= N; ++n) {
     int32_t nf[7];
     for (int k = 1; k <= 6; ++k) nf[k] = o.F(k, n);
-    double uf[7], vf[7], wf[7], bzf[7];
+    real uf[7], vf[7], wf[7], bzf[7];
     for (int k = 1; k <= 6; ++k) {
       uf[k] = o.fu(nf[k]);
       vf[k] = o.fv(nf[k]);
       wf[k] = o.fw(nf[k]);
       bzf[k] = o.fbz(nf[k]);
     }
-    const double du_dx = green_gauss(o, uf, nf, n, 1), du_dy = green_gauss(o, uf, nf, n, 2),
+    const real du_dx = green_gauss(o, uf, nf, n, 1), du_dy = green_gauss(o, uf, nf, n, 2),
                  du_dz = green_gauss(o, uf, nf, n, 3);
-    const double dv_dx = green_gauss(o, vf, nf, n, 1), dv_dy = green_gauss(o, vf, nf, n, 2),
+    const real dv_dx = green_gauss(o, vf, nf, n, 1), dv_dy = green_gauss(o, vf, nf, n, 2),
                  dv_dz = green_gauss(o, vf, nf, n, 3);
-    const double dw_dx = green_gauss(o, wf, nf, n, 1), dw_dy = green_gauss(o, wf, nf, n, 2),
+    const real dw_dx = green_gauss(o, wf, nf, n, 1), dw_dy = green_gauss(o, wf, nf, n, 2),
                  dw_dz = green_gauss(o, wf, nf, n, 3);
-    const double dbz_dz = green_gauss(o, bzf, nf, n, 3);  // faces_bx = faces_by = 0
-    const double Dila = du_dx + dv_dy + dw_dz;
+    const real dbz_dz = green_gauss(o, bzf, nf, n, 3);  // faces_bx = faces_by = 0
+    const real Dila = du_dx + dv_dy + dw_dz;
     o.dila(n) = Dila;
     o.RBp(n) = -(du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) -
                2.0 * (du_dy * dv_dx + dv_dz * dw_dy + dw_dx * du_dz) - dbz_dz + Dila / (2 * DT);
@@ -1031,66 +1053,66 @@ void pressure_sources(nim_oracle &o) {
 }
 
 // apply_pressure_bc for boundary face i (bc.f90:148-339); reads pr.
-double pressure_bc_face(const nim_oracle &o, const V1 &pr, int64_t i) {
+real pressure_bc_face(const nim_oracle &o, const V1 &pr, int64_t i) {
   const int64_t M1 = o.BCm[i];
   const int pos = o.BCpos[i];
   const int32_t fw = o.BCf[i];
-  const double *n = &o.fnormal(1, fw);
-  const double b[3] = {0., 0., o.fbz(fw)};
-  const double b_n = dot3(b, n);
-  double vn[6];
+  const real *n = &o.fnormal(1, fw);
+  const real b[3] = {0., 0., o.fbz(fw)};
+  const real b_n = dot3(b, n);
+  real vn[6];
   for (int j = 1; j <= 5; ++j) {
     const int32_t pt = o.BCpts(j, i);
-    const double v[3] = {o.fu(pt), o.fv(pt), o.fw(pt)};
+    const real v[3] = {o.fu(pt), o.fv(pt), o.fw(pt)};
     vn[j] = dot3(v, n);
   }
-  const double d2udn2 = -(o.BCa(1, i) * vn[1]) - o.BCa(2, i) * vn[2] - o.BCa(3, i) * vn[3] - o.BCa(4, i) * vn[4] -
+  const real d2udn2 = -(o.BCa(1, i) * vn[1]) - o.BCa(2, i) * vn[2] - o.BCa(3, i) * vn[3] - o.BCa(4, i) * vn[4] -
                         o.BCa(5, i) * vn[5];
   const int d = (pos + 1) / 2;
   const int e1 = (d == 1) ? 2 : 1, e2 = (d == 3) ? 2 : 3;
   const int fn = pos;
-  double B2 = tangential(o, pr, M1, fn, e1);
+  real B2 = tangential(o, pr, M1, fn, e1);
   // position 6, centred branch, uses meshes_gij_faces(3,2,...) (bc.f90:318)
   const bool centred_e1 = (o.NB(2 * e1 - 1, M1) != 0 && o.NB(2 * e1, M1) != 0);
   const int e1g = (pos == 6 && centred_e1) ? 2 : e1;
   B2 = B2 * o.gf(d, e1g, fn, M1);
-  const double B3 = tangential(o, pr, M1, fn, e2) * o.gf(d, e2, fn, M1);
-  const double B1 = o.BCap(8, i) * (o.RDp(M1) + o.RBp(M1));
-  double s = 0.0;
+  const real B3 = tangential(o, pr, M1, fn, e2) * o.gf(d, e2, fn, M1);
+  const real B1 = o.BCap(8, i) * (o.RDp(M1) + o.RBp(M1));
+  real s = 0.0;
   bool first = true;
   for (int k = 1; k <= 6; ++k) {
     if (k == pos) continue;
-    const double t = o.BCap(k, i) * pr(o.F(k, M1));
+    const real t = o.BCap(k, i) * pr(o.F(k, M1));
     s = first ? -t : s - t;
     first = false;
   }
-  const double w = o.P.w_p2;
+  const real w = o.P.w_p2;
   return (1 - w) * pr(o.F(pos, M1)) +
-         w / (o.BCap(pos, i)) * (s + B1 - B2 - B3 + (o.P.nu * o.P.rho * d2udn2 - b_n * o.P.rho));
+         w / (o.BCap(pos, i)) * (s + B1 - B2 - B3 + (o.nu * o.P.rho * d2udn2 - b_n * o.P.rho));
 }
 
 // integrate_pressure_field_i for the +d face of cell n1 (nse.f90:1105-1288).
-double pressure_face(const nim_oracle &o, const V1 &pr, int d, int64_t n1) {
+real pressure_face(const nim_oracle &o, const V1 &pr, int d, int64_t n1) {
   const int64_t n2 = o.NB(2 * d, n1);
   const VK<15> &A = (d == 1) ? o.AApx : (d == 2) ? o.AApy : o.AApz;
   const int e1 = (d == 1) ? 2 : 1, e2 = (d == 3) ? 2 : 3;
-  const double B1 = (o.RDp(n1) + o.RBp(n1)) * A(13, n1);
-  const double B2 = (o.RDp(n2) + o.RBp(n2)) * A(15, n1);
-  const double B3 = (o.gf(d, e1, 2 * d - 1, n2) - o.gf(d, e1, 2 * d, n1)) * tangential(o, pr, n1, 2 * d, e1);
-  const double B4 = (o.gf(d, e2, 2 * d - 1, n2) - o.gf(d, e2, 2 * d, n1)) * tangential(o, pr, n1, 2 * d, e2);
+  const real B1 = (o.RDp(n1) + o.RBp(n1)) * A(13, n1);
+  const real B2 = (o.RDp(n2) + o.RBp(n2)) * A(15, n1);
+  const real B3 = (o.gf(d, e1, 2 * d - 1, n2) - o.gf(d, e1, 2 * d, n1)) * tangential(o, pr, n1, 2 * d, e1);
+  const real B4 = (o.gf(d, e2, 2 * d - 1, n2) - o.gf(d, e2, 2 * d, n1)) * tangential(o, pr, n1, 2 * d, e2);
   // the ten off-diagonal terms in source order: (coefficient, face, cell)
   static const int tab[3][10][3] = {
       {{1, 1, 1}, {3, 2, 2}, {4, 3, 1}, {5, 4, 1}, {6, 3, 2}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
       {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {7, 4, 2}, {8, 5, 1}, {9, 6, 1}, {10, 5, 2}, {11, 6, 2}},
       {{1, 1, 1}, {2, 2, 1}, {3, 1, 2}, {4, 2, 2}, {5, 3, 1}, {6, 4, 1}, {7, 3, 2}, {8, 4, 2}, {9, 5, 1}, {11, 6, 2}}};
   static const int diag[3] = {2, 6, 10};
-  double s = 0.0;
+  real s = 0.0;
   for (int t = 0; t < 10; ++t) {
     const int64_t cell = (tab[d - 1][t][2] == 1) ? n1 : n2;
-    const double term = A(tab[d - 1][t][0], n1) * pr(o.F(tab[d - 1][t][1], cell));
+    const real term = A(tab[d - 1][t][0], n1) * pr(o.F(tab[d - 1][t][1], cell));
     s = (t == 0) ? -term : s - term;
   }
-  const double w = o.P.w_p;
+  const real w = o.P.w_p;
   return (1 - w) * pr(o.F(2 * d, n1)) + w / (A(diag[d - 1], n1)) * (s + B1 + B2 + B3 + B4);
 }
 
@@ -1104,9 +1126,9 @@ void zero_flux(nim_oracle &o) {
     const int in = (pos == 5) ? 6 : 5;
     const int32_t f1 = o.BCf[i], f2 = o.F(in, M), f3 = o.F(in, o.NB(in, M)), f4 = o.F(in, o.NB(in, o.NB(in, M)));
     auto dist = [&](int32_t a, int32_t b) {
-      return std::sqrt(sq(o.fmid(1, a) - o.fmid(1, b)) + sq(o.fmid(2, a) - o.fmid(2, b)) + sq(o.fmid(3, a) - o.fmid(3, b)));
+      return sqrt(sq(o.fmid(1, a) - o.fmid(1, b)) + sq(o.fmid(2, a) - o.fmid(2, b)) + sq(o.fmid(3, a) - o.fmid(3, b)));
     };
-    const double h1 = dist(f1, f2), h2 = dist(f2, f3), h3 = dist(f3, f4);
+    const real h1 = dist(f1, f2), h2 = dist(f2, f3), h3 = dist(f3, f4);
     o.fT(f1) = (+((h1 + h2) * (h1 + h2 + h3)) / (h1 * h2 * (h2 + h3)) * o.fT(f2) -
                 (h1 * (h1 + h2 + h3)) / (h2 * h3 * (h1 + h2)) * o.fT(f3) +
                 (h1 * (h1 + h2)) / (h3 * (h2 + h3) * (h1 + h2 + h3)) * o.fT(f4)) /
@@ -1116,23 +1138,23 @@ void zero_flux(nim_oracle &o) {
 
 // find_error (nse.f90:260-325)
 void find_error(nim_oracle &o) {
-  double e[5] = {0, 0, 0, 0, 0};
+  real e[5] = {0, 0, 0, 0, 0};
   V1 *cur[5] = {&o.fu, &o.fv, &o.fw, &o.fp, &o.fT};
   V1 *old[5] = {&o.fuo, &o.fvo, &o.fwo, &o.fpo, &o.fTo};
   for (int64_t i = 1; i <= o.NFACE; ++i)
     for (int k = 0; k < 5; ++k) {
-      e[k] = std::max(e[k], std::fabs((*cur[k])(i) - (*old[k])(i)));
+      e[k] = std::max(e[k], fabs((*cur[k])(i) - (*old[k])(i)));
       (*old[k])(i) = (*cur[k])(i);
     }
   if (o.P.dpdx_tolerance) {
-    double ex = 0, ey = 0, ez = 0;
+    real ex = 0, ey = 0, ez = 0;
     for (int64_t i = 1; i <= o.NMESH; ++i) {
       o.dpdx(i) = (o.fp(o.F(2, i)) - o.fp(o.F(1, i))) / 2. * o.xi_x(1, 1, i);
       o.dpdy(i) = (o.fp(o.F(4, i)) - o.fp(o.F(3, i))) / 2. * o.xi_x(2, 2, i);
       o.dpdz(i) = (o.fp(o.F(6, i)) - o.fp(o.F(5, i))) / 2. * o.xi_x(3, 3, i);
-      ex = std::max(ex, std::fabs(o.dpdx(i) - o.dpdxo(i)));
-      ey = std::max(ey, std::fabs(o.dpdy(i) - o.dpdyo(i)));
-      ez = std::max(ez, std::fabs(o.dpdz(i) - o.dpdzo(i)));
+      ex = std::max(ex, fabs(o.dpdx(i) - o.dpdxo(i)));
+      ey = std::max(ey, fabs(o.dpdy(i) - o.dpdyo(i)));
+      ez = std::max(ez, fabs(o.dpdz(i) - o.dpdzo(i)));
       o.dpdxo(i) = o.dpdx(i);
       o.dpdyo(i) = o.dpdy(i);
       o.dpdzo(i) = o.dpdz(i);
@@ -1142,10 +1164,10 @@ void find_error(nim_oracle &o) {
   V1 *cc[4] = {&o.uxyz, &o.vxyz, &o.wxyz, &o.Txyz};
   V1 *co[4] = {&o.uoc, &o.voc, &o.woc, &o.Toc};
   const int slot[4] = {0, 1, 2, 4};
-  double ce[4] = {0, 0, 0, 0};
+  real ce[4] = {0, 0, 0, 0};
   for (int64_t i = 1; i <= o.NMESH; ++i)
     for (int k = 0; k < 4; ++k) {
-      ce[k] = std::max(ce[k], std::fabs((*cc[k])(i) - (*co[k])(i)));
+      ce[k] = std::max(ce[k], fabs((*cc[k])(i) - (*co[k])(i)));
       (*co[k])(i) = (*cc[k])(i);
     }
   for (int k = 0; k < 4; ++k) e[slot[k]] = std::max(e[slot[k]], ce[k]);
@@ -1162,7 +1184,7 @@ void iteration(nim_oracle &o) {
   V1 *vo[3] = {&o.uold, &o.vold, &o.wold};
   V1 *RD[3] = {&o.RDu, &o.RDv, &o.RDw};
   V1 *RB[3] = {&o.RBu, &o.RBv, &o.RBw};
-  const double wv[3] = {o.P.w_u, o.P.w_v, o.P.w_w};
+  const real wv[3] = {o.P.w_u, o.P.w_v, o.P.w_w};
   VK<5> *MF[3] = {&o.MF1, &o.MF2, &o.MF3};
   VK<5> *MTF[3] = {&o.MTF1, &o.MTF2, &o.MTF3};
 
@@ -1170,7 +1192,7 @@ void iteration(nim_oracle &o) {
   velocity_sources(o);
   const bool f1 = (o.P.formulation == 1);
   auto vcell = [&](int k, int64_t i) {
-    const double B = (0. + (*RD[k])(i) + (*RB[k])(i));  // R_C = 0
+    const real B = (0. + (*RD[k])(i) + (*RB[k])(i));  // R_C = 0
     return f1 ? cell_update_f1(o, *vf[k], (*vc[k])(i), (*vo[k])(i), B, i, wv[k])
               : cell_update(o, *vf[k], (*vc[k])(i), (*vo[k])(i), B, o.MF4, i, wv[k]);
   };
@@ -1230,7 +1252,7 @@ void iteration(nim_oracle &o) {
   temperature_constants(o);
   zero_flux(o);
 #pragma omp parallel for schedule(static) num_threads(nt)
-  for (int64_t i = 1; i <= N; ++i) o.RDT(i) = o.P.alpha * diffusion_source(o, o.fT, i);
+  for (int64_t i = 1; i <= N; ++i) o.RDT(i) = o.alpha * diffusion_source(o, o.fT, i);
   if (seq) {
 #pragma omp parallel for schedule(static) num_threads(nt)
     for (int64_t q = 0; q < N; ++q) {
@@ -1255,45 +1277,45 @@ void iteration(nim_oracle &o) {
 
 // check_steady_state (nse.f90:1316-1332) and evaluate_D (nse.f90:2504-2537)
 void after_integrate(nim_oracle &o) {
-  const double tdt = 2 * o.P.DT;
-  double mu = 0, mv = 0, mw = 0, mT = 0;
+  const real tdt = 2 * o.P.DT;
+  real mu = 0, mv = 0, mw = 0, mT = 0;
   for (int64_t i = 1; i <= o.NMESH; ++i) {
-    mu = std::max(mu, std::fabs(o.uxyz(i) - o.uold(i)) / tdt);
-    mv = std::max(mv, std::fabs(o.vxyz(i) - o.vold(i)) / tdt);
-    mw = std::max(mw, std::fabs(o.wxyz(i) - o.wold(i)) / tdt);
-    mT = std::max(mT, std::fabs(o.Txyz(i) - o.Told(i)) / tdt);
+    mu = std::max(mu, fabs(o.uxyz(i) - o.uold(i)) / tdt);
+    mv = std::max(mv, fabs(o.vxyz(i) - o.vold(i)) / tdt);
+    mw = std::max(mw, fabs(o.wxyz(i) - o.wold(i)) / tdt);
+    mT = std::max(mT, fabs(o.Txyz(i) - o.Told(i)) / tdt);
   }
   o.dudt_max = std::max(mw, std::max(mu, mv));
   o.dTdt_max = mT;
-  double sum1 = 0.0;
+  real sum1 = 0.0;
   for (int64_t n = 1; n <= o.NMESH; ++n) {
     int32_t nf[7];
     for (int k = 1; k <= 6; ++k) nf[k] = o.F(k, n);
-    double uf[7], vf[7], wf[7];
+    real uf[7], vf[7], wf[7];
     for (int k = 1; k <= 6; ++k) {
       uf[k] = o.fu(nf[k]);
       vf[k] = o.fv(nf[k]);
       wf[k] = o.fw(nf[k]);
     }
-    const double Dila = green_gauss(o, uf, nf, n, 1) + green_gauss(o, vf, nf, n, 2) + green_gauss(o, wf, nf, n, 3);
+    const real Dila = green_gauss(o, uf, nf, n, 1) + green_gauss(o, vf, nf, n, 2) + green_gauss(o, wf, nf, n, 3);
     o.dila(n) = Dila;
     sum1 = sum1 + Dila * Dila;
   }
-  o.Dilatation = std::sqrt(sum1 / o.NMESH);
+  o.Dilatation = sqrt(sum1 / o.NMESH);
 }
 
 void fill_integrate_stats(const nim_oracle &o, nim_step_stats *s, int iters) {
   if (!s) return;
   s->step = o.STEP;
   s->iters = iters;
-  s->err_u = o.err[0];
-  s->err_v = o.err[1];
-  s->err_w = o.err[2];
-  s->err_p = o.err[3];
-  s->err_T = o.err[4];
-  s->dilatation = o.Dilatation;
-  s->dudt_max = o.dudt_max;
-  s->dTdt_max = o.dTdt_max;
+  s->err_u = val(o.err[0]);
+  s->err_v = val(o.err[1]);
+  s->err_w = val(o.err[2]);
+  s->err_p = val(o.err[3]);
+  s->err_T = val(o.err[4]);
+  s->dilatation = val(o.Dilatation);
+  s->dudt_max = val(o.dudt_max);
+  s->dTdt_max = val(o.dTdt_max);
 }
 
 // The visiting orders of the Gauss-Seidel sweeps.  SEQUENTIAL: cell number
@@ -1338,7 +1360,7 @@ void visiting_orders(nim_oracle &o, int NT, int NR, int NZ) {
 }  // namespace
 
 // ================================================================ C API
-extern "C" int nim_oracle_create(const nim_mesh_desc *m, const nim_params *p, int32_t schedule,
+extern "C" int NIM_ORACLE_FN(create)(const nim_mesh_desc *m, const nim_params *p, int32_t schedule,
                                  int32_t threads, nim_oracle **out) {
   if (!m || !p || !out) return NIM_ERR_BAD_ARG;
   if (m->nmesh <= 0 || m->nface <= 0 || m->nnode <= 0 || m->nbcface <= 0) return NIM_ERR_BAD_ARG;
@@ -1347,7 +1369,9 @@ extern "C" int nim_oracle_create(const nim_mesh_desc *m, const nim_params *p, in
   o->sched = schedule;
   o->nthreads = threads > 0 ? threads : 1;
   o->P = *p;
-  o->Re = 1. / p->nu;       // parameters.f90:172
+  o->nu = p->nu;
+  o->alpha = p->alpha;
+  o->Re = 1. / o->nu;       // parameters.f90:172
   o->inv_Re = 1 / o->Re;    // the 1/Re factor of calculate_R_D2
   o->NMESH = m->nmesh;
   o->NFACE = m->nface;
@@ -1406,7 +1430,7 @@ extern "C" int nim_oracle_create(const nim_mesh_desc *m, const nim_params *p, in
 
 // initialize_nse (nse.f90:89-112) + apply_all_dirichlet_bcs (bc.f90:13-57),
 // TI = DT, STEP = 1 (nse.f90:31-32).
-extern "C" int nim_oracle_init(nim_oracle *o) {
+extern "C" int NIM_ORACLE_FN(init)(nim_oracle *o) {
   if (!o) return NIM_ERR_BAD_ARG;
   o->TI = o->P.DT;
   o->STEP = 1;
@@ -1436,7 +1460,7 @@ extern "C" int nim_oracle_init(nim_oracle *o) {
   return NIM_OK;
 }
 
-extern "C" int nim_oracle_begin_step(nim_oracle *o) {
+extern "C" int NIM_ORACLE_FN(begin_step)(nim_oracle *o) {
   if (!o || !o->initialized) return NIM_ERR_STATE;
   if (o->P.formulation == 1)
     velocity_constants_f1(*o);
@@ -1445,14 +1469,14 @@ extern "C" int nim_oracle_begin_step(nim_oracle *o) {
   return NIM_OK;
 }
 
-extern "C" int nim_oracle_iterate(nim_oracle *o, int32_t n, nim_step_stats *s) {
+extern "C" int NIM_ORACLE_FN(iterate)(nim_oracle *o, int32_t n, nim_step_stats *s) {
   if (!o || !o->initialized) return NIM_ERR_STATE;
   for (int32_t k = 0; k < n; ++k) iteration(*o);
   fill_integrate_stats(*o, s, n);
   return NIM_OK;
 }
 
-extern "C" int nim_oracle_integrate(nim_oracle *o, nim_step_stats *s) {
+extern "C" int NIM_ORACLE_FN(integrate)(nim_oracle *o, nim_step_stats *s) {
   if (!o || !o->initialized) return NIM_ERR_STATE;
   int cnt = 0;
   double e[5] = {1., 1., 1., 1., 1.};
@@ -1470,7 +1494,7 @@ extern "C" int nim_oracle_integrate(nim_oracle *o, nim_step_stats *s) {
     }
     ++cnt;
     iteration(*o);
-    for (int k = 0; k < 5; ++k) e[k] = o->err[k];
+    for (int k = 0; k < 5; ++k) e[k] = val(o->err[k]);
     bool finite = true;
     for (int k = 0; k < 5; ++k) finite = finite && std::isfinite(e[k]);
     if (!finite) {
@@ -1485,7 +1509,7 @@ extern "C" int nim_oracle_integrate(nim_oracle *o, nim_step_stats *s) {
 }
 
 // update_time_step (nse.f90:1292-1313) + find_Nu2 (nse.f90:2699-2798)
-extern "C" int nim_oracle_end_step(nim_oracle *o, nim_step_stats *s) {
+extern "C" int NIM_ORACLE_FN(end_step)(nim_oracle *o, nim_step_stats *s) {
   if (!o || !o->initialized) return NIM_ERR_STATE;
   const int step_done = o->STEP;
   o->STEP = o->STEP + 1;
@@ -1503,7 +1527,7 @@ extern "C" int nim_oracle_end_step(nim_oracle *o, nim_step_stats *s) {
                 o->fp(o->F(5, i)) + o->fp(o->F(6, i))) / 6.0;
     o->dila_old(i) = o->dila(i);
   }
-  double sum1 = 0., sum2 = 0., sumA1 = 0., sumA2 = 0.;
+  real sum1 = 0., sum2 = 0., sumA1 = 0., sumA2 = 0.;
   for (int64_t i = 1; i <= o->NBF; ++i) {
     const int pos = o->BCpos[i];
     if (pos != 1 && pos != 2) continue;
@@ -1512,16 +1536,16 @@ extern "C" int nim_oracle_end_step(nim_oracle *o, nim_step_stats *s) {
     const int32_t f1 = o->BCf[i], f2 = o->F(in, M), f3 = o->F(in, o->NB(in, M)),
                   f4 = o->F(in, o->NB(in, o->NB(in, M)));
     auto dist = [&](int32_t a, int32_t b) {
-      return std::sqrt(sq(o->fmid(1, a) - o->fmid(1, b)) + sq(o->fmid(2, a) - o->fmid(2, b)) +
+      return sqrt(sq(o->fmid(1, a) - o->fmid(1, b)) + sq(o->fmid(2, a) - o->fmid(2, b)) +
                        sq(o->fmid(3, a) - o->fmid(3, b)));
     };
-    const double h1 = dist(f1, f2), h2 = dist(f2, f3), h3 = dist(f3, f4);
-    const double inner = -((1. / h1 + 1. / (h1 + h2) + 1. / (h1 + h2 + h3)) * o->fT(f1)) +
+    const real h1 = dist(f1, f2), h2 = dist(f2, f3), h3 = dist(f3, f4);
+    const real inner = -((1. / h1 + 1. / (h1 + h2) + 1. / (h1 + h2 + h3)) * o->fT(f1)) +
                          ((h1 + h2) * (h1 + h2 + h3)) / (h1 * h2 * (h2 + h3)) * o->fT(f2) -
                          (h1 * (h1 + h2 + h3)) / (h2 * h3 * (h1 + h2)) * o->fT(f3) +
                          (h1 * (h1 + h2)) / (h3 * (h2 + h3) * (h1 + h2 + h3)) * o->fT(f4);
-    const double dTdx = (pos == 1) ? -(inner) : inner;
-    const double A = o->faces_area(o->F(pos, M));
+    const real dTdx = (pos == 1) ? -(inner) : inner;
+    const real A = o->faces_area(o->F(pos, M));
     if (pos == 1) {
       sum2 = sum2 + A * dTdx;
       sumA2 = sumA2 + A;
@@ -1530,26 +1554,29 @@ extern "C" int nim_oracle_end_step(nim_oracle *o, nim_step_stats *s) {
       sumA1 = sumA1 + A;
     }
   }
+  const real nu_outer = -(sum1 / sumA1 * o->P.R_o), nu_inner = -(sum2 / sumA2 * o->P.R_i);
+  o->nu_tan[0] = tan_of(nu_inner);
+  o->nu_tan[1] = tan_of(nu_outer);
   if (s) {
     s->step = step_done;
-    s->nu_outer = -(sum1 / sumA1 * o->P.R_o);
-    s->nu_inner = -(sum2 / sumA2 * o->P.R_i);
-    s->area_outer = sumA1;
-    s->area_inner = sumA2;
-    s->time = o->TI;
+    s->nu_outer = val(nu_outer);
+    s->nu_inner = val(nu_inner);
+    s->area_outer = val(sumA1);
+    s->area_inner = val(sumA2);
+    s->time = val(o->TI);
   }
   return NIM_OK;
 }
 
 // The solve_nse time loop (nse.f90:47-75)
-extern "C" int nim_oracle_step(nim_oracle *o, int32_t nsteps, nim_step_stats *per, int32_t *done) {
+extern "C" int NIM_ORACLE_FN(step)(nim_oracle *o, int32_t nsteps, nim_step_stats *per, int32_t *done) {
   if (!o || !o->initialized) return NIM_ERR_STATE;
   int32_t k = 0;
   int status = NIM_OK;
   for (; k < nsteps; ++k) {
     nim_step_stats st{};
-    nim_oracle_begin_step(o);
-    status = nim_oracle_integrate(o, &st);
+    NIM_ORACLE_FN(begin_step)(o);
+    status = NIM_ORACLE_FN(integrate)(o, &st);
     if (status != NIM_OK) {
       st.status = status;
       if (per) per[k] = st;
@@ -1561,7 +1588,7 @@ extern "C" int nim_oracle_step(nim_oracle *o, int32_t nsteps, nim_step_stats *pe
       ++k;
       break;
     }
-    nim_oracle_end_step(o, &st);
+    NIM_ORACLE_FN(end_step)(o, &st);
     if (per) per[k] = st;
   }
   if (done) *done = k;
@@ -1619,15 +1646,15 @@ V1 *field_ptr(nim_oracle &o, int32_t f) {
 }
 }  // namespace
 
-extern "C" int nim_oracle_get(nim_oracle *o, int32_t f, double *out, int64_t n) {
+extern "C" int NIM_ORACLE_FN(get)(nim_oracle *o, int32_t f, double *out, int64_t n) {
   if (!o || !out) return NIM_ERR_BAD_ARG;
   const int64_t len = field_len(*o, f);
   if (len < 0 || n < len) return NIM_ERR_BAD_ARG;
   if (V1 *v = field_ptr(*o, f)) {
-    std::memcpy(out, v->d.data() + 1, sizeof(double) * len);
+    for (int64_t i = 0; i < len; ++i) out[i] = val(v->d[i + 1]);
     return NIM_OK;
   }
-  const double *src = nullptr;
+  const real *src = nullptr;
   switch (f) {
     case NIM_FIELD_FACES_NORMAL: src = o->fnormal.d.data() + 3; break;
     case NIM_FIELD_FACES_MID: src = o->fmid.d.data() + 3; break;
@@ -1647,56 +1674,101 @@ extern "C" int nim_oracle_get(nim_oracle *o, int32_t f, double *out, int64_t n) 
     default: break;
   }
   if (src) {
-    std::memcpy(out, src, sizeof(double) * len);
+    for (int64_t i = 0; i < len; ++i) out[i] = val(src[i]);
     return NIM_OK;
   }
   if (f == NIM_FIELD_MESHES_G) {
     for (int64_t i = 1; i <= o->NMESH; ++i) {
-      out[3 * (i - 1) + 0] = o->G1(i);
-      out[3 * (i - 1) + 1] = o->G2(i);
-      out[3 * (i - 1) + 2] = o->G3(i);
+      out[3 * (i - 1) + 0] = val(o->G1(i));
+      out[3 * (i - 1) + 1] = val(o->G2(i));
+      out[3 * (i - 1) + 2] = val(o->G3(i));
     }
     return NIM_OK;
   }
   if (f == NIM_FIELD_BCS_FACES_A) {
     for (int64_t b = 1; b <= o->NBF; ++b)
-      for (int k = 1; k <= 5; ++k) out[5 * (b - 1) + k - 1] = o->BCa(k, b);
+      for (int k = 1; k <= 5; ++k) out[5 * (b - 1) + k - 1] = val(o->BCa(k, b));
     return NIM_OK;
   }
   return NIM_ERR_BAD_ARG;
 }
 
-extern "C" int nim_oracle_set(nim_oracle *o, int32_t f, const double *in, int64_t n) {
+extern "C" int NIM_ORACLE_FN(set)(nim_oracle *o, int32_t f, const double *in, int64_t n) {
   if (!o || !in) return NIM_ERR_BAD_ARG;
   const int64_t len = field_len(*o, f);
   V1 *v = field_ptr(*o, f);
   if (!v || len < 0 || n < len || f >= NIM_FIELD_MESHES_VOLUME) return NIM_ERR_BAD_ARG;
-  std::memcpy(v->d.data() + 1, in, sizeof(double) * len);
+  for (int64_t i = 0; i < len; ++i) v->d[i + 1] = in[i];  // values; derivatives start at zero
   return NIM_OK;
 }
 
-extern "C" double nim_oracle_max_rc(nim_oracle *o) { return o ? o->max_rc : -1.0; }
-extern "C" void nim_oracle_destroy(nim_oracle *o) { delete o; }
+extern "C" double NIM_ORACLE_FN(max_rc)(nim_oracle *o) { return o ? o->max_rc : -1.0; }
+extern "C" void NIM_ORACLE_FN(destroy)(nim_oracle *o) { delete o; }
 
-extern "C" void nim_oracle_set_threads(nim_oracle *o, int32_t threads) {
+extern "C" void NIM_ORACLE_FN(set_threads)(nim_oracle *o, int32_t threads) {
   if (o) o->nthreads = threads > 0 ? threads : 1;
 }
 
 // M_A(d,1:6) of nim.f90:181-287 for one direction (exposed for the
 // continuity test of the exact and series branches).
-extern "C" void nim_oracle_nim_coefficients(double u, double k, double gminus, double gplus, double v_limit,
+extern "C" void NIM_ORACLE_FN(nim_coefficients)(double u, double k, double gminus, double gplus, double v_limit,
                                             double *A) {
-  nim_direction(u, k, gminus, gplus, v_limit, A);
+  real a[6];
+  nim_direction(u, k, gminus, gplus, v_limit, a);
+  for (int q = 0; q < 6; ++q) A[q] = val(a[q]);
 }
 
-extern "C" void nim_oracle_nim1_coefficients(double u, double F, double D, double v_limit, double *out) {
+extern "C" void NIM_ORACLE_FN(nim1_coefficients)(double u, double F, double D, double v_limit, double *out) {
   const Nim1 r = nim1_direction(u, F, 2 * u / F, v_limit);
-  out[0] = r.B;
-  out[1] = r.C;
-  out[2] = nim1_E(r, u, F, D);
-  out[3] = nim1_F(r, u, F, D);
-  out[4] = r.G;
-  out[5] = r.H;
-  out[6] = r.I;
-  out[7] = r.J;
+  out[0] = val(r.B);
+  out[1] = val(r.C);
+  out[2] = val(nim1_E(r, u, F, D));
+  out[3] = val(nim1_F(r, u, F, D));
+  out[4] = val(r.G);
+  out[5] = val(r.H);
+  out[6] = val(r.I);
+  out[7] = val(r.J);
 }
+
+#ifdef NIM_ORACLE_TANGENT
+// ---- tangent-linear entry points: the derivatives along one direction of
+// (nu, alpha) and the initial/boundary values.
+// Seeds d nu and d alpha (Re and 1/Re follow, parameters.f90:172).  For a
+// derivative with respect to Ra or Pr: nu = sqrt(Pr / Ra) and alpha = nu / Pr
+// (g_beta = th_tc = 1, parameters.f90:169-173), so d/dRa seeds
+// (-nu / (2 Ra), -alpha / (2 Ra)) and d/dPr (nu / (2 Pr), -alpha / (2 Pr)).
+extern "C" int nim_oracle_tl_seed_params(nim_oracle *o, double dnu, double dalpha) {
+  if (!o) return NIM_ERR_BAD_ARG;
+  o->nu = nimtl::Dual(o->P.nu, dnu);
+  o->alpha = nimtl::Dual(o->P.alpha, dalpha);
+  o->Re = 1. / o->nu;
+  o->inv_Re = 1 / o->Re;
+  return NIM_OK;
+}
+// derivatives of a state field (the values as nim_oracle_tl_get returns them)
+extern "C" int nim_oracle_tl_get_tangent(nim_oracle *o, int32_t f, double *out, int64_t n) {
+  if (!o || !out) return NIM_ERR_BAD_ARG;
+  const int64_t len = field_len(*o, f);
+  V1 *v = field_ptr(*o, f);
+  if (!v || len < 0 || n < len) return NIM_ERR_BAD_ARG;
+  for (int64_t i = 0; i < len; ++i) out[i] = v->d[i + 1].t;
+  return NIM_OK;
+}
+// seeds the derivatives of a state field (e.g. of the outer-wall faces of
+// faces_T: the Dirichlet temperatures, written once at init and never swept)
+extern "C" int nim_oracle_tl_set_tangent(nim_oracle *o, int32_t f, const double *in, int64_t n) {
+  if (!o || !in) return NIM_ERR_BAD_ARG;
+  const int64_t len = field_len(*o, f);
+  V1 *v = field_ptr(*o, f);
+  if (!v || len < 0 || n < len || f >= NIM_FIELD_MESHES_VOLUME) return NIM_ERR_BAD_ARG;
+  for (int64_t i = 0; i < len; ++i) v->d[i + 1].t = in[i];
+  return NIM_OK;
+}
+// d Nu_inner, d Nu_outer of the last end_step (find_Nu2, nse.f90:2794-2795)
+extern "C" int nim_oracle_tl_nu_tangent(nim_oracle *o, double *out2) {
+  if (!o || !out2) return NIM_ERR_BAD_ARG;
+  out2[0] = o->nu_tan[0];
+  out2[1] = o->nu_tan[1];
+  return NIM_OK;
+}
+#endif

@@ -61,6 +61,21 @@ void nim_oracle_nim_coefficients(double u, double k, double gminus, double gplus
    for speed u, diffusivity F and Det = D */
 void nim_oracle_nim1_coefficients(double u, double F, double D, double v_limit, double *out);
 
+/* Tangent-linear build (libnim_oracle_tl.so, oracle/nim_oracle_tl.cpp): the
+   same source with dual-number values.  It exports nim_oracle_tl_<name>
+   for every nim_oracle_<name> above (arguments alike, on a nim_oracle_tl
+   handle; the values are the FP64 oracle's bit for bit) and the calls
+   below, which seed and read the derivatives along one direction of
+   (nu, alpha) and the state fields.  The FP64 tangent-linear reference
+   gradient of the Nusselt numbers with respect to Ra, Pr (through nu =
+   sqrt(Pr/Ra), alpha = nu/Pr) and the Dirichlet wall temperatures. */
+typedef struct nim_oracle_tl nim_oracle_tl;
+int nim_oracle_tl_seed_params(nim_oracle_tl *o, double dnu, double dalpha);
+int nim_oracle_tl_get_tangent(nim_oracle_tl *o, int32_t field, double *out, int64_t n);
+int nim_oracle_tl_set_tangent(nim_oracle_tl *o, int32_t field, const double *in, int64_t n);
+/* d Nu_inner, d Nu_outer of the last end_step */
+int nim_oracle_tl_nu_tangent(nim_oracle_tl *o, double *out2);
+
 /* The oracle's own cylinder mesh (create_hollow + deform_nodes + the
    renumbering of fill_global_geometry, followed loop by loop): fills
    arrays sized as nim_mesh_sizes() gives, like nim_mesh_build(), without

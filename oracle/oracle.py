@@ -22,6 +22,30 @@ SEQUENTIAL = 0
 PARALLEL = 1
 LEVELS = 2        # SEQUENTIAL arithmetic, cells and wall faces in level order
 _lib = None
+_tl_lib = None
+
+
+def _bind(L: C.CDLL, pre: str):
+    """argtypes of the time-advance entry points <pre>create ... <pre>set_threads."""
+    vp = C.c_void_p
+    dp = C.POINTER(C.c_double)
+
+    def sig(name, args, res=C.c_int):
+        f = getattr(L, pre + name)
+        f.argtypes, f.restype = args, res
+    sig("create", [C.POINTER(_abi.MeshDesc), C.POINTER(_abi.Params), C.c_int32, C.c_int32, C.POINTER(vp)])
+    sig("init", [vp])
+    sig("begin_step", [vp])
+    sig("integrate", [vp, C.POINTER(_abi.StepStats)])
+    sig("iterate", [vp, C.c_int32, C.POINTER(_abi.StepStats)])
+    sig("end_step", [vp, C.POINTER(_abi.StepStats)])
+    sig("step", [vp, C.c_int32, C.POINTER(_abi.StepStats), C.POINTER(C.c_int32)])
+    sig("get", [vp, C.c_int32, dp, C.c_int64])
+    sig("set", [vp, C.c_int32, dp, C.c_int64])
+    sig("max_rc", [vp], C.c_double)
+    sig("destroy", [vp], None)
+    sig("set_threads", [vp, C.c_int32], None)
+    sig("nim_coefficients", [C.c_double] * 5 + [dp], None)
 
 
 def lib() -> C.CDLL:
@@ -31,38 +55,33 @@ def lib() -> C.CDLL:
         if not path.exists():
             raise FileNotFoundError(f"{path} missing: run make -C oracle")
         L = C.CDLL(str(path))
-        vp = C.c_void_p
-        L.nim_oracle_create.argtypes = [C.POINTER(_abi.MeshDesc), C.POINTER(_abi.Params), C.c_int32,
-                                        C.c_int32, C.POINTER(vp)]
-        L.nim_oracle_create.restype = C.c_int
-        for n in ("nim_oracle_init", "nim_oracle_begin_step"):
-            getattr(L, n).argtypes = [vp]
-            getattr(L, n).restype = C.c_int
-        L.nim_oracle_integrate.argtypes = [vp, C.POINTER(_abi.StepStats)]
-        L.nim_oracle_integrate.restype = C.c_int
-        L.nim_oracle_iterate.argtypes = [vp, C.c_int32, C.POINTER(_abi.StepStats)]
-        L.nim_oracle_iterate.restype = C.c_int
-        L.nim_oracle_end_step.argtypes = [vp, C.POINTER(_abi.StepStats)]
-        L.nim_oracle_end_step.restype = C.c_int
-        L.nim_oracle_step.argtypes = [vp, C.c_int32, C.POINTER(_abi.StepStats), C.POINTER(C.c_int32)]
-        L.nim_oracle_step.restype = C.c_int
-        L.nim_oracle_get.argtypes = [vp, C.c_int32, C.POINTER(C.c_double), C.c_int64]
-        L.nim_oracle_get.restype = C.c_int
-        L.nim_oracle_set.argtypes = [vp, C.c_int32, C.POINTER(C.c_double), C.c_int64]
-        L.nim_oracle_set.restype = C.c_int
-        L.nim_oracle_max_rc.argtypes = [vp]
-        L.nim_oracle_max_rc.restype = C.c_double
-        L.nim_oracle_destroy.argtypes = [vp]
-        L.nim_oracle_destroy.restype = None
-        L.nim_oracle_set_threads.argtypes = [vp, C.c_int32]
-        L.nim_oracle_set_threads.restype = None
+        _bind(L, "nim_oracle_")
         ip = C.POINTER(C.c_int32)
         L.nim_oracle_mesh_build.argtypes = [C.POINTER(_abi.MeshParams), C.POINTER(C.c_double)] + [ip] * 8
         L.nim_oracle_mesh_build.restype = C.c_int
-        L.nim_oracle_nim_coefficients.argtypes = [C.c_double] * 5 + [C.POINTER(C.c_double)]
-        L.nim_oracle_nim_coefficients.restype = None
         _lib = L
     return _lib
+
+
+def tl_lib() -> C.CDLL:
+    """The tangent-linear build (nim_oracle_tl.cpp): dual-number values."""
+    global _tl_lib
+    if _tl_lib is None:
+        path = _HERE / "_build" / "libnim_oracle_tl.so"
+        if not path.exists():
+            raise FileNotFoundError(f"{path} missing: run make -C oracle")
+        L = C.CDLL(str(path))
+        _bind(L, "nim_oracle_tl_")
+        vp, dp = C.c_void_p, C.POINTER(C.c_double)
+        L.nim_oracle_tl_seed_params.argtypes = [vp, C.c_double, C.c_double]
+        L.nim_oracle_tl_seed_params.restype = C.c_int
+        for n in ("get_tangent", "set_tangent"):
+            getattr(L, "nim_oracle_tl_" + n).argtypes = [vp, C.c_int32, dp, C.c_int64]
+            getattr(L, "nim_oracle_tl_" + n).restype = C.c_int
+        L.nim_oracle_tl_nu_tangent.argtypes = [vp, dp]
+        L.nim_oracle_tl_nu_tangent.restype = C.c_int
+        _tl_lib = L
+    return _tl_lib
 
 
 class OracleMesh:
@@ -122,17 +141,24 @@ def temperature_noise(mesh, amp: float, seed: int):
 class Oracle:
     """The reference algorithm on the CPU, one call per reference subroutine."""
 
+    _pre = "nim_oracle_"
+
+    def _lib(self) -> C.CDLL:
+        return lib()
+
+    def _f(self, name: str):
+        return getattr(self._lib(), self._pre + name)
+
     def __init__(self, mesh, params: _abi.Params, schedule: int = SEQUENTIAL, threads: int = 1):
         self.mesh = mesh
         self.params = params
         self._h = C.c_void_p()
-        st = lib().nim_oracle_create(C.byref(mesh.desc), C.byref(params), schedule, threads,
-                                     C.byref(self._h))
-        _abi.check(st, "nim_oracle_create")
+        st = self._f("create")(C.byref(mesh.desc), C.byref(params), schedule, threads, C.byref(self._h))
+        _abi.check(st, self._pre + "create")
 
     def close(self):
         if self._h:
-            lib().nim_oracle_destroy(self._h)
+            self._f("destroy")(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):
@@ -142,43 +168,41 @@ class Oracle:
             pass
 
     def init(self):
-        _abi.check(lib().nim_oracle_init(self._h), "nim_oracle_init")
+        _abi.check(self._f("init")(self._h), "init")
 
     def begin_step(self):
-        _abi.check(lib().nim_oracle_begin_step(self._h), "nim_oracle_begin_step")
+        _abi.check(self._f("begin_step")(self._h), "begin_step")
 
     def integrate(self) -> _abi.StepStats:
         s = _abi.StepStats()
-        st = lib().nim_oracle_integrate(self._h, C.byref(s))
+        st = self._f("integrate")(self._h, C.byref(s))
         s.status = st
         return s
 
     def iterate(self, n: int) -> _abi.StepStats:
         s = _abi.StepStats()
-        _abi.check(lib().nim_oracle_iterate(self._h, n, C.byref(s)), "nim_oracle_iterate")
+        _abi.check(self._f("iterate")(self._h, n, C.byref(s)), "iterate")
         return s
 
     def end_step(self) -> _abi.StepStats:
         s = _abi.StepStats()
-        _abi.check(lib().nim_oracle_end_step(self._h, C.byref(s)), "nim_oracle_end_step")
+        _abi.check(self._f("end_step")(self._h, C.byref(s)), "end_step")
         return s
 
     def step(self, n: int):
         arr = (_abi.StepStats * max(n, 1))()
         done = C.c_int32()
-        st = lib().nim_oracle_step(self._h, n, arr, C.byref(done))
+        st = self._f("step")(self._h, n, arr, C.byref(done))
         return st, [arr[i] for i in range(done.value)]
 
     def get(self, field: int, n: int) -> np.ndarray:
         out = np.zeros(n, dtype=np.float64)
-        _abi.check(lib().nim_oracle_get(self._h, field, out.ctypes.data_as(C.POINTER(C.c_double)), n),
-                   "nim_oracle_get")
+        _abi.check(self._f("get")(self._h, field, out.ctypes.data_as(C.POINTER(C.c_double)), n), "get")
         return out
 
     def set(self, field: int, a: np.ndarray):
         a = np.ascontiguousarray(a, dtype=np.float64)
-        _abi.check(lib().nim_oracle_set(self._h, field, a.ctypes.data_as(C.POINTER(C.c_double)), a.size),
-                   "nim_oracle_set")
+        _abi.check(self._f("set")(self._h, field, a.ctypes.data_as(C.POINTER(C.c_double)), a.size), "set")
 
     def add_temperature_noise(self, amp: float, seed: int):
         """The seeded initial-temperature noise of the benchmark cases."""
@@ -190,10 +214,55 @@ class Oracle:
             self.set(f, self.get(f, self.mesh.nmesh) + cells)
 
     def set_threads(self, n: int):
-        lib().nim_oracle_set_threads(self._h, n)
+        self._f("set_threads")(self._h, n)
 
     def max_rc(self) -> float:
-        return lib().nim_oracle_max_rc(self._h)
+        return self._f("max_rc")(self._h)
+
+
+class TangentOracle(Oracle):
+    """The oracle's tangent-linear build: the FP64 oracle's values bit for
+    bit, and along one seeded direction their derivatives.  Seeds: d nu and
+    d alpha (seed_params; with_respect_to gives the seeds of Ra and Pr), and
+    the derivatives of the state fields (set_tangent after init(): e.g. the
+    outer-wall Dirichlet faces of faces_T)."""
+
+    _pre = "nim_oracle_tl_"
+
+    def _lib(self) -> C.CDLL:
+        return tl_lib()
+
+    def seed_params(self, dnu: float, dalpha: float):
+        _abi.check(self._f("seed_params")(self._h, dnu, dalpha), "seed_params")
+
+    @staticmethod
+    def with_respect_to(name: str, Ra: float, Pr: float):
+        """(d nu, d alpha) for d/dRa or d/dPr: nu = sqrt(Pr / Ra), alpha =
+        nu / Pr (parameters.f90:169-173 with g_beta = th_tc = 1)."""
+        nu = (Pr / Ra) ** 0.5
+        alpha = nu / Pr
+        if name == "Ra":
+            return -nu / (2 * Ra), -alpha / (2 * Ra)
+        if name == "Pr":
+            return nu / (2 * Pr), -alpha / (2 * Pr)
+        raise ValueError(name)
+
+    def get_tangent(self, field: int, n: int) -> np.ndarray:
+        out = np.zeros(n, dtype=np.float64)
+        _abi.check(self._f("get_tangent")(self._h, field, out.ctypes.data_as(C.POINTER(C.c_double)), n),
+                   "get_tangent")
+        return out
+
+    def set_tangent(self, field: int, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        _abi.check(self._f("set_tangent")(self._h, field, a.ctypes.data_as(C.POINTER(C.c_double)), a.size),
+                   "set_tangent")
+
+    def nu_tangent(self):
+        """(d Nu_inner, d Nu_outer) of the last end_step."""
+        out = np.zeros(2, dtype=np.float64)
+        _abi.check(self._f("nu_tangent")(self._h, out.ctypes.data_as(C.POINTER(C.c_double))), "nu_tangent")
+        return float(out[0]), float(out[1])
 
 
 def nim1_coefficients(u: float, F: float, D: float, v_limit: float = 1e-2):
