@@ -414,6 +414,38 @@ int64_t nim_gpu_launch_count(nim_ctx *ctx);
 int nim_gpu_profile_iterations(nim_ctx *ctx, int32_t n, double *ms, int32_t cap);
 const char *nim_gpu_profile_name(nim_ctx *ctx, int32_t k);
 
+/* ---------------------------------------------------- tangent-linear steps
+   Forward-mode derivatives of the time advance (no counterpart in the
+   reference): a dual copy of the iterate (value and derivative along one
+   seeded direction) advanced by the dual instantiations of the step's
+   kernels, the derivative of the hot- and cold-wall Nusselt numbers
+   (find_Nu2, nse.f90:2794) with respect to Ra, Pr (through nu = sqrt(Pr/Ra),
+   alpha = nu/Pr, parameters.f90:169-173) and the Dirichlet wall
+   temperatures.  The FP64 tangent-linear gradient the adjoint is checked
+   against; the values are the FP64 parallel path's bit for bit.
+   Parallel schedule and formulation 2 only; the FP64 state of the context
+   is left as it was (the dual state is a copy). */
+/* Copies the context's current FP64 state (after nim_gpu_init or between
+   steps) into the dual state with zero derivatives and zero seeds.  The
+   first call allocates it (~3.4 kB per cell). */
+int nim_gpu_tangent_begin(nim_ctx *ctx);
+/* Seeds d nu and d alpha (1/Re follows).  d/dRa: (-nu/(2 Ra), -alpha/(2 Ra));
+   d/dPr: (nu/(2 Pr), -alpha/(2 Pr)). */
+int nim_gpu_tangent_seed(nim_ctx *ctx, double dnu, double dalpha);
+/* Seeds the derivatives of a state field (faces u, v, w, p, T; cells u, v, w,
+   T, their old and time-averaged values, meshes_p, meshes_dila), n values
+   in the layout of nim_gpu_download; e.g. the outer-wall faces of faces_T
+   for the Dirichlet wall temperatures. */
+int nim_gpu_tangent_seed_field(nim_ctx *ctx, nim_field field, const double *tangent, int64_t n);
+/* nsteps steps of the dual state (nim_gpu_step's work: begin_step, the inner
+   loop to the reference's test, update_time_step, find_Nu2); per_step the
+   values' statistics, dnu[2k], dnu[2k+1] = d Nu_inner, d Nu_outer of step k.
+   Either output may be NULL. */
+int nim_gpu_tangent_step(nim_ctx *ctx, int32_t nsteps, nim_step_stats *per_step, double *dnu);
+/* Value and derivative of a state field of the dual state (fields as
+   nim_gpu_tangent_seed_field). */
+int nim_gpu_tangent_get(nim_ctx *ctx, nim_field field, double *value, double *tangent, int64_t n);
+
 /* Self-test of the bounded device waits (no counterpart in the reference):
    runs the wait that the TMA-staged sweeps use on an mbarrier that no copy
    will complete, at most `tries` (1..2^20) times, and returns the status the

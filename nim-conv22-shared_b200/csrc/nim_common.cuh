@@ -125,17 +125,19 @@ __host__ __device__ inline BFace bface(const Dims &d, int b) {
 
 // x^n for the constant exponents of nim.f90's series, multiplied in the order
 // gfortran's gfc_conv_powi emits (x^n = x^(n-t[n]) * x^t[n]).
-struct Pw {
-  double p[13];
-  __host__ __device__ explicit Pw(double x) {
+template <class V>
+struct PwT {
+  V p[13];
+  __host__ __device__ explicit PwT(V x) {
     p[0] = 1.0; p[1] = x;
     p[2] = p[1] * p[1]; p[3] = p[1] * p[2]; p[4] = p[2] * p[2];
     p[5] = p[2] * p[3]; p[6] = p[3] * p[3]; p[7] = p[3] * p[4];
     p[8] = p[4] * p[4]; p[9] = p[3] * p[6]; p[10] = p[5] * p[5];
     p[11] = p[5] * p[6]; p[12] = p[6] * p[6];
   }
-  __host__ __device__ double operator[](int n) const { return p[n]; }
+  __host__ __device__ V operator[](int n) const { return p[n]; }
 };
+using Pw = PwT<double>;
 
 // 5-point Gauss-Legendre rule (parameters.f90:18-22), filled once from the
 // host with the same expressions.

@@ -120,6 +120,14 @@ struct nim_ctx {
   int graph32_iters = 0;
   int phase = 0;
   int last_lowp = 0, last_hi = 0;
+  // tangent-linear state (nim_gpu_tangent_*): dual copies of the geometry
+  // and of the iterate, their own control block and step counter
+  bool dual_alloc = false, dual_ready = false;
+  GeoT<DualD> gD{};
+  FieldsT<DualD> FD{};
+  Ctrl *ctlD = nullptr;
+  int32_t dual_STEP = 0;
+  double dual_TI = 0;
   // z-slab s of slab_count (nim_gpu_create_slab; slab_count 0: the whole
   // mesh): global plane of local plane 0, and per side (0: the slab below,
   // 1: above) whether it has a neighbour and the element spans of its halo
@@ -259,6 +267,7 @@ Phys make_phys(const nim_params &p) {
   P.max_iters = p.max_iters;
   P.dpdx_tolerance = p.dpdx_tolerance;
   P.formulation = p.formulation;
+  P.d_nu = P.d_alpha = P.d_inv_Re = 0.0;  // seeded by nim_gpu_tangent_seed
   return P;
 }
 
@@ -326,6 +335,14 @@ int launch_vel(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F
       TRY(mark(x, "k_vel_face"));
     }
   }
+  return NIM_OK;
+}
+// the tangent-linear state (formulation 2): the gather forms of both sweeps
+int launch_vel(nim_ctx *x, cudaStream_t s, const GeoT<DualD> &g, const FieldsT<DualD> &F) {
+  k_vel_cell<false, 2><<<x->g3, dim3(CB, 3), 0, s>>>(x->d, g, F, x->phys, x->ctl);
+  TRY(mark(x, "k_vel_cell"));
+  k_vel_face<<<x->g3, dim3(CB, 3), 0, s>>>(x->d, g, F, x->phys, x->ctl);
+  TRY(mark(x, "k_vel_face"));
   return NIM_OK;
 }
 
@@ -2157,6 +2174,293 @@ extern "C" int nim_gpu_selftest_exp(const double *x, double *y, int64_t n) {
   cudaFree(dx);
   cudaFree(dy);
   return st;
+}
+
+// ---- tangent-linear steps (forward mode): a dual copy of the iterate and
+// geometry advanced by the dual instantiations of the step's kernels
+namespace {
+
+int dual_alloc(nim_ctx *x) {
+  const Dims &d = x->d;
+  const size_t Nc = d.Nc, NF = d.NF, NB = d.NBF;
+  GeoT<DualD> &h = x->gD;
+  TRY(dalloc(x, &h.vol, Nc));
+  TRY(dalloc(x, &h.G, 3 * Nc));
+  TRY(dalloc(x, &h.gij, 9 * Nc));
+  TRY(dalloc(x, &h.xi, 9 * Nc));
+  TRY(dalloc(x, &h.gfd, 6 * Nc));
+  TRY(dalloc(x, &h.dg, 6 * Nc));
+  TRY(dalloc(x, &h.area, NF));
+  TRY(dalloc(x, &h.normal, 3 * NF));
+  TRY(dalloc(x, &h.AA, 45 * Nc));
+  h.bcpts = x->g.bcpts;  // integer: shared with the FP64 side
+  TRY(dalloc(x, &h.bca, 5 * NB));
+  TRY(dalloc(x, &h.bcap, 8 * NB));
+  TRY(dalloc(x, &h.bcg, 2 * NB));
+  TRY(dalloc(x, &h.zf, 4 * NB));
+  TRY(dalloc(x, &h.nuw, 4 * NB));
+  FieldsT<DualD> &H = x->FD;
+  for (int q = 0; q < 5; ++q) TRY(dalloc(x, &H.f[q], 2 * NF));
+  for (int q = 0; q < 4; ++q) {
+    TRY(dalloc(x, &H.c[q], Nc));
+    TRY(dalloc(x, &H.co[q], Nc));
+    TRY(dalloc(x, &H.ct[q], Nc));
+  }
+  TRY(dalloc(x, &H.mp, Nc));
+  TRY(dalloc(x, &H.dila, Nc));
+  TRY(dalloc(x, &H.dila_old, Nc));
+  TRY(dalloc(x, &H.Rp, Nc));
+  TRY(dalloc(x, &H.MA, 18 * Nc));
+  TRY(dalloc(x, &H.MF4, 8 * Nc));
+  TRY(dalloc(x, &H.MF, 15 * Nc));
+  TRY(dalloc(x, &H.MTF, 15 * Nc));
+  TRY(dalloc(x, &H.MTA, 18 * Nc));
+  TRY(dalloc(x, &H.dpd, 3 * Nc));
+  H.part = x->F.part;  // per-block partial sums: FP64, shared
+  TRY(dalloc(x, &x->ctlD, 1));
+  x->dual_alloc = true;
+  return NIM_OK;
+}
+
+// the FP64 geometry and iterate into the dual arrays, derivatives zero
+int dual_copy(nim_ctx *x) {
+  const Dims &d = x->d;
+  const size_t Nc = d.Nc, NF = d.NF, NB = d.NBF;
+  const Geo &g = x->g;
+  GeoT<DualD> &h = x->gD;
+  Cvt c;
+  c.add(g.vol, h.vol, Nc);
+  c.add(g.G, h.G, 3 * Nc);
+  c.add(g.gij, h.gij, 9 * Nc);
+  c.add(g.xi, h.xi, 9 * Nc);
+  c.add(g.gfd, h.gfd, 6 * Nc);
+  c.add(g.dg, h.dg, 6 * Nc);
+  c.add(g.area, h.area, NF);
+  c.add(g.normal, h.normal, 3 * NF);
+  c.add(g.AA, h.AA, 45 * Nc);
+  c.add(g.bca, h.bca, 5 * NB);
+  c.add(g.bcap, h.bcap, 8 * NB);
+  c.add(g.bcg, h.bcg, 2 * NB);
+  c.add(g.zf, h.zf, 4 * NB);
+  c.add(g.nuw, h.nuw, 4 * NB);
+  TRY((run_cvt<double, DualD>(x, c)));
+  const Fields &F = x->F;
+  FieldsT<DualD> &H = x->FD;
+  Cvt s;
+  for (int q = 0; q < 5; ++q) s.add(F.f[q], H.f[q], 2 * NF);
+  for (int q = 0; q < 4; ++q) {
+    s.add(F.c[q], H.c[q], Nc);
+    s.add(F.co[q], H.co[q], Nc);
+    s.add(F.ct[q], H.ct[q], Nc);
+  }
+  s.add(F.mp, H.mp, Nc);
+  s.add(F.dila, H.dila, Nc);
+  s.add(F.dila_old, H.dila_old, Nc);
+  s.add(F.dpd, H.dpd, 3 * Nc);
+  TRY((run_cvt<double, DualD>(x, s)));
+  CK(cudaMemcpyAsync(x->ctlD, x->ctl, sizeof(Ctrl), cudaMemcpyDeviceToDevice, x->stream));
+  return NIM_OK;
+}
+
+// the dual state of a field: its array (both halves of a face field) or null
+struct DualView {
+  DualD *p = nullptr, *p1 = nullptr;
+  int n = 0;
+  bool face = false;
+};
+int dual_view(nim_ctx *x, nim_field f, int par, DualView &v) {
+  const Dims &d = x->d;
+  FieldsT<DualD> &H = x->FD;
+  auto cellf = [&](DualD *p) { v.p = p; v.n = d.Nc; };
+  switch (f) {
+    case NIM_FIELD_FACES_U: case NIM_FIELD_FACES_V: case NIM_FIELD_FACES_W: case NIM_FIELD_FACES_P:
+    case NIM_FIELD_FACES_T:
+      v.p = H.f[(int)f] + (size_t)par * d.NF;
+      v.p1 = H.f[(int)f] + (size_t)(1 - par) * d.NF;
+      v.n = d.NF;
+      v.face = true;
+      return NIM_OK;
+    case NIM_FIELD_MESHES_U: case NIM_FIELD_MESHES_V: case NIM_FIELD_MESHES_W: case NIM_FIELD_MESHES_T:
+      cellf(H.c[(int)f - 5]); return NIM_OK;
+    case NIM_FIELD_MESHES_U_OLD: case NIM_FIELD_MESHES_V_OLD: case NIM_FIELD_MESHES_W_OLD:
+    case NIM_FIELD_MESHES_T_OLD:
+      cellf(H.co[(int)f - 9]); return NIM_OK;
+    case NIM_FIELD_MESHES_UT: case NIM_FIELD_MESHES_VT: case NIM_FIELD_MESHES_WT: case NIM_FIELD_MESHES_TT:
+      cellf(H.ct[(int)f - 13]); return NIM_OK;
+    case NIM_FIELD_MESHES_P: cellf(H.mp); return NIM_OK;
+    case NIM_FIELD_MESHES_DILA: cellf(H.dila); return NIM_OK;
+    default: return NIM_ERR_BAD_ARG;
+  }
+}
+
+__global__ void k_dual_gather(const DualD *__restrict__ src, const int *__restrict__ perm, int n,
+                              double *__restrict__ v, double *__restrict__ t) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DualD a = src[perm ? perm[i] : i];
+  v[i] = a.v;
+  t[i] = a.t;
+}
+__global__ void k_dual_seed(const double *__restrict__ t, const int *__restrict__ perm, int n, DualD *dst,
+                            DualD *dst1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int s = perm ? perm[i] : i;
+  dst[s].t = t[i];
+  if (dst1) dst1[s].t = t[i];
+}
+
+// the dual state's control block stands in for the context's while a dual
+// step runs (the kernels and read_ctrl use x->ctl)
+struct DualCtl {
+  nim_ctx *x;
+  Ctrl *keep;
+  explicit DualCtl(nim_ctx *c) : x(c), keep(c->ctl) { x->ctl = x->ctlD; }
+  ~DualCtl() { x->ctl = keep; }
+};
+
+constexpr int kDualCap = 4000000;  // passes per step without max_iters
+
+// one dual step: begin_step, the inner loop until the reference's test holds,
+// after_integrate, update_time_step, find_Nu2; d Nu_inner, d Nu_outer
+int dual_step(nim_ctx *x, nim_step_stats *s, double *dnu2) {
+  const Dims &d = x->d;
+  cudaStream_t st = x->stream;
+  DualCtl use(x);
+  k_step_reset<<<1, 1, 0, st>>>(x->ctl);
+  k_vel_coef_A<<<x->nblk_c, BLK, 0, st>>>(d, x->gD, x->FD, x->phys);
+  k_vel_coef_F<<<x->nblk_c, BLK, 0, st>>>(d, x->FD, x->phys);
+  CK(cudaGetLastError());
+  x->launches += 3;
+  for (;;) {
+    for (int k = 0; k < 8; ++k) TRY(launch_parallel(x, x->gD, x->FD, 0));
+    TRY(read_ctrl(x));
+    if (x->ctl_host->done) break;
+    if (x->ctl_host->step_iters >= kDualCap) {
+      x->ctl_host->status = NIM_ERR_NOT_CONVERGED;
+      break;
+    }
+  }
+  const int status = x->ctl_host->status;
+  k_after_integrate<<<x->nblk_c, BLK, 0, st>>>(d, x->gD, x->FD, x->phys, x->ctl, x->nblk_c);
+  k_finish_sum<<<1, BLK, 0, st>>>(x->F.part, x->nblk_c, 1, x->sums);
+  CK(cudaGetLastError());
+  x->launches += 2;
+  CK(cudaMemcpyAsync(x->host_sums, x->sums, sizeof(double), cudaMemcpyDeviceToHost, st));
+  TRY(read_ctrl(x));
+  if (s) {
+    fill_iter_stats(x, s);
+    s->status = status;
+    s->iters_fp32 = 0;
+    s->dilatation = std::sqrt(x->host_sums[0] / d.Nc);
+    s->dudt_max = bits_to_double(x->ctl_host->red[0]);
+    s->dTdt_max = bits_to_double(x->ctl_host->red[1]);
+  }
+  if (status != NIM_OK) return status;
+  const int nr = 2 * d.NT * d.NZ, gn = grid(nr);
+  k_update_time<<<x->nblk_c, BLK, 0, st>>>(d, x->FD, x->ctl);
+  k_nusselt<<<gn, BLK, 0, st>>>(d, x->gD, x->FD, x->ctl, gn);
+  k_finish_sum<<<1, BLK, 0, st>>>(x->F.part, gn, 8, x->sums);
+  CK(cudaGetLastError());
+  x->launches += 3;
+  CK(cudaMemcpyAsync(x->host_sums, x->sums, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const double *h = x->host_sums;
+  const DualD sum1(h[0], h[4]), sumA1(h[1], h[5]), sum2(h[2], h[6]), sumA2(h[3], h[7]);
+  const DualD nu_outer = -(sum1 / sumA1 * x->params.R_o), nu_inner = -(sum2 / sumA2 * x->params.R_i);
+  const int32_t step_done = x->dual_STEP;
+  x->dual_STEP = x->dual_STEP + 1;
+  x->dual_TI = x->dual_TI + 2 * x->params.DT;
+  if (s) {
+    s->step = step_done;
+    s->nu_outer = nu_outer.v;
+    s->nu_inner = nu_inner.v;
+    s->area_outer = sumA1.v;
+    s->area_inner = sumA2.v;
+    s->time = x->dual_TI;
+  }
+  if (dnu2) {
+    dnu2[0] = nu_inner.t;
+    dnu2[1] = nu_outer.t;
+  }
+  return NIM_OK;
+}
+}  // namespace
+
+extern "C" int nim_gpu_tangent_begin(nim_ctx *x) {
+  if (!x) return NIM_ERR_BAD_ARG;
+  if (!x->initialized || x->in_step) return NIM_ERR_STATE;
+  if (x->seq || x->phys.formulation != 2 || x->slab_count) return NIM_ERR_BAD_ARG;
+  CK(cudaSetDevice(x->device));
+  if (!x->dual_alloc) TRY(dual_alloc(x));
+  TRY(dual_copy(x));
+  x->phys.d_nu = x->phys.d_alpha = x->phys.d_inv_Re = 0.0;
+  x->dual_STEP = x->STEP;
+  x->dual_TI = x->TI;
+  x->dual_ready = true;
+  CK(cudaStreamSynchronize(x->stream));
+  return NIM_OK;
+}
+
+extern "C" int nim_gpu_tangent_seed(nim_ctx *x, double dnu, double dalpha) {
+  if (!x) return NIM_ERR_BAD_ARG;
+  if (!x->dual_ready) return NIM_ERR_STATE;
+  // Re = 1/nu and 1/Re as the time advance forms them (parameters.f90:172)
+  const DualD nu(x->phys.nu, dnu);
+  const DualD Re = DualD(1.) / nu;
+  const DualD inv_Re = DualD(1.) / Re;
+  x->phys.d_nu = dnu;
+  x->phys.d_alpha = dalpha;
+  x->phys.d_inv_Re = inv_Re.t;
+  return NIM_OK;
+}
+
+extern "C" int nim_gpu_tangent_seed_field(nim_ctx *x, nim_field f, const double *t, int64_t n) {
+  if (!x || !t) return NIM_ERR_BAD_ARG;
+  if (!x->dual_ready) return NIM_ERR_STATE;
+  CK(cudaSetDevice(x->device));
+  DualCtl use(x);
+  TRY(read_ctrl(x));
+  DualView v;
+  TRY(dual_view(x, f, x->ctl_host->iter & 1, v));
+  if (n < v.n) return NIM_ERR_BAD_ARG;
+  CK(cudaMemcpyAsync(x->scratch, t, sizeof(double) * v.n, cudaMemcpyHostToDevice, x->stream));
+  k_dual_seed<<<grid(v.n), BLK, 0, x->stream>>>(x->scratch, v.face ? x->perm : nullptr, v.n, v.p, v.p1);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(x->stream));
+  return NIM_OK;
+}
+
+extern "C" int nim_gpu_tangent_get(nim_ctx *x, nim_field f, double *value, double *tangent, int64_t n) {
+  if (!x || !value || !tangent) return NIM_ERR_BAD_ARG;
+  if (!x->dual_ready) return NIM_ERR_STATE;
+  CK(cudaSetDevice(x->device));
+  DualCtl use(x);
+  TRY(read_ctrl(x));
+  DualView v;
+  TRY(dual_view(x, f, x->ctl_host->iter & 1, v));
+  if (n < v.n) return NIM_ERR_BAD_ARG;
+  double *sv = x->scratch, *stt = x->scratch + v.n;
+  k_dual_gather<<<grid(v.n), BLK, 0, x->stream>>>(v.p, v.face ? x->perm : nullptr, v.n, sv, stt);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(value, sv, sizeof(double) * v.n, cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaMemcpyAsync(tangent, stt, sizeof(double) * v.n, cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  return NIM_OK;
+}
+
+extern "C" int nim_gpu_tangent_step(nim_ctx *x, int32_t nsteps, nim_step_stats *per_step, double *dnu) {
+  if (!x || nsteps < 0) return NIM_ERR_BAD_ARG;
+  if (!x->dual_ready) return NIM_ERR_STATE;
+  CK(cudaSetDevice(x->device));
+  for (int32_t k = 0; k < nsteps; ++k) {
+    nim_step_stats rec;
+    std::memset(&rec, 0, sizeof(rec));
+    const int st = dual_step(x, &rec, dnu ? dnu + 2 * k : nullptr);
+    if (per_step) per_step[k] = rec;
+    if (st != NIM_OK) return st;
+  }
+  return NIM_OK;
 }
 
 extern "C" int nim_gpu_selftest_nim_coef(const double *u, const double *k, int64_t n, int32_t precision,

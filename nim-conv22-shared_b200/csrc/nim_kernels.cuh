@@ -32,8 +32,28 @@
 
 #include "nim_common.cuh"
 #include "nim_exp.cuh"
+#include "nim_dual.cuh"
 
 namespace nim {
+
+// Arithmetic type of a kernel over storage type R: double for the FP64
+// path, float for the float mirror of the FP32 phase (whose kernels compute
+// in float, with only the change maxima and reductions in double), DualD
+// for the tangent-linear state (value and derivative).
+template <class R>
+struct ArithOf {
+  using type = double;
+};
+template <>
+struct ArithOf<float> {
+  using type = float;
+};
+template <>
+struct ArithOf<DualD> {
+  using type = DualD;
+};
+template <class R>
+using Ar = typename ArithOf<R>::type;
 
 // ------------------------------------------------------------ device state
 // Geometry and field arrays, by storage type R: double for the FP64 path;
@@ -99,7 +119,24 @@ struct Phys {
   double inv_rho;  // 1/rho
   int max_iters, dpdx_tolerance;
   int formulation; // nim_formulation: 1 or 2
+  // derivatives of nu, alpha and 1/Re along the seeded direction: read only
+  // by the dual instantiations (nim_gpu_tangent_*), zero otherwise
+  double d_nu, d_alpha, d_inv_Re;
 };
+// a parameter as the arithmetic type V sees it: its value, and in the dual
+// instantiations its seeded derivative
+template <class V>
+struct ParOf {
+  __device__ __forceinline__ static V get(double v, double) { return V(v); }
+};
+template <>
+struct ParOf<DualD> {
+  __device__ __forceinline__ static DualD get(double v, double t) { return DualD(v, t); }
+};
+template <class V>
+__device__ __forceinline__ V pv(double v, double t) {
+  return ParOf<V>::get(v, t);
+}
 
 // Control block in device memory; k_iter_end is its only writer during an
 // iteration, the host reads it between batches.
@@ -628,37 +665,37 @@ __global__ void k_apply_dirichlet(Dims d, Geo g, Fields F) {
 // ============================================================= per step
 // NIM coefficients of one direction for contravariant speed u and
 // diffusivity k: M_A(d,1:6) / MT_A(d,1:6) (nim.f90:181-287, 354-460).
-__device__ __forceinline__ void nim_direction(double u, double k, double gminus, double gplus, double v_limit,
-                                              double A[6]) {
-  const double a = 1.;
-  const double Re = 2 * a * u / k;
+template <class V>
+__device__ __forceinline__ void nim_direction(V u, V k, V gminus, V gplus, double v_limit, V A[6]) {
+  const V a = V(1.);
+  const V Re = 2 * a * u / k;
   if (fabs(Re) > v_limit) {
-    const double e = nim_exp(Re);
-    A[0] = (2 * a / (k * (1. / e - 1.)) + 1. / u) * gplus;
-    A[1] = (-(2 * a / (k * (1. - e))) - 1. / u) * gminus;
-    A[2] = (u / (k * (1. / e - 1.))) * gplus;
-    A[3] = (u / (k * (1. - e))) * gminus;
+    const V e = nim_exp(Re);
+    A[0] = (2 * a / (k * (V(1.) / e - V(1.))) + V(1.) / u) * gplus;
+    A[1] = (-(2 * a / (k * (V(1.) - e))) - V(1.) / u) * gminus;
+    A[2] = (u / (k * (V(1.) / e - V(1.)))) * gplus;
+    A[3] = (u / (k * (V(1.) - e))) * gminus;
     if (Re > 0) {
-      A[4] = (-k + (a * u * (1. / e + 1.) / (-(1. / e) + 1.))) / (u * u);
-      A[5] = 1. / (-(1. / e) + 1.) - 1. / (Re);
+      A[4] = (-k + (a * u * (V(1.) / e + V(1.)) / (-(V(1.) / e) + V(1.)))) / (u * u);
+      A[5] = V(1.) / (-(V(1.) / e) + V(1.)) - V(1.) / (Re);
     } else {
-      A[4] = (-k + (a * u * (1. + e) / (-1. + e))) / (u * u);
-      A[5] = e / (-1. + e) - 1. / (Re);
+      A[4] = (-k + (a * u * (V(1.) + e) / (-V(1.) + e))) / (u * u);
+      A[5] = e / (-V(1.) + e) - V(1.) / (Re);
     }
   } else {
-    const Pw U(u), K(k);
-    A[0] = (-(a / k) - (u) / (3. * K[2]) + (U[3]) / (45. * K[4]) - (2 * U[5]) / (945. * K[6]) +
-            -((U[7]) / (4725. * K[8])) - (2 * U[9]) / (93555. * K[10])) * gplus;
-    A[1] = (-(a / k) + (u) / (3. * K[2]) - (U[3]) / (45. * K[4]) + (2 * U[5]) / (945. * K[6]) -
-            -((U[7]) / (4725. * K[8])) + (2 * U[9]) / (93555. * K[10])) * gminus;
-    A[2] = (-(1 / (2. * a)) - u / (2. * k) - (U[2]) / (6. * K[2]) + (U[4]) / (90. * K[4]) -
-            -((U[6]) / (945. * K[6])) + (U[8]) / (9450. * K[8]) - (U[10]) / (93555. * K[10])) * gplus;
-    A[3] = (-(1 / (2. * a)) + u / (2. * k) - (U[2]) / (6. * K[2]) + (U[4]) / (90. * K[4]) -
-            -((U[6]) / (945. * K[6])) + (U[8]) / (9450. * K[8]) - (U[10]) / (93555. * K[10])) * gminus;
-    A[4] = 1. / (3. * k) - (U[2]) / (45. * K[3]) + (2 * U[4]) / (945. * K[5]) - -((U[6]) / (4725. * K[7])) +
-           (2 * U[8]) / (93555. * K[9]) - -((1382 * U[10]) / (6.38512875e8 * K[11]));
-    A[5] = 0.5 + (u) / (6. * k) - (U[3]) / (90. * K[3]) + (U[5]) / (945. * K[5]) - -((U[7]) / (9450. * K[7])) +
-           (U[9]) / (93555. * K[9]);
+    const PwT<V> U(u), K(k);
+    A[0] = (-(a / k) - (u) / (V(3.) * K[2]) + (U[3]) / (V(45.) * K[4]) - (2 * U[5]) / (V(945.) * K[6]) +
+            -((U[7]) / (V(4725.) * K[8])) - (2 * U[9]) / (V(93555.) * K[10])) * gplus;
+    A[1] = (-(a / k) + (u) / (V(3.) * K[2]) - (U[3]) / (V(45.) * K[4]) + (2 * U[5]) / (V(945.) * K[6]) -
+            -((U[7]) / (V(4725.) * K[8])) + (2 * U[9]) / (V(93555.) * K[10])) * gminus;
+    A[2] = (-(1 / (V(2.) * a)) - u / (V(2.) * k) - (U[2]) / (V(6.) * K[2]) + (U[4]) / (V(90.) * K[4]) -
+            -((U[6]) / (V(945.) * K[6])) + (U[8]) / (V(9450.) * K[8]) - (U[10]) / (V(93555.) * K[10])) * gplus;
+    A[3] = (-(1 / (V(2.) * a)) + u / (V(2.) * k) - (U[2]) / (V(6.) * K[2]) + (U[4]) / (V(90.) * K[4]) -
+            -((U[6]) / (V(945.) * K[6])) + (U[8]) / (V(9450.) * K[8]) - (U[10]) / (V(93555.) * K[10])) * gminus;
+    A[4] = V(1.) / (V(3.) * k) - (U[2]) / (V(45.) * K[3]) + (2 * U[4]) / (V(945.) * K[5]) - -((U[6]) / (V(4725.) * K[7])) +
+           (2 * U[8]) / (V(93555.) * K[9]) - -((1382 * U[10]) / (V(6.38512875e8) * K[11]));
+    A[5] = V(0.5) + (u) / (V(6.) * k) - (U[3]) / (V(90.) * K[3]) + (U[5]) / (V(945.) * K[5]) - -((U[7]) / (V(9450.) * K[7])) +
+           (U[9]) / (V(93555.) * K[9]);
   }
 }
 
@@ -734,43 +771,47 @@ __global__ void k_nim_coef_selftest(const double *u, const double *k, double *A,
 
 // contravariant component dd (1..3) of a Cartesian velocity in cell c
 template <class R>
-__device__ __forceinline__ double contravariant(const R *xi, int Nc, int c, int dd, double u, double v, double w) {
+__device__ __forceinline__ Ar<R> contravariant(const R *xi, int Nc, int c, int dd, Ar<R> u, Ar<R> v, Ar<R> w) {
   return u * xi[(dd - 1 + 0) * Nc + c] + v * xi[(dd - 1 + 3) * Nc + c] + w * xi[(dd - 1 + 6) * Nc + c];
 }
 
 // calculate_velocity_nim_constants_formulation2, first pass (nim.f90:165-289)
-__global__ void __launch_bounds__(BLK) k_vel_coef_A(Dims d, Geo g, Fields F, Phys P) {
+template <class R>
+__global__ void __launch_bounds__(BLK) k_vel_coef_A(Dims d, GeoT<R> g, FieldsT<R> F, Phys P) {
+  using V = Ar<R>;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.Nc) return;
   const size_t Nc = d.Nc;
-  const double ut = F.ct[0][c], vt = F.ct[1][c], wt = F.ct[2][c];
+  const V ut = F.ct[0][c], vt = F.ct[1][c], wt = F.ct[2][c];
   for (int dd = 1; dd <= 3; ++dd) {
-    const double u = contravariant(g.xi, Nc, c, dd, ut, vt, wt);
-    double A[6];
-    nim_direction(u, g.gij[(size_t)(dd - 1 + 3 * (dd - 1)) * Nc + c] * P.nu, g.gfd[(2 * (dd - 1)) * Nc + c],
-                  g.gfd[(2 * (dd - 1) + 1) * Nc + c], P.v_limit, A);
+    const V u = contravariant(g.xi, Nc, c, dd, ut, vt, wt);
+    V A[6];
+    nim_direction<V>(u, g.gij[(size_t)(dd - 1 + 3 * (dd - 1)) * Nc + c] * pv<V>(P.nu, P.d_nu),
+                     g.gfd[(2 * (dd - 1)) * Nc + c], g.gfd[(2 * (dd - 1) + 1) * Nc + c], P.v_limit, A);
     for (int k = 0; k < 6; ++k) F.MA[(size_t)(3 * k + dd - 1) * Nc + c] = A[k];
   }
 }
 
 // M_F4 and M_F1..3 from M_A (nim.f90:293-328); also used for the
 // temperature's MT_F (nim.f90:466-500).
-__device__ __forceinline__ void form_F4(const double A[3][6], double DT, double F4[8]) {
-  F4[1] = 0.5 * (1. / A[0][4] + 1. / A[1][4] + 1. / A[2][4] - 1. / DT);
+template <class V>
+__device__ __forceinline__ void form_F4(const V A[3][6], V DT, V F4[8]) {
+  F4[1] = V(0.5) * (V(1.) / A[0][4] + V(1.) / A[1][4] + V(1.) / A[2][4] - V(1.) / DT);
   F4[2] = -(A[0][5] / A[0][4]);
-  F4[3] = (A[0][5] - 1.) / A[0][4];
+  F4[3] = (A[0][5] - V(1.)) / A[0][4];
   F4[4] = -(A[1][5] / A[1][4]);
-  F4[5] = (A[1][5] - 1.) / A[1][4];
+  F4[5] = (A[1][5] - V(1.)) / A[1][4];
   F4[6] = -(A[2][5] / A[2][4]);
-  F4[7] = (A[2][5] - 1.) / A[2][4];
+  F4[7] = (A[2][5] - V(1.)) / A[2][4];
   F4[0] = F4[1] + F4[2] + F4[3] + F4[4] + F4[5] + F4[6] + F4[7];
 }
-__device__ __forceinline__ void form_Fd(const double Ai[6], const double A2[6], double G[5]) {
+template <class V>
+__device__ __forceinline__ void form_Fd(const V Ai[6], const V A2[6], V G[5]) {
   G[1] = Ai[2] - (Ai[0] * Ai[5] / Ai[4]);
   G[2] = A2[3] - A2[1] / A2[4] + A2[1] * A2[5] / A2[4];
-  G[3] = Ai[0] / (2. * Ai[4]);
-  G[4] = A2[1] / (2. * A2[4]);
-  G[0] = G[1] + G[2] + 2. * G[3] + 2. * G[4];
+  G[3] = Ai[0] / (V(2.) * Ai[4]);
+  G[4] = A2[1] / (V(2.) * A2[4]);
+  G[0] = G[1] + G[2] + V(2.) * G[3] + V(2.) * G[4];
 }
 
 // form_Fd and form_F4 with slot 4 holding 1/A4 (the float MT_A of the FP32
@@ -795,22 +836,24 @@ __device__ __forceinline__ void form_F4_rcp(const V A[3][6], V DT, V F4[8]) {
   F4[0] = F4[1] + F4[2] + F4[3] + F4[4] + F4[5] + F4[6] + F4[7];
 }
 
-__global__ void __launch_bounds__(BLK) k_vel_coef_F(Dims d, Fields F, Phys P) {
+template <class R>
+__global__ void __launch_bounds__(BLK) k_vel_coef_F(Dims d, FieldsT<R> F, Phys P) {
+  using V = Ar<R>;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.Nc) return;
   const Cell x = Cell::of(d, c);
   const size_t Nc = d.Nc;
-  double A[3][6];
+  V A[3][6];
   for (int dd = 0; dd < 3; ++dd)
     for (int k = 0; k < 6; ++k) A[dd][k] = F.MA[(size_t)(3 * k + dd) * Nc + c];
-  double F4[8];
-  form_F4(A, P.DT, F4);
+  V F4[8];
+  form_F4<V>(A, P.DT, F4);
   for (int k = 0; k < 8; ++k) F.MF4[(size_t)k * Nc + c] = F4[k];
   for (int dd = 1; dd <= 3; ++dd) {
-    double G[5] = {0., 0., 0., 0., 0.};
+    V G[5] = {0., 0., 0., 0., 0.};
     if (x.has_nb(d, 2 * dd)) {
       const int i2 = x.nb(d, 2 * dd).c;
-      double A2[6];
+      V A2[6];
       for (int k = 0; k < 6; ++k) A2[k] = F.MA[(size_t)(3 * k + dd - 1) * Nc + i2];
       form_Fd(A[dd - 1], A2, G);
     }
@@ -1008,20 +1051,6 @@ __global__ void __launch_bounds__(BLK) k_vel1_coef_F(Dims d, Geo g, Fields F, Ph
 // Load policies: the parallel kernels read with plain (L1-cached) loads; the
 // reference-order sweeps read data that other SMs rewrote one level earlier
 // (LdCoh below).
-// Arithmetic type of a kernel over storage type R: double for the FP64
-// path, float for the float mirror of the FP32 phase (whose kernels compute
-// in float, with only the change maxima and reductions in double).
-template <class R>
-struct ArithOf {
-  using type = double;
-};
-template <>
-struct ArithOf<float> {
-  using type = float;
-};
-template <class R>
-using Ar = typename ArithOf<R>::type;
-
 struct LdPlain {
   template <class T>
   __device__ __forceinline__ static Ar<T> ld(const T *p, size_t i) { return p[i]; }
@@ -1226,6 +1255,9 @@ __global__ void k_wait_selftest(Ctrl *ctl, int tries) {
 // nim_exp over n arguments (self-test of the exp the NIM coefficients use)
 
 __device__ __forceinline__ double errv(double nw, double old, bool first) { return fabs(nw - (first ? 0.0 : old)); }
+__device__ __forceinline__ double errv(const DualD &nw, const DualD &old, bool first) {
+  return errv(nw.v, old.v, first);
+}
 // max that keeps a NaN (fmax would drop it and hide a blow-up)
 __device__ __forceinline__ double nmax(double a, double b) { return (b > a || b != b) ? b : a; }
 
@@ -1275,7 +1307,7 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, GeoT<R> g, FieldsT<
     const V base = (q == 2) ? -(V(P.g_beta) * V(0.5) * (F.c[3][c] + F.co[3][c])) : V(0.);
     const V RB = base + V(P.inv_rho) * green_gauss(g, NF, invV, pf, f, q);
     const R *fr = F.f[q] + par * NF;
-    const V RD = V(P.inv_Re) * diffusion_source(d, g, fr, x, f);
+    const V RD = pv<V>(P.inv_Re, P.d_inv_Re) * diffusion_source(d, g, fr, x, f);
     const V B = (V(0.) + RD + RB);
     if (SRC_ONLY || FORM == 1) F.Bv[(size_t)q * Nc + c] = B;
     if (!SRC_ONLY) {
@@ -1502,7 +1534,7 @@ __global__ void __launch_bounds__(CB3, minb<R>(VC2_MINB, VC2_MINB_F)) k_vel_cell
       term(5, V(0.5) * (((V)o1[6] - z1_m1) / V(4.) - ((V)o1[5] - z_m1) / V(4.)),
            V(0.5) * ((z1_p2 - (V)o0[6]) / V(4.) - (z_p2 - (V)o0[5]) / V(4.)));
     }
-    const V RD0 = V(P.inv_Re) * s0, RD1 = V(P.inv_Re) * s1;
+    const V RD0 = pv<V>(P.inv_Re, P.d_inv_Re) * s0, RD1 = pv<V>(P.inv_Re, P.d_inv_Re) * s1;
     const V B0 = (V(0.) + RD0 + RB0), B1 = (V(0.) + RD1 + RB1);
     // cell update (cell_update), term by term
     R cv0, cv1, co0, co1, a0, a1;
@@ -1780,7 +1812,7 @@ __global__ void __launch_bounds__(CB3, VCN_MINB) k_vel_cellN(Dims d, GeoT<R> g, 
     R out[NP];
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
-      const V B = (V(0.) + V(P.inv_Re) * s[p] + RB[p]);
+      const V B = (V(0.) + pv<V>(P.inv_Re, P.d_inv_Re) * s[p] + RB[p]);
       const V nw = stored<R>((1 - w) * (V)cv[p] + (w / F40[p]) * (u[p] + B));
       out[p] = (R)nw;
       e[q] = nmax(e[q], errv(nw, cv[p], first));
@@ -2284,7 +2316,7 @@ __global__ void __launch_bounds__(3 * CT_T, CT_MINB)
       const V pz = (fr[6] - fr[5]) / V(2.);
       const R *G = g.G, *gij = g.gij;
       const V RD =
-          V(P.inv_Re) * (G[c] * px + G[Nc + c] * py + G[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy -
+          pv<V>(P.inv_Re, P.d_inv_Re) * (G[c] * px + G[Nc + c] * py + G[2 * Nc + c] * pz - gij[3 * Nc + c] * pxy -
                       gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz - gij[2 * Nc + c] * pzx - gij[7 * Nc + c] * pyz -
                       gij[5 * Nc + c] * pzy);
       const V B = (V(0.) + RD + RB);
@@ -2418,7 +2450,7 @@ __device__ __forceinline__ Ar<R> p_bc_value(const Dims &d, const GeoT<R> &g, con
   }
   const V w = V(P.w_p2);
   return (1 - w) * Ld::ld(pr, fw0) +
-         w / (ap[(pos - 1) * NB + b]) * (s + B1 - B2 - B3 + (V(P.nu) * V(P.rho) * d2udn2 - b_n * V(P.rho)));
+         w / (ap[(pos - 1) * NB + b]) * (s + B1 - B2 - B3 + (pv<V>(P.nu, P.d_nu) * V(P.rho) * d2udn2 - b_n * V(P.rho)));
 }
 
 // ---- K4: apply_pressure_bc, every wall face from the values before the pass
@@ -2605,11 +2637,12 @@ __global__ void __launch_bounds__(BLK) k_p_dpdx(Dims d, GeoT<R> g, FieldsT<R> F,
     int f[7];
     cell_faces(d, x, f);
     const R *p = F.f[3] + newhalf(ctl) * NF;
-    const double v[3] = {stored<R>((p[f[2]] - p[f[1]]) / 2. * g.xi[0 * Nc + c]),
-                         stored<R>((p[f[4]] - p[f[3]]) / 2. * g.xi[4 * Nc + c]),
-                         stored<R>((p[f[6]] - p[f[5]]) / 2. * g.xi[8 * Nc + c])};
+    using V = Ar<R>;
+    const V v[3] = {stored<R>((p[f[2]] - p[f[1]]) / V(2.) * g.xi[0 * Nc + c]),
+                    stored<R>((p[f[4]] - p[f[3]]) / V(2.) * g.xi[4 * Nc + c]),
+                    stored<R>((p[f[6]] - p[f[5]]) / V(2.) * g.xi[8 * Nc + c])};
     for (int q = 0; q < 3; ++q) {
-      if (d.owns(x.k)) e[0] = nmax(e[0], fabs(v[q] - F.dpd[q * Nc + c]));
+      if (d.owns(x.k)) e[0] = nmax(e[0], fabs(val(v[q]) - val(F.dpd[q * Nc + c])));
       F.dpd[q * Nc + c] = v[q];
     }
   }
@@ -2668,13 +2701,14 @@ __global__ void __launch_bounds__(BLK, 4) k_T_coef(Dims d, GeoT<R> g, FieldsT<R>
     A[4] = 1.f / A[4];  // k_T_cell, the one reader, only divides by A4 (A4 = 4h/k > 0)
     for (int q = 0; q < 6; ++q) F.MTA[(3 * q + dd - 1) * Nc + c] = A[q];
   } else {
-    const double ut = 0.5 * (F.c[0][c] + F.co[0][c]);
-    const double vt = 0.5 * (F.c[1][c] + F.co[1][c]);
-    const double wt = 0.5 * (F.c[2][c] + F.co[2][c]);
-    const double u = contravariant(g.xi, Nc, c, dd, ut, vt, wt);
-    double A[6];
-    nim_direction(u, g.gij[(dd - 1 + 3 * (dd - 1)) * Nc + c] * P.alpha, g.gfd[(2 * (dd - 1)) * Nc + c],
-                  g.gfd[(2 * (dd - 1) + 1) * Nc + c], P.v_limit, A);
+    using V = Ar<R>;
+    const V ut = V(0.5) * (F.c[0][c] + F.co[0][c]);
+    const V vt = V(0.5) * (F.c[1][c] + F.co[1][c]);
+    const V wt = V(0.5) * (F.c[2][c] + F.co[2][c]);
+    const V u = contravariant(g.xi, Nc, c, dd, ut, vt, wt);
+    V A[6];
+    nim_direction<V>(u, g.gij[(dd - 1 + 3 * (dd - 1)) * Nc + c] * pv<V>(P.alpha, P.d_alpha),
+                     g.gfd[(2 * (dd - 1)) * Nc + c], g.gfd[(2 * (dd - 1) + 1) * Nc + c], P.v_limit, A);
     for (int q = 0; q < 6; ++q) F.MTA[(3 * q + dd - 1) * Nc + c] = A[q];
   }
 }
@@ -2758,7 +2792,7 @@ __global__ void __launch_bounds__(CB3, minb<R>(5, TCELL_MINB_F)) k_T_cell(Dims d
     const V pxy = sX[0][0][tx], pzy = sX[0][1][tx], pyx = sX[1][0][tx], pzx = sX[1][1][tx];
     const V pxz = sX[2][0][tx], pyz = sX[2][1][tx];
     const R *gij = g.gij;
-    const V RDT = V(P.alpha) * (sG[tx] - gij[3 * Nc + c] * pxy - gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz -
+    const V RDT = pv<V>(P.alpha, P.d_alpha) * (sG[tx] - gij[3 * Nc + c] * pxy - gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz -
                                   gij[2 * Nc + c] * pzx - gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
     if (SRC_ONLY) {
       for (int k = 0; k < 8; ++k) F.MTF4[(size_t)k * Nc + c] = F4[k];
@@ -3090,7 +3124,12 @@ __global__ void __launch_bounds__(BLK) k_seq_pbc(Dims d, Geo g, Fields F, Phys P
 
 // ====================================================== end of integrate
 // check_steady_state (nse.f90:1316-1332) + evaluate_D (nse.f90:2504-2537)
-__global__ void __launch_bounds__(BLK) k_after_integrate(Dims d, Geo g, Fields F, Phys P, Ctrl *ctl, int nblk) {
+// (the dual instantiation: the maxima and the sum of squares of the values;
+// meshes_dila with its derivative)
+template <class R>
+__global__ void __launch_bounds__(BLK) k_after_integrate(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl,
+                                                         int nblk) {
+  using V = Ar<R>;
   __shared__ BlockRed red;
   red_init<2>(red);
   const int par = parity(ctl);
@@ -3101,22 +3140,22 @@ __global__ void __launch_bounds__(BLK) k_after_integrate(Dims d, Geo g, Fields F
     const size_t NF = d.NF;
     const double tdt = 2 * P.DT;
     double mu = 0.;
-    for (int q = 0; q < 3; ++q) mu = nmax(mu, fabs(F.c[q][c] - F.co[q][c]) / tdt);
+    for (int q = 0; q < 3; ++q) mu = nmax(mu, fabs(val(F.c[q][c]) - val(F.co[q][c])) / tdt);
     m[0] = mu;
-    m[1] = fabs(F.c[3][c] - F.co[3][c]) / tdt;
+    m[1] = fabs(val(F.c[3][c]) - val(F.co[3][c])) / tdt;
     int f[7];
     cell_faces(d, x, f);
-    double uf[7], vf[7], wf[7];
+    V uf[7], vf[7], wf[7];
     for (int k = 1; k <= 6; ++k) {
       uf[k] = F.f[0][par * NF + f[k]];
       vf[k] = F.f[1][par * NF + f[k]];
       wf[k] = F.f[2][par * NF + f[k]];
     }
-    const double invV = 1. / g.vol[c];
-    const double Dila = green_gauss(g, NF, invV, uf, f, 0) + green_gauss(g, NF, invV, vf, f, 1) +
-                        green_gauss(g, NF, invV, wf, f, 2);
+    const V invV = V(1.) / g.vol[c];
+    const V Dila = green_gauss(g, NF, invV, uf, f, 0) + green_gauss(g, NF, invV, vf, f, 1) +
+                   green_gauss(g, NF, invV, wf, f, 2);
     F.dila[c] = Dila;
-    s[0] = Dila * Dila;
+    s[0] = val(Dila) * val(Dila);
     if (!d.owns(x.k)) m[0] = m[1] = s[0] = 0.;
   }
   block_max<2>(red, m, ctl->red);
@@ -3141,28 +3180,34 @@ __global__ void k_finish_sum(const double *part, int nblk, int nsum, double *out
 }
 
 // update_time_step (nse.f90:1292-1313)
-__global__ void __launch_bounds__(BLK) k_update_time(Dims d, Fields F, Ctrl *ctl) {
+template <class R>
+__global__ void __launch_bounds__(BLK) k_update_time(Dims d, FieldsT<R> F, Ctrl *ctl) {
+  using V = Ar<R>;
   const int par = parity(ctl);
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.Nc) return;
   const Cell x = Cell::of(d, c);
   for (int q = 0; q < 4; ++q) {
-    F.ct[q][c] = (F.co[q][c] + F.c[q][c]) / 2.;
+    F.ct[q][c] = (F.co[q][c] + F.c[q][c]) / V(2.);
     F.co[q][c] = F.c[q][c];
   }
   int f[7];
   cell_faces(d, x, f);
-  const double *p = F.f[3] + par * (size_t)d.NF;
-  F.mp[c] = (p[f[1]] + p[f[2]] + p[f[3]] + p[f[4]] + p[f[5]] + p[f[6]]) / 6.0;
+  const R *p = F.f[3] + par * (size_t)d.NF;
+  F.mp[c] = (p[f[1]] + p[f[2]] + p[f[3]] + p[f[4]] + p[f[5]] + p[f[6]]) / V(6.0);
   F.dila_old[c] = F.dila[c];
 }
 
 // find_Nu2 (nse.f90:2699-2798): wall-normal one-sided dT/dn on the inner
 // (position 1) and outer (position 2) walls, area weighted.
-__global__ void __launch_bounds__(BLK) k_nusselt(Dims d, Geo g, Fields F, Ctrl *ctl, int nblk) {
+// (the dual instantiation sums the four values, then their derivatives:
+// eight partial sums)
+template <class R>
+__global__ void __launch_bounds__(BLK) k_nusselt(Dims d, GeoT<R> g, FieldsT<R> F, Ctrl *ctl, int nblk) {
+  using V = Ar<R>;
   const int par = parity(ctl);
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  double s[4] = {0., 0., 0., 0.};  // sum1, sumA1 (outer), sum2, sumA2 (inner)
+  V s[4] = {0., 0., 0., 0.};  // sum1, sumA1 (outer), sum2, sumA2 (inner)
   const int nr = 2 * d.NT * d.NZ;
   if (q < nr) {
     const int b = 2 * d.plane + q;
@@ -3170,13 +3215,13 @@ __global__ void __launch_bounds__(BLK) k_nusselt(Dims d, Geo g, Fields F, Ctrl *
     const BFace B = bface(d, b);
     const int in = (B.pos == 1) ? 2 : 1;
     const Cell c2 = B.cell.nb(d, in), c3 = c2.nb(d, in);
-    const double *T = F.f[4] + par * NF;
-    const double *w = g.nuw;
+    const R *T = F.f[4] + par * NF;
+    const R *w = g.nuw;
     const int f1 = B.cell.face(d, B.pos);
-    const double inner = -((w[b]) * T[f1]) + w[NB + b] * T[B.cell.face(d, in)] - w[2 * NB + b] * T[c2.face(d, in)] +
-                         w[3 * NB + b] * T[c3.face(d, in)];
-    const double dTdx = (B.pos == 1) ? -(inner) : inner;
-    const double A = g.area[f1];
+    const V inner = -((w[b]) * T[f1]) + w[NB + b] * T[B.cell.face(d, in)] - w[2 * NB + b] * T[c2.face(d, in)] +
+                    w[3 * NB + b] * T[c3.face(d, in)];
+    const V dTdx = (B.pos == 1) ? -(inner) : inner;
+    const V A = g.area[f1];
     if (B.pos == 1) {
       s[2] = A * dTdx;
       s[3] = A;
@@ -3186,7 +3231,12 @@ __global__ void __launch_bounds__(BLK) k_nusselt(Dims d, Geo g, Fields F, Ctrl *
     }
     if (!d.owns(B.cell.k)) s[0] = s[1] = s[2] = s[3] = 0.;
   }
-  block_sum<4>(s, F.part, nblk);
+  if constexpr (std::is_same<V, DualD>::value) {
+    const double sv[8] = {s[0].v, s[1].v, s[2].v, s[3].v, s[0].t, s[1].t, s[2].t, s[3].t};
+    block_sum<8>(sv, F.part, nblk);
+  } else {
+    block_sum<4>(s, F.part, nblk);
+  }
 }
 
 // max |value| of the Dirichlet walls per field (u, v, w, -, T): find_error

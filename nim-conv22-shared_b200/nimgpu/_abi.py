@@ -156,6 +156,16 @@ def gpu_lib() -> C.CDLL:
         lib.nim_gpu_step.restype = C.c_int
         lib.nim_gpu_download.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.c_int64]
         lib.nim_gpu_download.restype = C.c_int
+        lib.nim_gpu_tangent_begin.argtypes = [vp]
+        lib.nim_gpu_tangent_begin.restype = C.c_int
+        lib.nim_gpu_tangent_seed.argtypes = [vp, C.c_double, C.c_double]
+        lib.nim_gpu_tangent_seed.restype = C.c_int
+        lib.nim_gpu_tangent_seed_field.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.c_int64]
+        lib.nim_gpu_tangent_seed_field.restype = C.c_int
+        lib.nim_gpu_tangent_step.argtypes = [vp, C.c_int32, C.POINTER(StepStats), C.POINTER(C.c_double)]
+        lib.nim_gpu_tangent_step.restype = C.c_int
+        lib.nim_gpu_tangent_get.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64]
+        lib.nim_gpu_tangent_get.restype = C.c_int
         lib.nim_gpu_upload.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.c_int64]
         lib.nim_gpu_upload.restype = C.c_int
         lib.nim_gpu_set_graph_iters.argtypes = [vp, C.c_int32]

@@ -174,6 +174,48 @@ class NimSolver:
     def get(self, field: int, n: int | None = None) -> np.ndarray:
         return self.download(field)
 
+    # -- tangent-linear steps (forward-mode derivatives of the time advance)
+    def tangent_begin(self):
+        """Dual copy of the current state, zero derivatives and seeds."""
+        _abi.check(self.lib.nim_gpu_tangent_begin(self._h), "nim_gpu_tangent_begin")
+
+    def tangent_seed(self, dnu: float, dalpha: float):
+        _abi.check(self.lib.nim_gpu_tangent_seed(self._h, dnu, dalpha), "nim_gpu_tangent_seed")
+
+    @staticmethod
+    def tangent_seed_of(name: str, Ra: float, Pr: float):
+        """(d nu, d alpha) of d/dRa or d/dPr: nu = sqrt(Pr / Ra), alpha =
+        nu / Pr (parameters.f90:169-173 with g_beta = th_tc = 1)."""
+        nu = (Pr / Ra) ** 0.5
+        alpha = nu / Pr
+        if name == "Ra":
+            return -nu / (2 * Ra), -alpha / (2 * Ra)
+        if name == "Pr":
+            return nu / (2 * Pr), -alpha / (2 * Pr)
+        raise ValueError(name)
+
+    def tangent_seed_field(self, field: int, tangent: np.ndarray):
+        a = np.ascontiguousarray(tangent, dtype=np.float64)
+        _abi.check(self.lib.nim_gpu_tangent_seed_field(self._h, field, a.ctypes.data_as(C.POINTER(C.c_double)),
+                                                       a.size), "nim_gpu_tangent_seed_field")
+
+    def tangent_step(self, nsteps: int):
+        """nsteps dual steps: (per-step statistics of the values, array
+        (nsteps, 2) of d Nu_inner, d Nu_outer)."""
+        arr = (_abi.StepStats * max(nsteps, 1))()
+        dnu = np.zeros((max(nsteps, 1), 2), dtype=np.float64)
+        st = self.lib.nim_gpu_tangent_step(self._h, nsteps, arr, dnu.ctypes.data_as(C.POINTER(C.c_double)))
+        _abi.check(st, "nim_gpu_tangent_step")
+        return [arr[i] for i in range(nsteps)], dnu[:nsteps]
+
+    def tangent_get(self, field: int):
+        """(value, derivative) of a state field of the dual state."""
+        n = field_len(field, self.mesh)
+        v, t = np.empty(n), np.empty(n)
+        _abi.check(self.lib.nim_gpu_tangent_get(self._h, field, v.ctypes.data_as(C.POINTER(C.c_double)),
+                                                t.ctypes.data_as(C.POINTER(C.c_double)), n), "nim_gpu_tangent_get")
+        return v, t
+
     def set(self, field: int, values: np.ndarray):
         self.upload(field, values)
 
