@@ -37,6 +37,10 @@ It also carries "slabs": the same steps from the same start with the mesh
 split into two z-slabs on the one device (nim_slab_step: halo exchange after
 each part of every pass), their throughput against the whole mesh and
 whether iterations and final fields match the whole-mesh run exactly.
+
+--tangent adds "tangent": the same steps on the tangent-linear path
+(nim_gpu_tangent_*, d/dRa seeded), its throughput against the FP64 run,
+whether its values repeat that run's, and d Nu_hot / dRa per step.
 """
 from __future__ import annotations
 
@@ -539,6 +543,45 @@ def run_mixed(case, mesh, args, fp64_stats, fp64_fields, fp64_value, fp64_ms_ste
     }
 
 
+def run_tangent(case, mesh, args, fp64_stats, fp64_value, fp64_ms_step):
+    """The FP64 run's steps again, from the same start, on the tangent-linear
+    path seeded with d/dRa (nim_gpu_tangent_*): device-timed throughput of
+    the same K steps, whether its values repeat the FP64 run's (iteration
+    counts and Nusselt numbers), and d Nu_inner / dRa per step."""
+    import torch
+    import nimgpu
+    s = nimgpu.NimSolver(mesh, case.params(**stop_over(args)))
+    s.initialize_nse()
+    s.add_temperature_noise(case.noise, case.seed)
+    s.tangent_begin()
+    s.tangent_seed(*nimgpu.NimSolver.tangent_seed_of("Ra", case.Ra, case.Pr))
+    stream = torch.cuda.ExternalStream(s.stream_handle)
+    recs, dnus = [], []
+    if args.warmup > 0:
+        r, d = s.tangent_step(args.warmup)
+        recs += r
+        dnus += list(d[:, 0])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    r, d = s.tangent_step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    recs += r
+    dnus += list(d[:, 0])
+    iters = sum(x.iters for x in r)
+    value = case.ncells * iters / (ms / 1e3)
+    s.close()
+    same = [(a.iters, a.nu_inner) for a in recs] == [(b.iters, b.nu_inner) for b in fp64_stats[:len(recs)]]
+    return {
+        "value": value, "unit": UNIT, "ms_per_step": ms / max(args.steps, 1), "iterations": iters,
+        "vs_fp64": value / fp64_value, "step_time_vs_fp64": fp64_ms_step / (ms / max(args.steps, 1)),
+        "dtype": "dual f64 (value and derivative)", "seed": "d/dRa",
+        "values_equal_fp64_run": same, "dnu_inner_dRa_per_step": [float(x) for x in dnus],
+    }
+
+
 def run_slabs(case, mesh, args, fp64_stats, fp64_fields, fp64_value, nslab=2):
     """The FP64 run's steps again, from the same start, as nslab z-slabs of
     the mesh on this device; wall clock around the synchronous group step
@@ -586,6 +629,8 @@ def main():
                     help="stop every inner loop when each field's change is below this (FP64, pressure by its "
                          "gradients) instead of the reference's tolerances")
     ap.add_argument("--no-slabs", action="store_true", help="skip the two-slab comparison")
+    ap.add_argument("--tangent", action="store_true",
+                    help="also run the same steps on the tangent-linear path (d/dRa seeded)")
     ap.add_argument("--replicas", action="store_true",
                     help="N > 1: every rank advances its own copy of --case (no decomposition)")
     ap.add_argument("--decompose", action="store_true",
@@ -697,6 +742,10 @@ def main():
         mixed = run_mixed(case, mesh, args, warm_stats + list(stats), fp64_fields, value, ms / max(args.steps, 1),
                           peak, peak_kind)
 
+    tangent = None
+    if args.tangent and world == 1 and prec == _abi.PRECISION_FP64 and sched == _abi.SCHEDULE_PARALLEL:
+        tangent = run_tangent(case, mesh, args, warm_stats + list(stats), value, ms / max(args.steps, 1))
+
     slabs = None
     if want_slabs:
         try:
@@ -740,6 +789,7 @@ def main():
         "iters_fp32": sum(s.iters_fp32 for s in stats),
         "mixed": mixed,
         "slabs": slabs,
+        "tangent": tangent,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
