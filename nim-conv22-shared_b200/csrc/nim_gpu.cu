@@ -407,8 +407,19 @@ template <class R>
 int launch_pressure(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F) {
   const Dims &d = x->d;
   const dim3 g3 = x->g3;
-  k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
-  TRY(mark(x, "k_p_src"));
+  bool quad = false;
+  if constexpr (std::is_same<R, float>::value) {
+    if (x->cell_quad) {  // the float mirror, four cells a thread
+      const dim3 gq((d.NT + 127) / 128, (d.NR + 3) / 4, d.NZ);
+      k_p_srcN<R, 4><<<gq, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+      TRY(mark(x, "k_p_srcN"));
+      quad = true;
+    }
+  }
+  if (!quad) {
+    k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+    TRY(mark(x, "k_p_src"));
+  }
   k_p_bc<<<x->nblk_b, BLK, 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_p_bc"));
   k_p_bc_copy<<<x->nblk_b, BLK, 0, s>>>(d, F, x->ctl);

@@ -173,6 +173,7 @@ constexpr int VC2_MINB = 3;  // resident blocks per SM asked of k_vel_cell2 (56 
 // for: computing in float they need about half the FP64 registers
 constexpr int VC2_MINB_F = 3, PSRC_MINB_F = 4, PFACE_MINB_F = 5, TCELL_MINB_F = 5, TFACE_MINB_F = 4;
 constexpr int VCN_MINB = 2;  // k_vel_cellN (four float cells a thread)
+constexpr int PSN_MINB = 2;  // k_p_srcN (four float cells a thread)
 template <class R>
 constexpr int minb(int fp64, int fp32) {
   return sizeof(R) == 8 ? fp64 : fp32;
@@ -2408,6 +2409,217 @@ __global__ void __launch_bounds__(CB3, minb<R>(4, PSRC_MINB_F)) k_p_src(Dims d, 
                                     gij[1 * Nc + c] * pyx - gij[6 * Nc + c] * pxz - gij[2 * Nc + c] * pzx -
                                     gij[7 * Nc + c] * pyz - gij[5 * Nc + c] * pzy);
     F.Rp[c] = RDp + RBp;
+  }
+}
+
+// ---- K3, NP cells per thread (the float mirror, n_theta % NP == 0):
+// k_p_src over NP theta-adjacent cells, every value the cells share a row
+// for in one NP-wide vector load (as k_vel_cellN).  Thread y forms the
+// gradients of velocity component y (y = 1 also d(bz)/dz) and two of the six
+// cross derivatives of p for the NP cells; thread 0 combines them in the
+// reference's order.  Each cell's arithmetic is k_p_src's.
+template <class R, int NP>
+__global__ void __launch_bounds__(CB3, PSN_MINB) k_p_srcN(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  using V = Ar<R>;
+  if (ctl->done) return;
+  __shared__ V sh[3][3][CB * NP];  // gradients of u, v, w
+  __shared__ V sX[3][2][CB * NP];  // cross derivatives of p
+  __shared__ V sbz[CB * NP];
+  const int par = parity(ctl);
+  const int tx = threadIdx.x;
+  const int i = blockIdx.x * (32 * NP) + NP * (tx & 31);
+  const int j = blockIdx.y * (CB / 32) + (tx >> 5);
+  const int k = blockIdx.z;
+  const bool active = i < d.NT && j < d.NR;
+  const int Nc = d.Nc, NF = d.NF, NT = d.NT, NR = d.NR, pl = d.plane;
+  const int c = i + NT * (j + NR * k);
+  const int im1 = (i == 0) ? NT - 1 : i - 1, ipn = (i + NP >= NT) ? i + NP - NT : i + NP;
+  const int f1 = c + NT * k;
+  const int fi[7] = {0, f1, f1 + NT, d.offT + c, d.offT + c + 1, d.offZ + c, d.offZ + c + pl};
+  const int f4b = d.offT + c - i + ipn;
+  auto faceN = [&](const R *a, int m, R (&v)[NP]) {
+    if (m == 4) {
+      R t[NP];
+      ldN<R, NP>(a, fi[3], t);
+#pragma unroll
+      for (int p = 0; p + 1 < NP; ++p) v[p] = t[p + 1];
+      v[NP - 1] = a[f4b];
+    } else {
+      ldN<R, NP>(a, fi[m], v);
+    }
+  };
+  const R *fp = F.f[3] + par * NF;
+  auto along = [&](bool lo, bool hi, V v0, V va, V vb) {
+    return lo ? tang_vals(true, false, v0, va, vb, V(0.), V(0.))
+              : hi ? tang_vals(false, true, v0, V(0.), V(0.), va, vb) : tang_vals(false, false, v0, vb, V(0.), va, V(0.));
+  };
+  if (active) by_dir(threadIdx.y, [&](auto Q) {
+    constexpr int q = decltype(Q)::value - 1;
+    R vol[NP];
+    ldN<R, NP>(g.vol, c, vol);
+    V invV[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) invV[p] = V(1.) / vol[p];
+    // green_gauss (terms of faces 2, 1, 4, 3, 6, 5, then the volume factor)
+    auto gauss = [&](const R (&phi)[7][NP], int cc, V (&out)[NP]) {
+      const R *nc = g.normal + (size_t)cc * NF;
+      const int order[6] = {2, 1, 4, 3, 6, 5};
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        const int m = order[t];
+        R a[NP], n[NP];
+        faceN(g.area, m, a);
+        faceN(nc, m, n);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          const V tp = (V)phi[m][p] * a[p] * (n[p]);
+          out[p] = (t == 0) ? tp : (t & 1) ? out[p] - tp : out[p] + tp;
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) out[p] = invV[p] * out[p];
+    };
+    {
+      const R *fq = F.f[q] + newhalf(ctl) * NF;
+      R vf[7][NP];
+#pragma unroll
+      for (int m = 1; m <= 6; ++m) faceN(fq, m, vf[m]);
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        V gg[NP];
+        gauss(vf, cc, gg);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) sh[q][cc][tx * NP + p] = gg[p];
+      }
+    }
+    if (q == 1) {
+      const R *fT = F.f[4] + par * NF;
+      R bzf[7][NP];
+#pragma unroll
+      for (int m = 1; m <= 6; ++m) {
+        R t[NP];
+        faceN(fT, m, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) bzf[m][p] = -(pv<V>(P.g_beta, 0.) * (t[p]));
+      }
+      V gz[NP];
+      gauss(bzf, 2, gz);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) sbz[tx * NP + p] = gz[p];
+    }
+    // p's faces of the NP cells
+    R o[7][NP];
+#pragma unroll
+    for (int m = 1; m <= 6; ++m) faceN(fp, m, o[m]);
+    const bool rlo = (j == 0), rhi = (j == NR - 1);
+    const int ra = rlo ? j + 1 : j - 1, rb = rlo ? j + 2 : (rhi ? j - 2 : j + 1);
+    const bool zlo = (k == 0), zhi = (k == d.NZ - 1);
+    const int ka = zlo ? k + 1 : k - 1, kb = zlo ? k + 2 : (zhi ? k - 2 : k + 1);
+    if (q == 0) {  // pxy (r faces along theta), pzy (z faces along theta)
+      const int rrow = NT * (j + (NR + 1) * k), zlev = d.offZ + NT * (j + NR * k);
+      const V r_m1 = fp[rrow + im1], r_pn = fp[rrow + ipn], r1_m1 = fp[rrow + NT + im1], r1_pn = fp[rrow + NT + ipn];
+      const V z_m1 = fp[zlev + im1], z_pn = fp[zlev + ipn], z1_m1 = fp[zlev + pl + im1], z1_pn = fp[zlev + pl + ipn];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const V up2 = (p + 1 < NP) ? (V)o[2][p + 1] : r1_pn, um2 = (p > 0) ? (V)o[2][p - 1] : r1_m1;
+        const V up1 = (p + 1 < NP) ? (V)o[1][p + 1] : r_pn, um1 = (p > 0) ? (V)o[1][p - 1] : r_m1;
+        sX[0][0][tx * NP + p] = V(0.5) * ((up2 - um2) / V(4.) - (up1 - um1) / V(4.));
+        const V up6 = (p + 1 < NP) ? (V)o[6][p + 1] : z1_pn, um6 = (p > 0) ? (V)o[6][p - 1] : z1_m1;
+        const V up5 = (p + 1 < NP) ? (V)o[5][p + 1] : z_pn, um5 = (p > 0) ? (V)o[5][p - 1] : z_m1;
+        sX[0][1][tx * NP + p] = V(0.5) * ((up6 - um6) / V(4.) - (up5 - um5) / V(4.));
+      }
+    } else if (q == 1) {  // pyx (theta faces along r), pzx (z faces along r)
+      const int tra = d.offT + NT * (ra + NR * k), trb = d.offT + NT * (rb + NR * k);
+      const int zra = d.offZ + NT * (ra + NR * k), zrb = d.offZ + NT * (rb + NR * k);
+      R av[NP + 1], bv[NP + 1];
+      {
+        R t[NP];
+        ldN<R, NP>(fp, tra + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) av[p] = t[p];
+        ldN<R, NP>(fp, trb + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) bv[p] = t[p];
+        av[NP] = fp[tra + ipn];
+        bv[NP] = fp[trb + ipn];
+      }
+      R za[NP], zb[NP], zA[NP], zB[NP];
+      ldN<R, NP>(fp, zra + i, za);
+      ldN<R, NP>(fp, zrb + i, zb);
+      ldN<R, NP>(fp, zra + pl + i, zA);
+      ldN<R, NP>(fp, zrb + pl + i, zB);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        sX[1][0][tx * NP + p] =
+            V(0.5) * (along(rlo, rhi, o[4][p], av[p + 1], bv[p + 1]) - along(rlo, rhi, o[3][p], av[p], bv[p]));
+        sX[1][1][tx * NP + p] =
+            V(0.5) * (along(rlo, rhi, o[6][p], zA[p], zB[p]) - along(rlo, rhi, o[5][p], za[p], zb[p]));
+      }
+    } else {  // pxz (r faces along z), pyz (theta faces along z)
+      const int rka = NT * (j + (NR + 1) * ka), rkb = NT * (j + (NR + 1) * kb);
+      const int tka = d.offT + NT * (j + NR * ka), tkb = d.offT + NT * (j + NR * kb);
+      R pa[NP], pb[NP], pA[NP], pB[NP];
+      ldN<R, NP>(fp, rka + i, pa);
+      ldN<R, NP>(fp, rkb + i, pb);
+      ldN<R, NP>(fp, rka + NT + i, pA);
+      ldN<R, NP>(fp, rkb + NT + i, pB);
+      R av[NP + 1], bv[NP + 1];
+      {
+        R t[NP];
+        ldN<R, NP>(fp, tka + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) av[p] = t[p];
+        ldN<R, NP>(fp, tkb + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) bv[p] = t[p];
+        av[NP] = fp[tka + ipn];
+        bv[NP] = fp[tkb + ipn];
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        sX[2][0][tx * NP + p] =
+            V(0.5) * (along(zlo, zhi, o[2][p], pA[p], pB[p]) - along(zlo, zhi, o[1][p], pa[p], pb[p]));
+        sX[2][1][tx * NP + p] =
+            V(0.5) * (along(zlo, zhi, o[4][p], av[p + 1], bv[p + 1]) - along(zlo, zhi, o[3][p], av[p], bv[p]));
+      }
+    }
+  });
+  __syncthreads();
+  if (active && threadIdx.y == 0) {
+    R o[7][NP];
+#pragma unroll
+    for (int m = 1; m <= 6; ++m) faceN(fp, m, o[m]);
+    R G0[NP], G1[NP], G2[NP];
+    ldN<R, NP>(g.G, c, G0);
+    ldN<R, NP>(g.G + Nc, c, G1);
+    ldN<R, NP>(g.G + 2 * Nc, c, G2);
+    R dila[NP], rp[NP];
+    const int slot[6] = {3, 1, 6, 2, 7, 5};
+    R gs[6][NP];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) ldN<R, NP>(g.gij + slot[s] * Nc, c, gs[s]);
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const int e = tx * NP + p;
+      const V du_dx = sh[0][0][e], du_dy = sh[0][1][e], du_dz = sh[0][2][e];
+      const V dv_dx = sh[1][0][e], dv_dy = sh[1][1][e], dv_dz = sh[1][2][e];
+      const V dw_dx = sh[2][0][e], dw_dy = sh[2][1][e], dw_dz = sh[2][2][e];
+      const V dbz_dz = sbz[e];
+      const V Dila = du_dx + dv_dy + dw_dz;
+      dila[p] = Dila;
+      const V RBp = -(du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) -
+                    V(2) * (du_dy * dv_dx + dv_dz * dw_dy + dw_dx * du_dz) - dbz_dz + Dila / (2 * V(P.DT));
+      const V pxy = sX[0][0][e], pzy = sX[0][1][e], pyx = sX[1][0][e], pzx = sX[1][1][e];
+      const V pxz = sX[2][0][e], pyz = sX[2][1][e];
+      const V px = (o[2][p] - o[1][p]) / V(2);
+      const V py = (o[4][p] - o[3][p]) / V(2);
+      const V pz = (o[6][p] - o[5][p]) / V(2);
+      const V RDp = V(P.inv_rho) * (G0[p] * px + G1[p] * py + G2[p] * pz - gs[0][p] * pxy - gs[1][p] * pyx -
+                                    gs[2][p] * pxz - gs[3][p] * pzx - gs[4][p] * pyz - gs[5][p] * pzy);
+      rp[p] = RDp + RBp;
+    }
+    stN<R, NP>(F.dila, c, dila);
+    stN<R, NP>(F.Rp, c, rp);
   }
 }
 
