@@ -441,8 +441,19 @@ int launch_temperature(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const Field
   TRY(mark(x, "k_zero_flux"));
   k_T_coef<<<dim3(3, x->nblk_c), BLK, 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_T_coef"));
-  k_T_cell<false><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
-  TRY(mark(x, "k_T_cell"));
+  bool quad = false;
+  if constexpr (std::is_same<R, float>::value) {
+    if (x->cell_quad) {  // the float mirror, four cells a thread
+      const dim3 gq((d.NT + 127) / 128, (d.NR + 3) / 4, d.NZ);
+      k_T_cellN<R, 4><<<gq, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+      TRY(mark(x, "k_T_cellN"));
+      quad = true;
+    }
+  }
+  if (!quad) {
+    k_T_cell<false><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+    TRY(mark(x, "k_T_cell"));
+  }
   k_T_face<<<x->g8, BLK, 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_T_face"));
   return NIM_OK;

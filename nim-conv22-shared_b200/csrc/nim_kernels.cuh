@@ -174,6 +174,7 @@ constexpr int VC2_MINB = 3;  // resident blocks per SM asked of k_vel_cell2 (56 
 constexpr int VC2_MINB_F = 3, PSRC_MINB_F = 4, PFACE_MINB_F = 5, TCELL_MINB_F = 5, TFACE_MINB_F = 4;
 constexpr int VCN_MINB = 2;  // k_vel_cellN (four float cells a thread)
 constexpr int PSN_MINB = 2;  // k_p_srcN (four float cells a thread)
+constexpr int TCN_MINB = 2;  // k_T_cellN (four float cells a thread)
 template <class R>
 constexpr int minb(int fp64, int fp32) {
   return sizeof(R) == 8 ? fp64 : fp32;
@@ -3017,6 +3018,248 @@ __global__ void __launch_bounds__(CB3, minb<R>(5, TCELL_MINB_F)) k_T_cell(Dims d
     }
   }
   if (!SRC_ONLY && d.owns(blockIdx.z)) block_max<1, CB3>(red, e, ctl->err[par] + 4);
+}
+
+// ---- K7b, NP cells per thread (the float mirror's parallel passes,
+// n_theta % NP == 0): k_T_cell over NP theta-adjacent cells with NP-wide
+// vector loads and stores (as k_vel_cellN).  Thread y forms MT_F of
+// direction y+1 (the +theta neighbour's MT_A is the group's own vector
+// shifted by one cell, and one single load for the last cell) and two of the
+// six cross derivatives of T; thread 1 forms MT_F4, thread 2 the G_i d_i T
+// prefix; thread 0 assembles R_D_T and the cell update.  Each cell's
+// arithmetic is k_T_cell's.
+template <class R, int NP>
+__global__ void __launch_bounds__(CB3, TCN_MINB) k_T_cellN(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  using V = Ar<R>;
+  if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<1>(red);
+  __shared__ V sX[3][2][CB * NP];  // cross derivatives
+  __shared__ V sF4[8][CB * NP];    // MT_F4, formed by thread 1
+  __shared__ V sG[CB * NP];        // G1 dT/dx + G2 dT/dy + G3 dT/dz, by thread 2
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int tx = threadIdx.x;
+  const int i = blockIdx.x * (32 * NP) + NP * (tx & 31);
+  const int j = blockIdx.y * (CB / 32) + (tx >> 5);
+  const int k = blockIdx.z;
+  const bool active = i < d.NT && j < d.NR;
+  const int Nc = d.Nc, NF = d.NF, NT = d.NT, NR = d.NR, pl = d.plane;
+  const int c = i + NT * (j + NR * k);
+  const int im1 = (i == 0) ? NT - 1 : i - 1, ipn = (i + NP >= NT) ? i + NP - NT : i + NP;
+  const int f1 = c + NT * k;
+  const int fi[7] = {0, f1, f1 + NT, d.offT + c, d.offT + c + 1, d.offZ + c, d.offZ + c + pl};
+  const int f4b = d.offT + c - i + ipn;
+  auto faceN = [&](const R *a, int m, R (&v)[NP]) {
+    if (m == 4) {
+      R t[NP];
+      ldN<R, NP>(a, fi[3], t);
+#pragma unroll
+      for (int p = 0; p + 1 < NP; ++p) v[p] = t[p + 1];
+      v[NP - 1] = a[f4b];
+    } else {
+      ldN<R, NP>(a, fi[m], v);
+    }
+  };
+  const R *T = F.f[4] + par * NF;
+  auto along = [&](bool lo, bool hi, V v0, V va, V vb) {
+    return lo ? tang_vals(true, false, v0, va, vb, V(0.), V(0.))
+              : hi ? tang_vals(false, true, v0, V(0.), V(0.), va, vb) : tang_vals(false, false, v0, vb, V(0.), va, V(0.));
+  };
+  double e[1] = {0.};
+  if (active) by_dir(threadIdx.y, [&](auto D) {
+    constexpr int dd = decltype(D)::value, y = dd - 1;
+    const R *MA = F.MTA + (size_t)y * Nc;  // MT_A(q, dd) at MA[3q Nc]
+    // MT_F of direction dd (nim.f90:477-500) from MT_A of the cells and of
+    // their +dd neighbours
+    {
+      const bool nb = (dd == 1) ? (j < NR - 1) : (dd == 3) ? (k < d.NZ - 1) : true;
+      R A[6][NP];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) ldN<R, NP>(MA + 3 * q * Nc, c, A[q]);
+      V G[5][NP];
+#pragma unroll
+      for (int p = 0; p < NP; ++p)
+        for (int s = 0; s < 5; ++s) G[s][p] = V(0.);
+      if (nb) {
+        const int slots[4] = {1, 3, 4, 5};
+        R B[6][NP];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int q = slots[u];
+          if (dd == 2) {
+#pragma unroll
+            for (int p = 0; p + 1 < NP; ++p) B[q][p] = A[q][p + 1];
+            B[q][NP - 1] = MA[3 * q * Nc + c - i + ipn];
+          } else {
+            ldN<R, NP>(MA + 3 * q * Nc, c + (dd == 1 ? NT : pl), B[q]);
+          }
+        }
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          V a[6], a2[6], gg[5];
+          for (int q = 0; q < 6; ++q) a[q] = A[q][p];
+          a2[0] = a2[2] = V(0.);  // not used by form_Fd
+          a2[1] = B[1][p];
+          a2[3] = B[3][p];
+          a2[4] = B[4][p];
+          a2[5] = B[5][p];
+          if constexpr (std::is_same<R, float>::value)
+            form_Fd_rcp(a, a2, gg);
+          else
+            form_Fd(a, a2, gg);
+          for (int s = 0; s < 5; ++s) G[s][p] = gg[s];
+        }
+      }
+#pragma unroll
+      for (int s = 0; s < 5; ++s) {
+        R out[NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) out[p] = G[s][p];
+        stN<R, NP>(F.MTF + (size_t)(5 * (dd - 1) + s) * Nc, c, out);
+      }
+    }
+    // T's faces of the NP cells
+    R o[7][NP];
+#pragma unroll
+    for (int m = 1; m <= 6; ++m) faceN(T, m, o[m]);
+    const bool rlo = (j == 0), rhi = (j == NR - 1);
+    const int ra = rlo ? j + 1 : j - 1, rb = rlo ? j + 2 : (rhi ? j - 2 : j + 1);
+    const bool zlo = (k == 0), zhi = (k == d.NZ - 1);
+    const int ka = zlo ? k + 1 : k - 1, kb = zlo ? k + 2 : (zhi ? k - 2 : k + 1);
+    // cross derivatives of calculate_R_D_T: y=0 pxy,pzy  y=1 pyx,pzx  y=2 pxz,pyz
+    if (y == 0) {
+      const int rrow = NT * (j + (NR + 1) * k), zlev = d.offZ + NT * (j + NR * k);
+      const V r_m1 = T[rrow + im1], r_pn = T[rrow + ipn], r1_m1 = T[rrow + NT + im1], r1_pn = T[rrow + NT + ipn];
+      const V z_m1 = T[zlev + im1], z_pn = T[zlev + ipn], z1_m1 = T[zlev + pl + im1], z1_pn = T[zlev + pl + ipn];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const V up2 = (p + 1 < NP) ? (V)o[2][p + 1] : r1_pn, um2 = (p > 0) ? (V)o[2][p - 1] : r1_m1;
+        const V up1 = (p + 1 < NP) ? (V)o[1][p + 1] : r_pn, um1 = (p > 0) ? (V)o[1][p - 1] : r_m1;
+        sX[0][0][tx * NP + p] = V(0.5) * ((up2 - um2) / V(4.) - (up1 - um1) / V(4.));
+        const V up6 = (p + 1 < NP) ? (V)o[6][p + 1] : z1_pn, um6 = (p > 0) ? (V)o[6][p - 1] : z1_m1;
+        const V up5 = (p + 1 < NP) ? (V)o[5][p + 1] : z_pn, um5 = (p > 0) ? (V)o[5][p - 1] : z_m1;
+        sX[0][1][tx * NP + p] = V(0.5) * ((up6 - um6) / V(4.) - (up5 - um5) / V(4.));
+      }
+    } else if (y == 1) {
+      const int tra = d.offT + NT * (ra + NR * k), trb = d.offT + NT * (rb + NR * k);
+      const int zra = d.offZ + NT * (ra + NR * k), zrb = d.offZ + NT * (rb + NR * k);
+      R av[NP + 1], bv[NP + 1];
+      {
+        R t[NP];
+        ldN<R, NP>(T, tra + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) av[p] = t[p];
+        ldN<R, NP>(T, trb + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) bv[p] = t[p];
+        av[NP] = T[tra + ipn];
+        bv[NP] = T[trb + ipn];
+      }
+      R za[NP], zb[NP], zA[NP], zB[NP];
+      ldN<R, NP>(T, zra + i, za);
+      ldN<R, NP>(T, zrb + i, zb);
+      ldN<R, NP>(T, zra + pl + i, zA);
+      ldN<R, NP>(T, zrb + pl + i, zB);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        sX[1][0][tx * NP + p] =
+            V(0.5) * (along(rlo, rhi, o[4][p], av[p + 1], bv[p + 1]) - along(rlo, rhi, o[3][p], av[p], bv[p]));
+        sX[1][1][tx * NP + p] =
+            V(0.5) * (along(rlo, rhi, o[6][p], zA[p], zB[p]) - along(rlo, rhi, o[5][p], za[p], zb[p]));
+      }
+      // MT_F4 (nim.f90:466-475)
+      R a4[3][NP], a5[3][NP];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        ldN<R, NP>(F.MTA + (size_t)(12 + q) * Nc, c, a4[q]);
+        ldN<R, NP>(F.MTA + (size_t)(15 + q) * Nc, c, a5[q]);
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        V Am[3][6], F4[8];
+        for (int q = 0; q < 3; ++q) {
+          Am[q][4] = a4[q][p];
+          Am[q][5] = a5[q][p];
+        }
+        if constexpr (std::is_same<R, float>::value)
+          form_F4_rcp(Am, V(P.DT), F4);
+        else
+          form_F4(Am, V(P.DT), F4);
+        for (int q = 0; q < 8; ++q) sF4[q][tx * NP + p] = F4[q];
+      }
+    } else {
+      const int rka = NT * (j + (NR + 1) * ka), rkb = NT * (j + (NR + 1) * kb);
+      const int tka = d.offT + NT * (j + NR * ka), tkb = d.offT + NT * (j + NR * kb);
+      R pa[NP], pb[NP], pA[NP], pB[NP];
+      ldN<R, NP>(T, rka + i, pa);
+      ldN<R, NP>(T, rkb + i, pb);
+      ldN<R, NP>(T, rka + NT + i, pA);
+      ldN<R, NP>(T, rkb + NT + i, pB);
+      R av[NP + 1], bv[NP + 1];
+      {
+        R t[NP];
+        ldN<R, NP>(T, tka + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) av[p] = t[p];
+        ldN<R, NP>(T, tkb + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) bv[p] = t[p];
+        av[NP] = T[tka + ipn];
+        bv[NP] = T[tkb + ipn];
+      }
+      R G0[NP], G1[NP], G2[NP];
+      ldN<R, NP>(g.G, c, G0);
+      ldN<R, NP>(g.G + Nc, c, G1);
+      ldN<R, NP>(g.G + 2 * Nc, c, G2);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        sX[2][0][tx * NP + p] =
+            V(0.5) * (along(zlo, zhi, o[2][p], pA[p], pB[p]) - along(zlo, zhi, o[1][p], pa[p], pb[p]));
+        sX[2][1][tx * NP + p] =
+            V(0.5) * (along(zlo, zhi, o[4][p], av[p + 1], bv[p + 1]) - along(zlo, zhi, o[3][p], av[p], bv[p]));
+        // the leading G_i d_i T terms of R_D_T, in source order
+        const V px = (o[2][p] - o[1][p]) / V(2.);
+        const V py = (o[4][p] - o[3][p]) / V(2.);
+        const V pz = (o[6][p] - o[5][p]) / V(2.);
+        sG[tx * NP + p] = G0[p] * px + G1[p] * py + G2[p] * pz;
+      }
+    }
+  });
+  __syncthreads();
+  if (active && threadIdx.y == 0) {
+    R o[7][NP];
+#pragma unroll
+    for (int m = 1; m <= 6; ++m) faceN(T, m, o[m]);
+    const int slot[6] = {3, 1, 6, 2, 7, 5};
+    R gs[6][NP];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) ldN<R, NP>(g.gij + slot[s] * Nc, c, gs[s]);
+    R cur[NP], old[NP], out[NP];
+    ldN<R, NP>(F.c[3], c, cur);
+    ldN<R, NP>(F.co[3], c, old);
+    const V w = V(P.w[3]);
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const int e2 = tx * NP + p;
+      V F4[8];
+      for (int q = 0; q < 8; ++q) F4[q] = sF4[q][e2];
+      const V pxy = sX[0][0][e2], pzy = sX[0][1][e2], pyx = sX[1][0][e2], pzx = sX[1][1][e2];
+      const V pxz = sX[2][0][e2], pyz = sX[2][1][e2];
+      const V RDT = pv<V>(P.alpha, P.d_alpha) * (sG[e2] - gs[0][p] * pxy - gs[1][p] * pyx - gs[2][p] * pxz -
+                                                  gs[3][p] * pzx - gs[4][p] * pyz - gs[5][p] * pzy);
+      // cell_update (nse.f90:1018-1026), term by term
+      const V c0 = cur[p];
+      const V nw = stored<R>((1 - w) * c0 + (w / F4[0]) * (+F4[1] * (V)old[p] + F4[2] * (V)o[1][p] +
+                                                            F4[3] * (V)o[2][p] + F4[4] * (V)o[3][p] +
+                                                            F4[5] * (V)o[4][p] + F4[6] * (V)o[5][p] +
+                                                            F4[7] * (V)o[6][p] + (RDT + V(0.))));
+      out[p] = (R)nw;
+      e[0] = nmax(e[0], errv(nw, c0, first));
+    }
+    stN<R, NP>(F.c[3], c, out);
+  }
+  if (d.owns(blockIdx.z)) block_max<1, CB3>(red, e, ctl->err[par] + 4);
 }
 
 // ---- K8: +xi face updates of T (nse.f90:1033-1088), cur -> next; the z-wall
