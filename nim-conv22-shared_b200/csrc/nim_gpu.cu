@@ -424,8 +424,16 @@ int launch_pressure(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<
   TRY(mark(x, "k_p_bc"));
   k_p_bc_copy<<<x->nblk_b, BLK, 0, s>>>(d, F, x->ctl);
   TRY(mark(x, "k_p_bc_copy"));
-  k_p_face<<<g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
-  TRY(mark(x, "k_p_face"));
+  if (quad) {
+    if constexpr (std::is_same<R, float>::value) {
+      const dim3 gq((d.NT + 127) / 128, (d.NR + 3) / 4, d.NZ);
+      k_p_faceN<R, 4><<<gq, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+      TRY(mark(x, "k_p_faceN"));
+    }
+  } else {
+    k_p_face<<<g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+    TRY(mark(x, "k_p_face"));
+  }
   if (x->phys.dpdx_tolerance) {
     k_p_dpdx<<<x->nblk_c, BLK, 0, s>>>(d, g, F, x->ctl);
     TRY(mark(x, "k_p_dpdx"));

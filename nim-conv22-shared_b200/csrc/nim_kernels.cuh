@@ -175,6 +175,7 @@ constexpr int VC2_MINB_F = 3, PSRC_MINB_F = 4, PFACE_MINB_F = 5, TCELL_MINB_F = 
 constexpr int VCN_MINB = 2;  // k_vel_cellN (four float cells a thread)
 constexpr int PSN_MINB = 2;  // k_p_srcN (four float cells a thread)
 constexpr int TCN_MINB = 2;  // k_T_cellN (four float cells a thread)
+constexpr int PFN_MINB = 2;  // k_p_faceN (four float faces a thread)
 template <class R>
 constexpr int minb(int fp64, int fp32) {
   return sizeof(R) == 8 ? fp64 : fp32;
@@ -2832,6 +2833,195 @@ __global__ void __launch_bounds__(CB3, minb<R>(5, PFACE_MINB_F)) k_p_face(Dims d
       e[0] = errv(nw, pr[fo], first);
     });
   }
+  if (d.owns(blockIdx.z)) block_max<1, CB3>(red, e, ctl->err[par] + 3);
+}
+
+// ---- K5, NP cells per thread (the float mirror, n_theta % NP == 0):
+// k_p_face over NP theta-adjacent cells.  Thread y updates the +xi face of
+// direction y+1 of the NP cells from NP-wide vector loads: the faces of the
+// cells and of their +neighbours (for theta the group's own vectors shifted
+// by one cell, plus single loads for the last cell's neighbour), AA, R_p and
+// the metric differences; the theta faces' new values are stored one by one
+// (they start one cell off the vector boundary).  Each face's arithmetic is
+// p_face_value's.
+template <class R, int NP>
+__global__ void __launch_bounds__(CB3, PFN_MINB) k_p_faceN(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  using V = Ar<R>;
+  if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<1>(red);
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int tx = threadIdx.x;
+  const int i = blockIdx.x * (32 * NP) + NP * (tx & 31);
+  const int j = blockIdx.y * (CB / 32) + (tx >> 5);
+  const int k = blockIdx.z;
+  double e[1] = {0.};
+  if (i < d.NT && j < d.NR) by_dir(threadIdx.y, [&](auto D) {
+    constexpr int dd = decltype(D)::value;
+    const int Nc = d.Nc, NF = d.NF, NT = d.NT, NR = d.NR, pl = d.plane;
+    if ((dd == 1 && j == NR - 1) || (dd == 3 && k == d.NZ - 1)) return;  // a wall face: apply_pressure_bc's
+    const int c = i + NT * (j + NR * k);
+    const int im1 = (i == 0) ? NT - 1 : i - 1, ipn = (i + NP >= NT) ? i + NP - NT : i + NP;
+    const R *pr = F.f[3] + par * NF;
+    // faces 1..6 of the NP cells starting at (i, jj, kk) (face 4: the +theta
+    // face of cell p is the -theta face of cell p+1)
+    auto group = [&](int jj, int kk, R (&v)[7][NP]) {
+      const int cc = i + NT * (jj + NR * kk), ff = cc + NT * kk;
+      ldN<R, NP>(pr, ff, v[1]);
+      ldN<R, NP>(pr, ff + NT, v[2]);
+      R t[NP];
+      ldN<R, NP>(pr, d.offT + cc, t);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) v[3][p] = t[p];
+#pragma unroll
+      for (int p = 0; p + 1 < NP; ++p) v[4][p] = t[p + 1];
+      v[4][NP - 1] = pr[d.offT + cc - i + ipn];
+      ldN<R, NP>(pr, d.offZ + cc, v[5]);
+      ldN<R, NP>(pr, d.offZ + cc + pl, v[6]);
+    };
+    R ox[7][NP], on[7][NP];
+    group(j, k, ox);
+    if (dd == 1) {
+      group(j + 1, k, on);
+    } else if (dd == 3) {
+      group(j, k + 1, on);
+    } else {  // the +theta neighbours: cells i+1 .. i+NP
+      const int cw = c - i + ipn;  // the last cell's neighbour
+      const int iw = (ipn == NT - 1) ? 0 : ipn + 1;
+#pragma unroll
+      for (int p = 0; p + 1 < NP; ++p) {
+        on[1][p] = ox[1][p + 1];
+        on[2][p] = ox[2][p + 1];
+        on[4][p] = ox[4][p + 1];
+        on[5][p] = ox[5][p + 1];
+        on[6][p] = ox[6][p + 1];
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) on[3][p] = ox[4][p];
+      on[1][NP - 1] = pr[cw + NT * k];
+      on[2][NP - 1] = pr[cw + NT * k + NT];
+      on[4][NP - 1] = pr[d.offT + cw - ipn + iw];
+      on[5][NP - 1] = pr[d.offZ + cw];
+      on[6][NP - 1] = pr[d.offZ + cw + pl];
+    }
+    const R *A = g.AA + (size_t)15 * (dd - 1) * Nc;
+    constexpr int diag = (dd == 1) ? 2 : (dd == 2) ? 6 : 10;
+    // the ten off-diagonal terms, in source order
+    V s[NP];
+#pragma unroll
+    for (int t = 0; t < 10; ++t) {
+      const int pt = p_term(dd, t), coef = pt & 15, fpos = (pt >> 4) & 7, cell = pt >> 7;
+      R a[NP];
+      ldN<R, NP>(A + (size_t)(coef - 1) * Nc, c, a);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const V term = a[p] * (V)((cell == 1) ? ox[fpos][p] : on[fpos][p]);
+        s[p] = (t == 0) ? -term : s[p] - term;
+      }
+    }
+    // R_p of the cells and of their +neighbours
+    R rp[NP], rn[NP], a12[NP], a14[NP], ad[NP], dg0[NP], dg1[NP];
+    ldN<R, NP>(F.Rp, c, rp);
+    if (dd == 2) {
+#pragma unroll
+      for (int p = 0; p + 1 < NP; ++p) rn[p] = rp[p + 1];
+      rn[NP - 1] = F.Rp[c - i + ipn];
+    } else {
+      ldN<R, NP>(F.Rp, c + (dd == 1 ? NT : pl), rn);
+    }
+    ldN<R, NP>(A + 12 * (size_t)Nc, c, a12);
+    ldN<R, NP>(A + 14 * (size_t)Nc, c, a14);
+    ldN<R, NP>(A + (size_t)(diag - 1) * Nc, c, ad);
+    ldN<R, NP>(g.dg + (size_t)(2 * (dd - 1)) * Nc, c, dg0);
+    ldN<R, NP>(g.dg + (size_t)(2 * (dd - 1) + 1) * Nc, c, dg1);
+    // tangential derivatives of face 2dd along tr1(dd) and tr2(dd)
+    V t1[NP], t2[NP];
+    const bool rlo = (j == 0), rhi = (j == NR - 1);
+    const int ra = rlo ? j + 1 : j - 1, rb = rlo ? j + 2 : (rhi ? j - 2 : j + 1);
+    const bool zlo = (k == 0), zhi = (k == d.NZ - 1);
+    const int ka = zlo ? k + 1 : k - 1, kb = zlo ? k + 2 : (zhi ? k - 2 : k + 1);
+    auto along = [&](bool lo, bool hi, V v0, V va, V vb) {
+      return lo ? tang_vals(true, false, v0, va, vb, V(0.), V(0.))
+                : hi ? tang_vals(false, true, v0, V(0.), V(0.), va, vb) : tang_vals(false, false, v0, vb, V(0.), va, V(0.));
+    };
+    if (dd == 1) {  // face 2 (r faces of row j+1): along theta (centred), along z
+      const int rrow = NT * (j + 1 + (NR + 1) * k);
+      const V m1 = pr[rrow + im1], pn = pr[rrow + ipn];
+      R za[NP], zb[NP];
+      ldN<R, NP>(pr, NT * (j + 1 + (NR + 1) * ka) + i, za);
+      ldN<R, NP>(pr, NT * (j + 1 + (NR + 1) * kb) + i, zb);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const V up = (p + 1 < NP) ? (V)ox[2][p + 1] : pn, um = (p > 0) ? (V)ox[2][p - 1] : m1;
+        t1[p] = (up - um) / V(4.);
+        t2[p] = along(zlo, zhi, ox[2][p], za[p], zb[p]);
+      }
+    } else if (dd == 2) {  // face 4 (theta faces at i+1 ..): along r, along z
+      const int tra = d.offT + NT * (ra + NR * k), trb = d.offT + NT * (rb + NR * k);
+      const int tka = d.offT + NT * (j + NR * ka), tkb = d.offT + NT * (j + NR * kb);
+      R av[NP + 1], bv[NP + 1], ca[NP + 1], cb[NP + 1];
+      {
+        R t[NP];
+        ldN<R, NP>(pr, tra + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) av[p] = t[p];
+        ldN<R, NP>(pr, trb + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) bv[p] = t[p];
+        ldN<R, NP>(pr, tka + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) ca[p] = t[p];
+        ldN<R, NP>(pr, tkb + i, t);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) cb[p] = t[p];
+        av[NP] = pr[tra + ipn];
+        bv[NP] = pr[trb + ipn];
+        ca[NP] = pr[tka + ipn];
+        cb[NP] = pr[tkb + ipn];
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        t1[p] = along(rlo, rhi, ox[4][p], av[p + 1], bv[p + 1]);
+        t2[p] = along(zlo, zhi, ox[4][p], ca[p + 1], cb[p + 1]);
+      }
+    } else {  // face 6 (z faces of level k+1): along r, along theta (centred)
+      const int zra = d.offZ + NT * (ra + NR * k) + pl, zrb = d.offZ + NT * (rb + NR * k) + pl;
+      const int zlev = d.offZ + NT * (j + NR * k) + pl;
+      R za[NP], zb[NP];
+      ldN<R, NP>(pr, zra + i, za);
+      ldN<R, NP>(pr, zrb + i, zb);
+      const V m1 = pr[zlev + im1], pn = pr[zlev + ipn];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        t1[p] = along(rlo, rhi, ox[6][p], za[p], zb[p]);
+        const V up = (p + 1 < NP) ? (V)ox[6][p + 1] : pn, um = (p > 0) ? (V)ox[6][p - 1] : m1;
+        t2[p] = (up - um) / V(4.);
+      }
+    }
+    const V w = V(P.w_p);
+    R out[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const V B1 = (rp[p]) * a12[p];
+      const V B2 = (rn[p]) * a14[p];
+      const V B3 = (dg0[p]) * t1[p];
+      const V B4 = (dg1[p]) * t2[p];
+      const V old = ox[2 * dd][p];
+      const V nw = stored<R>((1 - w) * old + w / (ad[p]) * (s[p] + B1 + B2 + B3 + B4));
+      out[p] = (R)nw;
+      e[0] = nmax(e[0], errv(nw, old, first));
+    }
+    R *dst = F.f[3] + (1 - par) * NF;
+    if (dd == 2) {
+#pragma unroll
+      for (int p = 0; p + 1 < NP; ++p) dst[d.offT + c + p + 1] = out[p];
+      dst[d.offT + c - i + ipn] = out[NP - 1];
+    } else {
+      const int f1 = c + NT * k;
+      stN<R, NP>(dst, dd == 1 ? f1 + NT : d.offZ + c + pl, out);
+    }
+  });
   if (d.owns(blockIdx.z)) block_max<1, CB3>(red, e, ctl->err[par] + 3);
 }
 
