@@ -407,16 +407,15 @@ template <class R>
 int launch_pressure(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F) {
   const Dims &d = x->d;
   const dim3 g3 = x->g3;
-  bool quad = false;
-  if constexpr (std::is_same<R, float>::value) {
-    if (x->cell_quad) {  // the float mirror, four cells a thread
-      const dim3 gq((d.NT + 127) / 128, (d.NR + 3) / 4, d.NZ);
+  // the float mirror sweeps four theta-adjacent cells a thread (n_theta % 4 == 0)
+  const bool quad = std::is_same<R, float>::value && x->cell_quad;
+  const dim3 gq((d.NT + 127) / 128, (d.NR + 3) / 4, d.NZ);
+  if (quad) {
+    if constexpr (std::is_same<R, float>::value) {
       k_p_srcN<R, 4><<<gq, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
       TRY(mark(x, "k_p_srcN"));
-      quad = true;
     }
-  }
-  if (!quad) {
+  } else {
     k_p_src<<<g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
     TRY(mark(x, "k_p_src"));
   }
@@ -426,7 +425,6 @@ int launch_pressure(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<
   TRY(mark(x, "k_p_bc_copy"));
   if (quad) {
     if constexpr (std::is_same<R, float>::value) {
-      const dim3 gq((d.NT + 127) / 128, (d.NR + 3) / 4, d.NZ);
       k_p_faceN<R, 4><<<gq, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
       TRY(mark(x, "k_p_faceN"));
     }
@@ -449,19 +447,18 @@ int launch_temperature(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const Field
   TRY(mark(x, "k_zero_flux"));
   k_T_coef<<<dim3(3, x->nblk_c), BLK, 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_T_coef"));
-  bool quad = false;
   if constexpr (std::is_same<R, float>::value) {
-    if (x->cell_quad) {  // the float mirror, four cells a thread
+    if (x->cell_quad) {  // the float mirror: four theta-adjacent cells a thread
       const dim3 gq((d.NT + 127) / 128, (d.NR + 3) / 4, d.NZ);
       k_T_cellN<R, 4><<<gq, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
       TRY(mark(x, "k_T_cellN"));
-      quad = true;
+      k_T_faceN<R, 4><<<gq, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+      TRY(mark(x, "k_T_faceN"));
+      return NIM_OK;
     }
   }
-  if (!quad) {
-    k_T_cell<false><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
-    TRY(mark(x, "k_T_cell"));
-  }
+  k_T_cell<false><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+  TRY(mark(x, "k_T_cell"));
   k_T_face<<<x->g8, BLK, 0, s>>>(d, g, F, x->phys, x->ctl);
   TRY(mark(x, "k_T_face"));
   return NIM_OK;

@@ -176,6 +176,7 @@ constexpr int VCN_MINB = 2;  // k_vel_cellN (four float cells a thread)
 constexpr int PSN_MINB = 2;  // k_p_srcN (four float cells a thread)
 constexpr int TCN_MINB = 2;  // k_T_cellN (four float cells a thread)
 constexpr int PFN_MINB = 2;  // k_p_faceN (four float faces a thread)
+constexpr int TFN_MINB = 2;  // k_T_faceN (four float faces a thread)
 template <class R>
 constexpr int minb(int fp64, int fp32) {
   return sizeof(R) == 8 ? fp64 : fp32;
@@ -3485,6 +3486,122 @@ __global__ void __launch_bounds__(BLK, minb<R>(4, TFACE_MINB_F)) k_T_face(Dims d
     if (x.k == d.NZ - 1) Tn[x.face(d, 6)] = T[x.face(d, 6)];
   }
   if (d.owns(blockIdx.z)) block_max<1>(red, e, ctl->err[par] + 4);
+}
+
+// ---- K8, NP cells per thread (the float mirror, n_theta % NP == 0):
+// k_T_face over NP theta-adjacent cells, block (CB, 3): thread y updates the
+// +xi face of direction y+1 of the NP cells from NP-wide vector loads (the
+// +theta neighbours as k_p_faceN forms them) and carries the z-wall values
+// to the next half (thread 2).  Each face's arithmetic is face_update's.
+template <class R, int NP>
+__global__ void __launch_bounds__(CB3, TFN_MINB) k_T_faceN(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  using V = Ar<R>;
+  if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<1>(red);
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int tx = threadIdx.x;
+  const int i = blockIdx.x * (32 * NP) + NP * (tx & 31);
+  const int j = blockIdx.y * (CB / 32) + (tx >> 5);
+  const int k = blockIdx.z;
+  double e[1] = {0.};
+  if (i < d.NT && j < d.NR) by_dir(threadIdx.y, [&](auto D) {
+    constexpr int dd = decltype(D)::value;
+    const int Nc = d.Nc, NF = d.NF, NT = d.NT, NR = d.NR, pl = d.plane;
+    const int c = i + NT * (j + NR * k);
+    const int ipn = (i + NP >= NT) ? i + NP - NT : i + NP;
+    const R *T = F.f[4] + par * NF;
+    R *Tn = F.f[4] + (1 - par) * NF;
+    if (dd == 3) {  // the z-wall values set by apply_zero_flux travel to the next half
+      R t[NP];
+      if (k == 0) {
+        ldN<R, NP>(T, d.offZ + c, t);
+        stN<R, NP>(Tn, d.offZ + c, t);
+      }
+      if (k == d.NZ - 1) {
+        ldN<R, NP>(T, d.offZ + c + pl, t);
+        stN<R, NP>(Tn, d.offZ + c + pl, t);
+      }
+    }
+    if ((dd == 1 && j == NR - 1) || (dd == 3 && k == d.NZ - 1)) return;  // a wall face
+    auto group = [&](int jj, int kk, R (&v)[7][NP]) {
+      const int cc = i + NT * (jj + NR * kk), ff = cc + NT * kk;
+      ldN<R, NP>(T, ff, v[1]);
+      ldN<R, NP>(T, ff + NT, v[2]);
+      R t[NP];
+      ldN<R, NP>(T, d.offT + cc, t);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) v[3][p] = t[p];
+#pragma unroll
+      for (int p = 0; p + 1 < NP; ++p) v[4][p] = t[p + 1];
+      v[4][NP - 1] = T[d.offT + cc - i + ipn];
+      ldN<R, NP>(T, d.offZ + cc, v[5]);
+      ldN<R, NP>(T, d.offZ + cc + pl, v[6]);
+    };
+    R ox[7][NP], on[7][NP], cx[NP], cxo[NP], cn[NP], cno[NP];
+    group(j, k, ox);
+    ldN<R, NP>(F.c[3], c, cx);
+    ldN<R, NP>(F.co[3], c, cxo);
+    if (dd == 1 || dd == 3) {
+      if (dd == 1)
+        group(j + 1, k, on);
+      else
+        group(j, k + 1, on);
+      ldN<R, NP>(F.c[3], c + (dd == 1 ? NT : pl), cn);
+      ldN<R, NP>(F.co[3], c + (dd == 1 ? NT : pl), cno);
+    } else {  // the +theta neighbours: cells i+1 .. i+NP
+      const int cw = c - i + ipn;
+      const int iw = (ipn == NT - 1) ? 0 : ipn + 1;
+#pragma unroll
+      for (int p = 0; p + 1 < NP; ++p) {
+        on[1][p] = ox[1][p + 1];
+        on[2][p] = ox[2][p + 1];
+        on[4][p] = ox[4][p + 1];
+        on[5][p] = ox[5][p + 1];
+        on[6][p] = ox[6][p + 1];
+        cn[p] = cx[p + 1];
+        cno[p] = cxo[p + 1];
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) on[3][p] = ox[4][p];
+      on[1][NP - 1] = T[cw + NT * k];
+      on[2][NP - 1] = T[cw + NT * k + NT];
+      on[4][NP - 1] = T[d.offT + cw - ipn + iw];
+      on[5][NP - 1] = T[d.offZ + cw];
+      on[6][NP - 1] = T[d.offZ + cw + pl];
+      cn[NP - 1] = F.c[3][cw];
+      cno[NP - 1] = F.co[3][cw];
+    }
+    R Fd[5][NP], dg0[NP], dg1[NP];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) ldN<R, NP>(F.MTF + (size_t)(5 * (dd - 1) + q) * Nc, c, Fd[q]);
+    ldN<R, NP>(g.dg + (size_t)(2 * (dd - 1)) * Nc, c, dg0);
+    ldN<R, NP>(g.dg + (size_t)(2 * (dd - 1) + 1) * Nc, c, dg1);
+    constexpr int e1 = (dd == 1) ? 2 : 1, e2 = (dd == 3) ? 2 : 3;  // tr1(dd), tr2(dd)
+    const V w = V(P.w[3]);
+    R out[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const V B3 = (dg0[p]) * ((V)ox[2 * e1][p] - ox[2 * e1 - 1][p] + on[2 * e1][p] - on[2 * e1 - 1][p]) / V(4.0);
+      const V B4 = (dg1[p]) * ((V)ox[2 * e2][p] - ox[2 * e2 - 1][p] + on[2 * e2][p] - on[2 * e2 - 1][p]) / V(4.0);
+      const V old = ox[2 * dd][p];
+      const V nw = stored<R>((1 - w) * old + (w / Fd[0][p]) * (+Fd[1][p] * (V)ox[2 * dd - 1][p] +
+                                                                 Fd[2][p] * (V)on[2 * dd][p] +
+                                                                 Fd[3][p] * ((V)cx[p] + cxo[p]) +
+                                                                 Fd[4][p] * ((V)cn[p] + cno[p]) - B3 - B4));
+      out[p] = (R)nw;
+      e[0] = nmax(e[0], errv(nw, old, first));
+    }
+    if (dd == 2) {
+#pragma unroll
+      for (int p = 0; p + 1 < NP; ++p) Tn[d.offT + c + p + 1] = out[p];
+      Tn[d.offT + c - i + ipn] = out[NP - 1];
+    } else {
+      stN<R, NP>(Tn, dd == 1 ? c + NT * k + NT : d.offZ + c + pl, out);
+    }
+  });
+  if (d.owns(blockIdx.z)) block_max<1, CB3>(red, e, ctl->err[par] + 4);
 }
 
 // ---- K9: end of one pass (find_error's maxima, the do-while test of
