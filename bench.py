@@ -81,6 +81,7 @@ KERNEL_BYTES_PER_CELL = {
     "k_T_cellN": 8 * 48,    # the float mirror's form of k_T_cell (same words)
     "k_p_faceN": 8 * 52,    # the float mirror's form of k_p_face (same words)
     "k_T_faceN": 8 * 29,    # the float mirror's form of k_T_face (same words)
+    "k_vel_faceN": 8 * 45,  # the float mirror's form of k_vel_face (same words)
     "k_p_face": 8 * 52,     # faces p (3) Rp (1) AA used (39) dg (6); write faces p (3)
     "k_T_coef": 8 * 42,     # cells+old u,v,w (6) xi (9) g^ij diagonal (3) gfd (6); write MT_A (18)
     "k_T_cell": 8 * 48,     # MT_A (18) faces T (3) G (3) g^ij (6) T,T_old (2); write T, MT_F (16)

@@ -112,7 +112,8 @@ struct nim_ctx {
   // k_vel_cell_tile (TMA-staged cell sweep of u, v, w, formulation 2)
   bool cell_tile = false;
   bool cell_pair = false;  // k_vel_cell2: two theta-adjacent cells per thread
-  bool cell_quad = false;  // the float mirror's cell sweep as k_vel_cellN, four cells a thread
+  bool cell_quad = false;  // the float mirror's sweeps four cells a thread (k_vel_cellN, k_p_srcN, ...)
+  bool face_quad = false;  // and its face sweep of u, v, w as k_vel_faceN
   VelCellMaps cmap64{}, cmap32{};
   GeoT<float> g32{};
   FieldsT<float> F32{};
@@ -322,7 +323,13 @@ int launch_vel(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F
       k_vel_cell<false, 2><<<x->g3, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
       TRY(mark(x, "k_vel_cell"));
     }
-    if (x->bulk) {
+    if (std::is_same<R, float>::value && x->face_quad) {
+      if constexpr (std::is_same<R, float>::value) {  // the float mirror, four cells a thread
+        const dim3 gq((d.NT + 127) / 128, (d.NR + 3) / 4, d.NZ);
+        k_vel_faceN<R, 4><<<gq, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+        TRY(mark(x, "k_vel_faceN"));
+      }
+    } else if (x->bulk) {
       const dim3 gt((d.NT + 31) / 32, (d.NR + VT_R - 1) / VT_R, (d.NZ + x->tile_kc - 1) / x->tile_kc);
       const VelFaceMaps &M = std::is_same<R, double>::value ? x->vmap64 : x->vmap32;
       if (x->slab_count)
@@ -945,8 +952,10 @@ static bool encode_vel_cell_maps(const Dims &d, const FieldsT<R> &F, VelCellMaps
 // (two theta-adjacent cells per thread, paired loads) when n_theta is even,
 // and for the float mirror as k_vel_cellN (four cells a thread, float4
 // loads) when n_theta % 4 == 0; NIM_CELL_SWEEP=gather forces k_vel_cell,
-// =pair k_vel_cell2, =tile k_vel_cell_tile (under the tile's n_theta
-// conditions).
+// =pair k_vel_cell2 (and the float mirror's other sweeps in their
+// one-cell forms), =tile k_vel_cell_tile (under the tile's n_theta
+// conditions).  The float mirror's face sweep of u, v, w runs four cells a
+// thread as well (k_vel_faceN) unless NIM_FACE_SWEEP names a form.
 static int choose_face_sweep(nim_ctx *x) {
   const Dims &d = x->d;
   int sms = 0;
@@ -970,6 +979,7 @@ static int choose_face_sweep(nim_ctx *x) {
   // the float mirror's sweeps four cells a thread when n_theta % 4 == 0
   x->cell_pair = !x->cell_tile && d.NT % 2 == 0 && !x->seq && x->params.formulation == 2 && cell != "gather";
   x->cell_quad = x->cell_pair && d.NT % 4 == 0 && cell != "pair";
+  x->face_quad = x->cell_quad && force != "tile" && force != "gather";
   return NIM_OK;
 }
 

@@ -177,6 +177,7 @@ constexpr int PSN_MINB = 2;  // k_p_srcN (four float cells a thread)
 constexpr int TCN_MINB = 2;  // k_T_cellN (four float cells a thread)
 constexpr int PFN_MINB = 2;  // k_p_faceN (four float faces a thread)
 constexpr int TFN_MINB = 2;  // k_T_faceN (four float faces a thread)
+constexpr int VFN_MINB = 2;  // k_vel_faceN (four float faces a thread)
 template <class R>
 constexpr int minb(int fp64, int fp32) {
   return sizeof(R) == 8 ? fp64 : fp32;
@@ -3488,6 +3489,95 @@ __global__ void __launch_bounds__(BLK, minb<R>(4, TFACE_MINB_F)) k_T_face(Dims d
   if (d.owns(blockIdx.z)) block_max<1>(red, e, ctl->err[par] + 4);
 }
 
+// The +xi_dd face updates of one field (faces fr of the current half, new
+// values into fn) for the NP theta-adjacent cells of a group starting at
+// (i, j, k), from NP-wide vector loads: the faces of the cells and of their
+// +dd neighbours (for theta the group's own vectors shifted by one cell,
+// plus single loads for the last cell's neighbour) and the cell and old-cell
+// values cv, co; the theta faces' new values are stored one by one (they
+// start one cell off the vector boundary).  Each face's arithmetic is
+// face_update's.  Returns the largest change.
+template <int dd, class R, int NP>
+__device__ __forceinline__ double face_updateN(const Dims &d, int i, int j, int k, const R *fr, R *fn, const R *cv,
+                                               const R *co, const R (&Fd)[5][NP], const R (&dg0)[NP],
+                                               const R (&dg1)[NP], Ar<R> w, bool first) {
+  using V = Ar<R>;
+  const int NT = d.NT, NR = d.NR, pl = d.plane;
+  const int c = i + NT * (j + NR * k);
+  const int ipn = (i + NP >= NT) ? i + NP - NT : i + NP;
+  auto group = [&](int jj, int kk, R (&v)[7][NP]) {
+    const int cc = i + NT * (jj + NR * kk), ff = cc + NT * kk;
+    ldN<R, NP>(fr, ff, v[1]);
+    ldN<R, NP>(fr, ff + NT, v[2]);
+    R t[NP];
+    ldN<R, NP>(fr, d.offT + cc, t);
+#pragma unroll
+    for (int p = 0; p < NP; ++p) v[3][p] = t[p];
+#pragma unroll
+    for (int p = 0; p + 1 < NP; ++p) v[4][p] = t[p + 1];
+    v[4][NP - 1] = fr[d.offT + cc - i + ipn];
+    ldN<R, NP>(fr, d.offZ + cc, v[5]);
+    ldN<R, NP>(fr, d.offZ + cc + pl, v[6]);
+  };
+  R ox[7][NP], on[7][NP], cx[NP], cxo[NP], cn[NP], cno[NP];
+  group(j, k, ox);
+  ldN<R, NP>(cv, c, cx);
+  ldN<R, NP>(co, c, cxo);
+  if (dd == 1 || dd == 3) {
+    if (dd == 1)
+      group(j + 1, k, on);
+    else
+      group(j, k + 1, on);
+    ldN<R, NP>(cv, c + (dd == 1 ? NT : pl), cn);
+    ldN<R, NP>(co, c + (dd == 1 ? NT : pl), cno);
+  } else {  // the +theta neighbours: cells i+1 .. i+NP
+    const int cw = c - i + ipn;
+    const int iw = (ipn == NT - 1) ? 0 : ipn + 1;
+#pragma unroll
+    for (int p = 0; p + 1 < NP; ++p) {
+      on[1][p] = ox[1][p + 1];
+      on[2][p] = ox[2][p + 1];
+      on[4][p] = ox[4][p + 1];
+      on[5][p] = ox[5][p + 1];
+      on[6][p] = ox[6][p + 1];
+      cn[p] = cx[p + 1];
+      cno[p] = cxo[p + 1];
+    }
+#pragma unroll
+    for (int p = 0; p < NP; ++p) on[3][p] = ox[4][p];
+    on[1][NP - 1] = fr[cw + NT * k];
+    on[2][NP - 1] = fr[cw + NT * k + NT];
+    on[4][NP - 1] = fr[d.offT + cw - ipn + iw];
+    on[5][NP - 1] = fr[d.offZ + cw];
+    on[6][NP - 1] = fr[d.offZ + cw + pl];
+    cn[NP - 1] = cv[cw];
+    cno[NP - 1] = co[cw];
+  }
+  constexpr int e1 = (dd == 1) ? 2 : 1, e2 = (dd == 3) ? 2 : 3;  // tr1(dd), tr2(dd)
+  double err = 0.;
+  R out[NP];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    const V B3 = (dg0[p]) * ((V)ox[2 * e1][p] - ox[2 * e1 - 1][p] + on[2 * e1][p] - on[2 * e1 - 1][p]) / V(4.0);
+    const V B4 = (dg1[p]) * ((V)ox[2 * e2][p] - ox[2 * e2 - 1][p] + on[2 * e2][p] - on[2 * e2 - 1][p]) / V(4.0);
+    const V old = ox[2 * dd][p];
+    const V nw = stored<R>((1 - w) * old + (w / Fd[0][p]) * (+Fd[1][p] * (V)ox[2 * dd - 1][p] +
+                                                               Fd[2][p] * (V)on[2 * dd][p] +
+                                                               Fd[3][p] * ((V)cx[p] + cxo[p]) +
+                                                               Fd[4][p] * ((V)cn[p] + cno[p]) - B3 - B4));
+    out[p] = (R)nw;
+    err = nmax(err, errv(nw, old, first));
+  }
+  if (dd == 2) {
+#pragma unroll
+    for (int p = 0; p + 1 < NP; ++p) fn[d.offT + c + p + 1] = out[p];
+    fn[d.offT + c - i + ipn] = out[NP - 1];
+  } else {
+    stN<R, NP>(fn, dd == 1 ? c + NT * k + NT : d.offZ + c + pl, out);
+  }
+  return err;
+}
+
 // ---- K8, NP cells per thread (the float mirror, n_theta % NP == 0):
 // k_T_face over NP theta-adjacent cells, block (CB, 3): thread y updates the
 // +xi face of direction y+1 of the NP cells from NP-wide vector loads (the
@@ -3602,6 +3692,40 @@ __global__ void __launch_bounds__(CB3, TFN_MINB) k_T_faceN(Dims d, GeoT<R> g, Fi
     }
   });
   if (d.owns(blockIdx.z)) block_max<1, CB3>(red, e, ctl->err[par] + 4);
+}
+
+// ---- K2, NP cells per thread (the float mirror, n_theta % NP == 0): the
+// +xi face updates of u, v, w (nse.f90:878-1005) over NP theta-adjacent
+// cells, block (CB, 3): thread y updates the +xi face of direction y+1 of
+// the NP cells for each component (face_updateN), as k_vel_face.
+template <class R, int NP>
+__global__ void __launch_bounds__(CB3, VFN_MINB) k_vel_faceN(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  if (ctl->done) return;
+  __shared__ BlockRed red;
+  red_init<3>(red);
+  const int par = parity(ctl);
+  const bool first = ctl->first;
+  const int tx = threadIdx.x;
+  const int i = blockIdx.x * (32 * NP) + NP * (tx & 31);
+  const int j = blockIdx.y * (CB / 32) + (tx >> 5);
+  const int k = blockIdx.z;
+  double e[3] = {0., 0., 0.};
+  if (i < d.NT && j < d.NR) by_dir(threadIdx.y, [&](auto D) {
+    constexpr int dd = decltype(D)::value;
+    if ((dd == 1 && j == d.NR - 1) || (dd == 3 && k == d.NZ - 1)) return;  // a wall face
+    const int Nc = d.Nc, NF = d.NF;
+    const int c = i + d.NT * (j + d.NR * k);
+    R Fd[5][NP], dg0[NP], dg1[NP];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) ldN<R, NP>(F.MF + (size_t)(5 * (dd - 1) + q) * Nc, c, Fd[q]);
+    ldN<R, NP>(g.dg + (size_t)(2 * (dd - 1)) * Nc, c, dg0);
+    ldN<R, NP>(g.dg + (size_t)(2 * (dd - 1) + 1) * Nc, c, dg1);
+#pragma unroll 1
+    for (int q = 0; q < 3; ++q)
+      e[q] = face_updateN<dd>(d, i, j, k, F.f[q] + par * NF, F.f[q] + (1 - par) * NF, F.c[q], F.co[q], Fd, dg0, dg1,
+                              Ar<R>(P.w[q]), first);
+  });
+  if (d.owns(blockIdx.z)) block_max<3, CB3>(red, e, ctl->err[par]);
 }
 
 // ---- K9: end of one pass (find_error's maxima, the do-while test of

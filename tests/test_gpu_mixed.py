@@ -149,8 +149,8 @@ def test_profile_runs_fp32_passes_and_keeps_fp64_fields():
     pa, pb = a.profile_iterations(2), b.profile_iterations(2)
     # the same kernels, but the float mirror's cell sweeps take four cells
     # a thread (n_theta % 4 == 0)
-    quad = {"k_vel_cell2": "k_vel_cellN", "k_p_src": "k_p_srcN", "k_p_face": "k_p_faceN", "k_T_cell": "k_T_cellN",
-            "k_T_face": "k_T_faceN"}
+    quad = {"k_vel_cell2": "k_vel_cellN", "k_vel_face": "k_vel_faceN", "k_vel_face_tile": "k_vel_faceN",
+            "k_p_src": "k_p_srcN", "k_p_face": "k_p_faceN", "k_T_cell": "k_T_cellN", "k_T_face": "k_T_faceN"}
     assert [quad.get(k, k) for k in pa] == list(pb)
     assert all(v > 0 for v in pb.values())
     for f, v in zip(STATE, before):

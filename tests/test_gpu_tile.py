@@ -130,16 +130,19 @@ def test_pair_and_gather_cell_sweeps_are_bitwise_equal(monkeypatch, precision, d
 @pytest.mark.parametrize("dims", [(40, 6, 26), (132, 5, 7)])
 def test_quad_and_pair_float_cell_sweeps_are_bitwise_equal(monkeypatch, dims):
     """The mixed path's FP32 passes with the four-cells-a-thread sweeps
-    (k_vel_cellN, k_p_srcN, k_p_faceN, k_T_cellN, k_T_faceN: float4 loads;
-    the default for n_theta % 4 == 0) against k_vel_cell2, k_p_src,
-    k_p_face, k_T_cell and k_T_face: whole steps to the bit (theta seams,
-    walls, a partial 128-cell patch)."""
+    (k_vel_cellN, k_vel_faceN, k_p_srcN, k_p_faceN, k_T_cellN, k_T_faceN:
+    float4 loads; the default for n_theta % 4 == 0) against k_vel_cell2,
+    k_vel_face, k_p_src, k_p_face, k_T_cell and k_T_face: whole steps to
+    the bit (theta seams, walls, a partial 128-cell patch)."""
     case = config.small_case(*dims, steps=2)
-    monkeypatch.setenv("NIM_FACE_SWEEP", "gather")
     outs = []
-    for form, kernels in (("pair", ("k_vel_cell2", "k_p_src", "k_p_face", "k_T_cell", "k_T_face")),
-                          ("", ("k_vel_cellN", "k_p_srcN", "k_p_faceN", "k_T_cellN", "k_T_faceN"))):
+    for form, kernels in (("pair", ("k_vel_cell2", "k_vel_face", "k_p_src", "k_p_face", "k_T_cell", "k_T_face")),
+                          ("", ("k_vel_cellN", "k_vel_faceN", "k_p_srcN", "k_p_faceN", "k_T_cellN", "k_T_faceN"))):
         monkeypatch.setenv("NIM_CELL_SWEEP", form)
+        if form:
+            monkeypatch.setenv("NIM_FACE_SWEEP", "gather")
+        else:
+            monkeypatch.delenv("NIM_FACE_SWEEP", raising=False)
         s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()), case.params(precision=_abi.PRECISION_MIXED))
         s.initialize_nse()
         s.add_temperature_noise(case.noise, case.seed)
