@@ -414,12 +414,22 @@ template <class R>
 int launch_pressure(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<R> &F) {
   const Dims &d = x->d;
   const dim3 g3 = x->g3;
-  // the float mirror sweeps four theta-adjacent cells a thread (n_theta % 4 == 0)
+  // the float mirror sweeps four theta-adjacent cells a thread (n_theta % 4
+  // == 0), the FP64 path two (n_theta even: double2 loads; measured at C2,
+  // k_p_face 154 -> 113 us, k_p_src 160 -> 159 us; the temperature and
+  // velocity sweeps stay one cell a thread, their pair forms were slower)
   const bool quad = std::is_same<R, float>::value && x->cell_quad;
+  const bool pair = std::is_same<R, double>::value && x->cell_pair;
   const dim3 gq((d.NT + 127) / 128, (d.NR + 3) / 4, d.NZ);
+  const dim3 gp((d.NT + 63) / 64, (d.NR + 3) / 4, d.NZ);
   if (quad) {
     if constexpr (std::is_same<R, float>::value) {
       k_p_srcN<R, 4><<<gq, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+      TRY(mark(x, "k_p_srcN"));
+    }
+  } else if (pair) {
+    if constexpr (std::is_same<R, double>::value) {
+      k_p_srcN<R, 2><<<gp, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
       TRY(mark(x, "k_p_srcN"));
     }
   } else {
@@ -433,6 +443,11 @@ int launch_pressure(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<
   if (quad) {
     if constexpr (std::is_same<R, float>::value) {
       k_p_faceN<R, 4><<<gq, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
+      TRY(mark(x, "k_p_faceN"));
+    }
+  } else if (pair) {
+    if constexpr (std::is_same<R, double>::value) {
+      k_p_faceN<R, 2><<<gp, dim3(CB, 3), 0, s>>>(d, g, F, x->phys, x->ctl);
       TRY(mark(x, "k_p_faceN"));
     }
   } else {

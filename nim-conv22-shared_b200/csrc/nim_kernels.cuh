@@ -173,9 +173,9 @@ constexpr int VC2_MINB = 3;  // resident blocks per SM asked of k_vel_cell2 (56 
 // for: computing in float they need about half the FP64 registers
 constexpr int VC2_MINB_F = 3, PSRC_MINB_F = 4, PFACE_MINB_F = 5, TCELL_MINB_F = 5, TFACE_MINB_F = 4;
 constexpr int VCN_MINB = 2;  // k_vel_cellN (four float cells a thread)
-constexpr int PSN_MINB = 2;  // k_p_srcN (four float cells a thread)
+constexpr int PSN_MINB = 2;  // k_p_srcN (four float or two FP64 cells a thread)
 constexpr int TCN_MINB = 2;  // k_T_cellN (four float cells a thread)
-constexpr int PFN_MINB = 2;  // k_p_faceN (four float faces a thread)
+constexpr int PFN_MINB = 2;  // k_p_faceN (four float or two FP64 faces a thread)
 constexpr int TFN_MINB = 2;  // k_T_faceN (four float faces a thread)
 constexpr int VFN_MINB = 2;  // k_vel_faceN (four float faces a thread)
 template <class R>
@@ -2416,7 +2416,8 @@ __global__ void __launch_bounds__(CB3, minb<R>(4, PSRC_MINB_F)) k_p_src(Dims d, 
   }
 }
 
-// ---- K3, NP cells per thread (the float mirror, n_theta % NP == 0):
+// ---- K3, NP cells per thread (the float mirror with NP = 4, the FP64 path
+// with NP = 2; n_theta % NP == 0):
 // k_p_src over NP theta-adjacent cells, every value the cells share a row
 // for in one NP-wide vector load (as k_vel_cellN).  Thread y forms the
 // gradients of velocity component y (y = 1 also d(bz)/dz) and two of the six
@@ -2838,7 +2839,8 @@ __global__ void __launch_bounds__(CB3, minb<R>(5, PFACE_MINB_F)) k_p_face(Dims d
   if (d.owns(blockIdx.z)) block_max<1, CB3>(red, e, ctl->err[par] + 3);
 }
 
-// ---- K5, NP cells per thread (the float mirror, n_theta % NP == 0):
+// ---- K5, NP cells per thread (the float mirror with NP = 4, the FP64 path
+// with NP = 2; n_theta % NP == 0):
 // k_p_face over NP theta-adjacent cells.  Thread y updates the +xi face of
 // direction y+1 of the NP cells from NP-wide vector loads: the faces of the
 // cells and of their +neighbours (for theta the group's own vectors shifted

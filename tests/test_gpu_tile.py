@@ -107,8 +107,9 @@ def test_tile_and_gather_forms_are_bitwise_equal(monkeypatch, precision):
 @pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
 @pytest.mark.parametrize("dims", [(40, 6, 26), (130, 5, 7)])
 def test_pair_and_gather_cell_sweeps_are_bitwise_equal(monkeypatch, precision, dims):
-    """k_vel_cell2 (two theta-adjacent cells per thread, paired loads)
-    against k_vel_cell: whole steps to the bit (theta seams, walls, a
+    """k_vel_cell2 (two theta-adjacent cells per thread, paired loads), and
+    in FP64 k_p_srcN / k_p_faceN with two cells a thread, against k_vel_cell,
+    k_p_src and k_p_face: whole steps to the bit (theta seams, walls, a
     partial 64-cell patch)."""
     case = config.small_case(*dims, steps=2)
     monkeypatch.setenv("NIM_FACE_SWEEP", "gather")
@@ -120,7 +121,11 @@ def test_pair_and_gather_cell_sweeps_are_bitwise_equal(monkeypatch, precision, d
         s.add_temperature_noise(case.noise, case.seed)
         recs = s.solve_nse(2)
         outs.append(([(r.iters, r.iters_fp32, r.nu_inner) for r in recs], [s.download(f) for f in STATE]))
-        assert ("k_vel_cell2" if form == "pair" else "k_vel_cell") in s.profile_iterations(1)
+        prof = s.profile_iterations(1)
+        assert ("k_vel_cell2" if form == "pair" else "k_vel_cell") in prof
+        if precision == _abi.PRECISION_FP64:  # the FP64 pressure sweeps take the pairs too
+            want = ("k_p_srcN", "k_p_faceN") if form == "pair" else ("k_p_src", "k_p_face")
+            assert all(k in prof for k in want), list(prof)
         s.close()
     assert outs[0][0] == outs[1][0]
     for a, b in zip(outs[0][1], outs[1][1]):
