@@ -114,6 +114,7 @@ struct nim_ctx {
   bool cell_pair = false;  // k_vel_cell2: two theta-adjacent cells per thread
   bool cell_quad = false;  // the float mirror's sweeps four cells a thread (k_vel_cellN, k_p_srcN, ...)
   bool face_quad = false;  // and its face sweep of u, v, w as k_vel_faceN
+  bool press_pair = false; // the FP64 pressure sweeps two cells a thread (k_p_srcN, k_p_faceN)
   VelCellMaps cmap64{}, cmap32{};
   GeoT<float> g32{};
   FieldsT<float> F32{};
@@ -419,7 +420,7 @@ int launch_pressure(nim_ctx *x, cudaStream_t s, const GeoT<R> &g, const FieldsT<
   // k_p_face 154 -> 113 us, k_p_src 160 -> 159 us; the temperature and
   // velocity sweeps stay one cell a thread, their pair forms were slower)
   const bool quad = std::is_same<R, float>::value && x->cell_quad;
-  const bool pair = std::is_same<R, double>::value && x->cell_pair;
+  const bool pair = std::is_same<R, double>::value && x->press_pair;
   const dim3 gq((d.NT + 127) / 128, (d.NR + 3) / 4, d.NZ);
   const dim3 gp((d.NT + 63) / 64, (d.NR + 3) / 4, d.NZ);
   if (quad) {
@@ -968,8 +969,8 @@ static bool encode_vel_cell_maps(const Dims &d, const FieldsT<R> &F, VelCellMaps
 // and for the float mirror as k_vel_cellN (four cells a thread, float4
 // loads) when n_theta % 4 == 0; NIM_CELL_SWEEP=gather forces k_vel_cell,
 // =pair k_vel_cell2 (and the float mirror's other sweeps in their
-// one-cell forms), =tile k_vel_cell_tile (under the tile's n_theta
-// conditions).  The float mirror's face sweep of u, v, w runs four cells a
+// one-cell forms), =quad the four-cell forms on any n_theta % 4 == 0,
+// =tile k_vel_cell_tile (under the tile's n_theta conditions).  The float mirror's face sweep of u, v, w runs four cells a
 // thread as well (k_vel_faceN) unless NIM_FACE_SWEEP names a form.
 static int choose_face_sweep(nim_ctx *x) {
   const Dims &d = x->d;
@@ -993,8 +994,17 @@ static int choose_face_sweep(nim_ctx *x) {
   // the paired-load form whenever n_theta is even, unless another is asked for;
   // the float mirror's sweeps four cells a thread when n_theta % 4 == 0
   x->cell_pair = !x->cell_tile && d.NT % 2 == 0 && !x->seq && x->params.formulation == 2 && cell != "gather";
-  x->cell_quad = x->cell_pair && d.NT % 4 == 0 && cell != "pair";
+  // the NP-cells-a-thread sweeps run a row of n_theta / NP threads per
+  // theta row of the patch; below 3/4 of the warp's lanes (small meshes,
+  // the enclosures of a batch) the idle lanes cost more than the wider
+  // loads save.  NIM_CELL_SWEEP=quad / =pair force them.
+  auto lane_use = [&](int np) {
+    const int lanes = d.NT / np;
+    return (double)lanes / (32.0 * ((lanes + 31) / 32));
+  };
+  x->cell_quad = x->cell_pair && d.NT % 4 == 0 && cell != "pair" && (cell == "quad" || lane_use(4) >= 0.75);
   x->face_quad = x->cell_quad && force != "tile" && force != "gather";
+  x->press_pair = x->cell_pair && (cell == "pair" || cell == "quad" || lane_use(2) >= 0.75);
   return NIM_OK;
 }
 

@@ -136,15 +136,16 @@ def test_pair_and_gather_cell_sweeps_are_bitwise_equal(monkeypatch, precision, d
 def test_quad_and_pair_float_cell_sweeps_are_bitwise_equal(monkeypatch, dims):
     """The mixed path's FP32 passes with the four-cells-a-thread sweeps
     (k_vel_cellN, k_vel_faceN, k_p_srcN, k_p_faceN, k_T_cellN, k_T_faceN:
-    float4 loads; the default for n_theta % 4 == 0) against k_vel_cell2,
+    float4 loads; the default for n_theta % 4 == 0 when n_theta / 4 fills
+    3/4 of a warp, forced here) against k_vel_cell2,
     k_vel_face, k_p_src, k_p_face, k_T_cell and k_T_face: whole steps to
     the bit (theta seams, walls, a partial 128-cell patch)."""
     case = config.small_case(*dims, steps=2)
     outs = []
     for form, kernels in (("pair", ("k_vel_cell2", "k_vel_face", "k_p_src", "k_p_face", "k_T_cell", "k_T_face")),
-                          ("", ("k_vel_cellN", "k_vel_faceN", "k_p_srcN", "k_p_faceN", "k_T_cellN", "k_T_faceN"))):
-        monkeypatch.setenv("NIM_CELL_SWEEP", form)
-        if form:
+                          ("quad", ("k_vel_cellN", "k_vel_faceN", "k_p_srcN", "k_p_faceN", "k_T_cellN", "k_T_faceN"))):
+        monkeypatch.setenv("NIM_CELL_SWEEP", form)  # quad: forced on these narrow meshes
+        if form == "pair":
             monkeypatch.setenv("NIM_FACE_SWEEP", "gather")
         else:
             monkeypatch.delenv("NIM_FACE_SWEEP", raising=False)
@@ -160,6 +161,29 @@ def test_quad_and_pair_float_cell_sweeps_are_bitwise_equal(monkeypatch, dims):
     assert all(r[1] > 0 for r in outs[0][0])  # the FP32 phase ran
     for a, b in zip(outs[0][1], outs[1][1]):
         assert np.array_equal(a, b)
+
+
+def test_n_cell_forms_follow_lane_use(monkeypatch):
+    """Without an override the NP-cells-a-thread sweeps run only when
+    n_theta / NP threads fill at least 3/4 of a warp's lanes: four float
+    cells at n_theta = 128 and 96, not at 40; two FP64 cells in the pressure
+    sweeps at n_theta = 64 and 48, not at 40."""
+    monkeypatch.delenv("NIM_FACE_SWEEP", raising=False)
+    monkeypatch.delenv("NIM_CELL_SWEEP", raising=False)
+    for nt, quad in ((128, True), (96, True), (40, False)):
+        case = config.small_case(nt, 8, 6)
+        s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()), case.params(precision=_abi.PRECISION_MIXED))
+        s.initialize_nse()
+        prof = s.profile_iterations(1)  # the FP32 passes
+        assert ("k_vel_cellN" in prof) == quad and ("k_p_faceN" in prof) == quad, (nt, list(prof))
+        s.close()
+    for nt, pair in ((64, True), (48, True), (40, False)):
+        case = config.small_case(nt, 8, 6)
+        s = nimgpu.NimSolver(nimgpu.Mesh(case.mesh_params()), case.params())
+        s.initialize_nse()
+        prof = s.profile_iterations(1)
+        assert ("k_p_srcN" in prof) == pair and ("k_p_faceN" in prof) == pair, (nt, list(prof))
+        s.close()
 
 
 def test_automatic_choice(monkeypatch):
