@@ -25,7 +25,9 @@ the host cores on the same workload, one inner iteration per step.
 
 --case batch times the batched extension instead: 64 seeded enclosures of
 uneven size (a x a x 0.75a cells, a in [24, 64]) and Ra, Pr advanced
-together by nim_batch_step, against the same 64 cases run one at a time.
+together, every pass kernel launched once for all of them
+(nim_batch_step_fused; also as 64 streams, nim_batch_step), against the
+same 64 cases run one at a time.
 
 On one GPU the line also carries "mixed": the same steps from the same
 start with nim_params.precision = NIM_PRECISION_MIXED (FP32 passes, then
@@ -399,11 +401,12 @@ def run_slab_ranks(args, rank, world, local):
 
 
 def run_batch(args, rank, world, local):
-    """The batched extension: 64 seeded enclosures advanced together by
-    nim_batch_step, against the same cases one at a time (nim_gpu_step per
-    instance).  Wall clock between device-wide synchronisations: the batch
-    spans 64 streams and its host-side scheduling is part of what is
-    measured.  With --precision mixed the batch runs the mixed path and the
+    """The batched extension: 64 seeded enclosures advanced together, with
+    every pass kernel launched once for all of them (nim_batch_step_fused,
+    the line's value) and as 64 streams of per-enclosure graphs
+    (nim_batch_step), against the same cases one at a time (nim_gpu_step per
+    instance).  Wall clock between device-wide synchronisations: the
+    host-side scheduling is part of what is measured.  With --precision mixed the batch runs the mixed path and the
     one-at-a-time baseline stays FP64."""
     import torch
     import nimgpu
@@ -429,16 +432,25 @@ def run_batch(args, rank, world, local):
     def cells_iters(recs_per_instance):
         return sum(c.ncells * sum(r.iters for r in recs) for c, recs in zip(cases, recs_per_instance))
 
-    solvers = build(prec)
-    # warm-up steps double as the autotuner's trials of the graph length
-    best_g, tune, _ = nimgpu.autotune_batch(solvers, candidates=(4, 8, 16, 32), steps_each=1)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    recs_b = nimgpu.batch_step(solvers, steps)
-    torch.cuda.synchronize()
-    tb = time.perf_counter() - t0
-    for s in solvers:
-        s.close()
+    def timed_batch(fused):
+        solvers = build(prec)
+        # warm-up steps double as the autotuner's trials of the graph length
+        best_g, tune, _ = nimgpu.autotune_batch(solvers, candidates=(4, 8, 16, 32), steps_each=1, fused=fused)
+        torch.cuda.synchronize()
+        l0 = sum(s.launch_count() for s in solvers)
+        t0 = time.perf_counter()
+        recs = nimgpu.batch_step(solvers, steps, fused=fused)
+        torch.cuda.synchronize()
+        tb = time.perf_counter() - t0
+        launches = sum(s.launch_count() for s in solvers) - l0
+        for s in solvers:
+            s.close()
+        return recs, tb, best_g, tune, launches
+
+    # the fused launches (one persistent launch per pass kernel for all 64),
+    # then the multi-stream form (64 streams of per-enclosure graphs)
+    recs_b, tb, best_g, tune, launches_f = timed_batch(True)
+    recs_s, ts, best_gs, tune_s, _ = timed_batch(False)
     solvers = build(_abi.PRECISION_FP64)
     for s in solvers:
         s.solve_nse(4)  # the batch's warm-up / tuning steps
@@ -449,8 +461,10 @@ def run_batch(args, rank, world, local):
     t1 = time.perf_counter() - t0
     for s in solvers:
         s.close()
-    vb, v1 = cells_iters(recs_b) / tb, cells_iters(recs_1) / t1
+    vb, v1, vs = cells_iters(recs_b) / tb, cells_iters(recs_1) / t1, cells_iters(recs_s) / ts
     same = [[r.iters for r in a] == [r.iters for r in b] for a, b in zip(recs_b, recs_1)]
+    key = lambda rr: [(r.iters, r.iters_fp32, r.nu_inner, r.nu_outer, r.dilatation) for r in rr]
+    same_streams = all(key(a) == key(b) for a, b in zip(recs_b, recs_s))
     nu_err = max(abs(a[-1].nu_inner - b[-1].nu_inner) / abs(b[-1].nu_inner) for a, b in zip(recs_b, recs_1))
     line = {
         "metric": METRIC, "value": vb, "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": max(args.warmup, 1),
@@ -463,6 +477,13 @@ def run_batch(args, rank, world, local):
                                "Pr in {0.71, 7.0}, dt=1e-3",
                    "cells": sum(c.ncells for c in cases), "instances": len(cases),
                    "timing": "wall clock between device synchronisations"},
+        "form": "fused: one persistent launch per pass kernel over all enclosures (nim_batch_step_fused)",
+        "gpu_launches": launches_f,
+        "streams": {"value": vs, "unit": UNIT, "ms_per_step": 1e3 * ts / steps,
+                    "form": "64 streams of per-enclosure graphs (nim_batch_step)",
+                    "autotune_graph_iters": best_gs,
+                    "records_equal_to_fused": same_streams},
+        "fused_vs_streams": vb / vs,
         "one_at_a_time": {"value": v1, "unit": UNIT, "ms_per_step": 1e3 * t1 / steps, "precision": "fp64"},
         "nu_inner_rel_err_vs_one_at_a_time": nu_err,
         "batch_speedup": vb / v1,

@@ -263,6 +263,24 @@ int nim_gpu_set_graph_iters(nim_ctx *ctx, int32_t n);
    NIM_OK. */
 int nim_batch_step(int32_t n, nim_ctx *const *ctx, int32_t nsteps, nim_step_stats *per, int32_t *done);
 
+/* nim_batch_step with every kernel of a pass launched once for the whole
+   batch (no counterpart in the reference).  Each pass kernel runs as a
+   persistent grid (a few blocks per SM) over a work list of (enclosure,
+   block) items, rebuilt on the device at the start of every pass from each
+   enclosure's stop flag, so enclosures whose inner loop has converged drop
+   out and the rest share the GPU; the passes are replayed as CUDA graphs
+   of nim_gpu_set_graph_iters passes (the first context's setting), and
+   between graph launches the host ends the step of each enclosure whose
+   loop has stopped and starts its next one, so every enclosure advances
+   at its own pace.  The work of each enclosure, and so its result, is
+   bit-identical to nim_gpu_step's and nim_batch_step's; per and done as
+   for nim_batch_step.  All contexts on
+   one device, parallel schedule, formulation 2, the same precision, at
+   most 256 (NIM_ERR_BAD_ARG otherwise).  While the call runs, the
+   contexts' work goes to a stream of its own; each context's stream is
+   synchronised at entry and given back at return. */
+int nim_batch_step_fused(int32_t n, nim_ctx *const *ctx, int32_t nsteps, nim_step_stats *per, int32_t *done);
+
 /* ---- z-slab decomposition (no counterpart in the reference, which runs
    one enclosure on one node).  The n_z cell planes split into nslab
    contiguous slabs of n_z / nslab or one more planes (at least 2 each).

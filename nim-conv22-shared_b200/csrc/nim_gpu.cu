@@ -31,6 +31,7 @@
 #include "nim_gpu.h"
 #include "nim_common.cuh"
 #include "nim_kernels.cuh"
+#include "nim_batch.cuh"
 
 using namespace nim;
 
@@ -1369,6 +1370,18 @@ int iterations_launch(nim_ctx *x, int batches) {
   return ctrl_async(x);
 }
 
+// check_steady_state and evaluate_D after the inner loop (nse.f90:167-168),
+// queued with the copy of the control block
+int after_loop_start(nim_ctx *x) {
+  const Dims &d = x->d;
+  k_after_integrate<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->g, x->F, x->phys, x->ctl, x->nblk_c);
+  k_finish_sum<<<1, BLK, 0, x->stream>>>(x->F.part, x->nblk_c, 1, x->sums);
+  CK(cudaGetLastError());
+  x->launches += 2;
+  CK(cudaMemcpyAsync(x->host_sums, x->sums, sizeof(double), cudaMemcpyDeviceToHost, x->stream));
+  return ctrl_async(x);
+}
+
 // integrate_nse, first batch: launch ahead by the previous step's count
 int integrate_start(nim_ctx *x) {
   const int G = x->graph_G;
@@ -1409,13 +1422,7 @@ int integrate_advance(nim_ctx *x) {
     TRY(iterations_launch(x, std::max(1, (x->last_hi * 7 / 8) / x->graph_G)));
     return 1;
   }
-  const Dims &d = x->d;
-  k_after_integrate<<<x->nblk_c, BLK, 0, x->stream>>>(d, x->g, x->F, x->phys, x->ctl, x->nblk_c);
-  k_finish_sum<<<1, BLK, 0, x->stream>>>(x->F.part, x->nblk_c, 1, x->sums);
-  CK(cudaGetLastError());
-  x->launches += 2;
-  CK(cudaMemcpyAsync(x->host_sums, x->sums, sizeof(double), cudaMemcpyDeviceToHost, x->stream));
-  TRY(ctrl_async(x));
+  TRY(after_loop_start(x));
   return 0;
 }
 
@@ -1614,6 +1621,356 @@ extern "C" int nim_batch_step(int32_t n, nim_ctx *const *ctx, int32_t nsteps, ni
       if (phase[i] == FINISHED) --left;
     }
     if (!moved) std::this_thread::yield();
+  }
+  return first_error;
+}
+
+// ---- a batch in fused launches (nim_batch_step_fused): every kernel of a
+// pass launched once for all the batch's enclosures (nim_batch.cuh)
+namespace {
+struct FusedBatch {
+  int n = 0;
+  bool mixed = false;
+  int G = 4;  // passes per graph launch
+  bool wide = false;  // batched kernels at one resident block per SM fewer
+  cudaStream_t s = nullptr;
+  BatchArgs args{};
+  void *dev = nullptr;                // tables, phases, work list, states
+  int *phase_host = nullptr;          // pinned
+  BatchState *state_host = nullptr;   // pinned
+  bool use[2][BS_COUNT] = {};         // per phase (float, double): slots some enclosure runs
+  int blocks[2][BS_COUNT] = {};       // persistent grid of each slot's kernel
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // passes over phases {FP32}, {FP64}, both
+  std::vector<nim_ctx *> ctx;
+  std::vector<cudaStream_t> own;      // the contexts' streams, back in place at the end
+  size_t state_dev_offset = 0;
+  ~FusedBatch() {
+    if (s) cudaStreamSynchronize(s);
+    for (size_t i = 0; i < own.size(); ++i) ctx[i]->stream = own[i];
+    for (auto &g : graph)
+      if (g) cudaGraphExecDestroy(g);
+    if (dev) cudaFree(dev);
+    if (phase_host) cudaFreeHost(phase_host);
+    if (state_host) cudaFreeHost(state_host);
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
+template <class K>
+int persistent_blocks(K kern, int threads, int sms, int &out) {
+  int nb = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, 0));
+  out = std::max(1, nb) * sms;
+  return NIM_OK;
+}
+
+template <class R, int W>
+int fused_occupancy(FusedBatch &B, int sms) {
+  constexpr int ph = sizeof(R) == 4 ? 0 : 1;
+  int *b = B.blocks[ph];
+  TRY(persistent_blocks(kb_vel_cell2<R, W>, CB3, sms, b[BS_VEL_CELL2]));
+  TRY(persistent_blocks(kb_vel_cell<R, W>, CB3, sms, b[BS_VEL_CELL]));
+  TRY(persistent_blocks(kb_vel_face<R, W>, CB3, sms, b[BS_VEL_FACE]));
+  if constexpr (ph == 1) {
+    TRY(persistent_blocks(kb_p_src2<W>, CB3, sms, b[BS_P_SRC2]));
+    TRY(persistent_blocks(kb_p_face2<W>, CB3, sms, b[BS_P_FACE2]));
+  }
+  TRY(persistent_blocks(kb_p_src<R, W>, CB3, sms, b[BS_P_SRC]));
+  TRY(persistent_blocks(kb_p_bc<R, W>, BLK, sms, b[BS_P_BC]));
+  TRY(persistent_blocks(kb_p_bc_copy<R, W>, BLK, sms, b[BS_P_BC_COPY]));
+  TRY(persistent_blocks(kb_p_face<R, W>, CB3, sms, b[BS_P_FACE]));
+  TRY(persistent_blocks(kb_p_dpdx<R, W>, BLK, sms, b[BS_P_DPDX]));
+  TRY(persistent_blocks(kb_zero_flux<R, W>, BLK, sms, b[BS_ZERO_FLUX]));
+  TRY(persistent_blocks(kb_T_coef<R, W>, BLK, sms, b[BS_T_COEF]));
+  TRY(persistent_blocks(kb_T_cell<R, W>, CB3, sms, b[BS_T_CELL]));
+  TRY(persistent_blocks(kb_T_face<R, W>, BLK, sms, b[BS_T_FACE]));
+  return NIM_OK;
+}
+
+// the slots of one storage type, in launch_parallel's order
+template <class R, int W>
+int fused_slots(FusedBatch &B) {
+  constexpr int ph = sizeof(R) == 4 ? 0 : 1;
+  const bool *u = B.use[ph];
+  const int *b = B.blocks[ph];
+  const dim3 t3(CB, 3);
+  cudaStream_t s = B.s;
+  const BatchArgs &A = B.args;
+  if (u[BS_VEL_CELL2]) kb_vel_cell2<R, W><<<b[BS_VEL_CELL2], t3, 0, s>>>(A);
+  if (u[BS_VEL_CELL]) kb_vel_cell<R, W><<<b[BS_VEL_CELL], t3, 0, s>>>(A);
+  if (u[BS_VEL_FACE]) kb_vel_face<R, W><<<b[BS_VEL_FACE], t3, 0, s>>>(A);
+  if constexpr (ph == 1) {
+    if (u[BS_P_SRC2]) kb_p_src2<W><<<b[BS_P_SRC2], t3, 0, s>>>(A);
+  }
+  if (u[BS_P_SRC]) kb_p_src<R, W><<<b[BS_P_SRC], t3, 0, s>>>(A);
+  if (u[BS_P_BC]) kb_p_bc<R, W><<<b[BS_P_BC], BLK, 0, s>>>(A);
+  if (u[BS_P_BC_COPY]) kb_p_bc_copy<R, W><<<b[BS_P_BC_COPY], BLK, 0, s>>>(A);
+  if constexpr (ph == 1) {
+    if (u[BS_P_FACE2]) kb_p_face2<W><<<b[BS_P_FACE2], t3, 0, s>>>(A);
+  }
+  if (u[BS_P_FACE]) kb_p_face<R, W><<<b[BS_P_FACE], t3, 0, s>>>(A);
+  if (u[BS_P_DPDX]) kb_p_dpdx<R, W><<<b[BS_P_DPDX], BLK, 0, s>>>(A);
+  if (u[BS_ZERO_FLUX]) kb_zero_flux<R, W><<<b[BS_ZERO_FLUX], BLK, 0, s>>>(A);
+  if (u[BS_T_COEF]) kb_T_coef<R, W><<<b[BS_T_COEF], BLK, 0, s>>>(A);
+  if (u[BS_T_CELL]) kb_T_cell<R, W><<<b[BS_T_CELL], t3, 0, s>>>(A);
+  if (u[BS_T_FACE]) kb_T_face<R, W><<<b[BS_T_FACE], BLK, 0, s>>>(A);
+  CK(cudaGetLastError());
+  return NIM_OK;
+}
+template <class R>
+int fused_slots_of(FusedBatch &B) {
+  return B.wide ? fused_slots<R, 1>(B) : fused_slots<R, 0>(B);
+}
+
+int fused_launches(const FusedBatch &B, int phases) {
+  int k = 2;  // k_batch_plan, k_batch_iter_end
+  for (int ph = 0; ph < 2; ++ph)
+    if (phases & (1 << ph))
+      for (int q = 0; q < BS_COUNT; ++q) k += B.use[ph][q] ? 1 : 0;
+  return k;
+}
+
+// G passes over the enclosures in the given phases (bit 0: FP32, bit 1: FP64)
+int fused_graph(FusedBatch &B, int phases) {
+  cudaGraphExec_t &exec = B.graph[phases - 1];
+  if (exec) return NIM_OK;
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(B.s, cudaStreamCaptureModeThreadLocal));
+  int st = NIM_OK;
+  for (int k = 0; k < B.G && st == NIM_OK; ++k) {
+    k_batch_plan<<<1, 1024, 0, B.s>>>(B.args);
+    if (phases & 1) st = fused_slots_of<float>(B);
+    if (st == NIM_OK && (phases & 2)) st = fused_slots_of<double>(B);
+    k_batch_iter_end<<<(B.n + 127) / 128, 128, 0, B.s>>>(B.args);
+  }
+  const cudaError_t e = cudaStreamEndCapture(B.s, &g);
+  if (st != NIM_OK || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return st != NIM_OK ? st : NIM_ERR_CUDA;
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
+  cudaGraphDestroy(g);
+  return ei == cudaSuccess ? NIM_OK : NIM_ERR_CUDA;
+}
+
+int fused_upload_phase(FusedBatch &B) {
+  CK(cudaMemcpyAsync((void *)B.args.phase, B.phase_host, sizeof(int) * B.n, cudaMemcpyHostToDevice, B.s));
+  return NIM_OK;
+}
+
+// the per-enclosure tables, the work list and the persistent grid sizes;
+// every context's work moves to the batch stream until B goes out of scope
+int fused_setup(FusedBatch &B, int32_t n, nim_ctx *const *ctx) {
+  B.n = n;
+  B.ctx.assign(ctx, ctx + n);
+  B.mixed = ctx[0]->mixed;
+  B.G = ctx[0]->graph_G;
+  CK(cudaStreamCreateWithFlags(&B.s, cudaStreamNonBlocking));
+  for (int32_t i = 0; i < n; ++i) CK(cudaStreamSynchronize(ctx[i]->stream));
+  for (int32_t i = 0; i < n; ++i) {
+    B.own.push_back(ctx[i]->stream);
+    ctx[i]->stream = B.s;
+  }
+  // device block: i64[n], i32[n], grid[2][n][BS_COUNT], phase[n], state[n], plan
+  auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  const size_t o64 = 0, o32 = o64 + up(sizeof(BatchInst<double>) * n), og = o32 + up(sizeof(BatchInst<float>) * n),
+               oph = og + up(sizeof(BatchGrid) * 2 * n * BS_COUNT), ost = oph + up(sizeof(int) * n),
+               opl = ost + up(sizeof(BatchState) * n), bytes = opl + up(sizeof(BatchPlan));
+  CK(cudaMalloc(&B.dev, bytes));
+  CK(cudaMallocHost(&B.phase_host, sizeof(int) * n));
+  CK(cudaMallocHost(&B.state_host, sizeof(BatchState) * n));
+  char *base = static_cast<char *>(B.dev);
+  std::vector<BatchInst<double>> h64(n);
+  std::vector<BatchInst<float>> h32(n);
+  std::vector<BatchGrid> grids(2 * (size_t)n * BS_COUNT, BatchGrid{0u, 0u, 0u});
+  for (int32_t i = 0; i < n; ++i) {
+    const nim_ctx *x = ctx[i];
+    const Dims &d = x->d;
+    h64[i] = BatchInst<double>{d, x->g, x->F, x->phys, x->ctl};
+    if (B.mixed) h32[i] = BatchInst<float>{d, x->g32, x->F32, x->phys, x->ctl};
+    // the one-cell sweeps over runs of consecutive cells of a plane (FlatBlock)
+    const BatchGrid f3{(unsigned)((d.plane + CB - 1) / CB), 1u, (unsigned)d.NZ};
+    const BatchGrid f8{(unsigned)((d.plane + BLK - 1) / BLK), 1u, (unsigned)d.NZ};
+    const BatchGrid gp{(unsigned)(d.NT + 63) / 64, (unsigned)(d.NR + 3) / 4, (unsigned)d.NZ};
+    const BatchGrid gb{(unsigned)x->nblk_b, 1u, 1u};
+    for (int ph = 0; ph < 2; ++ph) {
+      if (ph == 0 && !B.mixed) continue;
+      BatchGrid *G = &grids[((size_t)ph * n + i) * BS_COUNT];
+      // the enclosure's sweeps in the forms the batch has, all of which give
+      // the bits of the enclosure's own pass: the two-cell forms where a row
+      // of n_theta / 2 threads fills 3/4 of a warp's lanes, else the
+      // one-cell forms over consecutive cells (the TMA-staged and four-cell
+      // sweeps of large meshes are replaced by their gather forms)
+      const int lanes2 = d.NT / 2;
+      const bool rows2 = (double)lanes2 / (32.0 * ((lanes2 + 31) / 32)) >= 0.75;
+      if ((x->cell_pair || x->cell_quad) && rows2)
+        G[BS_VEL_CELL2] = gp;
+      else
+        G[BS_VEL_CELL] = f3;
+      G[BS_VEL_FACE] = f3;
+      if (ph == 1 && x->press_pair) {
+        G[BS_P_SRC2] = gp;
+        G[BS_P_FACE2] = gp;
+      } else {
+        G[BS_P_SRC] = f3;
+        G[BS_P_FACE] = f3;
+      }
+      G[BS_P_BC] = gb;
+      G[BS_P_BC_COPY] = gb;
+      if (x->phys.dpdx_tolerance) G[BS_P_DPDX] = BatchGrid{(unsigned)x->nblk_c, 1u, 1u};
+      G[BS_ZERO_FLUX] = BatchGrid{(unsigned)grid(2 * d.plane), 1u, 1u};
+      G[BS_T_COEF] = BatchGrid{3u, (unsigned)x->nblk_c, 1u};
+      G[BS_T_CELL] = f3;
+      G[BS_T_FACE] = f8;
+      for (int q = 0; q < BS_COUNT; ++q) B.use[ph][q] = B.use[ph][q] || G[q].x > 0;
+    }
+  }
+  CK(cudaMemcpyAsync(base + o64, h64.data(), sizeof(BatchInst<double>) * n, cudaMemcpyHostToDevice, B.s));
+  if (B.mixed)
+    CK(cudaMemcpyAsync(base + o32, h32.data(), sizeof(BatchInst<float>) * n, cudaMemcpyHostToDevice, B.s));
+  CK(cudaMemcpyAsync(base + og, grids.data(), sizeof(BatchGrid) * grids.size(), cudaMemcpyHostToDevice, B.s));
+  CK(cudaMemsetAsync(base + oph, 0, sizeof(int) * n, B.s));
+  CK(cudaStreamSynchronize(B.s));  // the host vectors go out of scope
+  B.args.i64 = reinterpret_cast<const BatchInst<double> *>(base + o64);
+  B.args.i32 = B.mixed ? reinterpret_cast<const BatchInst<float> *>(base + o32) : nullptr;
+  B.args.grid = reinterpret_cast<const BatchGrid *>(base + og);
+  B.args.phase = reinterpret_cast<const int *>(base + oph);
+  B.args.plan = reinterpret_cast<BatchPlan *>(base + opl);
+  B.args.n = n;
+  B.state_dev_offset = ost;
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx[0]->device));
+  // NIM_BATCH_BOUNDS=wide: the batched kernels one resident block per SM
+  // below the plain kernels' bound (more registers, fewer spills)
+  const char *bounds = std::getenv("NIM_BATCH_BOUNDS");
+  B.wide = bounds && std::string(bounds) == "wide";
+  if (B.mixed) TRY((B.wide ? fused_occupancy<float, 1>(B, sms) : fused_occupancy<float, 0>(B, sms)));
+  TRY((B.wide ? fused_occupancy<double, 1>(B, sms) : fused_occupancy<double, 0>(B, sms)));
+  return NIM_OK;
+}
+}  // namespace
+
+extern "C" int nim_batch_step_fused(int32_t n, nim_ctx *const *ctx, int32_t nsteps, nim_step_stats *per,
+                                    int32_t *done) {
+  if (n <= 0 || n > kBatchMax || !ctx || nsteps < 0) return NIM_ERR_BAD_ARG;
+  for (int32_t i = 0; i < n; ++i) {
+    if (!ctx[i] || lone_slab(ctx[i])) return NIM_ERR_BAD_ARG;
+    if (!ctx[i]->initialized || ctx[i]->in_step) return NIM_ERR_STATE;
+    if (ctx[i]->device != ctx[0]->device || ctx[i]->seq || ctx[i]->phys.formulation != 2 ||
+        ctx[i]->mixed != ctx[0]->mixed)
+      return NIM_ERR_BAD_ARG;
+    for (int32_t j = 0; j < i; ++j)
+      if (ctx[j] == ctx[i]) return NIM_ERR_BAD_ARG;
+  }
+  if (done)
+    for (int32_t i = 0; i < n; ++i) done[i] = 0;
+  if (nsteps == 0) return NIM_OK;
+  CK(cudaSetDevice(ctx[0]->device));
+  FusedBatch B;
+  TRY(fused_setup(B, n, ctx));
+  BatchState *state_dev = reinterpret_cast<BatchState *>(static_cast<char *>(B.dev) + B.state_dev_offset);
+  // Per enclosure: RUN (its inner loop is in the fused passes, phase 1 or
+  // 2), AFTER (check_steady_state / evaluate_D queued), END
+  // (update_time_step / find_Nu2 queued), FIN.  Every enclosure goes
+  // through its own steps at its own pace: one whose loop has stopped ends
+  // its step and starts the next while the others keep iterating.
+  enum { RUN, AFTER, END, FIN };
+  std::vector<int> st(n, RUN), k(n, 0);
+  std::vector<nim_step_stats> rec(n);
+  int first_error = NIM_OK;
+  int *ph = B.phase_host;
+  auto start_step = [&](int32_t i) -> int {
+    nim_ctx *x = ctx[i];
+    std::memset(&rec[i], 0, sizeof(nim_step_stats));
+    TRY(nim_gpu_begin_step(x));
+    x->run.capped = false;
+    x->run.launched = 0;
+    x->run.cap = (x->params.max_iters > 0) ? (long long)x->params.max_iters + 2 * B.G : 100000000LL;
+    if (B.mixed) {  // FP32 phase from the narrowed FP64 iterate
+      TRY(mirror_state(x, 0));
+      k_lowp_begin<<<1, 1, 0, B.s>>>(x->ctl);
+      CK(cudaGetLastError());
+      x->launches += 1;
+    }
+    ph[i] = B.mixed ? 1 : 2;
+    st[i] = RUN;
+    return NIM_OK;
+  };
+  // a step's record is complete: the next step, or the enclosure is done
+  auto finish = [&](int32_t i, int status) -> int {
+    if (per) per[(size_t)i * nsteps + k[i]] = rec[i];
+    ++k[i];
+    if (done) done[i] = k[i];
+    if (status != NIM_OK && first_error == NIM_OK) first_error = status;
+    if (status != NIM_OK || rec[i].steady || k[i] == nsteps) {
+      st[i] = FIN;
+      return NIM_OK;
+    }
+    return start_step(i);
+  };
+  for (int32_t i = 0; i < n; ++i) TRY(start_step(i));
+  TRY(fused_upload_phase(B));
+  for (;;) {
+    int phases = 0, busy = 0;
+    for (int32_t i = 0; i < n; ++i) {
+      if (st[i] == RUN) phases |= (ph[i] == 1) ? 1 : 2;
+      busy += (st[i] != FIN) ? 1 : 0;
+    }
+    if (!busy) break;
+    if (phases) {
+      TRY(fused_graph(B, phases));
+      CK(cudaGraphLaunch(B.graph[phases - 1], B.s));
+      ctx[0]->launches += (long long)B.G * fused_launches(B, phases);
+      for (int32_t i = 0; i < n; ++i)
+        if (st[i] == RUN) ctx[i]->run.launched += B.G;
+      k_batch_state<<<(n + 127) / 128, 128, 0, B.s>>>(B.args, state_dev);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(B.state_host, state_dev, sizeof(BatchState) * n, cudaMemcpyDeviceToHost, B.s));
+    }
+    // every copy queued so far (states, control blocks, sums) has landed
+    CK(cudaStreamSynchronize(B.s));
+    bool changed = false;
+    for (int32_t i = 0; i < n; ++i) {
+      nim_ctx *x = ctx[i];
+      if (st[i] == RUN) {
+        const bool stopped = B.state_host[i].done != 0;
+        if (stopped && ph[i] == 1 && B.state_host[i].status == NIM_OK) {
+          // FP32 phase over: widen its iterate, FP64 passes to the reference's test
+          TRY(mirror_state(x, 1));
+          k_lowp_end<<<1, 1, 0, B.s>>>(x->ctl);
+          CK(cudaGetLastError());
+          x->launches += 1;
+          ph[i] = 2;
+          changed = true;
+        } else if (stopped || x->run.launched >= x->run.cap) {
+          x->run.capped = !stopped;
+          ph[i] = 0;
+          changed = true;
+          TRY(after_loop_start(x));
+          st[i] = AFTER;
+        }
+      } else if (st[i] == AFTER) {
+        const int s = integrate_finish(x, &rec[i]);
+        rec[i].status = s;
+        if (s != NIM_OK) {
+          x->in_step = false;
+          TRY(finish(i, s));
+        } else if (steady_exit(x, rec[i])) {
+          rec[i].steady = 1;
+          x->in_step = false;
+          TRY(finish(i, NIM_OK));
+        } else {
+          TRY(end_start(x));
+          st[i] = END;
+        }
+        changed = changed || st[i] == RUN;
+      } else if (st[i] == END) {
+        end_finish(x, &rec[i]);
+        TRY(finish(i, NIM_OK));
+        changed = changed || st[i] == RUN;
+      }
+    }
+    if (changed) TRY(fused_upload_phase(B));
   }
   return first_error;
 }

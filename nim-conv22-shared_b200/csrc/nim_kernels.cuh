@@ -1259,6 +1259,37 @@ __global__ void k_wait_selftest(Ctrl *ctl, int tries) {
 
 // nim_exp over n arguments (self-test of the exp the NIM coefficients use)
 
+// The block coordinates a pass kernel's body works on.  LaunchBlock reads
+// the launch's own blockIdx where the body uses a coordinate (the plain
+// kernels: the same code as reading blockIdx directly); BatchBlock holds the
+// coordinates of one block of one enclosure's grid, decoded by a fused batch
+// launch (k_batch_*) from its work list.
+struct LaunchBlockX {
+  __device__ __forceinline__ operator unsigned() const { return ::blockIdx.x; }
+};
+struct LaunchBlockY {
+  __device__ __forceinline__ operator unsigned() const { return ::blockIdx.y; }
+};
+struct LaunchBlockZ {
+  __device__ __forceinline__ operator unsigned() const { return ::blockIdx.z; }
+};
+struct LaunchBlock {
+  LaunchBlockX x;
+  LaunchBlockY y;
+  LaunchBlockZ z;
+};
+struct BatchBlock {
+  unsigned x, y, z;
+};
+// A block of a fused batch launch over cells in cell order: x numbers the
+// runs of blockDim.x consecutive cells of plane z (y unused).  Every lane
+// has a cell whatever n_theta is, where the 32-wide theta patches of
+// patch_cell leave lanes idle on narrow meshes (n_theta = 40: 5 of 8 warps'
+// lanes busy); only patch_cell's kernels take it.
+struct FlatBlock {
+  unsigned x, y, z;
+};
+
 __device__ __forceinline__ double errv(double nw, double old, bool first) { return fabs(nw - (first ? 0.0 : old)); }
 __device__ __forceinline__ double errv(const DualD &nw, const DualD &old, bool first) {
   return errv(nw.v, old.v, first);
@@ -1270,12 +1301,22 @@ __device__ __forceinline__ double nmax(double a, double b) { return (b > a || b 
 // cells of one z-plane: grid (ceil(NT/32), ceil(NR/R), NZ), threadIdx.x
 // spans the patch (R = blockDim.x / 32).  No division by run-time sizes, and
 // the +-r neighbours of a cell mostly sit in the same block.
-__device__ __forceinline__ bool patch_cell(const Dims &d, Cell &x) {
-  const int i = blockIdx.x * 32 + (threadIdx.x & 31);
-  const int j = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int k = blockIdx.z;
+// bi: the block's coordinates, blockIdx itself (LaunchBlock) or those of a
+// block of one enclosure's grid inside a fused batch launch (BatchBlock)
+template <class BI>
+__device__ __forceinline__ bool patch_cell(const Dims &d, Cell &x, const BI bi) {
+  const int i = bi.x * 32 + (threadIdx.x & 31);
+  const int j = bi.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int k = bi.z;
   x = Cell::at(d, i, j, k);
   return i < d.NT && j < d.NR;
+}
+__device__ __forceinline__ bool patch_cell(const Dims &d, Cell &x) { return patch_cell(d, x, LaunchBlock{}); }
+__device__ __forceinline__ bool patch_cell(const Dims &d, Cell &x, const FlatBlock bi) {
+  const int t = (int)bi.x * (int)blockDim.x + (int)threadIdx.x;  // cell of plane z in cell order
+  const int j = t / d.NT, i = t - j * d.NT;
+  x = Cell::at(d, i, j, (int)bi.z);
+  return j < d.NR;
 }
 
 // ---- K1: velocity sources + cell update (update_velocity_sources
@@ -1288,8 +1329,8 @@ __device__ __forceinline__ bool patch_cell(const Dims &d, Cell &x) {
 // FORM 1 (nim_formulation = 1): the a_t cell update of integrate_velocity_
 // field_i (nse.f90:341-378); the R sums are stored too, for the face sweep
 // reads them at both cells of a face.
-template <bool SRC_ONLY, int FORM, class R>
-__global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+template <bool SRC_ONLY, int FORM, class R, class BI>
+__device__ __forceinline__ void vel_cell_body(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P, Ctrl *ctl, const BI blockIdx) {
   using V = Ar<R>;
   if (ctl->done) return;
   __shared__ BlockRed red;
@@ -1298,7 +1339,7 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, GeoT<R> g, FieldsT<
   const bool first = ctl->first;
   const int q = threadIdx.y;
   Cell x;
-  const bool act = patch_cell(d, x);
+  const bool act = patch_cell(d, x, blockIdx);
   const int c = x.c;
   double e[3] = {0., 0., 0.};
   if (act) {
@@ -1333,6 +1374,10 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, GeoT<R> g, FieldsT<
   }
   // blocks of one z plane: a plane another slab owns adds nothing
   if (!SRC_ONLY && d.owns(blockIdx.z)) block_max<3, CB3>(red, e, ctl->err[par]);
+}
+template <bool SRC_ONLY, int FORM, class R>
+__global__ void __launch_bounds__(CB3, 3) k_vel_cell(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  vel_cell_body<SRC_ONLY, FORM, R>(d, g, F, P, ctl, LaunchBlock{});
 }
 
 // ---- K1, vectorised form (parallel schedule, formulation 2): k_vel_cell
@@ -1378,8 +1423,8 @@ __device__ __forceinline__ V tang_vals(bool lo, bool hi, V v0, V vp1, V vp2, V v
 // SLAB: a z-slab context, whose maxima skip the planes a neighbour owns (a
 // separate instantiation: at this kernel's register bound the test alone
 // costs spills)
-template <class R, bool SLAB = false>
-__global__ void __launch_bounds__(CB3, minb<R>(VC2_MINB, VC2_MINB_F)) k_vel_cell2(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+template <class R, bool SLAB = false, class BI = LaunchBlock>
+__device__ __forceinline__ void vel_cell2_body(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P, Ctrl *ctl, const BI blockIdx) {
   using V = Ar<R>;
   if (ctl->done) return;
   __shared__ BlockRed red;
@@ -1565,6 +1610,10 @@ __global__ void __launch_bounds__(CB3, minb<R>(VC2_MINB, VC2_MINB_F)) k_vel_cell
     e[q] = nmax(errv(nw0, cv0, first), errv(nw1, cv1, first));
   }
   if (!SLAB || d.owns(k)) block_max<3, CB3>(red, e, ctl->err[par]);
+}
+template <class R, bool SLAB = false>
+__global__ void __launch_bounds__(CB3, minb<R>(VC2_MINB, VC2_MINB_F)) k_vel_cell2(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  vel_cell2_body<R, SLAB>(d, g, F, P, ctl, LaunchBlock{});
 }
 
 // ---- K1, NP cells per thread: k_vel_cell2's sweep over NP theta-adjacent
@@ -1829,8 +1878,8 @@ __global__ void __launch_bounds__(CB3, VCN_MINB) k_vel_cellN(Dims d, GeoT<R> g, 
 
 // ---- K2: +xi face updates of u, v, w (nse.f90:878-1005).
 // Block (CB, 3): threadIdx.y = direction.
-template <class R>
-__global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+template <class R, class BI>
+__device__ __forceinline__ void vel_face_body(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P, Ctrl *ctl, const BI blockIdx) {
   using V = Ar<R>;
   if (ctl->done) return;
   __shared__ BlockRed red;
@@ -1838,7 +1887,7 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, GeoT<R> g, FieldsT<
   const int par = parity(ctl);
   const bool first = ctl->first;
   Cell x;
-  const bool act = patch_cell(d, x);
+  const bool act = patch_cell(d, x, blockIdx);
   const int c = x.c;
   double e[3] = {0., 0., 0.};
   if (act) {
@@ -1861,6 +1910,10 @@ __global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, GeoT<R> g, FieldsT<
     });
   }
   if (d.owns(blockIdx.z)) block_max<3, CB3>(red, e, ctl->err[par]);
+}
+template <class R>
+__global__ void __launch_bounds__(CB3, 3) k_vel_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  vel_face_body<R>(d, g, F, P, ctl, LaunchBlock{});
 }
 
 // ---- K2, z-marching form: the same face updates, one block per patch of
@@ -2354,8 +2407,8 @@ __global__ void __launch_bounds__(3 * CT_T, CT_MINB)
 // calculate_R_D_p2 1863-1997).  Block (CB, 3): thread y forms the gradient of
 // velocity component y and two of the six cross derivatives of p (y = 1 also
 // d(bz)/dz); thread 0 combines them in the reference's order.
-template <class R>
-__global__ void __launch_bounds__(CB3, minb<R>(4, PSRC_MINB_F)) k_p_src(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+template <class R, class BI>
+__device__ __forceinline__ void p_src_body(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P, Ctrl *ctl, const BI blockIdx) {
   if (ctl->done) return;
   using A = Ar<R>;
   __shared__ A sh[3][3][CB];  // gradients of u, v, w
@@ -2364,7 +2417,7 @@ __global__ void __launch_bounds__(CB3, minb<R>(4, PSRC_MINB_F)) k_p_src(Dims d, 
   const int par = parity(ctl);
   const int q = threadIdx.y, tx = threadIdx.x;
   Cell x;
-  const bool active = patch_cell(d, x);
+  const bool active = patch_cell(d, x, blockIdx);
   const int c = x.c;
   int f[7];
   const size_t Nc = d.Nc, NF = d.NF;
@@ -2415,6 +2468,10 @@ __global__ void __launch_bounds__(CB3, minb<R>(4, PSRC_MINB_F)) k_p_src(Dims d, 
     F.Rp[c] = RDp + RBp;
   }
 }
+template <class R>
+__global__ void __launch_bounds__(CB3, minb<R>(4, PSRC_MINB_F)) k_p_src(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  p_src_body<R>(d, g, F, P, ctl, LaunchBlock{});
+}
 
 // ---- K3, NP cells per thread (the float mirror with NP = 4, the FP64 path
 // with NP = 2; n_theta % NP == 0):
@@ -2423,8 +2480,8 @@ __global__ void __launch_bounds__(CB3, minb<R>(4, PSRC_MINB_F)) k_p_src(Dims d, 
 // gradients of velocity component y (y = 1 also d(bz)/dz) and two of the six
 // cross derivatives of p for the NP cells; thread 0 combines them in the
 // reference's order.  Each cell's arithmetic is k_p_src's.
-template <class R, int NP>
-__global__ void __launch_bounds__(CB3, PSN_MINB) k_p_srcN(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+template <class R, int NP, class BI>
+__device__ __forceinline__ void p_srcN_body(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P, Ctrl *ctl, const BI blockIdx) {
   using V = Ar<R>;
   if (ctl->done) return;
   __shared__ V sh[3][3][CB * NP];  // gradients of u, v, w
@@ -2627,6 +2684,10 @@ __global__ void __launch_bounds__(CB3, PSN_MINB) k_p_srcN(Dims d, GeoT<R> g, Fie
     stN<R, NP>(F.Rp, c, rp);
   }
 }
+template <class R, int NP>
+__global__ void __launch_bounds__(CB3, PSN_MINB) k_p_srcN(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  p_srcN_body<R, NP>(d, g, F, P, ctl, LaunchBlock{});
+}
 
 // ---- apply_pressure_bc for wall face b (bc.f90:148-339): the new value
 // from the pressures pr, the new velocities fu/fv/fwv and the temperatures fT
@@ -2671,8 +2732,8 @@ __device__ __forceinline__ Ar<R> p_bc_value(const Dims &d, const GeoT<R> &g, con
 }
 
 // ---- K4: apply_pressure_bc, every wall face from the values before the pass
-template <class R>
-__global__ void __launch_bounds__(BLK) k_p_bc(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+template <class R, class BI>
+__device__ __forceinline__ void p_bc_body(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P, Ctrl *ctl, const BI blockIdx) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
@@ -2692,9 +2753,13 @@ __global__ void __launch_bounds__(BLK) k_p_bc(Dims d, GeoT<R> g, FieldsT<R> F, P
   }
   block_max<1>(red, e, ctl->err[par] + 3);
 }
-
 template <class R>
-__global__ void k_p_bc_copy(Dims d, FieldsT<R> F, Ctrl *ctl) {
+__global__ void __launch_bounds__(BLK) k_p_bc(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  p_bc_body<R>(d, g, F, P, ctl, LaunchBlock{});
+}
+
+template <class R, class BI>
+__device__ __forceinline__ void p_bc_copy_body(const Dims &d, const FieldsT<R> &F, Ctrl *ctl, const BI blockIdx) {
   if (ctl->done) return;
   const int par = parity(ctl);
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2702,6 +2767,10 @@ __global__ void k_p_bc_copy(Dims d, FieldsT<R> F, Ctrl *ctl) {
   const BFace B = bface(d, b);
   const int f = B.cell.face(d, B.pos);
   F.f[3][par * d.NF + f] = F.f[3][(1 - par) * d.NF + f];
+}
+template <class R>
+__global__ void k_p_bc_copy(Dims d, FieldsT<R> F, Ctrl *ctl) {
+  p_bc_copy_body<R>(d, F, ctl, LaunchBlock{});
 }
 
 // (coefficient, face, cell) of the ten off-diagonal terms of the pressure
@@ -2814,15 +2883,15 @@ __global__ void __launch_bounds__(CB3, 2) k_vel1_face(Dims d, GeoT<R> g, FieldsT
 
 // ---- K5: integrate_pressure_field_i, cur -> next.
 // Block (CB, 3): threadIdx.y = direction.
-template <class R>
-__global__ void __launch_bounds__(CB3, minb<R>(5, PFACE_MINB_F)) k_p_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+template <class R, class BI>
+__device__ __forceinline__ void p_face_body(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P, Ctrl *ctl, const BI blockIdx) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
   const int par = parity(ctl);
   const bool first = ctl->first;
   Cell x;
-  const bool act = patch_cell(d, x);
+  const bool act = patch_cell(d, x, blockIdx);
   double e[1] = {0.};
   if (act) {
     by_dir(threadIdx.y, [&](auto D) {
@@ -2838,6 +2907,10 @@ __global__ void __launch_bounds__(CB3, minb<R>(5, PFACE_MINB_F)) k_p_face(Dims d
   }
   if (d.owns(blockIdx.z)) block_max<1, CB3>(red, e, ctl->err[par] + 3);
 }
+template <class R>
+__global__ void __launch_bounds__(CB3, minb<R>(5, PFACE_MINB_F)) k_p_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  p_face_body<R>(d, g, F, P, ctl, LaunchBlock{});
+}
 
 // ---- K5, NP cells per thread (the float mirror with NP = 4, the FP64 path
 // with NP = 2; n_theta % NP == 0):
@@ -2848,8 +2921,8 @@ __global__ void __launch_bounds__(CB3, minb<R>(5, PFACE_MINB_F)) k_p_face(Dims d
 // the metric differences; the theta faces' new values are stored one by one
 // (they start one cell off the vector boundary).  Each face's arithmetic is
 // p_face_value's.
-template <class R, int NP>
-__global__ void __launch_bounds__(CB3, PFN_MINB) k_p_faceN(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+template <class R, int NP, class BI>
+__device__ __forceinline__ void p_faceN_body(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P, Ctrl *ctl, const BI blockIdx) {
   using V = Ar<R>;
   if (ctl->done) return;
   __shared__ BlockRed red;
@@ -3028,10 +3101,14 @@ __global__ void __launch_bounds__(CB3, PFN_MINB) k_p_faceN(Dims d, GeoT<R> g, Fi
   });
   if (d.owns(blockIdx.z)) block_max<1, CB3>(red, e, ctl->err[par] + 3);
 }
+template <class R, int NP>
+__global__ void __launch_bounds__(CB3, PFN_MINB) k_p_faceN(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  p_faceN_body<R, NP>(d, g, F, P, ctl, LaunchBlock{});
+}
 
 // ---- K5b (is_dpdx_tolerance): cell pressure gradients (nse.f90:292-307)
-template <class R>
-__global__ void __launch_bounds__(BLK) k_p_dpdx(Dims d, GeoT<R> g, FieldsT<R> F, Ctrl *ctl) {
+template <class R, class BI>
+__device__ __forceinline__ void p_dpdx_body(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, Ctrl *ctl, const BI blockIdx) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
@@ -3055,10 +3132,14 @@ __global__ void __launch_bounds__(BLK) k_p_dpdx(Dims d, GeoT<R> g, FieldsT<R> F,
   }
   block_max<1>(red, e, ctl->err[par] + 5);
 }
+template <class R>
+__global__ void __launch_bounds__(BLK) k_p_dpdx(Dims d, GeoT<R> g, FieldsT<R> F, Ctrl *ctl) {
+  p_dpdx_body<R>(d, g, F, ctl, LaunchBlock{});
+}
 
 // ---- K6: apply_zero_flux (bc.f90:345-390) on the z walls, in place
-template <class R>
-__global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, GeoT<R> g, FieldsT<R> F, Ctrl *ctl) {
+template <class R, class BI>
+__device__ __forceinline__ void zero_flux_body(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, Ctrl *ctl, const BI blockIdx) {
   if (ctl->done) return;
   __shared__ BlockRed red;
   red_init<1>(red);
@@ -3080,6 +3161,10 @@ __global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, GeoT<R> g, FieldsT<R>
   }
   block_max<1>(red, e, ctl->err[par] + 4);
 }
+template <class R>
+__global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, GeoT<R> g, FieldsT<R> F, Ctrl *ctl) {
+  zero_flux_body<R>(d, g, F, ctl, LaunchBlock{});
+}
 
 // ---- K7a: calculate_temperature_nim_constants_formulation2, first part
 // (nim.f90:334-464): MT_A(1:6) of every cell and direction, from the cell
@@ -3090,8 +3175,8 @@ __global__ void __launch_bounds__(BLK) k_zero_flux(Dims d, GeoT<R> g, FieldsT<R>
 // directions of the same cells run side by side and share their loads.
 // The float instantiation (the FP32 phase) computes in float with
 // nim_direction_f32, which makes it bound by its bytes.
-template <class R>
-__global__ void __launch_bounds__(BLK, 4) k_T_coef(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+template <class R, class BI>
+__device__ __forceinline__ void T_coef_body(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P, Ctrl *ctl, const BI blockIdx) {
   if (ctl->done) return;
   const int c = blockIdx.y * BLK + threadIdx.x;
   if (c >= d.Nc) return;
@@ -3119,6 +3204,10 @@ __global__ void __launch_bounds__(BLK, 4) k_T_coef(Dims d, GeoT<R> g, FieldsT<R>
     for (int q = 0; q < 6; ++q) F.MTA[(3 * q + dd - 1) * Nc + c] = A[q];
   }
 }
+template <class R>
+__global__ void __launch_bounds__(BLK, 4) k_T_coef(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  T_coef_body<R>(d, g, F, P, ctl, LaunchBlock{});
+}
 
 // ---- K7b: the rest of calculate_temperature_nim_constants_formulation2
 // (MT_F4, MT_F1..3, nim.f90:466-500), calculate_R_D_T (nse.f90:2000-2134)
@@ -3128,8 +3217,8 @@ __global__ void __launch_bounds__(BLK, 4) k_T_coef(Dims d, GeoT<R> g, FieldsT<R>
 // in the reference's order.
 // SRC_ONLY (reference-order schedule): store MT_F4 and R_D_T and leave the
 // update to k_seq_T.
-template <bool SRC_ONLY, class R>
-__global__ void __launch_bounds__(CB3, minb<R>(5, TCELL_MINB_F)) k_T_cell(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+template <bool SRC_ONLY, class R, class BI>
+__device__ __forceinline__ void T_cell_body(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P, Ctrl *ctl, const BI blockIdx) {
   using V = Ar<R>;
   if (ctl->done) return;
   __shared__ BlockRed red;
@@ -3141,7 +3230,7 @@ __global__ void __launch_bounds__(CB3, minb<R>(5, TCELL_MINB_F)) k_T_cell(Dims d
   const bool first = ctl->first;
   const int tx = threadIdx.x;
   Cell x;
-  const bool active = patch_cell(d, x);
+  const bool active = patch_cell(d, x, blockIdx);
   const int c = x.c;
   double e[1] = {0.};
   const size_t Nc = d.Nc, NF = d.NF;
@@ -3212,6 +3301,10 @@ __global__ void __launch_bounds__(CB3, minb<R>(5, TCELL_MINB_F)) k_T_cell(Dims d
     }
   }
   if (!SRC_ONLY && d.owns(blockIdx.z)) block_max<1, CB3>(red, e, ctl->err[par] + 4);
+}
+template <bool SRC_ONLY, class R>
+__global__ void __launch_bounds__(CB3, minb<R>(5, TCELL_MINB_F)) k_T_cell(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  T_cell_body<SRC_ONLY, R>(d, g, F, P, ctl, LaunchBlock{});
 }
 
 // ---- K7b, NP cells per thread (the float mirror's parallel passes,
@@ -3458,8 +3551,8 @@ __global__ void __launch_bounds__(CB3, TCN_MINB) k_T_cellN(Dims d, GeoT<R> g, Fi
 
 // ---- K8: +xi face updates of T (nse.f90:1033-1088), cur -> next; the z-wall
 // values set by apply_zero_flux travel to the next half too
-template <class R>
-__global__ void __launch_bounds__(BLK, minb<R>(4, TFACE_MINB_F)) k_T_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+template <class R, class BI>
+__device__ __forceinline__ void T_face_body(const Dims &d, const GeoT<R> &g, const FieldsT<R> &F, const Phys &P, Ctrl *ctl, const BI blockIdx) {
   using V = Ar<R>;
   if (ctl->done) return;
   __shared__ BlockRed red;
@@ -3467,7 +3560,7 @@ __global__ void __launch_bounds__(BLK, minb<R>(4, TFACE_MINB_F)) k_T_face(Dims d
   const int par = parity(ctl);
   const bool first = ctl->first;
   Cell x;
-  const bool act = patch_cell(d, x);
+  const bool act = patch_cell(d, x, blockIdx);
   const int c = x.c;
   double e[1] = {0.};
   if (act) {
@@ -3489,6 +3582,10 @@ __global__ void __launch_bounds__(BLK, minb<R>(4, TFACE_MINB_F)) k_T_face(Dims d
     if (x.k == d.NZ - 1) Tn[x.face(d, 6)] = T[x.face(d, 6)];
   }
   if (d.owns(blockIdx.z)) block_max<1>(red, e, ctl->err[par] + 4);
+}
+template <class R>
+__global__ void __launch_bounds__(BLK, minb<R>(4, TFACE_MINB_F)) k_T_face(Dims d, GeoT<R> g, FieldsT<R> F, Phys P, Ctrl *ctl) {
+  T_face_body<R>(d, g, F, P, ctl, LaunchBlock{});
 }
 
 // The +xi_dd face updates of one field (faces fr of the current half, new
@@ -3737,7 +3834,8 @@ __global__ void __launch_bounds__(CB3, VFN_MINB) k_vel_faceN(Dims d, GeoT<R> g, 
 // that is still above its tolerance to a new smallest change; the FP64
 // passes that follow apply the reference's test.  max_iters bounds both
 // phases together.
-__global__ void k_iter_end(Ctrl *ctl, Phys P, int lowp) {
+template <class BI>
+__device__ __forceinline__ void iter_end_body(Ctrl *ctl, const Phys &P, int lowp, const BI blockIdx) {
   if (ctl->done) return;
   const int par = ctl->iter & ctl->pmask;
   double e[5];
@@ -3787,6 +3885,9 @@ __global__ void k_iter_end(Ctrl *ctl, Phys P, int lowp) {
     ctl->done = 1;
     ctl->status = -3;  // NIM_ERR_NOT_CONVERGED
   }
+}
+__global__ void k_iter_end(Ctrl *ctl, Phys P, int lowp) {
+  iter_end_body(ctl, P, lowp, LaunchBlock{});
 }
 
 // start of the FP32 phase of a mixed-precision step (after k_step_reset)

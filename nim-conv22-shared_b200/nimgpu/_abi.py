@@ -173,6 +173,9 @@ def gpu_lib() -> C.CDLL:
         lib.nim_batch_step.argtypes = [C.c_int32, C.POINTER(vp), C.c_int32, C.POINTER(StepStats),
                                        C.POINTER(C.c_int32)]
         lib.nim_batch_step.restype = C.c_int
+        lib.nim_batch_step_fused.argtypes = [C.c_int32, C.POINTER(vp), C.c_int32, C.POINTER(StepStats),
+                                             C.POINTER(C.c_int32)]
+        lib.nim_batch_step_fused.restype = C.c_int
         lib.nim_slab_layout.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]
         lib.nim_slab_layout.restype = C.c_int
         lib.nim_slab_halo.argtypes = [C.c_int32] * 6 + [C.POINTER(C.c_int64)] * 2

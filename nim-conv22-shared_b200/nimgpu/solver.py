@@ -223,21 +223,23 @@ class NimSolver:
         apply_temperature_noise(self.get, self.set, self.mesh, amp, seed)
 
 
-def batch_step(solvers, nsteps: int, raise_on_error: bool = True):
+def batch_step(solvers, nsteps: int, raise_on_error: bool = True, fused: bool = False):
     """nim_batch_step: advance several NimSolvers (one device) by nsteps
-    together; returns per-solver lists of step records."""
+    together; returns per-solver lists of step records.  fused: every pass
+    kernel launched once for the whole batch (nim_batch_step_fused)."""
     n = len(solvers)
     lib = _abi.gpu_lib()
     handles = (C.c_void_p * n)(*[s._h.value for s in solvers])
     per = (_abi.StepStats * max(n * nsteps, 1))()
     done = (C.c_int32 * n)()
-    st = lib.nim_batch_step(n, handles, nsteps, per, done)
+    fn = lib.nim_batch_step_fused if fused else lib.nim_batch_step
+    st = fn(n, handles, nsteps, per, done)
     if raise_on_error:
-        _abi.check(st, "nim_batch_step")
+        _abi.check(st, "nim_batch_step_fused" if fused else "nim_batch_step")
     return [[per[i * nsteps + k] for k in range(done[i])] for i in range(n)]
 
 
-def autotune_batch(solvers, candidates=(4, 8, 16, 32), steps_each: int = 1):
+def autotune_batch(solvers, candidates=(4, 8, 16, 32), steps_each: int = 1, fused: bool = False):
     """Pick the graph length of a batch by measurement: advance the batch
     steps_each steps with each candidate (these are real steps of the run:
     the iterates do not depend on the graph length) and keep the fastest
@@ -250,7 +252,7 @@ def autotune_batch(solvers, candidates=(4, 8, 16, 32), steps_each: int = 1):
         for s in solvers:
             s.set_graph_iters(g)
         t0 = time.perf_counter()
-        recs = batch_step(solvers, steps_each)
+        recs = batch_step(solvers, steps_each, fused=fused)
         dt = time.perf_counter() - t0
         work = sum(c * sum(r.iters for r in rr) for c, rr in zip(cells, recs))
         timing[g] = dt / max(work, 1)

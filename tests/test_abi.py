@@ -76,6 +76,8 @@ def test_argument_errors_without_device(gpu_lib):
     assert gpu_lib.nim_gpu_output_begin(None, 0, None, 0, None) == _abi.NIM_ERR_BAD_ARG
     assert gpu_lib.nim_gpu_output_wait(None, 0) == _abi.NIM_ERR_BAD_ARG
     assert gpu_lib.nim_batch_step(0, None, 1, None, None) == _abi.NIM_ERR_BAD_ARG
+    assert gpu_lib.nim_batch_step_fused(0, None, 1, None, None) == _abi.NIM_ERR_BAD_ARG
+    assert gpu_lib.nim_batch_step_fused(257, None, 1, None, None) == _abi.NIM_ERR_BAD_ARG
     # an unknown schedule is refused before any device call
     import nimgpu
     mesh = nimgpu.Mesh(config.small_case().mesh_params())
