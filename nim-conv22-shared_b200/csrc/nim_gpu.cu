@@ -581,7 +581,12 @@ int mirror_geometry(nim_ctx *x) {
   c.add(g.bcap, h.bcap, 8 * NB);
   c.add(g.bcg, h.bcg, 2 * NB);
   c.add(g.zf, h.zf, 4 * NB);
-  return run_cvt<double, float>(x, c);
+  TRY((run_cvt<double, float>(x, c)));
+  // 1/vol in float from the float volumes: the float sweeps' own division
+  k_reciprocal<float><<<x->nblk_c, BLK, 0, x->stream>>>(h.vol, h.rvol, d.Nc);
+  CK(cudaGetLastError());
+  x->launches += 1;
+  return NIM_OK;
 }
 
 // velocity NIM constants (every step, after nim_gpu_begin_step's kernels)
@@ -1105,6 +1110,7 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x, 
   const size_t Nc = d.Nc, NF = d.NF, NB = d.NBF;
   Geo &g = x->g;
   TRY(dalloc(x, &g.vol, Nc));
+  TRY(dalloc(x, &g.rvol, Nc));
   TRY(dalloc(x, &g.G, 3 * Nc));
   TRY(dalloc(x, &g.gij, 9 * Nc));
   TRY(dalloc(x, &g.xi, 9 * Nc));
@@ -1151,6 +1157,7 @@ static int create_impl(const nim_mesh_desc *m, const nim_params *p, nim_ctx *x, 
   if (x->mixed) {
     GeoT<float> &h = x->g32;
     TRY(dalloc(x, &h.vol, Nc));
+    TRY(dalloc(x, &h.rvol, Nc));
     TRY(dalloc(x, &h.G, 3 * Nc));
     TRY(dalloc(x, &h.gij, 9 * Nc));
     TRY(dalloc(x, &h.xi, 9 * Nc));
@@ -1264,6 +1271,7 @@ extern "C" int nim_gpu_init(nim_ctx *x) {
   k_run_reset<<<1, 1, 0, s>>>(x->ctl, x->seq ? 0 : 1);
   k_cell_geometry<<<x->nblk_c, BLK, 0, s>>>(d, x->gq, x->node_xyz, x->g);
   k_metric_derived<<<x->nblk_c, BLK, 0, s>>>(d, x->g);
+  k_reciprocal<double><<<x->nblk_c, BLK, 0, s>>>(x->g.vol, x->g.rvol, d.Nc);
   k_pressure_coeffs<<<x->nblk_c, BLK, 0, s>>>(d, x->g, x->params.rho);
   k_bc_geometry<<<x->nblk_b, BLK, 0, s>>>(d, x->gq, x->node_xyz, x->g, x->params.rho, x->bcv);
   // initial conditions: zero (general.f90:16-31), then the Dirichlet faces

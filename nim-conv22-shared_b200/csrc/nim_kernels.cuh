@@ -81,6 +81,8 @@ struct GeoT {
   R *zf;      // [4][NBF]  zero-flux weights (B, C, D, A) for z walls
   R *nuw;     // [4][NBF]  find_Nu2 weights (A, B, C, D) for r walls
   R *bcval;   // [4][NBF]  Dirichlet face values of u, v, w, T
+  R *rvol;    // [Nc]      1/vol, formed once at init in the storage type's own
+              //           division (null in the dual copy, whose kernels divide)
 };
 using Geo = GeoT<double>;
 
@@ -136,6 +138,16 @@ struct ParOf<DualD> {
 template <class V>
 __device__ __forceinline__ V pv(double v, double t) {
   return ParOf<V>::get(v, t);
+}
+// 1/vol of cell c: the stored reciprocal (the same IEEE division in the
+// storage type, formed once at init), or the division itself for the dual
+// copy
+template <class R>
+__device__ __forceinline__ Ar<R> inv_vol(const GeoT<R> &g, int c) {
+  if constexpr (std::is_same<R, double>::value || std::is_same<R, float>::value)
+    return g.rvol[c];
+  else
+    return Ar<R>(1.) / g.vol[c];
 }
 
 // Control block in device memory; k_iter_end is its only writer during an
@@ -395,6 +407,15 @@ __global__ void __launch_bounds__(BLK) k_cell_geometry(Dims d, GaussRule gq, con
     if (owns_face(d, x, fn)) g.area[x.face(d, fn)] = A;
     for (int n = 0; n < 9; ++n) g.gf[(n + 9 * (fn - 1)) * Nc + c] = K[n] / A;
   }
+}
+
+// 1/vol per cell, once at init: the sweeps' Green-Gauss factor (1/V of
+// nse.f90:2866-2903) read instead of divided on every pass; the same IEEE
+// division, so the same bits
+template <class R>
+__global__ void __launch_bounds__(BLK) k_reciprocal(const R *__restrict__ v, R *__restrict__ r, int n) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) r[c] = R(1) / v[c];
 }
 
 // Compact per-cell copies of the metric entries the sweeps read: the
@@ -1349,7 +1370,7 @@ __device__ __forceinline__ void vel_cell_body(const Dims &d, const GeoT<R> &g, c
     const R *fp = F.f[3] + par * NF;
     V pf[7];
     for (int k = 1; k <= 6; ++k) pf[k] = fp[f[k]];
-    const V invV = V(1.) / g.vol[c];
+    const V invV = inv_vol(g, c);
     const V base = (q == 2) ? -(V(P.g_beta) * V(0.5) * (F.c[3][c] + F.co[3][c])) : V(0.);
     const V RB = base + V(P.inv_rho) * green_gauss(g, NF, invV, pf, f, q);
     const R *fr = F.f[q] + par * NF;
@@ -2426,7 +2447,7 @@ __device__ __forceinline__ void p_src_body(const Dims &d, const GeoT<R> &g, cons
     cell_faces(d, x, f);
     by_dir(threadIdx.y, [&](auto Q) {
       constexpr int q = decltype(Q)::value - 1;
-      const A invV = A(1) / g.vol[c];
+      const A invV = inv_vol(g, c);
       const R *fq = F.f[q] + newhalf(ctl) * NF;
       A vf[7];
       for (int k = 1; k <= 6; ++k) vf[k] = fq[f[k]];
@@ -2518,10 +2539,10 @@ __device__ __forceinline__ void p_srcN_body(const Dims &d, const GeoT<R> &g, con
   if (active) by_dir(threadIdx.y, [&](auto Q) {
     constexpr int q = decltype(Q)::value - 1;
     R vol[NP];
-    ldN<R, NP>(g.vol, c, vol);
     V invV[NP];
+    ldN<R, NP>(g.rvol, c, vol);  // 1/vol
 #pragma unroll
-    for (int p = 0; p < NP; ++p) invV[p] = V(1.) / vol[p];
+    for (int p = 0; p < NP; ++p) invV[p] = vol[p];
     // green_gauss (terms of faces 2, 1, 4, 3, 6, 5, then the volume factor)
     auto gauss = [&](const R (&phi)[7][NP], int cc, V (&out)[NP]) {
       const R *nc = g.normal + (size_t)cc * NF;
