@@ -415,7 +415,7 @@ def run_batch(args, rank, world, local):
     torch.cuda.set_device(local)
     if world > 1 and rank != 0:
         return 0
-    cases = config.batch_cases(64)
+    cases = config.batch_cases(args.instances)
     steps = max(args.steps // 5, 1)
 
     prec = _abi.PRECISION_MIXED if args.precision == "mixed" else _abi.PRECISION_FP64
@@ -472,7 +472,7 @@ def run_batch(args, rank, world, local):
         "warmup_note": "4 warm-up steps, one per autotuner candidate",
         "dtype": "f64" if prec == _abi.PRECISION_FP64 else "f32+f64", "precision": args.precision,
         "data": "synthetic (seeded meshes, physics and T noise)",
-        "config": {"workload": "batch: 64 cylinder enclosures D=1 H=1, hexagon side U[0.1,0.3], "
+        "config": {"workload": f"batch: {len(cases)} cylinder enclosures D=1 H=1, hexagon side U[0.1,0.3], "
                                "a x a x round(0.75a) cells, a in [24,64], Ra log-uniform [1e3,1e6], "
                                "Pr in {0.71, 7.0}, dt=1e-3",
                    "cells": sum(c.ncells for c in cases), "instances": len(cases),
@@ -651,6 +651,8 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 passes over a float mirror, then FP64 passes (nim_params.precision)")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
+    ap.add_argument("--instances", type=int, default=64,
+                    help="--case batch: the first N of the 64 seeded enclosures (a smaller case for profiling)")
     ap.add_argument("--stop-tol", type=float, default=None,
                     help="stop every inner loop when each field's change is below this (FP64, pressure by its "
                          "gradients) instead of the reference's tolerances")

@@ -24,14 +24,14 @@ constexpr int kBatchMax = 256;  // enclosures in one fused batch
 
 // the kernel forms a fused pass launches (one persistent launch each)
 enum BatchSlot {
-  BS_VEL_CELL2,  // k_vel_cell2 (n_theta even)
+  BS_VEL_CELL2,  // k_vel_cell2 (n_theta even), pairs of cells in cell order (FlatBlock)
   BS_VEL_CELL,   // k_vel_cell (formulation 2), cells in cell order (FlatBlock)
   BS_VEL_FACE,   // k_vel_face (FlatBlock)
-  BS_P_SRC2,     // k_p_srcN<double, 2>
+  BS_P_SRC2,     // k_p_srcN<double, 2> (FlatBlock)
   BS_P_SRC,      // k_p_src (FlatBlock)
   BS_P_BC,       // k_p_bc
   BS_P_BC_COPY,  // k_p_bc_copy
-  BS_P_FACE2,    // k_p_faceN<double, 2>
+  BS_P_FACE2,    // k_p_faceN<double, 2> (FlatBlock)
   BS_P_FACE,     // k_p_face (FlatBlock)
   BS_P_DPDX,     // k_p_dpdx (is_dpdx_tolerance)
   BS_ZERO_FLUX,  // k_zero_flux
@@ -194,7 +194,7 @@ __device__ __forceinline__ void batch_items(const BatchArgs &A, Body &&body) {
 constexpr int wider(int blocks, int w) { return blocks - w > 1 ? blocks - w : 1; }
 template <class R, int W>
 __global__ void __launch_bounds__(CB3, wider(minb<R>(VC2_MINB, VC2_MINB_F), W)) kb_vel_cell2(BatchArgs A) {
-  batch_items<BS_VEL_CELL2, R>(A, [&](const BatchInst<R> &I, BatchBlock b) {
+  batch_items<BS_VEL_CELL2, R, FlatBlock>(A, [&](const BatchInst<R> &I, FlatBlock b) {
     vel_cell2_body<R, false>(I.d, I.g, I.F, I.P, I.ctl, b);
   });
 }
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(CB3, wider(3, W)) kb_vel_face(BatchArgs A) {
 }
 template <int W>
 __global__ void __launch_bounds__(CB3, wider(PSN_MINB, W)) kb_p_src2(BatchArgs A) {
-  batch_items<BS_P_SRC2, double>(A, [&](const BatchInst<double> &I, BatchBlock b) {
+  batch_items<BS_P_SRC2, double, FlatBlock>(A, [&](const BatchInst<double> &I, FlatBlock b) {
     p_srcN_body<double, 2>(I.d, I.g, I.F, I.P, I.ctl, b);
   });
 }
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(BLK) kb_p_bc_copy(BatchArgs A) {
 }
 template <int W>
 __global__ void __launch_bounds__(CB3, wider(PFN_MINB, W)) kb_p_face2(BatchArgs A) {
-  batch_items<BS_P_FACE2, double>(A, [&](const BatchInst<double> &I, BatchBlock b) {
+  batch_items<BS_P_FACE2, double, FlatBlock>(A, [&](const BatchInst<double> &I, FlatBlock b) {
     p_faceN_body<double, 2>(I.d, I.g, I.F, I.P, I.ctl, b);
   });
 }

@@ -1799,26 +1799,26 @@ int fused_setup(FusedBatch &B, int32_t n, nim_ctx *const *ctx) {
     // the one-cell sweeps over runs of consecutive cells of a plane (FlatBlock)
     const BatchGrid f3{(unsigned)((d.plane + CB - 1) / CB), 1u, (unsigned)d.NZ};
     const BatchGrid f8{(unsigned)((d.plane + BLK - 1) / BLK), 1u, (unsigned)d.NZ};
-    const BatchGrid gp{(unsigned)(d.NT + 63) / 64, (unsigned)(d.NR + 3) / 4, (unsigned)d.NZ};
+    const BatchGrid f3p{(unsigned)((d.plane / 2 + CB - 1) / CB), 1u, (unsigned)d.NZ};  // pairs of cells
     const BatchGrid gb{(unsigned)x->nblk_b, 1u, 1u};
     for (int ph = 0; ph < 2; ++ph) {
       if (ph == 0 && !B.mixed) continue;
       BatchGrid *G = &grids[((size_t)ph * n + i) * BS_COUNT];
       // the enclosure's sweeps in the forms the batch has, all of which give
-      // the bits of the enclosure's own pass: the two-cell forms where a row
-      // of n_theta / 2 threads fills 3/4 of a warp's lanes, else the
-      // one-cell forms over consecutive cells (the TMA-staged and four-cell
-      // sweeps of large meshes are replaced by their gather forms)
-      const int lanes2 = d.NT / 2;
-      const bool rows2 = (double)lanes2 / (32.0 * ((lanes2 + 31) / 32)) >= 0.75;
-      if ((x->cell_pair || x->cell_quad) && rows2)
-        G[BS_VEL_CELL2] = gp;
+      // the bits of the enclosure's own pass, over consecutive cells of a
+      // plane (every lane busy whatever n_theta): the two-cell forms for
+      // even n_theta (FP64 pressure sweeps too), else the one-cell forms
+      // (the TMA-staged and four-cell sweeps of large meshes are replaced
+      // by their gather forms)
+      const bool pair = d.NT % 2 == 0 && (x->cell_pair || x->cell_quad);
+      if (pair)
+        G[BS_VEL_CELL2] = f3p;
       else
         G[BS_VEL_CELL] = f3;
       G[BS_VEL_FACE] = f3;
-      if (ph == 1 && x->press_pair) {
-        G[BS_P_SRC2] = gp;
-        G[BS_P_FACE2] = gp;
+      if (ph == 1 && pair) {
+        G[BS_P_SRC2] = f3p;
+        G[BS_P_FACE2] = f3p;
       } else {
         G[BS_P_SRC] = f3;
         G[BS_P_FACE] = f3;

@@ -1333,6 +1333,21 @@ __device__ __forceinline__ bool patch_cell(const Dims &d, Cell &x, const BI bi) 
   return i < d.NT && j < d.NR;
 }
 __device__ __forceinline__ bool patch_cell(const Dims &d, Cell &x) { return patch_cell(d, x, LaunchBlock{}); }
+// The first of the NP theta-adjacent cells of this thread in the NP-cells-
+// a-thread sweeps (block (CB, 3)): rows of 32 NP cells (theta) x CB/32 (r)
+// per block, or with a FlatBlock runs of CB groups of NP consecutive cells
+// of plane z (n_theta % NP == 0).  Row j < NR for a thread with cells.
+template <int NP, class BI>
+__device__ __forceinline__ void group_cell(const Dims &d, const BI bi, int &i, int &j) {
+  i = bi.x * (32 * NP) + NP * (threadIdx.x & 31);
+  j = bi.y * (CB / 32) + (threadIdx.x >> 5);
+}
+template <int NP>
+__device__ __forceinline__ void group_cell(const Dims &d, const FlatBlock bi, int &i, int &j) {
+  const int t = (int)bi.x * CB + (int)threadIdx.x, per = d.NT / NP;  // group of plane z
+  j = t / per;
+  i = NP * (t - j * per);
+}
 __device__ __forceinline__ bool patch_cell(const Dims &d, Cell &x, const FlatBlock bi) {
   const int t = (int)bi.x * (int)blockDim.x + (int)threadIdx.x;  // cell of plane z in cell order
   const int j = t / d.NT, i = t - j * d.NT;
@@ -1453,8 +1468,9 @@ __device__ __forceinline__ void vel_cell2_body(const Dims &d, const GeoT<R> &g, 
   const int par = parity(ctl);
   const bool first = ctl->first;
   const int q = threadIdx.y;
-  const int i = blockIdx.x * 64 + 2 * (threadIdx.x & 31);
-  const int j = blockIdx.y * (CB / 32) + (threadIdx.x >> 5);
+  int i = blockIdx.x * 64 + 2 * (threadIdx.x & 31);
+  int j = blockIdx.y * (CB / 32) + (threadIdx.x >> 5);
+  if constexpr (std::is_same<BI, FlatBlock>::value) group_cell<2>(d, blockIdx, i, j);
   const int k = blockIdx.z;
   double e[3] = {0., 0., 0.};
   if (i < d.NT && j < d.NR) {
@@ -2510,8 +2526,8 @@ __device__ __forceinline__ void p_srcN_body(const Dims &d, const GeoT<R> &g, con
   __shared__ V sbz[CB * NP];
   const int par = parity(ctl);
   const int tx = threadIdx.x;
-  const int i = blockIdx.x * (32 * NP) + NP * (tx & 31);
-  const int j = blockIdx.y * (CB / 32) + (tx >> 5);
+  int i, j;
+  group_cell<NP>(d, blockIdx, i, j);
   const int k = blockIdx.z;
   const bool active = i < d.NT && j < d.NR;
   const int Nc = d.Nc, NF = d.NF, NT = d.NT, NR = d.NR, pl = d.plane;
@@ -2951,8 +2967,8 @@ __device__ __forceinline__ void p_faceN_body(const Dims &d, const GeoT<R> &g, co
   const int par = parity(ctl);
   const bool first = ctl->first;
   const int tx = threadIdx.x;
-  const int i = blockIdx.x * (32 * NP) + NP * (tx & 31);
-  const int j = blockIdx.y * (CB / 32) + (tx >> 5);
+  int i, j;
+  group_cell<NP>(d, blockIdx, i, j);
   const int k = blockIdx.z;
   double e[1] = {0.};
   if (i < d.NT && j < d.NR) by_dir(threadIdx.y, [&](auto D) {
