@@ -1496,13 +1496,27 @@ __device__ __forceinline__ void vel_cell2_body(const Dims &d, const GeoT<R> &g, 
     V gs0 = V(0.), gs1 = V(0.);
     {
       const int order[6] = {2, 1, 4, 3, 6, 5};
+      // face 3 of both cells, loaded with face 4's turn: the pair's second
+      // value is also face 4 of the first cell
+      R p3[2], a3[2], n3[2];
 #pragma unroll
       for (int t = 0; t < 6; ++t) {
         const int m = order[t];
         R p0, p1, a0, a1, n0, n1;
-        face2(pp, m, p0, p1);
-        face2(g.area, m, a0, a1);
-        face2(nq, m, n0, n1);
+        if (m == 4) {
+          ld2(pp, fi[3], p3[0], p3[1]);
+          ld2(g.area, fi[3], a3[0], a3[1]);
+          ld2(nq, fi[3], n3[0], n3[1]);
+          p0 = p3[1], a0 = a3[1], n0 = n3[1];
+          p1 = pp[f4b], a1 = g.area[f4b], n1 = nq[f4b];
+        } else if (m == 3) {
+          p0 = p3[0], a0 = a3[0], n0 = n3[0];
+          p1 = p3[1], a1 = a3[1], n1 = n3[1];
+        } else {
+          face2(pp, m, p0, p1);
+          face2(g.area, m, a0, a1);
+          face2(nq, m, n0, n1);
+        }
         const V t0 = (V)p0 * a0 * (n0), t1 = (V)p1 * a1 * (n1);
         if (t == 0) {
           gs0 = t0;
@@ -1535,7 +1549,10 @@ __device__ __forceinline__ void vel_cell2_body(const Dims &d, const GeoT<R> &g, 
     // own faces of component q (stored values)
     const R *fr = F.f[q] + par * NF;
     R o0[7], o1[7];
-    for (int m = 1; m <= 6; ++m) face2(fr, m, o0[m], o1[m]);
+    for (int m = 1; m <= 6; ++m)
+      if (m != 4) face2(fr, m, o0[m], o1[m]);
+    o0[4] = o1[3];  // face 4 of cell i is face 3 of cell i+1
+    o1[4] = fr[f4b];
     // rows / planes a and b: the -e,+e neighbours (centred), +1,+2 (lo) or -1,-2 (hi)
     auto along = [&](bool lo, bool hi, V v0, V va, V vb) {
       return lo ? tang_vals(true, false, v0, va, vb, V(0.), V(0.))
