@@ -277,6 +277,102 @@ __global__ void __launch_bounds__(BLK, wider(minb<R>(4, TFACE_MINB_F), W)) kb_T_
   });
 }
 
+// ---- the same pass kernels as plain (non-persistent) launches over up to
+// kGroup enclosures whose arguments travel in the launch's own parameters:
+// block b -> enclosure by a search over running block counts in the
+// parameter block, so the enclosure index, its arrays and its sizes are
+// launch constants read from the constant bank, as in the plain kernels,
+// instead of values in registers.  Every enclosure's blocks are launched
+// each pass; those of an enclosure whose loop has stopped, or that iterates
+// in the other precision, return at once.
+constexpr int kGroup = 40;  // enclosures per launch: 40 x 704 bytes of arguments
+template <class R>
+struct BatchGroup {
+  int n;             // enclosures in the group
+  int ph;            // the phase this launch serves (1: FP32 mirror, 2: FP64)
+  int first;         // the group's first enclosure in the batch
+  const int *phase;  // [batch] the enclosures' phases
+  unsigned off[kGroup + 1];
+  BatchGrid grid[kGroup];
+  BatchInst<R> inst[kGroup];
+};
+static_assert(sizeof(BatchGroup<double>) < 32000, "kernel parameters stay below 32 KB");
+
+template <class R, class BI, class Body>
+__device__ __forceinline__ void group_item(const BatchGroup<R> &L, Body &&body) {
+  const unsigned w = blockIdx.x;
+  int lo = 0, hi = L.n - 1;  // the last a with off[a] <= w
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (L.off[mid] <= w)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  if (L.phase[L.first + lo] != L.ph) return;
+  const BatchGrid gr = L.grid[lo];
+  const unsigned l = w - L.off[lo], r = l / gr.x;
+  BI b;
+  b.x = l - r * gr.x;
+  b.y = r % gr.y;
+  b.z = r / gr.y;
+  body(L.inst[lo], b);
+}
+template <class R>
+__global__ void __launch_bounds__(CB3, minb<R>(VC2_MINB, VC2_MINB_F)) kg_vel_cell2(const __grid_constant__ BatchGroup<R> L) {
+  group_item<R, FlatBlock>(L, [&](const BatchInst<R> &I, FlatBlock b) { vel_cell2_body<R, false>(I.d, I.g, I.F, I.P, I.ctl, b); });
+}
+template <class R>
+__global__ void __launch_bounds__(CB3, 3) kg_vel_cell(const __grid_constant__ BatchGroup<R> L) {
+  group_item<R, FlatBlock>(L, [&](const BatchInst<R> &I, FlatBlock b) { vel_cell_body<false, 2, R>(I.d, I.g, I.F, I.P, I.ctl, b); });
+}
+template <class R>
+__global__ void __launch_bounds__(CB3, 3) kg_vel_face(const __grid_constant__ BatchGroup<R> L) {
+  group_item<R, FlatBlock>(L, [&](const BatchInst<R> &I, FlatBlock b) { vel_face_body<R>(I.d, I.g, I.F, I.P, I.ctl, b); });
+}
+__global__ void __launch_bounds__(CB3, PSN_MINB) kg_p_src2(const __grid_constant__ BatchGroup<double> L) {
+  group_item<double, FlatBlock>(L, [&](const BatchInst<double> &I, FlatBlock b) { p_srcN_body<double, 2>(I.d, I.g, I.F, I.P, I.ctl, b); });
+}
+template <class R>
+__global__ void __launch_bounds__(CB3, minb<R>(4, PSRC_MINB_F)) kg_p_src(const __grid_constant__ BatchGroup<R> L) {
+  group_item<R, FlatBlock>(L, [&](const BatchInst<R> &I, FlatBlock b) { p_src_body<R>(I.d, I.g, I.F, I.P, I.ctl, b); });
+}
+template <class R>
+__global__ void __launch_bounds__(BLK) kg_p_bc(const __grid_constant__ BatchGroup<R> L) {
+  group_item<R, BatchBlock>(L, [&](const BatchInst<R> &I, BatchBlock b) { p_bc_body<R>(I.d, I.g, I.F, I.P, I.ctl, b); });
+}
+template <class R>
+__global__ void __launch_bounds__(BLK) kg_p_bc_copy(const __grid_constant__ BatchGroup<R> L) {
+  group_item<R, BatchBlock>(L, [&](const BatchInst<R> &I, BatchBlock b) { p_bc_copy_body<R>(I.d, I.F, I.ctl, b); });
+}
+__global__ void __launch_bounds__(CB3, PFN_MINB) kg_p_face2(const __grid_constant__ BatchGroup<double> L) {
+  group_item<double, FlatBlock>(L, [&](const BatchInst<double> &I, FlatBlock b) { p_faceN_body<double, 2>(I.d, I.g, I.F, I.P, I.ctl, b); });
+}
+template <class R>
+__global__ void __launch_bounds__(CB3, minb<R>(5, PFACE_MINB_F)) kg_p_face(const __grid_constant__ BatchGroup<R> L) {
+  group_item<R, FlatBlock>(L, [&](const BatchInst<R> &I, FlatBlock b) { p_face_body<R>(I.d, I.g, I.F, I.P, I.ctl, b); });
+}
+template <class R>
+__global__ void __launch_bounds__(BLK) kg_p_dpdx(const __grid_constant__ BatchGroup<R> L) {
+  group_item<R, BatchBlock>(L, [&](const BatchInst<R> &I, BatchBlock b) { p_dpdx_body<R>(I.d, I.g, I.F, I.ctl, b); });
+}
+template <class R>
+__global__ void __launch_bounds__(BLK) kg_zero_flux(const __grid_constant__ BatchGroup<R> L) {
+  group_item<R, BatchBlock>(L, [&](const BatchInst<R> &I, BatchBlock b) { zero_flux_body<R>(I.d, I.g, I.F, I.ctl, b); });
+}
+template <class R>
+__global__ void __launch_bounds__(BLK, 4) kg_T_coef(const __grid_constant__ BatchGroup<R> L) {
+  group_item<R, BatchBlock>(L, [&](const BatchInst<R> &I, BatchBlock b) { T_coef_body<R>(I.d, I.g, I.F, I.P, I.ctl, b); });
+}
+template <class R>
+__global__ void __launch_bounds__(CB3, minb<R>(5, TCELL_MINB_F)) kg_T_cell(const __grid_constant__ BatchGroup<R> L) {
+  group_item<R, FlatBlock>(L, [&](const BatchInst<R> &I, FlatBlock b) { T_cell_body<false, R>(I.d, I.g, I.F, I.P, I.ctl, b); });
+}
+template <class R>
+__global__ void __launch_bounds__(BLK, minb<R>(4, TFACE_MINB_F)) kg_T_face(const __grid_constant__ BatchGroup<R> L) {
+  group_item<R, FlatBlock>(L, [&](const BatchInst<R> &I, FlatBlock b) { T_face_body<R>(I.d, I.g, I.F, I.P, I.ctl, b); });
+}
+
 // find_error's stop test of every enclosure iterating this pass, in its
 // phase's form (k_iter_end; lowp for the FP32 phase)
 __global__ void k_batch_iter_end(BatchArgs A) {

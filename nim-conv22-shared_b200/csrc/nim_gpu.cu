@@ -1641,6 +1641,11 @@ struct FusedBatch {
   bool mixed = false;
   int G = 4;  // passes per graph launch
   bool wide = false;  // batched kernels at one resident block per SM fewer
+  // NIM_BATCH_FORM=grid: plain launches over groups of kGroup enclosures
+  // whose arguments are kernel parameters (kg_*), one per slot and group
+  bool grid_form = false;
+  std::vector<BatchGroup<float>> grp32[BS_COUNT];
+  std::vector<BatchGroup<double>> grp64[BS_COUNT];
   cudaStream_t s = nullptr;
   BatchArgs args{};
   void *dev = nullptr;                // tables, phases, work list, states
@@ -1730,11 +1735,52 @@ int fused_slots_of(FusedBatch &B) {
   return B.wide ? fused_slots<R, 1>(B) : fused_slots<R, 0>(B);
 }
 
+// one slot's launch over one group of enclosures (NIM_BATCH_FORM=grid)
+template <class R>
+void group_launch(int slot, const BatchGroup<R> &L, cudaStream_t s) {
+  const unsigned nb = L.off[L.n];
+  const dim3 t3(CB, 3);
+  switch (slot) {
+    case BS_VEL_CELL2: kg_vel_cell2<R><<<nb, t3, 0, s>>>(L); break;
+    case BS_VEL_CELL: kg_vel_cell<R><<<nb, t3, 0, s>>>(L); break;
+    case BS_VEL_FACE: kg_vel_face<R><<<nb, t3, 0, s>>>(L); break;
+    case BS_P_SRC: kg_p_src<R><<<nb, t3, 0, s>>>(L); break;
+    case BS_P_BC: kg_p_bc<R><<<nb, BLK, 0, s>>>(L); break;
+    case BS_P_BC_COPY: kg_p_bc_copy<R><<<nb, BLK, 0, s>>>(L); break;
+    case BS_P_FACE: kg_p_face<R><<<nb, t3, 0, s>>>(L); break;
+    case BS_P_DPDX: kg_p_dpdx<R><<<nb, BLK, 0, s>>>(L); break;
+    case BS_ZERO_FLUX: kg_zero_flux<R><<<nb, BLK, 0, s>>>(L); break;
+    case BS_T_COEF: kg_T_coef<R><<<nb, BLK, 0, s>>>(L); break;
+    case BS_T_CELL: kg_T_cell<R><<<nb, t3, 0, s>>>(L); break;
+    case BS_T_FACE: kg_T_face<R><<<nb, BLK, 0, s>>>(L); break;
+    default:
+      if constexpr (std::is_same<R, double>::value) {
+        if (slot == BS_P_SRC2) kg_p_src2<<<nb, t3, 0, s>>>(L);
+        if (slot == BS_P_FACE2) kg_p_face2<<<nb, t3, 0, s>>>(L);
+      }
+  }
+}
+template <class R>
+int group_slots(FusedBatch &B) {
+  constexpr int ph = sizeof(R) == 4 ? 0 : 1;
+  for (int q = 0; q < BS_COUNT; ++q) {
+    if (!B.use[ph][q]) continue;
+    if constexpr (ph == 0) {
+      for (const auto &L : B.grp32[q]) group_launch<float>(q, L, B.s);
+    } else {
+      for (const auto &L : B.grp64[q]) group_launch<double>(q, L, B.s);
+    }
+  }
+  CK(cudaGetLastError());
+  return NIM_OK;
+}
+
 int fused_launches(const FusedBatch &B, int phases) {
-  int k = 2;  // k_batch_plan, k_batch_iter_end
+  int k = B.grid_form ? 1 : 2;  // k_batch_iter_end, and k_batch_plan for the persistent form
   for (int ph = 0; ph < 2; ++ph)
     if (phases & (1 << ph))
-      for (int q = 0; q < BS_COUNT; ++q) k += B.use[ph][q] ? 1 : 0;
+      for (int q = 0; q < BS_COUNT; ++q)
+        k += !B.use[ph][q] ? 0 : !B.grid_form ? 1 : (int)(ph ? B.grp64[q].size() : B.grp32[q].size());
   return k;
 }
 
@@ -1746,9 +1792,14 @@ int fused_graph(FusedBatch &B, int phases) {
   CK(cudaStreamBeginCapture(B.s, cudaStreamCaptureModeThreadLocal));
   int st = NIM_OK;
   for (int k = 0; k < B.G && st == NIM_OK; ++k) {
-    k_batch_plan<<<1, 1024, 0, B.s>>>(B.args);
-    if (phases & 1) st = fused_slots_of<float>(B);
-    if (st == NIM_OK && (phases & 2)) st = fused_slots_of<double>(B);
+    if (B.grid_form) {
+      if (phases & 1) st = group_slots<float>(B);
+      if (st == NIM_OK && (phases & 2)) st = group_slots<double>(B);
+    } else {
+      k_batch_plan<<<1, 1024, 0, B.s>>>(B.args);
+      if (phases & 1) st = fused_slots_of<float>(B);
+      if (st == NIM_OK && (phases & 2)) st = fused_slots_of<double>(B);
+    }
     k_batch_iter_end<<<(B.n + 127) / 128, 128, 0, B.s>>>(B.args);
   }
   const cudaError_t e = cudaStreamEndCapture(B.s, &g);
@@ -1846,6 +1897,42 @@ int fused_setup(FusedBatch &B, int32_t n, nim_ctx *const *ctx) {
   B.args.plan = reinterpret_cast<BatchPlan *>(base + opl);
   B.args.n = n;
   B.state_dev_offset = ost;
+  const char *form = std::getenv("NIM_BATCH_FORM");
+  B.grid_form = form && std::string(form) == "grid";
+  if (B.grid_form) {
+    for (int ph = 0; ph < 2; ++ph) {
+      if (ph == 0 && !B.mixed) continue;
+      for (int q = 0; q < BS_COUNT; ++q) {
+        if (!B.use[ph][q]) continue;
+        for (int g0 = 0; g0 < n; g0 += kGroup) {
+          const int m = std::min(kGroup, n - g0);
+          auto fill = [&](auto &L, const auto &h) {
+            L.n = m;
+            L.ph = ph + 1;
+            L.first = g0;
+            L.phase = B.args.phase;
+            unsigned acc = 0;
+            for (int a = 0; a < m; ++a) {
+              const BatchGrid gr = grids[((size_t)ph * n + g0 + a) * BS_COUNT + q];
+              L.off[a] = acc;
+              L.grid[a] = gr;
+              L.inst[a] = h[g0 + a];
+              acc += gr.x * gr.y * gr.z;
+            }
+            L.off[m] = acc;
+            return acc;
+          };
+          if (ph == 0) {
+            B.grp32[q].emplace_back();
+            if (fill(B.grp32[q].back(), h32) == 0) B.grp32[q].pop_back();
+          } else {
+            B.grp64[q].emplace_back();
+            if (fill(B.grp64[q].back(), h64) == 0) B.grp64[q].pop_back();
+          }
+        }
+      }
+    }
+  }
   int sms = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx[0]->device));
   // NIM_BATCH_BOUNDS=wide: the batched kernels one resident block per SM

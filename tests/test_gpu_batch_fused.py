@@ -107,3 +107,23 @@ def test_fused_batch_arguments():
         assert lib.nim_batch_step_fused(2, h, 1, None, None) == _abi.NIM_ERR_BAD_ARG
     for s in (a, b, seq):
         s.close()
+
+
+def test_grid_form_equals_persistent_form(monkeypatch):
+    """NIM_BATCH_FORM=grid: the pass kernels as plain launches over groups of
+    enclosures whose arguments are kernel parameters; the same bits as the
+    persistent form and as one at a time."""
+    cases = uneven_cases()[:3]
+    alone = []
+    for c in cases:
+        s = make(c, precision=_abi.PRECISION_MIXED)
+        alone.append((records(s.solve_nse(2)), [s.download(f) for f in STATE]))
+        s.close()
+    monkeypatch.setenv("NIM_BATCH_FORM", "grid")
+    batch = [make(c, precision=_abi.PRECISION_MIXED) for c in cases]
+    recs = nimgpu.batch_step(batch, 2, fused=True)
+    for s, r, (want_recs, want_fields) in zip(batch, recs, alone):
+        assert records(r) == want_recs
+        for f, w in zip(STATE, want_fields):
+            assert np.array_equal(s.download(f), w), f
+        s.close()
