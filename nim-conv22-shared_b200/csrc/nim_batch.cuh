@@ -282,16 +282,16 @@ __global__ void __launch_bounds__(BLK, wider(minb<R>(4, TFACE_MINB_F), W)) kb_T_
 // block b -> enclosure by a search over running block counts in the
 // parameter block, so the enclosure index, its arrays and its sizes are
 // launch constants read from the constant bank, as in the plain kernels,
-// instead of values in registers.  Every enclosure's blocks are launched
-// each pass; those of an enclosure whose loop has stopped, or that iterates
-// in the other precision, return at once.
+// instead of values in registers.  The host groups the enclosures that
+// iterate in the launch's precision; the blocks of one whose loop stops
+// between the host's reads of the stop flags return at once.
 constexpr int kGroup = 40;  // enclosures per launch: 40 x 704 bytes of arguments
 template <class R>
 struct BatchGroup {
   int n;             // enclosures in the group
   int ph;            // the phase this launch serves (1: FP32 mirror, 2: FP64)
-  int first;         // the group's first enclosure in the batch
   const int *phase;  // [batch] the enclosures' phases
+  int idx[kGroup];   // the members' indices in the batch
   unsigned off[kGroup + 1];
   BatchGrid grid[kGroup];
   BatchInst<R> inst[kGroup];
@@ -309,7 +309,7 @@ __device__ __forceinline__ void group_item(const BatchGroup<R> &L, Body &&body) 
     else
       hi = mid - 1;
   }
-  if (L.phase[L.first + lo] != L.ph) return;
+  if (L.phase[L.idx[lo]] != L.ph) return;
   const BatchGrid gr = L.grid[lo];
   const unsigned l = w - L.off[lo], r = l / gr.x;
   BI b;

@@ -1642,10 +1642,14 @@ struct FusedBatch {
   int G = 4;  // passes per graph launch
   bool wide = false;  // batched kernels at one resident block per SM fewer
   // NIM_BATCH_FORM=grid: plain launches over groups of kGroup enclosures
-  // whose arguments are kernel parameters (kg_*), one per slot and group
+  // whose arguments are kernel parameters (kg_*), one per slot and group,
+  // the groups rebuilt from the enclosures iterating in each precision
   bool grid_form = false;
   std::vector<BatchGroup<float>> grp32[BS_COUNT];
   std::vector<BatchGroup<double>> grp64[BS_COUNT];
+  std::vector<BatchGrid> grids;  // [2][n][BS_COUNT]
+  std::vector<BatchInst<double>> h64;
+  std::vector<BatchInst<float>> h32;
   cudaStream_t s = nullptr;
   BatchArgs args{};
   void *dev = nullptr;                // tables, phases, work list, states
@@ -1775,6 +1779,50 @@ int group_slots(FusedBatch &B) {
   return NIM_OK;
 }
 
+// the groups of the enclosures whose phase is ph + 1 (host copy of the
+// phases), per slot
+void fused_groups(FusedBatch &B, const int *phase) {
+  for (int q = 0; q < BS_COUNT; ++q) {
+    B.grp32[q].clear();
+    B.grp64[q].clear();
+  }
+  for (int ph = 0; ph < 2; ++ph) {
+    std::vector<int> mem;
+    for (int i = 0; i < B.n; ++i)
+      if (phase[i] == ph + 1) mem.push_back(i);
+    for (int q = 0; q < BS_COUNT; ++q) {
+      if (!B.use[ph][q]) continue;
+      for (size_t g0 = 0; g0 < mem.size(); g0 += kGroup) {
+        const int m = (int)std::min<size_t>(kGroup, mem.size() - g0);
+        auto fill = [&](auto &L, const auto &h) {
+          L.n = m;
+          L.ph = ph + 1;
+          L.phase = B.args.phase;
+          unsigned acc = 0;
+          for (int a = 0; a < m; ++a) {
+            const int i = mem[g0 + a];
+            const BatchGrid gr = B.grids[((size_t)ph * B.n + i) * BS_COUNT + q];
+            L.idx[a] = i;
+            L.off[a] = acc;
+            L.grid[a] = gr;
+            L.inst[a] = h[i];
+            acc += gr.x * gr.y * gr.z;
+          }
+          L.off[m] = acc;
+          return acc;
+        };
+        if (ph == 0) {
+          B.grp32[q].emplace_back();
+          if (fill(B.grp32[q].back(), B.h32) == 0) B.grp32[q].pop_back();
+        } else {
+          B.grp64[q].emplace_back();
+          if (fill(B.grp64[q].back(), B.h64) == 0) B.grp64[q].pop_back();
+        }
+      }
+    }
+  }
+}
+
 int fused_launches(const FusedBatch &B, int phases) {
   int k = B.grid_form ? 1 : 2;  // k_batch_iter_end, and k_batch_plan for the persistent form
   for (int ph = 0; ph < 2; ++ph)
@@ -1792,14 +1840,9 @@ int fused_graph(FusedBatch &B, int phases) {
   CK(cudaStreamBeginCapture(B.s, cudaStreamCaptureModeThreadLocal));
   int st = NIM_OK;
   for (int k = 0; k < B.G && st == NIM_OK; ++k) {
-    if (B.grid_form) {
-      if (phases & 1) st = group_slots<float>(B);
-      if (st == NIM_OK && (phases & 2)) st = group_slots<double>(B);
-    } else {
-      k_batch_plan<<<1, 1024, 0, B.s>>>(B.args);
-      if (phases & 1) st = fused_slots_of<float>(B);
-      if (st == NIM_OK && (phases & 2)) st = fused_slots_of<double>(B);
-    }
+    k_batch_plan<<<1, 1024, 0, B.s>>>(B.args);
+    if (phases & 1) st = fused_slots_of<float>(B);
+    if (st == NIM_OK && (phases & 2)) st = fused_slots_of<double>(B);
     k_batch_iter_end<<<(B.n + 127) / 128, 128, 0, B.s>>>(B.args);
   }
   const cudaError_t e = cudaStreamEndCapture(B.s, &g);
@@ -1899,39 +1942,10 @@ int fused_setup(FusedBatch &B, int32_t n, nim_ctx *const *ctx) {
   B.state_dev_offset = ost;
   const char *form = std::getenv("NIM_BATCH_FORM");
   B.grid_form = form && std::string(form) == "grid";
-  if (B.grid_form) {
-    for (int ph = 0; ph < 2; ++ph) {
-      if (ph == 0 && !B.mixed) continue;
-      for (int q = 0; q < BS_COUNT; ++q) {
-        if (!B.use[ph][q]) continue;
-        for (int g0 = 0; g0 < n; g0 += kGroup) {
-          const int m = std::min(kGroup, n - g0);
-          auto fill = [&](auto &L, const auto &h) {
-            L.n = m;
-            L.ph = ph + 1;
-            L.first = g0;
-            L.phase = B.args.phase;
-            unsigned acc = 0;
-            for (int a = 0; a < m; ++a) {
-              const BatchGrid gr = grids[((size_t)ph * n + g0 + a) * BS_COUNT + q];
-              L.off[a] = acc;
-              L.grid[a] = gr;
-              L.inst[a] = h[g0 + a];
-              acc += gr.x * gr.y * gr.z;
-            }
-            L.off[m] = acc;
-            return acc;
-          };
-          if (ph == 0) {
-            B.grp32[q].emplace_back();
-            if (fill(B.grp32[q].back(), h32) == 0) B.grp32[q].pop_back();
-          } else {
-            B.grp64[q].emplace_back();
-            if (fill(B.grp64[q].back(), h64) == 0) B.grp64[q].pop_back();
-          }
-        }
-      }
-    }
+  if (B.grid_form) {  // kept for the groups (fused_groups)
+    B.grids = grids;
+    B.h64 = h64;
+    B.h32 = h32;
   }
   int sms = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx[0]->device));
@@ -2005,6 +2019,7 @@ extern "C" int nim_batch_step_fused(int32_t n, nim_ctx *const *ctx, int32_t nste
   };
   for (int32_t i = 0; i < n; ++i) TRY(start_step(i));
   TRY(fused_upload_phase(B));
+  bool regroup = true;  // the grid form's groups follow the phases
   for (;;) {
     int phases = 0, busy = 0;
     for (int32_t i = 0; i < n; ++i) {
@@ -2013,8 +2028,20 @@ extern "C" int nim_batch_step_fused(int32_t n, nim_ctx *const *ctx, int32_t nste
     }
     if (!busy) break;
     if (phases) {
-      TRY(fused_graph(B, phases));
-      CK(cudaGraphLaunch(B.graph[phases - 1], B.s));
+      if (B.grid_form) {
+        // the groups of this interval's enclosures, then G passes launched
+        // directly (the groups change as enclosures change phase)
+        if (regroup) fused_groups(B, ph);
+        regroup = false;
+        for (int k = 0; k < B.G; ++k) {
+          if (phases & 1) TRY(group_slots<float>(B));
+          if (phases & 2) TRY(group_slots<double>(B));
+          k_batch_iter_end<<<(n + 127) / 128, 128, 0, B.s>>>(B.args);
+        }
+      } else {
+        TRY(fused_graph(B, phases));
+        CK(cudaGraphLaunch(B.graph[phases - 1], B.s));
+      }
       ctx[0]->launches += (long long)B.G * fused_launches(B, phases);
       for (int32_t i = 0; i < n; ++i)
         if (st[i] == RUN) ctx[i]->run.launched += B.G;
@@ -2066,6 +2093,7 @@ extern "C" int nim_batch_step_fused(int32_t n, nim_ctx *const *ctx, int32_t nste
       }
     }
     if (changed) TRY(fused_upload_phase(B));
+    regroup = regroup || changed;
   }
   return first_error;
 }
