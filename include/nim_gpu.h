@@ -278,7 +278,11 @@ int nim_batch_step(int32_t n, nim_ctx *const *ctx, int32_t nsteps, nim_step_stat
    one device, parallel schedule, formulation 2, the same precision, at
    most 256 (NIM_ERR_BAD_ARG otherwise).  While the call runs, the
    contexts' work goes to a stream of its own; each context's stream is
-   synchronised at entry and given back at return. */
+   synchronised at entry and given back at return.  With the environment
+   variable NIM_BATCH_FORM=grid the kernels run instead as plain launches
+   over groups of up to 40 enclosures whose arguments are kernel
+   parameters, regrouped as enclosures change precision (faster for FP64
+   batches); the results are the same bits. */
 int nim_batch_step_fused(int32_t n, nim_ctx *const *ctx, int32_t nsteps, nim_step_stats *per, int32_t *done);
 
 /* ---- z-slab decomposition (no counterpart in the reference, which runs
